@@ -1,0 +1,196 @@
+"""Synthetic scenes and ray batches for the workloads the backend is measured on.
+
+All inputs are generated from seeds (no datasets exist for this path). Geometry is an FP32
+triangle soup (n, 9): v0.xyz v1.xyz v2.xyz; triangle ids are soup indices.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import types as T
+
+
+@dataclass
+class Scene:
+    verts: np.ndarray                      # (n, 9) float32
+    tri_material: np.ndarray               # (n,) uint32
+    materials: list = field(default_factory=list)   # dicts: type, rgb, roughness, eta, k
+    lights: list = field(default_factory=list)      # dicts: type, tri, radiance, radius, center
+    camera: dict | None = None             # position, look_at, up, vfov, width, height
+
+    @property
+    def n_tri(self) -> int:
+        return int(self.verts.shape[0])
+
+    def materials_array(self):
+        arr = (T.fl_material * max(1, len(self.materials)))()
+        for i, m in enumerate(self.materials):
+            arr[i].type = m.get("type", T.FL_MAT_LAMBERT)
+            arr[i].rgb[:] = list(m.get("rgb", (0.5, 0.5, 0.5)))
+            arr[i].roughness = m.get("roughness", 0.0)
+            arr[i].eta = m.get("eta", 1.5)
+            arr[i].k = m.get("k", 0.0)
+        return arr
+
+    def lights_array(self):
+        arr = (T.fl_light * max(1, len(self.lights)))()
+        for i, l in enumerate(self.lights):
+            arr[i].type = l["type"]
+            arr[i].tri = l.get("tri", 0)
+            arr[i].radiance = l["radiance"]
+            arr[i].radius = l.get("radius", 0.0)
+            arr[i].center[:] = list(l.get("center", (0.0, 0.0, 0.0)))
+        return arr
+
+    def desc(self):
+        """fl_scene_desc plus the buffers it points to (keep the tuple alive while used)."""
+        verts = np.ascontiguousarray(self.verts, dtype=np.float32)
+        tm = np.ascontiguousarray(self.tri_material, dtype=np.uint32)
+        mats = self.materials_array()
+        lights = self.lights_array()
+        d = T.fl_scene_desc()
+        d.verts = verts.ctypes.data_as(C.POINTER(C.c_float))
+        d.n_tri = verts.shape[0]
+        d.tri_material = tm.ctypes.data_as(C.POINTER(C.c_uint32))
+        d.materials = C.cast(mats, C.POINTER(T.fl_material))
+        d.n_materials = len(self.materials)
+        d.lights = C.cast(lights, C.POINTER(T.fl_light))
+        d.n_lights = len(self.lights)
+        return d, (verts, tm, mats, lights)
+
+    def camera_struct(self, width=None, height=None):
+        c = self.camera
+        cam = T.fl_camera()
+        cam.position[:] = list(c["position"])
+        cam.look_at[:] = list(c["look_at"])
+        cam.up[:] = list(c.get("up", (0.0, 1.0, 0.0)))
+        cam.vfov_deg = c["vfov"]
+        cam.width = width or c["width"]
+        cam.height = height or c["height"]
+        return cam
+
+
+def render_params(spp, max_depth, mode=T.FL_SPECTRAL_HERO4, rr=1.0, wave_paths=0, sample_offset=0):
+    p = T.fl_render_params()
+    p.spp = spp
+    p.max_depth = max_depth
+    p.rr_threshold = rr
+    p.spectral_mode = mode
+    p.wave_paths = wave_paths
+    p.sample_offset = sample_offset
+    return p
+
+
+# ----------------------------------------------------------------------------- geometry helpers
+
+def _quad(p0, p1, p2, p3):
+    """two triangles (p0,p1,p2), (p0,p2,p3); normal = (p1-p0) x (p2-p0)"""
+    return [list(p0) + list(p1) + list(p2), list(p0) + list(p2) + list(p3)]
+
+
+def _box(cx, cz, sx, sy, sz, angle_deg):
+    """axis box of size (sx, sy, sz) standing on y = 0, centred at (cx, cz), rotated about y."""
+    a = math.radians(angle_deg)
+    ca, sa = math.cos(a), math.sin(a)
+
+    def P(x, y, z):
+        dx, dz = x - cx, z - cz
+        return (cx + dx * ca + dz * sa, y, cz - dx * sa + dz * ca)
+
+    x0, x1 = cx - sx / 2, cx + sx / 2
+    z0, z1 = cz - sz / 2, cz + sz / 2
+    y0, y1 = 0.0, sy
+    c = [P(x0, y0, z0), P(x1, y0, z0), P(x1, y0, z1), P(x0, y0, z1),
+         P(x0, y1, z0), P(x1, y1, z0), P(x1, y1, z1), P(x0, y1, z1)]
+    faces = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (2, 3, 7, 6), (1, 2, 6, 5), (3, 0, 4, 7)]
+    tris = []
+    for f in faces:
+        tris += _quad(*(c[i] for i in f))
+    return tris
+
+
+def cornell(width=256, height=256) -> Scene:
+    """Cornell-style box of 36 triangles (unit-cube room open at z = 0, two rotated boxes,
+    0.25 x 0.25 ceiling light at y = 0.999 facing down with constant spectral radiance 10)."""
+    tris, mats = [], []
+    WHITE, RED, GREEN = 0, 1, 2
+    # floor, ceiling, back wall (white)
+    tris += _quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)); mats += [WHITE] * 2
+    tris += _quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1)); mats += [WHITE] * 2
+    tris += _quad((0, 0, 1), (0, 1, 1), (1, 1, 1), (1, 0, 1)); mats += [WHITE] * 2
+    # image-left wall (x = 0, red), image-right wall (x = 1, green)
+    tris += _quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)); mats += [RED] * 2
+    tris += _quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)); mats += [GREEN] * 2
+    # short box (front, image right), tall box (back, image left)
+    tris += _box(0.66, 0.37, 0.3, 0.3, 0.3, -17.0); mats += [WHITE] * 12
+    tris += _box(0.33, 0.67, 0.3, 0.6, 0.3, 17.0); mats += [WHITE] * 12
+    # light quad, normal (0, -1, 0)
+    h, lo, hi = 0.999, 0.375, 0.625
+    light_first = len(tris)
+    tris += _quad((lo, h, lo), (hi, h, lo), (hi, h, hi), (lo, h, hi)); mats += [WHITE] * 2
+    verts = np.asarray(tris, dtype=np.float32)
+    materials = [
+        {"type": T.FL_MAT_LAMBERT, "rgb": (0.725, 0.725, 0.725)},
+        {"type": T.FL_MAT_LAMBERT, "rgb": (0.63, 0.065, 0.05)},
+        {"type": T.FL_MAT_LAMBERT, "rgb": (0.14, 0.45, 0.091)},
+    ]
+    lights = [{"type": T.FL_LIGHT_TRIANGLE, "tri": light_first + k, "radiance": 10.0} for k in range(2)]
+    cam = {"position": (0.5, 0.5, -1.4), "look_at": (0.5, 0.5, 0.0), "up": (0.0, 1.0, 0.0), "vfov": 40.0,
+           "width": width, "height": height}
+    return Scene(verts, np.asarray(mats, dtype=np.uint32), materials, lights, cam)
+
+
+# ----------------------------------------------------------------------------- ray-cast microbenchmark
+
+def triangle_soup(n_tri: int, seed: int = 1, sigma: float = 0.002) -> np.ndarray:
+    """n_tri triangles: centroids uniform in [0,1]^3, vertex = centroid + N(0, sigma^2) per component."""
+    rng = np.random.default_rng(seed)
+    c = rng.random((n_tri, 1, 3), dtype=np.float32)
+    e = rng.standard_normal((n_tri, 3, 3), dtype=np.float32) * np.float32(sigma)
+    return (c + e).reshape(n_tri, 9).astype(np.float32)
+
+
+def incoherent_rays(n: int, seed: int = 2, lo: float = -0.1, hi: float = 1.1):
+    """origins uniform in [lo, hi]^3, directions uniform on the sphere, tmin 0, tmax +inf."""
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
+    z = rng.uniform(-1.0, 1.0, n)
+    phi = rng.uniform(0.0, 2.0 * math.pi, n)
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    d = np.stack([r * np.cos(phi), r * np.sin(phi), z], axis=1).astype(np.float32)
+    org = np.empty((n, 4), np.float32)
+    dirs = np.empty((n, 4), np.float32)
+    org[:, :3] = o
+    org[:, 3] = 0.0
+    dirs[:, :3] = d
+    dirs[:, 3] = np.inf
+    return org, dirs
+
+
+def coherent_rays(width: int, height: int, position=(0.5, 0.5, -1.0), look_at=(0.5, 0.5, 0.5), vfov=60.0):
+    """pinhole primary rays through pixel centres, row 0 at the top."""
+    pos = np.asarray(position, np.float64)
+    w = pos - np.asarray(look_at, np.float64)
+    w /= np.linalg.norm(w)
+    u = np.cross([0.0, 1.0, 0.0], w)
+    u /= np.linalg.norm(u)
+    v = np.cross(w, u)
+    hh = math.tan(math.radians(vfov) / 2)
+    hw = hh * width / height
+    xs = (np.arange(width) + 0.5) / width
+    ys = 1.0 - (np.arange(height) + 0.5) / height
+    X, Y = np.meshgrid(xs, ys)
+    d = (-w[None, None, :] + (2 * X[..., None] - 1) * hw * u[None, None, :] + (2 * Y[..., None] - 1) * hh * v[None, None, :])
+    d /= np.linalg.norm(d, axis=-1, keepdims=True)
+    n = width * height
+    org = np.empty((n, 4), np.float32)
+    dirs = np.empty((n, 4), np.float32)
+    org[:, :3] = pos.astype(np.float32)
+    org[:, 3] = 0.0
+    dirs[:, :3] = d.reshape(n, 3).astype(np.float32)
+    dirs[:, 3] = np.inf
+    return org, dirs

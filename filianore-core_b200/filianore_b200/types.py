@@ -1,0 +1,129 @@
+"""ctypes mirrors of the structs in include/filianore_gpu.h (the C ABI)."""
+import ctypes as C
+
+FL_OK = 0
+FL_ERR_INVALID = -1
+FL_ERR_OOM = -2
+FL_ERR_CUDA = -3
+FL_ERR_TIMEOUT = -4
+FL_ERR_TRAVERSAL = -5
+FL_ERR_NOT_READY = -6
+FL_ERR_CAPACITY = -7
+FL_ERR_NO_DEVICE = -8
+
+FL_MEM_HOST = 0
+FL_MEM_DEVICE = 1
+
+FL_MAT_LAMBERT = 0
+FL_MAT_CONDUCTOR = 1
+FL_MAT_ROUGH_DIELECTRIC = 2
+FL_MAT_SMOOTH_DIELECTRIC = 3
+
+FL_LIGHT_TRIANGLE = 0
+FL_LIGHT_SPHERE = 1
+FL_LIGHT_ENV = 2
+
+FL_SPECTRAL_HERO4 = 0
+FL_SPECTRAL_BINS60 = 1
+
+
+class fl_spectral_tables(C.Structure):
+    _fields_ = [
+        ("cie_lambda", C.POINTER(C.c_float)),
+        ("cie_x", C.POINTER(C.c_float)),
+        ("cie_y", C.POINTER(C.c_float)),
+        ("cie_z", C.POINTER(C.c_float)),
+        ("n_cie", C.c_int32),
+        ("cie_y_integral", C.c_float),
+        ("rgb2spec_lambda", C.POINTER(C.c_float)),
+        ("n_rgb2spec", C.c_int32),
+        ("refl", C.POINTER(C.c_float) * 7),
+        ("illum", C.POINTER(C.c_float) * 7),
+    ]
+
+
+class fl_material(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("rgb", C.c_float * 3),
+        ("roughness", C.c_float),
+        ("eta", C.c_float),
+        ("k", C.c_float),
+        ("reserved", C.c_float),
+    ]
+
+
+class fl_light(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("tri", C.c_uint32),
+        ("radiance", C.c_float),
+        ("radius", C.c_float),
+        ("center", C.c_float * 3),
+        ("reserved", C.c_float),
+    ]
+
+
+class fl_scene_desc(C.Structure):
+    _fields_ = [
+        ("verts", C.POINTER(C.c_float)),
+        ("n_tri", C.c_uint32),
+        ("tri_material", C.POINTER(C.c_uint32)),
+        ("materials", C.POINTER(fl_material)),
+        ("n_materials", C.c_uint32),
+        ("lights", C.POINTER(fl_light)),
+        ("n_lights", C.c_uint32),
+    ]
+
+
+class fl_scene_info(C.Structure):
+    _fields_ = [
+        ("n_tri", C.c_uint32),
+        ("n_nodes", C.c_uint32),
+        ("n_leaves", C.c_uint32),
+        ("max_depth", C.c_uint32),
+        ("bvh_bytes", C.c_uint64),
+        ("build_ms", C.c_double),
+    ]
+
+
+class fl_hit(C.Structure):
+    _fields_ = [("id", C.c_int32), ("t", C.c_float), ("u", C.c_float), ("v", C.c_float)]
+
+
+class fl_camera(C.Structure):
+    _fields_ = [
+        ("position", C.c_float * 3),
+        ("look_at", C.c_float * 3),
+        ("up", C.c_float * 3),
+        ("vfov_deg", C.c_float),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+    ]
+
+
+class fl_render_params(C.Structure):
+    _fields_ = [
+        ("spp", C.c_int32),
+        ("max_depth", C.c_int32),
+        ("rr_threshold", C.c_float),
+        ("spectral_mode", C.c_int32),
+        ("wave_paths", C.c_int32),
+        ("sample_offset", C.c_uint32),
+        ("reserved", C.c_int32 * 2),
+    ]
+
+
+class fl_render_stats(C.Structure):
+    _fields_ = [
+        ("paths", C.c_uint64),
+        ("rays", C.c_uint64),
+        ("shadow_rays", C.c_uint64),
+        ("bounces", C.c_uint64),
+        ("ms", C.c_double),
+        ("traversal_errors", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+HIT_DTYPE = [("id", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")]

@@ -1,0 +1,238 @@
+/*
+ * filianore_gpu.h — C ABI of the B200 (sm_100a) spectral path-tracing backend.
+ *
+ * The reference (filianore-core, C++17) renders with a per-ray virtual call chain:
+ *   application loop -> Integrator::Li            src/filianore/integrators/integrator.h:17-18
+ *                    -> Scene::intersect          src/filianore/core/scene.h:24
+ *                    -> BVH::intersect            src/filianore/bvh/bvh.h:41 (embree4 rtcIntersect1)
+ * A GPU cannot be driven one ray at a time, so this ABI replaces that chain at two
+ * granularities:
+ *   - batch intersection (fl_trace_closest / fl_trace_occluded) replaces BVH::intersect
+ *     and rtcIntersect1 one-for-one, on arrays of rays;
+ *   - whole-image rendering (fl_render) replaces the absent application's loop over
+ *     pixels and samples that calls PathIntegrator::Li.
+ *
+ * Conventions (all functions):
+ *   - every call returns fl_status: FL_OK (0) or a negative error code; no exceptions
+ *     cross the boundary; fl_status_string() names a code, fl_last_error() gives detail;
+ *   - handles are opaque; the caller owns every buffer it passes, the library owns the
+ *     device memory behind a handle;
+ *   - pointers marked "host or device" are interpreted according to the `memory`
+ *     argument (FL_MEM_HOST: pageable or pinned host memory, copied inside the call;
+ *     FL_MEM_DEVICE: device pointers on the context's device, used in place);
+ *   - calls on one handle are serialised by an internal mutex; `stream` may be NULL
+ *     (the context's own stream) or a cudaStream_t cast to void*.
+ */
+#ifndef FILIANORE_GPU_H
+#define FILIANORE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t fl_status;
+
+enum {
+    FL_OK = 0,
+    FL_ERR_INVALID = -1,     /* bad argument (null pointer, size, enum value) */
+    FL_ERR_OOM = -2,         /* device or host allocation failed */
+    FL_ERR_CUDA = -3,        /* a CUDA runtime call failed; fl_last_error has the text */
+    FL_ERR_TIMEOUT = -4,     /* a bounded wait (host poll) ran out */
+    FL_ERR_TRAVERSAL = -5,   /* a traversal hit its stack or iteration bound; results partial */
+    FL_ERR_NOT_READY = -6,   /* serving: job not finished yet */
+    FL_ERR_CAPACITY = -7,    /* serving: queue or memory budget full, job not admitted */
+    FL_ERR_NO_DEVICE = -8    /* no CUDA device / kernel image missing for this GPU */
+};
+
+enum { FL_MEM_HOST = 0, FL_MEM_DEVICE = 1 };
+
+typedef struct fl_context fl_context;
+typedef struct fl_scene fl_scene;
+
+/* ------------------------------------------------------------------------- */
+/* Spectral tables                                                           */
+/* ------------------------------------------------------------------------- */
+/*
+ * The spectral data are supplied by the caller, exactly as the reference holds them in
+ * src/filianore/color/cie.h:8-951 (CIE 1931 2-degree observer at 1 nm over 360..830 nm,
+ * and the seven reflectance and seven illuminant RGB-to-spectrum basis curves sampled at
+ * 32 wavelengths over 380..720 nm). A reference-side integration passes those arrays
+ * directly (CIE_Wavelength, CIE_X, ..., RGBRefl2SpectWhite, ...). The library derives
+ * the 60-bin tables the reference builds in InitializeSpectrals
+ * (src/filianore/color/spectruminits.cpp:6-64) from them.
+ * Basis order in refl[] / illum[]: white, cyan, magenta, yellow, red, green, blue.
+ */
+typedef struct {
+    const float *cie_lambda; /* n_cie wavelengths (nm) */
+    const float *cie_x;
+    const float *cie_y;
+    const float *cie_z;
+    int32_t n_cie;           /* 471 in the reference */
+    float cie_y_integral;    /* 106.856895 in the reference (cie.h:11) */
+    const float *rgb2spec_lambda; /* n_rgb2spec wavelengths (nm) */
+    int32_t n_rgb2spec;      /* 32 in the reference */
+    const float *refl[7];
+    const float *illum[7];
+} fl_spectral_tables;
+
+/* ------------------------------------------------------------------------- */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------- */
+/* Replaces the global InitializeSpectrals() call (spectruminits.cpp:6) plus embree's
+ * rtcNewDevice (bvh.h:25-28): binds a CUDA device, uploads the spectral tables. */
+fl_status fl_context_create(int32_t device, const fl_spectral_tables *tables, fl_context **out);
+fl_status fl_context_destroy(fl_context *ctx);
+const char *fl_status_string(fl_status status);
+/* Copies the last error message of this context (or of the process when ctx is NULL). */
+fl_status fl_last_error(const fl_context *ctx, char *buf, size_t buf_len);
+
+/* The 60-bin tables the library derived from the caller's tables, for inspection:
+ * out has room for 17*60 floats in the order X, Y, Z, refl[0..6], illum[0..6]. */
+fl_status fl_context_binned_tables(const fl_context *ctx, float *out, size_t n_floats);
+
+/* ------------------------------------------------------------------------- */
+/* Scene                                                                     */
+/* ------------------------------------------------------------------------- */
+enum {
+    FL_MAT_LAMBERT = 0,          /* LambertMaterial            shading/materials/lambert.cpp:9-17 */
+    FL_MAT_CONDUCTOR = 1,        /* GGX MicrofacetReflection + FresnelConductor
+                                    shading/bxdfs/microfacetreflection.cpp, fresnel/fresnelconductor.cpp */
+    FL_MAT_ROUGH_DIELECTRIC = 2, /* GGX reflection + MicrofacetTransmission, FresnelDielectric
+                                    shading/closures/microfacettransmission.cpp */
+    FL_MAT_SMOOTH_DIELECTRIC = 3 /* FresnelSpecular              shading/closures/fresnelspecular.cpp */
+};
+
+typedef struct {
+    int32_t type;       /* FL_MAT_* */
+    float rgb[3];       /* reflectance (Lambert albedo / conductor tint / dielectric tint), upsampled
+                           with from_reflectance_rgb (color/spectrumoperations.cpp:113-147) */
+    float roughness;    /* alpha = roughness^2 (materials/standardsurface.cpp:104-106) */
+    float eta;          /* dielectric IOR, or conductor eta */
+    float k;            /* conductor absorption */
+    float reserved;
+} fl_material;
+
+enum {
+    FL_LIGHT_TRIANGLE = 0, /* DiffuseAreaIlluminant over one scene triangle (illuminants/diffusearea.cpp) */
+    FL_LIGHT_SPHERE = 1,   /* analytic sphere emitter (no reference class) */
+    FL_LIGHT_ENV = 2       /* constant environment radiance (no reference class) */
+};
+
+typedef struct {
+    int32_t type;          /* FL_LIGHT_* */
+    uint32_t tri;          /* FL_LIGHT_TRIANGLE: index of the emitting triangle in the soup */
+    float radiance;        /* constant spectral radiance (color * intensity in the reference) */
+    float radius;          /* FL_LIGHT_SPHERE */
+    float center[3];       /* FL_LIGHT_SPHERE */
+    float reserved;
+} fl_light;
+
+typedef struct {
+    const float *verts;             /* n_tri * 9 floats: v0.xyz v1.xyz v2.xyz, FP32 soup */
+    uint32_t n_tri;
+    const uint32_t *tri_material;   /* n_tri material indices, NULL = all 0 */
+    const fl_material *materials;
+    uint32_t n_materials;
+    const fl_light *lights;         /* order = the reference's Scene::illuminants order */
+    uint32_t n_lights;
+} fl_scene_desc;
+
+typedef struct {
+    uint32_t n_tri;
+    uint32_t n_nodes;          /* wide (8-ary) BVH nodes */
+    uint32_t n_leaves;
+    uint32_t max_depth;        /* deepest wide level */
+    uint64_t bvh_bytes;        /* node + triangle arrays in HBM */
+    double build_ms;           /* device build time (CUDA events) */
+} fl_scene_info;
+
+/* Replaces Scene::Scene + BVH::initialize_scene_geometry/finalise (core/scene.cpp:7-19,
+ * bvh/bvh.cpp:7-47): uploads the soup (host pointers) and builds the 8-wide BVH on the
+ * device. Triangle ids reported by traces are soup indices (= embree geomID order). */
+fl_status fl_scene_create(fl_context *ctx, const fl_scene_desc *desc, fl_scene **out);
+fl_status fl_scene_destroy(fl_scene *scene);
+fl_status fl_scene_get_info(const fl_scene *scene, fl_scene_info *info);
+
+/* ------------------------------------------------------------------------- */
+/* Batch ray queries                                                         */
+/* ------------------------------------------------------------------------- */
+/* Rays are SoA of float4: org_tmin[4*i..] = (ox, oy, oz, tmin), dir_tmax[4*i..] = (dx, dy, dz, tmax).
+ * A hit is 16 bytes: int32 triangle id (-1 = miss), float t, float u, float v where
+ * p = (1-u-v)*v0 + u*v1 + v*v2 (embree's barycentric convention). Intersection is
+ * watertight and double-sided; a hit needs tmin < t < tmax; equal t resolves to the
+ * lower triangle id. */
+typedef struct {
+    int32_t id;
+    float t, u, v;
+} fl_hit;
+
+/* Replaces BVH::intersect / rtcIntersect1 (bvh/bvh.cpp:49-84) for n rays. */
+fl_status fl_trace_closest(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
+                           fl_hit *hits, int32_t memory, void *stream);
+
+/* Shadow query with the reference's visibility rule (illuminants/illuminant.cpp:40-50):
+ * occluded[i] = 0 when the ray hits nothing in (tmin, tmax) or its closest hit is an
+ * emissive triangle, else 1. */
+fl_status fl_trace_occluded(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
+                            uint8_t *occluded, int32_t memory, void *stream);
+
+/* Traversal statistics of the last trace on this scene (device counters, instrumented
+ * launch): total wide nodes and triangles visited. */
+fl_status fl_trace_count(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
+                         int32_t memory, uint64_t *nodes_visited, uint64_t *tris_tested);
+
+/* ------------------------------------------------------------------------- */
+/* Rendering                                                                 */
+/* ------------------------------------------------------------------------- */
+/* PhysicalCamera (cameras/physical.h:11-43) with aperture 0 (a pinhole) and
+ * flipCameraDirection = true, the orientation in which it looks towards look_at (with
+ * false it faces away from look_at). Image column 0 lies towards -u, u = up x forward. */
+typedef struct {
+    float position[3];
+    float look_at[3];
+    float up[3];
+    float vfov_deg;
+    int32_t width, height;
+} fl_camera;
+
+enum {
+    FL_SPECTRAL_HERO4 = 0,  /* 4 hero wavelengths in 380..720 nm, rotation by 85 nm */
+    FL_SPECTRAL_BINS60 = 1  /* the reference's 60 fixed bins over 400..700 nm (principalspectrum.h:7-9) */
+};
+
+typedef struct {
+    int32_t spp;            /* samples per pixel */
+    int32_t max_depth;      /* RenderParams diffuse = reflection = transmission depth (core/renderparams.h:5-10) */
+    float rr_threshold;     /* PathIntegrator rrThreshold (pathintegrator.h:11-12), 1 by default */
+    int32_t spectral_mode;  /* FL_SPECTRAL_* */
+    int32_t wave_paths;     /* paths in flight per wavefront (0 = library default) */
+    uint32_t sample_offset; /* first sample index (progressive / multi-GPU sample split) */
+    int32_t reserved[2];
+} fl_render_params;
+
+typedef struct {
+    uint64_t paths;          /* camera samples completed */
+    uint64_t rays;           /* all rays traced: camera + continuation + shadow + MIS */
+    uint64_t shadow_rays;
+    uint64_t bounces;        /* path vertices shaded */
+    double ms;               /* device time of the render (CUDA events) */
+    uint32_t traversal_errors;
+    uint32_t reserved;
+} fl_render_stats;
+
+/* Renders the image: for pixel p and sample s the PCG32 stream is seeded with
+ * (initstate = p, initseq = 1) and advanced by s * 2^16 draws. film_rgb receives
+ * width*height*3 linear Rec.709 floats (the mean over samples of
+ * xyz_to_rgb(to_xyz(Li)), color/spectrumoperations.cpp:58-66,193-212), row 0 at the top.
+ * film_xyz64 (nullable) receives the FP64 XYZ sums (not divided by spp). */
+fl_status fl_render(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
+                    float *film_rgb, double *film_xyz64, int32_t memory, fl_render_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FILIANORE_GPU_H */

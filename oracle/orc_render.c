@@ -1,0 +1,953 @@
+/*
+ * ORACLE — test infrastructure only.
+ *
+ * CPU restatement of the reference's path integrator with its BSDFs and lights, one
+ * camera sample at a time, in the reference's operation order:
+ *   PathIntegrator::Li            src/filianore/integrators/pathintegrator.cpp:12-87
+ *   uniform_sample_all_lights     src/filianore/integrators/integrator.cpp:10-23
+ *   estimate_direct               src/filianore/integrators/integrator.cpp:25-110
+ *   power_heuristic               src/filianore/sampling/sampling.cpp:18-23
+ *   BSDF evaluate/sample/pdf      src/filianore/shading/bsdf.cpp:6-151
+ *   LambertBRDF                   src/filianore/shading/bxdfs/lambert.cpp:6-25
+ *   concentric disk / cosine      src/filianore/core/shadingcore.h:65-89
+ *   GGX D / Lambda / VNDF         src/filianore/shading/microfacets/ggx.cpp:12-57
+ *   G, pdf                        src/filianore/shading/microfacets/microfacet.cpp:6-17
+ *   MicrofacetReflectionBRDF      src/filianore/shading/bxdfs/microfacetreflection.cpp:13-61
+ *   MicrofacetTransmissionBRDF    src/filianore/shading/closures/microfacettransmission.cpp:70-239
+ *   FresnelSpecularBXDF           src/filianore/shading/closures/fresnelspecular.cpp:18-53
+ *   FresnelDielectric/Conductor   src/filianore/shading/fresnel/fresneldielectric.cpp:8-38,
+ *                                 src/filianore/shading/fresnel/fresnelconductor.cpp:9-33
+ *   DiffuseAreaIlluminant         src/filianore/illuminants/diffusearea.cpp:12-39
+ *   Shape::sample / Shape::pdf    src/filianore/shapes/shape.cpp:13-41
+ *   Triangle::intersect / sample  src/filianore/shapes/triangle.cpp:13-154
+ *   VisibilityEvaluator           src/filianore/illuminants/illuminant.cpp:40-50
+ *   PhysicalCamera                src/filianore/cameras/physical.h:11-43, physical.cpp:4-22
+ * The BVH hit record follows BVH::intersect (src/filianore/bvh/bvh.cpp:49-84) with the
+ * primitive and shading normal filled in (its pError is gamma<int>(5) == 0).
+ *
+ * Features the reference lacks (environment light, analytic sphere light, hero
+ * wavelengths, the render loop and its PCG32 seeding) are this project's own
+ * definitions, shared with the GPU backend.
+ */
+#include "oracle.h"
+
+#include <pthread.h>
+#include <stdlib.h>
+
+#define NL_MAX ORC_MAXLAMBDA
+#define INF_F (__builtin_inff())
+
+enum {
+    BSDF_REFLECTION = 1 << 0,
+    BSDF_TRANSMISSION = 1 << 1,
+    BSDF_DIFFUSE = 1 << 2,
+    BSDF_GLOSSY = 1 << 3,
+    BSDF_SPECULAR = 1 << 4,
+    BSDF_ALL = 31
+};
+
+typedef struct { float c[NL_MAX]; } spec;
+
+typedef struct {
+    const fl_scene_desc *sc;
+    const orc_tables *tab;
+    orc_bvh *bvh;
+    int32_t *tri_light;  /* light index per triangle or -1 */
+    int mode, nl;
+    spec *mat_refl60;    /* per material, 60-bin reflectance (BINS60 mode) */
+    int has_env;
+    float env_radiance;
+    int emissive_tris;
+} scene_ctx;
+
+/* ---------------------------------------------------------------- spectra */
+static inline void sp_set(spec *s, int nl, float v) { for (int i = 0; i < nl; ++i) s->c[i] = v; }
+static inline int sp_black(const spec *s, int nl) {
+    for (int i = 0; i < nl; ++i) if (s->c[i] != 0.f) return 0;
+    return 1;
+}
+static inline float sp_max(const spec *s, int nl) {
+    float m = s->c[0];
+    for (int i = 1; i < nl; ++i) m = m > s->c[i] ? m : s->c[i];
+    return m;
+}
+
+/* ---------------------------------------------------------------- rays / hits */
+typedef struct { v3 o, d; float tmin, tmax; } ray3;
+
+typedef struct {
+    float t;
+    v3 p, pError, wo, n, ns;
+    int32_t prim;   /* triangle id, or -2 - light index for a sphere-light hit */
+} isect_t;
+
+static float sphere_hit(const fl_light *L, const ray3 *r) {
+    /* analytic sphere: smallest root in (tmin, tmax), geometric form */
+    v3 c = v3m(L->center[0], L->center[1], L->center[2]);
+    v3 oc = v3_sub(r->o, c);
+    float a = v3_dot(r->d, r->d);
+    float b = v3_dot(oc, r->d);
+    float cc = v3_dot(oc, oc) - L->radius * L->radius;
+    float disc = b * b - a * cc;
+    if (disc < 0.f || a == 0.f) return -1.f;
+    float sq = sqrtf(disc);
+    float t0 = (-b - sq) / a, t1 = (-b + sq) / a;
+    if (t0 > r->tmin && t0 < r->tmax) return t0;
+    if (t1 > r->tmin && t1 < r->tmax) return t1;
+    return -1.f;
+}
+
+/* Scene::intersect -> BVH::intersect, plus analytic sphere lights */
+static int scene_intersect(const scene_ctx *S, const ray3 *r, isect_t *is, uint64_t *rays) {
+    float ot[4] = {r->o.x, r->o.y, r->o.z, r->tmin};
+    float dt[4] = {r->d.x, r->d.y, r->d.z, r->tmax};
+    orc_ray rr;
+    orc_ray_precompute(ot, dt, &rr);
+    float t, u, v;
+    int32_t id = orc_bvh_closest(S->bvh, &rr, &t, &u, &v, NULL, NULL);
+    ++*rays;
+    float best = id >= 0 ? t : r->tmax;
+    int32_t sphere = -1;
+    for (uint32_t l = 0; l < S->sc->n_lights; ++l) {
+        const fl_light *L = &S->sc->lights[l];
+        if (L->type != FL_LIGHT_SPHERE) continue;
+        ray3 r2 = *r;
+        r2.tmax = best;
+        float ts = sphere_hit(L, &r2);
+        if (ts > 0.f && ts < best) { best = ts; sphere = (int32_t)l; }
+    }
+    if (id < 0 && sphere < 0) return 0;
+    is->t = best;
+    is->p = v3_add(r->o, v3_mul(r->d, best));
+    is->pError = v3m(0.f, 0.f, 0.f);
+    is->wo = v3_norm(v3_neg(r->d));
+    if (sphere >= 0) {
+        const fl_light *L = &S->sc->lights[sphere];
+        is->n = v3_norm(v3_sub(is->p, v3m(L->center[0], L->center[1], L->center[2])));
+        is->prim = -2 - sphere;
+    } else {
+        const float *tv = S->sc->verts + 9 * (size_t)id;
+        v3 v0 = v3m(tv[0], tv[1], tv[2]), v1 = v3m(tv[3], tv[4], tv[5]), v2 = v3m(tv[6], tv[7], tv[8]);
+        is->n = v3_norm(v3_cross(v3_sub(v1, v0), v3_sub(v2, v0)));
+        is->prim = id;
+    }
+    is->ns = is->n;
+    return 1;
+}
+
+static int32_t prim_light(const scene_ctx *S, int32_t prim) {
+    if (prim >= 0) return S->tri_light[prim];
+    if (prim <= -2) return -2 - prim;
+    return -1;
+}
+
+/* ---------------------------------------------------------------- shading frame */
+typedef struct {
+    v3 ng, ns, s, t;
+    int type;        /* FL_MAT_* */
+    float eta;       /* BSDF::eta */
+    spec R;          /* reflectance */
+    float ax, ay;    /* GGX alphas */
+    float mat_eta, mat_k;
+    int nl;
+} bsdf_t;
+
+static v3 to_local(const bsdf_t *b, v3 v) { return v3m(v3_dot(v, b->s), v3_dot(v, b->t), v3_dot(v, b->ns)); }
+static v3 to_world(const bsdf_t *b, v3 v) {
+    return v3_add(v3_add(v3_mul(b->s, v.x), v3_mul(b->t, v.y)), v3_mul(b->ns, v.z));
+}
+
+static inline float cos2t(v3 w) { return w.z * w.z; }
+static inline float sin2t(v3 w) { float v = 1.f - cos2t(w); return v > 0.f ? v : 0.f; }
+static inline float sint(v3 w) { return sqrtf(sin2t(w)); }
+static inline float tant(v3 w) { return sint(w) / w.z; }
+static inline float tan2t(v3 w) { return sin2t(w) / cos2t(w); }
+static inline float clampf_ref(float v, float lo, float hi) { if (v < lo) return lo; return v > hi ? hi : v; }
+static inline float cosphi(v3 w) { float st = sint(w); return st == 0.f ? 1.f : clampf_ref(w.x / st, -1.f, 1.f); }
+static inline float sinphi(v3 w) { float st = sint(w); return st == 0.f ? 0.f : clampf_ref(w.y / st, -1.f, 1.f); }
+static inline float cos2phi(v3 w) { return cosphi(w) * cosphi(w); }
+static inline float sin2phi(v3 w) { return sinphi(w) * sinphi(w); }
+static inline int same_hemi(v3 a, v3 b) { return a.z * b.z > 0; }
+
+/* ---- GGX (ggx.cpp) */
+static float ggx_D(const bsdf_t *b, v3 wh) {
+    float tan2Theta = tan2t(wh);
+    if (isinf(tan2Theta)) return 0.f;
+    const float cos4Theta = cos2t(wh) * cos2t(wh);
+    float e = (cos2phi(wh) / (b->ax * b->ax) + sin2phi(wh) / (b->ay * b->ay)) * tan2Theta;
+    return 1.f / (ORC_PI * b->ax * b->ay * cos4Theta * (1 + e) * (1 + e));
+}
+static float ggx_lambda(const bsdf_t *b, v3 w) {
+    float absTanTheta = fabsf(tant(w));
+    if (isinf(absTanTheta)) return 0.f;
+    float alpha = sqrtf(cos2phi(w) * b->ax * b->ax + sin2phi(w) * b->ay * b->ay);
+    float a2t2 = (alpha * absTanTheta) * (alpha * absTanTheta);
+    return (-1 + sqrtf(1.f + a2t2)) / 2;
+}
+static float ggx_G(const bsdf_t *b, v3 wo, v3 wi) { return 1 / (1 + ggx_lambda(b, wo) + ggx_lambda(b, wi)); }
+static float ggx_pdf(const bsdf_t *b, v3 wo, v3 wh) { (void)wo; return ggx_D(b, wh) * fabsf(wh.z); }
+static v3 ggx_sample_wh(const bsdf_t *b, v3 wo, float ux, float uy) {
+    v3 vh = v3_norm(v3m(wo.x * b->ax, wo.y * b->ay, wo.z));
+    if (vh.z < 0) vh = v3_neg(vh);
+    float lensq = vh.x * vh.x + vh.y * vh.y;
+    v3 T1 = lensq > 0 ? v3_div(v3m(-vh.y, vh.x, 0.f), sqrtf(lensq)) : v3m(1.f, 0.f, 0.f);
+    v3 T2 = v3_cross(vh, T1);
+    float r = sqrtf(ux);
+    float phi = 2.f * ORC_PI * uy;
+    float t1 = r * cosf(phi);
+    float t2 = r * sinf(phi);
+    float s = (float)((1.f + vh.z) * 0.5);
+    t2 = (1.f - s) * sqrtf(1 - (t1 * t1)) + (s * t2);
+    float zz = 1.f - t1 * t1 - t2 * t2;
+    v3 Nh = v3_add(v3_add(v3_mul(T1, t1), v3_mul(T2, t2)), v3_mul(vh, sqrtf(zz > 0.f ? zz : 0.f)));
+    return v3_norm(v3m(b->ax * Nh.x, b->ay * Nh.y, Nh.z > 1e-6f ? Nh.z : 1e-6f));
+}
+
+/* ---- Fresnel (fresneldielectric.cpp:8-38 with local copies, fresnelconductor.cpp:9-33) */
+static float fr_dielectric(float cosThetaI, float etaI, float etaT) {
+    cosThetaI = clampf_ref(cosThetaI, -1.f, 1.f);
+    int enter = cosThetaI > 0.0;
+    if (!enter) { float tmp = etaI; etaI = etaT; etaT = tmp; cosThetaI = fabsf(cosThetaI); }
+    float m = 1.f - cosThetaI * cosThetaI;
+    float sinThetaI = sqrtf(m > 0.f ? m : 0.f);
+    float sinThetaT = etaI / etaT * sinThetaI;
+    if (sinThetaT >= 1) return 1.f;
+    float m2 = 1 - sinThetaT * sinThetaT;
+    float cosThetaT = sqrtf(m2 > 0.f ? m2 : 0.f);
+    float Rparl = (etaT * cosThetaI - etaI * cosThetaT) / (etaT * cosThetaI + etaI * cosThetaT);
+    float Rperp = (etaI * cosThetaI - etaT * cosThetaT) / (etaI * cosThetaI + etaT * cosThetaT);
+    return (float)((Rparl * Rparl + Rperp * Rperp) * 0.5);
+}
+static float fr_conductor(float cosI, float etaT_, float k_) {
+    /* constant eta/k over wavelength: every spectral sample is the same */
+    cosI = fabsf(cosI);
+    cosI = clampf_ref(cosI, -1.f, 1.f);
+    float eta = etaT_ / 1.f;
+    float etak = k_ / 1.f;
+    float cosThetaI2 = cosI * cosI;
+    float sinThetaI2 = (float)(1. - cosThetaI2);
+    float eta2 = eta * eta;
+    float etak2 = etak * etak;
+    float t0 = eta2 - etak2 - sinThetaI2;
+    float a2plusb2 = sqrtf(t0 * t0 + 4.f * eta2 * etak2);
+    float t1 = a2plusb2 + cosThetaI2;
+    float a = sqrtf(0.5f * (a2plusb2 + t0));
+    float t2 = (float)2 * cosI * a;
+    float Rs = (t1 - t2) / (t1 + t2);
+    float t3 = cosThetaI2 * a2plusb2 + sinThetaI2 * sinThetaI2;
+    float t4 = t2 * sinThetaI2;
+    float Rp = Rs * (t3 - t4) / (t3 + t4);
+    return 0.5f * (Rp + Rs);
+}
+
+/* ---- lobes. Lobe ids: 0 lambert, 1 microfacet reflection, 2 microfacet transmission, 3 fresnel specular */
+static int lobe_type(int lobe) {
+    switch (lobe) {
+    case 0: return BSDF_REFLECTION | BSDF_DIFFUSE;
+    case 1: return BSDF_REFLECTION | BSDF_GLOSSY;
+    case 2: return BSDF_TRANSMISSION | BSDF_GLOSSY;
+    default: return BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR;
+    }
+}
+static int bsdf_lobes(const bsdf_t *b, int *lobes) {
+    switch (b->type) {
+    case FL_MAT_LAMBERT: lobes[0] = 0; return 1;
+    case FL_MAT_CONDUCTOR: lobes[0] = 1; return 1;
+    case FL_MAT_ROUGH_DIELECTRIC: lobes[0] = 1; lobes[1] = 2; return 2;
+    default: lobes[0] = 3; return 1;
+    }
+}
+static int matches(int type, int flags) { return (type & flags) == type; }
+
+/* lobe evaluate (spectrum) */
+static void lobe_eval(const bsdf_t *b, int lobe, v3 wo, v3 wi, spec *out) {
+    int nl = b->nl;
+    if (lobe == 0) {
+        for (int i = 0; i < nl; ++i) out->c[i] = b->R.c[i] * ORC_INV_PI * 1.f;
+        return;
+    }
+    if (lobe == 1) {
+        float cosThetaO = fabsf(wo.z), cosThetaI = fabsf(wi.z);
+        v3 wh = v3_add(wi, wo);
+        if (cosThetaI == 0 || cosThetaO == 0 || (wh.x == 0 && wh.y == 0 && wh.z == 0)) { sp_set(out, nl, 0.f); return; }
+        wh = v3_norm(wh);
+        v3 whf = v3_dot(wh, v3m(0.f, 0.f, 1.f)) < 0.f ? v3_neg(wh) : wh;
+        float cF = v3_dot(wi, whf);
+        float F = b->type == FL_MAT_CONDUCTOR ? fr_conductor(cF, b->mat_eta, b->mat_k) : fr_dielectric(cF, 1.f, b->mat_eta);
+        float D = ggx_D(b, wh), G = ggx_G(b, wo, wi);
+        float den = 4.f * cosThetaO * cosThetaI;
+        for (int i = 0; i < nl; ++i) out->c[i] = b->R.c[i] * 1.f * D * G * F / den;
+        return;
+    }
+    if (lobe == 2) {
+        if (same_hemi(wo, wi)) { sp_set(out, nl, 0.f); return; }
+        float cosThetaO = wo.z, cosThetaI = wi.z;
+        if (cosThetaI == 0 || cosThetaO == 0) { sp_set(out, nl, 0.f); return; }
+        float eta = wo.z > 0 ? (b->mat_eta / 1.f) : (1.f / b->mat_eta);
+        v3 wh = v3_norm(v3_add(wo, v3_mul(wi, eta)));
+        if (wh.z < 0) wh = v3_neg(wh);
+        if (v3_dot(wo, wh) * v3_dot(wi, wh) > 0) { sp_set(out, nl, 0.f); return; }
+        float F = fr_dielectric(v3_dot(wo, wh), 1.f, b->mat_eta);
+        float sqrtDenom = v3_dot(wo, wh) + eta * v3_dot(wi, wh);
+        float factor = (1 / eta);
+        float v = fabsf(ggx_D(b, wh) * ggx_G(b, wo, wi) * eta * eta * v3_absdot(wi, wh) * v3_absdot(wo, wh) * factor * factor /
+                        (cosThetaI * cosThetaO * sqrtDenom * sqrtDenom));
+        for (int i = 0; i < nl; ++i) out->c[i] = (1.f - F) * b->R.c[i] * v;
+        return;
+    }
+    sp_set(out, nl, 0.f);
+}
+
+static float lobe_pdf(const bsdf_t *b, int lobe, v3 wo, v3 wi) {
+    if (lobe == 0) return same_hemi(wo, wi) ? fabsf(wi.z) * ORC_INV_PI : 0.f;
+    if (lobe == 1) {
+        if (!same_hemi(wo, wi)) return 0.f;
+        v3 wh = v3_norm(v3_add(wo, wi));
+        return ggx_pdf(b, wo, wh) / (4.f * v3_dot(wo, wh));
+    }
+    if (lobe == 2) {
+        if (same_hemi(wo, wi)) return 0.f;
+        float eta = wo.z > 0 ? (b->mat_eta / 1.f) : (1.f / b->mat_eta);
+        v3 wh = v3_norm(v3_add(wo, v3_mul(wi, eta)));
+        if (v3_dot(wo, wh) * v3_dot(wi, wh) > 0) return 0.f;
+        float sqrtDenom = v3_dot(wo, wh) + eta * v3_dot(wi, wh);
+        float dwh_dwi = fabsf((eta * eta * v3_dot(wi, wh)) / (sqrtDenom * sqrtDenom));
+        return ggx_pdf(b, wo, wh) * dwh_dwi;
+    }
+    return 0.f;
+}
+
+/* lobe sample; *type may be overwritten by the lobe (fresnel specular) */
+static void lobe_sample(const bsdf_t *b, int lobe, v3 wo, v3 *wi, float ux, float uy, float *pdf, int *type, spec *f) {
+    int nl = b->nl;
+    if (lobe == 0) {
+        /* concentric_sample_disk + cosine_hemisphere_sample, shadingcore.h:65-89 */
+        float ox = ux * 2.f - 1.f, oy = uy * 2.f - 1.f;
+        float dx, dy;
+        if (ox == 0 && oy == 0) { dx = 0.f; dy = 0.f; }
+        else {
+            float theta, r;
+            if (fabsf(ox) > fabsf(oy)) { r = ox; theta = ORC_PI_OVER_4 * (oy / ox); }
+            else { r = oy; theta = ORC_PI_OVER_2 - ORC_PI_OVER_4 * (ox / oy); }
+            dx = r * cosf(theta); dy = r * sinf(theta);
+        }
+        float zz = 1.f - dx * dx - dy * dy;
+        *wi = v3m(dx, dy, sqrtf(zz > 0.f ? zz : 0.f));
+        if (wo.z < 0) wi->z *= -1.f;
+        *pdf = lobe_pdf(b, 0, wo, *wi);
+        lobe_eval(b, 0, wo, *wi, f);
+        return;
+    }
+    if (lobe == 1) {
+        if (wo.z == 0) { sp_set(f, nl, 0.f); return; }
+        v3 wh = ggx_sample_wh(b, wo, ux, uy);
+        if (v3_dot(wo, wh) < 0) { sp_set(f, nl, 0.f); return; }
+        /* reflect(wo, wh) = wh*2*dot(wo,wh) - wo */
+        *wi = v3_sub(v3_mul(v3_mul(wh, 2.f), v3_dot(wo, wh)), wo);
+        if (!same_hemi(wo, *wi)) { sp_set(f, nl, 0.f); return; }
+        *pdf = ggx_pdf(b, wo, wh) / (4.f * v3_dot(wo, wh));
+        lobe_eval(b, 1, wo, *wi, f);
+        return;
+    }
+    if (lobe == 2) {
+        if (wo.z == 0) { sp_set(f, nl, 0.f); return; }
+        v3 wh = ggx_sample_wh(b, wo, ux, uy);
+        if (v3_dot(wo, wh) < 0) { sp_set(f, nl, 0.f); return; }
+        float eta = wo.z > 0 ? (1.f / b->mat_eta) : (b->mat_eta / 1.f);
+        /* refract, geometry.h:314-330 */
+        float cosI = v3_dot(wo, wh);
+        float m = 1.f - (cosI * cosI);
+        float sinI2 = m > 0.f ? m : 0.f;
+        float sinT2 = eta * eta * sinI2;
+        if (sinT2 >= 1) { sp_set(f, nl, 0.f); return; }
+        float cosT = sqrtf(1 - sinT2);
+        *wi = v3_add(v3_mul(wo, -eta), v3_mul(wh, (eta * cosI - cosT)));
+        *pdf = lobe_pdf(b, 2, wo, *wi);
+        lobe_eval(b, 2, wo, *wi, f);
+        return;
+    }
+    /* fresnel specular */
+    float F = fr_dielectric(wo.z, 1.f, b->mat_eta);
+    if (ux < F) {
+        *wi = v3m(-wo.x, -wo.y, wo.z);
+        *type = BSDF_SPECULAR | BSDF_REFLECTION;
+        *pdf = F;
+        float ac = fabsf(wi->z);
+        for (int i = 0; i < nl; ++i) f->c[i] = b->R.c[i] * F / ac;
+    } else {
+        int entering = wo.z > 0;
+        float etaI = entering ? 1.f : b->mat_eta;
+        float etaT = entering ? b->mat_eta : 1.f;
+        v3 n = v3_dot(v3m(0.f, 0.f, 1.f), wo) < 0.f ? v3m(-0.f, -0.f, -1.f) : v3m(0.f, 0.f, 1.f);
+        float eta = etaI / etaT;
+        float cosI = v3_dot(wo, n);
+        float m = 1.f - (cosI * cosI);
+        float sinI2 = m > 0.f ? m : 0.f;
+        float sinT2 = eta * eta * sinI2;
+        if (sinT2 >= 1) { sp_set(f, nl, 0.f); return; }
+        float cosT = sqrtf(1 - sinT2);
+        *wi = v3_add(v3_mul(wo, -eta), v3_mul(n, (eta * cosI - cosT)));
+        float sc = (etaI * etaI) / (etaT * etaT);
+        *type = BSDF_SPECULAR | BSDF_TRANSMISSION;
+        *pdf = 1.f - F;
+        float ac = fabsf(wi->z);
+        for (int i = 0; i < nl; ++i) {
+            float ft = b->R.c[i] * (1.f - F);
+            ft *= sc;
+            f->c[i] = ft / ac;
+        }
+    }
+}
+
+static int bsdf_num_components(const bsdf_t *b, int flags) {
+    int lobes[4], n = bsdf_lobes(b, lobes), c = 0;
+    for (int i = 0; i < n; ++i) if (matches(lobe_type(lobes[i]), flags)) ++c;
+    return c;
+}
+
+/* BSDF::evaluate, bsdf.cpp:30-50 */
+static void bsdf_eval(const bsdf_t *b, v3 woW, v3 wiW, int flags, spec *out) {
+    v3 wi = to_local(b, wiW), wo = to_local(b, woW);
+    sp_set(out, b->nl, 0.f);
+    if (wo.z == 0) return;
+    int reflect = v3_dot(wiW, b->ng) * v3_dot(woW, b->ng) > 0;
+    int lobes[4], n = bsdf_lobes(b, lobes);
+    for (int i = 0; i < n; ++i) {
+        int ty = lobe_type(lobes[i]);
+        if (matches(ty, flags) && ((reflect && (ty & BSDF_REFLECTION)) || (!reflect && (ty & BSDF_TRANSMISSION)))) {
+            spec f;
+            lobe_eval(b, lobes[i], wo, wi, &f);
+            for (int k = 0; k < b->nl; ++k) out->c[k] += f.c[k];
+        }
+    }
+}
+
+/* BSDF::pdf, bsdf.cpp:127-151 */
+static float bsdf_pdf(const bsdf_t *b, v3 woW, v3 wiW, int flags) {
+    int lobes[4], n = bsdf_lobes(b, lobes);
+    if (n == 0) return 0.f;
+    v3 wi = to_local(b, wiW), wo = to_local(b, woW);
+    if (wo.z == 0) return 0.f;
+    float pdf = 0.f;
+    int mc = 0;
+    for (int i = 0; i < n; ++i)
+        if (matches(lobe_type(lobes[i]), flags)) { ++mc; pdf += lobe_pdf(b, lobes[i], wo, wi); }
+    return mc > 0 ? pdf / (float)mc : 0.f;
+}
+
+/* BSDF::sample, bsdf.cpp:52-125. Returns 0 when *pdf was left untouched (wo.z == 0). */
+static void bsdf_sample(const bsdf_t *b, v3 woW, v3 *wiW, float ux, float uy, float *pdf, int flags, int *sampledType,
+                        spec *f) {
+    int lobes[4], n = bsdf_lobes(b, lobes);
+    int mc = 0;
+    for (int i = 0; i < n; ++i) if (matches(lobe_type(lobes[i]), flags)) ++mc;
+    sp_set(f, b->nl, 0.f);
+    if (mc == 0) { *pdf = 0.f; *sampledType = 0; return; }
+    int comp = (int)floorf(ux * mc);
+    if (comp > mc - 1) comp = mc - 1;
+    int chosen = -1, count = comp;
+    for (int i = 0; i < n; ++i)
+        if (matches(lobe_type(lobes[i]), flags) && count-- == 0) { chosen = lobes[i]; break; }
+    float urx = ux * mc - comp;
+    if (urx > 1.f - ORC_SHADOW_EPSILON) urx = 1.f - ORC_SHADOW_EPSILON;
+    v3 wi = v3m(0.f, 0.f, 0.f), wo = to_local(b, woW);
+    if (wo.z == 0) return;
+    *pdf = 0.f;
+    int ctype = lobe_type(chosen);
+    *sampledType = ctype;
+    lobe_sample(b, chosen, wo, &wi, urx, uy, pdf, sampledType, f);
+    if (*pdf == 0) { *sampledType = 0; sp_set(f, b->nl, 0.f); return; }
+    *wiW = to_world(b, wi);
+    if (!(ctype & BSDF_SPECULAR) && mc > 1) {
+        for (int i = 0; i < n; ++i)
+            if (lobes[i] != chosen && matches(lobe_type(lobes[i]), flags)) *pdf += lobe_pdf(b, lobes[i], wo, wi);
+    }
+    if (mc > 1) *pdf /= mc;
+    if (!(ctype & BSDF_SPECULAR)) {
+        int reflect = v3_dot(*wiW, b->ng) * v3_dot(woW, b->ng) > 0;
+        sp_set(f, b->nl, 0.f);
+        for (int i = 0; i < n; ++i) {
+            int ty = lobe_type(lobes[i]);
+            if (matches(ty, flags) && ((reflect && (ty & BSDF_REFLECTION)) || (!reflect && (ty & BSDF_TRANSMISSION)))) {
+                spec g;
+                lobe_eval(b, lobes[i], wo, wi, &g);
+                for (int k = 0; k < b->nl; ++k) f->c[k] += g.c[k];
+            }
+        }
+    }
+}
+
+/* Material::compute_scattering_functions for the supported materials */
+static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda, bsdf_t *b) {
+    b->nl = S->nl;
+    b->ng = is->n;
+    b->ns = is->ns;
+    orc_coordinate_system(b->ns, &b->s, &b->t);
+    b->s = v3_norm(b->s);
+    uint32_t mi = 0;
+    if (is->prim >= 0 && S->sc->tri_material) mi = S->sc->tri_material[is->prim];
+    const fl_material *m = &S->sc->materials[mi];
+    b->type = m->type;
+    b->mat_eta = m->eta;
+    b->mat_k = m->k;
+    float a = m->roughness * m->roughness;
+    b->ax = a > 0.001f ? a : 0.001f;
+    b->ay = b->ax;
+    b->eta = (m->type == FL_MAT_ROUGH_DIELECTRIC || m->type == FL_MAT_SMOOTH_DIELECTRIC) ? m->eta : 1.f;
+    if (m->type == FL_MAT_LAMBERT) {
+        if (S->mode == FL_SPECTRAL_BINS60) b->R = S->mat_refl60[mi];
+        else orc_reflectance(S->tab, m->rgb, S->mode, lambda, b->R.c);
+    } else {
+        sp_set(&b->R, b->nl, 1.f);
+    }
+}
+
+/* ---------------------------------------------------------------- lights */
+/* Triangle::intersect (triangle.cpp:13-124): only p and n are used by Shape::pdf */
+static int tri_intersect_ref(const float *tv, const ray3 *r, v3 *p, v3 *n) {
+    v3 v1 = v3m(tv[0], tv[1], tv[2]), v2 = v3m(tv[3], tv[4], tv[5]), v3v = v3m(tv[6], tv[7], tv[8]);
+    v3 e1 = v3_sub(v2, v1), e2 = v3_sub(v3v, v1);
+    v3 nn = v3_cross(e1, e2);
+    float det = -v3_dot(r->d, nn);
+    v3 ao = v3_sub(r->o, v1);
+    v3 dao = v3_cross(ao, r->d);
+    float invDet = 1.f / det;
+    float alpha = v3_dot(e2, dao) * invDet;
+    float beta = -v3_dot(e1, dao) * invDet;
+    float t = v3_dot(ao, nn) * invDet;
+    if ((t < r->tmax && t > r->tmin) && alpha > 0 && beta > 0 && (alpha + beta) < 1.f) {
+        if (v3_len2(nn) == 0) return 0;
+        *p = v3_add(r->o, v3_mul(r->d, t));
+        *n = v3_norm(v3_cross(v3_sub(v1, v3v), v3_sub(v2, v3v)));
+        return 1;
+    }
+    return 0;
+}
+
+static float tri_area(const float *tv) {
+    v3 v1 = v3m(tv[0], tv[1], tv[2]), v2 = v3m(tv[3], tv[4], tv[5]), v3v = v3m(tv[6], tv[7], tv[8]);
+    return 0.5f * v3_len(v3_cross(v3_sub(v2, v1), v3_sub(v3v, v1)));
+}
+
+typedef struct {
+    int kind;         /* 0 none, 1 finite point (segment test), 2 direction to infinity */
+    v3 target;        /* light point (kind 1) */
+} vis_t;
+
+/* Illuminant::sample_li. Returns the radiance (constant over wavelength) via *Li. */
+static float light_sample_li(const scene_ctx *S, int li, const isect_t *ref, float ux, float uy, v3 *wi, float *pdf,
+                             vis_t *vis) {
+    const fl_light *L = &S->sc->lights[li];
+    vis->kind = 0;
+    if (L->type == FL_LIGHT_TRIANGLE) {
+        const float *tv = S->sc->verts + 9 * (size_t)L->tri;
+        v3 p0 = v3m(tv[0], tv[1], tv[2]), p1 = v3m(tv[3], tv[4], tv[5]), p2 = v3m(tv[6], tv[7], tv[8]);
+        /* Triangle::sample(u, pdf) */
+        float uu = sqrtf(ux);
+        float u1 = 1.f - uu;
+        float u2 = uy * uu;
+        v3 ip = v3_add(v3_add(v3_mul(p0, u1), v3_mul(p1, u2)), v3_mul(p2, (1.f - u1 - u2)));
+        v3 in = v3_norm(v3_cross(v3_sub(p1, p0), v3_sub(p2, p0)));
+        *pdf = 1.f / tri_area(tv);
+        /* Shape::sample(isect, u, pdf) */
+        v3 w = v3_sub(ip, ref->p);
+        if (v3_len2(w) == 0) *pdf = 0.f;
+        else {
+            w = v3_norm(w);
+            *pdf *= v3_len2(v3_sub(ref->p, ip)) / v3_absdot(in, v3_neg(w));
+            if (isinf(*pdf)) *pdf = 0.f;
+        }
+        /* DiffuseAreaIlluminant::sample_li */
+        if (*pdf == 0 || v3_len2(v3_sub(ip, ref->p)) == 0) { *pdf = 0.f; return 0.f; }
+        *wi = v3_norm(v3_sub(ip, ref->p));
+        vis->kind = 1;
+        vis->target = ip;
+        return v3_dot(in, v3m(-wi->x, -wi->y, -wi->z)) > 0.f ? L->radiance : 0.f;
+    }
+    if (L->type == FL_LIGHT_SPHERE) {
+        /* uniform area sampling of the sphere, converted to solid angle */
+        v3 c = v3m(L->center[0], L->center[1], L->center[2]);
+        float z = 1.f - 2.f * ux;
+        float rr = sqrtf(fmaxf(0.f, 1.f - z * z));
+        float phi = 2.f * ORC_PI * uy;
+        v3 nrm = v3m(rr * cosf(phi), rr * sinf(phi), z);
+        v3 ip = v3_add(c, v3_mul(nrm, L->radius));
+        float area = 4.f * ORC_PI * L->radius * L->radius;
+        v3 w = v3_sub(ip, ref->p);
+        float d2 = v3_len2(w);
+        if (d2 == 0) { *pdf = 0.f; return 0.f; }
+        w = v3_norm(w);
+        float cosl = v3_dot(nrm, v3_neg(w));
+        if (cosl <= 0.f) { *pdf = 0.f; return 0.f; }
+        *pdf = d2 / (cosl * area);
+        if (isinf(*pdf)) { *pdf = 0.f; return 0.f; }
+        *wi = w;
+        vis->kind = 1;
+        vis->target = ip;
+        return L->radiance;
+    }
+    /* environment: uniform sphere directions */
+    float z = 1.f - 2.f * ux;
+    float rr = sqrtf(fmaxf(0.f, 1.f - z * z));
+    float phi = 2.f * ORC_PI * uy;
+    *wi = v3m(rr * cosf(phi), rr * sinf(phi), z);
+    *pdf = ORC_INV_4_PI;
+    vis->kind = 2;
+    return L->radiance;
+}
+
+/* Illuminant::pdf_li */
+static float light_pdf_li(const scene_ctx *S, int li, const isect_t *ref, v3 wi) {
+    const fl_light *L = &S->sc->lights[li];
+    if (L->type == FL_LIGHT_TRIANGLE) {
+        const float *tv = S->sc->verts + 9 * (size_t)L->tri;
+        ray3 r = {orc_offset_point_origin(ref->p, ref->pError, ref->n, wi), wi, ORC_SHADOW_EPSILON, INF_F};
+        v3 p, n;
+        if (!tri_intersect_ref(tv, &r, &p, &n)) return 0.f;
+        float pdf = v3_len2(v3_sub(ref->p, p)) / (v3_absdot(n, v3_neg(wi)) * tri_area(tv));
+        if (isinf(pdf)) pdf = 0.f;
+        return pdf;
+    }
+    if (L->type == FL_LIGHT_SPHERE) {
+        ray3 r = {orc_offset_point_origin(ref->p, ref->pError, ref->n, wi), wi, ORC_SHADOW_EPSILON, INF_F};
+        float t = sphere_hit(L, &r);
+        if (t <= 0.f) return 0.f;
+        v3 p = v3_add(r.o, v3_mul(r.d, t));
+        v3 c = v3m(L->center[0], L->center[1], L->center[2]);
+        v3 nrm = v3_norm(v3_sub(p, c));
+        float area = 4.f * ORC_PI * L->radius * L->radius;
+        float cosl = v3_dot(nrm, v3_neg(wi));
+        if (cosl <= 0.f) return 0.f;
+        float pdf = v3_len2(v3_sub(ref->p, p)) / (cosl * area);
+        if (isinf(pdf)) pdf = 0.f;
+        return pdf;
+    }
+    return ORC_INV_4_PI;
+}
+
+/* radiance leaving a hit on light li towards w (AreaIlluminant::L, diffusearea.cpp:37-39) */
+static float light_L(const scene_ctx *S, int li, const isect_t *is, v3 w) {
+    const fl_light *L = &S->sc->lights[li];
+    if (L->type == FL_LIGHT_ENV) return 0.f;
+    return v3_dot(is->n, w) > 0.f ? L->radiance : 0.f;
+}
+
+/* VisibilityEvaluator::unoccluded (illuminant.cpp:40-50): no hit, or the closest hit
+ * carries an area light. Analytic sphere lights never occlude. */
+static int unoccluded(const scene_ctx *S, const isect_t *p0, const vis_t *vis, v3 wi, uint64_t *rays) {
+    ray3 r;
+    if (vis->kind == 1) {
+        v3 d = v3_sub(vis->target, p0->p);
+        r.o = orc_offset_point_origin(p0->p, p0->pError, p0->n, d);
+        r.d = d;
+        r.tmin = ORC_SHADOW_EPSILON;
+        r.tmax = 1.f - ORC_SHADOW_EPSILON;
+    } else {
+        r.o = orc_offset_point_origin(p0->p, p0->pError, p0->n, wi);
+        r.d = wi;
+        r.tmin = ORC_SHADOW_EPSILON;
+        r.tmax = INF_F;
+    }
+    float ot[4] = {r.o.x, r.o.y, r.o.z, r.tmin};
+    float dt[4] = {r.d.x, r.d.y, r.d.z, r.tmax};
+    orc_ray rr;
+    orc_ray_precompute(ot, dt, &rr);
+    float t, u, v;
+    int32_t id = orc_bvh_closest(S->bvh, &rr, &t, &u, &v, NULL, NULL);
+    ++*rays;
+    if (id < 0) return 1;
+    return S->tri_light[id] >= 0;
+}
+
+static float power_heuristic(float fPdf, float gPdf) {
+    float f = 1 * fPdf, g = 1 * gPdf;
+    return (f * f) / (f * f + g * g);
+}
+
+typedef struct { uint64_t rays, shadow_rays, bounces; } counters;
+
+/* estimate_direct, integrator.cpp:25-110 (area / sphere / environment lights are never delta) */
+static void estimate_direct(const scene_ctx *S, const isect_t *it, const bsdf_t *b, float usx, float usy, int li,
+                            float ulx, float uly, spec *Ld, counters *cn) {
+    const int nl = S->nl;
+    const int bsdfFlags = BSDF_ALL & ~BSDF_SPECULAR;
+    sp_set(Ld, nl, 0.f);
+    v3 wi = v3m(0.f, 0.f, 0.f);
+    float illumPdf = 0, scatteringPdf = 0;
+    vis_t vis;
+    float Lrad = light_sample_li(S, li, it, ulx, uly, &wi, &illumPdf, &vis);
+    if (illumPdf > 0 && Lrad != 0.f) {
+        spec f;
+        bsdf_eval(b, it->wo, wi, bsdfFlags, &f);
+        float ad = v3_absdot(wi, it->ns);
+        for (int i = 0; i < nl; ++i) f.c[i] *= ad;
+        scatteringPdf = bsdf_pdf(b, it->wo, wi, bsdfFlags);
+        if (!sp_black(&f, nl)) {
+            ++cn->shadow_rays;
+            if (!unoccluded(S, it, &vis, wi, &cn->rays)) Lrad = 0.f;
+            if (Lrad != 0.f) {
+                float weight = power_heuristic(illumPdf, scatteringPdf);
+                for (int i = 0; i < nl; ++i) Ld->c[i] += f.c[i] * Lrad * weight / illumPdf;
+            }
+        }
+    }
+    /* MIS - BSDF */
+    {
+        spec f;
+        int sampledType = 0;
+        bsdf_sample(b, it->wo, &wi, usx, usy, &scatteringPdf, bsdfFlags, &sampledType, &f);
+        float ad = v3_absdot(wi, it->ns);
+        for (int i = 0; i < nl; ++i) f.c[i] *= ad;
+        int sampledSpecular = (sampledType & BSDF_SPECULAR) != 0;
+        if (!sp_black(&f, nl) && scatteringPdf > 0) {
+            float weight = 1.f;
+            if (!sampledSpecular) {
+                illumPdf = light_pdf_li(S, li, it, wi);
+                if (illumPdf == 0) return;
+                weight = power_heuristic(scatteringPdf, illumPdf);
+            }
+            ray3 r = {orc_offset_point_origin(it->p, it->pError, it->n, wi), wi, ORC_SHADOW_EPSILON, INF_F};
+            isect_t li_is;
+            float Lv = 0.f;
+            if (scene_intersect(S, &r, &li_is, &cn->rays)) {
+                if (prim_light(S, li_is.prim) == li) Lv = light_L(S, li, &li_is, v3_neg(wi));
+            } else {
+                const fl_light *L = &S->sc->lights[li];
+                Lv = L->type == FL_LIGHT_ENV ? L->radiance : 0.f;
+            }
+            if (Lv != 0.f)
+                for (int i = 0; i < nl; ++i) Ld->c[i] += f.c[i] * Lv * 1.f * weight / scatteringPdf;
+        }
+    }
+}
+
+/* PathIntegrator::Li, pathintegrator.cpp:12-87 */
+static void path_Li(const scene_ctx *S, const fl_render_params *P, v3 o, v3 d, float tmin, const float *lambda,
+                    orc_pcg32 *rng, spec *L, counters *cn) {
+    const int nl = S->nl;
+    spec beta;
+    sp_set(L, nl, 0.f);
+    sp_set(&beta, nl, 1.f);
+    ray3 ray = {o, d, tmin, INF_F};
+    int specularBounce = 0;
+    float etaScale = 1.f;
+    const int depth = P->max_depth;
+    const float rrThreshold = P->rr_threshold;
+    for (int bounces = 0;; ++bounces) {
+        isect_t is;
+        int hit = scene_intersect(S, &ray, &is, &cn->rays);
+        if (bounces == 0 || specularBounce) {
+            if (hit) {
+                int li = prim_light(S, is.prim);
+                if (li >= 0) {
+                    float le = light_L(S, li, &is, v3_neg(ray.d));
+                    for (int i = 0; i < nl; ++i) L->c[i] += beta.c[i] * le;
+                }
+            } else if (S->has_env) {
+                /* escaped rays see the environment (Illuminant::le for infinite lights) */
+                for (int i = 0; i < nl; ++i) L->c[i] += beta.c[i] * S->env_radiance;
+            }
+        }
+        if (!hit) break;
+        ++cn->bounces;
+        bsdf_t b;
+        make_bsdf(S, &is, lambda, &b);
+        if (bsdf_num_components(&b, BSDF_ALL & ~BSDF_SPECULAR) > 0) {
+            spec Ls;
+            sp_set(&Ls, nl, 0.f);
+            for (uint32_t li = 0; li < S->sc->n_lights; ++li) {
+                float ulx = orc_pcg32_nextf(rng), uly = orc_pcg32_nextf(rng);
+                float usx = orc_pcg32_nextf(rng), usy = orc_pcg32_nextf(rng);
+                spec e;
+                estimate_direct(S, &is, &b, usx, usy, (int)li, ulx, uly, &e, cn);
+                for (int i = 0; i < nl; ++i) Ls.c[i] += e.c[i];
+            }
+            for (int i = 0; i < nl; ++i) L->c[i] += beta.c[i] * Ls.c[i];
+        }
+        v3 wo = v3_neg(ray.d), wi = v3m(0.f, 0.f, 0.f);
+        float pdf = 0.f;
+        int flags = 0;
+        spec f;
+        float ux = orc_pcg32_nextf(rng), uy = orc_pcg32_nextf(rng);
+        bsdf_sample(&b, wo, &wi, ux, uy, &pdf, BSDF_ALL, &flags, &f);
+        if (sp_black(&f, nl) || pdf == 0) break;
+        if (depth == bounces && (flags & BSDF_DIFFUSE)) break;
+        if ((depth == bounces && (flags & BSDF_SPECULAR)) || (depth == bounces && (flags & BSDF_GLOSSY))) break;
+        if (depth == bounces && (flags & BSDF_TRANSMISSION)) break;
+        float ad = v3_absdot(wi, is.ns);
+        for (int i = 0; i < nl; ++i) beta.c[i] *= f.c[i] * ad / pdf;
+        specularBounce = (flags & BSDF_SPECULAR) != 0;
+        if ((flags & BSDF_SPECULAR) && (flags & BSDF_TRANSMISSION)) {
+            float eta = b.eta;
+            etaScale *= (v3_dot(wo, is.n) > 0) ? (eta * eta) : 1.f / (eta * eta);
+        }
+        ray.o = orc_offset_point_origin(is.p, is.pError, is.n, wi);
+        ray.d = wi;
+        ray.tmin = ORC_SHADOW_EPSILON;
+        ray.tmax = INF_F;
+        spec rr;
+        for (int i = 0; i < nl; ++i) rr.c[i] = beta.c[i] * etaScale;
+        float mx = sp_max(&rr, nl);
+        if (mx < rrThreshold && bounces > 3) {
+            float q = 1.f - mx;
+            if (q < 0.05f) q = 0.05f;
+            if (orc_pcg32_nextf(rng) < q) break;
+            for (int i = 0; i < nl; ++i) beta.c[i] /= 1.f - q;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------- camera */
+void orc_camera_init(const fl_camera *c, orc_camera *out) {
+    v3 pos = v3m(c->position[0], c->position[1], c->position[2]);
+    v3 at = v3m(c->look_at[0], c->look_at[1], c->look_at[2]);
+    v3 up = v3m(c->up[0], c->up[1], c->up[2]);
+    float focusDistance = v3_len(v3_sub(pos, at));
+    float theta = c->vfov_deg * ORC_PI / 180.f;
+    float halfHeight = tanf(theta / 2.f);
+    float aspect = (float)c->width / (float)c->height;
+    float halfWidth = aspect * halfHeight;
+    v3 w = v3_norm(v3_sub(pos, at));
+    /* flipCameraDirection = true: the orientation in which the camera looks at look_at */
+    w = v3_mul(w, -1.f);
+    v3 u = v3_norm(v3_cross(up, w));
+    v3 v = v3_cross(w, u);
+    w = v3_mul(w, -1.f);
+    out->origin = pos;
+    out->u = u;
+    out->v = v;
+    out->lower_left = v3_sub(v3_sub(v3_sub(pos, v3_mul(v3_mul(u, halfWidth), focusDistance)),
+                                    v3_mul(v3_mul(v, focusDistance), halfHeight)),
+                             v3_mul(w, focusDistance));
+    out->horizontal = v3_mul(v3_mul(v3_mul(u, 2.f), halfWidth), focusDistance);
+    out->vertical = v3_mul(v3_mul(v3_mul(v, 2.f), halfHeight), focusDistance);
+}
+
+/* The render loop the reference lacks: sample (s, t) of pixel p, PhysicalCamera::awaken_ray
+ * with lens sample (0.5, 0.5) (a pinhole: the lens loop of physical.cpp:4-10 exits at once). */
+void orc_camera_ray(const orc_camera *cam, const fl_camera *c, uint32_t pixel, orc_pcg32 *rng, v3 *o, v3 *d,
+                    float *u_lambda) {
+    float ux = orc_pcg32_nextf(rng), uy = orc_pcg32_nextf(rng);
+    *u_lambda = orc_pcg32_nextf(rng);
+    uint32_t px = pixel % (uint32_t)c->width, py = pixel / (uint32_t)c->width;
+    float sx = ((float)px + ux) / (float)c->width;
+    float sy = ((float)((uint32_t)c->height - 1u - py) + uy) / (float)c->height;
+    /* random_point_on_lens((0.5, 0.5)) * lensRadius with lensRadius = 0 */
+    v3 p = v3_sub(v3_mul(v3m(0.5f, 0.5f, 0.f), 2.f), v3m(1.f, 1.f, 0.f));
+    v3 rd = v3_mul(p, 0.f);
+    v3 offset = v3_add(v3_mul(cam->u, rd.x), v3_mul(cam->v, rd.y));
+    *o = v3_add(cam->origin, offset);
+    v3 dir = v3_sub(v3_sub(v3_add(v3_add(cam->lower_left, v3_mul(cam->horizontal, sx)), v3_mul(cam->vertical, sy)),
+                           cam->origin),
+                    offset);
+    *d = v3_norm(dir);
+}
+
+/* ---------------------------------------------------------------- driver */
+typedef struct {
+    const scene_ctx *S;
+    const fl_camera *cam;
+    const orc_camera *oc;
+    const fl_render_params *P;
+    const orc_render_opts *opts;
+    double *film;
+    uint32_t total;
+    volatile uint32_t *next;
+    counters cn;
+    uint64_t paths;
+} worker_arg;
+
+static void *render_worker(void *argp) {
+    worker_arg *a = (worker_arg *)argp;
+    const scene_ctx *S = a->S;
+    const int nl = S->nl;
+    for (;;) {
+        uint32_t start = __atomic_fetch_add(a->next, 64u, __ATOMIC_RELAXED);
+        if (start >= a->total) break;
+        uint32_t end = start + 64u < a->total ? start + 64u : a->total;
+        for (uint32_t k = start; k < end; ++k) {
+            uint32_t pixel = a->opts && a->opts->pixels ? a->opts->pixels[k] : k;
+            double acc[3] = {0, 0, 0};
+            for (int s = 0; s < a->P->spp; ++s) {
+                orc_pcg32 rng;
+                orc_pcg32_seed(&rng, pixel, 1u);
+                uint64_t sidx = (uint64_t)a->P->sample_offset + (uint64_t)s;
+                if (sidx) orc_pcg32_advance(&rng, (int64_t)(sidx << 16));
+                v3 o, d;
+                float ul;
+                orc_camera_ray(a->oc, a->cam, pixel, &rng, &o, &d, &ul);
+                float lambda[4];
+                if (S->mode == FL_SPECTRAL_HERO4) {
+                    float l0 = 380.f + ul * 340.f;
+                    for (int j = 0; j < 4; ++j) {
+                        float l = l0 + 85.f * (float)j;
+                        lambda[j] = l >= 720.f ? l - 340.f : l;
+                    }
+                }
+                spec L;
+                path_Li(S, a->P, o, d, 0.f, lambda, &rng, &L, &a->cn);
+                double xyz[3];
+                orc_xyz_from_spectrum(S->tab, S->mode, lambda, L.c, xyz);
+                (void)nl;
+                acc[0] += xyz[0]; acc[1] += xyz[1]; acc[2] += xyz[2];
+                a->paths++;
+            }
+            a->film[3 * (size_t)pixel + 0] += acc[0];
+            a->film[3 * (size_t)pixel + 1] += acc[1];
+            a->film[3 * (size_t)pixel + 2] += acc[2];
+        }
+    }
+    return NULL;
+}
+
+int orc_render(const fl_scene_desc *sc, const orc_tables *tab, const fl_camera *cam, const fl_render_params *P,
+               const orc_render_opts *opts, double *film, orc_render_counts *counts) {
+    if (!sc || !tab || !cam || !P || !film || cam->width <= 0 || cam->height <= 0 || P->spp <= 0) return -1;
+    scene_ctx S;
+    memset(&S, 0, sizeof(S));
+    S.sc = sc;
+    S.tab = tab;
+    S.mode = P->spectral_mode;
+    S.nl = S.mode == FL_SPECTRAL_BINS60 ? ORC_NBINS : 4;
+    S.bvh = orc_bvh_build(sc->verts, sc->n_tri);
+    S.tri_light = (int32_t *)malloc(sizeof(int32_t) * (sc->n_tri ? sc->n_tri : 1));
+    for (uint32_t i = 0; i < sc->n_tri; ++i) S.tri_light[i] = -1;
+    for (uint32_t l = 0; l < sc->n_lights; ++l) {
+        if (sc->lights[l].type == FL_LIGHT_TRIANGLE && sc->lights[l].tri < sc->n_tri) {
+            S.tri_light[sc->lights[l].tri] = (int32_t)l;
+            S.emissive_tris++;
+        }
+        if (sc->lights[l].type == FL_LIGHT_ENV) { S.has_env = 1; S.env_radiance = sc->lights[l].radiance; }
+    }
+    S.mat_refl60 = (spec *)malloc(sizeof(spec) * (sc->n_materials ? sc->n_materials : 1));
+    for (uint32_t m = 0; m < sc->n_materials; ++m)
+        orc_reflectance(tab, sc->materials[m].rgb, FL_SPECTRAL_BINS60, NULL, S.mat_refl60[m].c);
+
+    orc_camera oc;
+    orc_camera_init(cam, &oc);
+    uint32_t total = opts && opts->pixels ? opts->n_pixels : (uint32_t)cam->width * (uint32_t)cam->height;
+    int nth = opts && opts->nthreads > 0 ? opts->nthreads : 1;
+    if (nth > 256) nth = 256;
+    volatile uint32_t next = 0;
+    pthread_t th[256];
+    worker_arg args[256];
+    for (int k = 0; k < nth; ++k) {
+        memset(&args[k], 0, sizeof(worker_arg));
+        args[k].S = &S; args[k].cam = cam; args[k].oc = &oc; args[k].P = P; args[k].opts = opts;
+        args[k].film = film; args[k].total = total; args[k].next = &next;
+        pthread_create(&th[k], NULL, render_worker, &args[k]);
+    }
+    orc_render_counts c = {0, 0, 0, 0};
+    for (int k = 0; k < nth; ++k) {
+        pthread_join(th[k], NULL);
+        c.paths += args[k].paths;
+        c.rays += args[k].cn.rays;
+        c.shadow_rays += args[k].cn.shadow_rays;
+        c.bounces += args[k].cn.bounces;
+    }
+    if (counts) *counts = c;
+    orc_bvh_free(S.bvh);
+    free(S.tri_light);
+    free(S.mat_refl60);
+    return 0;
+}

@@ -1,0 +1,283 @@
+/*
+ * Render driver for the reference's own integrator (test infrastructure only).
+ *
+ * filianore-core has no render loop, film or sampler with reproducible seeds (its
+ * Whitenoise sampler seeds mt19937 from std::random_device,
+ * src/filianore/sampling/samplers/whitenoise.h:25-28). This driver supplies them with the
+ * same definitions the GPU backend uses, and otherwise runs the reference unchanged:
+ *   - scene: one Triangle + LambertMaterial + optional DiffuseAreaIlluminant per soup
+ *     triangle (shapes/triangle.h, shading/materials/lambert.h, illuminants/diffusearea.h),
+ *     albedos upsampled with from_reflectance_rgb (color/spectrumoperations.cpp:113-147);
+ *   - camera: PhysicalCamera with aperture 0 and flipCameraDirection = true
+ *     (cameras/physical.h:11-43): with the default false the camera faces away from
+ *     its look-at point, with true it faces it;
+ *   - integrator: PathIntegrator(RenderParams{spp, d, d, d}, rr) (integrators/pathintegrator.h);
+ *   - sampler: a Sampler (sampling/sampler.h:10-19) over the vendored pcg32
+ *     (src/ext/pcg32.h), seeded per (pixel, sample) with seed(pixel, 1) and advance(sample << 16);
+ *     camera sample order: ux, uy, u_lambda (unused by the 60-bin spectra);
+ *   - film: sums over samples of to_xyz(Li) in double (color/spectrumoperations.cpp:193-207).
+ *
+ * Usage:
+ *   ref_render SCENE.bin OUT.bin     render a scene file written by tests/golden/scenefile.py
+ *   ref_render --tables OUT.bin      dump the raw and 60-bin spectral tables
+ *   ref_render --pcg OUT.bin         dump pcg32 known-answer sequences
+ */
+#include "filianore/cameras/physical.h"
+#include "filianore/color/cie.h"
+#include "filianore/color/spectruminits.h"
+#include "filianore/color/spectrumoperations.h"
+#include "filianore/core/interaction.h"
+#include "filianore/core/primitive.h"
+#include "filianore/core/scene.h"
+#include "filianore/illuminants/diffusearea.h"
+#include "filianore/integrators/pathintegrator.h"
+#include "filianore/sampling/sampler.h"
+#include "filianore/shading/materials/lambert.h"
+#include "filianore/shading/textures/constant.h"
+#include "filianore/shapes/triangle.h"
+#include "ext/pcg32.h"
+#include "../../include/filianore_gpu.h"
+
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace ref_shim {
+extern std::vector<const filianore::Primitive *> g_primitives;
+}
+
+using namespace filianore;
+
+namespace {
+
+class PCG32Sampler : public Sampler {
+public:
+    void reset(uint64_t pixel, uint64_t sample) {
+        rng.seed(pixel, 1u);
+        if (sample) rng.advance((int64_t)(sample << 16));
+    }
+    float get_1d() override { return rng.nextFloat(); }
+    Vector2f get_2d() override {
+        float x = get_1d();
+        float y = get_1d();
+        return Vector2f(x, y);
+    }
+    void prepare_next_sample() override {}
+
+private:
+    pcg32 rng;
+};
+
+struct SceneFileHeader {
+    char magic[8];
+    uint32_t n_tri, n_mat, n_light, spp, max_depth, spectral_mode, sample_offset, nthreads, n_pixels;
+    float rr_threshold;
+    fl_camera cam;
+};
+
+template <typename T>
+bool read_n(FILE *f, std::vector<T> &v, size_t n) {
+    v.resize(n);
+    return n == 0 || fread(v.data(), sizeof(T), n, f) == n;
+}
+
+int dump_tables(const char *out) {
+    InitializeSpectrals();
+    FILE *f = fopen(out, "wb");
+    if (!f) return 2;
+    int32_t counts[2] = {nCIESamples, nRGB2SpectSamples};
+    fwrite(counts, sizeof(int32_t), 2, f);
+    fwrite(&CIE_Y_Integral, sizeof(float), 1, f);
+    fwrite(CIE_Wavelength, sizeof(float), nCIESamples, f);
+    fwrite(CIE_X, sizeof(float), nCIESamples, f);
+    fwrite(CIE_Y, sizeof(float), nCIESamples, f);
+    fwrite(CIE_Z, sizeof(float), nCIESamples, f);
+    fwrite(RGB2SpectLambda, sizeof(float), nRGB2SpectSamples, f);
+    const float *refl[7] = {RGBRefl2SpectWhite, RGBRefl2SpectCyan, RGBRefl2SpectMagenta, RGBRefl2SpectYellow,
+                            RGBRefl2SpectRed, RGBRefl2SpectGreen, RGBRefl2SpectBlue};
+    const float *illum[7] = {RGBIllum2SpectWhite, RGBIllum2SpectCyan, RGBIllum2SpectMagenta, RGBIllum2SpectYellow,
+                             RGBIllum2SpectRed, RGBIllum2SpectGreen, RGBIllum2SpectBlue};
+    for (auto *p : refl) fwrite(p, sizeof(float), nRGB2SpectSamples, f);
+    for (auto *p : illum) fwrite(p, sizeof(float), nRGB2SpectSamples, f);
+    const PrincipalSpectrum *binned[17] = {&X, &Y, &Z,
+                                           &rgbRefl2SpectWhite, &rgbRefl2SpectCyan, &rgbRefl2SpectMagenta,
+                                           &rgbRefl2SpectYellow, &rgbRefl2SpectRed, &rgbRefl2SpectGreen,
+                                           &rgbRefl2SpectBlue,
+                                           &rgbIllum2SpectWhite, &rgbIllum2SpectCyan, &rgbIllum2SpectMagenta,
+                                           &rgbIllum2SpectYellow, &rgbIllum2SpectRed, &rgbIllum2SpectGreen,
+                                           &rgbIllum2SpectBlue};
+    for (auto *s : binned) fwrite(s->c, sizeof(float), nSpectralSamples, f);
+    /* from_reflectance_rgb of the Cornell albedos and to_xyz of a constant spectrum */
+    const float rgbs[4][3] = {{0.725f, 0.725f, 0.725f}, {0.63f, 0.065f, 0.05f}, {0.14f, 0.45f, 0.091f}, {0.2f, 0.9f, 0.5f}};
+    for (auto &c : rgbs) {
+        PrincipalSpectrum s = from_reflectance_rgb(Vector3f(c[0], c[1], c[2]));
+        fwrite(s.c, sizeof(float), nSpectralSamples, f);
+    }
+    Vector3f xyz = to_xyz(PrincipalSpectrum(1.f));
+    float x3[3] = {xyz.x, xyz.y, xyz.z};
+    fwrite(x3, sizeof(float), 3, f);
+    fclose(f);
+    return 0;
+}
+
+int dump_pcg(const char *out) {
+    FILE *f = fopen(out, "wb");
+    if (!f) return 2;
+    const uint64_t seeds[5][2] = {{0, 1}, {1, 1}, {12345, 1}, {42, 54}, {65535, 1}};
+    for (auto &s : seeds) {
+        pcg32 r(s[0], s[1]);
+        uint32_t v[16];
+        for (auto &x : v) x = r.nextUInt();
+        fwrite(v, sizeof(uint32_t), 16, f);
+    }
+    const int64_t advs[3] = {1, 1 << 16, 5 << 16};
+    for (int64_t a : advs) {
+        pcg32 r(7, 1);
+        r.advance(a);
+        uint32_t v[8];
+        for (auto &x : v) x = r.nextUInt();
+        fwrite(v, sizeof(uint32_t), 8, f);
+    }
+    pcg32 r(3, 1);
+    float fl[8];
+    for (auto &x : fl) x = r.nextFloat();
+    fwrite(fl, sizeof(float), 8, f);
+    fclose(f);
+    return 0;
+}
+
+int render(const char *scene_path, const char *out_path) {
+    FILE *f = fopen(scene_path, "rb");
+    if (!f) { fprintf(stderr, "cannot open %s\n", scene_path); return 2; }
+    SceneFileHeader h;
+    if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, "FLSCENE1", 8) != 0) {
+        fprintf(stderr, "bad scene file\n");
+        return 2;
+    }
+    std::vector<float> verts;
+    std::vector<uint32_t> tri_mat, pixels;
+    std::vector<fl_material> mats;
+    std::vector<fl_light> lights;
+    bool ok = read_n(f, verts, (size_t)h.n_tri * 9) && read_n(f, tri_mat, h.n_tri) && read_n(f, mats, h.n_mat) &&
+              read_n(f, lights, h.n_light) && read_n(f, pixels, h.n_pixels);
+    fclose(f);
+    if (!ok) { fprintf(stderr, "truncated scene file\n"); return 2; }
+    if (h.spectral_mode != FL_SPECTRAL_BINS60) {
+        fprintf(stderr, "the reference integrator only has 60-bin spectra\n");
+        return 2;
+    }
+
+    InitializeSpectrals();
+
+    std::vector<std::shared_ptr<Material>> materials;
+    for (const auto &m : mats) {
+        if (m.type != FL_MAT_LAMBERT) { fprintf(stderr, "harness supports Lambert materials only\n"); return 2; }
+        PrincipalSpectrum r = from_reflectance_rgb(Vector3f(m.rgb[0], m.rgb[1], m.rgb[2]));
+        materials.push_back(std::make_shared<LambertMaterial>(std::make_shared<ConstantTexture<PrincipalSpectrum>>(r)));
+    }
+    std::vector<std::shared_ptr<Shape>> shapes(h.n_tri);
+    for (uint32_t i = 0; i < h.n_tri; ++i) {
+        const float *v = &verts[9 * (size_t)i];
+        shapes[i] = std::make_shared<Triangle>(TriangleEntity(Vector3f(v[0], v[1], v[2])),
+                                               TriangleEntity(Vector3f(v[3], v[4], v[5])),
+                                               TriangleEntity(Vector3f(v[6], v[7], v[8])), false);
+    }
+    std::vector<std::shared_ptr<AreaIlluminant>> tri_light(h.n_tri);
+    std::vector<std::shared_ptr<Illuminant>> illuminants;
+    for (const auto &l : lights) {
+        if (l.type != FL_LIGHT_TRIANGLE || l.tri >= h.n_tri) {
+            fprintf(stderr, "harness supports triangle area lights only\n");
+            return 2;
+        }
+        auto al = std::make_shared<DiffuseAreaIlluminant>(Transform(), PrincipalSpectrum(1.f), l.radiance, (short)2,
+                                                          PrincipalSpectrum(0.f), shapes[l.tri]);
+        tri_light[l.tri] = al;
+        illuminants.push_back(al);
+    }
+    std::vector<std::shared_ptr<GeometricPrimitive>> prims(h.n_tri);
+    SceneGeometry geom;
+    auto mesh = std::make_shared<TriangleMesh>();
+    ref_shim::g_primitives.assign(h.n_tri, nullptr);
+    for (uint32_t i = 0; i < h.n_tri; ++i) {
+        prims[i] = std::make_shared<GeometricPrimitive>(shapes[i], materials[tri_mat[i]], tri_light[i]);
+        ref_shim::g_primitives[i] = prims[i].get();
+        auto bt = std::make_shared<BasicTriangle>();
+        const float *v = &verts[9 * (size_t)i];
+        bt->v1 = Vector3f(v[0], v[1], v[2]);
+        bt->v2 = Vector3f(v[3], v[4], v[5]);
+        bt->v3 = Vector3f(v[6], v[7], v[8]);
+        mesh->triangles.push_back(bt);
+    }
+    geom.triangleMeshes.push_back(mesh);
+    Scene scene(geom, illuminants);
+
+    const fl_camera &c = h.cam;
+    PhysicalCamera camera(Vector3f(c.position[0], c.position[1], c.position[2]),
+                          Vector3f(c.look_at[0], c.look_at[1], c.look_at[2]), c.width, c.height, c.vfov_deg, 0.f, 0.f,
+                          0.f, Vector3f(c.up[0], c.up[1], c.up[2]), true);
+    RenderParams rp{(int)h.spp, (int)h.max_depth, (int)h.max_depth, (int)h.max_depth};
+    PathIntegrator integrator(rp, h.rr_threshold);
+
+    const uint32_t W = (uint32_t)c.width, H = (uint32_t)c.height;
+    const uint32_t total = h.n_pixels ? h.n_pixels : W * H;
+    std::vector<double> film((size_t)W * H * 3, 0.0);
+    std::atomic<uint32_t> next{0};
+    unsigned nth = h.nthreads ? h.nthreads : std::thread::hardware_concurrency();
+    if (nth == 0) nth = 1;
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> threads;
+    for (unsigned k = 0; k < nth; ++k) {
+        threads.emplace_back([&]() {
+            PCG32Sampler sampler;
+            for (;;) {
+                uint32_t start = next.fetch_add(64);
+                if (start >= total) break;
+                uint32_t end = std::min(total, start + 64);
+                for (uint32_t q = start; q < end; ++q) {
+                    uint32_t pixel = h.n_pixels ? pixels[q] : q;
+                    uint32_t px = pixel % W, py = pixel / W;
+                    double acc[3] = {0, 0, 0};
+                    for (uint32_t s = 0; s < h.spp; ++s) {
+                        sampler.reset(pixel, (uint64_t)h.sample_offset + s);
+                        float ux = sampler.get_1d();
+                        float uy = sampler.get_1d();
+                        (void)sampler.get_1d(); /* hero-wavelength draw, unused by 60 bins */
+                        float sx = ((float)px + ux) / (float)W;
+                        float sy = ((float)(H - 1u - py) + uy) / (float)H;
+                        Ray ray = camera.awaken_ray(Vector2f(sx, sy), Vector2f(0.5f, 0.5f));
+                        PrincipalSpectrum L = integrator.Li(ray, scene, sampler, 0);
+                        Vector3f xyz = to_xyz(L);
+                        acc[0] += xyz.x;
+                        acc[1] += xyz.y;
+                        acc[2] += xyz.z;
+                    }
+                    film[3 * (size_t)pixel + 0] = acc[0];
+                    film[3 * (size_t)pixel + 1] = acc[1];
+                    film[3 * (size_t)pixel + 2] = acc[2];
+                }
+            }
+        });
+    }
+    for (auto &t : threads) t.join();
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    FILE *o = fopen(out_path, "wb");
+    if (!o) return 2;
+    fwrite(film.data(), sizeof(double), film.size(), o);
+    fclose(o);
+    printf("{\"pixels\": %u, \"spp\": %u, \"threads\": %u, \"seconds\": %.6f}\n", total, h.spp, nth, secs);
+    return 0;
+}
+
+} // namespace
+
+int main(int argc, char **argv) {
+    if (argc == 3 && strcmp(argv[1], "--tables") == 0) return dump_tables(argv[2]);
+    if (argc == 3 && strcmp(argv[1], "--pcg") == 0) return dump_pcg(argv[2]);
+    if (argc == 3) return render(argv[1], argv[2]);
+    fprintf(stderr, "usage: ref_render SCENE.bin OUT.bin | --tables OUT.bin | --pcg OUT.bin\n");
+    return 1;
+}

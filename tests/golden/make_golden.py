@@ -1,0 +1,65 @@
+"""Generates the committed fixtures under tests/golden/ from the reference itself.
+
+Runs only where the reference tree is present (it builds oracle/_ref/ref_render from the
+reference sources with oracle/Makefile). Outputs:
+  spectral_tables.npz   the reference's spectral data (color/cie.h: CIE 1931 observer,
+                        RGB->spectrum bases) as the reference binary reads them, plus the
+                        60-bin tables InitializeSpectrals builds and from_reflectance_rgb /
+                        to_xyz known answers
+  pcg32_kat.npz         pcg32 sequences from the vendored src/ext/pcg32.h
+  cornell_ref.npz       the reference integrator's XYZ film sums for the 36-triangle Cornell
+                        box: 64x64 at 4 spp (float64) and 256x256 at 16 spp (float32)
+Usage: python tests/golden/make_golden.py
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "filianore-core_b200"))
+
+import oracle  # noqa: E402
+from filianore_b200 import scenes, types as T  # noqa: E402
+
+
+def main():
+    oracle.build(ref=True)
+    tmp = tempfile.mkdtemp()
+    # spectral tables
+    tpath = os.path.join(tmp, "tables.bin")
+    import subprocess
+    subprocess.run([oracle.REF_BIN, "--tables", tpath], check=True)
+    t = oracle.load_tables_dump(tpath)
+    np.savez_compressed(os.path.join(HERE, "spectral_tables.npz"), **t)
+    # pcg32
+    ppath = os.path.join(tmp, "pcg.bin")
+    subprocess.run([oracle.REF_BIN, "--pcg", ppath], check=True)
+    raw = np.fromfile(ppath, np.uint8)
+    seq = np.frombuffer(raw[: 5 * 16 * 4], np.uint32).reshape(5, 16)
+    adv = np.frombuffer(raw[5 * 16 * 4: 5 * 16 * 4 + 3 * 8 * 4], np.uint32).reshape(3, 8)
+    flt = np.frombuffer(raw[5 * 16 * 4 + 3 * 8 * 4:], np.float32)
+    np.savez_compressed(os.path.join(HERE, "pcg32_kat.npz"),
+                        seeds=np.array([[0, 1], [1, 1], [12345, 1], [42, 54], [65535, 1]], np.uint64),
+                        seq=seq, adv_deltas=np.array([1, 1 << 16, 5 << 16], np.int64), adv=adv,
+                        float_seed=np.array([3, 1], np.uint64), floats=flt)
+    # Cornell box renders by the reference integrator
+    out = {}
+    for (W, H, spp, key, dt) in [(64, 64, 4, "small", np.float64), (256, 256, 16, "full", np.float32)]:
+        sc = scenes.cornell(W, H)
+        p = scenes.render_params(spp, 8, T.FL_SPECTRAL_BINS60)
+        spath = os.path.join(tmp, f"cornell_{key}.scene")
+        fpath = os.path.join(tmp, f"cornell_{key}.film")
+        oracle.write_scene_file(spath, sc, p)
+        film, info = oracle.run_reference(spath, fpath, W, H)
+        out[f"{key}_xyz"] = film.astype(dt)
+        out[f"{key}_spp"] = np.int32(spp)
+        print(key, info)
+    np.savez_compressed(os.path.join(HERE, "cornell_ref.npz"), **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,55 @@
+"""Pins the CPU oracle against the reference's own outputs (fixtures made by
+tests/golden/make_golden.py from the reference compiled in place)."""
+import os
+
+import numpy as np
+
+import oracle
+from filianore_b200 import scenes, types as T
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_pcg32_matches_vendored_pcg32():
+    g = np.load(os.path.join(GOLDEN, "pcg32_kat.npz"))
+    for (s, q), seq in zip(g["seeds"], g["seq"]):
+        assert np.array_equal(oracle.pcg32_sequence(int(s), int(q), 0, 16), seq)
+    for delta, seq in zip(g["adv_deltas"], g["adv"]):
+        assert np.array_equal(oracle.pcg32_sequence(7, 1, int(delta), 8), seq)
+
+
+def test_binned_tables_bit_exact(orc_tables, ref_tables):
+    # InitializeSpectrals (color/spectruminits.cpp:6-64) restated
+    assert np.array_equal(orc_tables.binned(), ref_tables["binned60"])
+
+
+def test_from_reflectance_rgb_bit_exact(orc_tables, ref_tables):
+    rgbs = [(0.725, 0.725, 0.725), (0.63, 0.065, 0.05), (0.14, 0.45, 0.091), (0.2, 0.9, 0.5)]
+    for rgb, want in zip(rgbs, ref_tables["refl60_kat"]):
+        assert np.array_equal(orc_tables.reflectance(rgb), want)
+
+
+def test_to_xyz_of_constant_spectrum(ref_tables):
+    # to_xyz(1) of the reference: Y of a unit constant spectrum is ~1 by construction
+    x = ref_tables["xyz_of_one"]
+    assert abs(float(x[1]) - 1.0) < 2e-3
+
+
+def test_oracle_render_equals_reference_integrator(orc_tables):
+    """60-bin restatement vs the reference's PathIntegrator on the Cornell box, same
+    per-pixel PCG streams: bit-exact at 64x64, 4 spp."""
+    g = np.load(os.path.join(GOLDEN, "cornell_ref.npz"))
+    sc = scenes.cornell(64, 64)
+    film, cnt = oracle.render(sc, orc_tables, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60))
+    assert cnt["paths"] == 64 * 64 * 4
+    assert np.array_equal(film, g["small_xyz"])
+
+
+def test_oracle_render_full_cornell_matches_reference(orc_tables):
+    """256x256, 16 spp, depth 8 (the CPU-runnable Cornell configuration); the fixture is
+    stored as float32, so the bound is float32 rounding."""
+    g = np.load(os.path.join(GOLDEN, "cornell_ref.npz"))
+    sc = scenes.cornell(256, 256)
+    film, _ = oracle.render(sc, orc_tables, scenes.render_params(16, 8, T.FL_SPECTRAL_BINS60))
+    ref = g["full_xyz"].astype(np.float64)
+    np.testing.assert_allclose(film, ref, rtol=2e-7, atol=1e-12)
