@@ -1,0 +1,375 @@
+// C ABI: contexts, spectral tables, scenes (include/filianore_gpu.h).
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "fl_internal.h"
+
+namespace fl {
+
+namespace {
+std::mutex g_err_mu;
+std::string g_last_error;  // errors not tied to a context (creation failures)
+}  // namespace
+
+void set_error(Context *ctx, const std::string &msg) {
+    if (ctx) ctx->last_error = msg;
+    std::lock_guard<std::mutex> lock(g_err_mu);
+    g_last_error = msg;
+}
+
+fl_status cuda_status(Context *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return FL_OK;
+    set_error(ctx, std::string(what) + ": " + cudaGetErrorString(e));
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation) return FL_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInvalidDevice || e == cudaErrorNoKernelImageForDevice ||
+        e == cudaErrorInsufficientDriver)
+        return FL_ERR_NO_DEVICE;
+    return FL_ERR_CUDA;
+}
+
+fl_status ensure_scratch(Context *ctx, size_t bytes, void **out) {
+    if (bytes > ctx->scratch_bytes) {
+        if (ctx->scratch) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ctx->scratch);
+            ctx->scratch = nullptr;
+            ctx->scratch_bytes = 0;
+        }
+        size_t want = bytes + bytes / 4;
+        cudaError_t e = cudaMalloc(&ctx->scratch, want);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "scratch allocation");
+        ctx->scratch_bytes = want;
+    }
+    *out = ctx->scratch;
+    return FL_OK;
+}
+
+// average_spectrum_samples (src/filianore/color/spectrumoperations.cpp:28-56), with the
+// reference's float/double mixing, so the 60-bin tables equal InitializeSpectrals'.
+static float lerp_ref(float t, float v1, float v2) { return (1.f - t) * v1 + t * v2; }
+
+float average_spectrum_samples(const float *wl, const float *vals, int n, float ws, float we) {
+    if (we <= wl[0]) return vals[0];
+    if (ws >= wl[n - 1]) return vals[n - 1];
+    if (n == 1) return vals[0];
+    float sum = 0;
+    if (ws < wl[0]) sum += vals[0] * (wl[0] - ws);
+    if (we > wl[n - 1]) sum += vals[n - 1] * (we - wl[n - 1]);
+    int i = 0;
+    while (ws > wl[i + 1]) ++i;
+    for (; i + 1 < n && we >= wl[i]; ++i) {
+        const float ss = std::max(ws, wl[i]);
+        const float se = std::min(we, wl[i + 1]);
+        const float ia = lerp_ref((ss - wl[i]) / (wl[i + 1] - wl[i]), vals[i], vals[i + 1]);
+        const float ib = lerp_ref((se - wl[i]) / (wl[i + 1] - wl[i]), vals[i], vals[i + 1]);
+        sum = (float)((double)sum + 0.5 * (double)(ia + ib) * (double)(se - ss));
+    }
+    return sum / (we - ws);
+}
+
+// Smits terms of from_reflectance_rgb (color/spectrumoperations.cpp:113-147): basis ids
+// (0 white, 1 cyan, 2 magenta, 3 yellow, 4 red, 5 green, 6 blue) and weights, in its order.
+void smits_terms(const float rgb[3], int basis[3], float w[3]) {
+    if (rgb[0] <= rgb[1] && rgb[0] <= rgb[2]) {
+        basis[0] = 0; w[0] = rgb[0];
+        if (rgb[1] <= rgb[2]) { basis[1] = 1; w[1] = rgb[1] - rgb[0]; basis[2] = 6; w[2] = rgb[2] - rgb[1]; }
+        else { basis[1] = 1; w[1] = rgb[2] - rgb[0]; basis[2] = 5; w[2] = rgb[1] - rgb[2]; }
+    } else if (rgb[1] <= rgb[0] && rgb[1] <= rgb[2]) {
+        basis[0] = 0; w[0] = rgb[1];
+        if (rgb[0] <= rgb[2]) { basis[1] = 2; w[1] = rgb[0] - rgb[1]; basis[2] = 6; w[2] = rgb[2] - rgb[0]; }
+        else { basis[1] = 2; w[1] = rgb[2] - rgb[1]; basis[2] = 4; w[2] = rgb[0] - rgb[2]; }
+    } else {
+        basis[0] = 0; w[0] = rgb[2];
+        if (rgb[0] <= rgb[1]) { basis[1] = 3; w[1] = rgb[0] - rgb[2]; basis[2] = 5; w[2] = rgb[1] - rgb[0]; }
+        else { basis[1] = 3; w[1] = rgb[1] - rgb[2]; basis[2] = 4; w[2] = rgb[0] - rgb[1]; }
+    }
+}
+
+}  // namespace fl
+
+using namespace fl;
+
+extern "C" {
+
+const char *fl_status_string(fl_status s) {
+    switch (s) {
+    case FL_OK: return "FL_OK";
+    case FL_ERR_INVALID: return "FL_ERR_INVALID";
+    case FL_ERR_OOM: return "FL_ERR_OOM";
+    case FL_ERR_CUDA: return "FL_ERR_CUDA";
+    case FL_ERR_TIMEOUT: return "FL_ERR_TIMEOUT";
+    case FL_ERR_TRAVERSAL: return "FL_ERR_TRAVERSAL";
+    case FL_ERR_NOT_READY: return "FL_ERR_NOT_READY";
+    case FL_ERR_CAPACITY: return "FL_ERR_CAPACITY";
+    case FL_ERR_NO_DEVICE: return "FL_ERR_NO_DEVICE";
+    default: return "FL_ERR_UNKNOWN";
+    }
+}
+
+fl_status fl_last_error(const fl_context *ctx_h, char *buf, size_t n) {
+    if (!buf || n == 0) return FL_ERR_INVALID;
+    const Context *ctx = reinterpret_cast<const Context *>(ctx_h);
+    std::string msg;
+    if (ctx) msg = ctx->last_error;
+    else {
+        std::lock_guard<std::mutex> lock(g_err_mu);
+        msg = g_last_error;
+    }
+    std::snprintf(buf, n, "%s", msg.c_str());
+    return FL_OK;
+}
+
+fl_status fl_context_create(int32_t device, const fl_spectral_tables *t, fl_context **out) {
+    if (!out) return FL_ERR_INVALID;
+    *out = nullptr;
+    if (!t || !t->cie_lambda || !t->cie_x || !t->cie_y || !t->cie_z || t->n_cie < 2 || !t->rgb2spec_lambda ||
+        t->n_rgb2spec < 2) {
+        set_error(nullptr, "incomplete spectral tables");
+        return FL_ERR_INVALID;
+    }
+    for (int b = 0; b < 7; ++b)
+        if (!t->refl[b] || !t->illum[b]) {
+            set_error(nullptr, "missing RGB-to-spectrum basis");
+            return FL_ERR_INVALID;
+        }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error(nullptr, "no CUDA device");
+        return FL_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) {
+        set_error(nullptr, "device index out of range");
+        return FL_ERR_INVALID;
+    }
+    Context *ctx = new Context();
+    ctx->device = device;
+    fl_status rc;
+#define CTX_TRY(call)                                        \
+    do {                                                     \
+        cudaError_t _e = (call);                             \
+        if (_e != cudaSuccess) {                             \
+            rc = cuda_status(nullptr, _e, #call);            \
+            fl_context_destroy(reinterpret_cast<fl_context *>(ctx)); \
+            return rc;                                       \
+        }                                                    \
+    } while (0)
+    CTX_TRY(cudaSetDevice(device));
+    CTX_TRY(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+    CTX_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CTX_TRY(cudaMalloc(&ctx->d_error, sizeof(int) * 4));
+    CTX_TRY(cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * 8));
+
+    // 60-bin tables as InitializeSpectrals builds them (color/spectruminits.cpp:6-64)
+    ctx->binned_host.assign(17 * 60, 0.f);
+    for (int i = 0; i < 60; ++i) {
+        const float wl0 = lerp_ref((float)i / 60.f, 400.f, 700.f);
+        const float wl1 = lerp_ref((float)(i + 1) / 60.f, 400.f, 700.f);
+        ctx->binned_host[i] = average_spectrum_samples(t->cie_lambda, t->cie_x, t->n_cie, wl0, wl1);
+        ctx->binned_host[60 + i] = average_spectrum_samples(t->cie_lambda, t->cie_y, t->n_cie, wl0, wl1);
+        ctx->binned_host[120 + i] = average_spectrum_samples(t->cie_lambda, t->cie_z, t->n_cie, wl0, wl1);
+        for (int b = 0; b < 7; ++b) {
+            ctx->binned_host[180 + 60 * b + i] =
+                average_spectrum_samples(t->rgb2spec_lambda, t->refl[b], t->n_rgb2spec, wl0, wl1);
+            ctx->binned_host[600 + 60 * b + i] =
+                average_spectrum_samples(t->rgb2spec_lambda, t->illum[b], t->n_rgb2spec, wl0, wl1);
+        }
+    }
+    SpectralTablesDev &T = ctx->tables;
+    T.cie_lambda0 = t->cie_lambda[0];
+    T.n_cie = t->n_cie;
+    T.cie_y_integral = t->cie_y_integral;
+    T.rgb_lambda0 = t->rgb2spec_lambda[0];
+    T.rgb_lambda1 = t->rgb2spec_lambda[t->n_rgb2spec - 1];
+    T.n_rgb = t->n_rgb2spec;
+    std::vector<float> cie(3 * (size_t)t->n_cie), bases(14 * (size_t)t->n_rgb2spec);
+    std::memcpy(cie.data(), t->cie_x, sizeof(float) * t->n_cie);
+    std::memcpy(cie.data() + t->n_cie, t->cie_y, sizeof(float) * t->n_cie);
+    std::memcpy(cie.data() + 2 * t->n_cie, t->cie_z, sizeof(float) * t->n_cie);
+    for (int b = 0; b < 7; ++b) {
+        std::memcpy(bases.data() + (size_t)b * t->n_rgb2spec, t->refl[b], sizeof(float) * t->n_rgb2spec);
+        std::memcpy(bases.data() + (size_t)(7 + b) * t->n_rgb2spec, t->illum[b], sizeof(float) * t->n_rgb2spec);
+    }
+    CTX_TRY(cudaMalloc(&T.cie_xyz, sizeof(float) * cie.size()));
+    CTX_TRY(cudaMalloc(&T.rgb_bases, sizeof(float) * bases.size()));
+    CTX_TRY(cudaMalloc(&T.binned, sizeof(float) * 17 * 60));
+    CTX_TRY(cudaMemcpy(T.cie_xyz, cie.data(), sizeof(float) * cie.size(), cudaMemcpyHostToDevice));
+    CTX_TRY(cudaMemcpy(T.rgb_bases, bases.data(), sizeof(float) * bases.size(), cudaMemcpyHostToDevice));
+    CTX_TRY(cudaMemcpy(T.binned, ctx->binned_host.data(), sizeof(float) * 17 * 60, cudaMemcpyHostToDevice));
+#undef CTX_TRY
+    *out = reinterpret_cast<fl_context *>(ctx);
+    return FL_OK;
+}
+
+fl_status fl_context_destroy(fl_context *ctx_h) {
+    Context *ctx = reinterpret_cast<Context *>(ctx_h);
+    if (!ctx) return FL_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->scratch);
+    cudaFree(ctx->d_error);
+    cudaFree(ctx->d_counters);
+    cudaFree(ctx->tables.cie_xyz);
+    cudaFree(ctx->tables.rgb_bases);
+    cudaFree(ctx->tables.binned);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return FL_OK;
+}
+
+fl_status fl_context_binned_tables(const fl_context *ctx_h, float *out, size_t n) {
+    const Context *ctx = reinterpret_cast<const Context *>(ctx_h);
+    if (!ctx || !out || n < 17 * 60) return FL_ERR_INVALID;
+    std::memcpy(out, ctx->binned_host.data(), sizeof(float) * 17 * 60);
+    return FL_OK;
+}
+
+fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **out) {
+    Context *ctx = reinterpret_cast<Context *>(ctx_h);
+    if (!ctx || !d || !out) return FL_ERR_INVALID;
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if ((d->n_tri && !d->verts) || (d->n_lights && !d->lights) || (d->n_materials == 0 || !d->materials)) {
+        set_error(ctx, "scene needs vertices for its triangles and at least one material");
+        return FL_ERR_INVALID;
+    }
+    for (uint32_t i = 0; i < d->n_materials; ++i)
+        if (d->materials[i].type < FL_MAT_LAMBERT || d->materials[i].type > FL_MAT_SMOOTH_DIELECTRIC) {
+            set_error(ctx, "unknown material type");
+            return FL_ERR_INVALID;
+        }
+    if (d->tri_material)
+        for (uint32_t i = 0; i < d->n_tri; ++i)
+            if (d->tri_material[i] >= d->n_materials) {
+                set_error(ctx, "triangle material index out of range");
+                return FL_ERR_INVALID;
+            }
+    std::vector<int32_t> tri_light(d->n_tri, -1);
+    Scene *s = new Scene();
+    s->ctx = ctx;
+    s->n_tri = d->n_tri;
+    for (uint32_t l = 0; l < d->n_lights; ++l) {
+        const fl_light &L = d->lights[l];
+        if (L.type == FL_LIGHT_TRIANGLE) {
+            if (L.tri >= d->n_tri) {
+                delete s;
+                set_error(ctx, "light triangle index out of range");
+                return FL_ERR_INVALID;
+            }
+            tri_light[L.tri] = (int32_t)l;
+            s->n_emissive_tris++;
+        } else if (L.type == FL_LIGHT_ENV) {
+            s->has_env = 1;
+            s->env_radiance = L.radiance;
+        } else if (L.type != FL_LIGHT_SPHERE) {
+            delete s;
+            set_error(ctx, "unknown light type");
+            return FL_ERR_INVALID;
+        }
+        s->lights_host.push_back(L);
+    }
+    std::vector<LightDev> lights_dev;
+    for (uint32_t l = 0; l < d->n_lights; ++l) {
+        const fl_light &L = d->lights[l];
+        LightDev ld{};
+        ld.type = L.type;
+        ld.tri = L.tri;
+        ld.radiance = L.radiance;
+        ld.radius = L.radius;
+        ld.cx = L.center[0]; ld.cy = L.center[1]; ld.cz = L.center[2];
+        if (L.type == FL_LIGHT_TRIANGLE) {
+            const float *v = d->verts + 9 * (size_t)L.tri;
+            v3 a = mk(v[0], v[1], v[2]), b = mk(v[3], v[4], v[5]), c = mk(v[6], v[7], v[8]);
+            ld.area = 0.5f * len(cross(sub(b, a), sub(c, a)));  // Triangle::area, triangle.cpp:130-132
+        } else if (L.type == FL_LIGHT_SPHERE) {
+            ld.area = 4.f * kPi * L.radius * L.radius;
+        }
+        lights_dev.push_back(ld);
+    }
+    for (uint32_t m = 0; m < d->n_materials; ++m) {
+        const fl_material &M = d->materials[m];
+        MaterialDev md{};
+        md.type = M.type;
+        md.rgb[0] = M.rgb[0]; md.rgb[1] = M.rgb[1]; md.rgb[2] = M.rgb[2];
+        const float a = M.roughness * M.roughness;
+        md.ax = md.ay = a > 0.001f ? a : 0.001f;  // GGXDistribution clamps alpha (ggx.cpp:7-10)
+        md.eta = M.eta;
+        md.k = M.k;
+        smits_terms(M.rgb, md.basis, md.w);
+        s->materials_host.push_back(md);
+    }
+    s->n_lights = d->n_lights;
+    s->n_materials = d->n_materials;
+
+    auto fail = [&](fl_status rc) {
+        fl_scene_destroy(reinterpret_cast<fl_scene *>(s));
+        return rc;
+    };
+    cudaError_t e;
+#define SC_TRY(call)                                            \
+    do {                                                        \
+        e = (call);                                             \
+        if (e != cudaSuccess) return fail(cuda_status(ctx, e, #call)); \
+    } while (0)
+    SC_TRY(cudaSetDevice(ctx->device));
+    const size_t nt = d->n_tri ? d->n_tri : 1;
+    SC_TRY(cudaMalloc(&s->soup, sizeof(float) * 9 * nt));
+    SC_TRY(cudaMalloc(&s->tri_material, sizeof(uint32_t) * nt));
+    SC_TRY(cudaMalloc(&s->tri_light, sizeof(int32_t) * nt));
+    SC_TRY(cudaMalloc(&s->materials, sizeof(MaterialDev) * d->n_materials));
+    SC_TRY(cudaMalloc(&s->lights, sizeof(LightDev) * (d->n_lights ? d->n_lights : 1)));
+    if (d->n_tri) {
+        SC_TRY(cudaMemcpyAsync(s->soup, d->verts, sizeof(float) * 9 * d->n_tri, cudaMemcpyHostToDevice, ctx->stream));
+        if (d->tri_material)
+            SC_TRY(cudaMemcpyAsync(s->tri_material, d->tri_material, sizeof(uint32_t) * d->n_tri,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+        else
+            SC_TRY(cudaMemsetAsync(s->tri_material, 0, sizeof(uint32_t) * d->n_tri, ctx->stream));
+        SC_TRY(cudaMemcpyAsync(s->tri_light, tri_light.data(), sizeof(int32_t) * d->n_tri, cudaMemcpyHostToDevice,
+                               ctx->stream));
+    }
+    SC_TRY(cudaMemcpyAsync(s->materials, s->materials_host.data(), sizeof(MaterialDev) * d->n_materials,
+                           cudaMemcpyHostToDevice, ctx->stream));
+    if (d->n_lights)
+        SC_TRY(cudaMemcpyAsync(s->lights, lights_dev.data(), sizeof(LightDev) * d->n_lights, cudaMemcpyHostToDevice,
+                               ctx->stream));
+#undef SC_TRY
+    fl_status rc = build_bvh(s);
+    if (rc != FL_OK) return fail(rc);
+    *out = reinterpret_cast<fl_scene *>(s);
+    return FL_OK;
+}
+
+fl_status fl_scene_destroy(fl_scene *scene) {
+    Scene *s = reinterpret_cast<Scene *>(scene);
+    if (!s) return FL_ERR_INVALID;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    cudaFree(s->nodes);
+    cudaFree(s->tris);
+    cudaFree(s->soup);
+    cudaFree(s->tri_material);
+    cudaFree(s->tri_light);
+    cudaFree(s->materials);
+    cudaFree(s->lights);
+    delete s;
+    return FL_OK;
+}
+
+fl_status fl_scene_get_info(const fl_scene *scene, fl_scene_info *info) {
+    const Scene *s = reinterpret_cast<const Scene *>(scene);
+    if (!s || !info) return FL_ERR_INVALID;
+    info->n_tri = s->n_tri;
+    info->n_nodes = s->n_nodes;
+    info->n_leaves = s->n_leaves;
+    info->max_depth = s->max_depth;
+    info->bvh_bytes = (uint64_t)s->n_nodes * sizeof(WideNode) + (uint64_t)s->n_tri * 48u;
+    info->build_ms = s->build_ms;
+    return FL_OK;
+}
+
+}  // extern "C"

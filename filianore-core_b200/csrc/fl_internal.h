@@ -1,0 +1,107 @@
+// Internal host-side state behind the opaque handles of include/filianore_gpu.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/filianore_gpu.h"
+#include "fl_device.cuh"
+
+namespace fl {
+
+// Device-resident spectral tables (raw tables for hero wavelengths, 60-bin tables for
+// the reference's fixed bins). Staged into shared memory by the shading kernels.
+struct SpectralTablesDev {
+    float cie_lambda0;      // first CIE wavelength (1 nm spacing)
+    int n_cie;
+    float cie_y_integral;
+    float rgb_lambda0, rgb_lambda1;
+    int n_rgb;
+    float *cie_xyz;         // 3 * n_cie (x, y, z rows)
+    float *rgb_bases;       // 14 * n_rgb (refl 0..6, illum 0..6)
+    float *binned;          // 17 * 60 (X, Y, Z, refl 0..6, illum 0..6)
+};
+
+struct Context {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string last_error;
+    std::vector<float> binned_host;  // 17 * 60
+    SpectralTablesDev tables{};
+    // grow-only scratch owned by the context (render wavefront state, trace staging)
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int *d_error = nullptr;             // traversal error counter
+    unsigned long long *d_counters = nullptr;  // 8 x u64 statistics
+};
+
+// Device material record (constant over the render).
+struct MaterialDev {
+    int type;
+    float rgb[3];
+    float ax, ay;
+    float eta, k;
+    int basis[3];       // Smits basis indices of from_reflectance_rgb
+    float w[3];         // and their weights
+};
+
+struct LightDev {
+    int type;
+    uint32_t tri;
+    float radiance;
+    float radius;
+    float cx, cy, cz;
+    float area;         // triangle or sphere area
+};
+
+struct Scene {
+    Context *ctx = nullptr;
+    uint32_t n_tri = 0;
+    uint32_t n_nodes = 0;
+    uint32_t n_leaves = 0;
+    uint32_t max_depth = 0;
+    double build_ms = 0.0;
+    WideNode *nodes = nullptr;        // n_nodes
+    float4 *tris = nullptr;           // 3 * n_tri, BVH order
+    float *soup = nullptr;            // 9 * n_tri, soup order (hit records, light sampling)
+    uint32_t *tri_material = nullptr; // soup order
+    int32_t *tri_light = nullptr;     // soup order, -1 = not emissive
+    MaterialDev *materials = nullptr;
+    uint32_t n_materials = 0;
+    LightDev *lights = nullptr;
+    uint32_t n_lights = 0;
+    uint32_t n_emissive_tris = 0;
+    int has_env = 0;
+    float env_radiance = 0.f;
+    std::vector<fl_light> lights_host;
+    std::vector<MaterialDev> materials_host;
+};
+
+// error plumbing -----------------------------------------------------------------------
+void set_error(Context *ctx, const std::string &msg);
+fl_status cuda_status(Context *ctx, cudaError_t e, const char *what);
+
+#define FL_CUDA_TRY(ctx, call)                                    \
+    do {                                                          \
+        cudaError_t _e = (call);                                  \
+        if (_e != cudaSuccess) return cuda_status(ctx, _e, #call); \
+    } while (0)
+
+// BVH build (fl_bvh_build.cu): builds nodes/tris of `s` from s->soup on ctx->stream.
+fl_status build_bvh(Scene *s);
+
+// traversal launches (fl_trace.cu); arrays are device pointers.
+enum TraceKind { kTraceClosest = 0, kTraceOccluded = 1, kTraceCount = 2 };
+fl_status launch_trace(Scene *s, const float4 *org_tmin, const float4 *dir_tmax, uint32_t n, fl_hit *hits,
+                       uint8_t *occluded, int kind, cudaStream_t stream);
+
+// context scratch: returns a device buffer of at least `bytes` (grow-only)
+fl_status ensure_scratch(Context *ctx, size_t bytes, void **out);
+
+}  // namespace fl

@@ -1,0 +1,180 @@
+// Batch ray queries: the replacement of BVH::intersect / rtcIntersect1
+// (src/filianore/bvh/bvh.cpp:49-84) and of the shadow test of
+// VisibilityEvaluator::unoccluded (src/filianore/illuminants/illuminant.cpp:40-50).
+#include <algorithm>
+
+#include "fl_internal.h"
+#include "fl_traverse.cuh"
+
+namespace fl {
+namespace {
+
+constexpr int kTraceBlock = 128;
+
+__device__ inline void warp_add_u64(unsigned long long *dst, uint32_t v) {
+    unsigned long long x = v;
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restrict__ nodes, uint32_t n_nodes,
+                                                       const float4 *__restrict__ tris, uint32_t n_tris,
+                                                       const int32_t *__restrict__ tri_light, int any_hit_ok,
+                                                       const float4 *__restrict__ org, const float4 *__restrict__ dir,
+                                                       uint32_t n, int4 *__restrict__ hits, uint8_t *__restrict__ occ,
+                                                       int *__restrict__ err, unsigned long long *__restrict__ counters) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    TraceStats st;
+    bool error = false;
+    TraceResult res;
+    res.id = -1;
+    res.t = 0.f; res.u = 0.f; res.v = 0.f;
+    if (active) {
+        const float4 o = __ldg(org + i);
+        const float4 d = __ldg(dir + i);
+        const RayPre r = ray_precompute(o, d);
+        res.t = r.tmax;
+        if (n_nodes > 0) {
+            if (KIND == kTraceOccluded && any_hit_ok)
+                res = traverse<true, false>(nodes, n_nodes, tris, n_tris, r, error, st);
+            else if (KIND == kTraceCount)
+                res = traverse<false, true>(nodes, n_nodes, tris, n_tris, r, error, st);
+            else
+                res = traverse<false, false>(nodes, n_nodes, tris, n_tris, r, error, st);
+        }
+        if (KIND == kTraceOccluded) {
+            // occluded unless nothing is hit or the closest hit carries an area light
+            occ[i] = (res.id >= 0 && (any_hit_ok || (uint32_t)res.id >= n_tris || tri_light[res.id] < 0)) ? 1 : 0;
+        } else if (KIND == kTraceClosest) {
+            int4 h;
+            h.x = res.id;
+            h.y = __float_as_int(res.t);
+            h.z = __float_as_int(res.id >= 0 ? res.u : 0.f);
+            h.w = __float_as_int(res.id >= 0 ? res.v : 0.f);
+            hits[i] = h;
+        }
+        if (error) atomicAdd(err, 1);
+    }
+    if (KIND == kTraceCount) {
+        warp_add_u64(&counters[0], st.nodes);
+        warp_add_u64(&counters[1], st.tris);
+    }
+}
+
+}  // namespace
+
+fl_status launch_trace(Scene *s, const float4 *org, const float4 *dir, uint32_t n, fl_hit *hits, uint8_t *occluded,
+                       int kind, cudaStream_t stream) {
+    if (n == 0) return FL_OK;
+    const uint32_t grid = (n + kTraceBlock - 1) / kTraceBlock;
+    const int any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
+    int4 *h = reinterpret_cast<int4 *>(hits);
+    switch (kind) {
+    case kTraceClosest:
+        k_trace<kTraceClosest><<<grid, kTraceBlock, 0, stream>>>(s->nodes, s->n_nodes, s->tris, s->n_tri, s->tri_light,
+                                                                 any_hit_ok, org, dir, n, h, occluded,
+                                                                 s->ctx->d_error, s->ctx->d_counters);
+        break;
+    case kTraceOccluded:
+        k_trace<kTraceOccluded><<<grid, kTraceBlock, 0, stream>>>(s->nodes, s->n_nodes, s->tris, s->n_tri, s->tri_light,
+                                                                  any_hit_ok, org, dir, n, h, occluded,
+                                                                  s->ctx->d_error, s->ctx->d_counters);
+        break;
+    default:
+        k_trace<kTraceCount><<<grid, kTraceBlock, 0, stream>>>(s->nodes, s->n_nodes, s->tris, s->n_tri, s->tri_light,
+                                                               any_hit_ok, org, dir, n, h, occluded, s->ctx->d_error,
+                                                               s->ctx->d_counters);
+        break;
+    }
+    return cuda_status(s->ctx, cudaGetLastError(), "trace launch");
+}
+
+}  // namespace fl
+
+using namespace fl;
+
+namespace {
+
+// Runs one query kind over n rays; host buffers are staged through context scratch in chunks.
+fl_status trace_common(fl_scene *scene_h, const float *org_tmin, const float *dir_tmax, uint32_t n, fl_hit *hits,
+                       uint8_t *occluded, int32_t memory, void *stream_v, int kind, uint64_t *nodes_out,
+                       uint64_t *tris_out) {
+    Scene *s = reinterpret_cast<Scene *>(scene_h);
+    if (!s) return FL_ERR_INVALID;
+    Context *ctx = s->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (n == 0) return FL_OK;
+    if (!org_tmin || !dir_tmax || (kind == kTraceClosest && !hits) || (kind == kTraceOccluded && !occluded)) {
+        set_error(ctx, "null ray or result buffer");
+        return FL_ERR_INVALID;
+    }
+    if (memory != FL_MEM_HOST && memory != FL_MEM_DEVICE) {
+        set_error(ctx, "memory must be FL_MEM_HOST or FL_MEM_DEVICE");
+        return FL_ERR_INVALID;
+    }
+    cudaStream_t st = stream_v ? reinterpret_cast<cudaStream_t>(stream_v) : ctx->stream;
+    FL_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_error, 0, sizeof(int), st));
+    FL_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_counters, 0, 8 * sizeof(unsigned long long), st));
+    fl_status rc = FL_OK;
+    if (memory == FL_MEM_DEVICE) {
+        rc = launch_trace(s, reinterpret_cast<const float4 *>(org_tmin), reinterpret_cast<const float4 *>(dir_tmax), n,
+                          hits, occluded, kind, st);
+        if (rc) return rc;
+    } else {
+        const uint32_t chunk = std::min<uint32_t>(n, 1u << 24);
+        const size_t per_ray = 32 + 16 + 1;
+        void *scratch = nullptr;
+        if ((rc = ensure_scratch(ctx, (size_t)chunk * per_ray + 256, &scratch))) return rc;
+        float4 *d_org = reinterpret_cast<float4 *>(scratch);
+        float4 *d_dir = d_org + chunk;
+        fl_hit *d_hits = reinterpret_cast<fl_hit *>(d_dir + chunk);
+        uint8_t *d_occ = reinterpret_cast<uint8_t *>(d_hits + chunk);
+        for (uint32_t off = 0; off < n; off += chunk) {
+            const uint32_t m = std::min(chunk, n - off);
+            FL_CUDA_TRY(ctx, cudaMemcpyAsync(d_org, org_tmin + 4 * (size_t)off, 16 * (size_t)m, cudaMemcpyHostToDevice, st));
+            FL_CUDA_TRY(ctx, cudaMemcpyAsync(d_dir, dir_tmax + 4 * (size_t)off, 16 * (size_t)m, cudaMemcpyHostToDevice, st));
+            if ((rc = launch_trace(s, d_org, d_dir, m, d_hits, d_occ, kind, st))) return rc;
+            if (kind == kTraceClosest)
+                FL_CUDA_TRY(ctx, cudaMemcpyAsync(hits + off, d_hits, 16 * (size_t)m, cudaMemcpyDeviceToHost, st));
+            else if (kind == kTraceOccluded)
+                FL_CUDA_TRY(ctx, cudaMemcpyAsync(occluded + off, d_occ, m, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    int err = 0;
+    unsigned long long cnt[2] = {0, 0};
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(&err, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    FL_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (nodes_out) *nodes_out = cnt[0];
+    if (tris_out) *tris_out = cnt[1];
+    if (err) {
+        set_error(ctx, std::to_string(err) + " rays hit the traversal stack or iteration bound");
+        return FL_ERR_TRAVERSAL;
+    }
+    return FL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fl_status fl_trace_closest(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n, fl_hit *hits,
+                           int32_t memory, void *stream) {
+    return trace_common(scene, org_tmin, dir_tmax, n, hits, nullptr, memory, stream, kTraceClosest, nullptr, nullptr);
+}
+
+fl_status fl_trace_occluded(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
+                            uint8_t *occluded, int32_t memory, void *stream) {
+    return trace_common(scene, org_tmin, dir_tmax, n, nullptr, occluded, memory, stream, kTraceOccluded, nullptr,
+                        nullptr);
+}
+
+fl_status fl_trace_count(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n, int32_t memory,
+                         uint64_t *nodes_visited, uint64_t *tris_tested) {
+    return trace_common(scene, org_tmin, dir_tmax, n, nullptr, nullptr, memory, nullptr, kTraceCount, nodes_visited,
+                        tris_tested);
+}
+
+}  // extern "C"

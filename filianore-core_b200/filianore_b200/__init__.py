@@ -1,0 +1,218 @@
+"""Python binding of the filianore B200 backend (ctypes over lib/libfilianore_b200.so).
+
+The library is the product: a C ABI (include/filianore_gpu.h) over hand-written sm_100a
+kernels. This module only marshals arguments; it has no compute path of its own, and it
+raises if the shared library is missing or fails to load.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import types as T
+from .types import *  # noqa: F401,F403
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libfilianore_b200.so")
+ROOT = os.path.dirname(PKG_DIR)
+TABLES_PATH = os.path.join(ROOT, "tests", "golden", "spectral_tables.npz")
+
+EXPORTED = [
+    "fl_context_create", "fl_context_destroy", "fl_status_string", "fl_last_error", "fl_context_binned_tables",
+    "fl_scene_create", "fl_scene_destroy", "fl_scene_get_info", "fl_trace_closest", "fl_trace_occluded",
+    "fl_trace_count", "fl_render",
+]
+
+_lib = None
+
+
+class FlError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} ({status})")
+        self.status = status
+
+
+def build() -> None:
+    import subprocess
+    subprocess.run(["make", "-s", "-C", PKG_DIR], check=True)
+
+
+def lib():
+    """Loads the shared library (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FlError(-8, f"{LIB_PATH} is not built; run `make -C {PKG_DIR}`")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        vp = C.c_void_p
+        L.fl_status_string.restype = C.c_char_p
+        L.fl_status_string.argtypes = [C.c_int32]
+        L.fl_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+        L.fl_context_create.argtypes = [C.c_int32, P(T.fl_spectral_tables), P(vp)]
+        L.fl_context_destroy.argtypes = [vp]
+        L.fl_context_binned_tables.argtypes = [vp, P(C.c_float), C.c_size_t]
+        L.fl_scene_create.argtypes = [vp, P(T.fl_scene_desc), P(vp)]
+        L.fl_scene_destroy.argtypes = [vp]
+        L.fl_scene_get_info.argtypes = [vp, P(T.fl_scene_info)]
+        L.fl_trace_closest.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_int32, vp]
+        L.fl_trace_occluded.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_int32, vp]
+        L.fl_trace_count.argtypes = [vp, vp, vp, C.c_uint32, C.c_int32, P(C.c_uint64), P(C.c_uint64)]
+        L.fl_render.argtypes = [vp, P(T.fl_camera), P(T.fl_render_params), vp, vp, C.c_int32, P(T.fl_render_stats)]
+        for name in EXPORTED:
+            if name not in ("fl_status_string",):
+                getattr(L, name).restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def check(status, ctx=None):
+    if status != 0:
+        buf = C.create_string_buffer(1024)
+        lib().fl_last_error(ctx, buf, 1024)
+        raise FlError(status, f"{lib().fl_status_string(status).decode()}: {buf.value.decode()}")
+
+
+def reference_tables(path: str = TABLES_PATH) -> dict:
+    """The reference's spectral data (color/cie.h) as stored by tests/golden/make_golden.py."""
+    return dict(np.load(path))
+
+
+def _tables_struct(t: dict):
+    keep = {k: np.ascontiguousarray(t[k], np.float32) for k in ("cie_lambda", "cie_x", "cie_y", "cie_z", "rgb_lambda")}
+    refl = [np.ascontiguousarray(r, np.float32) for r in t["refl"]]
+    illum = [np.ascontiguousarray(r, np.float32) for r in t["illum"]]
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))  # noqa: E731
+    s = T.fl_spectral_tables()
+    s.cie_lambda, s.cie_x, s.cie_y, s.cie_z = (fp(keep[k]) for k in ("cie_lambda", "cie_x", "cie_y", "cie_z"))
+    s.n_cie = keep["cie_lambda"].shape[0]
+    s.cie_y_integral = float(t["cie_y_integral"])
+    s.rgb2spec_lambda = fp(keep["rgb_lambda"])
+    s.n_rgb2spec = keep["rgb_lambda"].shape[0]
+    for b in range(7):
+        s.refl[b] = fp(refl[b])
+        s.illum[b] = fp(illum[b])
+    return s, (keep, refl, illum)
+
+
+def _ptr(x):
+    """device pointer of a torch tensor, or host pointer of a numpy array"""
+    if hasattr(x, "data_ptr"):
+        return C.c_void_p(x.data_ptr())
+    return C.c_void_p(x.ctypes.data)
+
+
+def _is_device(x):
+    return hasattr(x, "is_cuda") and x.is_cuda
+
+
+class Context:
+    def __init__(self, device: int = 0, tables: dict | None = None):
+        self.h = None
+        s, self._keep = _tables_struct(tables if tables is not None else reference_tables())
+        h = C.c_void_p()
+        check(lib().fl_context_create(device, C.byref(s), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().fl_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def binned_tables(self):
+        out = np.zeros(17 * 60, np.float32)
+        check(lib().fl_context_binned_tables(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size), self.h)
+        return out.reshape(17, 60)
+
+    def scene(self, scene_obj):
+        return SceneHandle(self, scene_obj)
+
+
+class SceneHandle:
+    def __init__(self, ctx: Context, sc):
+        self.ctx = ctx
+        self.h = None
+        self.src = sc
+        desc, keep = sc.desc()
+        h = C.c_void_p()
+        check(lib().fl_scene_create(ctx.h, C.byref(desc), C.byref(h)), ctx.h)
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().fl_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        i = T.fl_scene_info()
+        check(lib().fl_scene_get_info(self.h, C.byref(i)), self.ctx.h)
+        return {k: getattr(i, k) for k, _ in T.fl_scene_info._fields_}
+
+    # ------------------------------------------------------------------ queries
+    def trace_closest(self, org, dirs, out=None, stream=None):
+        """org, dirs: (n, 4) float32 numpy (host) or torch CUDA tensors (device).
+        Returns a structured numpy array (host) or fills/returns an (n, 4) int32 torch tensor."""
+        n = org.shape[0]
+        if _is_device(org):
+            import torch
+            if out is None:
+                out = torch.empty((n, 4), dtype=torch.int32, device=org.device)
+            check(lib().fl_trace_closest(self.h, _ptr(org), _ptr(dirs), n, _ptr(out), T.FL_MEM_DEVICE,
+                                         C.c_void_p(stream)), self.ctx.h)
+            return out
+        org = np.ascontiguousarray(org, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        hits = out if out is not None else np.zeros(n, dtype=T.HIT_DTYPE)
+        check(lib().fl_trace_closest(self.h, _ptr(org), _ptr(dirs), n, _ptr(hits), T.FL_MEM_HOST, None), self.ctx.h)
+        return hits
+
+    def trace_occluded(self, org, dirs):
+        n = org.shape[0]
+        if _is_device(org):
+            import torch
+            out = torch.empty(n, dtype=torch.uint8, device=org.device)
+            check(lib().fl_trace_occluded(self.h, _ptr(org), _ptr(dirs), n, _ptr(out), T.FL_MEM_DEVICE, None),
+                  self.ctx.h)
+            return out
+        org = np.ascontiguousarray(org, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        occ = np.zeros(n, np.uint8)
+        check(lib().fl_trace_occluded(self.h, _ptr(org), _ptr(dirs), n, _ptr(occ), T.FL_MEM_HOST, None), self.ctx.h)
+        return occ
+
+    def trace_count(self, org, dirs):
+        n = org.shape[0]
+        mem = T.FL_MEM_DEVICE if _is_device(org) else T.FL_MEM_HOST
+        if mem == T.FL_MEM_HOST:
+            org = np.ascontiguousarray(org, np.float32)
+            dirs = np.ascontiguousarray(dirs, np.float32)
+        nv, nt = C.c_uint64(0), C.c_uint64(0)
+        check(lib().fl_trace_count(self.h, _ptr(org), _ptr(dirs), n, mem, C.byref(nv), C.byref(nt)), self.ctx.h)
+        return nv.value, nt.value
+
+    def render(self, params, camera=None, film_rgb=None, film_xyz64=None, memory=None):
+        """Renders self.src's camera (or `camera`, an fl_camera). Host numpy films by default."""
+        cam = camera if camera is not None else self.src.camera_struct()
+        W, H = cam.width, cam.height
+        if film_rgb is None:
+            film_rgb = np.zeros((H, W, 3), np.float32)
+        mem = memory if memory is not None else (T.FL_MEM_DEVICE if _is_device(film_rgb) else T.FL_MEM_HOST)
+        stats = T.fl_render_stats()
+        xyz = _ptr(film_xyz64) if film_xyz64 is not None else None
+        check(lib().fl_render(self.h, C.byref(cam), C.byref(params), _ptr(film_rgb), xyz, mem, C.byref(stats)),
+              self.ctx.h)
+        return film_rgb, {k: getattr(stats, k) for k, _ in T.fl_render_stats._fields_ if k != "reserved"}

@@ -33,6 +33,12 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#define FL_API __attribute__((visibility("default")))
+#else
+#define FL_API
+#endif
+
 typedef int32_t fl_status;
 
 enum {
@@ -83,15 +89,15 @@ typedef struct {
 /* ------------------------------------------------------------------------- */
 /* Replaces the global InitializeSpectrals() call (spectruminits.cpp:6) plus embree's
  * rtcNewDevice (bvh.h:25-28): binds a CUDA device, uploads the spectral tables. */
-fl_status fl_context_create(int32_t device, const fl_spectral_tables *tables, fl_context **out);
-fl_status fl_context_destroy(fl_context *ctx);
-const char *fl_status_string(fl_status status);
+FL_API fl_status fl_context_create(int32_t device, const fl_spectral_tables *tables, fl_context **out);
+FL_API fl_status fl_context_destroy(fl_context *ctx);
+FL_API const char *fl_status_string(fl_status status);
 /* Copies the last error message of this context (or of the process when ctx is NULL). */
-fl_status fl_last_error(const fl_context *ctx, char *buf, size_t buf_len);
+FL_API fl_status fl_last_error(const fl_context *ctx, char *buf, size_t buf_len);
 
 /* The 60-bin tables the library derived from the caller's tables, for inspection:
  * out has room for 17*60 floats in the order X, Y, Z, refl[0..6], illum[0..6]. */
-fl_status fl_context_binned_tables(const fl_context *ctx, float *out, size_t n_floats);
+FL_API fl_status fl_context_binned_tables(const fl_context *ctx, float *out, size_t n_floats);
 
 /* ------------------------------------------------------------------------- */
 /* Scene                                                                     */
@@ -152,9 +158,9 @@ typedef struct {
 /* Replaces Scene::Scene + BVH::initialize_scene_geometry/finalise (core/scene.cpp:7-19,
  * bvh/bvh.cpp:7-47): uploads the soup (host pointers) and builds the 8-wide BVH on the
  * device. Triangle ids reported by traces are soup indices (= embree geomID order). */
-fl_status fl_scene_create(fl_context *ctx, const fl_scene_desc *desc, fl_scene **out);
-fl_status fl_scene_destroy(fl_scene *scene);
-fl_status fl_scene_get_info(const fl_scene *scene, fl_scene_info *info);
+FL_API fl_status fl_scene_create(fl_context *ctx, const fl_scene_desc *desc, fl_scene **out);
+FL_API fl_status fl_scene_destroy(fl_scene *scene);
+FL_API fl_status fl_scene_get_info(const fl_scene *scene, fl_scene_info *info);
 
 /* ------------------------------------------------------------------------- */
 /* Batch ray queries                                                         */
@@ -170,18 +176,18 @@ typedef struct {
 } fl_hit;
 
 /* Replaces BVH::intersect / rtcIntersect1 (bvh/bvh.cpp:49-84) for n rays. */
-fl_status fl_trace_closest(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
+FL_API fl_status fl_trace_closest(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
                            fl_hit *hits, int32_t memory, void *stream);
 
 /* Shadow query with the reference's visibility rule (illuminants/illuminant.cpp:40-50):
  * occluded[i] = 0 when the ray hits nothing in (tmin, tmax) or its closest hit is an
  * emissive triangle, else 1. */
-fl_status fl_trace_occluded(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
+FL_API fl_status fl_trace_occluded(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
                             uint8_t *occluded, int32_t memory, void *stream);
 
 /* Traversal statistics of the last trace on this scene (device counters, instrumented
  * launch): total wide nodes and triangles visited. */
-fl_status fl_trace_count(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
+FL_API fl_status fl_trace_count(fl_scene *scene, const float *org_tmin, const float *dir_tmax, uint32_t n,
                          int32_t memory, uint64_t *nodes_visited, uint64_t *tris_tested);
 
 /* ------------------------------------------------------------------------- */
@@ -228,7 +234,7 @@ typedef struct {
  * width*height*3 linear Rec.709 floats (the mean over samples of
  * xyz_to_rgb(to_xyz(Li)), color/spectrumoperations.cpp:58-66,193-212), row 0 at the top.
  * film_xyz64 (nullable) receives the FP64 XYZ sums (not divided by spp). */
-fl_status fl_render(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
+FL_API fl_status fl_render(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
                     float *film_rgb, double *film_xyz64, int32_t memory, fl_render_stats *stats);
 
 #ifdef __cplusplus

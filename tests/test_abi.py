@@ -1,0 +1,39 @@
+"""The C-ABI library loads and exports every symbol include/filianore_gpu.h declares
+(no compute calls: runs without a GPU)."""
+import ctypes
+import os
+import re
+
+import filianore_b200 as fb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", h)).read()
+            names |= set(re.findall(r"FL_API\s+[\w\s\*]+?\b(fl_\w+)\s*\(", text))
+    return names
+
+
+def test_header_declares_the_entry_points():
+    names = declared_symbols()
+    assert {"fl_context_create", "fl_scene_create", "fl_trace_closest", "fl_trace_occluded", "fl_render"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = fb.lib()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    assert set(fb.EXPORTED) >= declared_symbols() - set()
+
+
+def test_status_strings_and_no_device_error():
+    lib = fb.lib()
+    assert lib.fl_status_string(0) == b"FL_OK"
+    assert lib.fl_status_string(-5) == b"FL_ERR_TRAVERSAL"
+    # null tables are rejected before any device work
+    h = ctypes.c_void_p()
+    assert lib.fl_context_create(0, None, ctypes.byref(h)) == fb.FL_ERR_INVALID
