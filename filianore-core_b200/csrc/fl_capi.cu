@@ -47,6 +47,22 @@ fl_status ensure_scratch(Context *ctx, size_t bytes, void **out) {
     return FL_OK;
 }
 
+fl_status ensure_film_scratch(Context *ctx, size_t bytes, void **out) {
+    if (bytes > ctx->film_bytes) {
+        if (ctx->film_scratch) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ctx->film_scratch);
+            ctx->film_scratch = nullptr;
+            ctx->film_bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&ctx->film_scratch, bytes);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "film allocation");
+        ctx->film_bytes = bytes;
+    }
+    *out = ctx->film_scratch;
+    return FL_OK;
+}
+
 // average_spectrum_samples (src/filianore/color/spectrumoperations.cpp:28-56), with the
 // reference's float/double mixing, so the 60-bin tables equal InitializeSpectrals'.
 static float lerp_ref(float t, float v1, float v2) { return (1.f - t) * v1 + t * v2; }
@@ -211,6 +227,7 @@ fl_status fl_context_destroy(fl_context *ctx_h) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->scratch);
+    cudaFree(ctx->film_scratch);
     cudaFree(ctx->d_error);
     cudaFree(ctx->d_counters);
     cudaFree(ctx->tables.cie_xyz);
@@ -322,6 +339,21 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
     SC_TRY(cudaMalloc(&s->tri_light, sizeof(int32_t) * nt));
     SC_TRY(cudaMalloc(&s->materials, sizeof(MaterialDev) * d->n_materials));
     SC_TRY(cudaMalloc(&s->lights, sizeof(LightDev) * (d->n_lights ? d->n_lights : 1)));
+    SC_TRY(cudaMalloc(&s->mat_refl60, sizeof(float) * 60 * d->n_materials));
+    {
+        // from_reflectance_rgb (color/spectrumoperations.cpp:113-147) over the 60 bins
+        std::vector<float> refl((size_t)60 * d->n_materials);
+        for (uint32_t m = 0; m < d->n_materials; ++m) {
+            const MaterialDev &md = s->materials_host[m];
+            for (int i = 0; i < 60; ++i) {
+                float r = 0.f;
+                for (int k = 0; k < 3; ++k) r += ctx->binned_host[180 + 60 * md.basis[k] + i] * md.w[k];
+                r *= 0.94f;
+                refl[(size_t)m * 60 + i] = r < 0.f ? 0.f : r;
+            }
+        }
+        SC_TRY(cudaMemcpy(s->mat_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
+    }
     if (d->n_tri) {
         SC_TRY(cudaMemcpyAsync(s->soup, d->verts, sizeof(float) * 9 * d->n_tri, cudaMemcpyHostToDevice, ctx->stream));
         if (d->tri_material)
@@ -356,6 +388,7 @@ fl_status fl_scene_destroy(fl_scene *scene) {
     cudaFree(s->tri_light);
     cudaFree(s->materials);
     cudaFree(s->lights);
+    cudaFree(s->mat_refl60);
     delete s;
     return FL_OK;
 }

@@ -37,6 +37,8 @@ struct Context {
     // grow-only scratch owned by the context (render wavefront state, trace staging)
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
+    void *film_scratch = nullptr;       // render films (separate from the wave scratch)
+    size_t film_bytes = 0;
     int *d_error = nullptr;             // traversal error counter
     unsigned long long *d_counters = nullptr;  // 8 x u64 statistics
 };
@@ -73,6 +75,7 @@ struct Scene {
     uint32_t *tri_material = nullptr; // soup order
     int32_t *tri_light = nullptr;     // soup order, -1 = not emissive
     MaterialDev *materials = nullptr;
+    float *mat_refl60 = nullptr;      // n_materials x 60: from_reflectance_rgb in the 60 bins
     uint32_t n_materials = 0;
     LightDev *lights = nullptr;
     uint32_t n_lights = 0;
@@ -103,5 +106,9 @@ fl_status launch_trace(Scene *s, const float4 *org_tmin, const float4 *dir_tmax,
 
 // context scratch: returns a device buffer of at least `bytes` (grow-only)
 fl_status ensure_scratch(Context *ctx, size_t bytes, void **out);
+fl_status ensure_film_scratch(Context *ctx, size_t bytes, void **out);
+
+// Smits terms of from_reflectance_rgb (basis ids and weights, in the reference's order)
+void smits_terms(const float rgb[3], int basis[3], float w[3]);
 
 }  // namespace fl

@@ -1,3 +1,691 @@
-// Wavefront path tracer (declarations shared by the render translation units).
+// Wavefront path tracer: the GPU replacement of the absent application's loop over
+// pixels and samples that calls PathIntegrator::Li
+// (src/filianore/integrators/pathintegrator.cpp:12-87) with estimate_direct
+// (src/filianore/integrators/integrator.cpp:25-110) for every light.
+//
+// A wave holds up to `cap` camera samples. Per bounce, four kernels run over SoA queues:
+//   k_trace_paths  closest hit of every live path ray (8-wide BVH + analytic sphere lights)
+//   k_shade        emission, miss handling, and for every light the two NEE candidates
+//                  of estimate_direct (light sample -> shadow ray; BSDF sample -> MIS ray),
+//                  fully weighted; live paths are compacted into the continuation queue
+//   k_trace_rays2  shadow rays (reference visibility rule) and MIS rays (did the BSDF
+//                  sample reach this light?), one launch for both kinds
+//   k_continue     adds the visible NEE terms in the reference's order, samples the
+//                  continuation, applies depth cut-offs and Russian roulette, and
+//                  compacts surviving paths into the next queue
+// Random numbers are drawn in the reference's order (per light: uLight, uScatter; then
+// the BSDF sample; then RR), so a path consumes its PCG32 stream exactly as
+// PathIntegrator::Li does. Queues are compacted with warp ballots and one atomic per warp.
+// Kernels read their item counts from device memory, so a whole wave is enqueued without
+// host synchronisation. Finished paths add to_xyz(L) to an FP64 film with atomics.
 #pragma once
+
 #include "fl_internal.h"
+#include "fl_shading.cuh"
+#include "fl_traverse.cuh"
+
+namespace fl {
+
+struct WaveCounters {
+    uint32_t n_trace, n_cont, n_next, n_shadow;
+    unsigned long long rays, shadow_rays, bounces, paths;
+    int err;
+    int pad[3];
+};
+
+struct CamDev {
+    v3 origin, lower_left, horizontal, vertical, u, v;
+    int W, H;
+};
+
+struct RenderArgs {
+    // scene
+    const WideNode *nodes;
+    uint32_t n_nodes;
+    const float4 *tris;
+    uint32_t n_tri;
+    const float *soup;
+    const uint32_t *tri_material;
+    const int32_t *tri_light;
+    const MaterialDev *materials;
+    const float *mat_refl60;
+    const LightDev *lights;
+    int n_lights;
+    int any_hit_ok;
+    int has_env;
+    float env_radiance;
+    int has_spheres;
+    TablesArg tab;
+    CamDev cam;
+    // parameters
+    int spp, max_depth;
+    float rr_threshold;
+    uint32_t sample_offset;
+    unsigned long long wave_base, total;
+    uint32_t n_pix, cap;
+    // path state (slot-indexed, component-major for spectra: x[k * cap + slot])
+    uint32_t *pixel;
+    unsigned long long *rng;
+    float *beta, *L, *lambda0, *eta_scale;
+    uint32_t *flags;  // bits 0..7 bounce, bit 8 specular
+    float4 *ray_o, *ray_d;
+    int4 *hit;
+    // pending NEE terms: C*[(li * NL + k) * cap + slot], pflags[li * cap + slot]
+    float *CL, *CS;
+    uint32_t *pflags;
+    // shadow / MIS rays
+    float4 *sray_o, *sray_d;
+    uint32_t *stag;
+    uint32_t scap;
+    // queues
+    uint32_t *q_trace, *q_cont, *q_next;
+    WaveCounters *cnt;
+    double *film;
+};
+
+enum : uint32_t { kHasCL = 1u, kHasCS = 2u, kVisOK = 4u, kMisOK = 8u };
+
+// warp-aggregated queue append: returns this lane's position (valid when pred)
+__device__ inline uint32_t warp_append(uint32_t *counter, bool pred) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask) return 0;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ inline void warp_count(unsigned long long *dst, uint32_t v) {
+    unsigned long long x = v;
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
+}
+
+__device__ inline uint32_t load_count(const uint32_t *p) { return *(volatile const uint32_t *)p; }
+
+// grid-stride loop whose trip count is uniform within a warp (for the warp collectives)
+#define FL_WARP_UNIFORM_LOOP(i, n)                                                              \
+    for (uint32_t _base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u,                       \
+                  _stride = gridDim.x * blockDim.x, i = _base + (threadIdx.x & 31);             \
+         _base < (n); _base += _stride, i = _base + (threadIdx.x & 31))
+
+template <int NL>
+__device__ inline void load_spec(const float *a, uint32_t cap, uint32_t slot, Spec<NL> &s) {
+#pragma unroll
+    for (int k = 0; k < NL; ++k) s.c[k] = a[(size_t)k * cap + slot];
+}
+template <int NL>
+__device__ inline void store_spec(float *a, uint32_t cap, uint32_t slot, const Spec<NL> &s) {
+#pragma unroll
+    for (int k = 0; k < NL; ++k) a[(size_t)k * cap + slot] = s.c[k];
+}
+
+template <int NL>
+__device__ inline void finish_path(const RenderArgs &A, const SmemTables &sm, uint32_t slot, const Spec<NL> &L) {
+    double xyz[3];
+    spectrum_xyz<NL>(sm, A.tab, A.lambda0[slot], L, xyz);
+    const uint32_t pix = A.pixel[slot];
+    atomicAdd(&A.film[3 * (size_t)pix + 0], xyz[0]);
+    atomicAdd(&A.film[3 * (size_t)pix + 1], xyz[1]);
+    atomicAdd(&A.film[3 * (size_t)pix + 2], xyz[2]);
+}
+
+// the hit record of BVH::intersect (bvh.cpp:49-84): p = o + d t, n = normalize(Ng), wo = normalize(-d)
+__device__ inline Hit make_hit(const RenderArgs &A, float4 o4, float4 d4, int4 h) {
+    Hit r;
+    const v3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
+    const float t = __int_as_float(h.y);
+    r.p = add(o, mul(d, t));
+    r.wo = normalize(neg(d));
+    r.prim = h.x;
+    if (h.x >= 0) {
+        const v3 v0 = tri_v(A.soup, (uint32_t)h.x, 0), v1 = tri_v(A.soup, (uint32_t)h.x, 1),
+                 v2 = tri_v(A.soup, (uint32_t)h.x, 2);
+        r.n = normalize(cross(sub(v1, v0), sub(v2, v0)));
+    } else {
+        const LightDev &L = A.lights[-2 - h.x];
+        r.n = normalize(sub(r.p, mk(L.cx, L.cy, L.cz)));
+    }
+    return r;
+}
+
+__device__ inline int prim_light(const RenderArgs &A, int prim) {
+    if (prim >= 0) return A.tri_light[prim];
+    if (prim <= -2) return -2 - prim;
+    return -1;
+}
+
+template <int NL>
+__device__ inline void make_bsdf(const RenderArgs &A, const SmemTables &sm, const Hit &h, float lambda0, Bsdf<NL> &b) {
+    b.ng = h.n;
+    b.ns = h.n;
+    coordinate_system(b.ns, &b.s, &b.t);
+    b.s = normalize(b.s);
+    const uint32_t mi = h.prim >= 0 ? A.tri_material[h.prim] : 0u;
+    const MaterialDev m = A.materials[mi];
+    b.type = m.type;
+    b.mat_eta = m.eta;
+    b.mat_k = m.k;
+    b.ax = m.ax;
+    b.ay = m.ay;
+    b.eta = (m.type == FL_MAT_ROUGH_DIELECTRIC || m.type == FL_MAT_SMOOTH_DIELECTRIC) ? m.eta : 1.f;
+    if (m.type == FL_MAT_LAMBERT) reflectance<NL>(sm, A.tab, m, A.mat_refl60 + 60 * (size_t)mi, lambda0, b.R);
+    else b.R.set(1.f);
+}
+
+// closest hit over triangles and analytic sphere lights
+__device__ inline TraceResult closest_with_spheres(const RenderArgs &A, const RayPre &r, bool &err) {
+    TraceStats st;
+    TraceResult res;
+    if (A.n_nodes) res = traverse<false, false>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
+    else { res.id = -1; res.t = r.tmax; res.u = res.v = 0.f; }
+    if (A.has_spheres) {
+        const v3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
+        float best = res.id >= 0 ? res.t : r.tmax;
+        for (int l = 0; l < A.n_lights; ++l) {
+            const LightDev L = A.lights[l];
+            if (L.type != FL_LIGHT_SPHERE) continue;
+            const float ts = sphere_hit(L, o, d, r.tmin, best);
+            if (ts > 0.f && ts < best) {
+                best = ts;
+                res.id = -2 - l;
+                res.t = ts;
+                res.u = res.v = 0.f;
+            }
+        }
+    }
+    return res;
+}
+
+// ------------------------------------------------------------------------------ kernels
+
+template <int NL>
+__global__ void __launch_bounds__(128) k_raygen(RenderArgs A, uint32_t n_wave) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        A.cnt->n_trace = n_wave;
+        A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = 0;
+    }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_wave; k += gridDim.x * blockDim.x) {
+        const unsigned long long g = A.wave_base + k;
+        const uint32_t pix = (uint32_t)(g % A.n_pix);
+        const unsigned long long s = g / A.n_pix;
+        Pcg32 rng;
+        rng.seed(pix, 1u);
+        const unsigned long long sidx = (unsigned long long)A.sample_offset + s;
+        if (sidx) rng.advance(sidx << 16);
+        const float ux = rng.nextf(), uy = rng.nextf(), ul = rng.nextf();
+        const uint32_t px = pix % (uint32_t)A.cam.W, py = pix / (uint32_t)A.cam.W;
+        const float sx = __fdiv_rn(__fadd_rn((float)px, ux), (float)A.cam.W);
+        const float sy = __fdiv_rn(__fadd_rn((float)((uint32_t)A.cam.H - 1u - py), uy), (float)A.cam.H);
+        // PhysicalCamera::awaken_ray with lens sample (0.5, 0.5) and lensRadius 0
+        const v3 lp = sub(mul(mk(0.5f, 0.5f, 0.f), 2.f), mk(1.f, 1.f, 0.f));
+        const v3 rd = mul(lp, 0.f);
+        const v3 offset = add(mul(A.cam.u, rd.x), mul(A.cam.v, rd.y));
+        const v3 o = add(A.cam.origin, offset);
+        const v3 dir = sub(sub(add(add(A.cam.lower_left, mul(A.cam.horizontal, sx)), mul(A.cam.vertical, sy)),
+                               A.cam.origin),
+                           offset);
+        const v3 d = normalize(dir);
+        A.pixel[k] = pix;
+        A.rng[k] = rng.state;
+        A.lambda0[k] = 380.f + ul * 340.f;
+        A.eta_scale[k] = 1.f;
+        A.flags[k] = 0u;
+#pragma unroll
+        for (int c = 0; c < NL; ++c) {
+            A.beta[(size_t)c * A.cap + k] = 1.f;
+            A.L[(size_t)c * A.cap + k] = 0.f;
+        }
+        A.ray_o[k] = make_float4(o.x, o.y, o.z, 0.f);
+        A.ray_d[k] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
+        A.q_trace[k] = k;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->paths, (unsigned long long)n_wave);
+}
+
+static __global__ void __launch_bounds__(128) k_advance(WaveCounters *cnt) {
+    cnt->n_trace = cnt->n_next;
+    cnt->n_next = 0;
+    cnt->n_cont = 0;
+    cnt->n_shadow = 0;
+}
+
+static __global__ void __launch_bounds__(128) k_trace_paths(RenderArgs A) {
+    const uint32_t n = load_count(&A.cnt->n_trace);
+    uint32_t local = 0;
+    bool err = false;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t slot = A.q_trace[q];
+        const RayPre r = ray_precompute(A.ray_o[slot], A.ray_d[slot]);
+        const TraceResult res = closest_with_spheres(A, r, err);
+        A.hit[slot] = make_int4(res.id, __float_as_int(res.t), __float_as_int(res.u), __float_as_int(res.v));
+        ++local;
+    }
+    warp_count(&A.cnt->rays, local);
+    if (err) atomicAdd(&A.cnt->err, 1);
+}
+
+template <int NL>
+__global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
+    __shared__ SmemTables sm;
+    stage_tables(sm, A.tab, NL != 60);
+    const uint32_t n = load_count(&A.cnt->n_trace);
+    uint32_t shaded = 0;
+    FL_WARP_UNIFORM_LOOP(q, n) {
+        const bool active = q < n;
+        bool alive = false;
+        uint32_t slot = 0;
+        // NEE rays of this thread, emitted after the shading work (up to 2 per light)
+        if (active) {
+            slot = A.q_trace[q];
+            const int4 h = A.hit[slot];
+            const uint32_t fl = A.flags[slot];
+            const uint32_t bounce = fl & 0xffu;
+            const bool specular = (fl >> 8) & 1u;
+            const float4 o4 = A.ray_o[slot], d4 = A.ray_d[slot];
+            Spec<NL> beta, L;
+            load_spec<NL>(A.beta, A.cap, slot, beta);
+            load_spec<NL>(A.L, A.cap, slot, L);
+            const bool hit = h.x != -1;
+            Hit hr;
+            if (hit) hr = make_hit(A, o4, d4, h);
+            if (bounce == 0 || specular) {
+                if (hit) {
+                    const int li = prim_light(A, h.x);
+                    if (li >= 0) {
+                        const LightDev Ll = A.lights[li];
+                        const float le = dot(hr.n, mk(-d4.x, -d4.y, -d4.z)) > 0.f ? Ll.radiance : 0.f;
+#pragma unroll
+                        for (int c = 0; c < NL; ++c) L.c[c] += beta.c[c] * le;
+                    }
+                } else if (A.has_env) {
+#pragma unroll
+                    for (int c = 0; c < NL; ++c) L.c[c] += beta.c[c] * A.env_radiance;
+                }
+            }
+            if (!hit) {
+                finish_path<NL>(A, sm, slot, L);
+            } else {
+                ++shaded;
+                alive = true;
+                store_spec<NL>(A.L, A.cap, slot, L);
+                const float lambda0 = A.lambda0[slot];
+                Bsdf<NL> b;
+                make_bsdf<NL>(A, sm, hr, lambda0, b);
+                if (bsdf_num_components(b, kBsdfAll & ~kBsdfSpecular) > 0) {
+                    Pcg32 rng;
+                    rng.state = A.rng[slot];
+                    rng.inc = 3u;
+                    const int bsdfFlags = kBsdfAll & ~kBsdfSpecular;
+                    for (int li = 0; li < A.n_lights; ++li) {
+                        const float ulx = rng.nextf(), uly = rng.nextf();
+                        const float usx = rng.nextf(), usy = rng.nextf();
+                        const LightDev Ll = A.lights[li];
+                        uint32_t pf = 0;
+                        Spec<NL> CL, CS;
+                        CL.set(0.f);
+                        CS.set(0.f);
+                        // light sampling term
+                        float scatteringPdf = 0.f;
+                        v3 wi = mk(0.f, 0.f, 0.f);
+                        const LightSample ls = light_sample_li(Ll, A.soup, hr, ulx, uly);
+                        float illumPdf = ls.pdf;
+                        if (ls.vis_kind) wi = ls.wi;
+                        if (ls.pdf > 0 && ls.radiance != 0.f) {
+                            Spec<NL> f;
+                            bsdf_eval<NL>(b, hr.wo, wi, bsdfFlags, f);
+                            const float ad = absdot(wi, b.ns);
+#pragma unroll
+                            for (int c = 0; c < NL; ++c) f.c[c] *= ad;
+                            scatteringPdf = bsdf_pdf<NL>(b, hr.wo, wi, bsdfFlags);
+                            if (!f.black()) {
+                                const float weight = power_heuristic(illumPdf, scatteringPdf);
+#pragma unroll
+                                for (int c = 0; c < NL; ++c) CL.c[c] = f.c[c] * ls.radiance * weight / illumPdf;
+                                pf |= kHasCL;
+                                // shadow ray (VisibilityEvaluator::unoccluded)
+                                float4 so, sd;
+                                if (ls.vis_kind == 1) {
+                                    const v3 dd = sub(ls.target, hr.p);
+                                    const v3 oo = spawn_origin(hr.p, hr.n, dd);
+                                    so = make_float4(oo.x, oo.y, oo.z, kShadowEpsilon);
+                                    sd = make_float4(dd.x, dd.y, dd.z, 1.f - kShadowEpsilon);
+                                } else {
+                                    const v3 oo = spawn_origin(hr.p, hr.n, wi);
+                                    so = make_float4(oo.x, oo.y, oo.z, kShadowEpsilon);
+                                    sd = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
+                                }
+                                const uint32_t pos = atomicAdd(&A.cnt->n_shadow, 1u);
+                                if (pos < A.scap) {
+                                    A.sray_o[pos] = so;
+                                    A.sray_d[pos] = sd;
+                                    A.stag[pos] = (((uint32_t)li * A.cap + slot) << 1) | 0u;
+                                } else {
+                                    atomicAdd(&A.cnt->err, 1);
+                                }
+                            }
+                        }
+                        // BSDF sampling term
+                        {
+                            Spec<NL> f;
+                            int sampledType = 0;
+                            bsdf_sample<NL>(b, hr.wo, wi, usx, usy, scatteringPdf, bsdfFlags, sampledType, f);
+                            const float ad = absdot(wi, b.ns);
+#pragma unroll
+                            for (int c = 0; c < NL; ++c) f.c[c] *= ad;
+                            const bool sampledSpecular = (sampledType & kBsdfSpecular) != 0;
+                            if (!f.black() && scatteringPdf > 0) {
+                                float weight = 1.f;
+                                bool ok = true;
+                                if (!sampledSpecular) {
+                                    illumPdf = light_pdf_li(Ll, A.soup, hr, wi);
+                                    if (illumPdf == 0) ok = false;
+                                    else weight = power_heuristic(scatteringPdf, illumPdf);
+                                }
+                                const float Lrad = Ll.radiance;  // le() of the hit light, or of the environment on a miss
+                                if (ok && Lrad != 0.f) {
+#pragma unroll
+                                    for (int c = 0; c < NL; ++c)
+                                        CS.c[c] = f.c[c] * Lrad * 1.f * weight / scatteringPdf;
+                                    pf |= kHasCS;
+                                    const v3 oo = spawn_origin(hr.p, hr.n, wi);
+                                    const uint32_t pos = atomicAdd(&A.cnt->n_shadow, 1u);
+                                    if (pos < A.scap) {
+                                        A.sray_o[pos] = make_float4(oo.x, oo.y, oo.z, kShadowEpsilon);
+                                        A.sray_d[pos] = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
+                                        A.stag[pos] = (((uint32_t)li * A.cap + slot) << 1) | 1u;
+                                    } else {
+                                        atomicAdd(&A.cnt->err, 1);
+                                    }
+                                }
+                            }
+                        }
+                        A.pflags[(size_t)li * A.cap + slot] = pf;
+                        if (pf & kHasCL) store_spec<NL>(A.CL + (size_t)li * NL * A.cap, A.cap, slot, CL);
+                        if (pf & kHasCS) store_spec<NL>(A.CS + (size_t)li * NL * A.cap, A.cap, slot, CS);
+                    }
+                    A.rng[slot] = rng.state;
+                }
+            }
+        }
+        const uint32_t pos = warp_append(&A.cnt->n_cont, alive);
+        if (alive) A.q_cont[pos] = slot;
+    }
+    warp_count(&A.cnt->bounces, shaded);
+}
+
+// shadow rays (kind 0) and MIS rays (kind 1)
+static __global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
+    const uint32_t n = min(load_count(&A.cnt->n_shadow), A.scap);
+    uint32_t local = 0;
+    bool err = false;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t tag = A.stag[q];
+        const uint32_t kind = tag & 1u;
+        const uint32_t sl = tag >> 1;  // li * cap + slot
+        const uint32_t li = sl / A.cap;
+        const RayPre r = ray_precompute(A.sray_o[q], A.sray_d[q]);
+        uint32_t bit = 0;
+        if (kind == 0) {
+            TraceStats st;
+            TraceResult res;
+            if (A.n_nodes == 0) res.id = -1;
+            else if (A.any_hit_ok) res = traverse<true, false>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
+            else res = traverse<false, false>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
+            const bool unocc = res.id < 0 || A.tri_light[res.id] >= 0;
+            bit = unocc ? kVisOK : 0u;
+        } else {
+            const TraceResult res = closest_with_spheres(A, r, err);
+            const LightDev Ll = A.lights[li];
+            bool ok = false;
+            if (res.id == -1) ok = Ll.type == FL_LIGHT_ENV;
+            else if (prim_light(A, res.id) == (int)li) {
+                const int4 h = make_int4(res.id, __float_as_int(res.t), 0, 0);
+                const Hit hr = make_hit(A, A.sray_o[q], A.sray_d[q], h);
+                ok = dot(hr.n, mk(-r.dx, -r.dy, -r.dz)) > 0.f;
+            }
+            bit = ok ? kMisOK : 0u;
+        }
+        if (bit) atomicOr(&A.pflags[sl], bit);
+        ++local;
+    }
+    warp_count(&A.cnt->shadow_rays, local);
+    warp_count(&A.cnt->rays, local);
+    if (err) atomicAdd(&A.cnt->err, 1);
+}
+
+template <int NL>
+__global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
+    __shared__ SmemTables sm;
+    stage_tables(sm, A.tab, NL != 60);
+    const uint32_t n = load_count(&A.cnt->n_cont);
+    FL_WARP_UNIFORM_LOOP(q, n) {
+        const bool active = q < n;
+        bool alive = false;
+        uint32_t slot = 0;
+        if (active) {
+            slot = A.q_cont[q];
+            const int4 h = A.hit[slot];
+            const uint32_t fl = A.flags[slot];
+            const uint32_t bounce = fl & 0xffu;
+            const float4 o4 = A.ray_o[slot], d4 = A.ray_d[slot];
+            const Hit hr = make_hit(A, o4, d4, h);
+            const float lambda0 = A.lambda0[slot];
+            Bsdf<NL> b;
+            make_bsdf<NL>(A, sm, hr, lambda0, b);
+            Spec<NL> beta, L;
+            load_spec<NL>(A.beta, A.cap, slot, beta);
+            load_spec<NL>(A.L, A.cap, slot, L);
+            if (bsdf_num_components(b, kBsdfAll & ~kBsdfSpecular) > 0) {
+                // uniform_sample_all_lights: sum of the per-light estimate_direct results
+                Spec<NL> Ls;
+                Ls.set(0.f);
+                for (int li = 0; li < A.n_lights; ++li) {
+                    const uint32_t pf = A.pflags[(size_t)li * A.cap + slot];
+                    Spec<NL> Ld;
+                    Ld.set(0.f);
+                    if ((pf & kHasCL) && (pf & kVisOK)) {
+                        Spec<NL> c;
+                        load_spec<NL>(A.CL + (size_t)li * NL * A.cap, A.cap, slot, c);
+#pragma unroll
+                        for (int k = 0; k < NL; ++k) Ld.c[k] += c.c[k];
+                    }
+                    if ((pf & kHasCS) && (pf & kMisOK)) {
+                        Spec<NL> c;
+                        load_spec<NL>(A.CS + (size_t)li * NL * A.cap, A.cap, slot, c);
+#pragma unroll
+                        for (int k = 0; k < NL; ++k) Ld.c[k] += c.c[k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < NL; ++k) Ls.c[k] += Ld.c[k];
+                }
+#pragma unroll
+                for (int k = 0; k < NL; ++k) L.c[k] += beta.c[k] * Ls.c[k];
+            }
+            // continuation (pathintegrator.cpp:46-84)
+            Pcg32 rng;
+            rng.state = A.rng[slot];
+            rng.inc = 3u;
+            const v3 wo = mk(-d4.x, -d4.y, -d4.z);
+            v3 wi = mk(0.f, 0.f, 0.f);
+            float pdf = 0.f;
+            int sflags = 0;
+            Spec<NL> f;
+            const float ux = rng.nextf(), uy = rng.nextf();
+            bsdf_sample<NL>(b, wo, wi, ux, uy, pdf, kBsdfAll, sflags, f);
+            bool stop = f.black() || pdf == 0;
+            const int depth = A.max_depth;
+            const int bi = (int)bounce;
+            if (!stop && depth == bi && (sflags & kBsdfDiffuse)) stop = true;
+            if (!stop && ((depth == bi && (sflags & kBsdfSpecular)) || (depth == bi && (sflags & kBsdfGlossy)))) stop = true;
+            if (!stop && depth == bi && (sflags & kBsdfTransmission)) stop = true;
+            if (!stop) {
+                const float ad = absdot(wi, b.ns);
+#pragma unroll
+                for (int k = 0; k < NL; ++k) beta.c[k] *= f.c[k] * ad / pdf;
+                const bool spec_b = (sflags & kBsdfSpecular) != 0;
+                float etaScale = A.eta_scale[slot];
+                if ((sflags & kBsdfSpecular) && (sflags & kBsdfTransmission)) {
+                    const float eta = b.eta;
+                    etaScale *= (dot(wo, hr.n) > 0) ? (eta * eta) : 1.f / (eta * eta);
+                }
+                const v3 no = spawn_origin(hr.p, hr.n, wi);
+                float mx = beta.c[0] * etaScale;
+#pragma unroll
+                for (int k = 1; k < NL; ++k) mx = fmaxf(mx, beta.c[k] * etaScale);
+                if (mx < A.rr_threshold && bi > 3) {
+                    float qq = 1.f - mx;
+                    if (qq < 0.05f) qq = 0.05f;
+                    if (rng.nextf() < qq) stop = true;
+                    else {
+#pragma unroll
+                        for (int k = 0; k < NL; ++k) beta.c[k] /= 1.f - qq;
+                    }
+                }
+                if (!stop) {
+                    alive = true;
+                    store_spec<NL>(A.beta, A.cap, slot, beta);
+                    A.eta_scale[slot] = etaScale;
+                    A.flags[slot] = (bounce + 1u) | (spec_b ? 0x100u : 0u);
+                    A.ray_o[slot] = make_float4(no.x, no.y, no.z, kShadowEpsilon);
+                    A.ray_d[slot] = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
+                }
+            }
+            A.rng[slot] = rng.state;
+            if (alive) store_spec<NL>(A.L, A.cap, slot, L);
+            else finish_path<NL>(A, sm, slot, L);
+        }
+        const uint32_t pos = warp_append(&A.cnt->n_next, alive);
+        if (alive) A.q_next[pos] = slot;
+    }
+}
+
+static __global__ void k_resolve(const double *__restrict__ film, uint32_t n_pix, double inv_spp, float *__restrict__ rgb) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_pix; p += gridDim.x * blockDim.x) {
+        const float x = (float)(film[3 * (size_t)p] * inv_spp);
+        const float y = (float)(film[3 * (size_t)p + 1] * inv_spp);
+        const float z = (float)(film[3 * (size_t)p + 2] * inv_spp);
+        // xyz_to_rgb, color/spectrumoperations.cpp:58-66
+        rgb[3 * (size_t)p + 0] = 3.240479f * x - 1.537150f * y - 0.498535f * z;
+        rgb[3 * (size_t)p + 1] = -0.969256f * x + 1.875991f * y + 0.041556f * z;
+        rgb[3 * (size_t)p + 2] = 0.055648f * x - 0.204043f * y + 1.057311f * z;
+    }
+}
+
+// ------------------------------------------------------------------------------ host driver
+
+inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Renders all samples of the image into d_film (FP64 XYZ sums) wave by wave. Instantiated
+// per spectral mode in its own translation unit (the 60-bin one without FMA contraction).
+template <int NL>
+fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film,
+                       WaveCounters *h_cnt, cudaStream_t st) {
+    Context *ctx = s->ctx;
+    const int nl = (int)s->n_lights;
+    const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
+    const unsigned long long total = n_pix * (unsigned long long)p.spp;
+    const size_t per_slot = 92 + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
+    const size_t budget = (size_t)3 << 30;
+    size_t cap = p.wave_paths > 0 ? (size_t)p.wave_paths : (NL == 60 ? (size_t)1 << 19 : (size_t)1 << 21);
+    cap = std::min(cap, budget / per_slot);
+    cap = std::min<size_t>(cap, (size_t)total);
+    cap = std::max<size_t>(128, (cap + 127) & ~(size_t)127);
+    if (cap * (size_t)std::max(nl, 1) >= ((size_t)1 << 31)) {
+        set_error(ctx, "wave too large for the shadow-ray tags");
+        return FL_ERR_INVALID;
+    }
+    const size_t scap = cap * 2 * (size_t)nl;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes ? bytes : 1); return o; };
+    const size_t o_cnt = take(sizeof(WaveCounters));
+    const size_t o_pixel = take(4 * cap), o_rng = take(8 * cap), o_beta = take(4 * NL * cap), o_L = take(4 * NL * cap);
+    const size_t o_lam = take(4 * cap), o_eta = take(4 * cap), o_flags = take(4 * cap);
+    const size_t o_ro = take(16 * cap), o_rd = take(16 * cap), o_hit = take(16 * cap);
+    const size_t o_CL = take(4 * (size_t)NL * nl * cap), o_CS = take(4 * (size_t)NL * nl * cap);
+    const size_t o_pf = take(4 * (size_t)nl * cap);
+    const size_t o_so = take(16 * scap), o_sd = take(16 * scap), o_st = take(4 * scap);
+    const size_t o_qa = take(4 * cap), o_qb = take(4 * cap), o_qc = take(4 * cap);
+    void *base = nullptr;
+    fl_status rc = ensure_scratch(ctx, off, &base);
+    if (rc) return rc;
+    char *B = static_cast<char *>(base);
+
+    RenderArgs A{};
+    A.nodes = s->nodes;
+    A.n_nodes = s->n_nodes;
+    A.tris = s->tris;
+    A.n_tri = s->n_tri;
+    A.soup = s->soup;
+    A.tri_material = s->tri_material;
+    A.tri_light = s->tri_light;
+    A.materials = s->materials;
+    A.mat_refl60 = s->mat_refl60;
+    A.lights = s->lights;
+    A.n_lights = nl;
+    A.any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
+    A.has_env = s->has_env;
+    A.env_radiance = s->env_radiance;
+    A.has_spheres = 0;
+    for (const auto &l : s->lights_host) A.has_spheres |= (l.type == FL_LIGHT_SPHERE) ? 1 : 0;
+    const SpectralTablesDev &T = ctx->tables;
+    A.tab = TablesArg{T.cie_lambda0, T.n_cie, T.cie_y_integral, T.rgb_lambda0, T.rgb_lambda1, T.n_rgb,
+                      T.cie_xyz, T.rgb_bases, T.binned};
+    A.cam = cam;
+    A.spp = p.spp;
+    A.max_depth = p.max_depth;
+    A.rr_threshold = p.rr_threshold;
+    A.sample_offset = p.sample_offset;
+    A.total = total;
+    A.n_pix = (uint32_t)n_pix;
+    A.cap = (uint32_t)cap;
+    A.cnt = reinterpret_cast<WaveCounters *>(B + o_cnt);
+    A.pixel = reinterpret_cast<uint32_t *>(B + o_pixel);
+    A.rng = reinterpret_cast<unsigned long long *>(B + o_rng);
+    A.beta = reinterpret_cast<float *>(B + o_beta);
+    A.L = reinterpret_cast<float *>(B + o_L);
+    A.lambda0 = reinterpret_cast<float *>(B + o_lam);
+    A.eta_scale = reinterpret_cast<float *>(B + o_eta);
+    A.flags = reinterpret_cast<uint32_t *>(B + o_flags);
+    A.ray_o = reinterpret_cast<float4 *>(B + o_ro);
+    A.ray_d = reinterpret_cast<float4 *>(B + o_rd);
+    A.hit = reinterpret_cast<int4 *>(B + o_hit);
+    A.CL = reinterpret_cast<float *>(B + o_CL);
+    A.CS = reinterpret_cast<float *>(B + o_CS);
+    A.pflags = reinterpret_cast<uint32_t *>(B + o_pf);
+    A.sray_o = reinterpret_cast<float4 *>(B + o_so);
+    A.sray_d = reinterpret_cast<float4 *>(B + o_sd);
+    A.stag = reinterpret_cast<uint32_t *>(B + o_st);
+    A.scap = (uint32_t)scap;
+    A.film = d_film;
+    uint32_t *qa = reinterpret_cast<uint32_t *>(B + o_qa), *qb = reinterpret_cast<uint32_t *>(B + o_qb);
+    A.q_cont = reinterpret_cast<uint32_t *>(B + o_qc);
+    FL_CUDA_TRY(ctx, cudaMemsetAsync(A.cnt, 0, sizeof(WaveCounters), st));
+
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    const int g_trace = sms * 16, g_shade = sms * 8;
+    for (unsigned long long wb = 0; wb < total; wb += cap) {
+        const uint32_t n_wave = (uint32_t)std::min<unsigned long long>(cap, total - wb);
+        A.wave_base = wb;
+        A.q_trace = qa;
+        A.q_next = qb;
+        k_raygen<NL><<<std::min<uint32_t>((n_wave + 127) / 128, (uint32_t)sms * 32), 128, 0, st>>>(A, n_wave);
+        for (int b = 0; b <= p.max_depth; ++b) {
+            if (b > 0) {
+                k_advance<<<1, 1, 0, st>>>(A.cnt);
+                std::swap(A.q_trace, A.q_next);
+            }
+            k_trace_paths<<<g_trace, 128, 0, st>>>(A);
+            k_shade<NL><<<g_shade, 128, 0, st>>>(A);
+            k_trace_rays2<<<g_trace, 128, 0, st>>>(A);
+            k_continue<NL><<<g_shade, 128, 0, st>>>(A);
+        }
+        FL_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+    return FL_OK;
+}
+
+}  // namespace fl
