@@ -141,8 +141,8 @@ fl_status fl_last_error(const fl_context *ctx_h, char *buf, size_t n) {
 fl_status fl_context_create(int32_t device, const fl_spectral_tables *t, fl_context **out) {
     if (!out) return FL_ERR_INVALID;
     *out = nullptr;
-    if (!t || !t->cie_lambda || !t->cie_x || !t->cie_y || !t->cie_z || t->n_cie < 2 || !t->rgb2spec_lambda ||
-        t->n_rgb2spec < 2) {
+    if (!t || !t->cie_lambda || !t->cie_x || !t->cie_y || !t->cie_z || t->n_cie < 2 || t->n_cie > 512 ||
+        !t->rgb2spec_lambda || t->n_rgb2spec < 2 || t->n_rgb2spec > 64) {
         set_error(nullptr, "incomplete spectral tables");
         return FL_ERR_INVALID;
     }
