@@ -113,11 +113,15 @@ def _box(cx, cz, sx, sy, sz, angle_deg):
     return tris
 
 
-def cornell(width=256, height=256) -> Scene:
+def cornell(width=256, height=256, variant="lambert") -> Scene:
     """Cornell-style box of 36 triangles (unit-cube room open at z = 0, two rotated boxes,
-    0.25 x 0.25 ceiling light at y = 0.999 facing down with constant spectral radiance 10)."""
+    0.25 x 0.25 ceiling light at y = 0.999 facing down with constant spectral radiance 10).
+    variant "lambert": every surface Lambertian; "materials": short box GGX conductor
+    (roughness 0.3, eta 0.2, k 3.9), tall box rough dielectric (roughness 0.25, IOR 1.5);
+    "glass": short box conductor (roughness 0.05), tall box smooth glass (IOR 1.5)."""
     tris, mats = [], []
     WHITE, RED, GREEN = 0, 1, 2
+    SHORT, TALL = (3, 4) if variant != "lambert" else (WHITE, WHITE)
     # floor, ceiling, back wall (white)
     tris += _quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)); mats += [WHITE] * 2
     tris += _quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1)); mats += [WHITE] * 2
@@ -126,8 +130,8 @@ def cornell(width=256, height=256) -> Scene:
     tris += _quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)); mats += [RED] * 2
     tris += _quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)); mats += [GREEN] * 2
     # short box (front, image right), tall box (back, image left)
-    tris += _box(0.66, 0.37, 0.3, 0.3, 0.3, -17.0); mats += [WHITE] * 12
-    tris += _box(0.33, 0.67, 0.3, 0.6, 0.3, 17.0); mats += [WHITE] * 12
+    tris += _box(0.66, 0.37, 0.3, 0.3, 0.3, -17.0); mats += [SHORT] * 12
+    tris += _box(0.33, 0.67, 0.3, 0.6, 0.3, 17.0); mats += [TALL] * 12
     # light quad, normal (0, -1, 0)
     h, lo, hi = 0.999, 0.375, 0.625
     light_first = len(tris)
@@ -138,6 +142,12 @@ def cornell(width=256, height=256) -> Scene:
         {"type": T.FL_MAT_LAMBERT, "rgb": (0.63, 0.065, 0.05)},
         {"type": T.FL_MAT_LAMBERT, "rgb": (0.14, 0.45, 0.091)},
     ]
+    if variant == "materials":
+        materials += [{"type": T.FL_MAT_CONDUCTOR, "roughness": 0.3, "eta": 0.2, "k": 3.9},
+                      {"type": T.FL_MAT_ROUGH_DIELECTRIC, "roughness": 0.25, "eta": 1.5}]
+    elif variant == "glass":
+        materials += [{"type": T.FL_MAT_CONDUCTOR, "roughness": 0.05, "eta": 0.2, "k": 3.9},
+                      {"type": T.FL_MAT_SMOOTH_DIELECTRIC, "eta": 1.5}]
     lights = [{"type": T.FL_LIGHT_TRIANGLE, "tri": light_first + k, "radiance": 10.0} for k in range(2)]
     cam = {"position": (0.5, 0.5, -1.4), "look_at": (0.5, 0.5, 0.0), "up": (0.0, 1.0, 0.0), "vfov": 40.0,
            "width": width, "height": height}
@@ -194,3 +204,113 @@ def coherent_rays(width: int, height: int, position=(0.5, 0.5, -1.0), look_at=(0
     dirs[:, :3] = d.reshape(n, 3).astype(np.float32)
     dirs[:, 3] = np.inf
     return org, dirs
+
+
+# ----------------------------------------------------------------------------- procedural spheres
+
+def uv_sphere(slices: int, stacks: int) -> np.ndarray:
+    """unit UV sphere with fan poles: 2 * slices * (stacks - 1) triangles, outward winding
+    (stacks bands between the poles; slices=128, stacks=65 gives 16,384 triangles)."""
+    th = np.linspace(0.0, math.pi, stacks + 1)[1:-1]          # interior rings
+    ph = np.linspace(0.0, 2.0 * math.pi, slices + 1)[:-1]
+    st, ct = np.sin(th), np.cos(th)
+    ring = np.stack([st[:, None] * np.cos(ph)[None, :], np.broadcast_to(ct[:, None], (th.size, ph.size)),
+                     st[:, None] * np.sin(ph)[None, :]], -1)    # (rings, slices, 3)
+    top, bot = np.array([0.0, 1.0, 0.0]), np.array([0.0, -1.0, 0.0])
+    j = np.arange(slices)
+    jn = (j + 1) % slices
+    tris = []
+    r0 = ring[0]
+    tris.append(np.concatenate([np.broadcast_to(top, (slices, 3)), r0[jn], r0[j]], -1))
+    for k in range(ring.shape[0] - 1):
+        a, b = ring[k], ring[k + 1]
+        tris.append(np.concatenate([a[j], a[jn], b[jn]], -1))
+        tris.append(np.concatenate([a[j], b[jn], b[j]], -1))
+    rl = ring[-1]
+    tris.append(np.concatenate([np.broadcast_to(bot, (slices, 3)), rl[j], rl[jn]], -1))
+    return np.concatenate(tris, 0)
+
+
+def value_noise(p: np.ndarray, seed: int, freq: float = 3.0) -> np.ndarray:
+    """seeded 3D value noise in [-1, 1]: random lattice values, smoothstep-trilinear blend."""
+    rng = np.random.default_rng(seed)
+    table = rng.uniform(-1.0, 1.0, 4096)
+    perm = rng.permutation(4096)
+    q = p * freq
+    i0 = np.floor(q).astype(np.int64)
+    f = q - i0
+    w = f * f * (3.0 - 2.0 * f)
+
+    def lat(ix, iy, iz):
+        h = perm[(ix * 73856093 ^ iy * 19349663 ^ iz * 83492791) & 4095]
+        return table[h]
+
+    out = 0.0
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                wx = w[:, 0] if dx else 1 - w[:, 0]
+                wy = w[:, 1] if dy else 1 - w[:, 1]
+                wz = w[:, 2] if dz else 1 - w[:, 2]
+                out = out + wx * wy * wz * lat(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz)
+    return out
+
+
+def procedural_spheres(n_spheres=64, slices=128, stacks=65, width=1920, height=1080, seed=7, extent=10.0,
+                       sphere_light=(0.0, 6.0, 0.0, 0.5, 40.0), env=0.5) -> Scene:
+    """Spheres of `2 * slices * (stacks - 1)` triangles radially displaced by value noise of
+    amplitude 0.05 r, radii U[0.2, 1], centres U[-extent, extent]^2 resting on a 2-triangle
+    ground plane; 40% Lambert (albedo U[0.1, 0.9]), 40% GGX conductor (roughness U[0.05, 0.8],
+    eta 0.2, k 3.9), 20% rough dielectric (IOR 1.5, roughness U[0, 0.3]); constant environment
+    radiance plus one sphere light (x, y, z, radius, radiance). The default is the
+    1,048,578-triangle scene at 1920x1080."""
+    rng = np.random.default_rng(seed)
+    unit = uv_sphere(slices, stacks).reshape(-1, 3, 3)
+    flat = unit.reshape(-1, 3)
+    tris, mats, materials = [], [], []
+    g = 2.0 * extent
+    ground = np.array([[-g, 0, -g, -g, 0, g, g, 0, g], [-g, 0, -g, g, 0, g, g, 0, -g]], np.float32)
+    tris.append(ground)
+    materials.append({"type": 0, "rgb": (0.5, 0.5, 0.5)})
+    mats.append(np.zeros(2, np.uint32))
+    for s in range(n_spheres):
+        r = rng.uniform(0.2, 1.0)
+        cx, cz = rng.uniform(-extent, extent, 2)
+        disp = 1.0 + 0.05 * value_noise(flat, seed * 1000 + s)
+        v = (flat * (r * disp)[:, None] + np.array([cx, r, cz])).reshape(-1, 9)
+        tris.append(v.astype(np.float32))
+        u = rng.uniform()
+        if u < 0.4:
+            a = rng.uniform(0.1, 0.9)
+            materials.append({"type": 0, "rgb": (a, a, a)})
+        elif u < 0.8:
+            materials.append({"type": 1, "roughness": rng.uniform(0.05, 0.8), "eta": 0.2, "k": 3.9})
+        else:
+            materials.append({"type": 2, "roughness": rng.uniform(0.0, 0.3), "eta": 1.5})
+        mats.append(np.full(v.shape[0], len(materials) - 1, np.uint32))
+    verts = np.concatenate(tris, 0).astype(np.float32)
+    lx, ly, lz, lr, le = sphere_light
+    lights = [{"type": 1, "radiance": le, "radius": lr, "center": (lx, ly, lz)}, {"type": 2, "radiance": env}]
+    cam = {"position": (0.0, 7.0, -21.0), "look_at": (0.0, 0.5, 0.0), "up": (0.0, 1.0, 0.0), "vfov": 40.0,
+           "width": width, "height": height}
+    return Scene(verts, np.concatenate(mats), materials, lights, cam)
+
+
+def caustic(width=1024, height=1024, slices=256, stacks=129) -> Scene:
+    """Lambertian room of 12 triangles (albedo 0.7), a sphere light of radius 0.02 and
+    radiance 5e3, and a smooth glass sphere (IOR 1.5, radius 1, 2*slices*(stacks-1) =
+    65,536 triangles by default) above the floor."""
+    tris = []
+    lo, hi = -3.0, 3.0
+    c = [(lo, 0, lo), (hi, 0, lo), (hi, 0, hi), (lo, 0, hi), (lo, 6, lo), (hi, 6, lo), (hi, 6, hi), (lo, 6, hi)]
+    for f in [(0, 1, 2, 3), (7, 6, 5, 4), (0, 4, 5, 1), (2, 6, 7, 3), (1, 5, 6, 2), (3, 7, 4, 0)]:
+        tris += _quad(*(c[i] for i in f))
+    room = np.asarray(tris, np.float32)
+    glass = (uv_sphere(slices, stacks).reshape(-1, 3) * 1.0 + np.array([0.0, 1.6, 0.0])).reshape(-1, 9)
+    verts = np.concatenate([room, glass.astype(np.float32)], 0)
+    mats = np.concatenate([np.zeros(room.shape[0], np.uint32), np.ones(glass.shape[0], np.uint32)])
+    materials = [{"type": 0, "rgb": (0.7, 0.7, 0.7)}, {"type": 3, "eta": 1.5}]
+    lights = [{"type": 1, "radiance": 5e3, "radius": 0.02, "center": (0.3, 4.2, 0.2)}]
+    cam = {"position": (0.0, 3.0, -2.9), "look_at": (0.0, 1.0, 0.5), "up": (0.0, 1.0, 0.0), "vfov": 60.0,
+           "width": width, "height": height}
+    return Scene(verts, mats, materials, lights, cam)

@@ -5,9 +5,15 @@
  * Whitenoise sampler seeds mt19937 from std::random_device,
  * src/filianore/sampling/samplers/whitenoise.h:25-28). This driver supplies them with the
  * same definitions the GPU backend uses, and otherwise runs the reference unchanged:
- *   - scene: one Triangle + LambertMaterial + optional DiffuseAreaIlluminant per soup
- *     triangle (shapes/triangle.h, shading/materials/lambert.h, illuminants/diffusearea.h),
- *     albedos upsampled with from_reflectance_rgb (color/spectrumoperations.cpp:113-147);
+ *   - scene: one Triangle + Material + optional DiffuseAreaIlluminant per soup triangle
+ *     (shapes/triangle.h, illuminants/diffusearea.h). Materials: LambertMaterial
+ *     (shading/materials/lambert.h) with albedos upsampled by from_reflectance_rgb
+ *     (color/spectrumoperations.cpp:113-147), and three compositions of the reference's
+ *     BxDFs in the way StandardSurfaceMaterial builds them (materials/standardsurface.cpp:72-159):
+ *     GGX conductor = MicrofacetReflectionBRDF(GGX(r^2), FresnelConductor(1, eta, k), 1, 1);
+ *     rough dielectric = MicrofacetReflectionBRDF(GGX(r^2), FresnelDielectric(1, ior), 1, 1)
+ *     + MicrofacetTransmissionBRDF(1, 1, 1, 1, 1, ior, GGX(r^2)) in a BSDF with eta = ior;
+ *     smooth dielectric = FresnelSpecularBXDF(1, 1, 1, ior) in a BSDF with eta = ior;
  *   - camera: PhysicalCamera with aperture 0 and flipCameraDirection = true
  *     (cameras/physical.h:11-43): with the default false the camera faces away from
  *     its look-at point, with true it faces it;
@@ -32,7 +38,14 @@
 #include "filianore/illuminants/diffusearea.h"
 #include "filianore/integrators/pathintegrator.h"
 #include "filianore/sampling/sampler.h"
+#include "filianore/shading/bsdf.h"
+#include "filianore/shading/bxdfs/microfacetreflection.h"
+#include "filianore/shading/closures/fresnelspecular.h"
+#include "filianore/shading/closures/microfacettransmission.h"
+#include "filianore/shading/fresnel/fresnelconductor.h"
+#include "filianore/shading/fresnel/fresneldielectric.h"
 #include "filianore/shading/materials/lambert.h"
+#include "filianore/shading/microfacets/ggx.h"
 #include "filianore/shading/textures/constant.h"
 #include "filianore/shapes/triangle.h"
 #include "ext/pcg32.h"
@@ -84,6 +97,57 @@ bool read_n(FILE *f, std::vector<T> &v, size_t n) {
     v.resize(n);
     return n == 0 || fread(v.data(), sizeof(T), n, f) == n;
 }
+
+// Materials composed from the reference's BxDF classes (see the header comment).
+class ConductorMaterial : public Material {
+public:
+    ConductorMaterial(float alpha, float eta, float k) : alpha(alpha), eta(eta), k(k) {}
+    void compute_scattering_functions(SurfaceInteraction *isect) const override {
+        isect->bsdf = std::make_shared<BSDF>(*isect, 1.f);
+        auto distribution = std::make_shared<GGXDistribution>(alpha, alpha);
+        std::shared_ptr<Fresnel> fresnel =
+            std::make_shared<FresnelConductor>(PrincipalSpectrum(1.f), PrincipalSpectrum(eta), PrincipalSpectrum(k));
+        std::unique_ptr<BxDF> lobe =
+            std::make_unique<MicrofacetReflectionBRDF>(distribution, fresnel, PrincipalSpectrum(1.f), 1.f);
+        isect->bsdf->add(lobe);
+    }
+
+private:
+    float alpha, eta, k;
+};
+
+class RoughDielectricMaterial : public Material {
+public:
+    RoughDielectricMaterial(float alpha, float ior) : alpha(alpha), ior(ior) {}
+    void compute_scattering_functions(SurfaceInteraction *isect) const override {
+        isect->bsdf = std::make_shared<BSDF>(*isect, ior);
+        auto distribution = std::make_shared<GGXDistribution>(alpha, alpha);
+        std::shared_ptr<Fresnel> fresnel = std::make_shared<FresnelDielectric>(1.f, ior);
+        std::unique_ptr<BxDF> refl =
+            std::make_unique<MicrofacetReflectionBRDF>(distribution, fresnel, PrincipalSpectrum(1.f), 1.f);
+        isect->bsdf->add(refl);
+        std::unique_ptr<BxDF> trans = std::make_unique<MicrofacetTransmissionBRDF>(
+            PrincipalSpectrum(1.f), 1.f, PrincipalSpectrum(1.f), 1.f, 1.f, ior, distribution);
+        isect->bsdf->add(trans);
+    }
+
+private:
+    float alpha, ior;
+};
+
+class SmoothDielectricMaterial : public Material {
+public:
+    explicit SmoothDielectricMaterial(float ior) : ior(ior) {}
+    void compute_scattering_functions(SurfaceInteraction *isect) const override {
+        isect->bsdf = std::make_shared<BSDF>(*isect, ior);
+        std::unique_ptr<BxDF> lobe =
+            std::make_unique<FresnelSpecularBXDF>(PrincipalSpectrum(1.f), PrincipalSpectrum(1.f), 1.f, ior);
+        isect->bsdf->add(lobe);
+    }
+
+private:
+    float ior;
+};
 
 int dump_tables(const char *out) {
     InitializeSpectrals();
@@ -175,9 +239,21 @@ int render(const char *scene_path, const char *out_path) {
 
     std::vector<std::shared_ptr<Material>> materials;
     for (const auto &m : mats) {
-        if (m.type != FL_MAT_LAMBERT) { fprintf(stderr, "harness supports Lambert materials only\n"); return 2; }
-        PrincipalSpectrum r = from_reflectance_rgb(Vector3f(m.rgb[0], m.rgb[1], m.rgb[2]));
-        materials.push_back(std::make_shared<LambertMaterial>(std::make_shared<ConstantTexture<PrincipalSpectrum>>(r)));
+        const float alpha = m.roughness * m.roughness;
+        if (m.type == FL_MAT_LAMBERT) {
+            PrincipalSpectrum r = from_reflectance_rgb(Vector3f(m.rgb[0], m.rgb[1], m.rgb[2]));
+            materials.push_back(
+                std::make_shared<LambertMaterial>(std::make_shared<ConstantTexture<PrincipalSpectrum>>(r)));
+        } else if (m.type == FL_MAT_CONDUCTOR) {
+            materials.push_back(std::make_shared<ConductorMaterial>(alpha, m.eta, m.k));
+        } else if (m.type == FL_MAT_ROUGH_DIELECTRIC) {
+            materials.push_back(std::make_shared<RoughDielectricMaterial>(alpha, m.eta));
+        } else if (m.type == FL_MAT_SMOOTH_DIELECTRIC) {
+            materials.push_back(std::make_shared<SmoothDielectricMaterial>(m.eta));
+        } else {
+            fprintf(stderr, "unknown material type\n");
+            return 2;
+        }
     }
     std::vector<std::shared_ptr<Shape>> shapes(h.n_tri);
     for (uint32_t i = 0; i < h.n_tri; ++i) {

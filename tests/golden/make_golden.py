@@ -9,6 +9,9 @@ reference sources with oracle/Makefile). Outputs:
   pcg32_kat.npz         pcg32 sequences from the vendored src/ext/pcg32.h
   cornell_ref.npz       the reference integrator's XYZ film sums for the 36-triangle Cornell
                         box: 64x64 at 4 spp (float64) and 256x256 at 16 spp (float32)
+  cornell_materials_ref.npz  the same with GGX conductor + rough dielectric boxes
+                        ("materials") and conductor + smooth glass boxes ("glass"):
+                        64x64 at 4 spp (float64) and 128x128 at 16 spp (float32)
 Usage: python tests/golden/make_golden.py
 """
 import os
@@ -59,6 +62,19 @@ def main():
         out[f"{key}_spp"] = np.int32(spp)
         print(key, info)
     np.savez_compressed(os.path.join(HERE, "cornell_ref.npz"), **out)
+    # the same box with the GGX conductor / rough dielectric / smooth glass materials
+    out = {}
+    for variant in ("materials", "glass"):
+        for (W, spp, key, dt) in [(64, 4, "small", np.float64), (128, 16, "full", np.float32)]:
+            sc = scenes.cornell(W, W, variant)
+            p = scenes.render_params(spp, 8, T.FL_SPECTRAL_BINS60)
+            spath = os.path.join(tmp, f"{variant}_{key}.scene")
+            fpath = os.path.join(tmp, f"{variant}_{key}.film")
+            oracle.write_scene_file(spath, sc, p)
+            film, info = oracle.run_reference(spath, fpath, W, W)
+            out[f"{variant}_{key}_xyz"] = film.astype(dt)
+            print(variant, key, info)
+    np.savez_compressed(os.path.join(HERE, "cornell_materials_ref.npz"), **out)
 
 
 if __name__ == "__main__":
