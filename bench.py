@@ -2,20 +2,29 @@
 
 `python bench.py --gpus N --steps K --warmup W` prints one JSON line (rank 0).
 
-Workloads (all inputs synthetic and seeded, FP32):
+Workloads (all inputs synthetic and seeded, FP32 geometry):
+  render (default)  procedural scene of 1,048,578 triangles: 64 UV spheres of 16,384
+           triangles (radial value-noise displacement, amplitude 0.05 r) on a 2-triangle
+           ground plane; 40% Lambert, 40% GGX conductor (eta 0.2, k 3.9), 20% rough
+           dielectric (IOR 1.5); constant environment 0.5 plus one sphere light;
+           1920x1080, 64 spp, max depth 16, 4 hero wavelengths. One step = one frame.
+           The working set (path state ~0.8 GB per wave, BVH ~60 MB, film 50 MB) is
+           larger than the 126 MB L2, so no flush is needed between steps.
   raycast  8,388,608-triangle soup (centroids U[0,1]^3, edges N(0, 0.002^2)) and
            16,777,216 incoherent rays (origins U[-0.1,1.1]^3, directions uniform on the
-           sphere, tmax inf); one step = one closest-hit batch over all rays.
-           Inputs (768 MB of rays + ~1 GB of BVH) exceed the 126 MB L2, so no flush
-           is needed between steps.
-`--impl reference` times the CPU path on the host cores (rank 0 only) on the same
-workload: the CPU oracle's closest-hit traversal over a bounded sample of the rays.
-Multi-GPU: one process per GPU, each rank traces its own ray batch (different seed)
-against its own copy of the scene; no collective on the data path ("scaling": "weak").
+           sphere, tmax inf); one step = one closest-hit batch. Inputs exceed L2.
+`--impl reference` times the CPU implementation of the same workload on the host cores
+(rank 0 only): the CPU oracle, a restatement of the reference's integrator pinned
+bit-exact against the reference's own build, on a bounded sample of pixels or rays.
+Multi-GPU: one process per GPU. render: each rank renders its own 64-spp pass of the
+same image (samples offset by rank) and the FP64 films are summed to rank 0 with one
+NCCL reduce per frame; raycast: each rank traces its own ray batch (no collective).
+Per-GPU work is fixed as N grows ("scaling": "weak").
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -35,6 +44,7 @@ NODE_BYTES = 80
 TRI_BYTES = 48
 RAY_BYTES = 32
 HIT_BYTES = 16
+RENDER = {"width": 1920, "height": 1080, "spp": 64, "depth": 16}
 
 
 def load_peaks():
@@ -88,80 +98,180 @@ class ClockSampler:
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows)}
 
 
-def dist_setup(n_gpus):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+def dist_env():
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def raycast_workload(rank):
+# ----------------------------------------------------------------------------- workloads
+
+def render_scene():
+    from filianore_b200 import scenes
+    return scenes.procedural_spheres(64, 128, 65, RENDER["width"], RENDER["height"])
+
+
+def raycast_inputs(rank):
     from filianore_b200 import scenes
     tris = scenes.triangle_soup(N_TRI, seed=1)
     org, dirs = scenes.incoherent_rays(N_RAYS, seed=2 + rank)
     return tris, org, dirs
 
 
-def cpu_reference(args, world, rank):
-    """CPU baseline on the host cores: the oracle's BVH closest-hit over a ray sample."""
-    if rank != 0:
-        return None
+def cpu_render(steps, warmup, stride=64):
+    """The oracle's integrator (hero wavelengths, all host threads) on every `stride`-th pixel."""
     import oracle
-    tris, org, dirs = raycast_workload(0)
+    import filianore_b200 as fb
+    from filianore_b200 import scenes
+    sc = render_scene()
+    tab = oracle.Tables(fb.reference_tables())
+    n_pix = RENDER["width"] * RENDER["height"]
+    cores = os.cpu_count() or 1
+    rates, mrays = [], []
+    for i in range(warmup + steps):
+        pixels = np.arange(i % stride, n_pix, stride, dtype=np.uint32)
+        p = scenes.render_params(RENDER["spp"], RENDER["depth"], fb.FL_SPECTRAL_HERO4)
+        t0 = time.perf_counter()
+        _, cnt = oracle.render(sc, tab, p, nthreads=cores, pixels=pixels)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            rates.append(cnt["paths"] / dt)
+            mrays.append(cnt["rays"] / dt / 1e6)
+    return {"value": round(statistics.mean(mrays), 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+            "samples_per_s": round(statistics.mean(rates), 1),
+            "sample": f"every {stride}th pixel of the 1920x1080 frame ({n_pix // stride} pixels x 64 spp per step), "
+                      f"CPU oracle integrator (bit-exact restatement of the reference integrator; the scene's "
+                      f"environment and sphere lights have no reference class)"}
+
+
+def cpu_raycast(steps, warmup):
+    import oracle
+    tris, org, dirs = raycast_inputs(0)
     t0 = time.perf_counter()
     bvh = oracle.CpuBVH(tris)
     build_s = time.perf_counter() - t0
     cores = os.cpu_count() or 1
     sample = 1 << 20
     times = []
-    for i in range(args.warmup + args.steps):
+    for i in range(warmup + steps):
         sl = slice((i * sample) % N_RAYS, (i * sample) % N_RAYS + sample)
         t0 = time.perf_counter()
         bvh.trace(org[sl], dirs[sl], nthreads=cores)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            times.append(dt)
-    mrays = sample / statistics.mean(times) / 1e6
-    return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+        if i >= warmup:
+            times.append(time.perf_counter() - t0)
+    return {"value": round(sample / statistics.mean(times) / 1e6, 3), "unit": "Mrays/s", "cores": cores,
+            "kind": "port",
             "sample": f"{sample} of the {N_RAYS} incoherent rays per step against the full {N_TRI}-triangle soup "
                       f"(oracle binned-SAH BVH, build {build_s:.1f} s not timed)"}
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    args = ap.parse_args()
-    args.warmup = max(3, args.warmup)
-    world, rank, local = dist_setup(args.gpus)
-    config = {"workload": "raycast: 8,388,608-triangle soup, 16,777,216 incoherent rays, closest hit",
-              "n_tri": N_TRI, "rays_per_gpu": N_RAYS, "l2": "inputs larger than L2 (no flush)",
-              "parallelism": f"replicas x{world}"}
+def config_of(workload, world):
+    if workload == "render":
+        return {"workload": "render: procedural 1,048,578-triangle scene (64 displaced spheres, Lambert / GGX "
+                            "conductor / rough dielectric, environment + sphere light), 1920x1080, 64 spp, "
+                            "max depth 16, 4 hero wavelengths",
+                "n_tri": 1048578, "width": 1920, "height": 1080, "spp": 64, "max_depth": 16,
+                "l2": "working set larger than L2 (no flush)", "parallelism": f"sample split x{world}"}
+    return {"workload": "raycast: 8,388,608-triangle soup, 16,777,216 incoherent rays, closest hit",
+            "n_tri": N_TRI, "rays_per_gpu": N_RAYS, "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"replicas x{world}"}
 
-    if args.impl == "reference":
-        if rank == 0:
-            cb = cpu_reference(args, world, rank)
-            line = {"metric": "Mrays/s", "value": cb["value"], "unit": "Mrays/s", "n_gpus": world,
-                    "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                    "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
-                    "impl": "reference", "cpu_baseline": cb,
-                    "e2e": {"value": cb["value"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
-                            "d2h_bytes_per_step": 0}}
-            print(json.dumps(line), flush=True)
-        return
 
+# ----------------------------------------------------------------------------- GPU arms
+
+def gpu_render(args, world, rank, local, barrier, reduce_max):
     import torch
     import filianore_b200 as fb
-    torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    tris, org, dirs = raycast_workload(rank)
     from filianore_b200 import scenes
+    sc = render_scene()
+    ctx = fb.Context(local)
+    scene = ctx.scene(sc)
+    info = scene.info()
+    W, H = RENDER["width"], RENDER["height"]
+    film = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
+    xyz = torch.zeros((H, W, 3), dtype=torch.float64, device="cuda")
+
+    def params(flags=0, offset=0):
+        return scenes.render_params(RENDER["spp"], RENDER["depth"], fb.FL_SPECTRAL_HERO4, sample_offset=offset,
+                                    flags=flags)
+
+    def frame(p):
+        _, st = scene.render(p, film_rgb=film, film_xyz64=xyz, memory=fb.FL_MEM_DEVICE)
+        if world > 1:
+            import torch.distributed as dist
+            dist.reduce(xyz, dst=0, op=dist.ReduceOp.SUM)
+        return st
+
+    for _ in range(args.warmup):
+        frame(params(offset=rank * RENDER["spp"]))
+    # traversal work of one frame (instrumented, untimed)
+    cstats = frame(params(fb.FL_RENDER_COUNT, rank * RENDER["spp"]))
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    stats = []
+    for _ in range(args.steps):
+        stats.append(frame(params(fb.FL_RENDER_PROFILE, rank * RENDER["spp"])))
+    t_end.record()
+    barrier()
+    clk = clocks.stop()
+    dev_ms = sum(s["ms"] for s in stats)               # device time of the renders (library events)
+    wall_ms = t_start.elapsed_time(t_end)              # includes the film reduce for N > 1
+    total_ms = reduce_max(max(dev_ms, wall_ms))
+    rays = sum(s["rays"] for s in stats)
+    paths = sum(s["paths"] for s in stats)
+    value = world * rays / (total_ms / 1e3) / 1e6
+    samples_per_s = world * paths / (total_ms / 1e3)
+
+    # end to end through the C ABI: host film (D2H of the linear RGB image per frame)
+    host_film = torch.zeros((H, W, 3), dtype=torch.float32).pin_memory()
+    e2e_steps = max(2, args.steps // 2)
+    scene.render(params(offset=rank * RENDER["spp"]), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
+    barrier()
+    t0 = time.perf_counter()
+    e_rays = 0
+    for _ in range(e2e_steps):
+        _, st = scene.render(params(offset=rank * RENDER["spp"]), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
+        e_rays += st["rays"]
+    barrier()
+    e2e_s = reduce_max(time.perf_counter() - t0)
+    e2e = {"value": round(world * e_rays / e2e_s / 1e6, 3), "unit": "Mrays/s",
+           "samples_per_s": round(world * e2e_steps * W * H * RENDER["spp"] / e2e_s, 1),
+           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 3 * 4,
+           "note": "scene resident in HBM; camera and parameters travel as kernel arguments"}
+
+    peaks = load_peaks()
+    trav_ms = statistics.mean(s["ms_trace"] + s["ms_shadow"] for s in stats)
+    alg_bytes = cstats["rays"] * (RAY_BYTES + HIT_BYTES) + NODE_BYTES * cstats["nodes_visited"] + \
+        TRI_BYTES * cstats["tris_tested"]
+    achieved = alg_bytes / (trav_ms / 1e3) / 1e9
+    share = {k: round(statistics.mean(s[f"ms_{k}"] for s in stats) / statistics.mean(s["ms"] for s in stats), 4)
+             for k in ("trace", "shade", "shadow", "continue")}
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None, "peak_src": peaks["src"],
+                "kernel": "BVH traversal (k_trace_paths + k_trace_rays2)",
+                "alg_bytes_per_frame": int(alg_bytes), "traversal_ms_per_frame": round(trav_ms, 3),
+                "nodes_per_ray": round(cstats["nodes_visited"] / cstats["rays"], 2),
+                "tris_per_ray": round(cstats["tris_tested"] / cstats["rays"], 2), "time_share": share}
+    line = {"metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "samples_per_s": round(samples_per_s, 1),
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of("render", world),
+            "roofline": roofline, "e2e": e2e, "gpu_launches": sum(s["launches"] for s in stats), "clocks": clk,
+            "rays_per_frame": stats[0]["rays"], "paths_per_frame": stats[0]["paths"],
+            "bvh": {"nodes": info["n_nodes"], "depth": info["max_depth"], "build_ms": round(info["build_ms"], 2),
+                    "bytes": info["bvh_bytes"]}}
+    scene.close()
+    ctx.close()
+    return line
+
+
+def gpu_raycast(args, world, rank, local, barrier, reduce_max):
+    import torch
+    import filianore_b200 as fb
+    from filianore_b200 import scenes
+    tris, org, dirs = raycast_inputs(rank)
     sc = scenes.Scene(tris, np.zeros(N_TRI, np.uint32), [{"type": 0, "rgb": (0.5, 0.5, 0.5)}], [], None)
     ctx = fb.Context(local)
     scene = ctx.scene(sc)
@@ -172,13 +282,6 @@ def main():
     stream = torch.cuda.current_stream().cuda_stream
     nodes, trisv = scene.trace_count(d_org, d_dir)
     alg_bytes = N_RAYS * (RAY_BYTES + HIT_BYTES) + NODE_BYTES * nodes + TRI_BYTES * trisv
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-        torch.cuda.synchronize()
-
     for _ in range(args.warmup):
         scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
     clocks = ClockSampler(local)
@@ -195,62 +298,98 @@ def main():
     t_end.record()
     barrier()
     clk = clocks.stop()
-    total_ms = t_start.elapsed_time(t_end)
+    total_ms = reduce_max(t_start.elapsed_time(t_end))
     per_launch = [a.elapsed_time(b) for a, b in ev]
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
     value = world * N_RAYS * args.steps / (total_ms / 1e3) / 1e6
-
-    # end to end through the C ABI with pinned host buffers (H2D rays, D2H hits inside the call)
     h_org = torch.from_numpy(org).pin_memory()
     h_dir = torch.from_numpy(dirs).pin_memory()
     h_hits = torch.empty((N_RAYS, 4), dtype=torch.int32).pin_memory()
-    import ctypes as C
     L = fb.lib()
     e2e_steps = max(2, args.steps // 2)
-    L.fl_trace_closest(scene.h, C.c_void_p(h_org.data_ptr()), C.c_void_p(h_dir.data_ptr()), N_RAYS,
-                       C.c_void_p(h_hits.data_ptr()), fb.FL_MEM_HOST, None)
+
+    def host_call():
+        fb.check(L.fl_trace_closest(scene.h, C.c_void_p(h_org.data_ptr()), C.c_void_p(h_dir.data_ptr()), N_RAYS,
+                                    C.c_void_p(h_hits.data_ptr()), fb.FL_MEM_HOST, None), ctx.h)
+    host_call()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        fb.check(L.fl_trace_closest(scene.h, C.c_void_p(h_org.data_ptr()), C.c_void_p(h_dir.data_ptr()), N_RAYS,
-                                    C.c_void_p(h_hits.data_ptr()), fb.FL_MEM_HOST, None), ctx.h)
+        host_call()
     barrier()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = reduce_max((time.perf_counter() - t0) / e2e_steps)
     e2e = {"value": round(world * N_RAYS / e2e_s / 1e6, 3), "unit": "Mrays/s",
            "h2d_bytes_per_step": N_RAYS * RAY_BYTES, "d2h_bytes_per_step": N_RAYS * HIT_BYTES}
-
     peaks = load_peaks()
     launch_ms = statistics.mean(per_launch)
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
-                "peak_src": peaks["src"], "kernel": "k_trace<closest>",
-                "alg_bytes_per_launch": int(alg_bytes), "nodes_per_ray": round(nodes / N_RAYS, 2),
-                "tris_per_ray": round(trisv / N_RAYS, 2)}
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_reference(args, 1, 0)
-    if rank == 0:
-        line = {"metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": args.steps, "clocks": clk,
-                "bvh": {"nodes": info["n_nodes"], "depth": info["max_depth"], "build_ms": round(info["build_ms"], 2),
-                        "bytes": info["bvh_bytes"]}}
-        print(json.dumps(line), flush=True)
+                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None, "peak_src": peaks["src"],
+                "kernel": "k_trace<closest>", "alg_bytes_per_launch": int(alg_bytes),
+                "nodes_per_ray": round(nodes / N_RAYS, 2), "tris_per_ray": round(trisv / N_RAYS, 2)}
+    line = {"metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of("raycast", world), "roofline": roofline, "e2e": e2e, "gpu_launches": args.steps,
+            "clocks": clk, "bvh": {"nodes": info["n_nodes"], "depth": info["max_depth"],
+                                   "build_ms": round(info["build_ms"], 2), "bytes": info["bvh_bytes"]}}
     scene.close()
     ctx.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="render", choices=["render", "raycast"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_env()
+
+    if args.impl == "reference":
+        if rank == 0:
+            cb = cpu_render(args.steps, args.warmup) if args.workload == "render" else cpu_raycast(args.steps, args.warmup)
+            line = {"metric": "Mrays/s", "value": cb["value"], "unit": "Mrays/s", "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                    "config": config_of(args.workload, world), "impl": "reference", "cpu_baseline": cb,
+                    "e2e": {"value": cb["value"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}
+            if "samples_per_s" in cb:
+                line["samples_per_s"] = cb["samples_per_s"]
+            print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce_max(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([float(x)], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    run = gpu_render if args.workload == "render" else gpu_raycast
+    line = run(args, world, rank, local, barrier, reduce_max)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = (cpu_render(2, 0) if args.workload == "render" else cpu_raycast(3, 1))
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -6,9 +6,9 @@
 
 namespace fl {
 extern template fl_status render_waves<4>(Scene *, const CamDev &, const fl_render_params &, double *, WaveCounters *,
-                                          cudaStream_t);
+                                          RenderProfile *, cudaStream_t);
 extern template fl_status render_waves<60>(Scene *, const CamDev &, const fl_render_params &, double *,
-                                           WaveCounters *, cudaStream_t);
+                                           WaveCounters *, RenderProfile *, cudaStream_t);
 
 // PhysicalCamera::PhysicalCamera (cameras/physical.h:11-43) with aperture 0 and
 // flipCameraDirection = true (the orientation that faces look_at).
@@ -82,8 +82,10 @@ extern "C" fl_status fl_render(fl_scene *scene_h, const fl_camera *camera, const
     FL_CUDA_TRY(ctx, cudaEventCreate(&e1));
     FL_CUDA_TRY(ctx, cudaEventRecord(e0, st));
     WaveCounters hc{};
-    rc = p.spectral_mode == FL_SPECTRAL_BINS60 ? render_waves<60>(s, cam, p, d_xyz, &hc, st)
-                                               : render_waves<4>(s, cam, p, d_xyz, &hc, st);
+    RenderProfile prof;
+    prof.on = (p.flags & FL_RENDER_PROFILE) != 0;
+    rc = p.spectral_mode == FL_SPECTRAL_BINS60 ? render_waves<60>(s, cam, p, d_xyz, &hc, &prof, st)
+                                               : render_waves<4>(s, cam, p, d_xyz, &hc, &prof, st);
     if (rc) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
@@ -110,7 +112,15 @@ extern "C" fl_status fl_render(fl_scene *scene_h, const fl_camera *camera, const
         stats->bounces = hc.bounces;
         stats->ms = ms;
         stats->traversal_errors = (uint32_t)hc.err;
-        stats->reserved = 0;
+        stats->launches = prof.launches + 1;
+        double cls[4] = {0, 0, 0, 0};
+        if (prof.on) prof.sum(cls);
+        stats->ms_trace = cls[0];
+        stats->ms_shade = cls[1];
+        stats->ms_shadow = cls[2];
+        stats->ms_continue = cls[3];
+        stats->nodes_visited = hc.nodes;
+        stats->tris_tested = hc.tris;
     }
     if (hc.err) {
         set_error(ctx, std::to_string(hc.err) + " traversal or queue bound hits during the render");

@@ -20,6 +20,8 @@
 // host synchronisation. Finished paths add to_xyz(L) to an FP64 film with atomics.
 #pragma once
 
+#include <vector>
+
 #include "fl_internal.h"
 #include "fl_shading.cuh"
 #include "fl_traverse.cuh"
@@ -29,8 +31,37 @@ namespace fl {
 struct WaveCounters {
     uint32_t n_trace, n_cont, n_next, n_shadow;
     unsigned long long rays, shadow_rays, bounces, paths;
+    unsigned long long nodes, tris;  // FL_RENDER_COUNT
     int err;
     int pad[3];
+};
+
+// FL_RENDER_PROFILE: CUDA events bracketing every launch, grouped by kernel class
+struct RenderProfile {
+    bool on = false;
+    std::vector<cudaEvent_t> ev[4];  // pairs (start, stop) per class: trace, shade, shadow, continue
+    uint32_t launches = 0;
+    void mark(int cls, cudaStream_t st) {
+        if (!on) return;
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, st);
+        ev[cls].push_back(e);
+    }
+    void sum(double ms[4]) {
+        for (int c = 0; c < 4; ++c) {
+            ms[c] = 0.0;
+            for (size_t i = 0; i + 1 < ev[c].size(); i += 2) {
+                float t = 0.f;
+                cudaEventElapsedTime(&t, ev[c][i], ev[c][i + 1]);
+                ms[c] += t;
+            }
+        }
+    }
+    ~RenderProfile() {
+        for (auto &v : ev)
+            for (cudaEvent_t e : v) cudaEventDestroy(e);
+    }
 };
 
 struct CamDev {
@@ -176,10 +207,10 @@ __device__ inline void make_bsdf(const RenderArgs &A, const SmemTables &sm, cons
 }
 
 // closest hit over triangles and analytic sphere lights
-__device__ inline TraceResult closest_with_spheres(const RenderArgs &A, const RayPre &r, bool &err) {
-    TraceStats st;
+template <bool COUNT>
+__device__ inline TraceResult closest_with_spheres(const RenderArgs &A, const RayPre &r, bool &err, TraceStats &st) {
     TraceResult res;
-    if (A.n_nodes) res = traverse<false, false>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
+    if (A.n_nodes) res = traverse<false, COUNT>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
     else { res.id = -1; res.t = r.tmax; res.u = res.v = 0.f; }
     if (A.has_spheres) {
         const v3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
@@ -252,18 +283,24 @@ static __global__ void __launch_bounds__(128) k_advance(WaveCounters *cnt) {
     cnt->n_shadow = 0;
 }
 
-static __global__ void __launch_bounds__(128) k_trace_paths(RenderArgs A) {
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_trace_paths(RenderArgs A) {
     const uint32_t n = load_count(&A.cnt->n_trace);
     uint32_t local = 0;
     bool err = false;
+    TraceStats st;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const uint32_t slot = A.q_trace[q];
         const RayPre r = ray_precompute(A.ray_o[slot], A.ray_d[slot]);
-        const TraceResult res = closest_with_spheres(A, r, err);
+        const TraceResult res = closest_with_spheres<COUNT>(A, r, err, st);
         A.hit[slot] = make_int4(res.id, __float_as_int(res.t), __float_as_int(res.u), __float_as_int(res.v));
         ++local;
     }
     warp_count(&A.cnt->rays, local);
+    if (COUNT) {
+        warp_count(&A.cnt->nodes, st.nodes);
+        warp_count(&A.cnt->tris, st.tris);
+    }
     if (err) atomicAdd(&A.cnt->err, 1);
 }
 
@@ -417,10 +454,12 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
 }
 
 // shadow rays (kind 0) and MIS rays (kind 1)
-static __global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
     const uint32_t n = min(load_count(&A.cnt->n_shadow), A.scap);
     uint32_t local = 0;
     bool err = false;
+    TraceStats st;
     for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         const uint32_t tag = A.stag[q];
         const uint32_t kind = tag & 1u;
@@ -429,15 +468,14 @@ static __global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
         const RayPre r = ray_precompute(A.sray_o[q], A.sray_d[q]);
         uint32_t bit = 0;
         if (kind == 0) {
-            TraceStats st;
             TraceResult res;
             if (A.n_nodes == 0) res.id = -1;
-            else if (A.any_hit_ok) res = traverse<true, false>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
-            else res = traverse<false, false>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
+            else if (A.any_hit_ok) res = traverse<true, COUNT>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
+            else res = traverse<false, COUNT>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
             const bool unocc = res.id < 0 || A.tri_light[res.id] >= 0;
             bit = unocc ? kVisOK : 0u;
         } else {
-            const TraceResult res = closest_with_spheres(A, r, err);
+            const TraceResult res = closest_with_spheres<COUNT>(A, r, err, st);
             const LightDev Ll = A.lights[li];
             bool ok = false;
             if (res.id == -1) ok = Ll.type == FL_LIGHT_ENV;
@@ -453,6 +491,10 @@ static __global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
     }
     warp_count(&A.cnt->shadow_rays, local);
     warp_count(&A.cnt->rays, local);
+    if (COUNT) {
+        warp_count(&A.cnt->nodes, st.nodes);
+        warp_count(&A.cnt->tris, st.tris);
+    }
     if (err) atomicAdd(&A.cnt->err, 1);
 }
 
@@ -582,7 +624,7 @@ inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 // per spectral mode in its own translation unit (the 60-bin one without FMA contraction).
 template <int NL>
 fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film,
-                       WaveCounters *h_cnt, cudaStream_t st) {
+                       WaveCounters *h_cnt, RenderProfile *prof, cudaStream_t st) {
     Context *ctx = s->ctx;
     const int nl = (int)s->n_lights;
     const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
@@ -664,6 +706,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     A.q_cont = reinterpret_cast<uint32_t *>(B + o_qc);
     FL_CUDA_TRY(ctx, cudaMemsetAsync(A.cnt, 0, sizeof(WaveCounters), st));
 
+    const bool count = (p.flags & FL_RENDER_COUNT) != 0;
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
     const int g_trace = sms * 16, g_shade = sms * 8;
     for (unsigned long long wb = 0; wb < total; wb += cap) {
@@ -677,11 +720,23 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
                 k_advance<<<1, 1, 0, st>>>(A.cnt);
                 std::swap(A.q_trace, A.q_next);
             }
-            k_trace_paths<<<g_trace, 128, 0, st>>>(A);
+            prof->mark(0, st);
+            if (count) k_trace_paths<true><<<g_trace, 128, 0, st>>>(A);
+            else k_trace_paths<false><<<g_trace, 128, 0, st>>>(A);
+            prof->mark(0, st);
+            prof->mark(1, st);
             k_shade<NL><<<g_shade, 128, 0, st>>>(A);
-            k_trace_rays2<<<g_trace, 128, 0, st>>>(A);
+            prof->mark(1, st);
+            prof->mark(2, st);
+            if (count) k_trace_rays2<true><<<g_trace, 128, 0, st>>>(A);
+            else k_trace_rays2<false><<<g_trace, 128, 0, st>>>(A);
+            prof->mark(2, st);
+            prof->mark(3, st);
             k_continue<NL><<<g_shade, 128, 0, st>>>(A);
+            prof->mark(3, st);
+            prof->launches += b > 0 ? 5 : 4;
         }
+        prof->launches += 1;
         FL_CUDA_TRY(ctx, cudaGetLastError());
     }
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));

@@ -4,6 +4,6 @@
 #include "fl_render.cuh"
 
 namespace fl {
-template fl_status render_waves<60>(Scene *, const CamDev &, const fl_render_params &, double *, WaveCounters *,
+template fl_status render_waves<60>(Scene *, const CamDev &, const fl_render_params &, double *, WaveCounters *, RenderProfile *,
                                     cudaStream_t);
 }

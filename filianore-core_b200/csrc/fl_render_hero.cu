@@ -2,6 +2,6 @@
 #include "fl_render.cuh"
 
 namespace fl {
-template fl_status render_waves<4>(Scene *, const CamDev &, const fl_render_params &, double *, WaveCounters *,
+template fl_status render_waves<4>(Scene *, const CamDev &, const fl_render_params &, double *, WaveCounters *, RenderProfile *,
                                    cudaStream_t);
 }

@@ -23,6 +23,17 @@
 
 namespace fl {
 
+// sin/cos of the path sampling code. The 60-bin parity build (FL_PARITY_MATH) evaluates
+// them in double and rounds once, which gives the correctly rounded float result that
+// the host C library returns for std::sin/std::cos(float); the hero build uses sinf/cosf.
+#if defined(FL_PARITY_MATH)
+static __device__ inline float fl_sin(float x) { return (float)sin((double)x); }
+static __device__ inline float fl_cos(float x) { return (float)cos((double)x); }
+#else
+static __device__ inline float fl_sin(float x) { return sinf(x); }
+static __device__ inline float fl_cos(float x) { return cosf(x); }
+#endif
+
 enum : int {
     kBsdfReflection = 1 << 0,
     kBsdfTransmission = 1 << 1,
@@ -212,8 +223,8 @@ __device__ inline v3 ggx_sample_wh(const Bsdf<NL> &b, v3 wo, float ux, float uy)
     const v3 T2 = cross(vh, T1);
     const float r = sqrtf(ux);
     const float phi = 2.f * kPi * uy;
-    const float t1 = r * cosf(phi);
-    float t2 = r * sinf(phi);
+    const float t1 = r * fl_cos(phi);
+    float t2 = r * fl_sin(phi);
     const float s = (float)((1.f + vh.z) * 0.5);
     t2 = (1.f - s) * sqrtf(1 - (t1 * t1)) + (s * t2);
     const float zz = 1.f - t1 * t1 - t2 * t2;
@@ -347,8 +358,8 @@ __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, f
             float theta, r;
             if (fabsf(ox) > fabsf(oy)) { r = ox; theta = kPiOver4 * (oy / ox); }
             else { r = oy; theta = kPiOver2 - kPiOver4 * (ox / oy); }
-            dx = r * cosf(theta);
-            dy = r * sinf(theta);
+            dx = r * fl_cos(theta);
+            dy = r * fl_sin(theta);
         }
         const float zz = 1.f - dx * dx - dy * dy;
         wi = mk(dx, dy, sqrtf(zz > 0.f ? zz : 0.f));
@@ -601,7 +612,7 @@ __device__ inline LightSample light_sample_li(const LightDev &L, const float *__
         const float z = 1.f - 2.f * ux;
         const float rr = sqrtf(fmaxf(0.f, 1.f - z * z));
         const float phi = 2.f * kPi * uy;
-        const v3 nrm = mk(rr * cosf(phi), rr * sinf(phi), z);
+        const v3 nrm = mk(rr * fl_cos(phi), rr * fl_sin(phi), z);
         const v3 ip = add(c, mul(nrm, L.radius));
         v3 w = sub(ip, ref.p);
         const float d2 = len2(w);
@@ -621,7 +632,7 @@ __device__ inline LightSample light_sample_li(const LightDev &L, const float *__
     const float z = 1.f - 2.f * ux;
     const float rr = sqrtf(fmaxf(0.f, 1.f - z * z));
     const float phi = 2.f * kPi * uy;
-    ls.wi = mk(rr * cosf(phi), rr * sinf(phi), z);
+    ls.wi = mk(rr * fl_cos(phi), rr * fl_sin(phi), z);
     ls.pdf = kInv4Pi;
     ls.vis_kind = 2;
     ls.radiance = L.radiance;

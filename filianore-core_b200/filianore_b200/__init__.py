@@ -215,4 +215,4 @@ class SceneHandle:
         xyz = _ptr(film_xyz64) if film_xyz64 is not None else None
         check(lib().fl_render(self.h, C.byref(cam), C.byref(params), _ptr(film_rgb), xyz, mem, C.byref(stats)),
               self.ctx.h)
-        return film_rgb, {k: getattr(stats, k) for k, _ in T.fl_render_stats._fields_ if k != "reserved"}
+        return film_rgb, {k: getattr(stats, k) for k, _ in T.fl_render_stats._fields_}

@@ -74,8 +74,9 @@ class Scene:
         return cam
 
 
-def render_params(spp, max_depth, mode=T.FL_SPECTRAL_HERO4, rr=1.0, wave_paths=0, sample_offset=0):
+def render_params(spp, max_depth, mode=T.FL_SPECTRAL_HERO4, rr=1.0, wave_paths=0, sample_offset=0, flags=0):
     p = T.fl_render_params()
+    p.flags = flags
     p.spp = spp
     p.max_depth = max_depth
     p.rr_threshold = rr
@@ -291,8 +292,8 @@ def procedural_spheres(n_spheres=64, slices=128, stacks=65, width=1920, height=1
     verts = np.concatenate(tris, 0).astype(np.float32)
     lx, ly, lz, lr, le = sphere_light
     lights = [{"type": 1, "radiance": le, "radius": lr, "center": (lx, ly, lz)}, {"type": 2, "radiance": env}]
-    cam = {"position": (0.0, 7.0, -21.0), "look_at": (0.0, 0.5, 0.0), "up": (0.0, 1.0, 0.0), "vfov": 40.0,
-           "width": width, "height": height}
+    cam = {"position": (0.0, 0.7 * extent, -2.1 * extent), "look_at": (0.0, 0.5, 0.0), "up": (0.0, 1.0, 0.0),
+           "vfov": 40.0, "width": width, "height": height}
     return Scene(verts, np.concatenate(mats), materials, lights, cam)
 
 

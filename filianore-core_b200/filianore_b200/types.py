@@ -26,6 +26,9 @@ FL_LIGHT_ENV = 2
 FL_SPECTRAL_HERO4 = 0
 FL_SPECTRAL_BINS60 = 1
 
+FL_RENDER_PROFILE = 1
+FL_RENDER_COUNT = 2
+
 
 class fl_spectral_tables(C.Structure):
     _fields_ = [
@@ -110,7 +113,8 @@ class fl_render_params(C.Structure):
         ("spectral_mode", C.c_int32),
         ("wave_paths", C.c_int32),
         ("sample_offset", C.c_uint32),
-        ("reserved", C.c_int32 * 2),
+        ("flags", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -122,7 +126,13 @@ class fl_render_stats(C.Structure):
         ("bounces", C.c_uint64),
         ("ms", C.c_double),
         ("traversal_errors", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("launches", C.c_uint32),
+        ("ms_trace", C.c_double),
+        ("ms_shade", C.c_double),
+        ("ms_shadow", C.c_double),
+        ("ms_continue", C.c_double),
+        ("nodes_visited", C.c_uint64),
+        ("tris_tested", C.c_uint64),
     ]
 
 

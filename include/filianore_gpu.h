@@ -209,6 +209,11 @@ enum {
     FL_SPECTRAL_BINS60 = 1  /* the reference's 60 fixed bins over 400..700 nm (principalspectrum.h:7-9) */
 };
 
+enum {
+    FL_RENDER_PROFILE = 1,  /* time each kernel class with CUDA events (fl_render_stats.ms_*) */
+    FL_RENDER_COUNT = 2     /* count BVH nodes and triangles visited (instrumented traversal) */
+};
+
 typedef struct {
     int32_t spp;            /* samples per pixel */
     int32_t max_depth;      /* RenderParams diffuse = reflection = transmission depth (core/renderparams.h:5-10) */
@@ -216,17 +221,26 @@ typedef struct {
     int32_t spectral_mode;  /* FL_SPECTRAL_* */
     int32_t wave_paths;     /* paths in flight per wavefront (0 = library default) */
     uint32_t sample_offset; /* first sample index (progressive / multi-GPU sample split) */
-    int32_t reserved[2];
+    int32_t flags;          /* FL_RENDER_* */
+    int32_t reserved;
 } fl_render_params;
 
 typedef struct {
     uint64_t paths;          /* camera samples completed */
     uint64_t rays;           /* all rays traced: camera + continuation + shadow + MIS */
-    uint64_t shadow_rays;
+    uint64_t shadow_rays;    /* shadow + MIS rays */
     uint64_t bounces;        /* path vertices shaded */
     double ms;               /* device time of the render (CUDA events) */
     uint32_t traversal_errors;
-    uint32_t reserved;
+    uint32_t launches;       /* kernels launched by this call */
+    /* FL_RENDER_PROFILE: summed device time per kernel class */
+    double ms_trace;         /* camera / continuation rays */
+    double ms_shade;
+    double ms_shadow;        /* shadow + MIS rays */
+    double ms_continue;
+    /* FL_RENDER_COUNT: traversal work of all rays */
+    uint64_t nodes_visited;
+    uint64_t tris_tested;
 } fl_render_stats;
 
 /* Renders the image: for pixel p and sample s the PCG32 stream is seeded with
