@@ -30,6 +30,7 @@ namespace fl {
 
 struct WaveCounters {
     uint32_t n_trace, n_cont, n_next, n_shadow;
+    uint32_t fetch_trace, fetch_rays2, pad0, pad1;  // persistent-kernel work counters
     unsigned long long rays, shadow_rays, bounces, paths;
     unsigned long long nodes, tris;  // FL_RENDER_COUNT
     int err;
@@ -115,6 +116,19 @@ struct RenderArgs {
 };
 
 enum : uint32_t { kHasCL = 1u, kHasCS = 2u, kVisOK = 4u, kMisOK = 8u };
+
+// queue append from divergent code: one atomic per group of converged lanes
+__device__ inline uint32_t coalesced_append(uint32_t *counter, bool pred) {
+    const uint32_t active = __activemask();
+    const uint32_t mask = __ballot_sync(active, pred);
+    if (!pred) return 0;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
 
 // warp-aggregated queue append: returns this lane's position (valid when pred)
 __device__ inline uint32_t warp_append(uint32_t *counter, bool pred) {
@@ -206,30 +220,6 @@ __device__ inline void make_bsdf(const RenderArgs &A, const SmemTables &sm, cons
     else b.R.set(1.f);
 }
 
-// closest hit over triangles and analytic sphere lights
-template <bool COUNT>
-__device__ inline TraceResult closest_with_spheres(const RenderArgs &A, const RayPre &r, bool &err, TraceStats &st) {
-    TraceResult res;
-    if (A.n_nodes) res = traverse<false, COUNT>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
-    else { res.id = -1; res.t = r.tmax; res.u = res.v = 0.f; }
-    if (A.has_spheres) {
-        const v3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
-        float best = res.id >= 0 ? res.t : r.tmax;
-        for (int l = 0; l < A.n_lights; ++l) {
-            const LightDev L = A.lights[l];
-            if (L.type != FL_LIGHT_SPHERE) continue;
-            const float ts = sphere_hit(L, o, d, r.tmin, best);
-            if (ts > 0.f && ts < best) {
-                best = ts;
-                res.id = -2 - l;
-                res.t = ts;
-                res.u = res.v = 0.f;
-            }
-        }
-    }
-    return res;
-}
-
 // ------------------------------------------------------------------------------ kernels
 
 template <int NL>
@@ -237,6 +227,7 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A, uint32_t n_wave) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.cnt->n_trace = n_wave;
         A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = 0;
+        A.cnt->fetch_trace = A.cnt->fetch_rays2 = 0;
     }
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_wave; k += gridDim.x * blockDim.x) {
         const unsigned long long g = A.wave_base + k;
@@ -281,22 +272,61 @@ static __global__ void __launch_bounds__(128) k_advance(WaveCounters *cnt) {
     cnt->n_next = 0;
     cnt->n_cont = 0;
     cnt->n_shadow = 0;
+    cnt->fetch_trace = 0;
+    cnt->fetch_rays2 = 0;
 }
 
+// analytic sphere lights after the triangle traversal: closest of both
+__device__ inline void add_spheres(const RenderArgs &A, const RayPre &r, TraceResult &res) {
+    if (!A.has_spheres) return;
+    const v3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
+    float best = res.id >= 0 ? res.t : r.tmax;
+    for (int l = 0; l < A.n_lights; ++l) {
+        const LightDev L = A.lights[l];
+        if (L.type != FL_LIGHT_SPHERE) continue;
+        const float ts = sphere_hit(L, o, d, r.tmin, best);
+        if (ts > 0.f && ts < best) {
+            best = ts;
+            res.id = -2 - l;
+            res.t = ts;
+            res.u = res.v = 0.f;
+        }
+    }
+}
+
+constexpr int kRenderTraceSteps = 8;
+
+struct PathTraceItem {
+    const RenderArgs *A;
+    uint32_t slot;
+    bool any_hit;
+    RayPre ray;
+    TravState st;
+    __device__ bool begin(uint32_t q) {
+        slot = A->q_trace[q];
+        ray = ray_precompute(A->ray_o[slot], A->ray_d[slot]);
+        trav_init(st, ray);
+        return true;
+    }
+    __device__ void finish() {
+        TraceResult res = st.res;
+        add_spheres(*A, ray, res);
+        A->hit[slot] = make_int4(res.id, __float_as_int(res.t), __float_as_int(res.u), __float_as_int(res.v));
+    }
+};
+
+// camera and continuation rays: closest hit (persistent, lanes refilled as rays finish)
 template <bool COUNT>
 __global__ void __launch_bounds__(128) k_trace_paths(RenderArgs A) {
     const uint32_t n = load_count(&A.cnt->n_trace);
-    uint32_t local = 0;
     bool err = false;
     TraceStats st;
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const uint32_t slot = A.q_trace[q];
-        const RayPre r = ray_precompute(A.ray_o[slot], A.ray_d[slot]);
-        const TraceResult res = closest_with_spheres<COUNT>(A, r, err, st);
-        A.hit[slot] = make_int4(res.id, __float_as_int(res.t), __float_as_int(res.u), __float_as_int(res.v));
-        ++local;
-    }
-    warp_count(&A.cnt->rays, local);
+    PathTraceItem it;
+    it.A = &A;
+    it.any_hit = false;
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, A.nodes, A.n_nodes, A.tris, A.n_tri, err,
+                                               st);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->rays, (unsigned long long)n);
     if (COUNT) {
         warp_count(&A.cnt->nodes, st.nodes);
         warp_count(&A.cnt->tris, st.tris);
@@ -394,7 +424,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                                     so = make_float4(oo.x, oo.y, oo.z, kShadowEpsilon);
                                     sd = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
                                 }
-                                const uint32_t pos = atomicAdd(&A.cnt->n_shadow, 1u);
+                                const uint32_t pos = coalesced_append(&A.cnt->n_shadow, true);
                                 if (pos < A.scap) {
                                     A.sray_o[pos] = so;
                                     A.sray_d[pos] = sd;
@@ -428,7 +458,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                                         CS.c[c] = f.c[c] * Lrad * 1.f * weight / scatteringPdf;
                                     pf |= kHasCS;
                                     const v3 oo = spawn_origin(hr.p, hr.n, wi);
-                                    const uint32_t pos = atomicAdd(&A.cnt->n_shadow, 1u);
+                                    const uint32_t pos = coalesced_append(&A.cnt->n_shadow, true);
                                     if (pos < A.scap) {
                                         A.sray_o[pos] = make_float4(oo.x, oo.y, oo.z, kShadowEpsilon);
                                         A.sray_d[pos] = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
@@ -453,44 +483,60 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
     warp_count(&A.cnt->bounces, shaded);
 }
 
-// shadow rays (kind 0) and MIS rays (kind 1)
-template <bool COUNT>
-__global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
-    const uint32_t n = min(load_count(&A.cnt->n_shadow), A.scap);
-    uint32_t local = 0;
-    bool err = false;
-    TraceStats st;
-    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const uint32_t tag = A.stag[q];
-        const uint32_t kind = tag & 1u;
-        const uint32_t sl = tag >> 1;  // li * cap + slot
-        const uint32_t li = sl / A.cap;
-        const RayPre r = ray_precompute(A.sray_o[q], A.sray_d[q]);
+struct NeeRayItem {
+    const RenderArgs *A;
+    uint32_t q, kind, sl;
+    bool any_hit;
+    RayPre ray;
+    TravState st;
+    __device__ bool begin(uint32_t qq) {
+        q = qq;
+        const uint32_t tag = A->stag[q];
+        kind = tag & 1u;
+        sl = tag >> 1;  // li * cap + slot
+        ray = ray_precompute(A->sray_o[q], A->sray_d[q]);
+        any_hit = kind == 0 && A->any_hit_ok;
+        trav_init(st, ray);
+        return true;
+    }
+    __device__ void finish() {
+        const uint32_t li = sl / A->cap;
+        TraceResult res = st.res;
         uint32_t bit = 0;
         if (kind == 0) {
-            TraceResult res;
-            if (A.n_nodes == 0) res.id = -1;
-            else if (A.any_hit_ok) res = traverse<true, COUNT>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
-            else res = traverse<false, COUNT>(A.nodes, A.n_nodes, A.tris, A.n_tri, r, err, st);
-            const bool unocc = res.id < 0 || A.tri_light[res.id] >= 0;
+            // VisibilityEvaluator::unoccluded: no hit, or the closest hit is emissive
+            const bool unocc = res.id < 0 || A->tri_light[res.id] >= 0;
             bit = unocc ? kVisOK : 0u;
         } else {
-            const TraceResult res = closest_with_spheres<COUNT>(A, r, err, st);
-            const LightDev Ll = A.lights[li];
+            add_spheres(*A, ray, res);
+            const LightDev Ll = A->lights[li];
             bool ok = false;
             if (res.id == -1) ok = Ll.type == FL_LIGHT_ENV;
-            else if (prim_light(A, res.id) == (int)li) {
+            else if (prim_light(*A, res.id) == (int)li) {
                 const int4 h = make_int4(res.id, __float_as_int(res.t), 0, 0);
-                const Hit hr = make_hit(A, A.sray_o[q], A.sray_d[q], h);
-                ok = dot(hr.n, mk(-r.dx, -r.dy, -r.dz)) > 0.f;
+                const Hit hr = make_hit(*A, A->sray_o[q], A->sray_d[q], h);
+                ok = dot(hr.n, mk(-ray.dx, -ray.dy, -ray.dz)) > 0.f;
             }
             bit = ok ? kMisOK : 0u;
         }
-        if (bit) atomicOr(&A.pflags[sl], bit);
-        ++local;
+        if (bit) atomicOr(&A->pflags[sl], bit);
     }
-    warp_count(&A.cnt->shadow_rays, local);
-    warp_count(&A.cnt->rays, local);
+};
+
+// shadow rays (kind 0) and MIS rays (kind 1), persistent
+template <bool COUNT>
+__global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
+    const uint32_t n = min(load_count(&A.cnt->n_shadow), A.scap);
+    bool err = false;
+    TraceStats st;
+    NeeRayItem it;
+    it.A = &A;
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, A.nodes, A.n_nodes, A.tris, A.n_tri, err,
+                                               st);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&A.cnt->shadow_rays, (unsigned long long)n);
+        atomicAdd(&A.cnt->rays, (unsigned long long)n);
+    }
     if (COUNT) {
         warp_count(&A.cnt->nodes, st.nodes);
         warp_count(&A.cnt->tris, st.tris);

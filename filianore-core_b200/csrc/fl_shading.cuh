@@ -167,6 +167,9 @@ __device__ inline void spectrum_xyz(const SmemTables &sm, const TablesArg &t, fl
 }
 
 // ---------------------------------------------------------------------------- BSDF
+// The BSDF and light routines below are called from several places of the shading
+// kernels; they are kept out of line (__noinline__) so that each kernel holds one copy:
+// fully inlined, the shading kernel overflowed the instruction cache.
 template <int NL>
 struct Bsdf {
     v3 ng, ns, s, t;
@@ -438,7 +441,7 @@ __device__ inline int bsdf_num_components(const Bsdf<NL> &b, int flags) {
 }
 
 template <int NL>
-__device__ inline void bsdf_eval(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags, Spec<NL> &out) {
+__device__ __noinline__ void bsdf_eval(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags, Spec<NL> &out) {
     const v3 wi = to_local(b.s, b.t, b.ns, wiW), wo = to_local(b.s, b.t, b.ns, woW);
     out.set(0.f);
     if (wo.z == 0) return;
@@ -457,7 +460,7 @@ __device__ inline void bsdf_eval(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags, S
 }
 
 template <int NL>
-__device__ inline float bsdf_pdf(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags) {
+__device__ __noinline__ float bsdf_pdf(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags) {
     int lobes[2];
     const int n = mat_lobes(b.type, lobes);
     const v3 wi = to_local(b.s, b.t, b.ns, wiW), wo = to_local(b.s, b.t, b.ns, woW);
@@ -470,7 +473,7 @@ __device__ inline float bsdf_pdf(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags) {
 }
 
 template <int NL>
-__device__ inline void bsdf_sample(const Bsdf<NL> &b, v3 woW, v3 &wiW, float ux, float uy, float &pdf, int flags,
+__device__ __noinline__ void bsdf_sample(const Bsdf<NL> &b, v3 woW, v3 &wiW, float ux, float uy, float &pdf, int flags,
                                    int &sampledType, Spec<NL> &f) {
     int lobes[2];
     const int n = mat_lobes(b.type, lobes);
@@ -576,7 +579,7 @@ struct LightSample {
 };
 
 // Illuminant::sample_li for the three light types
-__device__ inline LightSample light_sample_li(const LightDev &L, const float *__restrict__ soup, const Hit &ref,
+static __device__ __noinline__ LightSample light_sample_li(const LightDev &L, const float *__restrict__ soup, const Hit &ref,
                                               float ux, float uy) {
     LightSample ls;
     ls.pdf = 0.f;
@@ -640,7 +643,7 @@ __device__ inline LightSample light_sample_li(const LightDev &L, const float *__
 }
 
 // Illuminant::pdf_li
-__device__ inline float light_pdf_li(const LightDev &L, const float *__restrict__ soup, const Hit &ref, v3 wi) {
+static __device__ __noinline__ float light_pdf_li(const LightDev &L, const float *__restrict__ soup, const Hit &ref, v3 wi) {
     if (L.type == FL_LIGHT_TRIANGLE) {
         const v3 o = spawn_origin(ref.p, ref.n, wi);
         v3 p, n;

@@ -17,6 +17,42 @@ __device__ inline void warp_add_u64(unsigned long long *dst, uint32_t v) {
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
 }
 
+constexpr int kTraceSteps = 8;
+
+template <int KIND>
+struct TraceItem {
+    const float4 *org, *dir;
+    int4 *hits;
+    uint8_t *occ;
+    const int32_t *tri_light;
+    uint32_t n_tris;
+    bool any_hit;
+    uint32_t q;
+    RayPre ray;
+    TravState st;
+    __device__ bool begin(uint32_t qq) {
+        q = qq;
+        ray = ray_precompute(__ldg(org + q), __ldg(dir + q));
+        trav_init(st, ray);
+        return true;
+    }
+    __device__ void finish() {
+        const TraceResult &res = st.res;
+        if (KIND == kTraceOccluded) {
+            // occluded unless nothing is hit or the closest hit carries an area light
+            occ[q] = (res.id >= 0 && (any_hit || (uint32_t)res.id >= n_tris || tri_light[res.id] < 0)) ? 1 : 0;
+        } else if (KIND == kTraceClosest) {
+            int4 h;
+            h.x = res.id;
+            h.y = __float_as_int(res.t);
+            h.z = __float_as_int(res.id >= 0 ? res.u : 0.f);
+            h.w = __float_as_int(res.id >= 0 ? res.v : 0.f);
+            hits[q] = h;
+        }
+    }
+};
+
+// persistent kernel: warps refill finished lanes with new rays (fl_traverse.cuh)
 template <int KIND>
 __global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restrict__ nodes, uint32_t n_nodes,
                                                        const float4 *__restrict__ tris, uint32_t n_tris,
@@ -24,43 +60,23 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restric
                                                        const float4 *__restrict__ org, const float4 *__restrict__ dir,
                                                        uint32_t n, int4 *__restrict__ hits, uint8_t *__restrict__ occ,
                                                        int *__restrict__ err, unsigned long long *__restrict__ counters) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = i < n;
+    TraceItem<KIND> it;
+    it.org = org;
+    it.dir = dir;
+    it.hits = hits;
+    it.occ = occ;
+    it.tri_light = tri_light;
+    it.n_tris = n_tris;
+    it.any_hit = KIND == kTraceOccluded && any_hit_ok;
     TraceStats st;
     bool error = false;
-    TraceResult res;
-    res.id = -1;
-    res.t = 0.f; res.u = 0.f; res.v = 0.f;
-    if (active) {
-        const float4 o = __ldg(org + i);
-        const float4 d = __ldg(dir + i);
-        const RayPre r = ray_precompute(o, d);
-        res.t = r.tmax;
-        if (n_nodes > 0) {
-            if (KIND == kTraceOccluded && any_hit_ok)
-                res = traverse<true, false>(nodes, n_nodes, tris, n_tris, r, error, st);
-            else if (KIND == kTraceCount)
-                res = traverse<false, true>(nodes, n_nodes, tris, n_tris, r, error, st);
-            else
-                res = traverse<false, false>(nodes, n_nodes, tris, n_tris, r, error, st);
-        }
-        if (KIND == kTraceOccluded) {
-            // occluded unless nothing is hit or the closest hit carries an area light
-            occ[i] = (res.id >= 0 && (any_hit_ok || (uint32_t)res.id >= n_tris || tri_light[res.id] < 0)) ? 1 : 0;
-        } else if (KIND == kTraceClosest) {
-            int4 h;
-            h.x = res.id;
-            h.y = __float_as_int(res.t);
-            h.z = __float_as_int(res.id >= 0 ? res.u : 0.f);
-            h.w = __float_as_int(res.id >= 0 ? res.v : 0.f);
-            hits[i] = h;
-        }
-        if (error) atomicAdd(err, 1);
-    }
+    uint32_t *fetch = reinterpret_cast<uint32_t *>(counters + 4);
+    persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, nodes, n_nodes, tris, n_tris, error, st);
     if (KIND == kTraceCount) {
         warp_add_u64(&counters[0], st.nodes);
         warp_add_u64(&counters[1], st.tris);
     }
+    if (error) atomicAdd(err, 1);
 }
 
 }  // namespace
@@ -68,7 +84,9 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restric
 fl_status launch_trace(Scene *s, const float4 *org, const float4 *dir, uint32_t n, fl_hit *hits, uint8_t *occluded,
                        int kind, cudaStream_t stream) {
     if (n == 0) return FL_OK;
-    const uint32_t grid = (n + kTraceBlock - 1) / kTraceBlock;
+    // persistent grid: up to 16 blocks of 128 threads per SM, never more than the rays need
+    const uint32_t grid = std::min<uint32_t>((n + kTraceBlock - 1) / kTraceBlock, (uint32_t)s->ctx->sm_count * 16u);
+    FL_CUDA_TRY(s->ctx, cudaMemsetAsync(s->ctx->d_counters + 4, 0, sizeof(unsigned long long), stream));
     const int any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
     int4 *h = reinterpret_cast<int4 *>(hits);
     switch (kind) {
