@@ -28,9 +28,12 @@
 
 namespace fl {
 
+constexpr int kShadeClasses = 5;  // 0: miss, 1 + material type (Lambert, conductor, rough / smooth dielectric)
+
 struct WaveCounters {
     uint32_t n_trace, n_cont, n_next, n_shadow;
     uint32_t fetch_trace, fetch_rays2, pad0, pad1;  // persistent-kernel work counters
+    uint32_t n_class[8];                            // shading queues by class
     unsigned long long rays, shadow_rays, bounces, paths;
     unsigned long long nodes, tris;  // FL_RENDER_COUNT
     int err;
@@ -111,6 +114,7 @@ struct RenderArgs {
     uint32_t scap;
     // queues
     uint32_t *q_trace, *q_cont, *q_next;
+    uint32_t *q_class;  // kShadeClasses x cap: traced paths grouped by what shades them
     WaveCounters *cnt;
     double *film;
 };
@@ -128,6 +132,18 @@ __device__ inline uint32_t coalesced_append(uint32_t *counter, bool pred) {
     if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
     base = __shfl_sync(mask, base, leader);
     return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// append to one of several queues from divergent code: lanes with the same class share an atomic
+__device__ inline uint32_t coalesced_append_class(uint32_t *counters, int cls) {
+    const uint32_t active = __activemask();
+    const uint32_t same = __match_any_sync(active, cls);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(same) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&counters[cls], (uint32_t)__popc(same));
+    base = __shfl_sync(same, base, leader);
+    return base + __popc(same & ((1u << lane) - 1u));
 }
 
 // warp-aggregated queue append: returns this lane's position (valid when pred)
@@ -228,6 +244,7 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A, uint32_t n_wave) {
         A.cnt->n_trace = n_wave;
         A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = 0;
         A.cnt->fetch_trace = A.cnt->fetch_rays2 = 0;
+        for (int c = 0; c < kShadeClasses; ++c) A.cnt->n_class[c] = 0;
     }
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_wave; k += gridDim.x * blockDim.x) {
         const unsigned long long g = A.wave_base + k;
@@ -274,6 +291,7 @@ static __global__ void __launch_bounds__(128) k_advance(WaveCounters *cnt) {
     cnt->n_shadow = 0;
     cnt->fetch_trace = 0;
     cnt->fetch_rays2 = 0;
+    for (int c = 0; c < kShadeClasses; ++c) cnt->n_class[c] = 0;
 }
 
 // analytic sphere lights after the triangle traversal: closest of both
@@ -312,6 +330,14 @@ struct PathTraceItem {
         TraceResult res = st.res;
         add_spheres(*A, ray, res);
         A->hit[slot] = make_int4(res.id, __float_as_int(res.t), __float_as_int(res.u), __float_as_int(res.v));
+        // group by shading work so that warps of k_shade / k_continue run one material's code
+        int cls = 0;
+        if (res.id != -1) {
+            const uint32_t mi = res.id >= 0 ? A->tri_material[res.id] : 0u;
+            cls = 1 + A->materials[mi].type;
+        }
+        const uint32_t pos = coalesced_append_class(A->cnt->n_class, cls);
+        A->q_class[(size_t)cls * A->cap + pos] = slot;
     }
 };
 
@@ -338,15 +364,19 @@ template <int NL>
 __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
     __shared__ SmemTables sm;
     stage_tables(sm, A.tab, NL != 60);
-    const uint32_t n = load_count(&A.cnt->n_trace);
+    uint32_t off[kShadeClasses + 1];
+    off[0] = 0;
+    for (int c = 0; c < kShadeClasses; ++c) off[c + 1] = off[c] + load_count(&A.cnt->n_class[c]);
+    const uint32_t n = off[kShadeClasses];
     uint32_t shaded = 0;
     FL_WARP_UNIFORM_LOOP(q, n) {
         const bool active = q < n;
         bool alive = false;
         uint32_t slot = 0;
-        // NEE rays of this thread, emitted after the shading work (up to 2 per light)
         if (active) {
-            slot = A.q_trace[q];
+            int c = 0;
+            while (q >= off[c + 1]) ++c;
+            slot = A.q_class[(size_t)c * A.cap + (q - off[c])];
             const int4 h = A.hit[slot];
             const uint32_t fl = A.flags[slot];
             const uint32_t bounce = fl & 0xffu;
@@ -675,7 +705,8 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     const int nl = (int)s->n_lights;
     const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
     const unsigned long long total = n_pix * (unsigned long long)p.spp;
-    const size_t per_slot = 92 + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
+    const size_t per_slot = 92 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl +
+                            72 * (size_t)nl;
     const size_t budget = (size_t)3 << 30;
     size_t cap = p.wave_paths > 0 ? (size_t)p.wave_paths : (NL == 60 ? (size_t)1 << 19 : (size_t)1 << 21);
     cap = std::min(cap, budget / per_slot);
@@ -696,6 +727,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     const size_t o_pf = take(4 * (size_t)nl * cap);
     const size_t o_so = take(16 * scap), o_sd = take(16 * scap), o_st = take(4 * scap);
     const size_t o_qa = take(4 * cap), o_qb = take(4 * cap), o_qc = take(4 * cap);
+    const size_t o_qk = take(4 * cap * kShadeClasses);
     void *base = nullptr;
     fl_status rc = ensure_scratch(ctx, off, &base);
     if (rc) return rc;
@@ -750,6 +782,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     A.film = d_film;
     uint32_t *qa = reinterpret_cast<uint32_t *>(B + o_qa), *qb = reinterpret_cast<uint32_t *>(B + o_qb);
     A.q_cont = reinterpret_cast<uint32_t *>(B + o_qc);
+    A.q_class = reinterpret_cast<uint32_t *>(B + o_qk);
     FL_CUDA_TRY(ctx, cudaMemsetAsync(A.cnt, 0, sizeof(WaveCounters), st));
 
     const bool count = (p.flags & FL_RENDER_COUNT) != 0;

@@ -15,7 +15,7 @@ from . import types as T
 from .types import *  # noqa: F401,F403
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "lib", "libfilianore_b200.so")
+LIB_PATH = os.environ.get("FILIANORE_B200_LIB", os.path.join(PKG_DIR, "lib", "libfilianore_b200.so"))
 ROOT = os.path.dirname(PKG_DIR)
 TABLES_PATH = os.path.join(ROOT, "tests", "golden", "spectral_tables.npz")
 
