@@ -6,13 +6,13 @@
 
 namespace fl {
 extern template fl_status render_waves<4>(Scene *, const CamDev &, const fl_render_params &, double *, WaveCounters *,
-                                          RenderProfile *, cudaStream_t);
+                                          RenderProfile *, cudaStream_t, void *, size_t);
 extern template fl_status render_waves<60>(Scene *, const CamDev &, const fl_render_params &, double *,
-                                           WaveCounters *, RenderProfile *, cudaStream_t);
+                                           WaveCounters *, RenderProfile *, cudaStream_t, void *, size_t);
 
 // PhysicalCamera::PhysicalCamera (cameras/physical.h:11-43) with aperture 0 and
 // flipCameraDirection = true (the orientation that faces look_at).
-static CamDev camera_basis(const fl_camera &c) {
+CamDev camera_basis_of(const fl_camera &c) {
     const v3 pos = mk(c.position[0], c.position[1], c.position[2]);
     const v3 at = mk(c.look_at[0], c.look_at[1], c.look_at[2]);
     const v3 up = mk(c.up[0], c.up[1], c.up[2]);
@@ -66,7 +66,7 @@ extern "C" fl_status fl_render(fl_scene *scene_h, const fl_camera *camera, const
     }
     FL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
-    const CamDev cam = camera_basis(*camera);
+    const CamDev cam = camera_basis_of(*camera);
     const size_t n_pix = (size_t)camera->width * camera->height;
     // film scratch: FP64 XYZ sums (unless the caller's device buffer is used) + FP32 RGB staging
     const bool own_xyz = !(film_xyz64 && memory == FL_MEM_DEVICE);

@@ -700,14 +700,15 @@ inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 // per spectral mode in its own translation unit (the 60-bin one without FMA contraction).
 template <int NL>
 fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film,
-                       WaveCounters *h_cnt, RenderProfile *prof, cudaStream_t st) {
+                       WaveCounters *h_cnt, RenderProfile *prof, cudaStream_t st, void *fixed_scratch = nullptr,
+                       size_t fixed_bytes = 0) {
     Context *ctx = s->ctx;
     const int nl = (int)s->n_lights;
     const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
     const unsigned long long total = n_pix * (unsigned long long)p.spp;
     const size_t per_slot = 92 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl +
                             72 * (size_t)nl;
-    const size_t budget = (size_t)3 << 30;
+    const size_t budget = fixed_scratch ? fixed_bytes : (size_t)3 << 30;
     size_t cap = p.wave_paths > 0 ? (size_t)p.wave_paths : (NL == 60 ? (size_t)1 << 19 : (size_t)1 << 21);
     cap = std::min(cap, budget / per_slot);
     cap = std::min<size_t>(cap, (size_t)total);
@@ -728,9 +729,14 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     const size_t o_so = take(16 * scap), o_sd = take(16 * scap), o_st = take(4 * scap);
     const size_t o_qa = take(4 * cap), o_qb = take(4 * cap), o_qc = take(4 * cap);
     const size_t o_qk = take(4 * cap * kShadeClasses);
-    void *base = nullptr;
-    fl_status rc = ensure_scratch(ctx, off, &base);
-    if (rc) return rc;
+    void *base = fixed_scratch;
+    if (!fixed_scratch) {
+        fl_status rc = ensure_scratch(ctx, off, &base);
+        if (rc) return rc;
+    } else if (off > fixed_bytes) {
+        set_error(ctx, "render state does not fit the fixed scratch buffer");
+        return FL_ERR_CAPACITY;
+    }
     char *B = static_cast<char *>(base);
 
     RenderArgs A{};

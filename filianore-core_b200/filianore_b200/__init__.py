@@ -22,7 +22,7 @@ TABLES_PATH = os.path.join(ROOT, "tests", "golden", "spectral_tables.npz")
 EXPORTED = [
     "fl_context_create", "fl_context_destroy", "fl_status_string", "fl_last_error", "fl_context_binned_tables",
     "fl_scene_create", "fl_scene_destroy", "fl_scene_get_info", "fl_trace_closest", "fl_trace_occluded",
-    "fl_trace_count", "fl_render",
+    "fl_trace_count", "fl_render", "fl_render_noalloc",
 ]
 
 _lib = None
@@ -61,6 +61,7 @@ def lib():
         L.fl_trace_occluded.argtypes = [vp, vp, vp, C.c_uint32, vp, C.c_int32, vp]
         L.fl_trace_count.argtypes = [vp, vp, vp, C.c_uint32, C.c_int32, P(C.c_uint64), P(C.c_uint64)]
         L.fl_render.argtypes = [vp, P(T.fl_camera), P(T.fl_render_params), vp, vp, C.c_int32, P(T.fl_render_stats)]
+        L.fl_render_noalloc.argtypes = [vp, P(T.fl_camera), P(T.fl_render_params), vp, vp, P(T.fl_render_stats)]
         for name in EXPORTED:
             if name not in ("fl_status_string",):
                 getattr(L, name).restype = C.c_int32

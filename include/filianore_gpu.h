@@ -251,6 +251,21 @@ typedef struct {
 FL_API fl_status fl_render(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
                     float *film_rgb, double *film_xyz64, int32_t memory, fl_render_stats *stats);
 
+/* fl_render_noalloc: fl_render for callers that cannot allocate device memory while they
+ * render (an application that owns and budgets all device memory, or code that must not
+ * trigger the implicit device synchronisation of cudaMalloc). It has no counterpart in the
+ * reference. It allocates nothing: no cudaMalloc/cudaFree, no events, no allocating library
+ * call. The path state lives in a fixed 32 MiB device array inside the library (held by
+ * every GPU that loads the library until exit); frames are rendered in waves that fit it,
+ * and a scene whose per-path state cannot fit even a minimal wave is rejected with
+ * FL_ERR_CAPACITY. film_rgb (width*height*3 floats) and film_xyz64 (width*height*3 doubles,
+ * the FP64 XYZ sums, cleared by the call) are caller-owned DEVICE buffers. All calls share
+ * the fixed array: calls whose GPU work overlaps race and give wrong images. The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress); make it before
+ * any stream capture. stats->ms is host wall time of the call. */
+FL_API fl_status fl_render_noalloc(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
+                                   float *film_rgb, double *film_xyz64, fl_render_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif
