@@ -20,6 +20,7 @@
 // host synchronisation. Finished paths add to_xyz(L) to an FP64 film with atomics.
 #pragma once
 
+#include <cstddef>
 #include <vector>
 
 #include "fl_internal.h"
@@ -29,6 +30,8 @@
 namespace fl {
 
 constexpr int kShadeClasses = 5;  // 0: miss, 1 + material type (Lambert, conductor, rough / smooth dielectric)
+constexpr int kMaxJobs = 64;      // jobs that can share one wave (serving)
+constexpr int kMaxSegs = 128;     // sample ranges per wave
 
 struct WaveCounters {
     uint32_t n_trace, n_cont, n_next, n_shadow;
@@ -73,8 +76,9 @@ struct CamDev {
     int W, H;
 };
 
-struct RenderArgs {
-    // scene
+// Everything one render job needs: its scene, camera, parameters and film. A wave's paths
+// may belong to different jobs (serving); every kernel looks its path's job up.
+struct JobDev {
     const WideNode *nodes;
     uint32_t n_nodes;
     const float4 *tris;
@@ -88,18 +92,37 @@ struct RenderArgs {
     int n_lights;
     int any_hit_ok;
     int has_env;
-    float env_radiance;
     int has_spheres;
-    TablesArg tab;
+    float env_radiance;
     CamDev cam;
-    // parameters
     int spp, max_depth;
     float rr_threshold;
     uint32_t sample_offset;
-    unsigned long long wave_base, total;
-    uint32_t n_pix, cap;
+    uint32_t n_pix;
+    double *film;  // FP64 XYZ sums, 3 per pixel
+};
+
+// A wave is a list of sample ranges: slots [slot_begin, slot_begin + count) render the
+// job's samples [sample_base, sample_base + count) in pixel-major order
+// (sample index = g / n_pix, pixel = g % n_pix).
+struct WaveSeg {
+    uint32_t job, slot_begin, count, pad;
+    unsigned long long sample_base, pad2;
+};
+struct WaveDesc {
+    uint32_t n_wave, n_seg, pad[2];
+    WaveSeg seg[kMaxSegs];
+};
+
+struct RenderArgs {
+    TablesArg tab;
+    const JobDev *jobs;      // device, kMaxJobs entries
+    const WaveDesc *wave;    // device
+    int nl;                  // pending-term slots per path: the most lights of any job
+    uint32_t cap;            // paths per wave
     // path state (slot-indexed, component-major for spectra: x[k * cap + slot])
     uint32_t *pixel;
+    uint16_t *job;
     unsigned long long *rng;
     float *beta, *L, *lambda0, *eta_scale;
     uint32_t *flags;  // bits 0..7 bounce, bit 8 specular
@@ -116,7 +139,6 @@ struct RenderArgs {
     uint32_t *q_trace, *q_cont, *q_next;
     uint32_t *q_class;  // kShadeClasses x cap: traced paths grouped by what shades them
     WaveCounters *cnt;
-    double *film;
 };
 
 enum : uint32_t { kHasCL = 1u, kHasCS = 2u, kVisOK = 4u, kMisOK = 8u };
@@ -184,17 +206,18 @@ __device__ inline void store_spec(float *a, uint32_t cap, uint32_t slot, const S
 }
 
 template <int NL>
-__device__ inline void finish_path(const RenderArgs &A, const SmemTables &sm, uint32_t slot, const Spec<NL> &L) {
+__device__ inline void finish_path(const RenderArgs &A, const JobDev &J, const SmemTables &sm, uint32_t slot,
+                                   const Spec<NL> &L) {
     double xyz[3];
     spectrum_xyz<NL>(sm, A.tab, A.lambda0[slot], L, xyz);
     const uint32_t pix = A.pixel[slot];
-    atomicAdd(&A.film[3 * (size_t)pix + 0], xyz[0]);
-    atomicAdd(&A.film[3 * (size_t)pix + 1], xyz[1]);
-    atomicAdd(&A.film[3 * (size_t)pix + 2], xyz[2]);
+    atomicAdd(&J.film[3 * (size_t)pix + 0], xyz[0]);
+    atomicAdd(&J.film[3 * (size_t)pix + 1], xyz[1]);
+    atomicAdd(&J.film[3 * (size_t)pix + 2], xyz[2]);
 }
 
 // the hit record of BVH::intersect (bvh.cpp:49-84): p = o + d t, n = normalize(Ng), wo = normalize(-d)
-__device__ inline Hit make_hit(const RenderArgs &A, float4 o4, float4 d4, int4 h) {
+__device__ inline Hit make_hit(const JobDev &A, float4 o4, float4 d4, int4 h) {
     Hit r;
     const v3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
     const float t = __int_as_float(h.y);
@@ -212,14 +235,15 @@ __device__ inline Hit make_hit(const RenderArgs &A, float4 o4, float4 d4, int4 h
     return r;
 }
 
-__device__ inline int prim_light(const RenderArgs &A, int prim) {
+__device__ inline int prim_light(const JobDev &A, int prim) {
     if (prim >= 0) return A.tri_light[prim];
     if (prim <= -2) return -2 - prim;
     return -1;
 }
 
 template <int NL>
-__device__ inline void make_bsdf(const RenderArgs &A, const SmemTables &sm, const Hit &h, float lambda0, Bsdf<NL> &b) {
+__device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const SmemTables &sm, const Hit &h,
+                                 float lambda0, Bsdf<NL> &b) {
     b.ng = h.n;
     b.ns = h.n;
     coordinate_system(b.ns, &b.s, &b.t);
@@ -232,14 +256,16 @@ __device__ inline void make_bsdf(const RenderArgs &A, const SmemTables &sm, cons
     b.ax = m.ax;
     b.ay = m.ay;
     b.eta = (m.type == FL_MAT_ROUGH_DIELECTRIC || m.type == FL_MAT_SMOOTH_DIELECTRIC) ? m.eta : 1.f;
-    if (m.type == FL_MAT_LAMBERT) reflectance<NL>(sm, A.tab, m, A.mat_refl60 + 60 * (size_t)mi, lambda0, b.R);
+    if (m.type == FL_MAT_LAMBERT) reflectance<NL>(sm, tab, m, A.mat_refl60 + 60 * (size_t)mi, lambda0, b.R);
     else b.R.set(1.f);
 }
 
 // ------------------------------------------------------------------------------ kernels
 
 template <int NL>
-__global__ void __launch_bounds__(128) k_raygen(RenderArgs A, uint32_t n_wave) {
+__global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
+    const uint32_t n_wave = A.wave->n_wave;
+    const uint32_t n_seg = A.wave->n_seg;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.cnt->n_trace = n_wave;
         A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = 0;
@@ -247,27 +273,32 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A, uint32_t n_wave) {
         for (int c = 0; c < kShadeClasses; ++c) A.cnt->n_class[c] = 0;
     }
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_wave; k += gridDim.x * blockDim.x) {
-        const unsigned long long g = A.wave_base + k;
-        const uint32_t pix = (uint32_t)(g % A.n_pix);
-        const unsigned long long s = g / A.n_pix;
+        uint32_t si = 0;
+        while (si + 1 < n_seg && k >= A.wave->seg[si + 1].slot_begin) ++si;
+        const WaveSeg sg = A.wave->seg[si];
+        const JobDev &J = A.jobs[sg.job];
+        const unsigned long long g = sg.sample_base + (k - sg.slot_begin);
+        const uint32_t pix = (uint32_t)(g % J.n_pix);
+        const unsigned long long s = g / J.n_pix;
         Pcg32 rng;
         rng.seed(pix, 1u);
-        const unsigned long long sidx = (unsigned long long)A.sample_offset + s;
+        const unsigned long long sidx = (unsigned long long)J.sample_offset + s;
         if (sidx) rng.advance(sidx << 16);
         const float ux = rng.nextf(), uy = rng.nextf(), ul = rng.nextf();
-        const uint32_t px = pix % (uint32_t)A.cam.W, py = pix / (uint32_t)A.cam.W;
-        const float sx = __fdiv_rn(__fadd_rn((float)px, ux), (float)A.cam.W);
-        const float sy = __fdiv_rn(__fadd_rn((float)((uint32_t)A.cam.H - 1u - py), uy), (float)A.cam.H);
+        const uint32_t px = pix % (uint32_t)J.cam.W, py = pix / (uint32_t)J.cam.W;
+        const float sx = __fdiv_rn(__fadd_rn((float)px, ux), (float)J.cam.W);
+        const float sy = __fdiv_rn(__fadd_rn((float)((uint32_t)J.cam.H - 1u - py), uy), (float)J.cam.H);
         // PhysicalCamera::awaken_ray with lens sample (0.5, 0.5) and lensRadius 0
         const v3 lp = sub(mul(mk(0.5f, 0.5f, 0.f), 2.f), mk(1.f, 1.f, 0.f));
         const v3 rd = mul(lp, 0.f);
-        const v3 offset = add(mul(A.cam.u, rd.x), mul(A.cam.v, rd.y));
-        const v3 o = add(A.cam.origin, offset);
-        const v3 dir = sub(sub(add(add(A.cam.lower_left, mul(A.cam.horizontal, sx)), mul(A.cam.vertical, sy)),
-                               A.cam.origin),
+        const v3 offset = add(mul(J.cam.u, rd.x), mul(J.cam.v, rd.y));
+        const v3 o = add(J.cam.origin, offset);
+        const v3 dir = sub(sub(add(add(J.cam.lower_left, mul(J.cam.horizontal, sx)), mul(J.cam.vertical, sy)),
+                               J.cam.origin),
                            offset);
         const v3 d = normalize(dir);
         A.pixel[k] = pix;
+        A.job[k] = (uint16_t)sg.job;
         A.rng[k] = rng.state;
         A.lambda0[k] = 380.f + ul * 340.f;
         A.eta_scale[k] = 1.f;
@@ -295,7 +326,7 @@ static __global__ void __launch_bounds__(128) k_advance(WaveCounters *cnt) {
 }
 
 // analytic sphere lights after the triangle traversal: closest of both
-__device__ inline void add_spheres(const RenderArgs &A, const RayPre &r, TraceResult &res) {
+__device__ inline void add_spheres(const JobDev &A, const RayPre &r, TraceResult &res) {
     if (!A.has_spheres) return;
     const v3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
     float best = res.id >= 0 ? res.t : r.tmax;
@@ -316,25 +347,35 @@ constexpr int kRenderTraceSteps = 8;
 
 struct PathTraceItem {
     const RenderArgs *A;
+    const JobDev *J;
+    const WideNode *nodes;
+    uint32_t n_nodes;
+    const float4 *tris;
+    uint32_t n_tris;
     uint32_t slot;
     bool any_hit;
     RayPre ray;
     TravState st;
     __device__ bool begin(uint32_t q) {
         slot = A->q_trace[q];
+        J = &A->jobs[A->job[slot]];
+        nodes = J->nodes;
+        n_nodes = J->n_nodes;
+        tris = J->tris;
+        n_tris = J->n_tri;
         ray = ray_precompute(A->ray_o[slot], A->ray_d[slot]);
         trav_init(st, ray);
         return true;
     }
     __device__ void finish() {
         TraceResult res = st.res;
-        add_spheres(*A, ray, res);
+        add_spheres(*J, ray, res);
         A->hit[slot] = make_int4(res.id, __float_as_int(res.t), __float_as_int(res.u), __float_as_int(res.v));
         // group by shading work so that warps of k_shade / k_continue run one material's code
         int cls = 0;
         if (res.id != -1) {
-            const uint32_t mi = res.id >= 0 ? A->tri_material[res.id] : 0u;
-            cls = 1 + A->materials[mi].type;
+            const uint32_t mi = res.id >= 0 ? J->tri_material[res.id] : 0u;
+            cls = 1 + J->materials[mi].type;
         }
         const uint32_t pos = coalesced_append_class(A->cnt->n_class, cls);
         A->q_class[(size_t)cls * A->cap + pos] = slot;
@@ -350,8 +391,7 @@ __global__ void __launch_bounds__(128) k_trace_paths(RenderArgs A) {
     PathTraceItem it;
     it.A = &A;
     it.any_hit = false;
-    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, A.nodes, A.n_nodes, A.tris, A.n_tri, err,
-                                               st);
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, err, st);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->rays, (unsigned long long)n);
     if (COUNT) {
         warp_count(&A.cnt->nodes, st.nodes);
@@ -377,6 +417,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
             int c = 0;
             while (q >= off[c + 1]) ++c;
             slot = A.q_class[(size_t)c * A.cap + (q - off[c])];
+            const JobDev &J = A.jobs[A.job[slot]];
             const int4 h = A.hit[slot];
             const uint32_t fl = A.flags[slot];
             const uint32_t bounce = fl & 0xffu;
@@ -387,39 +428,39 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
             load_spec<NL>(A.L, A.cap, slot, L);
             const bool hit = h.x != -1;
             Hit hr;
-            if (hit) hr = make_hit(A, o4, d4, h);
+            if (hit) hr = make_hit(J, o4, d4, h);
             if (bounce == 0 || specular) {
                 if (hit) {
-                    const int li = prim_light(A, h.x);
+                    const int li = prim_light(J, h.x);
                     if (li >= 0) {
-                        const LightDev Ll = A.lights[li];
+                        const LightDev Ll = J.lights[li];
                         const float le = dot(hr.n, mk(-d4.x, -d4.y, -d4.z)) > 0.f ? Ll.radiance : 0.f;
 #pragma unroll
                         for (int c = 0; c < NL; ++c) L.c[c] += beta.c[c] * le;
                     }
-                } else if (A.has_env) {
+                } else if (J.has_env) {
 #pragma unroll
-                    for (int c = 0; c < NL; ++c) L.c[c] += beta.c[c] * A.env_radiance;
+                    for (int c = 0; c < NL; ++c) L.c[c] += beta.c[c] * J.env_radiance;
                 }
             }
             if (!hit) {
-                finish_path<NL>(A, sm, slot, L);
+                finish_path<NL>(A, J, sm, slot, L);
             } else {
                 ++shaded;
                 alive = true;
                 store_spec<NL>(A.L, A.cap, slot, L);
                 const float lambda0 = A.lambda0[slot];
                 Bsdf<NL> b;
-                make_bsdf<NL>(A, sm, hr, lambda0, b);
+                make_bsdf<NL>(J, A.tab, sm, hr, lambda0, b);
                 if (bsdf_num_components(b, kBsdfAll & ~kBsdfSpecular) > 0) {
                     Pcg32 rng;
                     rng.state = A.rng[slot];
                     rng.inc = 3u;
                     const int bsdfFlags = kBsdfAll & ~kBsdfSpecular;
-                    for (int li = 0; li < A.n_lights; ++li) {
+                    for (int li = 0; li < J.n_lights; ++li) {
                         const float ulx = rng.nextf(), uly = rng.nextf();
                         const float usx = rng.nextf(), usy = rng.nextf();
-                        const LightDev Ll = A.lights[li];
+                        const LightDev Ll = J.lights[li];
                         uint32_t pf = 0;
                         Spec<NL> CL, CS;
                         CL.set(0.f);
@@ -427,7 +468,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                         // light sampling term
                         float scatteringPdf = 0.f;
                         v3 wi = mk(0.f, 0.f, 0.f);
-                        const LightSample ls = light_sample_li(Ll, A.soup, hr, ulx, uly);
+                        const LightSample ls = light_sample_li(Ll, J.soup, hr, ulx, uly);
                         float illumPdf = ls.pdf;
                         if (ls.vis_kind) wi = ls.wi;
                         if (ls.pdf > 0 && ls.radiance != 0.f) {
@@ -477,7 +518,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                                 float weight = 1.f;
                                 bool ok = true;
                                 if (!sampledSpecular) {
-                                    illumPdf = light_pdf_li(Ll, A.soup, hr, wi);
+                                    illumPdf = light_pdf_li(Ll, J.soup, hr, wi);
                                     if (illumPdf == 0) ok = false;
                                     else weight = power_heuristic(scatteringPdf, illumPdf);
                                 }
@@ -515,6 +556,11 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
 
 struct NeeRayItem {
     const RenderArgs *A;
+    const JobDev *J;
+    const WideNode *nodes;
+    uint32_t n_nodes;
+    const float4 *tris;
+    uint32_t n_tris;
     uint32_t q, kind, sl;
     bool any_hit;
     RayPre ray;
@@ -524,8 +570,13 @@ struct NeeRayItem {
         const uint32_t tag = A->stag[q];
         kind = tag & 1u;
         sl = tag >> 1;  // li * cap + slot
+        J = &A->jobs[A->job[sl % A->cap]];
+        nodes = J->nodes;
+        n_nodes = J->n_nodes;
+        tris = J->tris;
+        n_tris = J->n_tri;
         ray = ray_precompute(A->sray_o[q], A->sray_d[q]);
-        any_hit = kind == 0 && A->any_hit_ok;
+        any_hit = kind == 0 && J->any_hit_ok;
         trav_init(st, ray);
         return true;
     }
@@ -535,16 +586,16 @@ struct NeeRayItem {
         uint32_t bit = 0;
         if (kind == 0) {
             // VisibilityEvaluator::unoccluded: no hit, or the closest hit is emissive
-            const bool unocc = res.id < 0 || A->tri_light[res.id] >= 0;
+            const bool unocc = res.id < 0 || J->tri_light[res.id] >= 0;
             bit = unocc ? kVisOK : 0u;
         } else {
-            add_spheres(*A, ray, res);
-            const LightDev Ll = A->lights[li];
+            add_spheres(*J, ray, res);
+            const LightDev Ll = J->lights[li];
             bool ok = false;
             if (res.id == -1) ok = Ll.type == FL_LIGHT_ENV;
-            else if (prim_light(*A, res.id) == (int)li) {
+            else if (prim_light(*J, res.id) == (int)li) {
                 const int4 h = make_int4(res.id, __float_as_int(res.t), 0, 0);
-                const Hit hr = make_hit(*A, A->sray_o[q], A->sray_d[q], h);
+                const Hit hr = make_hit(*J, A->sray_o[q], A->sray_d[q], h);
                 ok = dot(hr.n, mk(-ray.dx, -ray.dy, -ray.dz)) > 0.f;
             }
             bit = ok ? kMisOK : 0u;
@@ -561,8 +612,7 @@ __global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
     TraceStats st;
     NeeRayItem it;
     it.A = &A;
-    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, A.nodes, A.n_nodes, A.tris, A.n_tri, err,
-                                               st);
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, err, st);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&A.cnt->shadow_rays, (unsigned long long)n);
         atomicAdd(&A.cnt->rays, (unsigned long long)n);
@@ -585,14 +635,15 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
         uint32_t slot = 0;
         if (active) {
             slot = A.q_cont[q];
+            const JobDev &J = A.jobs[A.job[slot]];
             const int4 h = A.hit[slot];
             const uint32_t fl = A.flags[slot];
             const uint32_t bounce = fl & 0xffu;
             const float4 o4 = A.ray_o[slot], d4 = A.ray_d[slot];
-            const Hit hr = make_hit(A, o4, d4, h);
+            const Hit hr = make_hit(J, o4, d4, h);
             const float lambda0 = A.lambda0[slot];
             Bsdf<NL> b;
-            make_bsdf<NL>(A, sm, hr, lambda0, b);
+            make_bsdf<NL>(J, A.tab, sm, hr, lambda0, b);
             Spec<NL> beta, L;
             load_spec<NL>(A.beta, A.cap, slot, beta);
             load_spec<NL>(A.L, A.cap, slot, L);
@@ -600,7 +651,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                 // uniform_sample_all_lights: sum of the per-light estimate_direct results
                 Spec<NL> Ls;
                 Ls.set(0.f);
-                for (int li = 0; li < A.n_lights; ++li) {
+                for (int li = 0; li < J.n_lights; ++li) {
                     const uint32_t pf = A.pflags[(size_t)li * A.cap + slot];
                     Spec<NL> Ld;
                     Ld.set(0.f);
@@ -634,7 +685,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             const float ux = rng.nextf(), uy = rng.nextf();
             bsdf_sample<NL>(b, wo, wi, ux, uy, pdf, kBsdfAll, sflags, f);
             bool stop = f.black() || pdf == 0;
-            const int depth = A.max_depth;
+            const int depth = J.max_depth;
             const int bi = (int)bounce;
             if (!stop && depth == bi && (sflags & kBsdfDiffuse)) stop = true;
             if (!stop && ((depth == bi && (sflags & kBsdfSpecular)) || (depth == bi && (sflags & kBsdfGlossy)))) stop = true;
@@ -653,7 +704,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                 float mx = beta.c[0] * etaScale;
 #pragma unroll
                 for (int k = 1; k < NL; ++k) mx = fmaxf(mx, beta.c[k] * etaScale);
-                if (mx < A.rr_threshold && bi > 3) {
+                if (mx < J.rr_threshold && bi > 3) {
                     float qq = 1.f - mx;
                     if (qq < 0.05f) qq = 0.05f;
                     if (rng.nextf() < qq) stop = true;
@@ -673,7 +724,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             }
             A.rng[slot] = rng.state;
             if (alive) store_spec<NL>(A.L, A.cap, slot, L);
-            else finish_path<NL>(A, sm, slot, L);
+            else finish_path<NL>(A, J, sm, slot, L);
         }
         const uint32_t pos = warp_append(&A.cnt->n_next, alive);
         if (alive) A.q_next[pos] = slot;
@@ -692,27 +743,37 @@ static __global__ void k_resolve(const double *__restrict__ film, uint32_t n_pix
     }
 }
 
-// ------------------------------------------------------------------------------ host driver
+// ------------------------------------------------------------------------------ host side
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Renders all samples of the image into d_film (FP64 XYZ sums) wave by wave. Instantiated
-// per spectral mode in its own translation unit (the 60-bin one without FMA contraction).
-template <int NL>
-fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film,
-                       WaveCounters *h_cnt, RenderProfile *prof, cudaStream_t st, void *fixed_scratch = nullptr,
-                       size_t fixed_bytes = 0) {
-    Context *ctx = s->ctx;
-    const int nl = (int)s->n_lights;
-    const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
-    const unsigned long long total = n_pix * (unsigned long long)p.spp;
-    const size_t per_slot = 92 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl +
-                            72 * (size_t)nl;
-    const size_t budget = fixed_scratch ? fixed_bytes : (size_t)3 << 30;
-    size_t cap = p.wave_paths > 0 ? (size_t)p.wave_paths : (NL == 60 ? (size_t)1 << 19 : (size_t)1 << 21);
-    cap = std::min(cap, budget / per_slot);
-    cap = std::min<size_t>(cap, (size_t)total);
-    cap = std::max<size_t>(128, (cap + 127) & ~(size_t)127);
+// bytes of wave state per path slot
+inline size_t wave_bytes_per_slot(int NL, int nl) {
+    return 94 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
+}
+
+// The device buffers of a wavefront: job table, wave descriptor, path state and queues.
+struct WaveBuffers {
+    RenderArgs A;
+    uint32_t *qa, *qb;
+    JobDev *d_jobs;
+    WaveDesc *d_wave;
+    size_t cap;
+};
+
+// Lays the buffers out in `fixed` (fixed_bytes) or in the context scratch. The wave holds
+// at most cap_request paths and no more than the buffer allows.
+inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, void *fixed, size_t fixed_bytes,
+                              WaveBuffers &W) {
+    const size_t per_slot = wave_bytes_per_slot(NL, nl);
+    const size_t head = align_up(sizeof(WaveCounters)) + align_up(sizeof(JobDev) * kMaxJobs) + align_up(sizeof(WaveDesc));
+    const size_t budget = fixed ? fixed_bytes : (size_t)3 << 30;
+    if (budget < head + 32 * 256 + 128 * per_slot) {
+        set_error(ctx, "render state does not fit the fixed scratch buffer");
+        return FL_ERR_CAPACITY;
+    }
+    size_t cap = std::min(cap_request, (budget - head - 32 * 256) / per_slot);
+    cap = std::max<size_t>(128, cap & ~(size_t)127);
     if (cap * (size_t)std::max(nl, 1) >= ((size_t)1 << 31)) {
         set_error(ctx, "wave too large for the shadow-ray tags");
         return FL_ERR_INVALID;
@@ -720,8 +781,10 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     const size_t scap = cap * 2 * (size_t)nl;
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes ? bytes : 1); return o; };
-    const size_t o_cnt = take(sizeof(WaveCounters));
-    const size_t o_pixel = take(4 * cap), o_rng = take(8 * cap), o_beta = take(4 * NL * cap), o_L = take(4 * NL * cap);
+    const size_t o_cnt = take(sizeof(WaveCounters)), o_jobs = take(sizeof(JobDev) * kMaxJobs),
+                 o_wave = take(sizeof(WaveDesc));
+    const size_t o_pixel = take(4 * cap), o_job = take(2 * cap), o_rng = take(8 * cap), o_beta = take(4 * NL * cap),
+                 o_L = take(4 * NL * cap);
     const size_t o_lam = take(4 * cap), o_eta = take(4 * cap), o_flags = take(4 * cap);
     const size_t o_ro = take(16 * cap), o_rd = take(16 * cap), o_hit = take(16 * cap);
     const size_t o_CL = take(4 * (size_t)NL * nl * cap), o_CS = take(4 * (size_t)NL * nl * cap);
@@ -729,8 +792,8 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     const size_t o_so = take(16 * scap), o_sd = take(16 * scap), o_st = take(4 * scap);
     const size_t o_qa = take(4 * cap), o_qb = take(4 * cap), o_qc = take(4 * cap);
     const size_t o_qk = take(4 * cap * kShadeClasses);
-    void *base = fixed_scratch;
-    if (!fixed_scratch) {
+    void *base = fixed;
+    if (!fixed) {
         fl_status rc = ensure_scratch(ctx, off, &base);
         if (rc) return rc;
     } else if (off > fixed_bytes) {
@@ -738,37 +801,21 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         return FL_ERR_CAPACITY;
     }
     char *B = static_cast<char *>(base);
-
-    RenderArgs A{};
-    A.nodes = s->nodes;
-    A.n_nodes = s->n_nodes;
-    A.tris = s->tris;
-    A.n_tri = s->n_tri;
-    A.soup = s->soup;
-    A.tri_material = s->tri_material;
-    A.tri_light = s->tri_light;
-    A.materials = s->materials;
-    A.mat_refl60 = s->mat_refl60;
-    A.lights = s->lights;
-    A.n_lights = nl;
-    A.any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
-    A.has_env = s->has_env;
-    A.env_radiance = s->env_radiance;
-    A.has_spheres = 0;
-    for (const auto &l : s->lights_host) A.has_spheres |= (l.type == FL_LIGHT_SPHERE) ? 1 : 0;
+    RenderArgs &A = W.A;
+    A = RenderArgs{};
     const SpectralTablesDev &T = ctx->tables;
     A.tab = TablesArg{T.cie_lambda0, T.n_cie, T.cie_y_integral, T.rgb_lambda0, T.rgb_lambda1, T.n_rgb,
                       T.cie_xyz, T.rgb_bases, T.binned};
-    A.cam = cam;
-    A.spp = p.spp;
-    A.max_depth = p.max_depth;
-    A.rr_threshold = p.rr_threshold;
-    A.sample_offset = p.sample_offset;
-    A.total = total;
-    A.n_pix = (uint32_t)n_pix;
+    W.d_jobs = reinterpret_cast<JobDev *>(B + o_jobs);
+    W.d_wave = reinterpret_cast<WaveDesc *>(B + o_wave);
+    A.jobs = W.d_jobs;
+    A.wave = W.d_wave;
+    A.nl = nl;
     A.cap = (uint32_t)cap;
+    A.scap = (uint32_t)scap;
     A.cnt = reinterpret_cast<WaveCounters *>(B + o_cnt);
     A.pixel = reinterpret_cast<uint32_t *>(B + o_pixel);
+    A.job = reinterpret_cast<uint16_t *>(B + o_job);
     A.rng = reinterpret_cast<unsigned long long *>(B + o_rng);
     A.beta = reinterpret_cast<float *>(B + o_beta);
     A.L = reinterpret_cast<float *>(B + o_L);
@@ -784,47 +831,110 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     A.sray_o = reinterpret_cast<float4 *>(B + o_so);
     A.sray_d = reinterpret_cast<float4 *>(B + o_sd);
     A.stag = reinterpret_cast<uint32_t *>(B + o_st);
-    A.scap = (uint32_t)scap;
-    A.film = d_film;
-    uint32_t *qa = reinterpret_cast<uint32_t *>(B + o_qa), *qb = reinterpret_cast<uint32_t *>(B + o_qb);
     A.q_cont = reinterpret_cast<uint32_t *>(B + o_qc);
     A.q_class = reinterpret_cast<uint32_t *>(B + o_qk);
-    FL_CUDA_TRY(ctx, cudaMemsetAsync(A.cnt, 0, sizeof(WaveCounters), st));
+    W.qa = reinterpret_cast<uint32_t *>(B + o_qa);
+    W.qb = reinterpret_cast<uint32_t *>(B + o_qb);
+    W.cap = cap;
+    return FL_OK;
+}
 
+// Enqueues one wave (camera rays of the samples in *W.d_wave, then max_depth + 1 bounces)
+// on `st`. Launch shapes do not depend on the wave's content, so the sequence can be
+// captured once into a CUDA graph and replayed for every wave.
+template <int NL>
+void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile *prof, int sms, cudaStream_t st) {
+    RenderArgs A = W.A;
+    A.q_trace = W.qa;
+    A.q_next = W.qb;
+    const int g_trace = sms * 16, g_shade = sms * 8;
+    k_raygen<NL><<<std::min<uint32_t>(((uint32_t)W.cap + 127) / 128, (uint32_t)sms * 32), 128, 0, st>>>(A);
+    prof->launches += 1;
+    for (int b = 0; b <= max_depth; ++b) {
+        if (b > 0) {
+            k_advance<<<1, 1, 0, st>>>(A.cnt);
+            std::swap(A.q_trace, A.q_next);
+            prof->launches += 1;
+        }
+        prof->mark(0, st);
+        if (count) k_trace_paths<true><<<g_trace, 128, 0, st>>>(A);
+        else k_trace_paths<false><<<g_trace, 128, 0, st>>>(A);
+        prof->mark(0, st);
+        prof->mark(1, st);
+        k_shade<NL><<<g_shade, 128, 0, st>>>(A);
+        prof->mark(1, st);
+        prof->mark(2, st);
+        if (count) k_trace_rays2<true><<<g_trace, 128, 0, st>>>(A);
+        else k_trace_rays2<false><<<g_trace, 128, 0, st>>>(A);
+        prof->mark(2, st);
+        prof->mark(3, st);
+        k_continue<NL><<<g_shade, 128, 0, st>>>(A);
+        prof->mark(3, st);
+        prof->launches += 4;
+    }
+}
+
+// The job record of one scene + camera + parameters (fl_render's single job).
+inline JobDev job_of(const Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film) {
+    JobDev j{};
+    j.nodes = s->nodes;
+    j.n_nodes = s->n_nodes;
+    j.tris = s->tris;
+    j.n_tri = s->n_tri;
+    j.soup = s->soup;
+    j.tri_material = s->tri_material;
+    j.tri_light = s->tri_light;
+    j.materials = s->materials;
+    j.mat_refl60 = s->mat_refl60;
+    j.lights = s->lights;
+    j.n_lights = (int)s->n_lights;
+    j.any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
+    j.has_env = s->has_env;
+    j.env_radiance = s->env_radiance;
+    j.has_spheres = 0;
+    for (const auto &l : s->lights_host) j.has_spheres |= (l.type == FL_LIGHT_SPHERE) ? 1 : 0;
+    j.cam = cam;
+    j.spp = p.spp;
+    j.max_depth = p.max_depth;
+    j.rr_threshold = p.rr_threshold;
+    j.sample_offset = p.sample_offset;
+    j.n_pix = (uint32_t)((uint64_t)cam.W * (uint64_t)cam.H);
+    j.film = d_film;
+    return j;
+}
+
+// Renders all samples of one image into d_film (FP64 XYZ sums) wave by wave, without host
+// synchronisation. Instantiated per spectral mode in its own translation unit (the 60-bin
+// one without FMA contraction).
+template <int NL>
+fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film,
+                       WaveCounters *h_cnt, RenderProfile *prof, cudaStream_t st, void *fixed_scratch = nullptr,
+                       size_t fixed_bytes = 0) {
+    Context *ctx = s->ctx;
+    const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
+    const unsigned long long total = n_pix * (unsigned long long)p.spp;
+    size_t cap_req = p.wave_paths > 0 ? (size_t)p.wave_paths : (NL == 60 ? (size_t)1 << 19 : (size_t)1 << 21);
+    cap_req = std::min<size_t>(cap_req, (size_t)total);
+    WaveBuffers W;
+    fl_status rc = wave_buffers(ctx, NL, (int)s->n_lights, cap_req, fixed_scratch, fixed_bytes, W);
+    if (rc) return rc;
+    const JobDev j = job_of(s, cam, p, d_film);
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_jobs, &j, sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    FL_CUDA_TRY(ctx, cudaMemsetAsync(W.A.cnt, 0, sizeof(WaveCounters), st));
     const bool count = (p.flags & FL_RENDER_COUNT) != 0;
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
-    const int g_trace = sms * 16, g_shade = sms * 8;
-    for (unsigned long long wb = 0; wb < total; wb += cap) {
-        const uint32_t n_wave = (uint32_t)std::min<unsigned long long>(cap, total - wb);
-        A.wave_base = wb;
-        A.q_trace = qa;
-        A.q_next = qb;
-        k_raygen<NL><<<std::min<uint32_t>((n_wave + 127) / 128, (uint32_t)sms * 32), 128, 0, st>>>(A, n_wave);
-        for (int b = 0; b <= p.max_depth; ++b) {
-            if (b > 0) {
-                k_advance<<<1, 1, 0, st>>>(A.cnt);
-                std::swap(A.q_trace, A.q_next);
-            }
-            prof->mark(0, st);
-            if (count) k_trace_paths<true><<<g_trace, 128, 0, st>>>(A);
-            else k_trace_paths<false><<<g_trace, 128, 0, st>>>(A);
-            prof->mark(0, st);
-            prof->mark(1, st);
-            k_shade<NL><<<g_shade, 128, 0, st>>>(A);
-            prof->mark(1, st);
-            prof->mark(2, st);
-            if (count) k_trace_rays2<true><<<g_trace, 128, 0, st>>>(A);
-            else k_trace_rays2<false><<<g_trace, 128, 0, st>>>(A);
-            prof->mark(2, st);
-            prof->mark(3, st);
-            k_continue<NL><<<g_shade, 128, 0, st>>>(A);
-            prof->mark(3, st);
-            prof->launches += b > 0 ? 5 : 4;
-        }
-        prof->launches += 1;
+    const size_t desc_bytes = offsetof(WaveDesc, seg) + sizeof(WaveSeg);
+    for (unsigned long long wb = 0; wb < total; wb += W.cap) {
+        WaveDesc d;
+        d.n_wave = (uint32_t)std::min<unsigned long long>(W.cap, total - wb);
+        d.n_seg = 1;
+        d.seg[0] = WaveSeg{0u, 0u, d.n_wave, 0u, wb, 0ull};
+        // pageable source: the copy is staged before the call returns, so `d` may be reused
+        FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
+        enqueue_wave<NL>(W, p.max_depth, count, prof, sms, st);
         FL_CUDA_TRY(ctx, cudaGetLastError());
     }
-    FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, W.A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
     return FL_OK;
 }
 

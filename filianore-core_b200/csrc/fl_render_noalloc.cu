@@ -80,9 +80,8 @@ extern "C" fl_status fl_render_noalloc(fl_scene *scene_h, const fl_camera *camer
     // the smallest wave (128 paths) must fit the fixed buffer
     const int nl = (int)s->n_lights;
     const int NL = p.spectral_mode == FL_SPECTRAL_BINS60 ? 60 : 4;
-    const size_t per_slot = 92 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl +
-                            72 * (size_t)nl;
-    const size_t fixed_overhead = 64 * 256;  // alignment of the arrays and the counters
+    const size_t per_slot = wave_bytes_per_slot(NL, nl);
+    const size_t fixed_overhead = 64 * 1024;  // counters, job table, wave descriptor, array alignment
     if (per_slot * 128 + fixed_overhead > kNoAllocScratchBytes) {
         set_error(ctx, "scene needs more render state per path than the 32 MiB fixed scratch of fl_render_noalloc holds");
         return FL_ERR_CAPACITY;

@@ -25,6 +25,9 @@ struct TraceItem {
     int4 *hits;
     uint8_t *occ;
     const int32_t *tri_light;
+    const WideNode *nodes;
+    uint32_t n_nodes;
+    const float4 *tris;
     uint32_t n_tris;
     bool any_hit;
     uint32_t q;
@@ -66,12 +69,15 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restric
     it.hits = hits;
     it.occ = occ;
     it.tri_light = tri_light;
+    it.nodes = nodes;
+    it.n_nodes = n_nodes;
+    it.tris = tris;
     it.n_tris = n_tris;
     it.any_hit = KIND == kTraceOccluded && any_hit_ok;
     TraceStats st;
     bool error = false;
     uint32_t *fetch = reinterpret_cast<uint32_t *>(counters + 4);
-    persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, nodes, n_nodes, tris, n_tris, error, st);
+    persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, error, st);
     if (KIND == kTraceCount) {
         warp_add_u64(&counters[0], st.nodes);
         warp_add_u64(&counters[1], st.tris);

@@ -173,12 +173,11 @@ __device__ __forceinline__ TraceResult traverse(const WideNode *__restrict__ nod
 
 // Persistent-warp work loop: every lane holds one item; lanes whose item finished fetch
 // the next one (one atomic per warp) every `steps` traversal steps. `Item` provides
-// begin(q) -> bool (false: nothing to trace, already finished) and finish(); the
-// traversal state lives in the item. Call with all 32 lanes of the warp.
+// begin(q) -> bool (false: nothing to trace, already finished), finish(), the traversal
+// state (st, ray, any_hit) and the acceleration structure it traverses (nodes, n_nodes,
+// tris, n_tris), which begin() may choose per item. Call with all 32 lanes of the warp.
 template <int STEPS, bool COUNT, class Item>
-__device__ __forceinline__ void persistent_trace(Item &it, uint32_t *fetch_counter, uint32_t n,
-                                                 const WideNode *__restrict__ nodes, uint32_t n_nodes,
-                                                 const float4 *__restrict__ tris, uint32_t n_tris, bool &error,
+__device__ __forceinline__ void persistent_trace(Item &it, uint32_t *fetch_counter, uint32_t n, bool &error,
                                                  TraceStats &stats) {
     uint2 stack[kTraversalStack];
     bool has = false;
@@ -196,7 +195,7 @@ __device__ __forceinline__ void persistent_trace(Item &it, uint32_t *fetch_count
                 const uint32_t q = base + __popc(need & ((1u << lane) - 1u));
                 if (q < n) {
                     has = it.begin(q);
-                    if (has && (n_nodes == 0 || !it.ray.valid)) {
+                    if (has && (it.n_nodes == 0 || !it.ray.valid)) {
                         it.finish();
                         has = false;
                     }
@@ -210,7 +209,8 @@ __device__ __forceinline__ void persistent_trace(Item &it, uint32_t *fetch_count
         if (has) {
 #pragma unroll 1
             for (int k = 0; k < STEPS; ++k) {
-                if (trav_step<COUNT>(it.st, stack, nodes, n_nodes, tris, n_tris, it.ray, it.any_hit, error, stats)) {
+                if (trav_step<COUNT>(it.st, stack, it.nodes, it.n_nodes, it.tris, it.n_tris, it.ray, it.any_hit, error,
+                                     stats)) {
                     it.finish();
                     has = false;
                     break;
