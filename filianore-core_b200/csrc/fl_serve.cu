@@ -1,0 +1,427 @@
+// Serving loop: continuous batching of render jobs (include/filianore_gpu.h, fl_server_*).
+//
+// A worker thread owns one GPU stream and a fixed set of wave buffers. Each iteration it
+//   1. admits queued jobs in arrival order while their films (and their scene, when it is
+//      not resident) fit the memory budget, evicting idle scenes least recently used first
+//      and building newly needed scenes on the device (fl_serve_sched.h has the policy);
+//   2. plans one wave: the path slots are split over all running jobs (water-filling), each
+//      job contributing one contiguous range of its samples, so several scenes' paths run
+//      in the same kernels;
+//   3. uploads the job table and the wave's sample ranges and replays the wave as a CUDA
+//      graph captured once at start-up (the launch sequence never changes; the kernels
+//      read what to do from device memory);
+//   4. after the wave, resolves the films of jobs that are complete and copies them to the
+//      host, where fl_server_poll / fl_server_wait pick them up.
+// Jobs that arrive while others run join at the next wave. Per-sample random streams depend
+// only on (pixel, sample index), so a job's image is the same alone and in any mix, up to
+// the order of the FP64 film additions.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <thread>
+
+#include "fl_render.cuh"
+#include "fl_serve_sched.h"
+
+namespace fl {
+CamDev camera_basis_of(const fl_camera &c);
+
+namespace {
+
+struct HostScene {
+    std::vector<float> verts;
+    std::vector<uint32_t> tri_material;
+    std::vector<fl_material> materials;
+    std::vector<fl_light> lights;
+    Scene *dev = nullptr;
+    uint64_t bytes = 0;
+};
+
+struct HostJob {
+    uint64_t scene = 0;
+    fl_camera cam{};
+    fl_render_params params{};
+    int slot = -1;
+    double *d_film = nullptr;
+    float *d_rgb = nullptr;
+    std::vector<float> rgb;
+    std::vector<double> xyz;
+    fl_status status = FL_ERR_NOT_READY;
+    fl_status fail = FL_OK;  // set when admission could not give the job a film; reported when it completes
+    double submit_ms = 0, start_ms = 0, done_ms = 0;
+};
+
+uint64_t scene_bytes_estimate(uint32_t n_tri, uint32_t n_mat) {
+    // nodes (< N/2 x 80 B) + BVH triangles 48 B + soup 36 B + material/light tables 8 B
+    return (uint64_t)n_tri * (40 + 48 + 36 + 8) + (uint64_t)n_mat * 300 + (1 << 20);
+}
+
+}  // namespace
+
+struct Server {
+    Context *ctx = nullptr;
+    fl_server_config cfg{};
+    cudaStream_t stream = nullptr;
+    void *wave_mem = nullptr;
+    size_t wave_bytes = 0;
+    WaveBuffers W{};
+    cudaGraphExec_t graph = nullptr;
+    std::vector<JobDev> table;  // kMaxJobs
+    std::vector<int> free_slots;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    std::thread worker;
+    ServeScheduler sched;
+    std::map<uint64_t, HostScene> scenes;
+    std::map<uint64_t, std::unique_ptr<HostJob>> jobs;
+    uint64_t next_scene = 1, next_job = 1;
+    std::chrono::steady_clock::time_point t0;
+    fl_server_stats stats{};
+    std::string error;
+
+    Server(uint64_t budget, int max_jobs) : sched(budget, max_jobs) {}
+    double now_ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+fl_status make_scene(Server *S, HostScene &h) {
+    fl_scene_desc d{};
+    d.verts = h.verts.data();
+    d.n_tri = (uint32_t)(h.verts.size() / 9);
+    d.tri_material = h.tri_material.data();
+    d.materials = h.materials.data();
+    d.n_materials = (uint32_t)h.materials.size();
+    d.lights = h.lights.data();
+    d.n_lights = (uint32_t)h.lights.size();
+    fl_scene *out = nullptr;
+    fl_status rc = fl_scene_create(reinterpret_cast<fl_context *>(S->ctx), &d, &out);
+    if (rc == FL_OK) h.dev = reinterpret_cast<Scene *>(out);
+    return rc;
+}
+
+void finish_job(Server *S, uint64_t jid, HostJob &job) {
+    const size_t n_pix = (size_t)job.cam.width * job.cam.height;
+    k_resolve<<<(uint32_t)std::min<size_t>((n_pix + 255) / 256, (size_t)S->ctx->sm_count * 8), 256, 0, S->stream>>>(
+        job.d_film, (uint32_t)n_pix, 1.0 / (double)job.params.spp, job.d_rgb);
+    job.rgb.resize(n_pix * 3);
+    job.xyz.resize(n_pix * 3);
+    cudaMemcpyAsync(job.rgb.data(), job.d_rgb, n_pix * 3 * sizeof(float), cudaMemcpyDeviceToHost, S->stream);
+    cudaMemcpyAsync(job.xyz.data(), job.d_film, n_pix * 3 * sizeof(double), cudaMemcpyDeviceToHost, S->stream);
+    cudaError_t e = cudaStreamSynchronize(S->stream);
+    cudaFree(job.d_film);
+    cudaFree(job.d_rgb);
+    job.d_film = nullptr;
+    job.d_rgb = nullptr;
+    std::lock_guard<std::mutex> lock(S->mu);
+    job.status = e == cudaSuccess ? FL_OK : FL_ERR_CUDA;
+    job.done_ms = S->now_ms();
+    if (job.slot >= 0) S->free_slots.push_back(job.slot);
+    job.slot = -1;
+    S->stats.jobs_done++;
+    (void)jid;
+}
+
+void worker_loop(Server *S) {
+    cudaSetDevice(S->ctx->device);
+    const size_t desc_head = offsetof(WaveDesc, seg);
+    while (true) {
+        ServeScheduler::Admission adm;
+        std::vector<ServeScheduler::Seg> segs;
+        {
+            std::unique_lock<std::mutex> lock(S->mu);
+            S->cv_work.wait(lock, [&] { return S->stop || !S->sched.idle(); });
+            if (S->stop) break;
+            adm = S->sched.admit();
+            // scenes: release, then build
+            for (uint64_t sid : adm.evict) {
+                HostScene &h = S->scenes[sid];
+                if (h.dev) fl_scene_destroy(reinterpret_cast<fl_scene *>(h.dev));
+                h.dev = nullptr;
+                S->stats.evictions++;
+            }
+            for (uint64_t jid : adm.rejected) {
+                auto it = S->jobs.find(jid);
+                if (it != S->jobs.end()) it->second->status = FL_ERR_CAPACITY;
+            }
+        }
+        if (!adm.rejected.empty()) S->cv_done.notify_all();
+        for (uint64_t sid : adm.build) {
+            HostScene &h = S->scenes[sid];
+            if (!h.dev && make_scene(S, h) == FL_OK) S->stats.builds++;
+        }
+        {
+            std::lock_guard<std::mutex> lock(S->mu);
+            for (uint64_t jid : adm.admitted) {
+                HostJob &job = *S->jobs[jid];
+                const size_t n_pix = (size_t)job.cam.width * job.cam.height;
+                HostScene &h = S->scenes[job.scene];
+                bool ok = h.dev != nullptr && !S->free_slots.empty();
+                if (ok && cudaMalloc(&job.d_film, n_pix * 3 * sizeof(double)) != cudaSuccess) ok = false;
+                if (ok && cudaMalloc(&job.d_rgb, n_pix * 3 * sizeof(float)) != cudaSuccess) ok = false;
+                if (!ok) {
+                    cudaGetLastError();
+                    cudaFree(job.d_film);
+                    job.d_film = nullptr;
+                    job.fail = FL_ERR_OOM;  // the scheduler still runs it; its samples are skipped
+                    continue;
+                }
+                cudaMemsetAsync(job.d_film, 0, n_pix * 3 * sizeof(double), S->stream);
+                job.slot = S->free_slots.back();
+                S->free_slots.pop_back();
+                job.start_ms = S->now_ms();
+                S->table[job.slot] = job_of(h.dev, camera_basis_of(job.cam), job.params, job.d_film);
+            }
+            segs = S->sched.plan_wave((uint32_t)S->W.cap);
+        }
+        if (!segs.empty()) {
+            WaveDesc d{};
+            uint32_t slot_begin = 0;
+            {
+                std::lock_guard<std::mutex> lock(S->mu);
+                for (const auto &sg : segs) {
+                    HostJob &job = *S->jobs[sg.job];
+                    if (job.slot < 0) continue;  // failed admission: its samples are skipped
+                    d.seg[d.n_seg++] = WaveSeg{(uint32_t)job.slot, slot_begin, sg.count, 0u, sg.sample_base, 0ull};
+                    slot_begin += sg.count;
+                    if (d.n_seg == kMaxSegs) break;
+                }
+            }
+            d.n_wave = slot_begin;
+            if (d.n_wave > 0) {
+                cudaMemcpyAsync(S->W.d_jobs, S->table.data(), sizeof(JobDev) * kMaxJobs, cudaMemcpyHostToDevice,
+                                S->stream);
+                cudaMemcpyAsync(S->W.d_wave, &d, desc_head + sizeof(WaveSeg) * d.n_seg, cudaMemcpyHostToDevice,
+                                S->stream);
+                cudaGraphLaunch(S->graph, S->stream);
+                cudaError_t e = cudaStreamSynchronize(S->stream);
+                std::lock_guard<std::mutex> lock(S->mu);
+                S->stats.waves++;
+                S->stats.paths += d.n_wave;
+                if (e != cudaSuccess) S->error = cudaGetErrorString(e);
+            }
+        }
+        std::vector<uint64_t> done;
+        {
+            std::lock_guard<std::mutex> lock(S->mu);
+            done = S->sched.finish_wave();
+        }
+        for (uint64_t jid : done) {
+            HostJob *job;
+            {
+                std::lock_guard<std::mutex> lock(S->mu);
+                job = S->jobs[jid].get();
+            }
+            if (job->d_film) finish_job(S, jid, *job);
+            else {
+                std::lock_guard<std::mutex> lock(S->mu);
+                job->done_ms = S->now_ms();
+                job->status = job->fail != FL_OK ? job->fail : FL_ERR_OOM;
+                if (job->slot >= 0) S->free_slots.push_back(job->slot);
+                job->slot = -1;
+            }
+        }
+        if (!done.empty()) S->cv_done.notify_all();
+    }
+}
+
+}  // namespace
+}  // namespace fl
+
+using namespace fl;
+
+extern "C" {
+
+fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_server **out) {
+    Context *ctx = reinterpret_cast<Context *>(ctx_h);
+    if (!ctx || !cfg || !out) return FL_ERR_INVALID;
+    *out = nullptr;
+    if (cfg->memory_budget_bytes == 0 || cfg->max_jobs <= 0 || cfg->max_jobs > kMaxJobs || cfg->max_depth < 0 ||
+        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64) {
+        set_error(ctx, "invalid server configuration");
+        return FL_ERR_INVALID;
+    }
+    auto S = std::make_unique<Server>(cfg->memory_budget_bytes, cfg->max_jobs);
+    S->ctx = ctx;
+    S->cfg = *cfg;
+    S->t0 = std::chrono::steady_clock::now();
+    FL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    FL_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    const size_t cap = cfg->wave_paths > 0 ? (size_t)cfg->wave_paths : ((size_t)1 << 21);
+    const size_t per_slot = wave_bytes_per_slot(4, cfg->max_lights);
+    S->wave_bytes = cap * per_slot + (1 << 20);
+    cudaError_t e = cudaMalloc(&S->wave_mem, S->wave_bytes);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(S->stream);
+        return cuda_status(ctx, e, "server wave buffers");
+    }
+    fl_status rc = wave_buffers(ctx, 4, cfg->max_lights, cap, S->wave_mem, S->wave_bytes, S->W);
+    if (rc) {
+        cudaFree(S->wave_mem);
+        cudaStreamDestroy(S->stream);
+        return rc;
+    }
+    S->table.assign(kMaxJobs, JobDev{});
+    for (int i = cfg->max_jobs - 1; i >= 0; --i) S->free_slots.push_back(i);
+    cudaMemsetAsync(S->W.A.cnt, 0, sizeof(WaveCounters), S->stream);
+    // capture the launch sequence of one wave once; every wave replays it
+    RenderProfile prof;
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        enqueue_wave<4>(S->W, cfg->max_depth, false, &prof, ctx->sm_count > 0 ? ctx->sm_count : 148, S->stream);
+        e = cudaStreamEndCapture(S->stream, &g);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&S->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaFree(S->wave_mem);
+        cudaStreamDestroy(S->stream);
+        return cuda_status(ctx, e, "wave graph capture");
+    }
+    cudaStreamSynchronize(S->stream);
+    Server *raw = S.release();
+    raw->worker = std::thread(worker_loop, raw);
+    *out = reinterpret_cast<fl_server *>(raw);
+    return FL_OK;
+}
+
+fl_status fl_server_destroy(fl_server *srv) {
+    Server *S = reinterpret_cast<Server *>(srv);
+    if (!S) return FL_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    if (S->worker.joinable()) S->worker.join();
+    cudaSetDevice(S->ctx->device);
+    cudaStreamSynchronize(S->stream);
+    for (auto &kv : S->jobs) {
+        cudaFree(kv.second->d_film);
+        cudaFree(kv.second->d_rgb);
+    }
+    for (auto &kv : S->scenes)
+        if (kv.second.dev) fl_scene_destroy(reinterpret_cast<fl_scene *>(kv.second.dev));
+    if (S->graph) cudaGraphExecDestroy(S->graph);
+    cudaFree(S->wave_mem);
+    cudaStreamDestroy(S->stream);
+    delete S;
+    return FL_OK;
+}
+
+fl_status fl_server_add_scene(fl_server *srv, const fl_scene_desc *d, uint64_t *scene_id) {
+    Server *S = reinterpret_cast<Server *>(srv);
+    if (!S || !d || !scene_id || !d->materials || d->n_materials == 0 || (d->n_tri && !d->verts) ||
+        (d->n_lights && !d->lights))
+        return FL_ERR_INVALID;
+    if ((int)d->n_lights > S->cfg.max_lights) {
+        set_error(S->ctx, "scene has more lights than the server was configured for");
+        return FL_ERR_INVALID;
+    }
+    HostScene h;
+    h.verts.assign(d->verts, d->verts + 9 * (size_t)d->n_tri);
+    if (d->tri_material) h.tri_material.assign(d->tri_material, d->tri_material + d->n_tri);
+    else h.tri_material.assign(d->n_tri, 0u);
+    h.materials.assign(d->materials, d->materials + d->n_materials);
+    if (d->n_lights) h.lights.assign(d->lights, d->lights + d->n_lights);
+    h.bytes = scene_bytes_estimate(d->n_tri, d->n_materials);
+    std::lock_guard<std::mutex> lock(S->mu);
+    const uint64_t id = S->next_scene++;
+    S->sched.add_scene(id, h.bytes);
+    S->scenes[id] = std::move(h);
+    *scene_id = id;
+    return FL_OK;
+}
+
+fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job_id) {
+    Server *S = reinterpret_cast<Server *>(srv);
+    if (!S || !job || !job_id) return FL_ERR_INVALID;
+    const fl_camera &c = job->camera;
+    const fl_render_params &p = job->params;
+    if (c.width <= 0 || c.height <= 0 || (uint64_t)c.width * c.height > (1ull << 31) || p.spp <= 0 ||
+        p.max_depth < 0 || p.max_depth > S->cfg.max_depth || p.spectral_mode != FL_SPECTRAL_HERO4) {
+        set_error(S->ctx, "invalid job (hero-wavelength mode, depth within the server's max_depth)");
+        return FL_ERR_INVALID;
+    }
+    auto hj = std::make_unique<HostJob>();
+    hj->cam = c;
+    hj->params = p;
+    hj->scene = job->scene_id;
+    const uint64_t film = (uint64_t)c.width * c.height * 3 * (sizeof(double) + sizeof(float));
+    const uint64_t samples = (uint64_t)c.width * c.height * (uint64_t)p.spp;
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        if (!S->sched.has_scene(job->scene_id)) {
+            set_error(S->ctx, "unknown scene id");
+            return FL_ERR_INVALID;
+        }
+        const uint64_t id = S->next_job++;
+        hj->submit_ms = S->now_ms();
+        S->jobs[id] = std::move(hj);
+        S->sched.submit(id, job->scene_id, film, samples);
+        S->stats.jobs_submitted++;
+        *job_id = id;
+    }
+    S->cv_work.notify_one();
+    return FL_OK;
+}
+
+static fl_status collect(Server *S, uint64_t job_id, float *film_rgb, double *film_xyz64, fl_job_stats *st) {
+    auto it = S->jobs.find(job_id);
+    if (it == S->jobs.end()) return FL_ERR_INVALID;
+    HostJob &j = *it->second;
+    if (j.status == FL_ERR_NOT_READY) return FL_ERR_NOT_READY;
+    if (st) {
+        st->submit_ms = j.submit_ms;
+        st->start_ms = j.start_ms;
+        st->done_ms = j.done_ms;
+        st->samples = (uint64_t)j.cam.width * j.cam.height * (uint64_t)j.params.spp;
+    }
+    const fl_status rc = j.status;
+    if (rc == FL_OK) {
+        if (film_rgb) std::memcpy(film_rgb, j.rgb.data(), j.rgb.size() * sizeof(float));
+        if (film_xyz64) std::memcpy(film_xyz64, j.xyz.data(), j.xyz.size() * sizeof(double));
+    }
+    S->jobs.erase(it);  // results are handed out once
+    return rc;
+}
+
+fl_status fl_server_poll(fl_server *srv, uint64_t job_id, float *film_rgb, double *film_xyz64, fl_job_stats *st) {
+    Server *S = reinterpret_cast<Server *>(srv);
+    if (!S) return FL_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(S->mu);
+    return collect(S, job_id, film_rgb, film_xyz64, st);
+}
+
+fl_status fl_server_wait(fl_server *srv, uint64_t job_id, int32_t timeout_ms, float *film_rgb, double *film_xyz64,
+                         fl_job_stats *st) {
+    Server *S = reinterpret_cast<Server *>(srv);
+    if (!S) return FL_ERR_INVALID;
+    std::unique_lock<std::mutex> lock(S->mu);
+    auto ready = [&] {
+        auto it = S->jobs.find(job_id);
+        return it == S->jobs.end() || it->second->status != FL_ERR_NOT_READY;
+    };
+    if (timeout_ms < 0) S->cv_done.wait(lock, ready);
+    else if (!S->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready)) return FL_ERR_TIMEOUT;
+    return collect(S, job_id, film_rgb, film_xyz64, st);
+}
+
+fl_status fl_server_get_stats(fl_server *srv, fl_server_stats *st) {
+    Server *S = reinterpret_cast<Server *>(srv);
+    if (!S || !st) return FL_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(S->mu);
+    *st = S->stats;
+    st->resident_bytes = S->sched.used();
+    st->running = (uint32_t)S->sched.running();
+    st->pending = (uint32_t)S->sched.pending();
+    return S->error.empty() ? FL_OK : FL_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,178 @@
+// Serving scheduler (host only, no CUDA): admission of render jobs by memory footprint,
+// scene residency with least-recently-used eviction, and the planning of shared waves.
+//
+// Policy:
+//  - Jobs are admitted first come, first served while (a) fewer than max_jobs run and
+//    (b) the job's film plus, when its scene is not resident, the scene fit the memory
+//    budget. To make room, resident scenes that no running or admitted job uses are
+//    evicted, least recently used first. The queue head blocks later jobs (no reordering),
+//    so admission order is arrival order. A job that could never fit is rejected.
+//  - Each wave splits its path slots over the running jobs by water-filling: jobs with
+//    fewer remaining samples than an equal share get all of them, the rest share what is
+//    left equally. Each job gets at most one contiguous sample range per wave, so its
+//    per-sample random streams do not depend on how it was batched.
+//  - A job is complete when all its samples were dispatched and the wave that carried its
+//    last samples has finished.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <vector>
+
+namespace fl {
+
+class ServeScheduler {
+public:
+    struct Seg {
+        uint64_t job;
+        uint32_t count;
+        uint64_t sample_base;
+    };
+    struct Admission {
+        std::vector<uint64_t> admitted;  // jobs that start running
+        std::vector<uint64_t> build;     // scenes to make resident (before the admitted jobs run)
+        std::vector<uint64_t> evict;     // scenes to release
+        std::vector<uint64_t> rejected;  // jobs that can never fit the budget
+    };
+
+    ServeScheduler(uint64_t budget_bytes, int max_jobs) : budget_(budget_bytes), max_jobs_(max_jobs) {}
+
+    void add_scene(uint64_t id, uint64_t bytes) { scenes_[id] = SceneState{bytes, false, 0, 0}; }
+    bool has_scene(uint64_t id) const { return scenes_.count(id) != 0; }
+    bool scene_resident(uint64_t id) const {
+        auto it = scenes_.find(id);
+        return it != scenes_.end() && it->second.resident;
+    }
+
+    void submit(uint64_t job, uint64_t scene, uint64_t film_bytes, uint64_t total_samples) {
+        jobs_[job] = JobState{scene, film_bytes, total_samples, 0, false, false};
+        pending_.push_back(job);
+    }
+
+    Admission admit() {
+        Admission a;
+        while (!pending_.empty() && (int)running_.size() < max_jobs_) {
+            const uint64_t j = pending_.front();
+            JobState &js = jobs_[j];
+            SceneState &sc = scenes_[js.scene];
+            const uint64_t need = js.film_bytes + (sc.resident ? 0 : sc.bytes);
+            if (need > budget_) {  // can never fit, even with every scene evicted
+                a.rejected.push_back(j);
+                pending_.pop_front();
+                jobs_.erase(j);
+                continue;
+            }
+            if (used_ + need > budget_) {
+                // evict idle resident scenes, least recently used first
+                std::vector<std::pair<uint64_t, uint64_t>> idle;  // (last_use, scene)
+                for (auto &kv : scenes_)
+                    if (kv.second.resident && kv.second.users == 0 && kv.first != js.scene)
+                        idle.push_back({kv.second.last_use, kv.first});
+                std::sort(idle.begin(), idle.end());
+                uint64_t freeable = 0;
+                for (auto &p : idle) freeable += scenes_[p.second].bytes;
+                if (used_ + need > budget_ + freeable) break;  // wait for running jobs to finish
+                for (auto &p : idle) {
+                    if (used_ + need <= budget_) break;
+                    SceneState &ev = scenes_[p.second];
+                    ev.resident = false;
+                    used_ -= ev.bytes;
+                    a.evict.push_back(p.second);
+                }
+            }
+            if (!sc.resident) {
+                sc.resident = true;
+                used_ += sc.bytes;
+                a.build.push_back(js.scene);
+            }
+            used_ += js.film_bytes;
+            sc.users += 1;
+            sc.last_use = ++clock_;
+            js.running = true;
+            running_.push_back(j);
+            a.admitted.push_back(j);
+            pending_.pop_front();
+        }
+        return a;
+    }
+
+    // Splits `cap` slots over running jobs that still have samples to dispatch.
+    std::vector<Seg> plan_wave(uint32_t cap) {
+        std::vector<std::pair<uint64_t, uint64_t>> want;  // (remaining, job)
+        for (uint64_t j : running_) {
+            const JobState &js = jobs_[j];
+            if (js.dispatched < js.total) want.push_back({js.total - js.dispatched, j});
+        }
+        std::sort(want.begin(), want.end());
+        std::vector<Seg> segs;
+        uint64_t left = cap;
+        size_t n = want.size();
+        for (size_t i = 0; i < want.size() && left > 0; ++i, --n) {
+            const uint64_t share = left / n;
+            const uint64_t give = std::min<uint64_t>(want[i].first, std::max<uint64_t>(share, 1));
+            if (give == 0) continue;
+            JobState &js = jobs_[want[i].second];
+            segs.push_back(Seg{want[i].second, (uint32_t)give, js.dispatched});
+            js.dispatched += give;
+            left -= give;
+        }
+        // keep admission (arrival) order inside the wave
+        std::sort(segs.begin(), segs.end(), [&](const Seg &a, const Seg &b) { return order(a.job) < order(b.job); });
+        return segs;
+    }
+
+    // Called when the last planned wave has finished: returns the jobs now complete and
+    // releases their film and their hold on the scene.
+    std::vector<uint64_t> finish_wave() {
+        std::vector<uint64_t> done;
+        for (auto it = running_.begin(); it != running_.end();) {
+            JobState &js = jobs_[*it];
+            if (js.dispatched >= js.total) {
+                done.push_back(*it);
+                used_ -= js.film_bytes;
+                SceneState &sc = scenes_[js.scene];
+                sc.users -= 1;
+                sc.last_use = ++clock_;
+                jobs_.erase(*it);
+                it = running_.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        return done;
+    }
+
+    uint64_t used() const { return used_; }
+    size_t running() const { return running_.size(); }
+    size_t pending() const { return pending_.size(); }
+    bool idle() const { return running_.empty() && pending_.empty(); }
+    const std::vector<uint64_t> &running_jobs() const { return running_; }
+
+private:
+    struct SceneState {
+        uint64_t bytes;
+        bool resident;
+        uint64_t last_use;
+        int users;
+    };
+    struct JobState {
+        uint64_t scene, film_bytes, total, dispatched;
+        bool running, done;
+    };
+    size_t order(uint64_t j) const {
+        return (size_t)(std::find(running_.begin(), running_.end(), j) - running_.begin());
+    }
+
+    uint64_t budget_;
+    int max_jobs_;
+    uint64_t used_ = 0;
+    uint64_t clock_ = 0;
+    std::map<uint64_t, SceneState> scenes_;
+    std::map<uint64_t, JobState> jobs_;
+    std::deque<uint64_t> pending_;
+    std::vector<uint64_t> running_;
+};
+
+}  // namespace fl

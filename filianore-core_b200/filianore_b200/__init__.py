@@ -22,7 +22,8 @@ TABLES_PATH = os.path.join(ROOT, "tests", "golden", "spectral_tables.npz")
 EXPORTED = [
     "fl_context_create", "fl_context_destroy", "fl_status_string", "fl_last_error", "fl_context_binned_tables",
     "fl_scene_create", "fl_scene_destroy", "fl_scene_get_info", "fl_trace_closest", "fl_trace_occluded",
-    "fl_trace_count", "fl_render", "fl_render_noalloc",
+    "fl_trace_count", "fl_render", "fl_render_noalloc", "fl_server_create", "fl_server_destroy",
+    "fl_server_add_scene", "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_get_stats",
 ]
 
 _lib = None
@@ -62,6 +63,13 @@ def lib():
         L.fl_trace_count.argtypes = [vp, vp, vp, C.c_uint32, C.c_int32, P(C.c_uint64), P(C.c_uint64)]
         L.fl_render.argtypes = [vp, P(T.fl_camera), P(T.fl_render_params), vp, vp, C.c_int32, P(T.fl_render_stats)]
         L.fl_render_noalloc.argtypes = [vp, P(T.fl_camera), P(T.fl_render_params), vp, vp, P(T.fl_render_stats)]
+        L.fl_server_create.argtypes = [vp, P(T.fl_server_config), P(vp)]
+        L.fl_server_destroy.argtypes = [vp]
+        L.fl_server_add_scene.argtypes = [vp, P(T.fl_scene_desc), P(C.c_uint64)]
+        L.fl_server_submit.argtypes = [vp, P(T.fl_job_desc), P(C.c_uint64)]
+        L.fl_server_poll.argtypes = [vp, C.c_uint64, vp, vp, P(T.fl_job_stats)]
+        L.fl_server_wait.argtypes = [vp, C.c_uint64, C.c_int32, vp, vp, P(T.fl_job_stats)]
+        L.fl_server_get_stats.argtypes = [vp, P(T.fl_server_stats)]
         for name in EXPORTED:
             if name not in ("fl_status_string",):
                 getattr(L, name).restype = C.c_int32
@@ -217,3 +225,59 @@ class SceneHandle:
         check(lib().fl_render(self.h, C.byref(cam), C.byref(params), _ptr(film_rgb), xyz, mem, C.byref(stats)),
               self.ctx.h)
         return film_rgb, {k: getattr(stats, k) for k, _ in T.fl_render_stats._fields_}
+
+
+class Server:
+    """Continuous-batching render server (fl_server_*): scenes stay resident under a memory
+    budget, running jobs share every wave."""
+
+    def __init__(self, ctx: Context, budget_bytes: int, max_depth: int = 16, max_jobs: int = 32, max_lights: int = 8,
+                 wave_paths: int = 0):
+        self.ctx = ctx
+        self.h = None
+        cfg = T.fl_server_config(budget_bytes, wave_paths, max_depth, max_jobs, max_lights)
+        h = C.c_void_p()
+        check(lib().fl_server_create(ctx.h, C.byref(cfg), C.byref(h)), ctx.h)
+        self.h = h
+        self.shapes = {}
+
+    def close(self):
+        if self.h:
+            lib().fl_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, sc) -> int:
+        desc, keep = sc.desc()
+        sid = C.c_uint64()
+        check(lib().fl_server_add_scene(self.h, C.byref(desc), C.byref(sid)), self.ctx.h)
+        return sid.value
+
+    def submit(self, scene_id: int, camera, params) -> int:
+        job = T.fl_job_desc(scene_id, camera, params)
+        jid = C.c_uint64()
+        check(lib().fl_server_submit(self.h, C.byref(job), C.byref(jid)), self.ctx.h)
+        self.shapes[jid.value] = (camera.height, camera.width)
+        return jid.value
+
+    def wait(self, job_id: int, timeout_ms: int = -1, want_xyz: bool = False):
+        H, W = self.shapes.pop(job_id)
+        rgb = np.zeros((H, W, 3), np.float32)
+        xyz = np.zeros((H, W, 3), np.float64) if want_xyz else None
+        st = T.fl_job_stats()
+        rc = lib().fl_server_wait(self.h, job_id, timeout_ms, _ptr(rgb), _ptr(xyz) if xyz is not None else None,
+                                  C.byref(st))
+        if rc != 0:
+            self.shapes[job_id] = (H, W)
+        check(rc, self.ctx.h)
+        return rgb, xyz, {k: getattr(st, k) for k, _ in T.fl_job_stats._fields_}
+
+    def stats(self):
+        st = T.fl_server_stats()
+        lib().fl_server_get_stats(self.h, C.byref(st))
+        return {k: getattr(st, k) for k, _ in T.fl_server_stats._fields_}

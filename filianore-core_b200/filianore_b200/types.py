@@ -137,3 +137,30 @@ class fl_render_stats(C.Structure):
 
 
 HIT_DTYPE = [("id", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")]
+
+
+class fl_server_config(C.Structure):
+    _fields_ = [
+        ("memory_budget_bytes", C.c_uint64),
+        ("wave_paths", C.c_int32),
+        ("max_depth", C.c_int32),
+        ("max_jobs", C.c_int32),
+        ("max_lights", C.c_int32),
+    ]
+
+
+class fl_job_desc(C.Structure):
+    _fields_ = [("scene_id", C.c_uint64), ("camera", fl_camera), ("params", fl_render_params)]
+
+
+class fl_job_stats(C.Structure):
+    _fields_ = [("submit_ms", C.c_double), ("start_ms", C.c_double), ("done_ms", C.c_double),
+                ("samples", C.c_uint64)]
+
+
+class fl_server_stats(C.Structure):
+    _fields_ = [
+        ("jobs_submitted", C.c_uint64), ("jobs_done", C.c_uint64), ("waves", C.c_uint64), ("paths", C.c_uint64),
+        ("builds", C.c_uint64), ("evictions", C.c_uint64), ("resident_bytes", C.c_uint64),
+        ("running", C.c_uint32), ("pending", C.c_uint32),
+    ]

@@ -251,6 +251,54 @@ typedef struct {
 FL_API fl_status fl_render(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
                     float *film_rgb, double *film_xyz64, int32_t memory, fl_render_stats *stats);
 
+/* ------------------------------------------------------------------------- */
+/* Serving: continuous batching of render jobs (no counterpart in the reference) */
+/* ------------------------------------------------------------------------- */
+/* A server keeps registered scenes resident in HBM under a memory budget (least recently
+ * used idle scenes are evicted and rebuilt on demand), admits jobs in arrival order as
+ * films and scenes fit, and renders the running jobs' samples together: every wave's path
+ * slots are split over the running jobs and run through the same kernels. A job's image is
+ * the one fl_render gives for the same scene, camera and parameters (hero mode). */
+typedef struct fl_server fl_server;
+
+typedef struct {
+    uint64_t memory_budget_bytes; /* resident scenes + films of running jobs */
+    int32_t wave_paths;           /* path slots per wave shared by running jobs (0 = 2^21) */
+    int32_t max_depth;            /* deepest job accepted; each wave runs this many bounces */
+    int32_t max_jobs;             /* jobs running at once, 1..64 */
+    int32_t max_lights;           /* most lights any scene may have, 0..64 */
+} fl_server_config;
+
+typedef struct {
+    uint64_t scene_id;
+    fl_camera camera;
+    fl_render_params params;      /* spectral_mode must be FL_SPECTRAL_HERO4 */
+} fl_job_desc;
+
+typedef struct {
+    double submit_ms, start_ms, done_ms;  /* server clock: submission, admission, image ready */
+    uint64_t samples;
+} fl_job_stats;
+
+typedef struct {
+    uint64_t jobs_submitted, jobs_done, waves, paths, builds, evictions, resident_bytes;
+    uint32_t running, pending;
+} fl_server_stats;
+
+FL_API fl_status fl_server_create(fl_context *ctx, const fl_server_config *cfg, fl_server **out);
+FL_API fl_status fl_server_destroy(fl_server *srv);
+/* copies the scene description; the scene is built on the device when a job needs it */
+FL_API fl_status fl_server_add_scene(fl_server *srv, const fl_scene_desc *desc, uint64_t *scene_id);
+FL_API fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job_id);
+/* FL_OK and the films (host buffers, nullable) once the job is done, FL_ERR_NOT_READY before;
+ * FL_ERR_CAPACITY for a job that can never fit the budget. Results are handed out once. */
+FL_API fl_status fl_server_poll(fl_server *srv, uint64_t job_id, float *film_rgb, double *film_xyz64,
+                                fl_job_stats *stats);
+/* as fl_server_poll, blocking up to timeout_ms (< 0: no limit); FL_ERR_TIMEOUT when it runs out */
+FL_API fl_status fl_server_wait(fl_server *srv, uint64_t job_id, int32_t timeout_ms, float *film_rgb,
+                                double *film_xyz64, fl_job_stats *stats);
+FL_API fl_status fl_server_get_stats(fl_server *srv, fl_server_stats *stats);
+
 /* fl_render_noalloc: fl_render for callers that cannot allocate device memory while they
  * render (an application that owns and budgets all device memory, or code that must not
  * trigger the implicit device synchronisation of cudaMalloc). It has no counterpart in the

@@ -1,0 +1,54 @@
+// Drives the serving scheduler (filianore-core_b200/csrc/fl_serve_sched.h) through fixed
+// scenarios and prints the decisions as text for tests/test_serve_sched.py.
+#include <cstdio>
+
+#include "../filianore-core_b200/csrc/fl_serve_sched.h"
+
+using fl::ServeScheduler;
+
+static void print_adm(const char *tag, const ServeScheduler::Admission &a) {
+    std::printf("%s admitted", tag);
+    for (auto j : a.admitted) std::printf(" %llu", (unsigned long long)j);
+    std::printf(" | build");
+    for (auto s : a.build) std::printf(" %llu", (unsigned long long)s);
+    std::printf(" | evict");
+    for (auto s : a.evict) std::printf(" %llu", (unsigned long long)s);
+    std::printf(" | rejected");
+    for (auto j : a.rejected) std::printf(" %llu", (unsigned long long)j);
+    std::printf("\n");
+}
+
+static void print_plan(const char *tag, const std::vector<ServeScheduler::Seg> &p) {
+    std::printf("%s", tag);
+    for (auto &s : p) std::printf(" %llu:%u@%llu", (unsigned long long)s.job, s.count, (unsigned long long)s.sample_base);
+    std::printf("\n");
+}
+
+int main() {
+    // budget 1000: scenes 1 (400 B), 2 (500 B), 3 (300 B); films of 100 B
+    ServeScheduler s(1000, 2);
+    s.add_scene(1, 400);
+    s.add_scene(2, 500);
+    s.add_scene(3, 300);
+    s.submit(10, 1, 100, 250);   // job 10 on scene 1, 250 samples
+    s.submit(11, 2, 100, 100);   // job 11 on scene 2
+    s.submit(12, 3, 100, 50);    // job 12 on scene 3: must wait (max_jobs 2 and memory)
+    s.submit(13, 1, 2000, 10);   // job 13 can never fit
+    print_adm("A1", s.admit());
+    std::printf("used %llu\n", (unsigned long long)s.used());
+    print_plan("P1", s.plan_wave(256));
+    print_plan("P2", s.plan_wave(256));
+    auto d = s.finish_wave();
+    std::printf("done");
+    for (auto j : d) std::printf(" %llu", (unsigned long long)j);
+    std::printf("\n");
+    print_adm("A2", s.admit());
+    print_plan("P3", s.plan_wave(256));
+    d = s.finish_wave();
+    std::printf("done");
+    for (auto j : d) std::printf(" %llu", (unsigned long long)j);
+    std::printf("\n");
+    print_adm("A3", s.admit());
+    std::printf("used %llu idle %d\n", (unsigned long long)s.used(), (int)s.idle());
+    return 0;
+}

@@ -1,0 +1,35 @@
+"""Host-side policy of the render server (no GPU): admission in arrival order by memory
+footprint, LRU eviction of idle scenes, rejection of jobs that can never fit, and the
+water-filling split of wave slots."""
+import os
+import subprocess
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def run_driver():
+    exe = os.path.join(tempfile.mkdtemp(), "serve_sched_check")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-o", exe, os.path.join(HERE, "serve_sched_check.cpp")], check=True)
+    return subprocess.run([exe], check=True, capture_output=True, text=True).stdout.splitlines()
+
+
+def test_scheduler_decisions():
+    out = run_driver()
+    # budget 1000: scene 1 (400) + film (100) fits; job 11 would need scene 2 (500) + film
+    # on top of that (1100 > 1000), so it waits and blocks the queue behind it
+    assert out[0] == "A1 admitted 10 | build 1 | evict | rejected"
+    assert out[1] == "used 500"
+    # a single running job gets the whole wave until all its samples are dispatched
+    assert out[2] == "P1 10:250@0"
+    assert out[3] == "P2"
+    assert out[4] == "done 10"
+    # scene 1 is now idle and is evicted (least recently used) to make room for scenes 2
+    # and 3; max_jobs = 2 stops admission before job 13
+    assert out[5] == "A2 admitted 11 12 | build 2 3 | evict 1 | rejected"
+    # water-filling: job 12 (50 samples) gets all of its samples, job 11 the rest
+    assert out[6] == "P3 11:100@0 12:50@0"
+    assert out[7] == "done 11 12"
+    # job 13's film alone exceeds the budget: rejected when it reaches the queue head
+    assert out[8] == "A3 admitted | build | evict | rejected 13"
+    assert out[9] == "used 800 idle 1"
