@@ -163,6 +163,123 @@ def cpu_raycast(steps, warmup):
                       f"(oracle binned-SAH BVH, build {build_s:.1f} s not timed)"}
 
 
+def serve_scene_pool(n_scenes=12, seed=11):
+    """procedural sphere scenes with triangle counts log-uniform in [10k, 4M]"""
+    from filianore_b200 import scenes
+    rng = np.random.default_rng(seed)
+    pool = []
+    for k in range(n_scenes):
+        target = float(np.exp(rng.uniform(np.log(1e4), np.log(4e6))))
+        slices, stacks = (128, 65) if target >= 16384 * 8 else (32, 17)
+        per = 2 * slices * (stacks - 1)
+        n_sph = max(1, int(round(target / per)))
+        pool.append(scenes.procedural_spheres(n_sph, slices, stacks, 256, 256, seed=100 + k,
+                                              extent=max(3.0, 10.0 * (n_sph / 64) ** 0.5)))
+    return pool
+
+
+def gpu_serve(args, world, rank, local, barrier, reduce_max):
+    """200 requests at 80% of the measured one-job-at-a-time capacity (Poisson arrivals):
+    the continuous-batching server against the plain GPU path serving one job at a time."""
+    import threading
+    import torch
+    import filianore_b200 as fb
+    from filianore_b200 import scenes
+    rng = np.random.default_rng(5)
+    pool = serve_scene_pool()
+    n_req = 200
+    reqs = []
+    for i in range(n_req):
+        sc = int(rng.integers(len(pool)))
+        res = int(rng.choice([128, 256, 512, 1024]))
+        spp = max(1, int(round(float(np.exp(rng.uniform(0.0, np.log(256.0)))))))
+        reqs.append((sc, res, spp))
+    ctx = fb.Context(local)
+    # plain GPU path, one job at a time, scenes resident: service time of every request
+    handles = [ctx.scene(sc) for sc in pool]
+    for h in handles[:2]:
+        h.render(scenes.render_params(1, 16), camera=h.src.camera_struct(64, 64))
+    service = []
+    samples = 0
+    for sc, res, spp in reqs:
+        cam = pool[sc].camera_struct(res, res)
+        t0 = time.perf_counter()
+        handles[sc].render(scenes.render_params(spp, 16, fb.FL_SPECTRAL_HERO4), camera=cam)
+        service.append(time.perf_counter() - t0)
+        samples += res * res * spp
+    for h in handles:
+        h.close()
+    mean_s = float(np.mean(service))
+    lam = 0.8 / mean_s
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, n_req))
+    # serial FIFO with the measured service times
+    t, serial_tti = 0.0, []
+    for a, s in zip(arrivals, service):
+        start = max(a, t)
+        t = start + s
+        serial_tti.append(t - a)
+    serial_makespan = t - arrivals[0]
+    budget = int(sum(sc.n_tri for sc in pool) * 132 * 0.6) + (2 << 30)
+    p = lambda v, q: float(np.percentile(np.asarray(v) * 1e3, q))  # noqa: E731
+
+    def run_server(policy):
+        # the server, driven in real time by the same arrivals
+        srv = fb.Server(ctx, budget_bytes=budget, max_depth=16, max_jobs=64, max_lights=4, policy=policy)
+        ids = [srv.add_scene(sc) for sc in pool]
+        job_ids = [None] * n_req
+        t_start = time.perf_counter()
+
+        def submitter():
+            for i, (sc, res, spp) in enumerate(reqs):
+                delay = arrivals[i] - (time.perf_counter() - t_start)
+                if delay > 0:
+                    time.sleep(delay)
+                job_ids[i] = srv.submit(ids[sc], pool[sc].camera_struct(res, res),
+                                        scenes.render_params(spp, 16, fb.FL_SPECTRAL_HERO4))
+        th = threading.Thread(target=submitter)
+        th.start()
+        tti, rows = [], []
+        last_done, first_submit = 0.0, None
+        for i in range(n_req):
+            while job_ids[i] is None:
+                time.sleep(0.0005)
+            _, _, st = srv.wait(job_ids[i], timeout_ms=600000)
+            tti.append((st["done_ms"] - st["submit_ms"]) / 1e3)
+            rows.append((tti[-1], i, st))
+            last_done = max(last_done, st["done_ms"])
+            first_submit = st["submit_ms"] if first_submit is None else min(first_submit, st["submit_ms"])
+        th.join()
+        sstats = srv.stats()
+        srv.close()
+        rows.sort(key=lambda r: -r[0])
+        slowest = [{"req": i, "samples": st["samples"], "tris": pool[reqs[i][0]].n_tri, "res": reqs[i][1],
+                    "spp": reqs[i][2], "queued_ms": round(st["start_ms"] - st["submit_ms"], 1),
+                    "tti_ms": round(t * 1e3, 1), "alone_ms": round(service[i] * 1e3, 1)} for t, i, st in rows[:4]]
+        makespan = (last_done - first_submit) / 1e3
+        return {"p50_ms": round(p(tti, 50), 2), "p99_ms": round(p(tti, 99), 2),
+                "samples_per_s": round(samples / makespan, 1), "server": sstats, "slowest": slowest}
+
+    results = {name: run_server(pol) for name, pol in (("shortest_first", fb.FL_SERVE_SHORTEST_FIRST),
+                                                        ("first_come", fb.FL_SERVE_FIRST_COME),
+                                                        ("fair_share", fb.FL_SERVE_FAIR_SHARE))}
+    ctx.close()
+    best = results["shortest_first"]
+    return {"metric": "p99 time-to-image", "value": best["p99_ms"], "unit": "ms", "n_gpus": world,
+            "steps": n_req, "warmup": 2, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "serve: 200 Poisson requests at 80% of the measured one-job-at-a-time capacity; "
+                                   "scenes from a pool of 12 procedural sphere scenes with triangle counts "
+                                   "log-uniform in [10k, 4M]; resolution in {128^2..1024^2}; spp log-uniform "
+                                   "in [1, 256]; depth 16; hero wavelengths",
+                       "scene_tris": [sc.n_tri for sc in pool], "memory_budget_bytes": budget,
+                       "arrival_rate_per_s": round(lam, 3), "parallelism": "1 GPU"},
+            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "samples_per_s": best["samples_per_s"],
+            "serial": {"p50_ms": round(p(serial_tti, 50), 2), "p99_ms": round(p(serial_tti, 99), 2),
+                       "samples_per_s": round(samples / serial_makespan, 1),
+                       "mean_service_ms": round(mean_s * 1e3, 3)},
+            "policies": results}
+
+
 def config_of(workload, world):
     if workload == "render":
         return {"workload": "render: procedural 1,048,578-triangle scene (64 displaced spheres, Lambert / GGX "
@@ -211,8 +328,11 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record()
     stats = []
-    for _ in range(args.steps):
-        stats.append(frame(params(fb.FL_RENDER_PROFILE, rank * RENDER["spp"])))
+    # the last timed frame also times every kernel launch with CUDA events (roofline); the
+    # others replay the per-wave CUDA graph
+    for k in range(args.steps):
+        flags = fb.FL_RENDER_PROFILE if k == args.steps - 1 else 0
+        stats.append(frame(params(flags, rank * RENDER["spp"])))
     t_end.record()
     barrier()
     clk = clocks.stop()
@@ -242,16 +362,17 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
            "note": "scene resident in HBM; camera and parameters travel as kernel arguments"}
 
     peaks = load_peaks()
-    trav_ms = statistics.mean(s["ms_trace"] + s["ms_shadow"] for s in stats)
+    prof = stats[-1]
+    trav_ms = prof["ms_trace"] + prof["ms_shadow"]
     alg_bytes = cstats["rays"] * (RAY_BYTES + HIT_BYTES) + NODE_BYTES * cstats["nodes_visited"] + \
         TRI_BYTES * cstats["tris_tested"]
     achieved = alg_bytes / (trav_ms / 1e3) / 1e9
-    share = {k: round(statistics.mean(s[f"ms_{k}"] for s in stats) / statistics.mean(s["ms"] for s in stats), 4)
-             for k in ("trace", "shade", "shadow", "continue")}
+    share = {k: round(prof[f"ms_{k}"] / prof["ms"], 4) for k in ("trace", "shade", "shadow", "continue")}
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None, "peak_src": peaks["src"],
                 "kernel": "BVH traversal (k_trace_paths + k_trace_rays2)",
                 "alg_bytes_per_frame": int(alg_bytes), "traversal_ms_per_frame": round(trav_ms, 3),
+                "profiled_frame_ms": round(prof["ms"], 3),
                 "nodes_per_ray": round(cstats["nodes_visited"] / cstats["rays"], 2),
                 "tris_per_ray": round(cstats["tris_tested"] / cstats["rays"], 2), "time_share": share}
     line = {"metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "samples_per_s": round(samples_per_s, 1),
@@ -343,7 +464,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="render", choices=["render", "raycast"])
+    ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -384,10 +505,10 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    run = gpu_render if args.workload == "render" else gpu_raycast
+    run = {"render": gpu_render, "raycast": gpu_raycast, "serve": gpu_serve}[args.workload]
     line = run(args, world, rank, local, barrier, reduce_max)
     if rank == 0:
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and args.workload != "serve":
             line["cpu_baseline"] = (cpu_render(2, 0) if args.workload == "render" else cpu_raycast(3, 1))
         print(json.dumps(line), flush=True)
     if world > 1:

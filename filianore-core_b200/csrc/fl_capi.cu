@@ -32,6 +32,11 @@ fl_status cuda_status(Context *ctx, cudaError_t e, const char *what) {
 
 fl_status ensure_scratch(Context *ctx, size_t bytes, void **out) {
     if (bytes > ctx->scratch_bytes) {
+        if (ctx->wave_graph) {  // captured against the old buffer
+            cudaGraphExecDestroy(ctx->wave_graph);
+            ctx->wave_graph = nullptr;
+            ctx->graph_base = nullptr;
+        }
         if (ctx->scratch) {
             cudaStreamSynchronize(ctx->stream);
             cudaFree(ctx->scratch);
@@ -226,6 +231,8 @@ fl_status fl_context_destroy(fl_context *ctx_h) {
     if (!ctx) return FL_ERR_INVALID;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
+    if (ctx->wave_graph) cudaGraphExecDestroy(ctx->wave_graph);
     cudaFree(ctx->scratch);
     cudaFree(ctx->film_scratch);
     cudaFree(ctx->d_error);

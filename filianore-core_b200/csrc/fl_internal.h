@@ -39,6 +39,12 @@ struct Context {
     size_t scratch_bytes = 0;
     void *film_scratch = nullptr;       // render films (separate from the wave scratch)
     size_t film_bytes = 0;
+    std::vector<cudaEvent_t> events;    // reusable timing events (FL_RENDER_PROFILE)
+    // one wave's launch sequence captured as a CUDA graph, with what it was captured for
+    cudaGraphExec_t wave_graph = nullptr;
+    const void *graph_base = nullptr;
+    size_t graph_cap = 0;
+    int graph_depth = -1, graph_nl_mode = -1, graph_count = -1;
     int *d_error = nullptr;             // traversal error counter
     unsigned long long *d_counters = nullptr;  // 8 x u64 statistics
 };

@@ -84,6 +84,7 @@ extern "C" fl_status fl_render(fl_scene *scene_h, const fl_camera *camera, const
     WaveCounters hc{};
     RenderProfile prof;
     prof.on = (p.flags & FL_RENDER_PROFILE) != 0;
+    prof.pool = &ctx->events;
     rc = p.spectral_mode == FL_SPECTRAL_BINS60 ? render_waves<60>(s, cam, p, d_xyz, &hc, &prof, st)
                                                : render_waves<4>(s, cam, p, d_xyz, &hc, &prof, st);
     if (rc) {

@@ -43,15 +43,25 @@ struct WaveCounters {
     int pad[3];
 };
 
-// FL_RENDER_PROFILE: CUDA events bracketing every launch, grouped by kernel class
+// FL_RENDER_PROFILE: CUDA events bracketing every launch, grouped by kernel class. The
+// events come from a pool owned by the context and are reused by later renders.
 struct RenderProfile {
     bool on = false;
+    std::vector<cudaEvent_t> *pool = nullptr;
+    size_t used = 0;
     std::vector<cudaEvent_t> ev[4];  // pairs (start, stop) per class: trace, shade, shadow, continue
     uint32_t launches = 0;
     void mark(int cls, cudaStream_t st) {
-        if (!on) return;
-        cudaEvent_t e;
-        cudaEventCreate(&e);
+        if (!on || !pool) return;
+        if (used == pool->size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                on = false;
+                return;
+            }
+            pool->push_back(e);
+        }
+        cudaEvent_t e = (*pool)[used++];
         cudaEventRecord(e, st);
         ev[cls].push_back(e);
     }
@@ -64,10 +74,6 @@ struct RenderProfile {
                 ms[c] += t;
             }
         }
-    }
-    ~RenderProfile() {
-        for (auto &v : ev)
-            for (cudaEvent_t e : v) cudaEventDestroy(e);
     }
 };
 
@@ -924,6 +930,33 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     const bool count = (p.flags & FL_RENDER_COUNT) != 0;
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
     const size_t desc_bytes = offsetof(WaveDesc, seg) + sizeof(WaveSeg);
+    // Replay one captured graph per wave: a depth-16 wave is ~85 launches, and its late
+    // bounces have so few paths that launching dominates. Not used by the allocation-free
+    // path (instantiating a graph allocates) nor when every launch is timed with events.
+    const bool use_graph = !fixed_scratch && !prof->on;
+    if (use_graph && (!ctx->wave_graph || ctx->graph_base != W.A.cnt || ctx->graph_cap != W.cap ||
+                      ctx->graph_depth != p.max_depth || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count)) {
+        if (ctx->wave_graph) {
+            cudaGraphExecDestroy(ctx->wave_graph);
+            ctx->wave_graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        RenderProfile off;
+        FL_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        enqueue_wave<NL>(W, p.max_depth, count, &off, sms, st);
+        FL_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
+        cudaError_t e = cudaGraphInstantiate(&ctx->wave_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            ctx->wave_graph = nullptr;
+            return cuda_status(ctx, e, "wave graph instantiation");
+        }
+        ctx->graph_base = W.A.cnt;
+        ctx->graph_cap = W.cap;
+        ctx->graph_depth = p.max_depth;
+        ctx->graph_nl_mode = NL;
+        ctx->graph_count = (int)count;
+    }
     for (unsigned long long wb = 0; wb < total; wb += W.cap) {
         WaveDesc d;
         d.n_wave = (uint32_t)std::min<unsigned long long>(W.cap, total - wb);
@@ -931,7 +964,12 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         d.seg[0] = WaveSeg{0u, 0u, d.n_wave, 0u, wb, 0ull};
         // pageable source: the copy is staged before the call returns, so `d` may be reused
         FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
-        enqueue_wave<NL>(W, p.max_depth, count, prof, sms, st);
+        if (use_graph) {
+            FL_CUDA_TRY(ctx, cudaGraphLaunch(ctx->wave_graph, st));
+            prof->launches += 1 + 5 * (uint32_t)p.max_depth + 4;
+        } else {
+            enqueue_wave<NL>(W, p.max_depth, count, prof, sms, st);
+        }
         FL_CUDA_TRY(ctx, cudaGetLastError());
     }
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, W.A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));

@@ -81,8 +81,31 @@ struct Server {
     std::chrono::steady_clock::time_point t0;
     fl_server_stats stats{};
     std::string error;
+    // device buffers of finished jobs, kept by size for the next jobs: cudaFree and
+    // cudaMalloc synchronise the device, which would stall the wave pipeline per job
+    std::multimap<size_t, void *> buffer_pool;
 
-    Server(uint64_t budget, int max_jobs) : sched(budget, max_jobs) {}
+    void *acquire(size_t bytes) {
+        auto it = buffer_pool.find(bytes);
+        if (it != buffer_pool.end()) {
+            void *p = it->second;
+            buffer_pool.erase(it);
+            return p;
+        }
+        void *p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return p;
+    }
+    void release(void *p, size_t bytes) {
+        if (!p) return;
+        if (buffer_pool.count(bytes) < 8) buffer_pool.insert({bytes, p});
+        else cudaFree(p);
+    }
+
+    Server(uint64_t budget, int max_jobs, int policy) : sched(budget, max_jobs, policy) {}
     double now_ms() const {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
@@ -114,11 +137,11 @@ void finish_job(Server *S, uint64_t jid, HostJob &job) {
     cudaMemcpyAsync(job.rgb.data(), job.d_rgb, n_pix * 3 * sizeof(float), cudaMemcpyDeviceToHost, S->stream);
     cudaMemcpyAsync(job.xyz.data(), job.d_film, n_pix * 3 * sizeof(double), cudaMemcpyDeviceToHost, S->stream);
     cudaError_t e = cudaStreamSynchronize(S->stream);
-    cudaFree(job.d_film);
-    cudaFree(job.d_rgb);
+    std::lock_guard<std::mutex> lock(S->mu);
+    S->release(job.d_film, n_pix * 3 * sizeof(double));
+    S->release(job.d_rgb, n_pix * 3 * sizeof(float));
     job.d_film = nullptr;
     job.d_rgb = nullptr;
-    std::lock_guard<std::mutex> lock(S->mu);
     job.status = e == cudaSuccess ? FL_OK : FL_ERR_CUDA;
     job.done_ms = S->now_ms();
     if (job.slot >= 0) S->free_slots.push_back(job.slot);
@@ -162,11 +185,13 @@ void worker_loop(Server *S) {
                 const size_t n_pix = (size_t)job.cam.width * job.cam.height;
                 HostScene &h = S->scenes[job.scene];
                 bool ok = h.dev != nullptr && !S->free_slots.empty();
-                if (ok && cudaMalloc(&job.d_film, n_pix * 3 * sizeof(double)) != cudaSuccess) ok = false;
-                if (ok && cudaMalloc(&job.d_rgb, n_pix * 3 * sizeof(float)) != cudaSuccess) ok = false;
+                if (ok) job.d_film = static_cast<double *>(S->acquire(n_pix * 3 * sizeof(double)));
+                if (ok) job.d_rgb = static_cast<float *>(S->acquire(n_pix * 3 * sizeof(float)));
+                if (!job.d_film || !job.d_rgb) ok = false;
                 if (!ok) {
-                    cudaGetLastError();
-                    cudaFree(job.d_film);
+                    S->release(job.d_film, n_pix * 3 * sizeof(double));
+                    S->release(job.d_rgb, n_pix * 3 * sizeof(float));
+                    job.d_rgb = nullptr;
                     job.d_film = nullptr;
                     job.fail = FL_ERR_OOM;  // the scheduler still runs it; its samples are skipped
                     continue;
@@ -198,9 +223,13 @@ void worker_loop(Server *S) {
                                 S->stream);
                 cudaMemcpyAsync(S->W.d_wave, &d, desc_head + sizeof(WaveSeg) * d.n_seg, cudaMemcpyHostToDevice,
                                 S->stream);
+                const auto w0 = std::chrono::steady_clock::now();
                 cudaGraphLaunch(S->graph, S->stream);
                 cudaError_t e = cudaStreamSynchronize(S->stream);
+                const double wave_ms =
+                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
                 std::lock_guard<std::mutex> lock(S->mu);
+                S->stats.busy_ms += wave_ms;
                 S->stats.waves++;
                 S->stats.paths += d.n_wave;
                 if (e != cudaSuccess) S->error = cudaGetErrorString(e);
@@ -242,11 +271,11 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     if (!ctx || !cfg || !out) return FL_ERR_INVALID;
     *out = nullptr;
     if (cfg->memory_budget_bytes == 0 || cfg->max_jobs <= 0 || cfg->max_jobs > kMaxJobs || cfg->max_depth < 0 ||
-        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64) {
+        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64 || cfg->policy < 0 || cfg->policy > 2) {
         set_error(ctx, "invalid server configuration");
         return FL_ERR_INVALID;
     }
-    auto S = std::make_unique<Server>(cfg->memory_budget_bytes, cfg->max_jobs);
+    auto S = std::make_unique<Server>(cfg->memory_budget_bytes, cfg->max_jobs, cfg->policy);
     S->ctx = ctx;
     S->cfg = *cfg;
     S->t0 = std::chrono::steady_clock::now();
@@ -306,6 +335,7 @@ fl_status fl_server_destroy(fl_server *srv) {
         cudaFree(kv.second->d_film);
         cudaFree(kv.second->d_rgb);
     }
+    for (auto &kv : S->buffer_pool) cudaFree(kv.second);
     for (auto &kv : S->scenes)
         if (kv.second.dev) fl_scene_destroy(reinterpret_cast<fl_scene *>(kv.second.dev));
     if (S->graph) cudaGraphExecDestroy(S->graph);

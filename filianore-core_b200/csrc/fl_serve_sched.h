@@ -7,9 +7,14 @@
 //    budget. To make room, resident scenes that no running or admitted job uses are
 //    evicted, least recently used first. The queue head blocks later jobs (no reordering),
 //    so admission order is arrival order. A job that could never fit is rejected.
-//  - Each wave splits its path slots over the running jobs by water-filling: jobs with
-//    fewer remaining samples than an equal share get all of them, the rest share what is
-//    left equally. Each job gets at most one contiguous sample range per wave, so its
+//  - Each wave is packed shortest-remaining-first (the default policy): running jobs are taken in order of
+//    the samples they still have to render and each takes as many of the wave's path
+//    slots as it can use. Small jobs finish within a wave or two; large jobs fill the
+//    rest of every wave, so the GPU stays full. (A simulation of this workload's Poisson
+//    load favoured this over first-come-first-served packing, equal sharing and a
+//    reserved share for the oldest job, at both the median and the 99th percentile.)
+//    The other policies are first come, first served packing and equal sharing
+//    (water-filling). Each job gets one contiguous sample range per wave, so its
 //    per-sample random streams do not depend on how it was batched.
 //  - A job is complete when all its samples were dispatched and the wave that carried its
 //    last samples has finished.
@@ -37,7 +42,10 @@ public:
         std::vector<uint64_t> rejected;  // jobs that can never fit the budget
     };
 
-    ServeScheduler(uint64_t budget_bytes, int max_jobs) : budget_(budget_bytes), max_jobs_(max_jobs) {}
+    enum Policy { kShortestFirst = 0, kFirstCome = 1, kFairShare = 2 };
+
+    ServeScheduler(uint64_t budget_bytes, int max_jobs, int policy = kShortestFirst)
+        : budget_(budget_bytes), max_jobs_(max_jobs), policy_(policy) {}
 
     void add_scene(uint64_t id, uint64_t bytes) { scenes_[id] = SceneState{bytes, false, 0, 0}; }
     bool has_scene(uint64_t id) const { return scenes_.count(id) != 0; }
@@ -105,18 +113,33 @@ public:
             const JobState &js = jobs_[j];
             if (js.dispatched < js.total) want.push_back({js.total - js.dispatched, j});
         }
-        std::sort(want.begin(), want.end());
         std::vector<Seg> segs;
         uint64_t left = cap;
-        size_t n = want.size();
-        for (size_t i = 0; i < want.size() && left > 0; ++i, --n) {
-            const uint64_t share = left / n;
-            const uint64_t give = std::min<uint64_t>(want[i].first, std::max<uint64_t>(share, 1));
-            if (give == 0) continue;
-            JobState &js = jobs_[want[i].second];
-            segs.push_back(Seg{want[i].second, (uint32_t)give, js.dispatched});
-            js.dispatched += give;
-            left -= give;
+        if (policy_ == kFairShare) {
+            // water-filling: jobs needing less than an equal share get all they need
+            std::sort(want.begin(), want.end());
+            size_t n = want.size();
+            for (size_t i = 0; i < want.size() && left > 0; ++i, --n) {
+                const uint64_t g = std::min<uint64_t>(want[i].first, std::max<uint64_t>(left / n, 1));
+                JobState &js = jobs_[want[i].second];
+                segs.push_back(Seg{want[i].second, (uint32_t)g, js.dispatched});
+                js.dispatched += g;
+                left -= g;
+            }
+        } else {
+            // shortest remaining first, or first come first served (running_ is in arrival order)
+            if (policy_ == kShortestFirst)
+                std::stable_sort(want.begin(), want.end(),
+                                 [](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
+                                     return a.first < b.first;
+                                 });
+            for (size_t i = 0; i < want.size() && left > 0; ++i) {
+                const uint64_t g = std::min<uint64_t>(want[i].first, left);
+                JobState &js = jobs_[want[i].second];
+                segs.push_back(Seg{want[i].second, (uint32_t)g, js.dispatched});
+                js.dispatched += g;
+                left -= g;
+            }
         }
         // keep admission (arrival) order inside the wave
         std::sort(segs.begin(), segs.end(), [&](const Seg &a, const Seg &b) { return order(a.job) < order(b.job); });
@@ -167,6 +190,7 @@ private:
 
     uint64_t budget_;
     int max_jobs_;
+    int policy_;
     uint64_t used_ = 0;
     uint64_t clock_ = 0;
     std::map<uint64_t, SceneState> scenes_;

@@ -232,10 +232,10 @@ class Server:
     budget, running jobs share every wave."""
 
     def __init__(self, ctx: Context, budget_bytes: int, max_depth: int = 16, max_jobs: int = 32, max_lights: int = 8,
-                 wave_paths: int = 0):
+                 wave_paths: int = 0, policy: int = 0):
         self.ctx = ctx
         self.h = None
-        cfg = T.fl_server_config(budget_bytes, wave_paths, max_depth, max_jobs, max_lights)
+        cfg = T.fl_server_config(budget_bytes, wave_paths, max_depth, max_jobs, max_lights, policy)
         h = C.c_void_p()
         check(lib().fl_server_create(ctx.h, C.byref(cfg), C.byref(h)), ctx.h)
         self.h = h

@@ -29,6 +29,10 @@ FL_SPECTRAL_BINS60 = 1
 FL_RENDER_PROFILE = 1
 FL_RENDER_COUNT = 2
 
+FL_SERVE_SHORTEST_FIRST = 0
+FL_SERVE_FIRST_COME = 1
+FL_SERVE_FAIR_SHARE = 2
+
 
 class fl_spectral_tables(C.Structure):
     _fields_ = [
@@ -146,6 +150,7 @@ class fl_server_config(C.Structure):
         ("max_depth", C.c_int32),
         ("max_jobs", C.c_int32),
         ("max_lights", C.c_int32),
+        ("policy", C.c_int32),
     ]
 
 
@@ -162,5 +167,5 @@ class fl_server_stats(C.Structure):
     _fields_ = [
         ("jobs_submitted", C.c_uint64), ("jobs_done", C.c_uint64), ("waves", C.c_uint64), ("paths", C.c_uint64),
         ("builds", C.c_uint64), ("evictions", C.c_uint64), ("resident_bytes", C.c_uint64),
-        ("running", C.c_uint32), ("pending", C.c_uint32),
+        ("running", C.c_uint32), ("pending", C.c_uint32), ("busy_ms", C.c_double),
     ]

@@ -267,7 +267,14 @@ typedef struct {
     int32_t max_depth;            /* deepest job accepted; each wave runs this many bounces */
     int32_t max_jobs;             /* jobs running at once, 1..64 */
     int32_t max_lights;           /* most lights any scene may have, 0..64 */
+    int32_t policy;               /* FL_SERVE_* wave packing */
 } fl_server_config;
+
+enum {
+    FL_SERVE_SHORTEST_FIRST = 0,  /* fewest remaining samples first (default) */
+    FL_SERVE_FIRST_COME = 1,      /* arrival order */
+    FL_SERVE_FAIR_SHARE = 2       /* equal shares (water-filling) */
+};
 
 typedef struct {
     uint64_t scene_id;
@@ -283,6 +290,7 @@ typedef struct {
 typedef struct {
     uint64_t jobs_submitted, jobs_done, waves, paths, builds, evictions, resident_bytes;
     uint32_t running, pending;
+    double busy_ms;               /* host wall time of the waves (launch to completion) */
 } fl_server_stats;
 
 FL_API fl_status fl_server_create(fl_context *ctx, const fl_server_config *cfg, fl_server **out);
