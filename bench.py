@@ -106,7 +106,7 @@ def dist_env():
 
 def render_scene():
     from filianore_b200 import scenes
-    return scenes.procedural_spheres(64, 128, 65, RENDER["width"], RENDER["height"])
+    return scenes.procedural_spheres(64, 128, 65, RENDER["width"], RENDER["height"])  # 1,048,578 triangles
 
 
 def raycast_inputs(rank):
@@ -137,7 +137,8 @@ def cpu_render(steps, warmup, stride=64):
             mrays.append(cnt["rays"] / dt / 1e6)
     return {"value": round(statistics.mean(mrays), 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
             "samples_per_s": round(statistics.mean(rates), 1),
-            "sample": f"every {stride}th pixel of the 1920x1080 frame ({n_pix // stride} pixels x 64 spp per step), "
+            "sample": f"every {stride}th pixel of the {RENDER['width']}x{RENDER['height']} frame "
+                      f"({n_pix // stride} pixels x {RENDER['spp']} spp per step), "
                       f"CPU oracle integrator (bit-exact restatement of the reference integrator; the scene's "
                       f"environment and sphere lights have no reference class)"}
 
@@ -149,7 +150,7 @@ def cpu_raycast(steps, warmup):
     bvh = oracle.CpuBVH(tris)
     build_s = time.perf_counter() - t0
     cores = os.cpu_count() or 1
-    sample = 1 << 20
+    sample = min(1 << 20, N_RAYS)
     times = []
     for i in range(warmup + steps):
         sl = slice((i * sample) % N_RAYS, (i * sample) % N_RAYS + sample)
@@ -261,7 +262,8 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
 
     results = {name: run_server(pol) for name, pol in (("shortest_first", fb.FL_SERVE_SHORTEST_FIRST),
                                                         ("first_come", fb.FL_SERVE_FIRST_COME),
-                                                        ("fair_share", fb.FL_SERVE_FAIR_SHARE))}
+                                                        ("fair_share", fb.FL_SERVE_FAIR_SHARE),
+                                                        ("shortest_first_aged", fb.FL_SERVE_SHORTEST_FIRST_AGED))}
     ctx.close()
     best = results["shortest_first"]
     return {"metric": "p99 time-to-image", "value": best["p99_ms"], "unit": "ms", "n_gpus": world,
@@ -282,12 +284,13 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
 
 def config_of(workload, world):
     if workload == "render":
+        W, H, spp = RENDER["width"], RENDER["height"], RENDER["spp"]
         return {"workload": "render: procedural 1,048,578-triangle scene (64 displaced spheres, Lambert / GGX "
-                            "conductor / rough dielectric, environment + sphere light), 1920x1080, 64 spp, "
+                            f"conductor / rough dielectric, environment + sphere light), {W}x{H}, {spp} spp, "
                             "max depth 16, 4 hero wavelengths",
-                "n_tri": 1048578, "width": 1920, "height": 1080, "spp": 64, "max_depth": 16,
+                "n_tri": 1048578, "width": W, "height": H, "spp": spp, "max_depth": 16,
                 "l2": "working set larger than L2 (no flush)", "parallelism": f"sample split x{world}"}
-    return {"workload": "raycast: 8,388,608-triangle soup, 16,777,216 incoherent rays, closest hit",
+    return {"workload": f"raycast: 8,388,608-triangle soup, {N_RAYS:,} incoherent rays, closest hit",
             "n_tri": N_TRI, "rays_per_gpu": N_RAYS, "l2": "inputs larger than L2 (no flush)",
             "parallelism": f"replicas x{world}"}
 
@@ -326,6 +329,7 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
     clocks.start()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
     t_start.record()
     stats = []
     # the last timed frame also times every kernel launch with CUDA events (roofline); the
@@ -334,6 +338,7 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
         flags = fb.FL_RENDER_PROFILE if k == args.steps - 1 else 0
         stats.append(frame(params(flags, rank * RENDER["spp"])))
     t_end.record()
+    torch.cuda.nvtx.range_pop()
     barrier()
     clk = clocks.stop()
     dev_ms = sum(s["ms"] for s in stats)               # device time of the renders (library events)
@@ -344,22 +349,32 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
     value = world * rays / (total_ms / 1e3) / 1e6
     samples_per_s = world * paths / (total_ms / 1e3)
 
-    # end to end through the C ABI: host film (D2H of the linear RGB image per frame)
+    # end to end through the C ABI, every step: the scene's triangles and material ids are
+    # uploaded from pinned host memory and its BVH is built (fl_scene_create), the frame is
+    # rendered, and the linear RGB film is read back into pinned host memory
+    pinned = scenes.Scene(torch.from_numpy(sc.verts).pin_memory().numpy(),
+                          torch.from_numpy(sc.tri_material).pin_memory().numpy(), sc.materials, sc.lights, sc.camera)
     host_film = torch.zeros((H, W, 3), dtype=torch.float32).pin_memory()
     e2e_steps = max(2, args.steps // 2)
-    scene.render(params(offset=rank * RENDER["spp"]), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
+
+    def e2e_step():
+        h = ctx.scene(pinned)
+        _, st = h.render(params(offset=rank * RENDER["spp"]), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
+        h.close()
+        return st
+    e2e_step()
     barrier()
     t0 = time.perf_counter()
     e_rays = 0
     for _ in range(e2e_steps):
-        _, st = scene.render(params(offset=rank * RENDER["spp"]), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
-        e_rays += st["rays"]
+        e_rays += e2e_step()["rays"]
     barrier()
     e2e_s = reduce_max(time.perf_counter() - t0)
     e2e = {"value": round(world * e_rays / e2e_s / 1e6, 3), "unit": "Mrays/s",
            "samples_per_s": round(world * e2e_steps * W * H * RENDER["spp"] / e2e_s, 1),
-           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 3 * 4,
-           "note": "scene resident in HBM; camera and parameters travel as kernel arguments"}
+           "h2d_bytes_per_step": int(pinned.verts.nbytes + pinned.tri_material.nbytes),
+           "d2h_bytes_per_step": W * H * 3 * 4,
+           "note": "per step: scene upload from pinned host memory + BVH build + render + film readback"}
 
     peaks = load_peaks()
     prof = stats[-1]
@@ -411,12 +426,14 @@ def gpu_raycast(args, world, rank, local, barrier, reduce_max):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
     t_start.record()
     for k in range(args.steps):
         ev[k][0].record()
         scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
         ev[k][1].record()
     t_end.record()
+    torch.cuda.nvtx.range_pop()
     barrier()
     clk = clocks.stop()
     total_ms = reduce_max(t_start.elapsed_time(t_end))
@@ -466,8 +483,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", default=None, help="render: WxH (smaller cases for profiling)")
+    ap.add_argument("--spp", type=int, default=None, help="render: samples per pixel")
+    ap.add_argument("--rays", type=int, default=None, help="raycast: rays per batch")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    global N_RAYS
+    if args.size:
+        RENDER["width"], RENDER["height"] = (int(v) for v in args.size.lower().split("x"))
+    if args.spp:
+        RENDER["spp"] = args.spp
+    if args.rays:
+        N_RAYS = args.rays
     world, rank, local = dist_env()
 
     if args.impl == "reference":

@@ -13,8 +13,9 @@
 //    rest of every wave, so the GPU stays full. (A simulation of this workload's Poisson
 //    load favoured this over first-come-first-served packing, equal sharing and a
 //    reserved share for the oldest job, at both the median and the 99th percentile.)
-//    The other policies are first come, first served packing and equal sharing
-//    (water-filling). Each job gets one contiguous sample range per wave, so its
+//    The other policies are first come, first served packing, equal sharing
+//    (water-filling), and shortest-remaining-first with a quarter of every wave reserved
+//    for the oldest running job. Each job gets one contiguous sample range per wave, so its
 //    per-sample random streams do not depend on how it was batched.
 //  - A job is complete when all its samples were dispatched and the wave that carried its
 //    last samples has finished.
@@ -42,7 +43,7 @@ public:
         std::vector<uint64_t> rejected;  // jobs that can never fit the budget
     };
 
-    enum Policy { kShortestFirst = 0, kFirstCome = 1, kFairShare = 2 };
+    enum Policy { kShortestFirst = 0, kFirstCome = 1, kFairShare = 2, kShortestFirstAged = 3 };
 
     ServeScheduler(uint64_t budget_bytes, int max_jobs, int policy = kShortestFirst)
         : budget_(budget_bytes), max_jobs_(max_jobs), policy_(policy) {}
@@ -127,8 +128,19 @@ public:
                 left -= g;
             }
         } else {
+            if (policy_ == kShortestFirstAged && !want.empty()) {
+                // the oldest running job (running_ is in arrival order) is guaranteed a
+                // quarter of the wave, which bounds how long shorter arrivals can starve it
+                const uint64_t g = std::min<uint64_t>(want[0].first, cap / 4);
+                JobState &js = jobs_[want[0].second];
+                segs.push_back(Seg{want[0].second, (uint32_t)g, js.dispatched});
+                js.dispatched += g;
+                left -= g;
+                want[0].first -= g;
+                if (want[0].first == 0) want.erase(want.begin());
+            }
             // shortest remaining first, or first come first served (running_ is in arrival order)
-            if (policy_ == kShortestFirst)
+            if (policy_ != kFirstCome)
                 std::stable_sort(want.begin(), want.end(),
                                  [](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
                                      return a.first < b.first;
@@ -136,7 +148,11 @@ public:
             for (size_t i = 0; i < want.size() && left > 0; ++i) {
                 const uint64_t g = std::min<uint64_t>(want[i].first, left);
                 JobState &js = jobs_[want[i].second];
-                segs.push_back(Seg{want[i].second, (uint32_t)g, js.dispatched});
+                auto same = std::find_if(segs.begin(), segs.end(), [&](const Seg &q) { return q.job == want[i].second; });
+                if (same != segs.end())
+                    same->count += (uint32_t)g;  // the oldest job's reserved range continues
+                else
+                    segs.push_back(Seg{want[i].second, (uint32_t)g, js.dispatched});
                 js.dispatched += g;
                 left -= g;
             }

@@ -32,6 +32,7 @@ FL_RENDER_COUNT = 2
 FL_SERVE_SHORTEST_FIRST = 0
 FL_SERVE_FIRST_COME = 1
 FL_SERVE_FAIR_SHARE = 2
+FL_SERVE_SHORTEST_FIRST_AGED = 3
 
 
 class fl_spectral_tables(C.Structure):

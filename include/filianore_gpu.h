@@ -273,7 +273,8 @@ typedef struct {
 enum {
     FL_SERVE_SHORTEST_FIRST = 0,  /* fewest remaining samples first (default) */
     FL_SERVE_FIRST_COME = 1,      /* arrival order */
-    FL_SERVE_FAIR_SHARE = 2       /* equal shares (water-filling) */
+    FL_SERVE_FAIR_SHARE = 2,      /* equal shares (water-filling) */
+    FL_SERVE_SHORTEST_FIRST_AGED = 3  /* shortest first, oldest job keeps a quarter of each wave */
 };
 
 typedef struct {

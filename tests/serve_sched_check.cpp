@@ -50,5 +50,16 @@ int main() {
     std::printf("\n");
     print_adm("A3", s.admit());
     std::printf("used %llu idle %d\n", (unsigned long long)s.used(), (int)s.idle());
+
+    // wave packing policies: jobs 20..23 (arrival order) with 300, 40, 200, 10 samples
+    const char *names[] = {"shortest", "first_come", "fair", "aged"};
+    for (int pol = 0; pol < 4; ++pol) {
+        ServeScheduler q(1 << 20, 8, pol);
+        q.add_scene(1, 100);
+        const uint64_t want[] = {300, 40, 200, 10};
+        for (int j = 0; j < 4; ++j) q.submit(20 + j, 1, 10, want[j]);
+        q.admit();
+        print_plan(names[pol], q.plan_wave(256));
+    }
     return 0;
 }

@@ -1,6 +1,6 @@
 """Host-side policy of the render server (no GPU): admission in arrival order by memory
 footprint, LRU eviction of idle scenes, rejection of jobs that can never fit, and the
-water-filling split of wave slots."""
+wave packing policies."""
 import os
 import subprocess
 import tempfile
@@ -33,3 +33,16 @@ def test_scheduler_decisions():
     # job 13's film alone exceeds the budget: rejected when it reaches the queue head
     assert out[8] == "A3 admitted | build | evict | rejected 13"
     assert out[9] == "used 800 idle 1"
+
+
+def test_wave_packing_policies():
+    out = run_driver()[10:]
+    # shortest remaining first: the three short jobs complete, the long one fills the rest
+    assert out[0] == "shortest 20:6@0 21:40@0 22:200@0 23:10@0"
+    # arrival order: the oldest job takes the whole wave
+    assert out[1] == "first_come 20:256@0"
+    # water-filling: 10 and 40 fit an equal share, the other two split the remaining 206
+    assert out[2] == "fair 20:103@0 21:40@0 22:103@0 23:10@0"
+    # the oldest job keeps a quarter of the wave (64), the rest goes shortest first
+    assert out[3] == "aged 20:64@0 21:40@0 22:142@0 23:10@0"
+
