@@ -282,6 +282,63 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
             "policies": results}
 
 
+def gpu_guide(args, world, rank, local, barrier, reduce_max):
+    """Learned path guiding on the caustic scene (1024 x 1024; glass sphere of 65,536
+    triangles under a sphere light of radius 0.02 and radiance 5e3; Lambert room of 12
+    triangles, albedo 0.7; max depth 8, hero wavelengths): the plain GPU path at 64 spp
+    against guided renders given a fraction of its wall time (training online during the
+    first 25% of each budget, passes of 4 spp), errors against a 4096-spp FP64 plain render."""
+    import filianore_b200 as fb
+    from filianore_b200 import scenes
+    R = RENDER["width"] if args.size else 1024
+    depth = 8
+    sc = scenes.caustic(R, R)
+    ctx = fb.Context(local)
+    s = ctx.scene(sc)
+    n_ref = args.spp if args.spp else 4096
+    ref = np.zeros((R, R, 3), np.float64)
+    _, rst = s.render(scenes.render_params(n_ref, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 24), film_xyz64=ref)
+    ref /= n_ref
+
+    def mse(img, spp):
+        return float(np.mean((img / spp - ref) ** 2))
+    # plain: 64 spp, timed through the C ABI (wall time of the call)
+    plain = np.zeros((R, R, 3), np.float64)
+    s.render(scenes.render_params(4, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 22))  # warm-up
+    t0 = time.perf_counter()
+    _, pst = s.render(scenes.render_params(64, depth, fb.FL_SPECTRAL_HERO4), film_xyz64=plain)
+    t_plain = (time.perf_counter() - t0) * 1e3
+    e_plain = mse(plain, 64)
+    runs = []
+    for frac in (1 / 8, 1 / 4, 1 / 3, 1 / 2, 1.0):
+        g = fb.Guide(ctx, seed=5, select_prob=0.5, batch=16384, max_records=1 << 19, steps_per_wave=16)
+        img = np.zeros((R, R, 3), np.float64)
+        t0 = time.perf_counter()
+        _, gst = g.render_timed(s, scenes.render_params(4, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20),
+                                budget_ms=frac * t_plain, train_fraction=0.25, film_xyz64=img)
+        wall = (time.perf_counter() - t0) * 1e3
+        spp = gst["paths"] // (R * R)
+        runs.append({"budget_frac": round(frac, 4), "wall_ms": round(wall, 1), "spp": int(spp),
+                     "mse": mse(img, spp), "adam_steps": g.info()["adam_steps"]})
+        g.close()
+    ok = [r for r in runs if r["mse"] <= e_plain]
+    t_match = min(r["wall_ms"] for r in ok) if ok else None
+    s.close()
+    ctx.close()
+    equal_time = runs[-1]
+    return {"metric": "guided wall time to the plain 64-spp MSE / plain wall time",
+            "value": round(t_match / t_plain, 4) if t_match else None, "unit": "ratio", "n_gpus": world,
+            "steps": len(runs), "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 render, f16 weights / f32 accumulate", "data": "synthetic",
+            "config": {"workload": f"guide: caustic scene {R}x{R}, glass sphere 65,536 tris, sphere light r 0.02 "
+                                   f"L 5e3, depth {depth}; MLP 80-64x4-40 (8 vMF lobes), Adam lr 1e-2, one-sample "
+                                   "MIS c 0.5, training in the first 25% of each budget",
+                       "reference_spp": n_ref, "parallelism": "1 GPU"},
+            "plain": {"spp": 64, "wall_ms": round(t_plain, 1), "device_ms": round(pst["ms"], 1), "mse": e_plain},
+            "guided": runs, "equal_time_mse_ratio": round(e_plain / equal_time["mse"], 3),
+            "reference_ms": round(rst["ms"], 1)}
+
+
 def config_of(workload, world):
     if workload == "render":
         W, H, spp = RENDER["width"], RENDER["height"], RENDER["spp"]
@@ -300,7 +357,7 @@ def config_of(workload, world):
 def gpu_render(args, world, rank, local, barrier, reduce_max):
     import torch
     import filianore_b200 as fb
-    from filianore_b200 import scenes
+    from filianore_b200 import dist as fdist, scenes
     sc = render_scene()
     ctx = fb.Context(local)
     scene = ctx.scene(sc)
@@ -316,14 +373,13 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
     def frame(p):
         _, st = scene.render(p, film_rgb=film, film_xyz64=xyz, memory=fb.FL_MEM_DEVICE)
         if world > 1:
-            import torch.distributed as dist
-            dist.reduce(xyz, dst=0, op=dist.ReduceOp.SUM)
+            fdist.reduce_film(xyz, dst=0)
         return st
 
     for _ in range(args.warmup):
-        frame(params(offset=rank * RENDER["spp"]))
+        frame(params(offset=fdist.rank_sample_offset(rank, RENDER["spp"])))
     # traversal work of one frame (instrumented, untimed)
-    cstats = frame(params(fb.FL_RENDER_COUNT, rank * RENDER["spp"]))
+    cstats = frame(params(fb.FL_RENDER_COUNT, fdist.rank_sample_offset(rank, RENDER["spp"])))
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
@@ -336,7 +392,7 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
     # others replay the per-wave CUDA graph
     for k in range(args.steps):
         flags = fb.FL_RENDER_PROFILE if k == args.steps - 1 else 0
-        stats.append(frame(params(flags, rank * RENDER["spp"])))
+        stats.append(frame(params(flags, fdist.rank_sample_offset(rank, RENDER["spp"]))))
     t_end.record()
     torch.cuda.nvtx.range_pop()
     barrier()
@@ -359,7 +415,7 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
 
     def e2e_step():
         h = ctx.scene(pinned)
-        _, st = h.render(params(offset=rank * RENDER["spp"]), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
+        _, st = h.render(params(offset=fdist.rank_sample_offset(rank, RENDER["spp"])), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
         h.close()
         return st
     e2e_step()
@@ -481,7 +537,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve"])
+    ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve", "guide"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", default=None, help="render: WxH (smaller cases for profiling)")
     ap.add_argument("--spp", type=int, default=None, help="render: samples per pixel")
@@ -532,10 +588,10 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    run = {"render": gpu_render, "raycast": gpu_raycast, "serve": gpu_serve}[args.workload]
+    run = {"render": gpu_render, "raycast": gpu_raycast, "serve": gpu_serve, "guide": gpu_guide}[args.workload]
     line = run(args, world, rank, local, barrier, reduce_max)
     if rank == 0:
-        if not args.no_cpu_baseline and args.workload != "serve":
+        if not args.no_cpu_baseline and args.workload in ("render", "raycast"):
             line["cpu_baseline"] = (cpu_render(2, 0) if args.workload == "render" else cpu_raycast(3, 1))
         print(json.dumps(line), flush=True)
     if world > 1:

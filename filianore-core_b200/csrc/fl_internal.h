@@ -88,6 +88,7 @@ struct Scene {
     uint32_t n_emissive_tris = 0;
     int has_env = 0;
     float env_radiance = 0.f;
+    float bmin[3] = {0.f, 0.f, 0.f}, bmax[3] = {0.f, 0.f, 0.f};  // bounds of the triangles
     std::vector<fl_light> lights_host;
     std::vector<MaterialDev> materials_host;
 };

@@ -23,6 +23,7 @@
 #include <cstddef>
 #include <vector>
 
+#include "fl_guide.cuh"
 #include "fl_internal.h"
 #include "fl_shading.cuh"
 #include "fl_traverse.cuh"
@@ -145,6 +146,7 @@ struct RenderArgs {
     uint32_t *q_trace, *q_cont, *q_next;
     uint32_t *q_class;  // kShadeClasses x cap: traced paths grouped by what shades them
     WaveCounters *cnt;
+    GuideArgs g;        // learned guiding (zero when off)
 };
 
 enum : uint32_t { kHasCL = 1u, kHasCS = 2u, kVisOK = 4u, kMisOK = 8u };
@@ -220,6 +222,30 @@ __device__ inline void finish_path(const RenderArgs &A, const JobDev &J, const S
     atomicAdd(&J.film[3 * (size_t)pix + 0], xyz[0]);
     atomicAdd(&J.film[3 * (size_t)pix + 1], xyz[1]);
     atomicAdd(&J.film[3 * (size_t)pix + 2], xyz[2]);
+    if constexpr (NL == 4) {
+        // guiding: the radiance gathered after each recorded vertex, divided by the
+        // throughput it was scaled by, estimates the incident radiance along the
+        // recorded direction (averaged over the hero wavelengths that carry any)
+        if (A.g.rec_idx) {
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const uint32_t idx = A.g.rec_idx[(size_t)r * A.cap + slot];
+                if (idx == kNoRecord) continue;
+                float *R = A.g.rec + (size_t)idx * kRecFloats;
+                float li = 0.f;
+                int nz = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float b = R[12 + k];
+                    if (b > 0.f) {
+                        li += fmaxf(L.c[k] - R[16 + k], 0.f) / b;
+                        ++nz;
+                    }
+                }
+                R[11] = nz ? li / (float)nz : 0.f;
+            }
+        }
+    }
 }
 
 // the hit record of BVH::intersect (bvh.cpp:49-84): p = o + d t, n = normalize(Ng), wo = normalize(-d)
@@ -317,6 +343,10 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
         A.ray_o[k] = make_float4(o.x, o.y, o.z, 0.f);
         A.ray_d[k] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
         A.q_trace[k] = k;
+        if (A.g.rec_idx) {
+            A.g.rec_idx[k] = kNoRecord;
+            A.g.rec_idx[(size_t)A.cap + k] = kNoRecord;
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->paths, (unsigned long long)n_wave);
 }
@@ -630,7 +660,81 @@ __global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
     if (err) atomicAdd(&A.cnt->err, 1);
 }
 
+// A training record at a Lambert vertex (the path's first two): the record is closed by
+// finish_path with the radiance the path gathers after it.
 template <int NL>
+__device__ inline void guide_record(const RenderArgs &A, uint32_t slot, const Hit &hr, float lambda0, v3 wi,
+                                    float pdf, const Spec<NL> &beta_after, const Spec<NL> &L_before) {
+    int r = -1;
+    if (A.g.rec_idx[slot] == kNoRecord) r = 0;
+    else if (A.g.rec_idx[(size_t)A.cap + slot] == kNoRecord) r = 1;
+    if (r < 0) return;
+    const uint32_t pos = atomicAdd(A.g.rec_count, 1u);
+    if (pos >= A.g.rec_cap) return;
+    const v3 nf = dot(hr.n, hr.wo) < 0.f ? neg(hr.n) : hr.n;
+    float *R = A.g.rec + (size_t)pos * kRecFloats;
+    float4 *R4 = reinterpret_cast<float4 *>(R);
+    R4[0] = make_float4(hr.p.x, hr.p.y, hr.p.z, nf.x);
+    R4[1] = make_float4(nf.y, nf.z, lambda0, wi.x);
+    R4[2] = make_float4(wi.y, wi.z, pdf, 0.f);
+    R4[3] = make_float4(beta_after.c[0], beta_after.c[1], beta_after.c[2], beta_after.c[3]);
+    R4[4] = make_float4(L_before.c[0], L_before.c[1], L_before.c[2], L_before.c[3]);
+    A.g.rec_idx[(size_t)r * A.cap + slot] = pos;
+}
+
+// Guide inference for the paths that hit a Lambert surface this bounce: 16 points per warp
+// on the tensor cores, mixture parameters to A.g.mix. Dynamic shared memory: the weights
+// plus 16 feature rows and 16 head rows per warp (guide_infer_smem_bytes).
+constexpr int kInferWarps = 4;
+inline size_t guide_infer_smem_bytes() {
+    return (size_t)kSmWHalves * 2 + (size_t)kInferWarps * (16 * kLdIn * 2 + 16 * kHeadLd * 4);
+}
+template <int NL>
+__global__ void __launch_bounds__(128) k_guide_infer(RenderArgs A) {
+    extern __shared__ __align__(16) unsigned char gsm[];
+    __half *sw = reinterpret_cast<__half *>(gsm);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __half *X = reinterpret_cast<__half *>(gsm + kSmWHalves * 2) + warp * 16 * kLdIn;
+    float *head = reinterpret_cast<float *>(gsm + kSmWHalves * 2 + kInferWarps * 16 * kLdIn * 2) + warp * 16 * kHeadLd;
+    const int cls = 1 + FL_MAT_LAMBERT;
+    const uint32_t n = load_count(&A.cnt->n_class[cls]);
+    if ((uint32_t)blockIdx.x * kInferWarps * 16 >= n) return;
+    guide_stage_weights(sw, A.g.w);
+    const uint32_t *q = A.q_class + (size_t)cls * A.cap;
+    for (uint32_t chunk = blockIdx.x * kInferWarps + warp; chunk * 16 < n; chunk += gridDim.x * kInferWarps) {
+        const uint32_t i = chunk * 16 + (lane & 15);
+        const bool valid = i < n;
+        uint32_t slot = 0;
+        __half *row = X + (lane & 15) * kLdIn;
+        if (valid) {
+            slot = q[i];
+            const JobDev &J = A.jobs[A.job[slot]];
+            const Hit hr = make_hit(J, A.ray_o[slot], A.ray_d[slot], A.hit[slot]);
+            const v3 nf = dot(hr.n, hr.wo) < 0.f ? neg(hr.n) : hr.n;
+            float pn[3];
+            guide_normalise(A.g.bmin, A.g.binv, hr.p, pn);
+            const float nn[3] = {nf.x, nf.y, nf.z};
+            guide_encode_part(pn, nn, (A.lambda0[slot] - 380.f) * (1.f / 340.f), lane >> 4, row);
+        } else {
+            uint4 *d = reinterpret_cast<uint4 *>(row + 40 * (lane >> 4));
+#pragma unroll
+            for (int k = 0; k < 5; ++k) d[k] = make_uint4(0, 0, 0, 0);
+        }
+        __syncwarp();
+        guide_forward_warp(sw, X, nullptr, 0, head);
+        __syncwarp();
+        if (valid && lane < 16) {
+            float m[kGuideOut];
+            guide_mixture(head + lane * kHeadLd, m);
+            float4 *dst = reinterpret_cast<float4 *>(A.g.mix + (size_t)slot * kGuideOut);
+#pragma unroll
+            for (int k = 0; k < kGuideOut / 4; ++k) dst[k] = make_float4(m[4 * k], m[4 * k + 1], m[4 * k + 2], m[4 * k + 3]);
+        }
+        __syncwarp();
+    }
+}
+
+template <int NL, bool GUIDE = false>
 __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
     __shared__ SmemTables sm;
     stage_tables(sm, A.tab, NL != 60);
@@ -688,8 +792,30 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             float pdf = 0.f;
             int sflags = 0;
             Spec<NL> f;
+            // guiding at Lambert vertices: one-sample MIS between the learned mixture
+            // (probability c) and the BSDF; an extra number picks the technique and the lobe
+            const float *gm = nullptr;
+            float c_sel = 0.f, u_sel = 1.f;
+            if constexpr (GUIDE) {
+                if (b.type == FL_MAT_LAMBERT && A.g.select > 0.f) {
+                    gm = A.g.mix + (size_t)slot * kGuideOut;
+                    if (gm[0] >= 0.f) {
+                        c_sel = A.g.select;
+                        u_sel = rng.nextf();
+                    }
+                }
+            }
             const float ux = rng.nextf(), uy = rng.nextf();
-            bsdf_sample<NL>(b, wo, wi, ux, uy, pdf, kBsdfAll, sflags, f);
+            if (GUIDE && u_sel < c_sel) {
+                wi = guide_mixture_sample(gm, u_sel / c_sel, ux, uy);
+                bsdf_eval<NL>(b, wo, wi, kBsdfAll, f);
+                pdf = bsdf_pdf<NL>(b, wo, wi, kBsdfAll);
+                sflags = kBsdfDiffuse | kBsdfReflection;
+            } else {
+                bsdf_sample<NL>(b, wo, wi, ux, uy, pdf, kBsdfAll, sflags, f);
+            }
+            if (GUIDE && c_sel > 0.f && !(f.black() || pdf == 0))
+                pdf = c_sel * guide_mixture_pdf(gm, wi) + (1.f - c_sel) * pdf;
             bool stop = f.black() || pdf == 0;
             const int depth = J.max_depth;
             const int bi = (int)bounce;
@@ -700,6 +826,9 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                 const float ad = absdot(wi, b.ns);
 #pragma unroll
                 for (int k = 0; k < NL; ++k) beta.c[k] *= f.c[k] * ad / pdf;
+                if constexpr (GUIDE && NL == 4) {
+                    if (A.g.record && b.type == FL_MAT_LAMBERT) guide_record(A, slot, hr, lambda0, wi, pdf, beta, L);
+                }
                 const bool spec_b = (sflags & kBsdfSpecular) != 0;
                 float etaScale = A.eta_scale[slot];
                 if ((sflags & kBsdfSpecular) && (sflags & kBsdfTransmission)) {
@@ -848,7 +977,7 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
 // Enqueues one wave (camera rays of the samples in *W.d_wave, then max_depth + 1 bounces)
 // on `st`. Launch shapes do not depend on the wave's content, so the sequence can be
 // captured once into a CUDA graph and replayed for every wave.
-template <int NL>
+template <int NL, bool GUIDE = false>
 void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile *prof, int sms, cudaStream_t st) {
     RenderArgs A = W.A;
     A.q_trace = W.qa;
@@ -874,7 +1003,13 @@ void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile
         else k_trace_rays2<false><<<g_trace, 128, 0, st>>>(A);
         prof->mark(2, st);
         prof->mark(3, st);
-        k_continue<NL><<<g_shade, 128, 0, st>>>(A);
+        if constexpr (GUIDE) {
+            if (A.g.select > 0.f) {
+                k_guide_infer<NL><<<sms * 2, 128, guide_infer_smem_bytes(), st>>>(A);
+                prof->launches += 1;
+            }
+        }
+        k_continue<NL, GUIDE><<<g_shade, 128, 0, st>>>(A);
         prof->mark(3, st);
         prof->launches += 4;
     }

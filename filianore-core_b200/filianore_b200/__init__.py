@@ -24,6 +24,8 @@ EXPORTED = [
     "fl_scene_create", "fl_scene_destroy", "fl_scene_get_info", "fl_trace_closest", "fl_trace_occluded",
     "fl_trace_count", "fl_render", "fl_render_noalloc", "fl_server_create", "fl_server_destroy",
     "fl_server_add_scene", "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_get_stats",
+    "fl_guide_create", "fl_guide_destroy", "fl_guide_render", "fl_guide_render_timed", "fl_guide_get_weights",
+    "fl_guide_set_weights", "fl_guide_get_info", "fl_guide_gradient", "fl_guide_eval",
 ]
 
 _lib = None
@@ -70,6 +72,18 @@ def lib():
         L.fl_server_poll.argtypes = [vp, C.c_uint64, vp, vp, P(T.fl_job_stats)]
         L.fl_server_wait.argtypes = [vp, C.c_uint64, C.c_int32, vp, vp, P(T.fl_job_stats)]
         L.fl_server_get_stats.argtypes = [vp, P(T.fl_server_stats)]
+        L.fl_guide_create.argtypes = [vp, P(T.fl_guide_config), P(vp)]
+        L.fl_guide_destroy.argtypes = [vp]
+        L.fl_guide_render.argtypes = [vp, vp, P(T.fl_camera), P(T.fl_render_params), C.c_int32, vp, vp, C.c_int32,
+                                      P(T.fl_render_stats)]
+        L.fl_guide_render_timed.argtypes = [vp, vp, P(T.fl_camera), P(T.fl_render_params), C.c_double, C.c_double,
+                                            vp, vp, C.c_int32, P(T.fl_render_stats)]
+        L.fl_guide_get_weights.argtypes = [vp, P(C.c_float)]
+        L.fl_guide_set_weights.argtypes = [vp, P(C.c_float)]
+        L.fl_guide_get_info.argtypes = [vp, P(C.c_int64), P(C.c_float)]
+        L.fl_guide_gradient.argtypes = [vp, P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float),
+                                        P(C.c_float)]
+        L.fl_guide_eval.argtypes = [vp, P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float)]
         for name in EXPORTED:
             if name not in ("fl_status_string",):
                 getattr(L, name).restype = C.c_int32
@@ -225,6 +239,89 @@ class SceneHandle:
         check(lib().fl_render(self.h, C.byref(cam), C.byref(params), _ptr(film_rgb), xyz, mem, C.byref(stats)),
               self.ctx.h)
         return film_rgb, {k: getattr(stats, k) for k, _ in T.fl_render_stats._fields_}
+
+
+class Guide:
+    """Learned path guide (fl_guide_*): an MLP proposal for continuation directions at Lambert
+    vertices, trained online on the renderer's own samples."""
+
+    def __init__(self, ctx: Context, seed: int = 1, learning_rate: float = 1e-2, select_prob: float = 0.5,
+                 batch: int = 16384, max_records: int = 1 << 20, steps_per_wave: int = 16):
+        self.ctx = ctx
+        self.h = None
+        cfg = T.fl_guide_config(seed, learning_rate, select_prob, batch, max_records, steps_per_wave)
+        h = C.c_void_p()
+        check(lib().fl_guide_create(ctx.h, C.byref(cfg), C.byref(h)), ctx.h)
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().fl_guide_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, scene: "SceneHandle", params, flags, camera=None, film_rgb=None, film_xyz64=None, memory=None):
+        cam = camera if camera is not None else scene.src.camera_struct()
+        if film_rgb is None:
+            film_rgb = np.zeros((cam.height, cam.width, 3), np.float32)
+        mem = memory if memory is not None else (T.FL_MEM_DEVICE if _is_device(film_rgb) else T.FL_MEM_HOST)
+        st = T.fl_render_stats()
+        xyz = _ptr(film_xyz64) if film_xyz64 is not None else None
+        check(lib().fl_guide_render(self.h, scene.h, C.byref(cam), C.byref(params), flags, _ptr(film_rgb), xyz, mem,
+                                    C.byref(st)), self.ctx.h)
+        return film_rgb, {k: getattr(st, k) for k, _ in T.fl_render_stats._fields_}
+
+    def render_timed(self, scene: "SceneHandle", params, budget_ms: float, train_fraction: float = 0.25, camera=None,
+                     film_rgb=None, film_xyz64=None, memory=None):
+        cam = camera if camera is not None else scene.src.camera_struct()
+        if film_rgb is None:
+            film_rgb = np.zeros((cam.height, cam.width, 3), np.float32)
+        mem = memory if memory is not None else (T.FL_MEM_DEVICE if _is_device(film_rgb) else T.FL_MEM_HOST)
+        st = T.fl_render_stats()
+        xyz = _ptr(film_xyz64) if film_xyz64 is not None else None
+        check(lib().fl_guide_render_timed(self.h, scene.h, C.byref(cam), C.byref(params), budget_ms, train_fraction,
+                                          _ptr(film_rgb), xyz, mem, C.byref(st)), self.ctx.h)
+        return film_rgb, {k: getattr(st, k) for k, _ in T.fl_render_stats._fields_}
+
+    def weights(self):
+        w = np.zeros(T.FL_GUIDE_PARAMS, np.float32)
+        check(lib().fl_guide_get_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))), self.ctx.h)
+        return w
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        check(lib().fl_guide_set_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))), self.ctx.h)
+
+    def info(self):
+        steps, loss = C.c_int64(), C.c_float()
+        check(lib().fl_guide_get_info(self.h, C.byref(steps), C.byref(loss)), self.ctx.h)
+        return {"adam_steps": steps.value, "last_loss": loss.value}
+
+    def gradient(self, records, bmin, bmax):
+        r = np.ascontiguousarray(records, np.float32)
+        g = np.zeros(T.FL_GUIDE_PARAMS, np.float32)
+        loss = C.c_float()
+        bn = np.asarray(bmin, np.float32)
+        bx = np.asarray(bmax, np.float32)
+        check(lib().fl_guide_gradient(self.h, r.ctypes.data_as(C.POINTER(C.c_float)), r.shape[0],
+                                      bn.ctypes.data_as(C.POINTER(C.c_float)), bx.ctypes.data_as(C.POINTER(C.c_float)),
+                                      g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)), self.ctx.h)
+        return g, loss.value
+
+    def eval(self, records, bmin, bmax):
+        r = np.ascontiguousarray(records, np.float32)
+        out = np.zeros((r.shape[0], 40), np.float32)
+        bn = np.asarray(bmin, np.float32)
+        bx = np.asarray(bmax, np.float32)
+        check(lib().fl_guide_eval(self.h, r.ctypes.data_as(C.POINTER(C.c_float)), r.shape[0],
+                                  bn.ctypes.data_as(C.POINTER(C.c_float)), bx.ctypes.data_as(C.POINTER(C.c_float)),
+                                  out.ctypes.data_as(C.POINTER(C.c_float))), self.ctx.h)
+        return out
 
 
 class Server:

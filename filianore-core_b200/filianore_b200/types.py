@@ -170,3 +170,22 @@ class fl_server_stats(C.Structure):
         ("builds", C.c_uint64), ("evictions", C.c_uint64), ("resident_bytes", C.c_uint64),
         ("running", C.c_uint32), ("pending", C.c_uint32), ("busy_ms", C.c_double),
     ]
+
+
+class fl_guide_config(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64),
+        ("learning_rate", C.c_float),
+        ("select_prob", C.c_float),
+        ("batch", C.c_int32),
+        ("max_records", C.c_int32),
+        ("steps_per_wave", C.c_int32),
+        ("reserved", C.c_int32 * 3),
+    ]
+
+
+FL_GUIDE_SAMPLE = 1
+FL_GUIDE_TRAIN = 2
+FL_GUIDE_PARAMS = 19968
+FL_GUIDE_RECORD_FLOATS = 20
+

@@ -323,6 +323,69 @@ FL_API fl_status fl_server_get_stats(fl_server *srv, fl_server_stats *stats);
 FL_API fl_status fl_render_noalloc(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
                                    float *film_rgb, double *film_xyz64, fl_render_stats *stats);
 
+/* ------------------------------------------------------------------------- */
+/* Learned path guiding (new: the reference samples directions from the BSDF only) */
+/* ------------------------------------------------------------------------- */
+/* A guide is an MLP (FP16 weights, FP32 accumulation on the tensor cores) mapping a surface
+ * point (12-band frequency encoding of the position in the scene bounds, normal, hero
+ * wavelength) through 4 hidden layers of width 64 (ReLU) to an 8-lobe von Mises-Fisher
+ * mixture over incident directions. At Lambert vertices the renderer samples the
+ * continuation from the mixture with probability select_prob and from the BSDF otherwise,
+ * weighting by the one-sample MIS density c q(w) + (1 - c) p_bsdf(w), so images stay
+ * unbiased for any weights. Training is online: the renderer records (point, direction,
+ * density, incident radiance estimate) at each path's first two Lambert vertices, and
+ * after every wave Adam minimises the radiance-weighted KL divergence
+ * -E[(L_i cos / p) log q] over minibatches of those records. Hero-wavelength mode only. */
+typedef struct fl_guide fl_guide;
+
+typedef struct {
+    uint64_t seed;           /* weight initialisation */
+    float learning_rate;     /* Adam step size (1e-2) */
+    float select_prob;       /* c in [0, 1): probability of sampling the mixture at a Lambert vertex */
+    int32_t batch;           /* records per Adam step, a multiple of 128 in [128, 65536] */
+    int32_t max_records;     /* records kept per wave, >= batch */
+    int32_t steps_per_wave;  /* most Adam steps after one wave, >= 1 */
+    int32_t reserved[3];
+} fl_guide_config;
+
+enum {
+    FL_GUIDE_SAMPLE = 1,  /* sample continuations from the guide (one-sample MIS) */
+    FL_GUIDE_TRAIN = 2    /* record training samples and take Adam steps after every wave */
+};
+
+#define FL_GUIDE_PARAMS 19968   /* weights: [64][80], 3 x [64][64], [40][64], row-major [out][in] */
+#define FL_GUIDE_RECORD_FLOATS 20
+
+FL_API fl_status fl_guide_create(fl_context *ctx, const fl_guide_config *cfg, fl_guide **out);
+FL_API fl_status fl_guide_destroy(fl_guide *guide);
+/* fl_render with guiding (flags FL_GUIDE_*); params->spectral_mode must be FL_SPECTRAL_HERO4. */
+FL_API fl_status fl_guide_render(fl_guide *guide, fl_scene *scene, const fl_camera *camera,
+                                 const fl_render_params *params, int32_t flags, float *film_rgb,
+                                 double *film_xyz64, int32_t memory, fl_render_stats *stats);
+/* Renders passes of params->spp samples per pixel until budget_ms of wall time have passed,
+ * training during the first train_fraction of the budget and sampling from the guide once it
+ * has taken an Adam step. The film is the average of all passes; stats->paths / (width *
+ * height) is the number of samples per pixel rendered, stats->ms the wall time. */
+FL_API fl_status fl_guide_render_timed(fl_guide *guide, fl_scene *scene, const fl_camera *camera,
+                                       const fl_render_params *params, double budget_ms, double train_fraction,
+                                       float *film_rgb, double *film_xyz64, int32_t memory,
+                                       fl_render_stats *stats);
+/* FP32 master weights (FL_GUIDE_PARAMS floats, host). Setting them resets Adam's moments. */
+FL_API fl_status fl_guide_get_weights(fl_guide *guide, float *weights);
+FL_API fl_status fl_guide_set_weights(fl_guide *guide, const float *weights);
+FL_API fl_status fl_guide_get_info(fl_guide *guide, int64_t *adam_steps, float *last_loss);
+/* Training loss and its gradient on n host records (FL_GUIDE_RECORD_FLOATS floats each:
+ * position 3, normal 3, wavelength, direction 3, density, incident radiance, then 8 unused)
+ * in the bounds [bmin, bmax]: grad (FL_GUIDE_PARAMS floats) = d/dweights of
+ * mean_i w_i * -log q(direction_i) with w_i = L_i cos_i / density_i / mean(w). Weights are
+ * unchanged. n <= max_records. */
+FL_API fl_status fl_guide_gradient(fl_guide *guide, const float *records, uint32_t n, const float bmin[3],
+                                   const float bmax[3], float *grad, float *loss);
+/* Mixture parameters (40 floats per record: pi[8], mu[8][3], kappa[8]) for the points of n
+ * host records in the bounds [bmin, bmax]. */
+FL_API fl_status fl_guide_eval(fl_guide *guide, const float *records, uint32_t n, const float bmin[3],
+                               const float bmax[3], float *mixture);
+
 #ifdef __cplusplus
 }
 #endif

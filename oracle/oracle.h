@@ -99,6 +99,16 @@ void orc_camera_ray(const orc_camera *cam, const fl_camera *c, uint32_t pixel, o
 void orc_reflectance(const orc_tables *t, const float rgb[3], int mode, const float *lambda, float *out);
 void orc_xyz_from_spectrum(const orc_tables *t, int mode, const float *lambda, const float *L, double *xyz);
 
+/* ---------------------------------------------------------------- guiding (orc_guide.c) */
+/* 1: evaluate without the GPU's FP16 roundings (for finite-difference checks) */
+void orc_guide_set_exact(int on);
+/* mixture parameters (40 floats per record) of the guide with FP32 weights w32 */
+void orc_guide_eval(const float *w32, const float *rec, uint32_t n, const float bmin[3], const float bmax[3],
+                    float *mix);
+/* gradient of the weighted training loss (FL_GUIDE_PARAMS floats); returns the mean loss */
+float orc_guide_gradient(const float *w32, const float *rec, uint32_t n, const float bmin[3], const float bmax[3],
+                         float *grad);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,11 @@ def lib():
         L.orc_render.argtypes = [P(T.fl_scene_desc), C.c_void_p, P(T.fl_camera), P(T.fl_render_params), C.c_void_p,
                                  P(C.c_double), C.c_void_p]
         L.orc_render.restype = C.c_int
+        L.orc_guide_eval.argtypes = [P(C.c_float), P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float)]
+        L.orc_guide_gradient.argtypes = [P(C.c_float), P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float),
+                                         P(C.c_float)]
+        L.orc_guide_gradient.restype = C.c_float
+        L.orc_guide_set_exact.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -238,3 +243,31 @@ def load_tables_dump(path):
     t["refl60_kat"] = take(4 * 60).reshape(4, 60)
     t["xyz_of_one"] = take(3)
     return t
+
+
+# ----------------------------------------------------------------------------- guiding
+
+def guide_eval(weights, records, bmin, bmax):
+    """mixture parameters (n, 40) of the guide network for the records' points"""
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    r = np.ascontiguousarray(records, dtype=np.float32)
+    out = np.zeros((r.shape[0], 40), np.float32)
+    lib().orc_guide_eval(_fp(w), _fp(r), r.shape[0], _fp(np.asarray(bmin, np.float32)),
+                         _fp(np.asarray(bmax, np.float32)), _fp(out))
+    return out
+
+
+def guide_set_exact(on: bool):
+    """evaluate the guide without FP16 roundings (finite-difference checks)"""
+    lib().orc_guide_set_exact(1 if on else 0)
+
+
+def guide_gradient(weights, records, bmin, bmax):
+    """(gradient, mean loss) of the weighted training loss"""
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    r = np.ascontiguousarray(records, dtype=np.float32)
+    g = np.zeros(w.shape[0], np.float32)
+    loss = lib().orc_guide_gradient(_fp(w), _fp(r), r.shape[0], _fp(np.asarray(bmin, np.float32)),
+                                    _fp(np.asarray(bmax, np.float32)), _fp(g))
+    return g, float(loss)
+

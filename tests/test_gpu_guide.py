@@ -1,0 +1,116 @@
+"""Learned path guiding on the GPU: the tensor-core forward pass and training gradient
+against the CPU oracle, the guided renderer without guiding against fl_render, the
+unbiasedness of the one-sample MIS estimator with an untrained network, and what the
+trained network gains on the caustic scene at equal samples per pixel."""
+import numpy as np
+import pytest
+
+import filianore_b200 as fb
+import guide_records as gr
+import oracle
+from filianore_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+LAYER = [(0, 5120), (5120, 9216), (9216, 13312), (13312, 17408), (17408, 19968)]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = fb.Context(0)
+    yield c
+    c.close()
+
+
+def test_gradient_matches_oracle(ctx):
+    """FP16 tensor-core forward + backward against the oracle (same FP16 roundings, double
+    accumulation): relative L2 error of every layer's gradient below 1e-2."""
+    g = fb.Guide(ctx, max_records=8192, batch=1024)
+    w = gr.weights(seed=11)
+    g.set_weights(w)
+    rec = gr.records(3000, seed=12)
+    gg, lg = g.gradient(rec, gr.BMIN, gr.BMAX)
+    gc, lc = oracle.guide_gradient(w, rec, gr.BMIN, gr.BMAX)
+    assert np.isfinite(gg).all()
+    assert abs(lg / lc - 1) < 1e-3, (lg, lc)
+    for lo, hi in LAYER:
+        err = np.linalg.norm(gg[lo:hi] - gc[lo:hi]) / np.linalg.norm(gc[lo:hi])
+        assert err < 1e-2, (lo, err)
+    g.close()
+
+
+def test_mixture_matches_oracle(ctx):
+    g = fb.Guide(ctx, max_records=8192, batch=1024)
+    w = gr.weights(seed=13)
+    g.set_weights(w)
+    rec = gr.records(1000, seed=14)
+    mg = g.eval(rec, gr.BMIN, gr.BMAX)
+    mc = oracle.guide_eval(w, rec, gr.BMIN, gr.BMAX)
+    assert np.abs(mg[:, :32] - mc[:, :32]).max() < 5e-3
+    assert np.abs(mg[:, 32:] / mc[:, 32:] - 1).max() < 5e-3
+    g.close()
+
+
+def test_unguided_pass_equals_plain_render(ctx):
+    """With guiding off (no sampling, no training) the guided wave loop draws the same
+    random numbers and takes the same paths as fl_render."""
+    sc = scenes.cornell(48, 48)
+    s = ctx.scene(sc)
+    p = scenes.render_params(8, 8, fb.FL_SPECTRAL_HERO4)
+    a = np.zeros((48, 48, 3), np.float64)
+    b = np.zeros((48, 48, 3), np.float64)
+    s.render(p, film_xyz64=a)
+    g = fb.Guide(ctx)
+    g.render(s, p, 0, film_xyz64=b)
+    assert np.array_equal(a, b)
+    g.close()
+    s.close()
+
+
+def test_untrained_guide_is_unbiased(ctx):
+    """One-sample MIS with an arbitrary (untrained) mixture: the image converges to the
+    plain render's. 1024 spp; tolerances are several standard errors."""
+    sc = scenes.cornell(32, 32)
+    s = ctx.scene(sc)
+    p = scenes.render_params(1024, 8, fb.FL_SPECTRAL_HERO4)
+    plain = np.zeros((32, 32, 3), np.float64)
+    s.render(p, film_xyz64=plain)
+    g = fb.Guide(ctx, seed=3, select_prob=0.5)
+    guided = np.zeros((32, 32, 3), np.float64)
+    g.render(s, scenes.render_params(1024, 8, fb.FL_SPECTRAL_HERO4, sample_offset=5000), fb.FL_GUIDE_SAMPLE,
+             film_xyz64=guided)
+    assert abs(guided.mean() / plain.mean() - 1) < 1.5e-2
+    bp = plain.reshape(4, 8, 4, 8, 3).mean(axis=(1, 3))
+    bg = guided.reshape(4, 8, 4, 8, 3).mean(axis=(1, 3))
+    assert np.all(np.abs(bg / bp - 1) < 6e-2), np.abs(bg / bp - 1).max()
+    g.close()
+    s.close()
+
+
+def mse(a, b):
+    return float(np.mean((a - b) ** 2))
+
+
+def test_trained_guide_lowers_caustic_error(ctx):
+    """Caustic scene (glass sphere under a tiny, bright sphere light), 128 x 128: after online
+    training the guided render's error against a 4096-spp plain render is lower than the
+    plain render's at the same number of samples."""
+    sc = scenes.caustic(128, 128, slices=64, stacks=33)
+    s = ctx.scene(sc)
+    H = W = 128
+    ref = np.zeros((H, W, 3), np.float64)
+    s.render(scenes.render_params(4096, 8, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20), film_xyz64=ref)
+    ref /= 4096
+    plain = np.zeros((H, W, 3), np.float64)
+    s.render(scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4), film_xyz64=plain)
+    g = fb.Guide(ctx, seed=5, select_prob=0.5, batch=16384, max_records=1 << 18, steps_per_wave=8)
+    for k in range(24):
+        flags = fb.FL_GUIDE_TRAIN | (fb.FL_GUIDE_SAMPLE if k > 0 else 0)
+        g.render(s, scenes.render_params(16, 8, fb.FL_SPECTRAL_HERO4, sample_offset=(1 << 16) + 16 * k), flags)
+    assert g.info()["adam_steps"] > 0
+    guided = np.zeros((H, W, 3), np.float64)
+    g.render(s, scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4), fb.FL_GUIDE_SAMPLE, film_xyz64=guided)
+    e_plain, e_guided = mse(plain / 64, ref), mse(guided / 64, ref)
+    assert e_guided < 0.7 * e_plain, (e_guided, e_plain)
+    g.close()
+    s.close()
