@@ -45,6 +45,12 @@ TRI_BYTES = 48
 RAY_BYTES = 32
 HIT_BYTES = 16
 RENDER = {"width": 1920, "height": 1080, "spp": 64, "depth": 16}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the roofline kernels,
+# measured with one-pass ncu captures of this command on a B200:
+#   raycast: one k_trace launch over the full 16,777,216 rays: 32.73 + 1.21 GB
+#   render:  k_trace_paths + k_trace_rays2 over the first 8 of the frame's 64 waves
+#            (272 launches): 5.762 + 0.368 GB, times 8 for the frame
+TRAFFIC = {"raycast": 33.94e9, "render": 49.04e9}
 
 
 def load_peaks():
@@ -285,9 +291,11 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
 def gpu_guide(args, world, rank, local, barrier, reduce_max):
     """Learned path guiding on the caustic scene (1024 x 1024; glass sphere of 65,536
     triangles under a sphere light of radius 0.02 and radiance 5e3; Lambert room of 12
-    triangles, albedo 0.7; max depth 8, hero wavelengths): the plain GPU path at 64 spp
-    against guided renders given a fraction of its wall time (training online during the
-    first 25% of each budget, passes of 4 spp), errors against a 4096-spp FP64 plain render."""
+    triangles, albedo 0.7; max depth 8, hero wavelengths): the plain GPU path at 256 spp
+    (--spp) against guided renders given a fraction of its wall time (training online during
+    the first 25% of each budget, passes of 4 spp), errors against a 4096-spp FP64 plain
+    render. The error is also split into the caustic region (the brightest 3% of the
+    reference) and the rest, with the mean radiance of the rest."""
     import filianore_b200 as fb
     from filianore_b200 import scenes
     R = RENDER["width"] if args.size else 1024
@@ -295,38 +303,53 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
     sc = scenes.caustic(R, R)
     ctx = fb.Context(local)
     s = ctx.scene(sc)
-    n_ref = args.spp if args.spp else 4096
+    n_ref = 4096
+    n_plain = args.spp if args.spp else 256
     ref = np.zeros((R, R, 3), np.float64)
     _, rst = s.render(scenes.render_params(n_ref, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 24), film_xyz64=ref)
     ref /= n_ref
+    lum = ref[..., 1]
+    region = lum >= np.quantile(lum, 0.97)
 
-    def mse(img, spp):
-        return float(np.mean((img / spp - ref) ** 2))
-    # plain: 64 spp, timed through the C ABI (wall time of the call)
+    def errors(img, spp):
+        e = np.mean((img / spp - ref) ** 2, axis=2)
+        return {"mse": float(e.mean()), "mse_caustic_region": float(e[region].mean()),
+                "mse_rest": float(e[~region].mean()), "mean_rest": float((img[~region] / spp).mean())}
     plain = np.zeros((R, R, 3), np.float64)
     s.render(scenes.render_params(4, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 22))  # warm-up
     t0 = time.perf_counter()
-    _, pst = s.render(scenes.render_params(64, depth, fb.FL_SPECTRAL_HERO4), film_xyz64=plain)
+    _, pst = s.render(scenes.render_params(n_plain, depth, fb.FL_SPECTRAL_HERO4), film_xyz64=plain)
     t_plain = (time.perf_counter() - t0) * 1e3
-    e_plain = mse(plain, 64)
+    e_plain = errors(plain, n_plain)
     runs = []
-    for frac in (1 / 8, 1 / 4, 1 / 3, 1 / 2, 1.0):
-        g = fb.Guide(ctx, seed=5, select_prob=0.5, batch=16384, max_records=1 << 19, steps_per_wave=16)
+    for frac in (1 / 3, 1 / 2, 1.0):
+        g = fb.Guide(ctx, seed=5, select_prob=0.5, batch=16384, max_records=1 << 21, steps_per_wave=64)
         img = np.zeros((R, R, 3), np.float64)
         t0 = time.perf_counter()
         _, gst = g.render_timed(s, scenes.render_params(4, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20),
                                 budget_ms=frac * t_plain, train_fraction=0.25, film_xyz64=img)
         wall = (time.perf_counter() - t0) * 1e3
         spp = gst["paths"] // (R * R)
-        runs.append({"budget_frac": round(frac, 4), "wall_ms": round(wall, 1), "spp": int(spp),
-                     "mse": mse(img, spp), "adam_steps": g.info()["adam_steps"]})
+        run = {"budget_frac": round(frac, 4), "wall_ms": round(wall, 1), "spp": int(spp),
+               "adam_steps": g.info()["adam_steps"]}
+        run.update(errors(img, spp))
+        if frac == 1.0:
+            # the trained guide at the plain render's sample count (sampling only)
+            img2 = np.zeros((R, R, 3), np.float64)
+            t0 = time.perf_counter()
+            g.render(s, scenes.render_params(n_plain, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 21),
+                     fb.FL_GUIDE_SAMPLE, film_xyz64=img2)
+            eq = {"wall_ms": round((time.perf_counter() - t0) * 1e3, 1)}
+            eq.update(errors(img2, n_plain))
+            run["trained_equal_spp"] = eq
+        runs.append(run)
         g.close()
-    ok = [r for r in runs if r["mse"] <= e_plain]
+    ok = [r for r in runs if r["mse"] <= e_plain["mse"]]
     t_match = min(r["wall_ms"] for r in ok) if ok else None
     s.close()
     ctx.close()
     equal_time = runs[-1]
-    return {"metric": "guided wall time to the plain 64-spp MSE / plain wall time",
+    return {"metric": f"guided wall time to the plain {n_plain}-spp MSE / plain wall time",
             "value": round(t_match / t_plain, 4) if t_match else None, "unit": "ratio", "n_gpus": world,
             "steps": len(runs), "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 render, f16 weights / f32 accumulate", "data": "synthetic",
@@ -334,9 +357,9 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
                                    f"L 5e3, depth {depth}; MLP 80-64x4-40 (8 vMF lobes), Adam lr 1e-2, one-sample "
                                    "MIS c 0.5, training in the first 25% of each budget",
                        "reference_spp": n_ref, "parallelism": "1 GPU"},
-            "plain": {"spp": 64, "wall_ms": round(t_plain, 1), "device_ms": round(pst["ms"], 1), "mse": e_plain},
-            "guided": runs, "equal_time_mse_ratio": round(e_plain / equal_time["mse"], 3),
-            "reference_ms": round(rst["ms"], 1)}
+            "plain": dict(spp=n_plain, wall_ms=round(t_plain, 1), device_ms=round(pst["ms"], 1), **e_plain),
+            "guided": runs, "equal_time_mse_ratio": round(e_plain["mse"] / equal_time["mse"], 3),
+            "reference": {"spp": n_ref, "device_ms": round(rst["ms"], 1), "mean_rest": float(ref[~region].mean())}}
 
 
 def config_of(workload, world):
@@ -439,8 +462,10 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
         TRI_BYTES * cstats["tris_tested"]
     achieved = alg_bytes / (trav_ms / 1e3) / 1e9
     share = {k: round(prof[f"ms_{k}"] / prof["ms"], 4) for k in ("trace", "shade", "shadow", "continue")}
+    full = RENDER["width"] == 1920 and RENDER["height"] == 1080 and RENDER["spp"] == 64
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None, "peak_src": peaks["src"],
+                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": TRAFFIC["render"] if full else None,
+                "traffic_unit": "bytes per frame (ncu, 8 of 64 waves x 8)", "peak_src": peaks["src"],
                 "kernel": "BVH traversal (k_trace_paths + k_trace_rays2)",
                 "alg_bytes_per_frame": int(alg_bytes), "traversal_ms_per_frame": round(trav_ms, 3),
                 "profiled_frame_ms": round(prof["ms"], 3),
@@ -517,8 +542,9 @@ def gpu_raycast(args, world, rank, local, barrier, reduce_max):
     launch_ms = statistics.mean(per_launch)
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None, "peak_src": peaks["src"],
-                "kernel": "k_trace<closest>", "alg_bytes_per_launch": int(alg_bytes),
+                "frac": round(achieved / peaks["hbm_gbs"], 4),
+                "traffic": TRAFFIC["raycast"] if N_RAYS == 1 << 24 else None, "traffic_unit": "bytes per launch (ncu)",
+                "peak_src": peaks["src"], "kernel": "k_trace<closest>", "alg_bytes_per_launch": int(alg_bytes),
                 "nodes_per_ray": round(nodes / N_RAYS, 2), "tris_per_ray": round(trisv / N_RAYS, 2)}
     line = {"metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,

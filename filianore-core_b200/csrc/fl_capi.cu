@@ -231,6 +231,12 @@ fl_status fl_context_create(int32_t device, const fl_spectral_tables *t, fl_cont
 fl_status fl_context_destroy(fl_context *ctx_h) {
     Context *ctx = reinterpret_cast<Context *>(ctx_h);
     if (!ctx) return FL_ERR_INVALID;
+    if (ctx->children.load() != 0) {
+        // scenes, guides or servers still refer to this context: keep it alive rather than
+        // leave them dangling
+        set_error(ctx, "context still has live scenes, guides or servers");
+        return FL_ERR_INVALID;
+    }
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
@@ -390,6 +396,8 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
 #undef SC_TRY
     fl_status rc = build_bvh(s);
     if (rc != FL_OK) return fail(rc);
+    ctx->children++;
+    s->counted = true;
     *out = reinterpret_cast<fl_scene *>(s);
     return FL_OK;
 }
@@ -407,6 +415,7 @@ fl_status fl_scene_destroy(fl_scene *scene) {
     cudaFree(s->materials);
     cudaFree(s->lights);
     cudaFree(s->mat_refl60);
+    if (s->counted) s->ctx->children--;
     delete s;
     return FL_OK;
 }

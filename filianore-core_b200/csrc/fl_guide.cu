@@ -4,7 +4,12 @@
 // Training minimises the radiance-weighted KL divergence between the normalised incident
 // radiance (times the cosine) and the guide's mixture q, estimated from the renderer's own
 // samples: loss = mean_i w_i * -log q(w_i | x_i), w_i = L_i cos_i / p_i / mean(w)
-// (p_i: the density the direction was sampled with). One CTA of 8 warps takes 128 records:
+// (p_i: the density the direction was sampled with). During rendering the minibatches are
+// drawn from the wave's records with probability proportional to w_i (stratified, by
+// inverse CDF over a prefix sum) and weighted 1: the same expected gradient, but the rare
+// records that carry most of the weight (caustic paths) are in every batch instead of in
+// one batch out of many. fl_guide_gradient evaluates the weighted loss over the given
+// records in order instead. One CTA of 8 warps takes 128 records:
 // each warp runs the forward pass of 16 records with the activations kept in shared
 // memory, the head gradient is computed per record in FP32, and the backward pass goes
 // layer by layer, the weight gradients dW^T = A^T dZ as tensor-core products over the
@@ -16,6 +21,8 @@
 #include <cmath>
 #include <mutex>
 #include <vector>
+
+#include <cub/device/device_scan.cuh>
 
 #include "fl_render.cuh"
 
@@ -41,7 +48,19 @@ struct TrainArgs {
     const float *wstat;        // [0] sum of record weights, [1] number of records
     float *loss;               // [0] += sum of weighted losses of the batch
     float bmin[3], binv[3];
+    const float *cdf;          // resampling: inclusive prefix sum of the record weights (null: in order)
+    uint32_t seed;             // resampling: stratification jitter of this batch
 };
+
+__device__ inline float hash01(uint32_t a, uint32_t b) {
+    uint32_t h = a * 0x9e3779b1u ^ (b + 0x7f4a7c15u) * 0x85ebca77u;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    return (float)(h >> 8) * (1.f / 16777216.f);
+}
 
 // record weight L cos / p (0 when the record cannot be learnt from)
 __device__ inline float record_weight(const float *R) {
@@ -90,11 +109,12 @@ __device__ inline float guide_head_grad(const float *h, v3 w, float *dh) {
         dh[8 + 3 * j] = (gx - mu[j][0] * mg) / len[j];
         dh[9 + 3 * j] = (gy - mu[j][1] * mg) / len[j];
         dh[10 + 3 * j] = (gz - mu[j][2] * mg) / len[j];
-        // log concentration: d log q_j / d log kappa = 1 - 2 kappa / expm1(2 kappa) + kappa (mu.w - 1)
-        const float sj = h[32 + j];
-        const bool inside = sj > kLogKappaMin && sj < kLogKappaMax;
+        // concentration: d log q_j / d log kappa = 1 - 2 kappa / expm1(2 kappa) + kappa (mu.w - 1),
+        // d log kappa / ds = (max - min) sigmoid' (s - shift)
+        const float sg = guide_sigmoid(h[32 + j]);
         const float k = kap[j];
-        dh[32 + j] = inside ? -r * (1.f - 2.f * k / expm1f(2.f * k) + k * (dp[j] - 1.f)) : 0.f;
+        dh[32 + j] = -r * (1.f - 2.f * k / expm1f(2.f * k) + k * (dp[j] - 1.f)) *
+                     (kLogKappaMax - kLogKappaMin) * sg * (1.f - sg);
     }
     return -lse;
 }
@@ -163,9 +183,11 @@ __device__ inline void guide_back_warp(const __half *Dcur, int Kt, const __half 
 __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
     extern __shared__ __align__(16) unsigned char tsm[];
     const uint32_t n_total = min(*T.rec_count, T.rec_cap);
-    const uint32_t begin = T.batch_begin + blockIdx.x * kTrainRows;
-    const uint32_t end = min(T.batch_begin + T.batch_size, n_total);
+    const uint32_t begin = T.cdf ? blockIdx.x * kTrainRows : T.batch_begin + blockIdx.x * kTrainRows;
+    const uint32_t end = T.cdf ? (n_total ? T.batch_size : 0u) : min(T.batch_begin + T.batch_size, n_total);
     if (begin >= end || !(T.wstat[0] > 0.f)) return;
+    const float total = T.cdf ? T.cdf[n_total - 1] : 0.f;
+    if (T.cdf && !(total > 0.f)) return;
     __half *sw = reinterpret_cast<__half *>(tsm);
     __half *X = sw + kSmWHalves;
     __half *Act = X + kTrainRows * kLdIn;
@@ -176,8 +198,20 @@ __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
     guide_stage_weights(sw, T.w);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = warp * 16;
-    const uint32_t i = begin + r0 + (lane & 15);
+    uint32_t i = begin + r0 + (lane & 15);
     const bool valid = i < end;
+    if (T.cdf && valid) {
+        // stratified draw proportional to the record weights: first record whose
+        // inclusive prefix sum exceeds u
+        const float u = ((float)i + hash01(T.seed, i)) / (float)T.batch_size * total;
+        uint32_t lo = 0, hi = n_total - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (T.cdf[mid] > u) hi = mid;
+            else lo = mid + 1;
+        }
+        i = lo;
+    }
     const float *R = T.rec + (size_t)(valid ? i : 0) * kRecFloats;
     // features of this warp's 16 records (two lanes per record)
     {
@@ -201,7 +235,8 @@ __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
         float loss = 0.f;
         if (valid) {
             const float wmean = T.wstat[0] / fmaxf(T.wstat[1], 1.f);
-            const float wn = fminf(record_weight(R) / wmean, kWeightClamp);
+            const float wr = record_weight(R);
+            const float wn = T.cdf ? (wr > 0.f ? 1.f : 0.f) : fminf(wr / wmean, kWeightClamp);
             if (wn > 0.f) {
                 const float nl = guide_head_grad(Head + (r0 + lane) * kHeadLd, mk(R[7], R[8], R[9]), dh);
                 loss = wn * nl;
@@ -236,12 +271,16 @@ __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
     guide_dw(X, kLdIn, 5, DzA, 8, T.grad + guide_woff(0), 80, 64);
 }
 
-// sum and count of the record weights of this wave
-__global__ void k_guide_stats(const float *rec, const uint32_t *rec_count, uint32_t rec_cap, float *wstat) {
+// sum and count of the record weights of this wave (and the weights themselves, when asked)
+__global__ void k_guide_stats(const float *rec, const uint32_t *rec_count, uint32_t rec_cap, float *wstat,
+                              float *weights) {
     const uint32_t n = min(*rec_count, rec_cap);
     float s = 0.f;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        s += record_weight(rec + (size_t)i * kRecFloats);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float w = record_weight(rec + (size_t)i * kRecFloats);
+        if (weights) weights[i] = w;
+        s += w;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0 && s != 0.f) atomicAdd(&wstat[0], s);
@@ -255,6 +294,7 @@ struct AdamArgs {
     uint32_t rec_cap, batch_begin, batch_size;
     const float *wstat;
     float lr, bc1, bc2;  // step size and the bias corrections 1 - beta^t
+    int resampled;       // batches drawn by weight: always batch_size records
 };
 
 // Adam (beta1 0.9, beta2 0.999, eps 1e-8) on the mean gradient of the batch; clears the gradient.
@@ -262,9 +302,9 @@ __global__ void k_guide_adam(AdamArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kGuideParams) return;
     const uint32_t n = min(*a.rec_count, a.rec_cap);
-    const bool step = a.batch_begin < n && a.wstat[0] > 0.f;
+    const bool step = (a.resampled ? n > 0 : a.batch_begin < n) && a.wstat[0] > 0.f;
     if (step) {
-        const float cnt = (float)min(a.batch_size, n - a.batch_begin);
+        const float cnt = a.resampled ? (float)a.batch_size : (float)min(a.batch_size, n - a.batch_begin);
         float g = a.grad[i] / (kLossScale * cnt);
         if (!isfinite(g)) g = 0.f;
         const float m = 0.9f * a.m[i] + 0.1f * g;
@@ -280,13 +320,14 @@ __global__ void k_guide_adam(AdamArgs a) {
 }
 
 // mixture parameters for host-given records (fl_guide_eval)
-__global__ void __launch_bounds__(128) k_guide_eval(const __half *w, const float *rec, uint32_t n, float b0, float b1,
-                                                    float b2, float i0, float i1, float i2, float *out) {
+__global__ void __launch_bounds__(32 * kInferWarps) k_guide_eval(const __half *w, const float *rec, uint32_t n, float b0,
+                                                                 float b1, float b2, float i0, float i1, float i2,
+                                                                 float *out) {
     extern __shared__ __align__(16) unsigned char gsm[];
     __half *sw = reinterpret_cast<__half *>(gsm);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __half *X = reinterpret_cast<__half *>(gsm + kSmWHalves * 2) + warp * 16 * kLdIn;
-    float *head = reinterpret_cast<float *>(gsm + kSmWHalves * 2 + kInferWarps * 16 * kLdIn * 2) + warp * 16 * kHeadLd;
+    float *head = reinterpret_cast<float *>(X);
     guide_stage_weights(sw, w);
     const float bmin[3] = {b0, b1, b2}, binv[3] = {i0, i1, i2};
     for (uint32_t chunk = blockIdx.x * kInferWarps + warp; chunk * 16 < n; chunk += gridDim.x * kInferWarps) {
@@ -320,6 +361,9 @@ struct Guide {
     float *mix = nullptr;
     uint32_t *rec_idx = nullptr;
     size_t slot_cap = 0;
+    float *wts = nullptr, *cdf = nullptr;  // per-record weights and their prefix sum
+    void *scan_tmp = nullptr;
+    size_t scan_bytes = 0;
     uint32_t *h_count = nullptr;  // pinned
     float *h_loss = nullptr;      // pinned
     int64_t steps = 0;
@@ -360,7 +404,7 @@ static fl_status guide_slots(Guide *G, size_t cap) {
     G->mix = nullptr;
     G->rec_idx = nullptr;
     G->slot_cap = 0;
-    FL_CUDA_TRY(ctx, cudaMalloc(&G->mix, cap * kGuideOut * sizeof(float)));
+    FL_CUDA_TRY(ctx, cudaMalloc(&G->mix, cap * kMixFloats * sizeof(float)));
     FL_CUDA_TRY(ctx, cudaMalloc(&G->rec_idx, cap * 2 * sizeof(uint32_t)));
     G->slot_cap = cap;
     return FL_OK;
@@ -380,8 +424,10 @@ static fl_status guide_train(Guide *G, uint32_t n, const float bmin[3], const fl
     FL_CUDA_TRY(ctx, cudaMemsetAsync(G->wstat, 0, 2 * sizeof(float), st));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(G->loss, 0, sizeof(float), st));
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
-    k_guide_stats<<<std::min<uint32_t>((n + 255) / 256, (uint32_t)sms * 4), 256, 0, st>>>(G->rec, G->rec_count,
-                                                                                           G->cfg.max_records, G->wstat);
+    k_guide_stats<<<std::min<uint32_t>((n + 255) / 256, (uint32_t)sms * 4), 256, 0, st>>>(
+        G->rec, G->rec_count, G->cfg.max_records, G->wstat, G->wts);
+    size_t tmp = G->scan_bytes;
+    FL_CUDA_TRY(ctx, cub::DeviceScan::InclusiveSum(G->scan_tmp, tmp, G->wts, G->cdf, (int)n, st));
     const uint32_t B = (uint32_t)G->cfg.batch;
     const uint32_t n_steps = std::min<uint32_t>((n + B - 1) / B, (uint32_t)G->cfg.steps_per_wave);
     for (uint32_t k = 0; k < n_steps; ++k) {
@@ -399,6 +445,8 @@ static fl_status guide_train(Guide *G, uint32_t n, const float bmin[3], const fl
             T.bmin[a] = bmin[a];
             T.binv[a] = binv[a];
         }
+        T.cdf = G->cdf;
+        T.seed = (uint32_t)G->steps;
         k_guide_train<<<(B + kTrainRows - 1) / kTrainRows, 32 * kTrainWarps, kTrainSmem, st>>>(T);
         G->steps += 1;
         AdamArgs a{};
@@ -415,6 +463,7 @@ static fl_status guide_train(Guide *G, uint32_t n, const float bmin[3], const fl
         a.lr = G->cfg.learning_rate;
         a.bc1 = 1.f - powf(0.9f, (float)G->steps);
         a.bc2 = 1.f - powf(0.999f, (float)G->steps);
+        a.resampled = 1;
         k_guide_adam<<<(kGuideParams + 255) / 256, 256, 0, st>>>(a);
     }
     FL_CUDA_TRY(ctx, cudaGetLastError());
@@ -438,6 +487,7 @@ static fl_status guide_pass(Guide *G, Scene *s, const CamDev &cam, const fl_rend
     const bool train = (flags & FL_GUIDE_TRAIN) != 0;
     float binv[3];
     bounds_of(s->bmin, s->bmax, binv);
+    for (int a = 0; a < 3; ++a) binv[a] *= G->cfg.position_scale;
     GuideArgs &ga = W.A.g;
     ga.w = G->w16;
     ga.mix = G->mix;
@@ -553,7 +603,7 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     const fl_guide_config c = *cfg;
     if (!(c.learning_rate > 0.f) || !(c.select_prob >= 0.f && c.select_prob < 1.f) || c.batch < 128 ||
         c.batch > 65536 || c.batch % 128 != 0 || c.max_records < c.batch || c.max_records > (1 << 26) ||
-        c.steps_per_wave < 1) {
+        c.steps_per_wave < 1 || !(c.position_scale >= 0.f && c.position_scale <= 1.f)) {
         set_error(ctx, "invalid guide configuration");
         return FL_ERR_INVALID;
     }
@@ -566,11 +616,13 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     Guide *G = new Guide();
     G->ctx = ctx;
     G->cfg = c;
+    if (G->cfg.position_scale == 0.f) G->cfg.position_scale = 1.f;
     const size_t P = align_up(kGuideParams * sizeof(float));
     const size_t bytes = align_up(kGuideParams * sizeof(__half)) + 4 * P + 256 + 256 + 256;
     auto fail = [&](cudaError_t e, const char *what) {
         cudaFree(G->mem);
         cudaFree(G->rec);
+        cudaFree(G->wts);
         cudaFreeHost(G->h_count);
         cudaFreeHost(G->h_loss);
         delete G;
@@ -580,6 +632,13 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     if (e) return fail(e, "guide state");
     e = cudaMalloc(&G->rec, (size_t)c.max_records * kRecFloats * sizeof(float));
     if (e) return fail(e, "guide records");
+    e = cub::DeviceScan::InclusiveSum(nullptr, G->scan_bytes, (const float *)nullptr, (float *)nullptr,
+                                      c.max_records, ctx->stream);
+    if (e) return fail(e, "guide scan size");
+    e = cudaMalloc(&G->wts, align_up((size_t)c.max_records * sizeof(float)) * 2 + G->scan_bytes);
+    if (e) return fail(e, "guide record weights");
+    G->cdf = reinterpret_cast<float *>(reinterpret_cast<char *>(G->wts) + align_up((size_t)c.max_records * sizeof(float)));
+    G->scan_tmp = reinterpret_cast<char *>(G->cdf) + align_up((size_t)c.max_records * sizeof(float));
     e = cudaMallocHost(&G->h_count, sizeof(uint32_t));
     if (e) return fail(e, "guide pinned counter");
     e = cudaMallocHost(&G->h_loss, sizeof(float));
@@ -602,11 +661,13 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     if (rc) {
         cudaFree(G->mem);
         cudaFree(G->rec);
+        cudaFree(G->wts);
         cudaFreeHost(G->h_count);
         cudaFreeHost(G->h_loss);
         delete G;
         return rc;
     }
+    ctx->children++;
     *out = reinterpret_cast<fl_guide *>(G);
     return FL_OK;
 }
@@ -620,10 +681,12 @@ extern "C" fl_status fl_guide_destroy(fl_guide *g_h) {
     cudaStreamSynchronize(ctx->stream);
     cudaFree(G->mem);
     cudaFree(G->rec);
+    cudaFree(G->wts);
     cudaFree(G->mix);
     cudaFree(G->rec_idx);
     cudaFreeHost(G->h_count);
     cudaFreeHost(G->h_loss);
+    ctx->children--;
     delete G;
     return FL_OK;
 }
@@ -766,8 +829,8 @@ extern "C" fl_status fl_guide_gradient(fl_guide *g_h, const float *records, uint
     FL_CUDA_TRY(ctx, cudaMemsetAsync(G->loss, 0, sizeof(float), st));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(G->grad, 0, sizeof(float) * kGuideParams, st));
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
-    k_guide_stats<<<std::min<uint32_t>((n + 255) / 256, (uint32_t)sms * 4), 256, 0, st>>>(G->rec, G->rec_count,
-                                                                                           G->cfg.max_records, G->wstat);
+    k_guide_stats<<<std::min<uint32_t>((n + 255) / 256, (uint32_t)sms * 4), 256, 0, st>>>(
+        G->rec, G->rec_count, G->cfg.max_records, G->wstat, nullptr);
     TrainArgs T{};
     T.w = G->w16;
     T.grad = G->grad;
@@ -796,6 +859,25 @@ extern "C" fl_status fl_guide_gradient(fl_guide *g_h, const float *records, uint
     return FL_OK;
 }
 
+extern "C" fl_status fl_guide_get_records(fl_guide *g_h, float *records, uint32_t max_n, uint32_t *n) {
+    Guide *G = reinterpret_cast<Guide *>(g_h);
+    if (!G || !n || (max_n && !records)) return FL_ERR_INVALID;
+    Context *ctx = G->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    FL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    uint32_t cnt = 0;
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(&cnt, G->rec_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    FL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    cnt = std::min<uint32_t>(cnt, (uint32_t)G->cfg.max_records);
+    const uint32_t m = std::min(cnt, max_n);
+    if (m)
+        FL_CUDA_TRY(ctx, cudaMemcpyAsync(records, G->rec, (size_t)m * kRecFloats * sizeof(float), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+    FL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *n = m;
+    return FL_OK;
+}
+
 extern "C" fl_status fl_guide_eval(fl_guide *g_h, const float *records, uint32_t n, const float bmin[3],
                                    const float bmax[3], float *mixture) {
     Guide *G = reinterpret_cast<Guide *>(g_h);
@@ -820,7 +902,8 @@ extern "C" fl_status fl_guide_eval(fl_guide *g_h, const float *records, uint32_t
     float *d_out = reinterpret_cast<float *>(reinterpret_cast<char *>(G->rec) + rec_bytes);
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(d_rec, records, (size_t)n * kRecFloats * sizeof(float), cudaMemcpyHostToDevice, st));
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
-    k_guide_eval<<<std::min<uint32_t>((n + 63) / 64, (uint32_t)sms * 2), 128, guide_infer_smem_bytes(), st>>>(
+    k_guide_eval<<<std::min<uint32_t>((n + 16 * kInferWarps - 1) / (16 * kInferWarps), (uint32_t)sms * 3),
+                   32 * kInferWarps, guide_infer_smem_bytes(), st>>>(
         G->w16, d_rec, n, bmin[0], bmin[1], bmin[2], binv[0], binv[1], binv[2], d_out);
     FL_CUDA_TRY(ctx, cudaGetLastError());
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(mixture, d_out, (size_t)n * kGuideOut * sizeof(float), cudaMemcpyDeviceToHost, st));

@@ -38,7 +38,10 @@ constexpr int kGuideLayers = 5;
 constexpr int kLdIn = 88, kLdH = 72, kHeadRowsPad = 48;
 constexpr int kSmWHalves = 64 * 88 + 3 * 64 * 72 + 48 * 72;  // 22,912
 constexpr int kHeadLd = 44;                                  // floats per head row in shared memory
-constexpr float kLogKappaMin = -2.f, kLogKappaMax = 7.f;
+// log concentration = min + (max - min) * sigmoid(s - shift): bounded, with a gradient
+// everywhere (a clamp would freeze a lobe that overshoots), about 0.4 at s = 0
+constexpr float kLogKappaMin = -2.f, kLogKappaMax = 7.f, kLogKappaShift = 2.f;
+constexpr int kMixFloats = 48;  // per path slot: pi[8], mu[8][3], kappa[8], log(pi * vMF normalisation)[8]
 constexpr int kRecFloats = 20;  // training record, see GuideArgs
 constexpr uint32_t kNoRecord = 0xffffffffu;
 
@@ -55,7 +58,7 @@ __host__ __device__ constexpr int guide_sm_ld(int l) { return l == 0 ? kLdIn : k
 // (per hero wavelength, before Russian roulette), 16-19 radiance gathered before it.
 struct GuideArgs {
     const __half *w;      // packed FP16 weights
-    float *mix;           // kGuideOut floats per path slot: pi[8], mu[8][3], kappa[8]; pi[0] < 0 = unusable
+    float *mix;           // kMixFloats per path slot (see kMixFloats); pi[0] < 0 = unusable
     uint32_t *rec_idx;    // 2 x cap open records per path (kNoRecord = none)
     float *rec;           // records
     uint32_t *rec_count;  // records written this wave
@@ -132,56 +135,30 @@ __device__ inline void guide_stage_weights(__half *sw, const __half *__restrict_
 // --------------------------------------------------------------------------- input encoding
 
 // Half of one point's 80 features (part 0: features 0..39, part 1: 40..79) as FP16, written
-// to `row` + 40 * part. pn is the position normalised to [0, 1]^3.
+// to `row` + 40 * part. pn is the position normalised to [0, 1]^3. Feature 2 (12 a + k) + {0, 1}
+// is sin / cos(2^k pi pn[a]); both halves of a warp run the same loop over their 20
+// (axis, band) pairs, so the two parts do not serialise.
 __device__ inline void guide_encode_part(const float pn[3], const float nf[3], float lam01, int part, __half *row) {
-    float f[40];
-    if (part == 0) {
+    uint32_t h[20];  // feature pairs as packed FP16
 #pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            float s, c;
-            sincospif(pn[0] * (float)(1 << k), &s, &c);
-            f[2 * k] = s;
-            f[2 * k + 1] = c;
-        }
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            float s, c;
-            sincospif(pn[1] * (float)(1 << k), &s, &c);
-            f[24 + 2 * k] = s;
-            f[24 + 2 * k + 1] = c;
-        }
-    } else {
-#pragma unroll
-        for (int k = 8; k < 12; ++k) {
-            float s, c;
-            sincospif(pn[1] * (float)(1 << k), &s, &c);
-            f[2 * (k - 8)] = s;
-            f[2 * (k - 8) + 1] = c;
-        }
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            float s, c;
-            sincospif(pn[2] * (float)(1 << k), &s, &c);
-            f[8 + 2 * k] = s;
-            f[8 + 2 * k + 1] = c;
-        }
-        f[32] = nf[0];
-        f[33] = nf[1];
-        f[34] = nf[2];
-        f[35] = lam01;
-        f[36] = 1.f;
-        f[37] = f[38] = f[39] = 0.f;
+    for (int i = 0; i < 20; ++i) {
+        const int pair = 20 * part + i;  // (axis, band) = (pair / 12, pair % 12); pairs >= 36 are not sines
+        const int a = pair < 36 ? pair / 12 : 0, k = pair < 36 ? pair % 12 : 0;
+        const float x = a == 0 ? pn[0] : (a == 1 ? pn[1] : pn[2]);
+        float sv, cv;
+        sincospif(x * __int_as_float((127 + k) << 23), &sv, &cv);
+        h[i] = pack_h2(sv, cv, false);
+    }
+    if (part == 1) {
+        // features 72..79
+        h[16] = pack_h2(nf[0], nf[1], false);
+        h[17] = pack_h2(nf[2], lam01, false);
+        h[18] = pack_h2(1.f, 0.f, false);
+        h[19] = 0u;
     }
     uint4 *dst = reinterpret_cast<uint4 *>(row + 40 * part);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
-        uint4 v;
-        v.x = pack_h2(f[8 * q + 0], f[8 * q + 1], false);
-        v.y = pack_h2(f[8 * q + 2], f[8 * q + 3], false);
-        v.z = pack_h2(f[8 * q + 4], f[8 * q + 5], false);
-        v.w = pack_h2(f[8 * q + 6], f[8 * q + 7], false);
-        dst[q] = v;
-    }
+    for (int q = 0; q < 5; ++q) dst[q] = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
 }
 
 __device__ inline void guide_normalise(const float bmin[3], const float binv[3], v3 p, float pn[3]) {
@@ -201,33 +178,34 @@ __device__ inline void guide_encode_record(const float *R, const float bmin[3], 
 
 // --------------------------------------------------------------------------- forward pass
 
-// One warp: the network on 16 points whose features are rows 0..15 of X (ld kLdIn).
+// One warp: the network on 16 points whose features are rows 0..15 of X (ld kLdIn); X is
+// read only by the first layer, so `head` may alias it.
 // When `act` is set, the four post-ReLU hidden layers are also stored to act + l * act_stride
 // (rows 0..15, ld kLdH) for the backward pass. The head goes to `head` (16 x kHeadLd floats).
 __device__ inline void guide_forward_warp(const __half *sw, const __half *X, __half *act, int act_stride,
                                           float *head) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    uint32_t a[5][4];
-#pragma unroll
-    for (int kt = 0; kt < 5; ++kt) ldsm_x4(a[kt], X + (lane & 15) * kLdIn + kt * 16 + (lane >> 4) * 8);
     // B operand rows (output features) and column half picked by this lane for x4 loads of two n-tiles
     const int brow = (lane & 7) + ((lane >> 4) << 3), bcol = ((lane >> 3) & 1) * 8;
     uint32_t h[4][4];
-    // layer 1 (K = 80)
+    // layer 1 (K = 80): one A tile of the features at a time
     {
         float acc[8][4];
 #pragma unroll
         for (int n = 0; n < 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
         const __half *W = sw + guide_sm_off(0);
 #pragma unroll
-        for (int np = 0; np < 4; ++np)
+        for (int kt = 0; kt < 5; ++kt) {
+            uint32_t a[4];
+            ldsm_x4(a, X + (lane & 15) * kLdIn + kt * 16 + (lane >> 4) * 8);
 #pragma unroll
-            for (int kt = 0; kt < 5; ++kt) {
+            for (int np = 0; np < 4; ++np) {
                 uint32_t b[4];
                 ldsm_x4(b, W + (np * 16 + brow) * kLdIn + kt * 16 + bcol);
-                mma16816(acc[2 * np], a[kt], b[0], b[1]);
-                mma16816(acc[2 * np + 1], a[kt], b[2], b[3]);
+                mma16816(acc[2 * np], a, b[0], b[1]);
+                mma16816(acc[2 * np + 1], a, b[2], b[3]);
             }
+        }
 #pragma unroll
         for (int kt = 0; kt < 4; ++kt) {
             h[kt][0] = pack_h2(acc[2 * kt][0], acc[2 * kt][1], true);
@@ -313,13 +291,17 @@ __device__ inline void guide_forward_warp(const __half *sw, const __half *X, __h
 
 // --------------------------------------------------------------------------- vMF mixture
 
-__device__ inline float guide_kappa(float s) { return expf(fminf(fmaxf(s, kLogKappaMin), kLogKappaMax)); }
+__device__ inline float guide_sigmoid(float s) { return 1.f / (1.f + expf(-(s - kLogKappaShift))); }
+__device__ inline float guide_log_kappa(float s) { return kLogKappaMin + (kLogKappaMax - kLogKappaMin) * guide_sigmoid(s); }
+__device__ inline float guide_kappa(float s) { return expf(guide_log_kappa(s)); }
 // log of the vMF normalisation kappa / (2 pi (1 - exp(-2 kappa)))
 __device__ inline float vmf_log_norm(float k) { return logf(k) - 1.8378770664f - logf(-expm1f(-2.f * k)); }
+__device__ inline float vmf_log_norm2(float k, float logk) { return logk - 1.8378770664f - log1pf(-expf(-2.f * k)); }
 
-// Mixture parameters of one point from its 40 head outputs: pi (softmax), mu (unit), kappa.
+// Mixture parameters of one point from its 40 head outputs: pi (softmax), mu (unit), kappa,
+// and with `lognorm` also log(pi_j * C(kappa_j)) in out[40..47] for the density.
 // Returns false (and marks pi[0] = -1) when the outputs are not finite.
-__device__ inline bool guide_mixture(const float *h, float *out) {
+__device__ inline bool guide_mixture(const float *h, float *out, bool lognorm = false) {
     float mx = h[0];
 #pragma unroll
     for (int j = 1; j < 8; ++j) mx = fmaxf(mx, h[j]);
@@ -339,20 +321,22 @@ __device__ inline bool guide_mixture(const float *h, float *out) {
         out[8 + 3 * j] = x * il;
         out[9 + 3 * j] = y * il;
         out[10 + 3 * j] = z * il;
-        out[32 + j] = guide_kappa(h[32 + j]);
+        const float lk = guide_log_kappa(h[32 + j]);
+        out[32 + j] = expf(lk);
+        if (lognorm) out[40 + j] = (h[j] - mx) - logf(sum) + vmf_log_norm2(out[32 + j], lk);
         ok = ok && isfinite(len) && len > 1e-6f && isfinite(h[32 + j]);
     }
     if (!ok) out[0] = -1.f;
     return ok;
 }
 
+// density of a mixture laid out by guide_mixture(.., lognorm = true)
 __device__ inline float guide_mixture_pdf(const float *__restrict__ m, v3 w) {
     float q = 0.f;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        const float k = m[32 + j];
         const float c = m[8 + 3 * j] * w.x + m[9 + 3 * j] * w.y + m[10 + 3 * j] * w.z;
-        q += m[j] * expf(vmf_log_norm(k) + k * (c - 1.f));
+        q += expf(m[40 + j] + m[32 + j] * (c - 1.f));
     }
     return q;
 }

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -45,6 +46,7 @@ struct Context {
     const void *graph_base = nullptr;
     size_t graph_cap = 0;
     int graph_depth = -1, graph_nl_mode = -1, graph_count = -1;
+    std::atomic<int> children{0};       // live scenes, guides and servers made from this context
     int *d_error = nullptr;             // traversal error counter
     unsigned long long *d_counters = nullptr;  // 8 x u64 statistics
 };
@@ -70,6 +72,7 @@ struct LightDev {
 
 struct Scene {
     Context *ctx = nullptr;
+    bool counted = false;  // included in ctx->children
     uint32_t n_tri = 0;
     uint32_t n_nodes = 0;
     uint32_t n_leaves = 0;

@@ -684,18 +684,18 @@ __device__ inline void guide_record(const RenderArgs &A, uint32_t slot, const Hi
 
 // Guide inference for the paths that hit a Lambert surface this bounce: 16 points per warp
 // on the tensor cores, mixture parameters to A.g.mix. Dynamic shared memory: the weights
-// plus 16 feature rows and 16 head rows per warp (guide_infer_smem_bytes).
-constexpr int kInferWarps = 4;
-inline size_t guide_infer_smem_bytes() {
-    return (size_t)kSmWHalves * 2 + (size_t)kInferWarps * (16 * kLdIn * 2 + 16 * kHeadLd * 4);
-}
+// plus, per warp, 16 feature rows that the 16 head rows overwrite once the first layer has
+// read them (16 x 88 halves = 16 x 44 floats; guide_infer_smem_bytes).
+constexpr int kInferWarps = 8;
+static_assert(kLdIn * 2 == kHeadLd * 4, "head rows alias the feature rows");
+inline size_t guide_infer_smem_bytes() { return (size_t)kSmWHalves * 2 + (size_t)kInferWarps * 16 * kLdIn * 2; }
 template <int NL>
-__global__ void __launch_bounds__(128) k_guide_infer(RenderArgs A) {
+__global__ void __launch_bounds__(32 * kInferWarps, 3) k_guide_infer(RenderArgs A) {
     extern __shared__ __align__(16) unsigned char gsm[];
     __half *sw = reinterpret_cast<__half *>(gsm);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     __half *X = reinterpret_cast<__half *>(gsm + kSmWHalves * 2) + warp * 16 * kLdIn;
-    float *head = reinterpret_cast<float *>(gsm + kSmWHalves * 2 + kInferWarps * 16 * kLdIn * 2) + warp * 16 * kHeadLd;
+    float *head = reinterpret_cast<float *>(X);
     const int cls = 1 + FL_MAT_LAMBERT;
     const uint32_t n = load_count(&A.cnt->n_class[cls]);
     if ((uint32_t)blockIdx.x * kInferWarps * 16 >= n) return;
@@ -723,13 +723,7 @@ __global__ void __launch_bounds__(128) k_guide_infer(RenderArgs A) {
         __syncwarp();
         guide_forward_warp(sw, X, nullptr, 0, head);
         __syncwarp();
-        if (valid && lane < 16) {
-            float m[kGuideOut];
-            guide_mixture(head + lane * kHeadLd, m);
-            float4 *dst = reinterpret_cast<float4 *>(A.g.mix + (size_t)slot * kGuideOut);
-#pragma unroll
-            for (int k = 0; k < kGuideOut / 4; ++k) dst[k] = make_float4(m[4 * k], m[4 * k + 1], m[4 * k + 2], m[4 * k + 3]);
-        }
+        if (valid && lane < 16) guide_mixture(head + lane * kHeadLd, A.g.mix + (size_t)slot * kMixFloats, true);
         __syncwarp();
     }
 }
@@ -798,7 +792,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             float c_sel = 0.f, u_sel = 1.f;
             if constexpr (GUIDE) {
                 if (b.type == FL_MAT_LAMBERT && A.g.select > 0.f) {
-                    gm = A.g.mix + (size_t)slot * kGuideOut;
+                    gm = A.g.mix + (size_t)slot * kMixFloats;
                     if (gm[0] >= 0.f) {
                         c_sel = A.g.select;
                         u_sel = rng.nextf();
@@ -1005,7 +999,7 @@ void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile
         prof->mark(3, st);
         if constexpr (GUIDE) {
             if (A.g.select > 0.f) {
-                k_guide_infer<NL><<<sms * 2, 128, guide_infer_smem_bytes(), st>>>(A);
+                k_guide_infer<NL><<<sms * 3, 32 * kInferWarps, guide_infer_smem_bytes(), st>>>(A);
                 prof->launches += 1;
             }
         }

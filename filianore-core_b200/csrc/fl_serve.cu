@@ -315,6 +315,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     }
     cudaStreamSynchronize(S->stream);
     Server *raw = S.release();
+    ctx->children++;
     raw->worker = std::thread(worker_loop, raw);
     *out = reinterpret_cast<fl_server *>(raw);
     return FL_OK;
@@ -341,6 +342,7 @@ fl_status fl_server_destroy(fl_server *srv) {
     if (S->graph) cudaGraphExecDestroy(S->graph);
     cudaFree(S->wave_mem);
     cudaStreamDestroy(S->stream);
+    S->ctx->children--;
     delete S;
     return FL_OK;
 }

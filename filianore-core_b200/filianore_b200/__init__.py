@@ -6,8 +6,10 @@ raises if the shared library is missing or fails to load.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -25,7 +27,7 @@ EXPORTED = [
     "fl_trace_count", "fl_render", "fl_render_noalloc", "fl_server_create", "fl_server_destroy",
     "fl_server_add_scene", "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_get_stats",
     "fl_guide_create", "fl_guide_destroy", "fl_guide_render", "fl_guide_render_timed", "fl_guide_get_weights",
-    "fl_guide_set_weights", "fl_guide_get_info", "fl_guide_gradient", "fl_guide_eval",
+    "fl_guide_set_weights", "fl_guide_get_info", "fl_guide_gradient", "fl_guide_eval", "fl_guide_get_records",
 ]
 
 _lib = None
@@ -84,6 +86,7 @@ def lib():
         L.fl_guide_gradient.argtypes = [vp, P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float),
                                         P(C.c_float)]
         L.fl_guide_eval.argtypes = [vp, P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float)]
+        L.fl_guide_get_records.argtypes = [vp, P(C.c_float), C.c_uint32, P(C.c_uint32)]
         for name in EXPORTED:
             if name not in ("fl_status_string",):
                 getattr(L, name).restype = C.c_int32
@@ -120,6 +123,21 @@ def _tables_struct(t: dict):
     return s, (keep, refl, illum)
 
 
+# Handles still open at interpreter exit are closed children first (guides and servers,
+# then scenes, then contexts) while the CUDA runtime is still up.
+_open = (weakref.WeakSet(), weakref.WeakSet(), weakref.WeakSet())
+
+
+@atexit.register
+def _close_all():
+    for group in _open:
+        for obj in list(group):
+            try:
+                obj.close()
+            except Exception:
+                pass
+
+
 def _ptr(x):
     """device pointer of a torch tensor, or host pointer of a numpy array"""
     if hasattr(x, "data_ptr"):
@@ -138,9 +156,14 @@ class Context:
         h = C.c_void_p()
         check(lib().fl_context_create(device, C.byref(s), C.byref(h)))
         self.h = h
+        self.children = weakref.WeakSet()  # scenes, guides and servers made from this context
+        _open[2].add(self)
 
     def close(self):
+        """closes the context's scenes, guides and servers first, then the context"""
         if self.h:
+            for c in list(self.children):
+                c.close()
             lib().fl_context_destroy(self.h)
             self.h = None
 
@@ -168,6 +191,8 @@ class SceneHandle:
         h = C.c_void_p()
         check(lib().fl_scene_create(ctx.h, C.byref(desc), C.byref(h)), ctx.h)
         self.h = h
+        _open[1].add(self)
+        ctx.children.add(self)
 
     def close(self):
         if self.h:
@@ -246,13 +271,16 @@ class Guide:
     vertices, trained online on the renderer's own samples."""
 
     def __init__(self, ctx: Context, seed: int = 1, learning_rate: float = 1e-2, select_prob: float = 0.5,
-                 batch: int = 16384, max_records: int = 1 << 20, steps_per_wave: int = 16):
+                 batch: int = 16384, max_records: int = 1 << 20, steps_per_wave: int = 16,
+                 position_scale: float = 1.0 / 16):
         self.ctx = ctx
         self.h = None
-        cfg = T.fl_guide_config(seed, learning_rate, select_prob, batch, max_records, steps_per_wave)
+        cfg = T.fl_guide_config(seed, learning_rate, select_prob, batch, max_records, steps_per_wave, position_scale)
         h = C.c_void_p()
         check(lib().fl_guide_create(ctx.h, C.byref(cfg), C.byref(h)), ctx.h)
         self.h = h
+        _open[0].add(self)
+        ctx.children.add(self)
 
     def close(self):
         if self.h:
@@ -313,6 +341,14 @@ class Guide:
                                       g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)), self.ctx.h)
         return g, loss.value
 
+    def records(self, max_n: int = 1 << 20):
+        """training records of the last trained wave, (n, 20)"""
+        out = np.zeros((max_n, T.FL_GUIDE_RECORD_FLOATS), np.float32)
+        n = C.c_uint32()
+        check(lib().fl_guide_get_records(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), max_n, C.byref(n)),
+              self.ctx.h)
+        return out[:n.value]
+
     def eval(self, records, bmin, bmax):
         r = np.ascontiguousarray(records, np.float32)
         out = np.zeros((r.shape[0], 40), np.float32)
@@ -336,6 +372,8 @@ class Server:
         h = C.c_void_p()
         check(lib().fl_server_create(ctx.h, C.byref(cfg), C.byref(h)), ctx.h)
         self.h = h
+        _open[0].add(self)
+        ctx.children.add(self)
         self.shapes = {}
 
     def close(self):

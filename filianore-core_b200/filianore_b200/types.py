@@ -180,7 +180,8 @@ class fl_guide_config(C.Structure):
         ("batch", C.c_int32),
         ("max_records", C.c_int32),
         ("steps_per_wave", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("position_scale", C.c_float),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

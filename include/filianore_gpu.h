@@ -90,6 +90,8 @@ typedef struct {
 /* Replaces the global InitializeSpectrals() call (spectruminits.cpp:6) plus embree's
  * rtcNewDevice (bvh.h:25-28): binds a CUDA device, uploads the spectral tables. */
 FL_API fl_status fl_context_create(int32_t device, const fl_spectral_tables *tables, fl_context **out);
+/* Destroy every scene, guide and server made from the context first: while any is alive
+ * the call returns FL_ERR_INVALID and the context stays valid. */
 FL_API fl_status fl_context_destroy(fl_context *ctx);
 FL_API const char *fl_status_string(fl_status status);
 /* Copies the last error message of this context (or of the process when ctx is NULL). */
@@ -345,7 +347,9 @@ typedef struct {
     int32_t batch;           /* records per Adam step, a multiple of 128 in [128, 65536] */
     int32_t max_records;     /* records kept per wave, >= batch */
     int32_t steps_per_wave;  /* most Adam steps after one wave, >= 1 */
-    int32_t reserved[3];
+    float position_scale;    /* positions enter the encoding as scale * (p - bmin) / (bmax - bmin), in (0, 1];
+                                0 means 1. Smaller values shift the 12 bands to coarser frequencies */
+    int32_t reserved[2];
 } fl_guide_config;
 
 enum {
@@ -381,6 +385,11 @@ FL_API fl_status fl_guide_get_info(fl_guide *guide, int64_t *adam_steps, float *
  * unchanged. n <= max_records. */
 FL_API fl_status fl_guide_gradient(fl_guide *guide, const float *records, uint32_t n, const float bmin[3],
                                    const float bmax[3], float *grad, float *loss);
+/* The training records of the last trained wave (at most max_n; *n receives the count),
+ * FL_GUIDE_RECORD_FLOATS floats each: position 3, normal 3, wavelength, direction 3,
+ * density, incident radiance estimate, path throughput after the vertex [4], radiance
+ * gathered before it [4]. */
+FL_API fl_status fl_guide_get_records(fl_guide *guide, float *records, uint32_t max_n, uint32_t *n);
 /* Mixture parameters (40 floats per record: pi[8], mu[8][3], kappa[8]) for the points of n
  * host records in the bounds [bmin, bmax]. */
 FL_API fl_status fl_guide_eval(fl_guide *guide, const float *records, uint32_t n, const float bmin[3],

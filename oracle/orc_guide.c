@@ -23,6 +23,7 @@
 #define G_WCLAMP 4096.0
 #define G_LKMIN -2.0
 #define G_LKMAX 7.0
+#define G_LKSHIFT 2.0
 
 static int g_exact = 0; /* 1: no FP16 rounding (finite-difference checks of the gradient) */
 void orc_guide_set_exact(int on) { g_exact = on; }
@@ -77,11 +78,9 @@ static void forward(const float *w, const float x[G_IN], float acts[4][G_H], dou
     }
 }
 
-static double kappa_of(double s) {
-    if (s < G_LKMIN) s = G_LKMIN;
-    if (s > G_LKMAX) s = G_LKMAX;
-    return exp(s);
-}
+/* log kappa = min + (max - min) * sigmoid(s - shift) */
+static double sigm(double s) { return 1.0 / (1.0 + exp(-(s - G_LKSHIFT))); }
+static double kappa_of(double s) { return exp(G_LKMIN + (G_LKMAX - G_LKMIN) * sigm(s)); }
 static double vmf_log_norm(double k) { return log(k) - log(2.0 * M_PI) - log(-expm1(-2.0 * k)); }
 
 /* d(-log q(d))/d(head); returns -log q(d) */
@@ -116,8 +115,8 @@ static double head_grad(const double h[G_OUT], const double d[3], double dh[G_OU
             mg += mu[j][a] * g[a];
         }
         for (int a = 0; a < 3; ++a) dh[8 + 3 * j + a] = (g[a] - mu[j][a] * mg) / len[j];
-        const double sj = h[32 + j], k = kap[j];
-        dh[32 + j] = (sj > G_LKMIN && sj < G_LKMAX) ? -r * (1.0 - 2.0 * k / expm1(2.0 * k) + k * (dp[j] - 1.0)) : 0.0;
+        const double sg = sigm(h[32 + j]), k = kap[j];
+        dh[32 + j] = -r * (1.0 - 2.0 * k / expm1(2.0 * k) + k * (dp[j] - 1.0)) * (G_LKMAX - G_LKMIN) * sg * (1.0 - sg);
     }
     return -lse;
 }

@@ -87,30 +87,35 @@ def test_untrained_guide_is_unbiased(ctx):
     s.close()
 
 
-def mse(a, b):
-    return float(np.mean((a - b) ** 2))
-
-
 def test_trained_guide_lowers_caustic_error(ctx):
-    """Caustic scene (glass sphere under a tiny, bright sphere light), 128 x 128: after online
-    training the guided render's error against a 4096-spp plain render is lower than the
-    plain render's at the same number of samples."""
-    sc = scenes.caustic(128, 128, slices=64, stacks=33)
+    """Caustic scene (glass sphere under a tiny, bright sphere light), 256 x 256: after online
+    training, the guided render's mean squared error against a 4096-spp plain render is
+    below 0.8 x the plain render's at the same 64 samples per pixel. Both errors are
+    averaged over six independent renders: single renders are dominated by a few caustic
+    fireflies."""
+    R = 256
+    sc = scenes.caustic(R, R, slices=128, stacks=65)
     s = ctx.scene(sc)
-    H = W = 128
-    ref = np.zeros((H, W, 3), np.float64)
+    ref = np.zeros((R, R, 3), np.float64)
     s.render(scenes.render_params(4096, 8, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20), film_xyz64=ref)
     ref /= 4096
-    plain = np.zeros((H, W, 3), np.float64)
-    s.render(scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4), film_xyz64=plain)
-    g = fb.Guide(ctx, seed=5, select_prob=0.5, batch=16384, max_records=1 << 18, steps_per_wave=8)
-    for k in range(24):
+
+    def mean_mse(render):
+        errs = []
+        for k in range(6):
+            img = np.zeros((R, R, 3), np.float64)
+            render(img, 7000 + 64 * k)
+            errs.append(np.mean((img / 64 - ref) ** 2))
+        return float(np.mean(errs))
+    e_plain = mean_mse(lambda f, off: s.render(scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4, sample_offset=off),
+                                               film_xyz64=f))
+    g = fb.Guide(ctx, seed=5, select_prob=0.5, batch=16384, max_records=1 << 19, steps_per_wave=32)
+    for k in range(48):
         flags = fb.FL_GUIDE_TRAIN | (fb.FL_GUIDE_SAMPLE if k > 0 else 0)
-        g.render(s, scenes.render_params(16, 8, fb.FL_SPECTRAL_HERO4, sample_offset=(1 << 16) + 16 * k), flags)
+        g.render(s, scenes.render_params(4, 8, fb.FL_SPECTRAL_HERO4, sample_offset=(1 << 16) + 4 * k), flags)
     assert g.info()["adam_steps"] > 0
-    guided = np.zeros((H, W, 3), np.float64)
-    g.render(s, scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4), fb.FL_GUIDE_SAMPLE, film_xyz64=guided)
-    e_plain, e_guided = mse(plain / 64, ref), mse(guided / 64, ref)
-    assert e_guided < 0.7 * e_plain, (e_guided, e_plain)
+    e_guided = mean_mse(lambda f, off: g.render(s, scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4, sample_offset=off),
+                                                fb.FL_GUIDE_SAMPLE, film_xyz64=f))
+    assert e_guided < 0.8 * e_plain, (e_guided, e_plain)
     g.close()
     s.close()
