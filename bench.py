@@ -335,11 +335,14 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
         run.update(errors(img, spp))
         if frac == 1.0:
             # the trained guide at the plain render's sample count (sampling only)
+            import torch
             img2 = np.zeros((R, R, 3), np.float64)
+            torch.cuda.nvtx.range_push("timed")
             t0 = time.perf_counter()
             g.render(s, scenes.render_params(n_plain, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 21),
                      fb.FL_GUIDE_SAMPLE, film_xyz64=img2)
             eq = {"wall_ms": round((time.perf_counter() - t0) * 1e3, 1)}
+            torch.cuda.nvtx.range_pop()
             eq.update(errors(img2, n_plain))
             run["trained_equal_spp"] = eq
         runs.append(run)

@@ -612,7 +612,9 @@ struct NeeRayItem {
         tris = J->tris;
         n_tris = J->n_tri;
         ray = ray_precompute(A->sray_o[q], A->sray_d[q]);
-        any_hit = kind == 0 && J->any_hit_ok;
+        // shadow rays stop at the first hit when no triangle emits; a MIS ray towards the
+        // environment only asks whether it escapes, so any triangle hit ends it as well
+        any_hit = kind == 0 ? J->any_hit_ok != 0 : J->lights[sl / A->cap].type == FL_LIGHT_ENV;
         trav_init(st, ray);
         return true;
     }
