@@ -1,0 +1,321 @@
+// filianore_gpu.hpp: C++ host adapter over the C ABI of filianore_gpu.h.
+//
+// It mirrors the reference's classes on this path, so that code written against
+// filianore-core reads the same against the GPU backend:
+//   SceneGeometry / TriangleMesh / BasicTriangle   src/filianore/bvh/bvh.h:11-21
+//   BVH (initialize, initialize_scene_geometry,     src/filianore/bvh/bvh.h:23-45,
+//        add_triangle_mesh, finalise, intersect,    src/filianore/bvh/bvh.cpp:7-88
+//        intersect_p, clean_up)
+//   Scene (geometry + illuminants, owns its BVH)   src/filianore/core/scene.h:12-27
+//   RenderParams                                    src/filianore/core/renderparams.h:5-10
+//   PathIntegrator(RenderParams, rrThreshold)       src/filianore/integrators/pathintegrator.h:9-22
+//   PhysicalCamera (position, look-at, up, fov)     src/filianore/cameras/physical.h:11-43
+// The types are this library's own (plain structs), not the reference's: a maintainer
+// converts at the boundary, as shown in the integration notes.
+//
+// Conventions kept from the reference: intersect / intersect_p return bool (hit or not)
+// and shrink ray.tMax on a hit; nothing throws. A failure of the library (no device, out of
+// memory) makes the call report a miss or false and leaves the message in last_error().
+// The GPU's granularity differs in one place: PathIntegrator renders whole images
+// (render), the replacement of the application's loop over Integrator::Li, instead of one
+// camera ray at a time.
+#ifndef FILIANORE_GPU_HPP
+#define FILIANORE_GPU_HPP
+
+#include <cmath>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "filianore_gpu.h"
+
+namespace filianore_gpu {
+
+struct Vector3f {
+    float x = 0.f, y = 0.f, z = 0.f;
+};
+
+struct BasicTriangle {
+    Vector3f v1, v2, v3;
+};
+
+// One mesh of the soup. `material` indexes Scene's materials (the reference attaches a
+// Material per GeometricPrimitive instead).
+struct TriangleMesh {
+    std::vector<std::shared_ptr<BasicTriangle>> triangles;
+    uint32_t material = 0;
+};
+
+struct SceneGeometry {
+    std::vector<std::shared_ptr<TriangleMesh>> triangleMeshes;
+};
+
+struct Ray {
+    Vector3f origin, dir;
+    float tMin = 0.f;
+    mutable float tMax = std::numeric_limits<float>::infinity();  // shrunk by intersect, as in the reference
+};
+
+// The part of the reference's SurfaceInteraction the hit provides: distance, point, the
+// geometric normal normalize(cross(v2 - v1, v3 - v1)), the primitive (soup index) and
+// embree's barycentrics.
+struct SurfaceInteraction {
+    float t = 0.f;
+    Vector3f p, n;
+    int primitive = -1;
+    float u = 0.f, v = 0.f;
+};
+
+struct RenderParams {
+    int samples = 1;
+    int diffuseRayDepth = 8;
+    int reflectionRayDepth = 8;
+    int transmissionRayDepth = 8;
+};
+
+struct PhysicalCamera {
+    Vector3f position, lookAt, up{0.f, 1.f, 0.f};
+    float fov = 40.f;  // vertical, degrees
+    int xRes = 256, yRes = 256;
+};
+
+// An illuminant: a triangle of the soup (DiffuseAreaIlluminant), an analytic sphere or a
+// constant environment (both new in this backend).
+struct Illuminant {
+    int type = FL_LIGHT_TRIANGLE;
+    uint32_t triangle = 0;
+    float radiance = 0.f;
+    Vector3f center;
+    float radius = 0.f;
+};
+
+inline fl_material LambertMaterial(float r, float g, float b) {
+    fl_material m{};
+    m.type = FL_MAT_LAMBERT;
+    m.rgb[0] = r;
+    m.rgb[1] = g;
+    m.rgb[2] = b;
+    return m;
+}
+
+inline std::string status_text(const fl_context *ctx, fl_status st) {
+    char buf[512] = {0};
+    fl_last_error(ctx, buf, sizeof(buf));
+    return std::string(fl_status_string(st)) + (buf[0] ? std::string(": ") + buf : std::string());
+}
+
+// The device and the spectral tables (the reference's InitializeSpectrals()).
+class Context {
+public:
+    Context(int device, const fl_spectral_tables &tables) {
+        st_ = fl_context_create(device, &tables, &ctx_);
+        if (st_ != FL_OK) error_ = status_text(nullptr, st_);
+    }
+    ~Context() {
+        if (ctx_) fl_context_destroy(ctx_);
+    }
+    Context(const Context &) = delete;
+    Context &operator=(const Context &) = delete;
+    bool ok() const { return ctx_ != nullptr; }
+    fl_context *get() const { return ctx_; }
+    const std::string &last_error() const { return error_; }
+
+private:
+    fl_context *ctx_ = nullptr;
+    fl_status st_ = FL_OK;
+    std::string error_;
+};
+
+// The acceleration structure (the reference's BVH over embree).
+class BVH {
+public:
+    BVH() = default;
+    ~BVH() { clean_up(); }
+    BVH(const BVH &) = delete;
+    BVH &operator=(const BVH &) = delete;
+
+    void initialize(Context &ctx) { ctx_ = &ctx; }
+    void clean_up() {
+        if (scene_) fl_scene_destroy(scene_);
+        scene_ = nullptr;
+    }
+
+    // Triangle ids are insertion order across meshes, as embree's geomIDs.
+    void initialize_scene_geometry(const SceneGeometry &geometry) {
+        for (const auto &mesh : geometry.triangleMeshes)
+            for (const auto &tri : mesh->triangles) add_triangle_mesh(tri, mesh->material);
+    }
+    void add_triangle_mesh(const std::shared_ptr<BasicTriangle> &tri, uint32_t material = 0) {
+        const BasicTriangle &t = *tri;
+        const float v[9] = {t.v1.x, t.v1.y, t.v1.z, t.v2.x, t.v2.y, t.v2.z, t.v3.x, t.v3.y, t.v3.z};
+        soup_.insert(soup_.end(), v, v + 9);
+        tri_material_.push_back(material);
+    }
+    // Builds the device BVH (embree's rtcCommitScene). Returns false on failure.
+    bool finalise(const std::vector<fl_material> &materials, const std::vector<fl_light> &lights) {
+        clean_up();
+        if (!ctx_ || !ctx_->ok()) {
+            error_ = "BVH::finalise without a valid context";
+            return false;
+        }
+        fl_scene_desc d{};
+        d.verts = soup_.data();
+        d.n_tri = (uint32_t)(soup_.size() / 9);
+        d.tri_material = tri_material_.data();
+        d.materials = materials.data();
+        d.n_materials = (uint32_t)materials.size();
+        d.lights = lights.data();
+        d.n_lights = (uint32_t)lights.size();
+        const fl_status st = fl_scene_create(ctx_->get(), &d, &scene_);
+        if (st != FL_OK) {
+            error_ = status_text(ctx_->get(), st);
+            scene_ = nullptr;
+            return false;
+        }
+        return true;
+    }
+
+    // One ray (the reference's per-ray call); renderers that batch use trace().
+    bool intersect(const Ray &ray, SurfaceInteraction *isect) const {
+        SurfaceInteraction h;
+        if (!trace(&ray, 1, &h) || h.primitive < 0) return false;
+        if (isect) *isect = h;
+        ray.tMax = h.t;
+        return true;
+    }
+    bool intersect_p(const Ray &ray) const {
+        if (!scene_) return false;
+        const float o[4] = {ray.origin.x, ray.origin.y, ray.origin.z, ray.tMin};
+        const float d[4] = {ray.dir.x, ray.dir.y, ray.dir.z, ray.tMax};
+        uint8_t occ = 0;
+        if (fl_trace_occluded(scene_, o, d, 1, &occ, FL_MEM_HOST, nullptr) != FL_OK) return false;
+        return occ != 0;
+    }
+    // Closest hits of n rays in one call; returns false when the library fails.
+    bool trace(const Ray *rays, uint32_t n, SurfaceInteraction *out) const {
+        if (!scene_) return false;
+        std::vector<float> o(4 * (size_t)n), d(4 * (size_t)n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const Ray &r = rays[i];
+            o[4 * i] = r.origin.x, o[4 * i + 1] = r.origin.y, o[4 * i + 2] = r.origin.z, o[4 * i + 3] = r.tMin;
+            d[4 * i] = r.dir.x, d[4 * i + 1] = r.dir.y, d[4 * i + 2] = r.dir.z, d[4 * i + 3] = r.tMax;
+        }
+        std::vector<fl_hit> hits(n);
+        if (fl_trace_closest(scene_, o.data(), d.data(), n, hits.data(), FL_MEM_HOST, nullptr) != FL_OK) return false;
+        for (uint32_t i = 0; i < n; ++i) {
+            SurfaceInteraction &s = out[i];
+            s = SurfaceInteraction{};
+            s.primitive = hits[i].id;
+            if (hits[i].id < 0) continue;
+            const Ray &r = rays[i];
+            s.t = hits[i].t;
+            s.u = hits[i].u;
+            s.v = hits[i].v;
+            s.p = Vector3f{r.origin.x + r.dir.x * s.t, r.origin.y + r.dir.y * s.t, r.origin.z + r.dir.z * s.t};
+            const float *v = &soup_[9 * (size_t)hits[i].id];
+            const float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+            const float e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+            Vector3f n{e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            const float len = std::sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
+            if (len > 0.f) n = Vector3f{n.x / len, n.y / len, n.z / len};
+            s.n = n;
+        }
+        return true;
+    }
+
+    fl_scene *get() const { return scene_; }
+    size_t triangle_count() const { return soup_.size() / 9; }
+    const std::string &last_error() const { return error_; }
+
+private:
+    Context *ctx_ = nullptr;
+    fl_scene *scene_ = nullptr;
+    std::vector<float> soup_;
+    std::vector<uint32_t> tri_material_;
+    std::string error_;
+};
+
+// Geometry plus illuminants, owning its BVH (the reference's Scene).
+class Scene {
+public:
+    Scene(Context &ctx, const SceneGeometry &geometry, const std::vector<fl_material> &materials,
+          const std::vector<Illuminant> &illuminants)
+        : illuminants(illuminants) {
+        bvh.initialize(ctx);
+        bvh.initialize_scene_geometry(geometry);
+        std::vector<fl_light> lights;
+        for (const Illuminant &il : illuminants) {
+            fl_light l{};
+            l.type = il.type;
+            l.tri = il.triangle;
+            l.radiance = il.radiance;
+            l.radius = il.radius;
+            l.center[0] = il.center.x;
+            l.center[1] = il.center.y;
+            l.center[2] = il.center.z;
+            lights.push_back(l);
+        }
+        ok_ = bvh.finalise(materials, lights);
+    }
+    ~Scene() { bvh.clean_up(); }
+    bool ok() const { return ok_; }
+    bool intersect(const Ray &ray, SurfaceInteraction *isect) const { return bvh.intersect(ray, isect); }
+    bool intersect_p(const Ray &ray) const { return bvh.intersect_p(ray); }
+
+    BVH bvh;
+    std::vector<Illuminant> illuminants;
+
+private:
+    bool ok_ = false;
+};
+
+// The path tracer. Its depths follow RenderParams; the device path uses one maximum depth,
+// so the three depths must be equal (the reference configurations set them equal).
+class PathIntegrator {
+public:
+    explicit PathIntegrator(const RenderParams &renderParams, float rrThreshold = 1.f)
+        : renderParams(renderParams), rrThreshold(rrThreshold) {}
+
+    // Renders the camera's image: linear RGB, xRes * yRes * 3 floats, row 0 at the top.
+    // spectral_mode: FL_SPECTRAL_BINS60 (the reference's 60 bins) or FL_SPECTRAL_HERO4.
+    // Returns false (message in last_error()) when the library fails.
+    bool render(const Scene &scene, const PhysicalCamera &camera, std::vector<float> &rgb,
+                int spectral_mode = FL_SPECTRAL_BINS60, fl_render_stats *stats = nullptr) const {
+        if (renderParams.diffuseRayDepth != renderParams.reflectionRayDepth ||
+            renderParams.diffuseRayDepth != renderParams.transmissionRayDepth) {
+            error_ = "the device path traces with one depth: diffuse, reflection and transmission depths must match";
+            return false;
+        }
+        fl_camera cam{};
+        cam.position[0] = camera.position.x, cam.position[1] = camera.position.y, cam.position[2] = camera.position.z;
+        cam.look_at[0] = camera.lookAt.x, cam.look_at[1] = camera.lookAt.y, cam.look_at[2] = camera.lookAt.z;
+        cam.up[0] = camera.up.x, cam.up[1] = camera.up.y, cam.up[2] = camera.up.z;
+        cam.vfov_deg = camera.fov;
+        cam.width = camera.xRes;
+        cam.height = camera.yRes;
+        fl_render_params p{};
+        p.spp = renderParams.samples;
+        p.max_depth = renderParams.diffuseRayDepth;
+        p.rr_threshold = rrThreshold;
+        p.spectral_mode = spectral_mode;
+        rgb.assign((size_t)camera.xRes * camera.yRes * 3, 0.f);
+        const fl_status st = fl_render(scene.bvh.get(), &cam, &p, rgb.data(), nullptr, FL_MEM_HOST, stats);
+        if (st != FL_OK) {
+            error_ = std::string(fl_status_string(st));
+            return false;
+        }
+        return true;
+    }
+    const std::string &last_error() const { return error_; }
+
+    const RenderParams renderParams;
+    const float rrThreshold;
+
+private:
+    mutable std::string error_;
+};
+
+}  // namespace filianore_gpu
+
+#endif  // FILIANORE_GPU_HPP

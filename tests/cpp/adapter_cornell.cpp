@@ -1,0 +1,144 @@
+// Drives the C++ adapter (include/filianore_gpu.hpp) the way code written against the
+// reference's classes would: SceneGeometry of BasicTriangles -> Scene (owning its BVH) ->
+// BVH::intersect per ray and BVH::trace in a batch -> PathIntegrator::render. Inputs and
+// outputs are raw little-endian files written and read by tests/test_cpp_adapter.py:
+//   adapter_cornell <input> <output>
+// input:  spectral tables (n_cie, y integral, lambda/x/y/z, n_rgb, lambda, refl[7], illum[7]),
+//         soup (n_tri, 9 floats per triangle, material per triangle), materials, lights,
+//         camera, samples, depth, spectral mode, rays (n, origin/tmin and direction/tmax)
+// output: the image (width * height * 3 floats), then per ray: intersect's (hit, id, t,
+//         tMax after the call) and trace's (id, t)
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/filianore_gpu.hpp"
+
+using namespace filianore_gpu;
+
+struct Reader {
+    FILE *f;
+    template <class T> T get() {
+        T v{};
+        if (fread(&v, sizeof(T), 1, f) != 1) throw 1;
+        return v;
+    }
+    template <class T> std::vector<T> arr(size_t n) {
+        std::vector<T> v(n);
+        if (n && fread(v.data(), sizeof(T), n, f) != n) throw 1;
+        return v;
+    }
+};
+
+int main(int argc, char **argv) {
+    if (argc != 3) {
+        std::fprintf(stderr, "usage: %s <input> <output>\n", argv[0]);
+        return 2;
+    }
+    FILE *in = std::fopen(argv[1], "rb");
+    if (!in) return 2;
+    Reader r{in};
+    std::vector<float> lam, x, y, z, rl;
+    std::vector<float> refl[7], illum[7];
+    fl_spectral_tables t{};
+    std::vector<fl_material> mats;
+    std::vector<fl_light> lights_raw;
+    fl_camera cam{};
+    SceneGeometry geometry;
+    int spp = 0, depth = 0, mode = 0;
+    std::vector<Ray> rays;
+    try {
+        const int n_cie = r.get<int32_t>();
+        t.cie_y_integral = r.get<float>();
+        lam = r.arr<float>(n_cie), x = r.arr<float>(n_cie), y = r.arr<float>(n_cie), z = r.arr<float>(n_cie);
+        const int n_rgb = r.get<int32_t>();
+        rl = r.arr<float>(n_rgb);
+        for (int b = 0; b < 7; ++b) refl[b] = r.arr<float>(n_rgb);
+        for (int b = 0; b < 7; ++b) illum[b] = r.arr<float>(n_rgb);
+        t.cie_lambda = lam.data(), t.cie_x = x.data(), t.cie_y = y.data(), t.cie_z = z.data(), t.n_cie = n_cie;
+        t.rgb2spec_lambda = rl.data(), t.n_rgb2spec = n_rgb;
+        for (int b = 0; b < 7; ++b) t.refl[b] = refl[b].data(), t.illum[b] = illum[b].data();
+        const uint32_t n_tri = r.get<uint32_t>();
+        const std::vector<float> soup = r.arr<float>(9 * (size_t)n_tri);
+        const std::vector<uint32_t> tri_mat = r.arr<uint32_t>(n_tri);
+        mats = r.arr<fl_material>(r.get<uint32_t>());
+        lights_raw = r.arr<fl_light>(r.get<uint32_t>());
+        cam = r.get<fl_camera>();
+        spp = r.get<int32_t>(), depth = r.get<int32_t>(), mode = r.get<int32_t>();
+        const uint32_t n_rays = r.get<uint32_t>();
+        const std::vector<float> org = r.arr<float>(4 * (size_t)n_rays), dir = r.arr<float>(4 * (size_t)n_rays);
+        // one mesh per triangle keeps the per-triangle materials and the soup order
+        for (uint32_t i = 0; i < n_tri; ++i) {
+            auto mesh = std::make_shared<TriangleMesh>();
+            auto tri = std::make_shared<BasicTriangle>();
+            const float *v = &soup[9 * (size_t)i];
+            tri->v1 = {v[0], v[1], v[2]}, tri->v2 = {v[3], v[4], v[5]}, tri->v3 = {v[6], v[7], v[8]};
+            mesh->triangles.push_back(tri);
+            mesh->material = tri_mat[i];
+            geometry.triangleMeshes.push_back(mesh);
+        }
+        for (uint32_t i = 0; i < n_rays; ++i) {
+            Ray ray;
+            ray.origin = {org[4 * i], org[4 * i + 1], org[4 * i + 2]};
+            ray.tMin = org[4 * i + 3];
+            ray.dir = {dir[4 * i], dir[4 * i + 1], dir[4 * i + 2]};
+            ray.tMax = dir[4 * i + 3];
+            rays.push_back(ray);
+        }
+    } catch (int) {
+        std::fprintf(stderr, "short input\n");
+        return 2;
+    }
+    std::fclose(in);
+
+    Context ctx(0, t);
+    if (!ctx.ok()) {
+        std::fprintf(stderr, "context: %s\n", ctx.last_error().c_str());
+        return 1;
+    }
+    std::vector<Illuminant> illuminants;
+    for (const fl_light &l : lights_raw) {
+        Illuminant il;
+        il.type = l.type, il.triangle = l.tri, il.radiance = l.radiance, il.radius = l.radius;
+        il.center = {l.center[0], l.center[1], l.center[2]};
+        illuminants.push_back(il);
+    }
+    int rc = 0;
+    {
+        Scene scene(ctx, geometry, mats, illuminants);
+        if (!scene.ok()) {
+            std::fprintf(stderr, "scene: %s\n", scene.bvh.last_error().c_str());
+            return 1;
+        }
+        RenderParams params;
+        params.samples = spp;
+        params.diffuseRayDepth = params.reflectionRayDepth = params.transmissionRayDepth = depth;
+        PathIntegrator integrator(params);
+        PhysicalCamera camera;
+        camera.position = {cam.position[0], cam.position[1], cam.position[2]};
+        camera.lookAt = {cam.look_at[0], cam.look_at[1], cam.look_at[2]};
+        camera.up = {cam.up[0], cam.up[1], cam.up[2]};
+        camera.fov = cam.vfov_deg, camera.xRes = cam.width, camera.yRes = cam.height;
+        std::vector<float> rgb;
+        if (!integrator.render(scene, camera, rgb, mode)) {
+            std::fprintf(stderr, "render: %s\n", integrator.last_error().c_str());
+            return 1;
+        }
+        std::vector<SurfaceInteraction> batch(rays.size());
+        if (!rays.empty() && !scene.bvh.trace(rays.data(), (uint32_t)rays.size(), batch.data())) rc = 1;
+        FILE *out = std::fopen(argv[2], "wb");
+        if (!out) return 2;
+        std::fwrite(rgb.data(), sizeof(float), rgb.size(), out);
+        for (size_t i = 0; i < rays.size(); ++i) {
+            SurfaceInteraction si;
+            const int32_t hit = scene.intersect(rays[i], &si) ? 1 : 0;  // shrinks rays[i].tMax on a hit
+            const int32_t id = hit ? si.primitive : -1;
+            const float rec[4] = {(float)hit, (float)id, hit ? si.t : 0.f, rays[i].tMax};
+            std::fwrite(rec, sizeof(float), 4, out);
+            const float b[2] = {(float)batch[i].primitive, batch[i].t};
+            std::fwrite(b, sizeof(float), 2, out);
+        }
+        std::fclose(out);
+    }
+    return rc;
+}
