@@ -30,7 +30,13 @@
 
 namespace fl {
 
-constexpr int kShadeClasses = 5;  // 0: miss, 1 + material type (Lambert, conductor, rough / smooth dielectric)
+// 0: miss, 1 + material type (Lambert, conductor, rough / smooth dielectric), and with
+// guiding on, kClassLambertLate: Lambert vertices past the guided ones (no inference)
+constexpr int kShadeClasses = 6;
+constexpr int kClassLambertLate = 5;
+constexpr int kGuidedVertices = 2;  // a path's first Lambert vertices are guided (and recorded)
+// path flags: bits 0..7 bounce, bit 8 specular, bits 9..10 Lambert vertices passed (guiding)
+__device__ __forceinline__ uint32_t lambert_count(uint32_t fl) { return (fl >> 9) & 3u; }
 constexpr int kMaxJobs = 64;      // jobs that can share one wave (serving)
 constexpr int kMaxSegs = 128;     // sample ranges per wave
 
@@ -412,6 +418,8 @@ struct PathTraceItem {
         if (res.id != -1) {
             const uint32_t mi = res.id >= 0 ? J->tri_material[res.id] : 0u;
             cls = 1 + J->materials[mi].type;
+            if (cls == 1 + FL_MAT_LAMBERT && A->g.select > 0.f && lambert_count(A->flags[slot]) >= kGuidedVertices)
+                cls = kClassLambertLate;
         }
         const uint32_t pos = coalesced_append_class(A->cnt->n_class, cls);
         A->q_class[(size_t)cls * A->cap + pos] = slot;
@@ -793,7 +801,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             const float *gm = nullptr;
             float c_sel = 0.f, u_sel = 1.f;
             if constexpr (GUIDE) {
-                if (b.type == FL_MAT_LAMBERT && A.g.select > 0.f) {
+                if (b.type == FL_MAT_LAMBERT && A.g.select > 0.f && lambert_count(fl) < kGuidedVertices) {
                     gm = A.g.mix + (size_t)slot * kMixFloats;
                     if (gm[0] >= 0.f) {
                         c_sel = A.g.select;
@@ -848,7 +856,12 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                     alive = true;
                     store_spec<NL>(A.beta, A.cap, slot, beta);
                     A.eta_scale[slot] = etaScale;
-                    A.flags[slot] = (bounce + 1u) | (spec_b ? 0x100u : 0u);
+                    uint32_t nfl = (bounce + 1u) | (spec_b ? 0x100u : 0u);
+                    if constexpr (GUIDE) {
+                        const uint32_t lc = lambert_count(fl) + (b.type == FL_MAT_LAMBERT ? 1u : 0u);
+                        nfl |= (lc < 3u ? lc : 3u) << 9;
+                    }
+                    A.flags[slot] = nfl;
                     A.ray_o[slot] = make_float4(no.x, no.y, no.z, kShadowEpsilon);
                     A.ray_d[slot] = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
                 }
