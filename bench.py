@@ -269,7 +269,8 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
     results = {name: run_server(pol) for name, pol in (("shortest_first", fb.FL_SERVE_SHORTEST_FIRST),
                                                         ("first_come", fb.FL_SERVE_FIRST_COME),
                                                         ("fair_share", fb.FL_SERVE_FAIR_SHARE),
-                                                        ("shortest_first_aged", fb.FL_SERVE_SHORTEST_FIRST_AGED))}
+                                                        ("shortest_first_aged", fb.FL_SERVE_SHORTEST_FIRST_AGED),
+                                                        ("response_ratio", fb.FL_SERVE_RESPONSE_RATIO))}
     ctx.close()
     best = results["shortest_first"]
     return {"metric": "p99 time-to-image", "value": best["p99_ms"], "unit": "ms", "n_gpus": world,

@@ -271,7 +271,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     if (!ctx || !cfg || !out) return FL_ERR_INVALID;
     *out = nullptr;
     if (cfg->memory_budget_bytes == 0 || cfg->max_jobs <= 0 || cfg->max_jobs > kMaxJobs || cfg->max_depth < 0 ||
-        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64 || cfg->policy < 0 || cfg->policy > 3) {
+        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64 || cfg->policy < 0 || cfg->policy > 4) {
         set_error(ctx, "invalid server configuration");
         return FL_ERR_INVALID;
     }

@@ -14,8 +14,9 @@
 //    load favoured this over first-come-first-served packing, equal sharing and a
 //    reserved share for the oldest job, at both the median and the 99th percentile.)
 //    The other policies are first come, first served packing, equal sharing
-//    (water-filling), and shortest-remaining-first with a quarter of every wave reserved
-//    for the oldest running job. Each job gets one contiguous sample range per wave, so its
+//    (water-filling), shortest-remaining-first with a quarter of every wave reserved for
+//    the oldest running job, and highest response ratio next ((waves waited + waves
+//    needed) / waves needed). Each job gets one contiguous sample range per wave, so its
 //    per-sample random streams do not depend on how it was batched.
 //  - A job is complete when all its samples were dispatched and the wave that carried its
 //    last samples has finished.
@@ -43,7 +44,7 @@ public:
         std::vector<uint64_t> rejected;  // jobs that can never fit the budget
     };
 
-    enum Policy { kShortestFirst = 0, kFirstCome = 1, kFairShare = 2, kShortestFirstAged = 3 };
+    enum Policy { kShortestFirst = 0, kFirstCome = 1, kFairShare = 2, kShortestFirstAged = 3, kResponseRatio = 4 };
 
     ServeScheduler(uint64_t budget_bytes, int max_jobs, int policy = kShortestFirst)
         : budget_(budget_bytes), max_jobs_(max_jobs), policy_(policy) {}
@@ -56,7 +57,7 @@ public:
     }
 
     void submit(uint64_t job, uint64_t scene, uint64_t film_bytes, uint64_t total_samples) {
-        jobs_[job] = JobState{scene, film_bytes, total_samples, 0, false, false};
+        jobs_[job] = JobState{scene, film_bytes, total_samples, 0, false, false, waves_};
         pending_.push_back(job);
     }
 
@@ -139,12 +140,25 @@ public:
                 want[0].first -= g;
                 if (want[0].first == 0) want.erase(want.begin());
             }
-            // shortest remaining first, or first come first served (running_ is in arrival order)
-            if (policy_ != kFirstCome)
+            if (policy_ == kResponseRatio) {
+                // highest response ratio next: (waves waited, this one included, + waves still
+                // needed) / waves still needed, so short jobs go first and a long job's
+                // priority grows while it waits
+                auto ratio = [&](const std::pair<uint64_t, uint64_t> &w) {
+                    const double need = std::max(1.0, (double)w.first / (double)cap);
+                    return ((double)(waves_ - jobs_[w.second].submit_wave + 1) + need) / need;
+                };
+                std::stable_sort(want.begin(), want.end(),
+                                 [&](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
+                                     return ratio(a) > ratio(b);
+                                 });
+            } else if (policy_ != kFirstCome) {
+                // shortest remaining first (first come first served keeps running_'s arrival order)
                 std::stable_sort(want.begin(), want.end(),
                                  [](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
                                      return a.first < b.first;
                                  });
+            }
             for (size_t i = 0; i < want.size() && left > 0; ++i) {
                 const uint64_t g = std::min<uint64_t>(want[i].first, left);
                 JobState &js = jobs_[want[i].second];
@@ -157,6 +171,7 @@ public:
                 left -= g;
             }
         }
+        ++waves_;
         // keep admission (arrival) order inside the wave
         std::sort(segs.begin(), segs.end(), [&](const Seg &a, const Seg &b) { return order(a.job) < order(b.job); });
         return segs;
@@ -199,6 +214,7 @@ private:
     struct JobState {
         uint64_t scene, film_bytes, total, dispatched;
         bool running, done;
+        uint64_t submit_wave;  // waves planned before the job was submitted
     };
     size_t order(uint64_t j) const {
         return (size_t)(std::find(running_.begin(), running_.end(), j) - running_.begin());
@@ -209,6 +225,7 @@ private:
     int policy_;
     uint64_t used_ = 0;
     uint64_t clock_ = 0;
+    uint64_t waves_ = 0;
     std::map<uint64_t, SceneState> scenes_;
     std::map<uint64_t, JobState> jobs_;
     std::deque<uint64_t> pending_;

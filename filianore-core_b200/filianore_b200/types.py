@@ -33,6 +33,7 @@ FL_SERVE_SHORTEST_FIRST = 0
 FL_SERVE_FIRST_COME = 1
 FL_SERVE_FAIR_SHARE = 2
 FL_SERVE_SHORTEST_FIRST_AGED = 3
+FL_SERVE_RESPONSE_RATIO = 4
 
 
 class fl_spectral_tables(C.Structure):

@@ -276,7 +276,8 @@ enum {
     FL_SERVE_SHORTEST_FIRST = 0,  /* fewest remaining samples first (default) */
     FL_SERVE_FIRST_COME = 1,      /* arrival order */
     FL_SERVE_FAIR_SHARE = 2,      /* equal shares (water-filling) */
-    FL_SERVE_SHORTEST_FIRST_AGED = 3  /* shortest first, oldest job keeps a quarter of each wave */
+    FL_SERVE_SHORTEST_FIRST_AGED = 3, /* shortest first, oldest job keeps a quarter of each wave */
+    FL_SERVE_RESPONSE_RATIO = 4   /* highest (waves waited + waves needed) / waves needed first */
 };
 
 typedef struct {

@@ -52,14 +52,33 @@ int main() {
     std::printf("used %llu idle %d\n", (unsigned long long)s.used(), (int)s.idle());
 
     // wave packing policies: jobs 20..23 (arrival order) with 300, 40, 200, 10 samples
-    const char *names[] = {"shortest", "first_come", "fair", "aged"};
-    for (int pol = 0; pol < 4; ++pol) {
+    const char *names[] = {"shortest", "first_come", "fair", "aged", "ratio"};
+    for (int pol = 0; pol < 5; ++pol) {
         ServeScheduler q(1 << 20, 8, pol);
         q.add_scene(1, 100);
         const uint64_t want[] = {300, 40, 200, 10};
         for (int j = 0; j < 4; ++j) q.submit(20 + j, 1, 10, want[j]);
         q.admit();
         print_plan(names[pol], q.plan_wave(256));
+    }
+
+    // response ratio over time: job 30 (2000 samples) waits while short jobs keep arriving;
+    // its ratio grows with the waves it waits, until it is served ahead of a newcomer
+    {
+        ServeScheduler q(1 << 20, 8, ServeScheduler::kResponseRatio);
+        q.add_scene(1, 100);
+        q.submit(30, 1, 10, 2000);
+        q.admit();
+        uint64_t next = 31;
+        for (int w = 0; w < 10; ++w) {
+            q.submit(next++, 1, 10, 200);  // one short job per wave
+            q.admit();
+            auto p = q.plan_wave(256);
+            std::printf("R%d", w);
+            for (auto &sg : p) std::printf(" %llu:%u", (unsigned long long)sg.job, sg.count);
+            std::printf("\n");
+            q.finish_wave();
+        }
     }
     return 0;
 }

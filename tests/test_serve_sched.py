@@ -45,4 +45,16 @@ def test_wave_packing_policies():
     assert out[2] == "fair 20:103@0 21:40@0 22:103@0 23:10@0"
     # the oldest job keeps a quarter of the wave (64), the rest goes shortest first
     assert out[3] == "aged 20:64@0 21:40@0 22:142@0 23:10@0"
+    # response ratio on the first wave (nobody has waited yet): shortest first
+    assert out[4] == "ratio 20:6@0 21:40@0 22:200@0 23:10@0"
+
+
+def test_response_ratio_bounds_waiting():
+    """A long job (2000 samples) while one short job (200) arrives every wave of 256: each
+    short job is served in the wave it arrives, the long one gets the rest, and once the long
+    job has waited long enough it takes a whole wave ahead of the newcomer."""
+    out = run_driver()[15:]
+    assert out[:6] == [f"R{w} 30:56 {31 + w}:200" for w in range(6)]
+    assert out[6] == "R6 30:256"
+    assert out[7] == "R7 30:56 37:200"
 
