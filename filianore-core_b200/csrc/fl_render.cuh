@@ -113,6 +113,7 @@ struct JobDev {
     uint32_t sample_offset;
     uint32_t n_pix;
     double *film;  // FP64 XYZ sums, 3 per pixel
+    int corrected_ggx;  // FL_RENDER_CORRECTED_GGX
 };
 
 // A wave is a list of sample ranges: slots [slot_begin, slot_begin + count) render the
@@ -294,6 +295,7 @@ __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const Sm
     b.ax = m.ax;
     b.ay = m.ay;
     b.eta = (m.type == FL_MAT_ROUGH_DIELECTRIC || m.type == FL_MAT_SMOOTH_DIELECTRIC) ? m.eta : 1.f;
+    b.corrected = A.corrected_ggx;
     if (m.type == FL_MAT_LAMBERT) reflectance<NL>(sm, tab, m, A.mat_refl60 + 60 * (size_t)mi, lambda0, b.R);
     else b.R.set(1.f);
 }
@@ -1050,6 +1052,7 @@ inline JobDev job_of(const Scene *s, const CamDev &cam, const fl_render_params &
     j.sample_offset = p.sample_offset;
     j.n_pix = (uint32_t)((uint64_t)cam.W * (uint64_t)cam.H);
     j.film = d_film;
+    j.corrected_ggx = (p.flags & FL_RENDER_CORRECTED_GGX) ? 1 : 0;
     return j;
 }
 

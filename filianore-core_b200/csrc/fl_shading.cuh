@@ -178,6 +178,7 @@ struct Bsdf {
     float ax, ay;
     float mat_eta, mat_k;
     Spec<NL> R;
+    int corrected;  // FL_RENDER_CORRECTED_GGX: VNDF density and sampling on wo's side
 };
 
 __device__ inline v3 to_local(v3 s, v3 t, v3 n, v3 v) { return mk(dot(v, s), dot(v, t), dot(v, n)); }
@@ -215,10 +216,30 @@ template <int NL>
 __device__ inline float ggx_G(const Bsdf<NL> &b, v3 wo, v3 wi) {
     return 1 / (1 + ggx_lambda(b, wo) + ggx_lambda(b, wi));
 }
+// Density of the sampled microfacet normal. Reference mode keeps MicrofacetDistribution::pdf
+// (microfacet.cpp:14-16), D(wh) |cos theta_h|, although sample_wh draws visible normals
+// (quirk Q1). Corrected mode uses the density of the visible normals that sample_wh draws
+// (Heitz 2018): G1(wo) |wo . wh| D(wh) / |cos theta_o|.
 template <int NL>
-__device__ inline float ggx_pdf(const Bsdf<NL> &b, v3 wh) { return ggx_D(b, wh) * fabsf(wh.z); }
+__device__ inline float ggx_pdf(const Bsdf<NL> &b, v3 wo, v3 wh) {
+    if (b.corrected) {
+        if (wo.z == 0.f) return 0.f;
+        return ggx_D(b, wh) * absdot(wo, wh) / ((1.f + ggx_lambda(b, wo)) * fabsf(wo.z));
+    }
+    return ggx_D(b, wh) * fabsf(wh.z);
+}
+template <int NL>
+__device__ inline v3 ggx_sample_wh_upper(const Bsdf<NL> &b, v3 wo, float ux, float uy);
+// GGXDistribution::sample_wh (ggx.cpp:32-57): always in the upper hemisphere, even for
+// wo.z < 0 (quirk Q2). Corrected mode samples around -wo and flips the normal back to
+// wo's side.
 template <int NL>
 __device__ inline v3 ggx_sample_wh(const Bsdf<NL> &b, v3 wo, float ux, float uy) {
+    if (b.corrected && wo.z < 0.f) return neg(ggx_sample_wh_upper(b, neg(wo), ux, uy));
+    return ggx_sample_wh_upper(b, wo, ux, uy);
+}
+template <int NL>
+__device__ inline v3 ggx_sample_wh_upper(const Bsdf<NL> &b, v3 wo, float ux, float uy) {
     v3 vh = normalize(mk(wo.x * b.ax, wo.y * b.ay, wo.z));
     if (vh.z < 0) vh = neg(vh);
     const float lensq = vh.x * vh.x + vh.y * vh.y;
@@ -336,7 +357,7 @@ __device__ inline float lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi) {
     if (lobe == 1) {
         if (!same_hemi(wo, wi)) return 0.f;
         const v3 wh = normalize(add(wo, wi));
-        return ggx_pdf(b, wh) / (4.f * dot(wo, wh));
+        return ggx_pdf(b, wo, wh) / (4.f * dot(wo, wh));
     }
     if (lobe == 2) {
         if (same_hemi(wo, wi)) return 0.f;
@@ -345,7 +366,7 @@ __device__ inline float lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi) {
         if (dot(wo, wh) * dot(wi, wh) > 0) return 0.f;
         const float sqrtDenom = dot(wo, wh) + eta * dot(wi, wh);
         const float dwh_dwi = fabsf((eta * eta * dot(wi, wh)) / (sqrtDenom * sqrtDenom));
-        return ggx_pdf(b, wh) * dwh_dwi;
+        return ggx_pdf(b, wo, wh) * dwh_dwi;
     }
     return 0.f;
 }
@@ -377,7 +398,7 @@ __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, f
         if (dot(wo, wh) < 0) { f.set(0.f); return; }
         wi = sub(mul(mul(wh, 2.f), dot(wo, wh)), wo);
         if (!same_hemi(wo, wi)) { f.set(0.f); return; }
-        pdf = ggx_pdf(b, wh) / (4.f * dot(wo, wh));
+        pdf = ggx_pdf(b, wo, wh) / (4.f * dot(wo, wh));
         lobe_eval(b, 1, wo, wi, f);
         return;
     }

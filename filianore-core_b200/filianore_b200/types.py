@@ -28,6 +28,7 @@ FL_SPECTRAL_BINS60 = 1
 
 FL_RENDER_PROFILE = 1
 FL_RENDER_COUNT = 2
+FL_RENDER_CORRECTED_GGX = 4
 
 FL_SERVE_SHORTEST_FIRST = 0
 FL_SERVE_FIRST_COME = 1

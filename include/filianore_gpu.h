@@ -213,7 +213,10 @@ enum {
 
 enum {
     FL_RENDER_PROFILE = 1,  /* time each kernel class with CUDA events (fl_render_stats.ms_*) */
-    FL_RENDER_COUNT = 2     /* count BVH nodes and triangles visited (instrumented traversal) */
+    FL_RENDER_COUNT = 2,    /* count BVH nodes and triangles visited (instrumented traversal) */
+    FL_RENDER_CORRECTED_GGX = 4 /* corrected GGX: the density of the visible normals the sampler draws,
+                                   sampled on wo's side (the reference keeps D |cos| and the upper
+                                   hemisphere, microfacet.cpp:14-16, ggx.cpp:32-57) */
 };
 
 typedef struct {

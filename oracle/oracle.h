@@ -99,6 +99,9 @@ void orc_camera_ray(const orc_camera *cam, const fl_camera *c, uint32_t pixel, o
 void orc_reflectance(const orc_tables *t, const float rgb[3], int mode, const float *lambda, float *out);
 void orc_xyz_from_spectrum(const orc_tables *t, int mode, const float *lambda, const float *L, double *xyz);
 
+/* f(wo, wi) |cos theta_i| of a non-Lambert material in its local frame, n directions */
+void orc_bsdf_fcos(const fl_material *m, const float wo[3], uint32_t n, const float *wi, int corrected, float *out);
+
 /* ---------------------------------------------------------------- guiding (orc_guide.c) */
 /* 1: evaluate without the GPU's FP16 roundings (for finite-difference checks) */
 void orc_guide_set_exact(int on);

@@ -59,6 +59,7 @@ def lib():
                                          P(C.c_float)]
         L.orc_guide_gradient.restype = C.c_float
         L.orc_guide_set_exact.argtypes = [C.c_int]
+        L.orc_bsdf_fcos.argtypes = [P(T.fl_material), P(C.c_float), C.c_uint32, P(C.c_float), C.c_int, P(C.c_float)]
         _lib = L
     return _lib
 
@@ -270,4 +271,13 @@ def guide_gradient(weights, records, bmin, bmax):
     loss = lib().orc_guide_gradient(_fp(w), _fp(r), r.shape[0], _fp(np.asarray(bmin, np.float32)),
                                     _fp(np.asarray(bmax, np.float32)), _fp(g))
     return g, float(loss)
+
+
+def bsdf_fcos(material, wo, wi, corrected=False):
+    """f(wo, wi) |cos theta_i| of a non-Lambert fl_material in its local frame (normal +z)"""
+    w = np.ascontiguousarray(wi, np.float32)
+    o = np.ascontiguousarray(wo, np.float32)
+    out = np.zeros(w.shape[0], np.float32)
+    lib().orc_bsdf_fcos(C.byref(material), _fp(o), w.shape[0], _fp(w), 1 if corrected else 0, _fp(out))
+    return out
 

@@ -58,6 +58,7 @@ typedef struct {
     int has_env;
     float env_radiance;
     int emissive_tris;
+    int corrected;       /* FL_RENDER_CORRECTED_GGX */
 } scene_ctx;
 
 /* ---------------------------------------------------------------- spectra */
@@ -150,6 +151,7 @@ typedef struct {
     float ax, ay;    /* GGX alphas */
     float mat_eta, mat_k;
     int nl;
+    int corrected;   /* FL_RENDER_CORRECTED_GGX */
 } bsdf_t;
 
 static v3 to_local(const bsdf_t *b, v3 v) { return v3m(v3_dot(v, b->s), v3_dot(v, b->t), v3_dot(v, b->ns)); }
@@ -185,8 +187,23 @@ static float ggx_lambda(const bsdf_t *b, v3 w) {
     return (-1 + sqrtf(1.f + a2t2)) / 2;
 }
 static float ggx_G(const bsdf_t *b, v3 wo, v3 wi) { return 1 / (1 + ggx_lambda(b, wo) + ggx_lambda(b, wi)); }
-static float ggx_pdf(const bsdf_t *b, v3 wo, v3 wh) { (void)wo; return ggx_D(b, wh) * fabsf(wh.z); }
+/* MicrofacetDistribution::pdf (microfacet.cpp:14-16): D |cos theta_h| (quirk Q1); the
+ * corrected mode uses the visible-normal density G1(wo) |wo.wh| D(wh) / |cos theta_o| */
+static float ggx_pdf(const bsdf_t *b, v3 wo, v3 wh) {
+    if (b->corrected) {
+        if (wo.z == 0.f) return 0.f;
+        return ggx_D(b, wh) * fabsf(v3_dot(wo, wh)) / ((1.f + ggx_lambda(b, wo)) * fabsf(wo.z));
+    }
+    return ggx_D(b, wh) * fabsf(wh.z);
+}
+static v3 ggx_sample_wh_upper(const bsdf_t *b, v3 wo, float ux, float uy);
+/* GGXDistribution::sample_wh (ggx.cpp:32-57) samples the upper hemisphere even for
+ * wo.z < 0 (quirk Q2); the corrected mode samples around -wo and flips back */
 static v3 ggx_sample_wh(const bsdf_t *b, v3 wo, float ux, float uy) {
+    if (b->corrected && wo.z < 0.f) return v3_neg(ggx_sample_wh_upper(b, v3_neg(wo), ux, uy));
+    return ggx_sample_wh_upper(b, wo, ux, uy);
+}
+static v3 ggx_sample_wh_upper(const bsdf_t *b, v3 wo, float ux, float uy) {
     v3 vh = v3_norm(v3m(wo.x * b->ax, wo.y * b->ay, wo.z));
     if (vh.z < 0) vh = v3_neg(vh);
     float lensq = vh.x * vh.x + vh.y * vh.y;
@@ -494,6 +511,7 @@ static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda
     b->ax = a > 0.001f ? a : 0.001f;
     b->ay = b->ax;
     b->eta = (m->type == FL_MAT_ROUGH_DIELECTRIC || m->type == FL_MAT_SMOOTH_DIELECTRIC) ? m->eta : 1.f;
+    b->corrected = S->corrected;
     if (m->type == FL_MAT_LAMBERT) {
         if (S->mode == FL_SPECTRAL_BINS60) b->R = S->mat_refl60[mi];
         else orc_reflectance(S->tab, m->rgb, S->mode, lambda, b->R.c);
@@ -908,6 +926,7 @@ int orc_render(const fl_scene_desc *sc, const orc_tables *tab, const fl_camera *
     S.sc = sc;
     S.tab = tab;
     S.mode = P->spectral_mode;
+    S.corrected = (P->flags & FL_RENDER_CORRECTED_GGX) != 0;
     S.nl = S.mode == FL_SPECTRAL_BINS60 ? ORC_NBINS : 4;
     S.bvh = orc_bvh_build(sc->verts, sc->n_tri);
     S.tri_light = (int32_t *)malloc(sizeof(int32_t) * (sc->n_tri ? sc->n_tri : 1));
@@ -951,3 +970,31 @@ int orc_render(const fl_scene_desc *sc, const orc_tables *tab, const fl_camera *
     free(S.mat_refl60);
     return 0;
 }
+
+/* f(wo, wi) |cos theta_i| of a non-Lambert material (reflectance 1, so the same at every
+ * wavelength) in its local frame (normal +z), for n directions wi: a reference-free check of
+ * the estimators, whose expectation under constant light is this function's integral. */
+void orc_bsdf_fcos(const fl_material *m, const float wo[3], uint32_t n, const float *wi, int corrected, float *out) {
+    bsdf_t b;
+    memset(&b, 0, sizeof(b));
+    b.nl = 1;
+    b.ng = b.ns = v3m(0.f, 0.f, 1.f);
+    b.s = v3m(1.f, 0.f, 0.f);
+    b.t = v3m(0.f, 1.f, 0.f);
+    b.type = m->type;
+    b.mat_eta = m->eta;
+    b.mat_k = m->k;
+    const float a = m->roughness * m->roughness;
+    b.ax = b.ay = a > 0.001f ? a : 0.001f;
+    b.eta = (m->type == FL_MAT_ROUGH_DIELECTRIC || m->type == FL_MAT_SMOOTH_DIELECTRIC) ? m->eta : 1.f;
+    b.R.c[0] = 1.f;
+    b.corrected = corrected;
+    const v3 o = v3m(wo[0], wo[1], wo[2]);
+    for (uint32_t i = 0; i < n; ++i) {
+        const v3 d = v3m(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        spec f;
+        bsdf_eval(&b, o, d, BSDF_ALL, &f);
+        out[i] = f.c[0] * fabsf(d.z);
+    }
+}
+
