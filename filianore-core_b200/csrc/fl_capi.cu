@@ -306,7 +306,15 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
         } else if (L.type == FL_LIGHT_ENV) {
             s->has_env = 1;
             s->env_radiance = L.radiance;
-        } else if (L.type != FL_LIGHT_SPHERE) {
+        } else if (L.type == FL_LIGHT_SPOT || L.type == FL_LIGHT_DIRECTIONAL) {
+            const float dl = L.direction[0] * L.direction[0] + L.direction[1] * L.direction[1] +
+                             L.direction[2] * L.direction[2];
+            if (!(dl > 0.f) || !std::isfinite(dl) || !std::isfinite(L.cone_angle) || !std::isfinite(L.penumbra_angle)) {
+                delete s;
+                set_error(ctx, "spot and directional lights need a direction (and finite angles)");
+                return FL_ERR_INVALID;
+            }
+        } else if (L.type != FL_LIGHT_SPHERE && L.type != FL_LIGHT_POINT) {
             delete s;
             set_error(ctx, "unknown light type");
             return FL_ERR_INVALID;
@@ -328,6 +336,15 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
             ld.area = 0.5f * len(cross(sub(b, a), sub(c, a)));  // Triangle::area, triangle.cpp:130-132
         } else if (L.type == FL_LIGHT_SPHERE) {
             ld.area = 4.f * kPi * L.radius * L.radius;
+        } else if (L.type == FL_LIGHT_SPOT) {
+            // SpotIlluminant (spot.cpp:6-20): the axis as given, cosines of the angles
+            ld.dx = L.direction[0]; ld.dy = L.direction[1]; ld.dz = L.direction[2];
+            ld.cos_cone = std::cos(L.cone_angle);
+            ld.cos_penumbra = std::cos(L.penumbra_angle);
+        } else if (L.type == FL_LIGHT_DIRECTIONAL) {
+            // DirectionalIlluminant (directional.cpp:6-12): towards the light, normalised
+            const v3 w = normalize(neg(mk(L.direction[0], L.direction[1], L.direction[2])));
+            ld.dx = w.x; ld.dy = w.y; ld.dz = w.z;
         }
         lights_dev.push_back(ld);
     }

@@ -66,8 +66,10 @@ struct LightDev {
     uint32_t tri;
     float radiance;
     float radius;
-    float cx, cy, cz;
+    float cx, cy, cz;   // sphere centre, point / spot position
     float area;         // triangle or sphere area
+    float dx, dy, dz;   // spot axis (as given); directional: normalize(-travel direction), towards the light
+    float cos_cone, cos_penumbra;  // spot
 };
 
 struct Scene {

@@ -525,7 +525,8 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                             for (int c = 0; c < NL; ++c) f.c[c] *= ad;
                             scatteringPdf = bsdf_pdf<NL>(b, hr.wo, wi, bsdfFlags);
                             if (!f.black()) {
-                                const float weight = power_heuristic(illumPdf, scatteringPdf);
+                                // delta lights are not weighted (integrator.cpp:57-58)
+                                const float weight = light_is_delta(Ll) ? 1.f : power_heuristic(illumPdf, scatteringPdf);
 #pragma unroll
                                 for (int c = 0; c < NL; ++c) CL.c[c] = f.c[c] * ls.radiance * weight / illumPdf;
                                 pf |= kHasCL;
@@ -551,8 +552,8 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                                 }
                             }
                         }
-                        // BSDF sampling term
-                        {
+                        // BSDF sampling term (none for delta lights, integrator.cpp:66)
+                        if (!light_is_delta(Ll)) {
                             Spec<NL> f;
                             int sampledType = 0;
                             bsdf_sample<NL>(b, hr.wo, wi, usx, usy, scatteringPdf, bsdfFlags, sampledType, f);

@@ -653,6 +653,43 @@ static __device__ __noinline__ LightSample light_sample_li(const LightDev &L, co
         ls.radiance = L.radiance;
         return ls;
     }
+    if (L.type == FL_LIGHT_POINT || L.type == FL_LIGHT_SPOT) {
+        // PointIlluminant / SpotIlluminant::sample_li (point.cpp:12-19, spot.cpp:22-29): a delta
+        // light (pdf 1), radiance color * intensity [* Falloff(-wi)] / evaluate_decay_rate, which
+        // is always |d|^2 (illuminant.cpp:16-35 falls through its switch)
+        const v3 pos = mk(L.cx, L.cy, L.cz);
+        ls.wi = normalize(sub(pos, ref.p));
+        ls.pdf = 1.f;
+        ls.vis_kind = 1;
+        ls.target = pos;
+        const float dL = len(sub(pos, ref.p));
+        const float strength = dL * dL;
+        float li = L.radiance;
+        if (L.type == FL_LIGHT_SPOT) {
+            // SpotIlluminant::Falloff (spot.cpp:43-57)
+            const float cosTheta = dot(normalize(neg(ls.wi)), normalize(mk(L.dx, L.dy, L.dz)));
+            float fo;
+            if (cosTheta < L.cos_cone) fo = 0.f;
+            else if (cosTheta > L.cos_penumbra) fo = 1.f;
+            else {
+                const float t = clampr((cosTheta - L.cos_cone) / (L.cos_penumbra - L.cos_cone), 0.f, 1.f);
+                fo = t * t * (3.f - 2.f * t);
+            }
+            li = li * fo;
+        }
+        ls.radiance = li / strength;
+        return ls;
+    }
+    if (L.type == FL_LIGHT_DIRECTIONAL) {
+        // DirectionalIlluminant::sample_li (directional.cpp:14-21): towards the light, the
+        // visibility target 2 * worldRadius (1000) away
+        ls.wi = mk(L.dx, L.dy, L.dz);
+        ls.pdf = 1.f;
+        ls.vis_kind = 1;
+        ls.target = add(ref.p, mul(ls.wi, 2.f * 1000.f));
+        ls.radiance = L.radiance;
+        return ls;
+    }
     const float z = 1.f - 2.f * ux;
     const float rr = sqrtf(fmaxf(0.f, 1.f - z * z));
     const float phi = 2.f * kPi * uy;
@@ -661,6 +698,10 @@ static __device__ __noinline__ LightSample light_sample_li(const LightDev &L, co
     ls.vis_kind = 2;
     ls.radiance = L.radiance;
     return ls;
+}
+
+__device__ inline bool light_is_delta(const LightDev &L) {
+    return L.type == FL_LIGHT_POINT || L.type == FL_LIGHT_SPOT || L.type == FL_LIGHT_DIRECTIONAL;
 }
 
 // Illuminant::pdf_li
@@ -687,6 +728,7 @@ static __device__ __noinline__ float light_pdf_li(const LightDev &L, const float
         if (isinf(pdf)) pdf = 0.f;
         return pdf;
     }
+    if (L.type == FL_LIGHT_POINT || L.type == FL_LIGHT_SPOT || L.type == FL_LIGHT_DIRECTIONAL) return 0.f;
     return kInv4Pi;
 }
 

@@ -44,6 +44,9 @@ class Scene:
             arr[i].radiance = l["radiance"]
             arr[i].radius = l.get("radius", 0.0)
             arr[i].center[:] = list(l.get("center", (0.0, 0.0, 0.0)))
+            arr[i].direction[:] = list(l.get("direction", (0.0, -1.0, 0.0)))
+            arr[i].cone_angle = l.get("cone_angle", 0.0)
+            arr[i].penumbra_angle = l.get("penumbra_angle", 0.0)
         return arr
 
     def desc(self):
@@ -295,6 +298,24 @@ def procedural_spheres(n_spheres=64, slices=128, stacks=65, width=1920, height=1
     cam = {"position": (0.0, 0.7 * extent, -2.1 * extent), "look_at": (0.0, 0.5, 0.0), "up": (0.0, 1.0, 0.0),
            "vfov": 40.0, "width": width, "height": height}
     return Scene(verts, np.concatenate(mats), materials, lights, cam)
+
+
+def delta_lights():
+    """A point light, a spot light (30 degree cone, 20 degree full-intensity core, tilted down
+    the box) and a directional light entering through the open side of the Cornell box."""
+    return [
+        {"type": T.FL_LIGHT_POINT, "radiance": 1.5, "center": (0.5, 0.8, 0.5)},
+        {"type": T.FL_LIGHT_SPOT, "radiance": 3.0, "center": (0.3, 0.95, 0.6), "direction": (0.1, -1.0, 0.2),
+         "cone_angle": float(np.radians(30.0)), "penumbra_angle": float(np.radians(20.0))},
+        {"type": T.FL_LIGHT_DIRECTIONAL, "radiance": 2.0, "direction": (0.2, -0.3, 1.0)},
+    ]
+
+
+def cornell_delta(width=64, height=64, variant="lambert") -> Scene:
+    """The Cornell box with the point, spot and directional lights of delta_lights() added to
+    its ceiling light."""
+    sc = cornell(width, height, variant)
+    return Scene(sc.verts, sc.tri_material, sc.materials, list(sc.lights) + delta_lights(), sc.camera)
 
 
 def caustic(width=1024, height=1024, slices=256, stacks=129) -> Scene:

@@ -22,6 +22,9 @@ FL_MAT_SMOOTH_DIELECTRIC = 3
 FL_LIGHT_TRIANGLE = 0
 FL_LIGHT_SPHERE = 1
 FL_LIGHT_ENV = 2
+FL_LIGHT_POINT = 3
+FL_LIGHT_SPOT = 4
+FL_LIGHT_DIRECTIONAL = 5
 
 FL_SPECTRAL_HERO4 = 0
 FL_SPECTRAL_BINS60 = 1
@@ -70,7 +73,9 @@ class fl_light(C.Structure):
         ("radiance", C.c_float),
         ("radius", C.c_float),
         ("center", C.c_float * 3),
-        ("reserved", C.c_float),
+        ("direction", C.c_float * 3),
+        ("cone_angle", C.c_float),
+        ("penumbra_angle", C.c_float),
     ]
 
 

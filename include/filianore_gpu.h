@@ -126,16 +126,26 @@ typedef struct {
 enum {
     FL_LIGHT_TRIANGLE = 0, /* DiffuseAreaIlluminant over one scene triangle (illuminants/diffusearea.cpp) */
     FL_LIGHT_SPHERE = 1,   /* analytic sphere emitter (no reference class) */
-    FL_LIGHT_ENV = 2       /* constant environment radiance (no reference class) */
+    FL_LIGHT_ENV = 2,      /* constant environment radiance (no reference class) */
+    FL_LIGHT_POINT = 3,    /* PointIlluminant (illuminants/point.cpp) */
+    FL_LIGHT_SPOT = 4,     /* SpotIlluminant (illuminants/spot.cpp) */
+    FL_LIGHT_DIRECTIONAL = 5 /* DirectionalIlluminant (illuminants/directional.cpp) */
 };
 
+/* Point and spot lights fall off as the squared distance whatever their decay setting: the
+ * reference's Illuminant::evaluate_decay_rate (illuminant.cpp:16-35) falls through its switch
+ * to d^2. Delta lights take no part in MIS (integrator.cpp:57-61, 66). */
 typedef struct {
     int32_t type;          /* FL_LIGHT_* */
     uint32_t tri;          /* FL_LIGHT_TRIANGLE: index of the emitting triangle in the soup */
     float radiance;        /* constant spectral radiance (color * intensity in the reference) */
     float radius;          /* FL_LIGHT_SPHERE */
-    float center[3];       /* FL_LIGHT_SPHERE */
-    float reserved;
+    float center[3];       /* FL_LIGHT_SPHERE: centre; FL_LIGHT_POINT / SPOT: position */
+    float direction[3];    /* FL_LIGHT_SPOT: axis the light shines along; FL_LIGHT_DIRECTIONAL: direction
+                              the light travels (the reference's dirIllum constructor argument) */
+    float cone_angle;      /* FL_LIGHT_SPOT: outer angle from the axis, radians (after the reference's
+                              degree and half-angle options) */
+    float penumbra_angle;  /* FL_LIGHT_SPOT: angle from the axis inside which the intensity is full */
 } fl_light;
 
 typedef struct {

@@ -80,14 +80,17 @@ struct PhysicalCamera {
     int xRes = 256, yRes = 256;
 };
 
-// An illuminant: a triangle of the soup (DiffuseAreaIlluminant), an analytic sphere or a
-// constant environment (both new in this backend).
+// An illuminant: a triangle of the soup (DiffuseAreaIlluminant), a point, spot or
+// directional light (PointIlluminant, SpotIlluminant, DirectionalIlluminant), an analytic
+// sphere or a constant environment (the last two new in this backend).
 struct Illuminant {
     int type = FL_LIGHT_TRIANGLE;
     uint32_t triangle = 0;
-    float radiance = 0.f;
-    Vector3f center;
+    float radiance = 0.f;  // color * intensity
+    Vector3f center;       // sphere centre, point / spot position
     float radius = 0.f;
+    Vector3f direction{0.f, -1.f, 0.f};  // spot axis, or the direction a directional light travels
+    float cone_angle = 0.f, penumbra_angle = 0.f;  // spot, radians from the axis
 };
 
 inline fl_material LambertMaterial(float r, float g, float b) {
@@ -254,6 +257,11 @@ public:
             l.center[0] = il.center.x;
             l.center[1] = il.center.y;
             l.center[2] = il.center.z;
+            l.direction[0] = il.direction.x;
+            l.direction[1] = il.direction.y;
+            l.direction[2] = il.direction.z;
+            l.cone_angle = il.cone_angle;
+            l.penumbra_angle = il.penumbra_angle;
             lights.push_back(l);
         }
         ok_ = bvh.finalise(materials, lights);

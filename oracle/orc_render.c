@@ -553,6 +553,10 @@ typedef struct {
 } vis_t;
 
 /* Illuminant::sample_li. Returns the radiance (constant over wavelength) via *Li. */
+static int light_is_delta(const fl_light *L) {
+    return L->type == FL_LIGHT_POINT || L->type == FL_LIGHT_SPOT || L->type == FL_LIGHT_DIRECTIONAL;
+}
+
 static float light_sample_li(const scene_ctx *S, int li, const isect_t *ref, float ux, float uy, v3 *wi, float *pdf,
                              vis_t *vis) {
     const fl_light *L = &S->sc->lights[li];
@@ -604,6 +608,40 @@ static float light_sample_li(const scene_ctx *S, int li, const isect_t *ref, flo
         vis->target = ip;
         return L->radiance;
     }
+    if (L->type == FL_LIGHT_POINT || L->type == FL_LIGHT_SPOT) {
+        /* PointIlluminant / SpotIlluminant::sample_li (point.cpp:12-19, spot.cpp:22-29);
+         * evaluate_decay_rate falls through its switch to |d|^2 (illuminant.cpp:16-35) */
+        v3 pos = v3m(L->center[0], L->center[1], L->center[2]);
+        *wi = v3_norm(v3_sub(pos, ref->p));
+        *pdf = 1.f;
+        vis->kind = 1;
+        vis->target = pos;
+        float dL = v3_len(v3_sub(pos, ref->p));
+        float strength = dL * dL;
+        float li = L->radiance;
+        if (L->type == FL_LIGHT_SPOT) {
+            /* SpotIlluminant::Falloff (spot.cpp:43-57) */
+            float cosCone = cosf(L->cone_angle), cosPen = cosf(L->penumbra_angle);
+            float cosTheta = v3_dot(v3_norm(v3_neg(*wi)), v3_norm(v3m(L->direction[0], L->direction[1], L->direction[2])));
+            float fo;
+            if (cosTheta < cosCone) fo = 0.f;
+            else if (cosTheta > cosPen) fo = 1.f;
+            else {
+                float t = clampf_ref((cosTheta - cosCone) / (cosPen - cosCone), 0.f, 1.f);
+                fo = t * t * (3.f - 2.f * t);
+            }
+            li = li * fo;
+        }
+        return li / strength;
+    }
+    if (L->type == FL_LIGHT_DIRECTIONAL) {
+        /* DirectionalIlluminant (directional.cpp:6-21): towards the light, target 2 * 1000 away */
+        *wi = v3_norm(v3_neg(v3m(L->direction[0], L->direction[1], L->direction[2])));
+        *pdf = 1.f;
+        vis->kind = 1;
+        vis->target = v3_add(ref->p, v3_mul(*wi, 2.f * 1000.f));
+        return L->radiance;
+    }
     /* environment: uniform sphere directions */
     float z = 1.f - 2.f * ux;
     float rr = sqrtf(fmaxf(0.f, 1.f - z * z));
@@ -640,6 +678,7 @@ static float light_pdf_li(const scene_ctx *S, int li, const isect_t *ref, v3 wi)
         if (isinf(pdf)) pdf = 0.f;
         return pdf;
     }
+    if (light_is_delta(L)) return 0.f;
     return ORC_INV_4_PI;
 }
 
@@ -704,13 +743,14 @@ static void estimate_direct(const scene_ctx *S, const isect_t *it, const bsdf_t 
             ++cn->shadow_rays;
             if (!unoccluded(S, it, &vis, wi, &cn->rays)) Lrad = 0.f;
             if (Lrad != 0.f) {
-                float weight = power_heuristic(illumPdf, scatteringPdf);
+                /* delta lights are not weighted (integrator.cpp:57-58) */
+                float weight = light_is_delta(&S->sc->lights[li]) ? 1.f : power_heuristic(illumPdf, scatteringPdf);
                 for (int i = 0; i < nl; ++i) Ld->c[i] += f.c[i] * Lrad * weight / illumPdf;
             }
         }
     }
-    /* MIS - BSDF */
-    {
+    /* MIS - BSDF, not for delta lights (integrator.cpp:66) */
+    if (!light_is_delta(&S->sc->lights[li])) {
         spec f;
         int sampledType = 0;
         bsdf_sample(b, it->wo, &wi, usx, usy, &scatteringPdf, bsdfFlags, &sampledType, &f);

@@ -36,6 +36,9 @@
 #include "filianore/core/primitive.h"
 #include "filianore/core/scene.h"
 #include "filianore/illuminants/diffusearea.h"
+#include "filianore/illuminants/directional.h"
+#include "filianore/illuminants/point.h"
+#include "filianore/illuminants/spot.h"
 #include "filianore/integrators/pathintegrator.h"
 #include "filianore/sampling/sampler.h"
 #include "filianore/shading/bsdf.h"
@@ -265,8 +268,25 @@ int render(const char *scene_path, const char *out_path) {
     std::vector<std::shared_ptr<AreaIlluminant>> tri_light(h.n_tri);
     std::vector<std::shared_ptr<Illuminant>> illuminants;
     for (const auto &l : lights) {
+        if (l.type == FL_LIGHT_POINT || l.type == FL_LIGHT_SPOT || l.type == FL_LIGHT_DIRECTIONAL) {
+            // the reference's delta lights, colour 1 times intensity, quadratic decay
+            const Vector3f dir(l.direction[0], l.direction[1], l.direction[2]);
+            if (l.type == FL_LIGHT_POINT)
+                illuminants.push_back(std::make_shared<PointIlluminant>(
+                    translate(l.center[0], l.center[1], l.center[2]), PrincipalSpectrum(1.f), l.radiance, (short)2,
+                    PrincipalSpectrum(0.f)));
+            else if (l.type == FL_LIGHT_SPOT)
+                illuminants.push_back(std::make_shared<SpotIlluminant>(
+                    translate(l.center[0], l.center[1], l.center[2]), dir, l.cone_angle, l.penumbra_angle, true, false,
+                    PrincipalSpectrum(1.f), l.radiance, (short)2, PrincipalSpectrum(0.f)));
+            else
+                // an identity transform: a default-constructed Transform is the zero matrix
+                illuminants.push_back(std::make_shared<DirectionalIlluminant>(
+                    translate(0.f, 0.f, 0.f), dir, PrincipalSpectrum(1.f), l.radiance, PrincipalSpectrum(0.f)));
+            continue;
+        }
         if (l.type != FL_LIGHT_TRIANGLE || l.tri >= h.n_tri) {
-            fprintf(stderr, "harness supports triangle area lights only\n");
+            fprintf(stderr, "harness supports triangle area lights and the delta lights only\n");
             return 2;
         }
         auto al = std::make_shared<DiffuseAreaIlluminant>(Transform(), PrincipalSpectrum(1.f), l.radiance, (short)2,

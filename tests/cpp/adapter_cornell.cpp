@@ -101,6 +101,8 @@ int main(int argc, char **argv) {
         Illuminant il;
         il.type = l.type, il.triangle = l.tri, il.radiance = l.radiance, il.radius = l.radius;
         il.center = {l.center[0], l.center[1], l.center[2]};
+        il.direction = {l.direction[0], l.direction[1], l.direction[2]};
+        il.cone_angle = l.cone_angle, il.penumbra_angle = l.penumbra_angle;
         illuminants.push_back(il);
     }
     int rc = 0;

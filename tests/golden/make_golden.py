@@ -12,6 +12,8 @@ reference sources with oracle/Makefile). Outputs:
   cornell_materials_ref.npz  the same with GGX conductor + rough dielectric boxes
                         ("materials") and conductor + smooth glass boxes ("glass"):
                         64x64 at 4 spp (float64) and 128x128 at 16 spp (float32)
+  cornell_delta_ref.npz the Cornell box ("lambert" and "materials") with the reference's
+                        point, spot and directional lights added: 64x64 at 4 spp (float64)
 Usage: python tests/golden/make_golden.py
 """
 import os
@@ -75,6 +77,18 @@ def main():
             out[f"{variant}_{key}_xyz"] = film.astype(dt)
             print(variant, key, info)
     np.savez_compressed(os.path.join(HERE, "cornell_materials_ref.npz"), **out)
+    # the box with the reference's point, spot and directional lights added
+    out = {}
+    for variant in ("lambert", "materials"):
+        sc = scenes.cornell_delta(64, 64, variant)
+        p = scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60)
+        spath = os.path.join(tmp, f"delta_{variant}.scene")
+        fpath = os.path.join(tmp, f"delta_{variant}.film")
+        oracle.write_scene_file(spath, sc, p)
+        film, info = oracle.run_reference(spath, fpath, 64, 64)
+        out[f"{variant}_xyz"] = film.astype(np.float64)
+        print("delta", variant, info)
+    np.savez_compressed(os.path.join(HERE, "cornell_delta_ref.npz"), **out)
 
 
 if __name__ == "__main__":

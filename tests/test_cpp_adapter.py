@@ -60,7 +60,7 @@ def write_input(path, sc, params, org, dirs):
 @pytest.mark.gpu
 def test_adapter_matches_c_abi(tmp_path):
     exe = build(str(tmp_path))
-    sc = scenes.cornell(48, 48)
+    sc = scenes.cornell_delta(48, 48)   # area, point, spot and directional lights
     params = scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60)
     rng = np.random.default_rng(3)
     n = 4096

@@ -134,3 +134,19 @@ def test_invalid_render_arguments(ctx):
     with pytest.raises(fb.FlError):
         s.render(scenes.render_params(1, 4, mode=7))
     s.close()
+
+
+@pytest.mark.parametrize("variant", ["lambert", "materials"])
+def test_delta_lights_match_reference_integrator(ctx, variant):
+    """Point, spot and directional lights beside the area light, 60-bin parity build, against
+    the reference integrator's own film (fixture)."""
+    g = np.load(os.path.join(GOLDEN, "cornell_delta_ref.npz"))
+    ref = g[f"{variant}_xyz"]
+    sc = scenes.cornell_delta(64, 64, variant)
+    s = ctx.scene(sc)
+    xyz = np.zeros((64, 64, 3), np.float64)
+    _, st = s.render(scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60), film_xyz64=xyz)
+    s.close()
+    close = np.all(np.abs(xyz - ref) <= np.maximum(1e-4 * np.abs(ref), 1e-6), axis=-1).mean()
+    assert close >= 0.99, close
+    assert abs(xyz.mean() / ref.mean() - 1) < 2e-3
