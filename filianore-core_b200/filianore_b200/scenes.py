@@ -34,7 +34,29 @@ class Scene:
             arr[i].roughness = m.get("roughness", 0.0)
             arr[i].eta = m.get("eta", 1.5)
             arr[i].k = m.get("k", 0.0)
+            arr[i].standard = -1
+        # StandardSurfaceMaterial parameters: materials with "standard" get consecutive indices
+        k = 0
+        for i, m in enumerate(self.materials):
+            if "standard" in m:
+                arr[i].type = T.FL_MAT_STANDARD
+                arr[i].standard = k
+                k += 1
         return arr
+
+    def standard_array(self):
+        """fl_standard_surface records of the materials that carry a "standard" dict"""
+        stds = [m["standard"] for m in self.materials if "standard" in m]
+        arr = (T.fl_standard_surface * max(1, len(stds)))()
+        for i, p in enumerate(stds):
+            for name, _ in T.fl_standard_surface._fields_:
+                if name in p:
+                    v = p[name]
+                    if isinstance(v, (tuple, list)):
+                        getattr(arr[i], name)[:] = list(v)
+                    else:
+                        setattr(arr[i], name, v)
+        return arr, len(stds)
 
     def lights_array(self):
         arr = (T.fl_light * max(1, len(self.lights)))()
@@ -63,7 +85,10 @@ class Scene:
         d.n_materials = len(self.materials)
         d.lights = C.cast(lights, C.POINTER(T.fl_light))
         d.n_lights = len(self.lights)
-        return d, (verts, tm, mats, lights)
+        stds, n_std = self.standard_array()
+        d.standard_surfaces = C.cast(stds, C.POINTER(T.fl_standard_surface))
+        d.n_standard_surfaces = n_std
+        return d, (verts, tm, mats, lights, stds)
 
     def camera_struct(self, width=None, height=None):
         c = self.camera
@@ -120,7 +145,8 @@ def _box(cx, cz, sx, sy, sz, angle_deg):
 def cornell(width=256, height=256, variant="lambert") -> Scene:
     """Cornell-style box of 36 triangles (unit-cube room open at z = 0, two rotated boxes,
     0.25 x 0.25 ceiling light at y = 0.999 facing down with constant spectral radiance 10).
-    variant "lambert": every surface Lambertian; "materials": short box GGX conductor
+    variant "lambert": every surface Lambertian; "standard" / "standard2": the boxes are
+    StandardSurface materials (see below); "materials": short box GGX conductor
     (roughness 0.3, eta 0.2, k 3.9), tall box rough dielectric (roughness 0.25, IOR 1.5);
     "glass": short box conductor (roughness 0.05), tall box smooth glass (IOR 1.5)."""
     tris, mats = [], []
@@ -152,6 +178,23 @@ def cornell(width=256, height=256, variant="lambert") -> Scene:
     elif variant == "glass":
         materials += [{"type": T.FL_MAT_CONDUCTOR, "roughness": 0.05, "eta": 0.2, "k": 3.9},
                       {"type": T.FL_MAT_SMOOTH_DIELECTRIC, "eta": 1.5}]
+    elif variant == "standard":
+        # StandardSurface: Oren-Nayar diffuse with sheen; Fresnel-blended anisotropic GGX with a clear coat
+        materials += [{"standard": {"kd": (0.8, 0.6, 0.3), "kd_weight": 1.0, "kd_roughness": 0.5,
+                                    "sheen_color": (0.9, 0.9, 1.0), "sheen_weight": 0.8, "sheen_roughness": 0.4}},
+                      {"standard": {"kd": (0.2, 0.4, 0.8), "kd_weight": 0.9, "kd_roughness": 0.3,
+                                    "ks": (0.9, 0.9, 0.9), "ks_weight": 0.8, "ks_roughness": 0.35,
+                                    "ks_anisotropic": 0.4, "ks_ior": 1.5, "fresnel_type": T.FL_FRESNEL_DIELECTRIC,
+                                    "coat_color": (1.0, 1.0, 1.0), "coat_weight": 0.6, "coat_ior": 1.5,
+                                    "coat_gloss": 0.7}}]
+    elif variant == "standard2":
+        # StandardSurface: Schlick-metallic blended lobe; glass-like specular transmission (R = ks, T = kt)
+        materials += [{"standard": {"kd": (0.5, 0.5, 0.5), "kd_weight": 0.5, "kd_roughness": 0.2,
+                                    "ks": (0.95, 0.7, 0.3), "ks_weight": 1.0, "ks_roughness": 0.25, "ks_ior": 1.5,
+                                    "fresnel_type": T.FL_FRESNEL_METALLIC}},
+                      {"standard": {"ks": (1.0, 1.0, 1.0), "ks_weight": 1.0, "ks_ior": 1.5, "ks_roughness": 0.2,
+                                    "kt": (0.9, 0.95, 1.0), "kt_weight": 1.0, "sheen_color": (1.0, 0.8, 0.8),
+                                    "sheen_weight": 0.3, "sheen_roughness": 0.5}}]
     lights = [{"type": T.FL_LIGHT_TRIANGLE, "tri": light_first + k, "radiance": 10.0} for k in range(2)]
     cam = {"position": (0.5, 0.5, -1.4), "look_at": (0.5, 0.5, 0.0), "up": (0.0, 1.0, 0.0), "vfov": 40.0,
            "width": width, "height": height}

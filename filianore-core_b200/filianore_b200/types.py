@@ -32,6 +32,9 @@ FL_SPECTRAL_BINS60 = 1
 FL_RENDER_PROFILE = 1
 FL_RENDER_COUNT = 2
 FL_RENDER_CORRECTED_GGX = 4
+FL_MAT_STANDARD = 4
+FL_FRESNEL_DIELECTRIC = 0
+FL_FRESNEL_METALLIC = 1
 
 FL_SERVE_SHORTEST_FIRST = 0
 FL_SERVE_FIRST_COME = 1
@@ -62,7 +65,7 @@ class fl_material(C.Structure):
         ("roughness", C.c_float),
         ("eta", C.c_float),
         ("k", C.c_float),
-        ("reserved", C.c_float),
+        ("standard", C.c_int32),
     ]
 
 
@@ -79,6 +82,18 @@ class fl_light(C.Structure):
     ]
 
 
+class fl_standard_surface(C.Structure):
+    _fields_ = [
+        ("kd", C.c_float * 3), ("kd_weight", C.c_float), ("kd_roughness", C.c_float),
+        ("ks", C.c_float * 3), ("ks_weight", C.c_float), ("ks_roughness", C.c_float), ("ks_anisotropic", C.c_float),
+        ("ks_ior", C.c_float), ("fresnel_type", C.c_int32),
+        ("kt", C.c_float * 3), ("kt_weight", C.c_float),
+        ("sheen_color", C.c_float * 3), ("sheen_weight", C.c_float), ("sheen_roughness", C.c_float),
+        ("coat_color", C.c_float * 3), ("coat_weight", C.c_float), ("coat_ior", C.c_float), ("coat_gloss", C.c_float),
+        ("thin_film_thickness", C.c_float), ("thin_film_ior", C.c_float), ("thin_walled", C.c_int32),
+    ]
+
+
 class fl_scene_desc(C.Structure):
     _fields_ = [
         ("verts", C.POINTER(C.c_float)),
@@ -88,6 +103,8 @@ class fl_scene_desc(C.Structure):
         ("n_materials", C.c_uint32),
         ("lights", C.POINTER(fl_light)),
         ("n_lights", C.c_uint32),
+        ("standard_surfaces", C.POINTER(fl_standard_surface)),
+        ("n_standard_surfaces", C.c_uint32),
     ]
 
 

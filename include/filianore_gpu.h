@@ -110,8 +110,34 @@ enum {
                                     shading/bxdfs/microfacetreflection.cpp, fresnel/fresnelconductor.cpp */
     FL_MAT_ROUGH_DIELECTRIC = 2, /* GGX reflection + MicrofacetTransmission, FresnelDielectric
                                     shading/closures/microfacettransmission.cpp */
-    FL_MAT_SMOOTH_DIELECTRIC = 3 /* FresnelSpecular              shading/closures/fresnelspecular.cpp */
+    FL_MAT_SMOOTH_DIELECTRIC = 3, /* FresnelSpecular             shading/closures/fresnelspecular.cpp */
+    FL_MAT_STANDARD = 4          /* StandardSurfaceMaterial      shading/materials/standardsurface.cpp:72-159;
+                                    parameters in fl_scene_desc.standard_surfaces[fl_material.standard] */
 };
+
+enum {
+    FL_FRESNEL_DIELECTRIC = 0,   /* FresnelType::Dielectric: Schlick with r0 from the specular IOR */
+    FL_FRESNEL_METALLIC = 1      /* FresnelType::Metallic: Schlick with r0 = the specular colour */
+};
+
+/* The StandardSurfaceMaterial's parameters with constant textures. Colours are upsampled
+ * with from_reflectance_rgb. The lobes follow compute_scattering_functions: Oren-Nayar
+ * diffuse (sigma = 90 * kd_roughness) when there is no specular weight; otherwise a Fresnel-
+ * blended diffuse + GGX specular lobe (or, with kt_weight > 0, FresnelSpecular with R = ks,
+ * T = kt); then an Estevez sheen lobe and a GTR1 clear coat when their weights are > 0.
+ * Not supported (fl_scene_create rejects them): thin-film interference, the measured-metal
+ * Fresnel (FresnelType::WavelengthDependentMetallic), thin-walled diffuse transmission and
+ * bump maps. */
+typedef struct {
+    float kd[3], kd_weight, kd_roughness;
+    float ks[3], ks_weight, ks_roughness, ks_anisotropic, ks_ior;
+    int32_t fresnel_type;        /* FL_FRESNEL_* */
+    float kt[3], kt_weight;
+    float sheen_color[3], sheen_weight, sheen_roughness;
+    float coat_color[3], coat_weight, coat_ior, coat_gloss;
+    float thin_film_thickness, thin_film_ior;  /* thickness must be 0 */
+    int32_t thin_walled;                       /* must be 0 */
+} fl_standard_surface;
 
 typedef struct {
     int32_t type;       /* FL_MAT_* */
@@ -120,7 +146,7 @@ typedef struct {
     float roughness;    /* alpha = roughness^2 (materials/standardsurface.cpp:104-106) */
     float eta;          /* dielectric IOR, or conductor eta */
     float k;            /* conductor absorption */
-    float reserved;
+    int32_t standard;   /* FL_MAT_STANDARD: index into fl_scene_desc.standard_surfaces */
 } fl_material;
 
 enum {
@@ -156,6 +182,8 @@ typedef struct {
     uint32_t n_materials;
     const fl_light *lights;         /* order = the reference's Scene::illuminants order */
     uint32_t n_lights;
+    const fl_standard_surface *standard_surfaces;  /* for FL_MAT_STANDARD materials (nullable) */
+    uint32_t n_standard_surfaces;
 } fl_scene_desc;
 
 typedef struct {

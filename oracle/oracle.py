@@ -208,6 +208,9 @@ def write_scene_file(path, scene, params, nthreads=0, pixels=None, width=None, h
         f.write(bytes(scene.materials_array())[: C.sizeof(T.fl_material) * len(scene.materials)])
         f.write(bytes(scene.lights_array())[: C.sizeof(T.fl_light) * len(scene.lights)])
         f.write(px.tobytes())
+        stds, n_std = scene.standard_array()
+        f.write(np.uint32(n_std).tobytes())
+        f.write(bytes(stds)[: C.sizeof(T.fl_standard_surface) * n_std])
 
 
 def run_reference(scene_path, out_path, W, H):

@@ -152,6 +152,16 @@ typedef struct {
     float mat_eta, mat_k;
     int nl;
     int corrected;   /* FL_RENDER_CORRECTED_GGX */
+    /* StandardSurfaceMaterial (FL_MAT_STANDARD): the lobes in the order
+     * compute_scattering_functions adds them and their parameters */
+    int std_n, std_lobes[4];
+    spec kd, ks, kt, sheen, coat;
+    float kd_weight, on_A, on_B;     /* OrenNayarBRDF(kd, kdweight, 90 * kdrough) */
+    float fb_A, fb_B;                /* the blended lobe's OrenNayarBRDF(kd, kdweight, kdrough) */
+    float ks_weight, ro;
+    int fresnel_type;
+    float sheen_weight, sheen_rough;
+    float coat_weight, coat_ior, coat_gloss;
 } bsdf_t;
 
 static v3 to_local(const bsdf_t *b, v3 v) { return v3m(v3_dot(v, b->s), v3_dot(v, b->t), v3_dot(v, b->ns)); }
@@ -258,11 +268,17 @@ static float fr_conductor(float cosI, float etaT_, float k_) {
 }
 
 /* ---- lobes. Lobe ids: 0 lambert, 1 microfacet reflection, 2 microfacet transmission, 3 fresnel specular */
+/* lobes: 0 Lambert, 1 GGX microfacet reflection, 2 GGX microfacet transmission,
+ * 3 FresnelSpecular (R = T = the material colour), and the StandardSurface lobes
+ * 4 Oren-Nayar, 5 Fresnel-blended diffuse + specular, 6 Estevez sheen, 7 GTR1 clear coat,
+ * 8 FresnelSpecular with R = ks, T = kt */
 static int lobe_type(int lobe) {
     switch (lobe) {
     case 0: return BSDF_REFLECTION | BSDF_DIFFUSE;
     case 1: return BSDF_REFLECTION | BSDF_GLOSSY;
     case 2: return BSDF_TRANSMISSION | BSDF_GLOSSY;
+    case 4: return BSDF_REFLECTION | BSDF_DIFFUSE;
+    case 5: case 6: case 7: return BSDF_REFLECTION | BSDF_GLOSSY;
     default: return BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR;
     }
 }
@@ -271,8 +287,78 @@ static int bsdf_lobes(const bsdf_t *b, int *lobes) {
     case FL_MAT_LAMBERT: lobes[0] = 0; return 1;
     case FL_MAT_CONDUCTOR: lobes[0] = 1; return 1;
     case FL_MAT_ROUGH_DIELECTRIC: lobes[0] = 1; lobes[1] = 2; return 2;
+    case FL_MAT_STANDARD:
+        for (int i = 0; i < b->std_n; ++i) lobes[i] = b->std_lobes[i];
+        return b->std_n;
     default: lobes[0] = 3; return 1;
     }
+}
+
+/* ---- StandardSurface lobes */
+/* OrenNayarBRDF::OrenNayarBRDF (orennayar.cpp:6-12): sigma in degrees */
+static void oren_nayar_ab(float sigma_deg, float *A, float *B) {
+    float sigma = (ORC_PI / 180.f) * sigma_deg;
+    float sigma2 = sigma * sigma;
+    *A = 1.f - (sigma2 / (2.f * (sigma2 + 0.33f)));
+    *B = 0.45f * sigma2 / (sigma2 + 0.09f);
+}
+/* OrenNayarBRDF::evaluate (orennayar.cpp:14-39) */
+static void oren_nayar_eval(const spec *R, float weight, float A, float B, v3 wo, v3 wi, int nl, spec *out) {
+    float sinThetaI = sint(wi), sinThetaO = sint(wo);
+    float maxCos = 0.f;
+    if (sinThetaI > 1e-4 && sinThetaO > 1e-4) {
+        float sinPhiI = sinphi(wi), cosPhiI = cosphi(wi), sinPhiO = sinphi(wo), cosPhiO = cosphi(wo);
+        float dCos = cosPhiI * cosPhiO + sinPhiI * sinPhiO;
+        maxCos = dCos > 0.f ? dCos : 0.f;
+    }
+    float sinAlpha, tanBeta;
+    if (fabsf(wi.z) > fabsf(wo.z)) { sinAlpha = sinThetaO; tanBeta = sinThetaI / fabsf(wi.z); }
+    else { sinAlpha = sinThetaI; tanBeta = sinThetaO / fabsf(wo.z); }
+    float v = (A + B * maxCos * sinAlpha * tanBeta);
+    for (int i = 0; i < nl; ++i) out->c[i] = R->c[i] * ORC_INV_PI * v * weight;
+}
+/* cosine_hemisphere_sample (shadingcore.h:65-89), flipped to wo's side */
+static v3 cos_hemi(v3 wo, float ux, float uy) {
+    float ox = ux * 2.f - 1.f, oy = uy * 2.f - 1.f, dx, dy;
+    if (ox == 0 && oy == 0) { dx = 0.f; dy = 0.f; }
+    else {
+        float theta, r;
+        if (fabsf(ox) > fabsf(oy)) { r = ox; theta = ORC_PI_OVER_4 * (oy / ox); }
+        else { r = oy; theta = ORC_PI_OVER_2 - ORC_PI_OVER_4 * (ox / oy); }
+        dx = r * cosf(theta); dy = r * sinf(theta);
+    }
+    float zz = 1.f - dx * dx - dy * dy;
+    v3 w = v3m(dx, dy, sqrtf(zz > 0.f ? zz : 0.f));
+    if (wo.z < 0) w.z *= -1.f;
+    return w;
+}
+static v3 reflect_wh(v3 wo, v3 wh) { return v3_sub(v3_mul(v3_mul(wh, 2.f), v3_dot(wo, wh)), wo); }
+/* EstevezSheenDistribution (estevez.cpp:8-34) */
+static float est_D(float r, v3 wh) {
+    float inv = 1.f / r;
+    return (2.f + inv) * powf(sint(wh), inv) / (2.f * ORC_PI);
+}
+static float est_plerp(float r, float p0, float p1) { return ((1.f - r) * (1.f - r)) * p0 + (1.f - ((1.f - r) * (1.f - r))) * p1; }
+static float est_lambda(float r, v3 w) {
+    float a = est_plerp(r, 25.3245f, 21.5473f), b = est_plerp(r, 3.32435f, 3.82987f), c = est_plerp(r, 0.16801f, 0.19823f);
+    float d = est_plerp(r, -1.27393f, -1.97760f), e = est_plerp(r, -4.85967f, -4.32054f);
+#define EST_L(v) (a / (1.f + b * powf((v), c)) + (d * (v)) + e)
+    float ac = fabsf(w.z);
+    if (ac < 0.5f) return expf(EST_L(ac));
+    float ex = 2.f * EST_L(0.5f) - EST_L(1.f - ac);
+#undef EST_L
+    return expf(ex);
+}
+/* ClearcoatReflectionBRDF helpers (clearcoat.cpp:6-19) */
+static float gtr1(float cosTheta, float alpha) {
+    float alpha2 = alpha * alpha;
+    return (alpha2 - 1) / (ORC_PI * logf(alpha2) * (1 + (alpha2 - 1) * cosTheta * cosTheta));
+}
+/* smithG_GGX calls the unqualified sqrt, which resolves to the double-precision C function:
+ * the sum and the division are carried in double and rounded to float on return */
+static float smith_g_ggx(float cosTheta, float alpha) {
+    float alpha2 = alpha * alpha, cosTheta2 = cosTheta * cosTheta;
+    return (float)(1.f / (cosTheta + sqrt((double)(alpha2 + cosTheta2 - alpha2 * cosTheta2))));
 }
 static int matches(int type, int flags) { return (type & flags) == type; }
 
@@ -312,6 +398,62 @@ static void lobe_eval(const bsdf_t *b, int lobe, v3 wo, v3 wi, spec *out) {
         for (int i = 0; i < nl; ++i) out->c[i] = (1.f - F) * b->R.c[i] * v;
         return;
     }
+    if (lobe == 4) { oren_nayar_eval(&b->kd, b->kd_weight, b->on_A, b->on_B, wo, wi, nl, out); return; }
+    if (lobe == 5) {
+        /* FresnelBlendedDiffuseSpecularBRDF::evaluate (fresnelblendeddiffspec.cpp:18-38) */
+        float r1 = 1.f - .5f * fabsf(wi.z);
+        float r1pow5 = (r1 * r1) * (r1 * r1) * r1;
+        float r2 = 1.f - .5f * fabsf(wo.z);
+        float r2pow5 = (r2 * r2) * (r2 * r2) * r2;
+        spec on;
+        oren_nayar_eval(&b->kd, b->kd_weight, b->fb_A, b->fb_B, wo, wi, nl, &on);
+        v3 wh = v3_add(wi, wo);
+        if (wh.x == 0 && wh.y == 0 && wh.z == 0) { sp_set(out, nl, 0.f); return; }
+        wh = v3_norm(wh);
+        float cF = v3_dot(wi, wh);
+        float D = ggx_D(b, wh);
+        float den = (4.f * v3_absdot(wi, wh) * fmaxf(fabsf(wi.z), fabsf(wo.z)));
+        float R1 = 1.f - cF;
+        for (int i = 0; i < nl; ++i) {
+            float diffuse = (28.f / 23.f) * on.c[i] * (1.f - b->ro) * (1 - r1pow5) * (1 - r2pow5);
+            float F;
+            if (b->fresnel_type == FL_FRESNEL_METALLIC) {
+                /* SchlickMetallic::evaluate (schlickmetallic.cpp:7-10), r0 = ks */
+                F = b->ks.c[i] + (1.f - b->ks.c[i]) * (R1 * R1 * R1 * R1 * R1);
+            } else {
+                /* SchlickDielectric::evaluate (schlickdielectric.cpp:7-11) */
+                F = b->ro + ((R1 * R1) * (R1 * R1) * R1) * (1.f - b->ro);
+            }
+            float specular = D * F / den;
+            specular = b->ks.c[i] * specular * b->ks_weight;
+            out->c[i] = diffuse + specular;
+        }
+        return;
+    }
+    if (lobe == 6) {
+        /* MicrofacetReflectionBRDF::evaluate (microfacetreflection.cpp:11-28) with the Estevez
+         * distribution and FresnelNull */
+        float cosThetaO = fabsf(wo.z), cosThetaI = fabsf(wi.z);
+        v3 wh = v3_add(wi, wo);
+        if (cosThetaI == 0 || cosThetaO == 0 || (wh.x == 0 && wh.y == 0 && wh.z == 0)) { sp_set(out, nl, 0.f); return; }
+        wh = v3_norm(wh);
+        float D = est_D(b->sheen_rough, wh);
+        float G = 1.f / (1.f + est_lambda(b->sheen_rough, wo) + est_lambda(b->sheen_rough, wi));
+        float den = 4.f * cosThetaO * cosThetaI;
+        for (int i = 0; i < nl; ++i) out->c[i] = b->sheen.c[i] * b->sheen_weight * D * G * 1.f / den;
+        return;
+    }
+    if (lobe == 7) {
+        /* ClearcoatReflectionBRDF::evaluate (clearcoat.cpp:28-41) */
+        v3 wh = v3_add(wi, wo);
+        if (wh.x == 0 && wh.y == 0 && wh.z == 0) { sp_set(out, nl, 0.f); return; }
+        wh = v3_norm(wh);
+        float Dr = gtr1(fabsf(wh.z), b->coat_gloss);
+        float Fr = fr_dielectric(v3_dot(wo, wh), 1.f, b->coat_ior);
+        float Gr = smith_g_ggx(fabsf(wo.z), .25f) * smith_g_ggx(fabsf(wi.z), .25f);
+        for (int i = 0; i < nl; ++i) out->c[i] = b->coat.c[i] * Fr * b->coat_weight * Gr * Dr / 4;
+        return;
+    }
     sp_set(out, nl, 0.f);
 }
 
@@ -330,6 +472,29 @@ static float lobe_pdf(const bsdf_t *b, int lobe, v3 wo, v3 wi) {
         float sqrtDenom = v3_dot(wo, wh) + eta * v3_dot(wi, wh);
         float dwh_dwi = fabsf((eta * eta * v3_dot(wi, wh)) / (sqrtDenom * sqrtDenom));
         return ggx_pdf(b, wo, wh) * dwh_dwi;
+    }
+    if (lobe == 4) return same_hemi(wo, wi) ? fabsf(wi.z) * ORC_INV_PI : 0.f;
+    if (lobe == 5) {
+        /* fresnelblendeddiffspec.cpp:61-67 */
+        if (!same_hemi(wo, wi)) return 0;
+        v3 wh = v3_norm(v3_add(wo, wi));
+        float pdf_wh = ggx_pdf(b, wo, wh);
+        return .5f * (fabsf(wi.z) * ORC_INV_PI + pdf_wh / (4 * v3_dot(wo, wh)));
+    }
+    if (lobe == 6) {
+        /* MicrofacetReflectionBRDF::pdf with MicrofacetDistribution::pdf = D |cos theta_h| */
+        if (!same_hemi(wo, wi)) return 0.f;
+        v3 wh = v3_norm(v3_add(wo, wi));
+        return est_D(b->sheen_rough, wh) * fabsf(wh.z) / (4.f * v3_dot(wo, wh));
+    }
+    if (lobe == 7) {
+        /* clearcoat.cpp:70-80 */
+        if (!same_hemi(wo, wi)) return 0;
+        v3 wh = v3_add(wi, wo);
+        if (wh.x == 0 && wh.y == 0 && wh.z == 0) return 0;
+        wh = v3_norm(wh);
+        float Dr = gtr1(fabsf(wh.z), b->coat_gloss);
+        return Dr * fabsf(wh.z) / (4 * v3_dot(wo, wh));
     }
     return 0.f;
 }
@@ -383,14 +548,66 @@ static void lobe_sample(const bsdf_t *b, int lobe, v3 wo, v3 *wi, float ux, floa
         lobe_eval(b, 2, wo, *wi, f);
         return;
     }
-    /* fresnel specular */
+    if (lobe == 4) {
+        *wi = cos_hemi(wo, ux, uy);
+        *pdf = lobe_pdf(b, 4, wo, *wi);
+        lobe_eval(b, 4, wo, *wi, f);
+        return;
+    }
+    if (lobe == 5) {
+        /* fresnelblendeddiffspec.cpp:40-59 */
+        if (ux < .5) {
+            float u0 = 2 * ux;
+            if (u0 > 1.f - ORC_SHADOW_EPSILON) u0 = 1.f - ORC_SHADOW_EPSILON;
+            *wi = cos_hemi(wo, u0, uy);
+        } else {
+            float u0 = 2 * (ux - .5f);
+            if (u0 > 1.f - ORC_SHADOW_EPSILON) u0 = 1.f - ORC_SHADOW_EPSILON;
+            v3 wh = ggx_sample_wh(b, wo, u0, uy);
+            *wi = reflect_wh(wo, wh);
+            if (!same_hemi(wo, *wi)) { sp_set(f, nl, 0.f); return; }
+        }
+        *pdf = lobe_pdf(b, 5, wo, *wi);
+        lobe_eval(b, 5, wo, *wi, f);
+        return;
+    }
+    if (lobe == 6) {
+        /* MicrofacetReflectionBRDF::sample (microfacetreflection.cpp:30-52); the Estevez
+         * sample_wh draws a cosine-weighted normal on wo's side (estevez.cpp:36-42) */
+        if (wo.z == 0) { sp_set(f, nl, 0.f); return; }
+        v3 wh = cos_hemi(wo, ux, uy);
+        if (v3_dot(wo, wh) < 0) { sp_set(f, nl, 0.f); return; }
+        *wi = reflect_wh(wo, wh);
+        if (!same_hemi(wo, *wi)) { sp_set(f, nl, 0.f); return; }
+        *pdf = est_D(b->sheen_rough, wh) * fabsf(wh.z) / (4.f * v3_dot(wo, wh));
+        lobe_eval(b, 6, wo, *wi, f);
+        return;
+    }
+    if (lobe == 7) {
+        /* clearcoat.cpp:43-68 */
+        if (wo.z == 0) { sp_set(f, nl, 0.f); return; }
+        float alpha2 = b->coat_gloss * b->coat_gloss;
+        float cosTheta = sqrtf(fmaxf(0.f, (1 - powf(alpha2, 1 - ux)) / (1 - alpha2)));
+        float sinTheta = sqrtf(fmaxf(0.f, 1 - cosTheta * cosTheta));
+        float phi = 2 * ORC_PI * uy;
+        v3 wh = v3m(sinTheta * cosf(phi), sinTheta * sinf(phi), cosTheta);
+        if (!same_hemi(wo, wh)) wh = v3_neg(wh);
+        *wi = reflect_wh(wo, wh);
+        if (!same_hemi(wo, *wi)) { sp_set(f, nl, 0.f); return; }
+        *pdf = lobe_pdf(b, 7, wo, *wi);
+        lobe_eval(b, 7, wo, *wi, f);
+        return;
+    }
+    /* fresnel specular (lobe 3; lobe 8 with R = ks, T = kt) */
+    const spec *Rs = lobe == 8 ? &b->ks : &b->R;
+    const spec *Ts = lobe == 8 ? &b->kt : &b->R;
     float F = fr_dielectric(wo.z, 1.f, b->mat_eta);
     if (ux < F) {
         *wi = v3m(-wo.x, -wo.y, wo.z);
         *type = BSDF_SPECULAR | BSDF_REFLECTION;
         *pdf = F;
         float ac = fabsf(wi->z);
-        for (int i = 0; i < nl; ++i) f->c[i] = b->R.c[i] * F / ac;
+        for (int i = 0; i < nl; ++i) f->c[i] = Rs->c[i] * F / ac;
     } else {
         int entering = wo.z > 0;
         float etaI = entering ? 1.f : b->mat_eta;
@@ -409,7 +626,7 @@ static void lobe_sample(const bsdf_t *b, int lobe, v3 wo, v3 *wi, float ux, floa
         *pdf = 1.f - F;
         float ac = fabsf(wi->z);
         for (int i = 0; i < nl; ++i) {
-            float ft = b->R.c[i] * (1.f - F);
+            float ft = Ts->c[i] * (1.f - F);
             ft *= sc;
             f->c[i] = ft / ac;
         }
@@ -517,6 +734,39 @@ static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda
         else orc_reflectance(S->tab, m->rgb, S->mode, lambda, b->R.c);
     } else {
         sp_set(&b->R, b->nl, 1.f);
+    }
+    if (m->type == FL_MAT_STANDARD) {
+        /* StandardSurfaceMaterial::compute_scattering_functions (standardsurface.cpp:72-159)
+         * with constant textures; thin film, measured metals and thin walls are rejected
+         * by the GPU's fl_scene_create and never reach here */
+        const fl_standard_surface *p = &S->sc->standard_surfaces[m->standard];
+        b->eta = (p->ks_weight > 0 && p->kt_weight > 0) ? p->ks_ior : 1.f;
+        b->mat_eta = p->ks_ior;
+        orc_reflectance(S->tab, p->kd, S->mode, lambda, b->kd.c);
+        orc_reflectance(S->tab, p->ks, S->mode, lambda, b->ks.c);
+        orc_reflectance(S->tab, p->kt, S->mode, lambda, b->kt.c);
+        orc_reflectance(S->tab, p->sheen_color, S->mode, lambda, b->sheen.c);
+        orc_reflectance(S->tab, p->coat_color, S->mode, lambda, b->coat.c);
+        b->kd_weight = p->kd_weight;
+        oren_nayar_ab(p->kd_roughness * 90.f, &b->on_A, &b->on_B);
+        oren_nayar_ab(p->kd_roughness, &b->fb_A, &b->fb_B);  /* the blended lobe passes the raw roughness as sigma */
+        float aspect = sqrtf(1.f - p->ks_anisotropic * 0.9f);
+        float a2 = p->ks_roughness * p->ks_roughness;
+        b->ax = fmaxf(.001f, a2 / aspect);
+        b->ay = fmaxf(.001f, a2 * aspect);
+        b->ro = ((1.f - p->ks_ior) / (1.f + p->ks_ior)) * ((1.f - p->ks_ior) / (1.f + p->ks_ior));
+        b->ks_weight = p->ks_weight;
+        b->fresnel_type = p->fresnel_type;
+        b->sheen_weight = p->sheen_weight;
+        b->sheen_rough = fmaxf(.001f, p->sheen_roughness);
+        b->coat_weight = p->coat_weight;
+        b->coat_ior = p->coat_ior;
+        b->coat_gloss = (1.f - p->coat_gloss) * .1f + p->coat_gloss * .001f;  /* lerp(gloss, .1, .001) */
+        b->std_n = 0;
+        if (p->kd_weight > 0 && p->ks_weight <= 0) b->std_lobes[b->std_n++] = 4;
+        if (p->ks_weight > 0) b->std_lobes[b->std_n++] = p->kt_weight > 0 ? 8 : 5;
+        if (p->sheen_weight > 0) b->std_lobes[b->std_n++] = 6;
+        if (p->coat_weight > 0) b->std_lobes[b->std_n++] = 7;
     }
 }
 

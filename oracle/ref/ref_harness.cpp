@@ -48,6 +48,7 @@
 #include "filianore/shading/fresnel/fresnelconductor.h"
 #include "filianore/shading/fresnel/fresneldielectric.h"
 #include "filianore/shading/materials/lambert.h"
+#include "filianore/shading/materials/standardsurface.h"
 #include "filianore/shading/microfacets/ggx.h"
 #include "filianore/shading/textures/constant.h"
 #include "filianore/shapes/triangle.h"
@@ -231,6 +232,10 @@ int render(const char *scene_path, const char *out_path) {
     std::vector<fl_light> lights;
     bool ok = read_n(f, verts, (size_t)h.n_tri * 9) && read_n(f, tri_mat, h.n_tri) && read_n(f, mats, h.n_mat) &&
               read_n(f, lights, h.n_light) && read_n(f, pixels, h.n_pixels);
+    // optional trailer: the StandardSurfaceMaterial parameters of FL_MAT_STANDARD materials
+    std::vector<fl_standard_surface> stds;
+    uint32_t n_std = 0;
+    if (ok && fread(&n_std, sizeof(n_std), 1, f) == 1) ok = read_n(f, stds, n_std);
     fclose(f);
     if (!ok) { fprintf(stderr, "truncated scene file\n"); return 2; }
     if (h.spectral_mode != FL_SPECTRAL_BINS60) {
@@ -253,6 +258,18 @@ int render(const char *scene_path, const char *out_path) {
             materials.push_back(std::make_shared<RoughDielectricMaterial>(alpha, m.eta));
         } else if (m.type == FL_MAT_SMOOTH_DIELECTRIC) {
             materials.push_back(std::make_shared<SmoothDielectricMaterial>(m.eta));
+        } else if (m.type == FL_MAT_STANDARD && m.standard >= 0 && (uint32_t)m.standard < stds.size()) {
+            // the reference's own StandardSurfaceMaterial with constant textures
+            const fl_standard_surface &p = stds[m.standard];
+            auto spec = [](const float c[3]) {
+                return std::make_shared<ConstantTexture<PrincipalSpectrum>>(from_reflectance_rgb(Vector3f(c[0], c[1], c[2])));
+            };
+            auto flt = [](float v) { return std::make_shared<ConstantTexture<float>>(v); };
+            materials.push_back(std::make_shared<StandardSurfaceMaterial>(
+                p.kd_weight, spec(p.kd), flt(p.kd_roughness), p.ks_weight, spec(p.ks), flt(p.ks_roughness),
+                flt(p.ks_anisotropic), p.fresnel_type, p.ks_ior, 0, p.sheen_weight, spec(p.sheen_color),
+                flt(p.sheen_roughness), p.kt_weight, spec(p.kt), p.coat_weight, spec(p.coat_color), p.coat_ior,
+                p.coat_gloss, p.thin_film_thickness, p.thin_film_ior, p.thin_walled != 0, nullptr));
         } else {
             fprintf(stderr, "unknown material type\n");
             return 2;

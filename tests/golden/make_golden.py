@@ -14,7 +14,12 @@ reference sources with oracle/Makefile). Outputs:
                         64x64 at 4 spp (float64) and 128x128 at 16 spp (float32)
   cornell_delta_ref.npz the Cornell box ("lambert" and "materials") with the reference's
                         point, spot and directional lights added: 64x64 at 4 spp (float64)
-Usage: python tests/golden/make_golden.py
+  cornell_standard_ref.npz  the Cornell box with StandardSurfaceMaterial boxes ("standard":
+                        Oren-Nayar + sheen, Fresnel-blended anisotropic GGX + clear coat;
+                        "standard2": Schlick-metallic blend, specular R/T glass + sheen):
+                        64x64 at 4 spp (float64)
+Usage: python tests/golden/make_golden.py [part ...]   (parts: tables pcg cornell materials
+       delta standard; default all)
 """
 import os
 import sys
@@ -31,16 +36,16 @@ import oracle  # noqa: E402
 from filianore_b200 import scenes, types as T  # noqa: E402
 
 
-def main():
-    oracle.build(ref=True)
-    tmp = tempfile.mkdtemp()
-    # spectral tables
-    tpath = os.path.join(tmp, "tables.bin")
+def tables(tmp):
     import subprocess
+    tpath = os.path.join(tmp, "tables.bin")
     subprocess.run([oracle.REF_BIN, "--tables", tpath], check=True)
     t = oracle.load_tables_dump(tpath)
     np.savez_compressed(os.path.join(HERE, "spectral_tables.npz"), **t)
-    # pcg32
+
+
+def pcg(tmp):
+    import subprocess
     ppath = os.path.join(tmp, "pcg.bin")
     subprocess.run([oracle.REF_BIN, "--pcg", ppath], check=True)
     raw = np.fromfile(ppath, np.uint8)
@@ -51,7 +56,10 @@ def main():
                         seeds=np.array([[0, 1], [1, 1], [12345, 1], [42, 54], [65535, 1]], np.uint64),
                         seq=seq, adv_deltas=np.array([1, 1 << 16, 5 << 16], np.int64), adv=adv,
                         float_seed=np.array([3, 1], np.uint64), floats=flt)
-    # Cornell box renders by the reference integrator
+
+
+def cornell(tmp):
+    """Cornell box renders by the reference integrator"""
     out = {}
     for (W, H, spp, key, dt) in [(64, 64, 4, "small", np.float64), (256, 256, 16, "full", np.float32)]:
         sc = scenes.cornell(W, H)
@@ -64,7 +72,10 @@ def main():
         out[f"{key}_spp"] = np.int32(spp)
         print(key, info)
     np.savez_compressed(os.path.join(HERE, "cornell_ref.npz"), **out)
-    # the same box with the GGX conductor / rough dielectric / smooth glass materials
+
+
+def materials(tmp):
+    """the same box with the GGX conductor / rough dielectric / smooth glass materials"""
     out = {}
     for variant in ("materials", "glass"):
         for (W, spp, key, dt) in [(64, 4, "small", np.float64), (128, 16, "full", np.float32)]:
@@ -77,7 +88,10 @@ def main():
             out[f"{variant}_{key}_xyz"] = film.astype(dt)
             print(variant, key, info)
     np.savez_compressed(os.path.join(HERE, "cornell_materials_ref.npz"), **out)
-    # the box with the reference's point, spot and directional lights added
+
+
+def delta(tmp):
+    """the box with the reference's point, spot and directional lights added"""
     out = {}
     for variant in ("lambert", "materials"):
         sc = scenes.cornell_delta(64, 64, variant)
@@ -91,5 +105,31 @@ def main():
     np.savez_compressed(os.path.join(HERE, "cornell_delta_ref.npz"), **out)
 
 
+def standard(tmp):
+    """the box with StandardSurfaceMaterial boxes"""
+    out = {}
+    for variant in ("standard", "standard2"):
+        sc = scenes.cornell(64, 64, variant)
+        p = scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60)
+        spath = os.path.join(tmp, f"{variant}.scene")
+        fpath = os.path.join(tmp, f"{variant}.film")
+        oracle.write_scene_file(spath, sc, p)
+        film, info = oracle.run_reference(spath, fpath, 64, 64)
+        out[f"{variant}_xyz"] = film.astype(np.float64)
+        print(variant, info)
+    np.savez_compressed(os.path.join(HERE, "cornell_standard_ref.npz"), **out)
+
+
+PARTS = {"tables": tables, "pcg": pcg, "cornell": cornell, "materials": materials, "delta": delta,
+         "standard": standard}
+
+
+def main(parts):
+    oracle.build(ref=True)
+    tmp = tempfile.mkdtemp()
+    for name in parts or list(PARTS):
+        PARTS[name](tmp)
+
+
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])
