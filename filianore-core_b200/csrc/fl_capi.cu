@@ -111,6 +111,56 @@ void smits_terms(const float rgb[3], int basis[3], float w[3]) {
     }
 }
 
+// from_reflectance_rgb (color/spectrumoperations.cpp:113-147) over the 60 bins, clamped
+// at zero (spectrum_clamp) from the Smits terms
+static void refl60(const std::vector<float> &binned, const int basis[3], const float w[3], float *out) {
+    for (int i = 0; i < 60; ++i) {
+        float r = 0.f;
+        for (int k = 0; k < 3; ++k) r += binned[180 + 60 * basis[k] + i] * w[k];
+        r *= 0.94f;
+        out[i] = r < 0.f ? 0.f : r;
+    }
+}
+
+// OrenNayarBRDF's A and B from sigma in degrees (bxdfs/orennayar.cpp:6-12)
+static void oren_nayar_ab(float sigma_deg, float *A, float *B) {
+    const float sigma = (kPi / 180.f) * sigma_deg;
+    const float sigma2 = sigma * sigma;
+    *A = 1.f - (sigma2 / (2.f * (sigma2 + 0.33f)));
+    *B = 0.45f * sigma2 / (sigma2 + 0.09f);
+}
+
+// StandardSurfaceMaterial::compute_scattering_functions (materials/standardsurface.cpp:72-159)
+// with constant textures: the lobes it adds and their parameters
+static StandardDev standard_dev(const fl_standard_surface &P) {
+    StandardDev d{};
+    d.eta = (P.ks_weight > 0 && P.kt_weight > 0) ? P.ks_ior : 1.f;
+    d.ior = P.ks_ior;
+    d.kd_weight = P.kd_weight;
+    oren_nayar_ab(P.kd_roughness * 90.f, &d.on_A, &d.on_B);  // sigma = 90 kdroughness
+    oren_nayar_ab(P.kd_roughness, &d.fb_A, &d.fb_B);         // the blended lobe passes kdroughness as sigma
+    const float aspect = std::sqrt(1.f - P.ks_anisotropic * 0.9f);
+    const float a2 = P.ks_roughness * P.ks_roughness;
+    d.ax = std::max(.001f, a2 / aspect);
+    d.ay = std::max(.001f, a2 * aspect);
+    d.ro = ((1.f - P.ks_ior) / (1.f + P.ks_ior)) * ((1.f - P.ks_ior) / (1.f + P.ks_ior));
+    d.ks_weight = P.ks_weight;
+    d.fresnel_type = P.fresnel_type;
+    d.sheen_weight = P.sheen_weight;
+    d.sheen_rough = std::max(.001f, P.sheen_roughness);
+    d.coat_weight = P.coat_weight;
+    d.coat_ior = P.coat_ior;
+    d.coat_gloss = (1.f - P.coat_gloss) * .1f + P.coat_gloss * .001f;  // lerp(gloss, .1, .001)
+    d.n_lobes = 0;
+    if (P.kd_weight > 0 && P.ks_weight <= 0) d.lobes[d.n_lobes++] = 4;
+    if (P.ks_weight > 0) d.lobes[d.n_lobes++] = P.kt_weight > 0 ? 8 : 5;
+    if (P.sheen_weight > 0) d.lobes[d.n_lobes++] = 6;
+    if (P.coat_weight > 0) d.lobes[d.n_lobes++] = 7;
+    const float *rgb[5] = {P.kd, P.ks, P.kt, P.sheen_color, P.coat_color};
+    for (int c = 0; c < 5; ++c) smits_terms(rgb[c], d.basis[c], d.w[c]);
+    return d;
+}
+
 }  // namespace fl
 
 using namespace fl;
@@ -269,11 +319,33 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
         set_error(ctx, "scene needs vertices for its triangles and at least one material");
         return FL_ERR_INVALID;
     }
-    for (uint32_t i = 0; i < d->n_materials; ++i)
-        if (d->materials[i].type < FL_MAT_LAMBERT || d->materials[i].type > FL_MAT_SMOOTH_DIELECTRIC) {
+    for (uint32_t i = 0; i < d->n_materials; ++i) {
+        const fl_material &M = d->materials[i];
+        if (M.type < FL_MAT_LAMBERT || M.type > FL_MAT_STANDARD) {
             set_error(ctx, "unknown material type");
             return FL_ERR_INVALID;
         }
+        if (M.type == FL_MAT_STANDARD &&
+            (!d->standard_surfaces || M.standard < 0 || (uint32_t)M.standard >= d->n_standard_surfaces)) {
+            set_error(ctx, "standard surface index out of range");
+            return FL_ERR_INVALID;
+        }
+    }
+    for (uint32_t i = 0; d->standard_surfaces && i < d->n_standard_surfaces; ++i) {
+        const fl_standard_surface &P = d->standard_surfaces[i];
+        if (P.fresnel_type != FL_FRESNEL_DIELECTRIC && P.fresnel_type != FL_FRESNEL_METALLIC) {
+            set_error(ctx, "standard surface: unsupported fresnel_type (the measured-metal Fresnel is not implemented)");
+            return FL_ERR_INVALID;
+        }
+        if (P.thin_film_thickness != 0.f) {
+            set_error(ctx, "standard surface: thin-film interference is not implemented (thickness must be 0)");
+            return FL_ERR_INVALID;
+        }
+        if (P.thin_walled != 0) {
+            set_error(ctx, "standard surface: thin-walled transmission is not implemented");
+            return FL_ERR_INVALID;
+        }
+    }
     if (d->tri_material)
         for (uint32_t i = 0; i < d->n_tri; ++i)
             if (d->tri_material[i] >= d->n_materials) {
@@ -358,8 +430,13 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
         md.eta = M.eta;
         md.k = M.k;
         smits_terms(M.rgb, md.basis, md.w);
+        md.standard = M.type == FL_MAT_STANDARD ? M.standard : 0;
         s->materials_host.push_back(md);
     }
+    const uint32_t n_std = d->standard_surfaces ? d->n_standard_surfaces : 0;
+    std::vector<StandardDev> std_host;
+    for (uint32_t i = 0; i < n_std; ++i) std_host.push_back(standard_dev(d->standard_surfaces[i]));
+    s->n_standard = n_std;
     s->n_lights = d->n_lights;
     s->n_materials = d->n_materials;
 
@@ -384,16 +461,19 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
     {
         // from_reflectance_rgb (color/spectrumoperations.cpp:113-147) over the 60 bins
         std::vector<float> refl((size_t)60 * d->n_materials);
-        for (uint32_t m = 0; m < d->n_materials; ++m) {
-            const MaterialDev &md = s->materials_host[m];
-            for (int i = 0; i < 60; ++i) {
-                float r = 0.f;
-                for (int k = 0; k < 3; ++k) r += ctx->binned_host[180 + 60 * md.basis[k] + i] * md.w[k];
-                r *= 0.94f;
-                refl[(size_t)m * 60 + i] = r < 0.f ? 0.f : r;
-            }
-        }
+        for (uint32_t m = 0; m < d->n_materials; ++m)
+            refl60(ctx->binned_host, s->materials_host[m].basis, s->materials_host[m].w, &refl[(size_t)m * 60]);
         SC_TRY(cudaMemcpy(s->mat_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
+    }
+    SC_TRY(cudaMalloc(&s->standard, sizeof(StandardDev) * (n_std ? n_std : 1)));
+    SC_TRY(cudaMalloc(&s->std_refl60, sizeof(float) * 300 * (n_std ? n_std : 1)));
+    if (n_std) {
+        std::vector<float> refl((size_t)300 * n_std);
+        for (uint32_t m = 0; m < n_std; ++m)
+            for (int c = 0; c < 5; ++c)
+                refl60(ctx->binned_host, std_host[m].basis[c], std_host[m].w[c], &refl[(size_t)m * 300 + 60 * c]);
+        SC_TRY(cudaMemcpy(s->standard, std_host.data(), sizeof(StandardDev) * n_std, cudaMemcpyHostToDevice));
+        SC_TRY(cudaMemcpy(s->std_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
     }
     if (d->n_tri) {
         SC_TRY(cudaMemcpyAsync(s->soup, d->verts, sizeof(float) * 9 * d->n_tri, cudaMemcpyHostToDevice, ctx->stream));
@@ -432,6 +512,8 @@ fl_status fl_scene_destroy(fl_scene *scene) {
     cudaFree(s->materials);
     cudaFree(s->lights);
     cudaFree(s->mat_refl60);
+    cudaFree(s->standard);
+    cudaFree(s->std_refl60);
     if (s->counted) s->ctx->children--;
     delete s;
     return FL_OK;

@@ -45,7 +45,7 @@ struct Context {
     cudaGraphExec_t wave_graph = nullptr;
     const void *graph_base = nullptr;
     size_t graph_cap = 0;
-    int graph_depth = -1, graph_nl_mode = -1, graph_count = -1;
+    int graph_depth = -1, graph_nl_mode = -1, graph_count = -1, graph_std = -1;
     std::atomic<int> children{0};       // live scenes, guides and servers made from this context
     int *d_error = nullptr;             // traversal error counter
     unsigned long long *d_counters = nullptr;  // 8 x u64 statistics
@@ -59,6 +59,27 @@ struct MaterialDev {
     float eta, k;
     int basis[3];       // Smits basis indices of from_reflectance_rgb
     float w[3];         // and their weights
+    int standard;       // FL_MAT_STANDARD: index into Scene::standard
+};
+
+// StandardSurfaceMaterial with constant textures, reduced on the host to what
+// compute_scattering_functions (materials/standardsurface.cpp:72-159) hands its BxDFs.
+// Lobe ids: 4 Oren-Nayar, 5 Fresnel-blended diffuse + specular, 6 Estevez sheen,
+// 7 GTR1 clear coat, 8 FresnelSpecular with R = ks and T = kt.
+struct StandardDev {
+    int n_lobes;
+    int lobes[4];         // in the order the material adds them
+    float eta;            // BSDF::eta: ks_ior with both specular and transmission weights, else 1
+    float ior;            // ks_ior (FresnelSpecular, Schlick r0)
+    float ax, ay;         // GGX alphas with the anisotropic aspect
+    float kd_weight, on_A, on_B;  // OrenNayarBRDF(kd, kdweight, 90 kdrough)
+    float fb_A, fb_B;             // the blended lobe's OrenNayarBRDF(kd, kdweight, kdrough)
+    float ks_weight, ro;
+    int fresnel_type;     // FL_FRESNEL_*
+    float sheen_weight, sheen_rough;
+    float coat_weight, coat_ior, coat_gloss;  // coat_gloss = lerp(gloss, .1, .001)
+    int basis[5][3];      // Smits terms of kd, ks, kt, sheen colour, coat colour
+    float w[5][3];
 };
 
 struct LightDev {
@@ -87,6 +108,9 @@ struct Scene {
     int32_t *tri_light = nullptr;     // soup order, -1 = not emissive
     MaterialDev *materials = nullptr;
     float *mat_refl60 = nullptr;      // n_materials x 60: from_reflectance_rgb in the 60 bins
+    StandardDev *standard = nullptr;  // n_standard StandardSurface records
+    float *std_refl60 = nullptr;      // n_standard x 5 x 60: their five colours in the 60 bins
+    uint32_t n_standard = 0;
     uint32_t n_materials = 0;
     LightDev *lights = nullptr;
     uint32_t n_lights = 0;

@@ -30,10 +30,13 @@
 
 namespace fl {
 
-// 0: miss, 1 + material type (Lambert, conductor, rough / smooth dielectric), and with
-// guiding on, kClassLambertLate: Lambert vertices past the guided ones (no inference)
-constexpr int kShadeClasses = 6;
-constexpr int kClassLambertLate = 5;
+// 0: miss, 1 + material type (Lambert, conductor, rough / smooth dielectric, standard
+// surface), and with guiding on, kClassLambertLate: Lambert vertices past the guided ones
+// (no inference)
+constexpr int kShadeClasses = 7;
+constexpr int kClassStandard = 1 + FL_MAT_STANDARD;
+constexpr int kClassLambertLate = 6;
+static_assert(1 + FL_MAT_STANDARD < kClassLambertLate, "one shading class per material type");
 constexpr int kGuidedVertices = 2;  // a path's first Lambert vertices are guided (and recorded)
 // path flags: bits 0..7 bounce, bit 8 specular, bits 9..10 Lambert vertices passed (guiding)
 __device__ __forceinline__ uint32_t lambert_count(uint32_t fl) { return (fl >> 9) & 3u; }
@@ -42,7 +45,8 @@ constexpr int kMaxSegs = 128;     // sample ranges per wave
 
 struct WaveCounters {
     uint32_t n_trace, n_cont, n_next, n_shadow;
-    uint32_t fetch_trace, fetch_rays2, pad0, pad1;  // persistent-kernel work counters
+    uint32_t fetch_trace, fetch_rays2;              // persistent-kernel work counters
+    uint32_t n_cont_std, pad1;                      // StandardSurface paths, from the back of q_cont
     uint32_t n_class[8];                            // shading queues by class
     unsigned long long rays, shadow_rays, bounces, paths;
     unsigned long long nodes, tris;  // FL_RENDER_COUNT
@@ -101,6 +105,8 @@ struct JobDev {
     const int32_t *tri_light;
     const MaterialDev *materials;
     const float *mat_refl60;
+    const StandardDev *standard;
+    const float *std_refl60;
     const LightDev *lights;
     int n_lights;
     int any_hit_ok;
@@ -280,7 +286,7 @@ __device__ inline int prim_light(const JobDev &A, int prim) {
     return -1;
 }
 
-template <int NL>
+template <int NL, bool STD>
 __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const SmemTables &sm, const Hit &h,
                                  float lambda0, Bsdf<NL> &b) {
     b.ng = h.n;
@@ -296,6 +302,23 @@ __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const Sm
     b.ay = m.ay;
     b.eta = (m.type == FL_MAT_ROUGH_DIELECTRIC || m.type == FL_MAT_SMOOTH_DIELECTRIC) ? m.eta : 1.f;
     b.corrected = A.corrected_ggx;
+    if (STD) {
+        // StandardSurfaceMaterial::compute_scattering_functions (materials/standardsurface.cpp:72-159)
+        // from the host-reduced record
+        const StandardDev *sd = A.standard + m.standard;
+        b.sd = sd;
+        b.eta = sd->eta;
+        b.mat_eta = sd->ior;
+        b.ax = sd->ax;
+        b.ay = sd->ay;
+        b.std60 = A.std_refl60 + 300 * (size_t)m.standard;
+        b.bases = sm.bases;
+        b.rgb_l0 = tab.rgb_lambda0;
+        b.rgb_l1 = tab.rgb_lambda1;
+        b.n_rgb = tab.n_rgb;
+        b.lambda0 = lambda0;
+        return;
+    }
     if (m.type == FL_MAT_LAMBERT) reflectance<NL>(sm, tab, m, A.mat_refl60 + 60 * (size_t)mi, lambda0, b.R);
     else b.R.set(1.f);
 }
@@ -308,7 +331,7 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
     const uint32_t n_seg = A.wave->n_seg;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         A.cnt->n_trace = n_wave;
-        A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = 0;
+        A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = A.cnt->n_cont_std = 0;
         A.cnt->fetch_trace = A.cnt->fetch_rays2 = 0;
         for (int c = 0; c < kShadeClasses; ++c) A.cnt->n_class[c] = 0;
     }
@@ -363,6 +386,7 @@ static __global__ void __launch_bounds__(128) k_advance(WaveCounters *cnt) {
     cnt->n_trace = cnt->n_next;
     cnt->n_next = 0;
     cnt->n_cont = 0;
+    cnt->n_cont_std = 0;
     cnt->n_shadow = 0;
     cnt->fetch_trace = 0;
     cnt->fetch_rays2 = 0;
@@ -446,13 +470,16 @@ __global__ void __launch_bounds__(128) k_trace_paths(RenderArgs A) {
     if (err) atomicAdd(&A.cnt->err, 1);
 }
 
-template <int NL>
+// STD: the StandardSurface instance, over the StandardSurface class alone; the other
+// instance takes every other class
+template <int NL, bool STD = false>
 __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
     __shared__ SmemTables sm;
     stage_tables(sm, A.tab, NL != 60);
     uint32_t off[kShadeClasses + 1];
     off[0] = 0;
-    for (int c = 0; c < kShadeClasses; ++c) off[c + 1] = off[c] + load_count(&A.cnt->n_class[c]);
+    for (int c = 0; c < kShadeClasses; ++c)
+        off[c + 1] = off[c] + ((c == kClassStandard) == STD ? load_count(&A.cnt->n_class[c]) : 0u);
     const uint32_t n = off[kShadeClasses];
     uint32_t shaded = 0;
     FL_WARP_UNIFORM_LOOP(q, n) {
@@ -497,8 +524,8 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                 store_spec<NL>(A.L, A.cap, slot, L);
                 const float lambda0 = A.lambda0[slot];
                 Bsdf<NL> b;
-                make_bsdf<NL>(J, A.tab, sm, hr, lambda0, b);
-                if (bsdf_num_components(b, kBsdfAll & ~kBsdfSpecular) > 0) {
+                make_bsdf<NL, STD>(J, A.tab, sm, hr, lambda0, b);
+                if (bsdf_num_components<STD>(b, kBsdfAll & ~kBsdfSpecular) > 0) {
                     Pcg32 rng;
                     rng.state = A.rng[slot];
                     rng.inc = 3u;
@@ -519,11 +546,11 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                         if (ls.vis_kind) wi = ls.wi;
                         if (ls.pdf > 0 && ls.radiance != 0.f) {
                             Spec<NL> f;
-                            bsdf_eval<NL>(b, hr.wo, wi, bsdfFlags, f);
+                            bsdf_eval<STD>(b, hr.wo, wi, bsdfFlags, f);
                             const float ad = absdot(wi, b.ns);
 #pragma unroll
                             for (int c = 0; c < NL; ++c) f.c[c] *= ad;
-                            scatteringPdf = bsdf_pdf<NL>(b, hr.wo, wi, bsdfFlags);
+                            scatteringPdf = bsdf_pdf<STD>(b, hr.wo, wi, bsdfFlags);
                             if (!f.black()) {
                                 // delta lights are not weighted (integrator.cpp:57-58)
                                 const float weight = light_is_delta(Ll) ? 1.f : power_heuristic(illumPdf, scatteringPdf);
@@ -556,7 +583,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                         if (!light_is_delta(Ll)) {
                             Spec<NL> f;
                             int sampledType = 0;
-                            bsdf_sample<NL>(b, hr.wo, wi, usx, usy, scatteringPdf, bsdfFlags, sampledType, f);
+                            bsdf_sample<STD>(b, hr.wo, wi, usx, usy, scatteringPdf, bsdfFlags, sampledType, f);
                             const float ad = absdot(wi, b.ns);
 #pragma unroll
                             for (int c = 0; c < NL; ++c) f.c[c] *= ad;
@@ -595,8 +622,8 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                 }
             }
         }
-        const uint32_t pos = warp_append(&A.cnt->n_cont, alive);
-        if (alive) A.q_cont[pos] = slot;
+        const uint32_t pos = warp_append(STD ? &A.cnt->n_cont_std : &A.cnt->n_cont, alive);
+        if (alive) A.q_cont[STD ? A.cap - 1 - pos : pos] = slot;
     }
     warp_count(&A.cnt->bounces, shaded);
 }
@@ -741,17 +768,17 @@ __global__ void __launch_bounds__(32 * kInferWarps, 3) k_guide_infer(RenderArgs 
     }
 }
 
-template <int NL, bool GUIDE = false>
+template <int NL, bool GUIDE = false, bool STD = false>
 __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
     __shared__ SmemTables sm;
     stage_tables(sm, A.tab, NL != 60);
-    const uint32_t n = load_count(&A.cnt->n_cont);
+    const uint32_t n = load_count(STD ? &A.cnt->n_cont_std : &A.cnt->n_cont);
     FL_WARP_UNIFORM_LOOP(q, n) {
         const bool active = q < n;
         bool alive = false;
         uint32_t slot = 0;
         if (active) {
-            slot = A.q_cont[q];
+            slot = A.q_cont[STD ? A.cap - 1 - q : q];
             const JobDev &J = A.jobs[A.job[slot]];
             const int4 h = A.hit[slot];
             const uint32_t fl = A.flags[slot];
@@ -760,11 +787,11 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             const Hit hr = make_hit(J, o4, d4, h);
             const float lambda0 = A.lambda0[slot];
             Bsdf<NL> b;
-            make_bsdf<NL>(J, A.tab, sm, hr, lambda0, b);
+            make_bsdf<NL, STD>(J, A.tab, sm, hr, lambda0, b);
             Spec<NL> beta, L;
             load_spec<NL>(A.beta, A.cap, slot, beta);
             load_spec<NL>(A.L, A.cap, slot, L);
-            if (bsdf_num_components(b, kBsdfAll & ~kBsdfSpecular) > 0) {
+            if (bsdf_num_components<STD>(b, kBsdfAll & ~kBsdfSpecular) > 0) {
                 // uniform_sample_all_lights: sum of the per-light estimate_direct results
                 Spec<NL> Ls;
                 Ls.set(0.f);
@@ -815,11 +842,11 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             const float ux = rng.nextf(), uy = rng.nextf();
             if (GUIDE && u_sel < c_sel) {
                 wi = guide_mixture_sample(gm, u_sel / c_sel, ux, uy);
-                bsdf_eval<NL>(b, wo, wi, kBsdfAll, f);
-                pdf = bsdf_pdf<NL>(b, wo, wi, kBsdfAll);
+                bsdf_eval<STD>(b, wo, wi, kBsdfAll, f);
+                pdf = bsdf_pdf<STD>(b, wo, wi, kBsdfAll);
                 sflags = kBsdfDiffuse | kBsdfReflection;
             } else {
-                bsdf_sample<NL>(b, wo, wi, ux, uy, pdf, kBsdfAll, sflags, f);
+                bsdf_sample<STD>(b, wo, wi, ux, uy, pdf, kBsdfAll, sflags, f);
             }
             if (GUIDE && c_sel > 0.f && !(f.black() || pdf == 0))
                 pdf = c_sel * guide_mixture_pdf(gm, wi) + (1.f - c_sel) * pdf;
@@ -989,8 +1016,10 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
 // Enqueues one wave (camera rays of the samples in *W.d_wave, then max_depth + 1 bounces)
 // on `st`. Launch shapes do not depend on the wave's content, so the sequence can be
 // captured once into a CUDA graph and replayed for every wave.
+// `standard`: the wave may hold StandardSurface materials, shaded by their own kernel instances.
 template <int NL, bool GUIDE = false>
-void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile *prof, int sms, cudaStream_t st) {
+void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile *prof, int sms, cudaStream_t st,
+                  bool standard) {
     RenderArgs A = W.A;
     A.q_trace = W.qa;
     A.q_next = W.qb;
@@ -1009,6 +1038,7 @@ void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile
         prof->mark(0, st);
         prof->mark(1, st);
         k_shade<NL><<<g_shade, 128, 0, st>>>(A);
+        if (standard) k_shade<NL, true><<<g_shade, 128, 0, st>>>(A);
         prof->mark(1, st);
         prof->mark(2, st);
         if (count) k_trace_rays2<true><<<g_trace, 128, 0, st>>>(A);
@@ -1022,8 +1052,9 @@ void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile
             }
         }
         k_continue<NL, GUIDE><<<g_shade, 128, 0, st>>>(A);
+        if (standard) k_continue<NL, GUIDE, true><<<g_shade, 128, 0, st>>>(A);
         prof->mark(3, st);
-        prof->launches += 4;
+        prof->launches += standard ? 6 : 4;
     }
 }
 
@@ -1039,6 +1070,8 @@ inline JobDev job_of(const Scene *s, const CamDev &cam, const fl_render_params &
     j.tri_light = s->tri_light;
     j.materials = s->materials;
     j.mat_refl60 = s->mat_refl60;
+    j.standard = s->standard;
+    j.std_refl60 = s->std_refl60;
     j.lights = s->lights;
     j.n_lights = (int)s->n_lights;
     j.any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
@@ -1076,6 +1109,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_jobs, &j, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(W.A.cnt, 0, sizeof(WaveCounters), st));
     const bool count = (p.flags & FL_RENDER_COUNT) != 0;
+    const bool standard = s->n_standard > 0;
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
     const size_t desc_bytes = offsetof(WaveDesc, seg) + sizeof(WaveSeg);
     // Replay one captured graph per wave: a depth-16 wave is ~85 launches, and its late
@@ -1083,7 +1117,8 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     // path (instantiating a graph allocates) nor when every launch is timed with events.
     const bool use_graph = !fixed_scratch && !prof->on;
     if (use_graph && (!ctx->wave_graph || ctx->graph_base != W.A.cnt || ctx->graph_cap != W.cap ||
-                      ctx->graph_depth != p.max_depth || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count)) {
+                      ctx->graph_depth != p.max_depth || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count ||
+                      ctx->graph_std != (int)standard)) {
         if (ctx->wave_graph) {
             cudaGraphExecDestroy(ctx->wave_graph);
             ctx->wave_graph = nullptr;
@@ -1091,7 +1126,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         cudaGraph_t g = nullptr;
         RenderProfile off;
         FL_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        enqueue_wave<NL>(W, p.max_depth, count, &off, sms, st);
+        enqueue_wave<NL>(W, p.max_depth, count, &off, sms, st, standard);
         FL_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
         cudaError_t e = cudaGraphInstantiate(&ctx->wave_graph, g, 0);
         cudaGraphDestroy(g);
@@ -1104,6 +1139,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         ctx->graph_depth = p.max_depth;
         ctx->graph_nl_mode = NL;
         ctx->graph_count = (int)count;
+        ctx->graph_std = (int)standard;
     }
     for (unsigned long long wb = 0; wb < total; wb += W.cap) {
         WaveDesc d;
@@ -1114,9 +1150,9 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
         if (use_graph) {
             FL_CUDA_TRY(ctx, cudaGraphLaunch(ctx->wave_graph, st));
-            prof->launches += 1 + 5 * (uint32_t)p.max_depth + 4;
+            prof->launches += 1 + (standard ? 7 : 5) * (uint32_t)p.max_depth + (standard ? 6 : 4);
         } else {
-            enqueue_wave<NL>(W, p.max_depth, count, prof, sms, st);
+            enqueue_wave<NL>(W, p.max_depth, count, prof, sms, st, standard);
         }
         FL_CUDA_TRY(ctx, cudaGetLastError());
     }

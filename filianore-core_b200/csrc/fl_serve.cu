@@ -303,7 +303,8 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     cudaGraph_t g = nullptr;
     e = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        enqueue_wave<4>(S->W, cfg->max_depth, false, &prof, ctx->sm_count > 0 ? ctx->sm_count : 148, S->stream);
+        // the server's waves may carry any scene: include the StandardSurface kernels
+        enqueue_wave<4>(S->W, cfg->max_depth, false, &prof, ctx->sm_count > 0 ? ctx->sm_count : 148, S->stream, true);
         e = cudaStreamEndCapture(S->stream, &g);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&S->graph, g, 0);

@@ -11,6 +11,12 @@
 //   FresnelSpecularBXDF         src/filianore/shading/closures/fresnelspecular.cpp:18-53
 //   FresnelDielectric           src/filianore/shading/fresnel/fresneldielectric.cpp:8-38 (no state)
 //   FresnelConductor            src/filianore/shading/fresnel/fresnelconductor.cpp:9-33
+//   StandardSurfaceMaterial     src/filianore/shading/materials/standardsurface.cpp:72-159, with
+//     OrenNayarBRDF               src/filianore/shading/bxdfs/orennayar.cpp:6-62
+//     FresnelBlendedDiffuseSpec.  src/filianore/shading/closures/fresnelblendeddiffspec.cpp:18-67
+//     Schlick dielectric/metallic src/filianore/shading/fresnel/schlick{dielectric,metallic}.cpp
+//     EstevezSheenDistribution    src/filianore/shading/microfacets/estevez.cpp:8-42
+//     ClearcoatReflectionBRDF     src/filianore/shading/bxdfs/clearcoat.cpp:6-80
 //   DiffuseAreaIlluminant       src/filianore/illuminants/diffusearea.cpp:12-39
 //   Shape::sample / Shape::pdf  src/filianore/shapes/shape.cpp:13-41
 //   Triangle::intersect/sample  src/filianore/shapes/triangle.cpp:13-154
@@ -32,6 +38,16 @@ static __device__ inline float fl_cos(float x) { return (float)cos((double)x); }
 #else
 static __device__ inline float fl_sin(float x) { return sinf(x); }
 static __device__ inline float fl_cos(float x) { return cosf(x); }
+#endif
+// pow/exp/log of the StandardSurface lobes, rounded once from double in the parity build
+#if defined(FL_PARITY_MATH)
+static __device__ inline float fl_pow(float x, float y) { return (float)pow((double)x, (double)y); }
+static __device__ inline float fl_exp(float x) { return (float)exp((double)x); }
+static __device__ inline float fl_log(float x) { return (float)log((double)x); }
+#else
+static __device__ inline float fl_pow(float x, float y) { return powf(x, y); }
+static __device__ inline float fl_exp(float x) { return expf(x); }
+static __device__ inline float fl_log(float x) { return logf(x); }
 #endif
 
 enum : int {
@@ -100,15 +116,19 @@ __device__ inline float hero_lambda(float lambda0, int k) {
     return l >= 720.f ? l - 340.f : l;
 }
 
-__device__ inline float basis_at(const SmemTables &sm, const TablesArg &t, int b, float l) {
-    const float x = (l - t.rgb_lambda0) / (t.rgb_lambda1 - t.rgb_lambda0) * (float)(t.n_rgb - 1);
-    const float *v = sm.bases + b * 64;
+// RGB basis b at wavelength l, linear in the staged table (bases: 14 rows of 64)
+__device__ inline float basis_value(const float *bases, float l0, float l1, int n, int b, float l) {
+    const float x = (l - l0) / (l1 - l0) * (float)(n - 1);
+    const float *v = bases + b * 64;
     if (x <= 0.f) return v[0];
-    if (x >= (float)(t.n_rgb - 1)) return v[t.n_rgb - 1];
+    if (x >= (float)(n - 1)) return v[n - 1];
     int j = (int)x;
-    if (j > t.n_rgb - 2) j = t.n_rgb - 2;
+    if (j > n - 2) j = n - 2;
     const float f = x - (float)j;
     return v[j] * (1.f - f) + v[j + 1] * f;
+}
+__device__ inline float basis_at(const SmemTables &sm, const TablesArg &t, int b, float l) {
+    return basis_value(sm.bases, t.rgb_lambda0, t.rgb_lambda1, t.n_rgb, b, l);
 }
 
 __device__ inline float cie_at(const SmemTables &sm, const TablesArg &t, int row, float l) {
@@ -121,7 +141,15 @@ __device__ inline float cie_at(const SmemTables &sm, const TablesArg &t, int row
     return v[j] * (1.f - f) + v[j + 1] * f;
 }
 
-// from_reflectance_rgb at the path's spectral samples (color/spectrumoperations.cpp:113-147)
+// from_reflectance_rgb at a hero wavelength from its Smits terms (color/spectrumoperations.cpp:113-147)
+__device__ inline float smits_at(const SmemTables &sm, const TablesArg &t, const int basis[3], const float w[3], float l) {
+    float r = 0.f;
+    for (int k = 0; k < 3; ++k) r += basis_at(sm, t, basis[k], l) * w[k];
+    r *= 0.94f;
+    return r < 0.f ? 0.f : r;
+}
+
+// from_reflectance_rgb at the path's spectral samples
 template <int NL>
 __device__ inline void reflectance(const SmemTables &sm, const TablesArg &t, const MaterialDev &m,
                                    const float *__restrict__ refl60, float lambda0, Spec<NL> &out) {
@@ -130,13 +158,7 @@ __device__ inline void reflectance(const SmemTables &sm, const TablesArg &t, con
         for (int i = 0; i < NL; ++i) out.c[i] = __ldg(refl60 + i);
     } else {
 #pragma unroll
-        for (int i = 0; i < NL; ++i) {
-            const float l = hero_lambda(lambda0, i);
-            float r = 0.f;
-            for (int k = 0; k < 3; ++k) r += basis_at(sm, t, m.basis[k], l) * m.w[k];
-            r *= 0.94f;
-            out.c[i] = r < 0.f ? 0.f : r;
-        }
+        for (int i = 0; i < NL; ++i) out.c[i] = smits_at(sm, t, m.basis, m.w, hero_lambda(lambda0, i));
     }
 }
 
@@ -179,7 +201,28 @@ struct Bsdf {
     float mat_eta, mat_k;
     Spec<NL> R;
     int corrected;  // FL_RENDER_CORRECTED_GGX: VNDF density and sampling on wo's side
+    // FL_MAT_STANDARD: the material record; its colours kd, ks, kt, sheen, coat (in this
+    // order) come from the 60-bin table in global memory, or are upsampled at the hero
+    // wavelengths when a lobe needs them, from the bases staged in shared memory
+    const StandardDev *sd;
+    const float *std60;
+    const float *bases;
+    float rgb_l0, rgb_l1;
+    int n_rgb;
+    float lambda0;
 };
+
+enum : int { kStdKd = 0, kStdKs = 1, kStdKt = 2, kStdSheen = 3, kStdCoat = 4 };
+template <int NL>
+__device__ inline float std_color(const Bsdf<NL> &b, int c, int i) {
+    if (NL == 60) return __ldg(b.std60 + 60 * c + i);
+    // from_reflectance_rgb at hero wavelength i (color/spectrumoperations.cpp:113-147)
+    const float l = hero_lambda(b.lambda0, i);
+    float r = 0.f;
+    for (int k = 0; k < 3; ++k) r += basis_value(b.bases, b.rgb_l0, b.rgb_l1, b.n_rgb, b.sd->basis[c][k], l) * b.sd->w[c][k];
+    r *= 0.94f;
+    return r < 0.f ? 0.f : r;
+}
 
 __device__ inline v3 to_local(v3 s, v3 t, v3 n, v3 v) { return mk(dot(v, s), dot(v, t), dot(v, n)); }
 __device__ inline v3 to_world(v3 s, v3 t, v3 n, v3 v) { return add(add(mul(s, v.x), mul(t, v.y)), mul(n, v.z)); }
@@ -292,26 +335,270 @@ __device__ inline float fr_conductor(float cosI, float etaT, float k) {
     return 0.5f * (Rp + Rs);
 }
 
-// lobes: 0 Lambert, 1 microfacet reflection, 2 microfacet transmission, 3 Fresnel specular
+// lobes: 0 Lambert, 1 microfacet reflection, 2 microfacet transmission, 3 Fresnel specular,
+// and the StandardSurface lobes 4 Oren-Nayar, 5 Fresnel-blended diffuse + specular,
+// 6 Estevez sheen, 7 GTR1 clear coat, 8 Fresnel specular with R = ks, T = kt
+constexpr int kMaxLobes = 4;
+// The BSDF routines are compiled twice: STD = false for the Lambert, GGX and glass
+// materials (lobes 0..3), STD = true for the StandardSurface (lobes 4..8), which the
+// shading kernels' StandardSurface instances call. Kept apart, the StandardSurface code
+// adds no calls, registers or branches to the other materials' kernels.
+template <bool STD>
 __device__ inline int lobe_type(int lobe) {
-    return lobe == 0 ? (kBsdfReflection | kBsdfDiffuse)
-                     : lobe == 1 ? (kBsdfReflection | kBsdfGlossy)
-                                 : lobe == 2 ? (kBsdfTransmission | kBsdfGlossy)
-                                             : (kBsdfReflection | kBsdfTransmission | kBsdfSpecular);
+    if (!STD)
+        return lobe == 0 ? (kBsdfReflection | kBsdfDiffuse)
+                         : lobe == 1 ? (kBsdfReflection | kBsdfGlossy)
+                                     : lobe == 2 ? (kBsdfTransmission | kBsdfGlossy)
+                                                 : (kBsdfReflection | kBsdfTransmission | kBsdfSpecular);
+    return lobe == 4 ? (kBsdfReflection | kBsdfDiffuse)
+                     : lobe == 8 ? (kBsdfReflection | kBsdfTransmission | kBsdfSpecular)
+                                 : (kBsdfReflection | kBsdfGlossy);
 }
-__device__ inline int mat_lobes(int type, int *lobes) {
-    switch (type) {
+template <bool STD, int NL>
+__device__ inline int mat_lobes(const Bsdf<NL> &b, int *lobes) {
+    if (STD) {
+#pragma unroll
+        for (int i = 0; i < kMaxLobes; ++i) lobes[i] = b.sd->lobes[i];
+        return b.sd->n_lobes;
+    }
+    switch (b.type) {
     case FL_MAT_LAMBERT: lobes[0] = 0; return 1;
     case FL_MAT_CONDUCTOR: lobes[0] = 1; return 1;
     case FL_MAT_ROUGH_DIELECTRIC: lobes[0] = 1; lobes[1] = 2; return 2;
     default: lobes[0] = 3; return 1;
     }
 }
+
+// ---- StandardSurface lobe helpers
+// OrenNayarBRDF::OrenNayarBRDF / evaluate (bxdfs/orennayar.cpp:6-39); A, B precomputed per material
+template <int NL>
+__device__ inline void oren_nayar_eval(const Bsdf<NL> &b, float A, float B, v3 wo, v3 wi, Spec<NL> &out) {
+    const float sinThetaI = sint(wi), sinThetaO = sint(wo);
+    float maxCos = 0.f;
+    if (sinThetaI > 1e-4 && sinThetaO > 1e-4) {
+        const float sinPhiI = sinphi(wi), cosPhiI = cosphi(wi), sinPhiO = sinphi(wo), cosPhiO = cosphi(wo);
+        const float dCos = cosPhiI * cosPhiO + sinPhiI * sinPhiO;
+        maxCos = dCos > 0.f ? dCos : 0.f;
+    }
+    float sinAlpha, tanBeta;
+    if (fabsf(wi.z) > fabsf(wo.z)) { sinAlpha = sinThetaO; tanBeta = sinThetaI / fabsf(wi.z); }
+    else { sinAlpha = sinThetaI; tanBeta = sinThetaO / fabsf(wo.z); }
+    const float v = (A + B * maxCos * sinAlpha * tanBeta);
+    const float weight = b.sd->kd_weight;
+#pragma unroll
+    for (int i = 0; i < NL; ++i) out.c[i] = std_color(b, kStdKd, i) * kInvPi * v * weight;
+}
+// cosine_hemisphere_sample over concentric_sample_disk (core/shadingcore.h:65-89), on wo's side
+__device__ inline v3 cos_hemi(v3 wo, float ux, float uy) {
+    const float ox = ux * 2.f - 1.f, oy = uy * 2.f - 1.f;
+    float dx, dy;
+    if (ox == 0 && oy == 0) { dx = 0.f; dy = 0.f; }
+    else {
+        float theta, r;
+        if (fabsf(ox) > fabsf(oy)) { r = ox; theta = kPiOver4 * (oy / ox); }
+        else { r = oy; theta = kPiOver2 - kPiOver4 * (ox / oy); }
+        dx = r * fl_cos(theta);
+        dy = r * fl_sin(theta);
+    }
+    const float zz = 1.f - dx * dx - dy * dy;
+    v3 wi = mk(dx, dy, sqrtf(zz > 0.f ? zz : 0.f));
+    if (wo.z < 0) wi.z *= -1.f;
+    return wi;
+}
+__device__ inline v3 reflect_wh(v3 wo, v3 wh) { return sub(mul(mul(wh, 2.f), dot(wo, wh)), wo); }
+// EstevezSheenDistribution D and Lambda (microfacets/estevez.cpp:11-34)
+__device__ inline float est_D(float r, v3 wh) {
+    const float inv = 1.f / r;
+    return (2.f + inv) * fl_pow(sint(wh), inv) / (2.f * kPi);
+}
+__device__ inline float est_plerp(float r, float p0, float p1) {
+    return ((1.f - r) * (1.f - r)) * p0 + (1.f - ((1.f - r) * (1.f - r))) * p1;
+}
+__device__ inline float est_lambda(float r, v3 w) {
+    const float a = est_plerp(r, 25.3245f, 21.5473f), b = est_plerp(r, 3.32435f, 3.82987f);
+    const float c = est_plerp(r, 0.16801f, 0.19823f), d = est_plerp(r, -1.27393f, -1.97760f);
+    const float e = est_plerp(r, -4.85967f, -4.32054f);
+    auto L = [&](float v) { return a / (1.f + b * fl_pow(v, c)) + (d * v) + e; };
+    const float ac = fabsf(w.z);
+    if (ac < 0.5f) return fl_exp(L(ac));
+    return fl_exp(2.f * L(0.5f) - L(1.f - ac));
+}
+// ClearcoatReflectionBRDF's GTR1 and Smith G (bxdfs/clearcoat.cpp:8-19). The reference's
+// smithG_GGX calls the unqualified sqrt, the double-precision C function, so the parity
+// build carries that sum and division in double.
+__device__ inline float gtr1(float cosTheta, float alpha) {
+    const float alpha2 = alpha * alpha;
+    return (alpha2 - 1) / (kPi * fl_log(alpha2) * (1 + (alpha2 - 1) * cosTheta * cosTheta));
+}
+__device__ inline float smith_g_ggx(float cosTheta, float alpha) {
+    const float alpha2 = alpha * alpha, cosTheta2 = cosTheta * cosTheta;
+#if defined(FL_PARITY_MATH)
+    return (float)(1.f / ((double)cosTheta + sqrt((double)(alpha2 + cosTheta2 - alpha2 * cosTheta2))));
+#else
+    return 1.f / (cosTheta + sqrtf(alpha2 + cosTheta2 - alpha2 * cosTheta2));
+#endif
+}
 __device__ inline bool matches(int type, int flags) { return (type & flags) == type; }
 
-// lobe evaluate into out (reference multiplication order)
+// StandardSurface lobes 4..7, out of line: they are the rarely run part of the shading
+// kernels, and kept apart their registers do not weigh on the Lambert and GGX code.
 template <int NL>
+__device__ __noinline__ void std_lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec<NL> &out) {
+    if (lobe == 4) { oren_nayar_eval(b, b.sd->on_A, b.sd->on_B, wo, wi, out); return; }
+    if (lobe == 5) {
+        // FresnelBlendedDiffuseSpecularBRDF::evaluate (closures/fresnelblendeddiffspec.cpp:18-38)
+        const StandardDev &sd = *b.sd;
+        const float r1 = 1.f - .5f * fabsf(wi.z);
+        const float r1pow5 = (r1 * r1) * (r1 * r1) * r1;
+        const float r2 = 1.f - .5f * fabsf(wo.z);
+        const float r2pow5 = (r2 * r2) * (r2 * r2) * r2;
+        v3 wh = add(wi, wo);
+        if (wh.x == 0 && wh.y == 0 && wh.z == 0) { out.set(0.f); return; }
+        oren_nayar_eval(b, sd.fb_A, sd.fb_B, wo, wi, out);
+        wh = normalize(wh);
+        const float cF = dot(wi, wh);
+        const float D = ggx_D(b, wh);
+        const float den = (4.f * absdot(wi, wh) * fmaxf(fabsf(wi.z), fabsf(wo.z)));
+        const float R1 = 1.f - cF;
+        const float ro = sd.ro, ksw = sd.ks_weight;
+        const bool metallic = sd.fresnel_type == FL_FRESNEL_METALLIC;
+        const float r1p5 = metallic ? (R1 * R1 * R1 * R1 * R1) : ((R1 * R1) * (R1 * R1) * R1);
+#pragma unroll
+        for (int i = 0; i < NL; ++i) {
+            const float diffuse = (28.f / 23.f) * out.c[i] * (1.f - ro) * (1 - r1pow5) * (1 - r2pow5);
+            const float ks = std_color(b, kStdKs, i);
+            // SchlickMetallic (r0 = ks, fresnel/schlickmetallic.cpp:7-10) or SchlickDielectric
+            // (fresnel/schlickdielectric.cpp:7-11)
+            const float F = metallic ? ks + (1.f - ks) * r1p5 : ro + r1p5 * (1.f - ro);
+            float specular = D * F / den;
+            specular = ks * specular * ksw;
+            out.c[i] = diffuse + specular;
+        }
+        return;
+    }
+    if (lobe == 6) {
+        // MicrofacetReflectionBRDF::evaluate with the Estevez distribution and FresnelNull
+        const float cosThetaO = fabsf(wo.z), cosThetaI = fabsf(wi.z);
+        v3 wh = add(wi, wo);
+        if (cosThetaI == 0 || cosThetaO == 0 || (wh.x == 0 && wh.y == 0 && wh.z == 0)) { out.set(0.f); return; }
+        wh = normalize(wh);
+        const float r = b.sd->sheen_rough, w = b.sd->sheen_weight;
+        const float D = est_D(r, wh);
+        const float G = 1.f / (1.f + est_lambda(r, wo) + est_lambda(r, wi));
+        const float den = 4.f * cosThetaO * cosThetaI;
+#pragma unroll
+        for (int i = 0; i < NL; ++i) out.c[i] = std_color(b, kStdSheen, i) * w * D * G * 1.f / den;
+        return;
+    }
+    if (lobe == 7) {
+        // ClearcoatReflectionBRDF::evaluate (bxdfs/clearcoat.cpp:28-41)
+        v3 wh = add(wi, wo);
+        if (wh.x == 0 && wh.y == 0 && wh.z == 0) { out.set(0.f); return; }
+        wh = normalize(wh);
+        const float Dr = gtr1(fabsf(wh.z), b.sd->coat_gloss);
+        const float Fr = fr_dielectric(dot(wo, wh), 1.f, b.sd->coat_ior);
+        const float Gr = smith_g_ggx(fabsf(wo.z), .25f) * smith_g_ggx(fabsf(wi.z), .25f);
+        const float w = b.sd->coat_weight;
+#pragma unroll
+        for (int i = 0; i < NL; ++i) out.c[i] = std_color(b, kStdCoat, i) * Fr * w * Gr * Dr / 4;
+        return;
+    }
+    out.set(0.f);
+}
+
+template <int NL>
+__device__ __noinline__ float std_lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi) {
+    if (lobe == 4) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.f;
+    if (lobe == 5) {
+        // closures/fresnelblendeddiffspec.cpp:61-67
+        if (!same_hemi(wo, wi)) return 0.f;
+        const v3 wh = normalize(add(wo, wi));
+        const float pdf_wh = ggx_pdf(b, wo, wh);
+        return .5f * (fabsf(wi.z) * kInvPi + pdf_wh / (4 * dot(wo, wh)));
+    }
+    if (lobe == 6) {
+        // MicrofacetReflectionBRDF::pdf with MicrofacetDistribution::pdf = D |cos theta_h|
+        if (!same_hemi(wo, wi)) return 0.f;
+        const v3 wh = normalize(add(wo, wi));
+        return est_D(b.sd->sheen_rough, wh) * fabsf(wh.z) / (4.f * dot(wo, wh));
+    }
+    if (lobe == 7) {
+        // bxdfs/clearcoat.cpp:70-80
+        if (!same_hemi(wo, wi)) return 0.f;
+        v3 wh = add(wi, wo);
+        if (wh.x == 0 && wh.y == 0 && wh.z == 0) return 0.f;
+        wh = normalize(wh);
+        const float Dr = gtr1(fabsf(wh.z), b.sd->coat_gloss);
+        return Dr * fabsf(wh.z) / (4 * dot(wo, wh));
+    }
+    return 0.f;
+}
+
+template <int NL>
+__device__ __noinline__ void std_lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, float ux, float uy, float &pdf,
+                                             Spec<NL> &f) {
+    if (lobe == 4) {
+        // OrenNayarBRDF::sample (bxdfs/orennayar.cpp:41-56): a cosine-weighted direction on wo's side
+        wi = cos_hemi(wo, ux, uy);
+        pdf = std_lobe_pdf(b, 4, wo, wi);
+        std_lobe_eval(b, 4, wo, wi, f);
+        return;
+    }
+    if (lobe == 5) {
+        // FresnelBlendedDiffuseSpecularBRDF::sample (closures/fresnelblendeddiffspec.cpp:40-59)
+        if (ux < .5) {
+            float u0 = 2 * ux;
+            if (u0 > 1.f - kShadowEpsilon) u0 = 1.f - kShadowEpsilon;
+            wi = cos_hemi(wo, u0, uy);
+        } else {
+            float u0 = 2 * (ux - .5f);
+            if (u0 > 1.f - kShadowEpsilon) u0 = 1.f - kShadowEpsilon;
+            wi = reflect_wh(wo, ggx_sample_wh(b, wo, u0, uy));
+            if (!same_hemi(wo, wi)) { f.set(0.f); return; }
+        }
+        pdf = std_lobe_pdf(b, 5, wo, wi);
+        std_lobe_eval(b, 5, wo, wi, f);
+        return;
+    }
+    if (lobe == 6) {
+        // MicrofacetReflectionBRDF::sample (bxdfs/microfacetreflection.cpp:30-52); the Estevez
+        // sample_wh is a cosine-weighted normal on wo's side (microfacets/estevez.cpp:36-42)
+        if (wo.z == 0) { f.set(0.f); return; }
+        const v3 wh = cos_hemi(wo, ux, uy);
+        if (dot(wo, wh) < 0) { f.set(0.f); return; }
+        wi = reflect_wh(wo, wh);
+        if (!same_hemi(wo, wi)) { f.set(0.f); return; }
+        pdf = est_D(b.sd->sheen_rough, wh) * fabsf(wh.z) / (4.f * dot(wo, wh));
+        std_lobe_eval(b, 6, wo, wi, f);
+        return;
+    }
+    if (lobe == 7) {
+        // ClearcoatReflectionBRDF::sample (bxdfs/clearcoat.cpp:43-68)
+        if (wo.z == 0) { f.set(0.f); return; }
+        const float g = b.sd->coat_gloss;
+        const float alpha2 = g * g;
+        const float cosTheta = sqrtf(fmaxf(0.f, (1 - fl_pow(alpha2, 1 - ux)) / (1 - alpha2)));
+        const float sinTheta = sqrtf(fmaxf(0.f, 1 - cosTheta * cosTheta));
+        const float phi = 2 * kPi * uy;
+        v3 wh = mk(sinTheta * fl_cos(phi), sinTheta * fl_sin(phi), cosTheta);
+        if (!same_hemi(wo, wh)) wh = neg(wh);
+        wi = reflect_wh(wo, wh);
+        if (!same_hemi(wo, wi)) { f.set(0.f); return; }
+        pdf = std_lobe_pdf(b, 7, wo, wi);
+        std_lobe_eval(b, 7, wo, wi, f);
+        return;
+    }
+    f.set(0.f);
+}
+
+// lobe evaluate into out (reference multiplication order)
+template <bool STD, int NL>
 __device__ inline void lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec<NL> &out) {
+    if (STD) {
+        if (lobe >= 4 && lobe <= 7) std_lobe_eval(b, lobe, wo, wi, out);
+        else out.set(0.f);
+        return;
+    }
     if (lobe == 0) {
 #pragma unroll
         for (int i = 0; i < NL; ++i) out.c[i] = b.R.c[i] * kInvPi * 1.f;
@@ -351,8 +638,9 @@ __device__ inline void lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec
     out.set(0.f);
 }
 
-template <int NL>
+template <bool STD, int NL>
 __device__ inline float lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi) {
+    if (STD) return (lobe >= 4 && lobe <= 7) ? std_lobe_pdf(b, lobe, wo, wi) : 0.f;
     if (lobe == 0) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.f;
     if (lobe == 1) {
         if (!same_hemi(wo, wi)) return 0.f;
@@ -371,25 +659,14 @@ __device__ inline float lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi) {
     return 0.f;
 }
 
-template <int NL>
+template <bool STD, int NL>
 __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, float ux, float uy, float &pdf,
                                    int &type, Spec<NL> &f) {
     if (lobe == 0) {
-        const float ox = ux * 2.f - 1.f, oy = uy * 2.f - 1.f;
-        float dx, dy;
-        if (ox == 0 && oy == 0) { dx = 0.f; dy = 0.f; }
-        else {
-            float theta, r;
-            if (fabsf(ox) > fabsf(oy)) { r = ox; theta = kPiOver4 * (oy / ox); }
-            else { r = oy; theta = kPiOver2 - kPiOver4 * (ox / oy); }
-            dx = r * fl_cos(theta);
-            dy = r * fl_sin(theta);
-        }
-        const float zz = 1.f - dx * dx - dy * dy;
-        wi = mk(dx, dy, sqrtf(zz > 0.f ? zz : 0.f));
-        if (wo.z < 0) wi.z *= -1.f;
-        pdf = lobe_pdf(b, 0, wo, wi);
-        lobe_eval(b, 0, wo, wi, f);
+        // LambertBRDF::sample: a cosine-weighted direction on wo's side
+        wi = cos_hemi(wo, ux, uy);
+        pdf = lobe_pdf<false>(b, 0, wo, wi);
+        lobe_eval<false>(b, 0, wo, wi, f);
         return;
     }
     if (lobe == 1) {
@@ -399,7 +676,7 @@ __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, f
         wi = sub(mul(mul(wh, 2.f), dot(wo, wh)), wo);
         if (!same_hemi(wo, wi)) { f.set(0.f); return; }
         pdf = ggx_pdf(b, wo, wh) / (4.f * dot(wo, wh));
-        lobe_eval(b, 1, wo, wi, f);
+        lobe_eval<false>(b, 1, wo, wi, f);
         return;
     }
     if (lobe == 2) {
@@ -414,10 +691,12 @@ __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, f
         if (sinT2 >= 1) { f.set(0.f); return; }
         const float cosT = sqrtf(1 - sinT2);
         wi = add(mul(wo, -eta), mul(wh, (eta * cosI - cosT)));
-        pdf = lobe_pdf(b, 2, wo, wi);
-        lobe_eval(b, 2, wo, wi, f);
+        pdf = lobe_pdf<false>(b, 2, wo, wi);
+        lobe_eval<false>(b, 2, wo, wi, f);
         return;
     }
+    if (STD && lobe >= 4 && lobe <= 7) { std_lobe_sample(b, lobe, wo, wi, ux, uy, pdf, f); return; }
+    // FresnelSpecularBXDF: lobe 3 with R = T = the material colour, lobe 8 with R = ks, T = kt
     const float F = fr_dielectric(wo.z, 1.f, b.mat_eta);
     if (ux < F) {
         wi = mk(-wo.x, -wo.y, wo.z);
@@ -425,7 +704,7 @@ __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, f
         pdf = F;
         const float ac = fabsf(wi.z);
 #pragma unroll
-        for (int i = 0; i < NL; ++i) f.c[i] = b.R.c[i] * F / ac;
+        for (int i = 0; i < NL; ++i) f.c[i] = (STD ? std_color(b, kStdKs, i) : b.R.c[i]) * F / ac;
     } else {
         const bool entering = wo.z > 0;
         const float etaI = entering ? 1.f : b.mat_eta;
@@ -445,92 +724,92 @@ __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, f
         const float ac = fabsf(wi.z);
 #pragma unroll
         for (int i = 0; i < NL; ++i) {
-            float ft = b.R.c[i] * (1.f - F);
+            float ft = (STD ? std_color(b, kStdKt, i) : b.R.c[i]) * (1.f - F);
             ft *= sc;
             f.c[i] = ft / ac;
         }
     }
 }
 
-template <int NL>
+template <bool STD, int NL>
 __device__ inline int bsdf_num_components(const Bsdf<NL> &b, int flags) {
-    int lobes[2];
-    const int n = mat_lobes(b.type, lobes);
+    int lobes[kMaxLobes];
+    const int n = mat_lobes<STD>(b, lobes);
     int c = 0;
-    for (int i = 0; i < n; ++i) c += matches(lobe_type(lobes[i]), flags) ? 1 : 0;
+    for (int i = 0; i < n; ++i) c += matches(lobe_type<STD>(lobes[i]), flags) ? 1 : 0;
     return c;
 }
 
-template <int NL>
+template <bool STD, int NL>
 __device__ __noinline__ void bsdf_eval(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags, Spec<NL> &out) {
     const v3 wi = to_local(b.s, b.t, b.ns, wiW), wo = to_local(b.s, b.t, b.ns, woW);
     out.set(0.f);
     if (wo.z == 0) return;
     const bool reflect = dot(wiW, b.ng) * dot(woW, b.ng) > 0;
-    int lobes[2];
-    const int n = mat_lobes(b.type, lobes);
+    int lobes[kMaxLobes];
+    const int n = mat_lobes<STD>(b, lobes);
     for (int i = 0; i < n; ++i) {
-        const int ty = lobe_type(lobes[i]);
+        const int ty = lobe_type<STD>(lobes[i]);
         if (matches(ty, flags) && ((reflect && (ty & kBsdfReflection)) || (!reflect && (ty & kBsdfTransmission)))) {
             Spec<NL> f;
-            lobe_eval(b, lobes[i], wo, wi, f);
+            lobe_eval<STD>(b, lobes[i], wo, wi, f);
 #pragma unroll
             for (int k = 0; k < NL; ++k) out.c[k] += f.c[k];
         }
     }
 }
 
-template <int NL>
+template <bool STD, int NL>
 __device__ __noinline__ float bsdf_pdf(const Bsdf<NL> &b, v3 woW, v3 wiW, int flags) {
-    int lobes[2];
-    const int n = mat_lobes(b.type, lobes);
+    int lobes[kMaxLobes];
+    const int n = mat_lobes<STD>(b, lobes);
     const v3 wi = to_local(b.s, b.t, b.ns, wiW), wo = to_local(b.s, b.t, b.ns, woW);
     if (wo.z == 0) return 0.f;
     float pdf = 0.f;
     int mc = 0;
     for (int i = 0; i < n; ++i)
-        if (matches(lobe_type(lobes[i]), flags)) { ++mc; pdf += lobe_pdf(b, lobes[i], wo, wi); }
+        if (matches(lobe_type<STD>(lobes[i]), flags)) { ++mc; pdf += lobe_pdf<STD>(b, lobes[i], wo, wi); }
     return mc > 0 ? pdf / (float)mc : 0.f;
 }
 
-template <int NL>
+template <bool STD, int NL>
 __device__ __noinline__ void bsdf_sample(const Bsdf<NL> &b, v3 woW, v3 &wiW, float ux, float uy, float &pdf, int flags,
                                    int &sampledType, Spec<NL> &f) {
-    int lobes[2];
-    const int n = mat_lobes(b.type, lobes);
+    int lobes[kMaxLobes];
+    const int n = mat_lobes<STD>(b, lobes);
     int mc = 0;
-    for (int i = 0; i < n; ++i) mc += matches(lobe_type(lobes[i]), flags) ? 1 : 0;
+    for (int i = 0; i < n; ++i) mc += matches(lobe_type<STD>(lobes[i]), flags) ? 1 : 0;
     f.set(0.f);
     if (mc == 0) { pdf = 0.f; sampledType = 0; return; }
     int comp = (int)floorf(ux * mc);
     if (comp > mc - 1) comp = mc - 1;
     int chosen = lobes[0], count = comp;
     for (int i = 0; i < n; ++i)
-        if (matches(lobe_type(lobes[i]), flags) && count-- == 0) { chosen = lobes[i]; break; }
+        if (matches(lobe_type<STD>(lobes[i]), flags) && count-- == 0) { chosen = lobes[i]; break; }
     float urx = ux * mc - comp;
     if (urx > 1.f - kShadowEpsilon) urx = 1.f - kShadowEpsilon;
     v3 wi = mk(0.f, 0.f, 0.f);
     const v3 wo = to_local(b.s, b.t, b.ns, woW);
     if (wo.z == 0) return;
     pdf = 0.f;
-    const int ctype = lobe_type(chosen);
+    const int ctype = lobe_type<STD>(chosen);
     sampledType = ctype;
-    lobe_sample(b, chosen, wo, wi, urx, uy, pdf, sampledType, f);
+    lobe_sample<STD>(b, chosen, wo, wi, urx, uy, pdf, sampledType, f);
     if (pdf == 0) { sampledType = 0; f.set(0.f); return; }
     wiW = to_world(b.s, b.t, b.ns, wi);
     if (!(ctype & kBsdfSpecular) && mc > 1) {
         for (int i = 0; i < n; ++i)
-            if (lobes[i] != chosen && matches(lobe_type(lobes[i]), flags)) pdf += lobe_pdf(b, lobes[i], wo, wi);
+            if (lobes[i] != chosen && matches(lobe_type<STD>(lobes[i]), flags)) pdf += lobe_pdf<STD>(b, lobes[i], wo, wi);
     }
     if (mc > 1) pdf /= mc;
     if (!(ctype & kBsdfSpecular)) {
         const bool reflect = dot(wiW, b.ng) * dot(woW, b.ng) > 0;
         f.set(0.f);
         for (int i = 0; i < n; ++i) {
-            const int ty = lobe_type(lobes[i]);
+            const int ty = lobe_type<STD>(lobes[i]);
             if (matches(ty, flags) && ((reflect && (ty & kBsdfReflection)) || (!reflect && (ty & kBsdfTransmission)))) {
                 Spec<NL> g;
-                lobe_eval(b, lobes[i], wo, wi, g);
+                lobe_eval<STD>(b, lobes[i], wo, wi, g);
 #pragma unroll
                 for (int k = 0; k < NL; ++k) f.c[k] += g.c[k];
             }

@@ -150,3 +150,48 @@ def test_delta_lights_match_reference_integrator(ctx, variant):
     close = np.all(np.abs(xyz - ref) <= np.maximum(1e-4 * np.abs(ref), 1e-6), axis=-1).mean()
     assert close >= 0.99, close
     assert abs(xyz.mean() / ref.mean() - 1) < 2e-3
+
+
+@pytest.mark.parametrize("variant", ["standard", "standard2"])
+def test_standard_surface_matches_reference_material(ctx, variant):
+    """StandardSurfaceMaterial boxes (Oren-Nayar, Fresnel-blended anisotropic GGX with Schlick
+    dielectric and metallic Fresnel, Estevez sheen, GTR1 clear coat, specular R/T glass),
+    60-bin parity build, against the reference's own material (fixture made by the reference
+    build). The near-specular glass chain amplifies last-ulp differences, so the bound is 99%
+    of pixels within 1e-4 relative (or 1e-6 absolute) and the image mean within 2e-3."""
+    g = np.load(os.path.join(GOLDEN, "cornell_standard_ref.npz"))
+    ref = g[f"{variant}_xyz"]
+    sc = scenes.cornell(64, 64, variant)
+    xyz, _, stats = render_xyz(ctx, sc, scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60))
+    assert stats["paths"] == 64 * 64 * 4 and stats["traversal_errors"] == 0
+    assert close_fraction(xyz, ref, 1e-4, 1e-6) >= 0.99
+    assert abs(xyz.mean() / ref.mean() - 1) < 2e-3
+
+
+@pytest.mark.parametrize("variant", ["standard", "standard2"])
+def test_standard_surface_hero_matches_oracle(ctx, orc_tables, variant):
+    """The same boxes in the hero-wavelength build (FMA contraction, single-precision pow,
+    exp, log) against the oracle's hero mode: >= 99% of pixels within 1e-3 relative and the
+    image mean within 2e-3."""
+    sc = scenes.cornell(64, 64, variant)
+    p = scenes.render_params(8, 8, fb.FL_SPECTRAL_HERO4)
+    xyz, _, stats = render_xyz(ctx, sc, p)
+    cpu, cnt = oracle.render(sc, orc_tables, p)
+    assert stats["paths"] == cnt["paths"]
+    assert close_fraction(xyz, cpu, 1e-3, 1e-5) >= 0.99
+    assert abs(xyz.mean() / cpu.mean() - 1) < 2e-3
+
+
+@pytest.mark.parametrize("bad", [{"thin_film_thickness": 400.0}, {"thin_walled": 1}, {"fresnel_type": 2},
+                                 {"fresnel_type": -1}])
+def test_standard_surface_rejects_unsupported_parts(ctx, bad):
+    """Thin-film interference, thin-walled transmission and the measured-metal Fresnel are
+    refused by fl_scene_create with FL_ERR_INVALID and a message, never rendered wrongly."""
+    sc = scenes.cornell(8, 8, "standard")
+    mats = [dict(m) for m in sc.materials]
+    mats[-1] = {"standard": dict(mats[-1]["standard"], **bad)}
+    bad_scene = scenes.Scene(sc.verts, sc.tri_material, mats, sc.lights, sc.camera)
+    with pytest.raises(fb.FlError) as e:
+        ctx.scene(bad_scene)
+    assert e.value.status == fb.FL_ERR_INVALID
+    assert "standard surface" in str(e.value)
