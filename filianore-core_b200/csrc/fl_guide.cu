@@ -290,6 +290,9 @@ __global__ void k_guide_stats(const float *rec, const uint32_t *rec_count, uint3
 struct AdamArgs {
     float *w32, *m, *v, *grad;
     __half *w16;
+    float *wavg;       // weight average (null: off), its decay and bias correction
+    __half *w16avg;
+    float beta, bc_avg;
     const uint32_t *rec_count;
     uint32_t rec_cap, batch_begin, batch_size;
     const float *wstat;
@@ -315,6 +318,11 @@ __global__ void k_guide_adam(AdamArgs a) {
         w = fminf(fmaxf(w, -60000.f), 60000.f);
         a.w32[i] = w;
         a.w16[i] = __float2half_rn(w);
+        if (a.wavg) {
+            const float e = a.beta * a.wavg[i] + (1.f - a.beta) * w;
+            a.wavg[i] = e;
+            a.w16avg[i] = __float2half_rn(e / a.bc_avg);
+        }
     }
     a.grad[i] = 0.f;
 }
@@ -356,6 +364,12 @@ struct Guide {
     void *mem = nullptr;  // weights, Adam state, gradient, statistics
     __half *w16 = nullptr;
     float *w32 = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr, *wstat = nullptr, *loss = nullptr;
+    // rendering weights: w16, or with weight_average > 0 the FP16 copy of the bias-corrected
+    // moving average wavg of the Adam iterates (avg_steps of them since the last upload)
+    float *wavg = nullptr;
+    __half *w16avg = nullptr;
+    int64_t avg_steps = 0;
+    const __half *render_weights() const { return cfg.weight_average > 0.f ? w16avg : w16; }
     uint32_t *rec_count = nullptr;
     float *rec = nullptr;
     float *mix = nullptr;
@@ -388,6 +402,10 @@ static fl_status guide_upload_weights(Guide *G, const std::vector<float> &w) {
     for (int i = 0; i < kGuideParams; ++i) h[i] = __float2half_rn(w[i]);
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(G->w32, w.data(), sizeof(float) * kGuideParams, cudaMemcpyHostToDevice, ctx->stream));
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(G->w16, h.data(), sizeof(__half) * kGuideParams, cudaMemcpyHostToDevice, ctx->stream));
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(G->w16avg, h.data(), sizeof(__half) * kGuideParams, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    FL_CUDA_TRY(ctx, cudaMemsetAsync(G->wavg, 0, sizeof(float) * kGuideParams, ctx->stream));
+    G->avg_steps = 0;
     FL_CUDA_TRY(ctx, cudaMemsetAsync(G->m, 0, sizeof(float) * kGuideParams, ctx->stream));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(G->v, 0, sizeof(float) * kGuideParams, ctx->stream));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(G->grad, 0, sizeof(float) * kGuideParams, ctx->stream));
@@ -464,6 +482,13 @@ static fl_status guide_train(Guide *G, uint32_t n, const float bmin[3], const fl
         a.bc1 = 1.f - powf(0.9f, (float)G->steps);
         a.bc2 = 1.f - powf(0.999f, (float)G->steps);
         a.resampled = 1;
+        if (G->cfg.weight_average > 0.f) {
+            G->avg_steps += 1;
+            a.wavg = G->wavg;
+            a.w16avg = G->w16avg;
+            a.beta = G->cfg.weight_average;
+            a.bc_avg = 1.f - powf(a.beta, (float)G->avg_steps);
+        }
         k_guide_adam<<<(kGuideParams + 255) / 256, 256, 0, st>>>(a);
     }
     FL_CUDA_TRY(ctx, cudaGetLastError());
@@ -489,7 +514,7 @@ static fl_status guide_pass(Guide *G, Scene *s, const CamDev &cam, const fl_rend
     bounds_of(s->bmin, s->bmax, binv);
     for (int a = 0; a < 3; ++a) binv[a] *= G->cfg.position_scale;
     GuideArgs &ga = W.A.g;
-    ga.w = G->w16;
+    ga.w = G->render_weights();
     ga.mix = G->mix;
     ga.rec_idx = train ? G->rec_idx : nullptr;
     ga.rec = G->rec;
@@ -603,7 +628,8 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     const fl_guide_config c = *cfg;
     if (!(c.learning_rate > 0.f) || !(c.select_prob >= 0.f && c.select_prob < 1.f) || c.batch < 128 ||
         c.batch > 65536 || c.batch % 128 != 0 || c.max_records < c.batch || c.max_records > (1 << 26) ||
-        c.steps_per_wave < 1 || !(c.position_scale >= 0.f && c.position_scale <= 1.f)) {
+        c.steps_per_wave < 1 || !(c.position_scale >= 0.f && c.position_scale <= 1.f) ||
+        !(c.weight_average >= 0.f && c.weight_average < 1.f)) {
         set_error(ctx, "invalid guide configuration");
         return FL_ERR_INVALID;
     }
@@ -618,7 +644,7 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     G->cfg = c;
     if (G->cfg.position_scale == 0.f) G->cfg.position_scale = 1.f;
     const size_t P = align_up(kGuideParams * sizeof(float));
-    const size_t bytes = align_up(kGuideParams * sizeof(__half)) + 4 * P + 256 + 256 + 256;
+    const size_t bytes = 2 * align_up(kGuideParams * sizeof(__half)) + 5 * P + 256 + 256 + 256;
     auto fail = [&](cudaError_t e, const char *what) {
         cudaFree(G->mem);
         cudaFree(G->rec);
@@ -653,6 +679,8 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     G->wstat = reinterpret_cast<float *>(B + 4 * P);
     G->loss = reinterpret_cast<float *>(B + 4 * P + 256);
     G->rec_count = reinterpret_cast<uint32_t *>(B + 4 * P + 512);
+    G->wavg = reinterpret_cast<float *>(B + 4 * P + 768);
+    G->w16avg = reinterpret_cast<__half *>(B + 5 * P + 768);
     e = cudaMemsetAsync(G->rec_count, 0, sizeof(uint32_t), ctx->stream);
     if (e) return fail(e, "guide counter");
     std::vector<float> w;

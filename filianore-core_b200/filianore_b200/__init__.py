@@ -272,10 +272,11 @@ class Guide:
 
     def __init__(self, ctx: Context, seed: int = 1, learning_rate: float = 1e-2, select_prob: float = 0.5,
                  batch: int = 16384, max_records: int = 1 << 20, steps_per_wave: int = 16,
-                 position_scale: float = 1.0 / 16):
+                 position_scale: float = 1.0 / 16, weight_average: float = 0.99):
         self.ctx = ctx
         self.h = None
-        cfg = T.fl_guide_config(seed, learning_rate, select_prob, batch, max_records, steps_per_wave, position_scale)
+        cfg = T.fl_guide_config(seed, learning_rate, select_prob, batch, max_records, steps_per_wave, position_scale,
+                                weight_average)
         h = C.c_void_p()
         check(lib().fl_guide_create(ctx.h, C.byref(cfg), C.byref(h)), ctx.h)
         self.h = h

@@ -205,7 +205,8 @@ class fl_guide_config(C.Structure):
         ("max_records", C.c_int32),
         ("steps_per_wave", C.c_int32),
         ("position_scale", C.c_float),
-        ("reserved", C.c_int32 * 2),
+        ("weight_average", C.c_float),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -391,7 +391,10 @@ typedef struct {
     int32_t steps_per_wave;  /* most Adam steps after one wave, >= 1 */
     float position_scale;    /* positions enter the encoding as scale * (p - bmin) / (bmax - bmin), in (0, 1];
                                 0 means 1. Smaller values shift the 12 bands to coarser frequencies */
-    int32_t reserved[2];
+    float weight_average;    /* beta in [0, 1): rendering samples from the exponential moving average
+                                (decay beta per Adam step, bias-corrected) of the weights Adam
+                                produces; 0 renders with Adam's current weights */
+    int32_t reserved;
 } fl_guide_config;
 
 enum {

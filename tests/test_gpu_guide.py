@@ -89,33 +89,48 @@ def test_untrained_guide_is_unbiased(ctx):
 
 def test_trained_guide_lowers_caustic_error(ctx):
     """Caustic scene (glass sphere under a tiny, bright sphere light), 256 x 256: after online
-    training, the guided render's mean squared error against a 4096-spp plain render is
-    below 0.8 x the plain render's at the same 64 samples per pixel. Both errors are
-    averaged over six independent renders: single renders are dominated by a few caustic
-    fireflies."""
+    training (48 passes of 4 spp, rendering with the weight average), the guided render's
+    mean squared error against a 4096-spp plain render is below the plain render's at the
+    same 64 samples per pixel: below 0.92 x over the image and 0.85 x in the caustic (the
+    brightest 3% of the reference). Errors are averaged over six renders per estimator, and
+    the guided one over two independently trained guides: training order varies from run to
+    run (atomics), and single guides measured 0.72-0.87 x over the image."""
     R = 256
     sc = scenes.caustic(R, R, slices=128, stacks=65)
     s = ctx.scene(sc)
     ref = np.zeros((R, R, 3), np.float64)
     s.render(scenes.render_params(4096, 8, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20), film_xyz64=ref)
     ref /= 4096
+    caustic = ref[..., 1] >= np.quantile(ref[..., 1], 0.97)
 
     def mean_mse(render):
-        errs = []
+        full, region = [], []
         for k in range(6):
             img = np.zeros((R, R, 3), np.float64)
             render(img, 7000 + 64 * k)
-            errs.append(np.mean((img / 64 - ref) ** 2))
-        return float(np.mean(errs))
+            d = (img / 64 - ref) ** 2
+            full.append(d.mean())
+            region.append(d[caustic].mean())
+        return np.array([np.mean(full), np.mean(region)])
     e_plain = mean_mse(lambda f, off: s.render(scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4, sample_offset=off),
                                                film_xyz64=f))
-    g = fb.Guide(ctx, seed=5, select_prob=0.5, batch=16384, max_records=1 << 19, steps_per_wave=32)
-    for k in range(48):
-        flags = fb.FL_GUIDE_TRAIN | (fb.FL_GUIDE_SAMPLE if k > 0 else 0)
-        g.render(s, scenes.render_params(4, 8, fb.FL_SPECTRAL_HERO4, sample_offset=(1 << 16) + 4 * k), flags)
-    assert g.info()["adam_steps"] > 0
-    e_guided = mean_mse(lambda f, off: g.render(s, scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4, sample_offset=off),
-                                                fb.FL_GUIDE_SAMPLE, film_xyz64=f))
-    assert e_guided < 0.8 * e_plain, (e_guided, e_plain)
-    g.close()
+    e_guided = []
+    for seed in (5, 6):
+        g = fb.Guide(ctx, seed=seed, select_prob=0.5, batch=16384, max_records=1 << 19, steps_per_wave=32,
+                     weight_average=0.99)
+        for k in range(48):
+            flags = fb.FL_GUIDE_TRAIN | (fb.FL_GUIDE_SAMPLE if k > 0 else 0)
+            g.render(s, scenes.render_params(4, 8, fb.FL_SPECTRAL_HERO4, sample_offset=(1 << 16) + 4 * k), flags)
+        assert g.info()["adam_steps"] > 0
+        e_guided.append(mean_mse(lambda f, off: g.render(
+            s, scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4, sample_offset=off), fb.FL_GUIDE_SAMPLE, film_xyz64=f)))
+        g.close()
+    ratio = np.mean(e_guided, axis=0) / e_plain
+    assert ratio[0] < 0.92 and ratio[1] < 0.85, (ratio, e_guided, e_plain)
     s.close()
+
+
+def test_guide_config_is_validated(ctx):
+    for bad in ({"weight_average": 1.0}, {"weight_average": -0.1}, {"batch": 100}, {"select_prob": 1.0}):
+        with pytest.raises(fb.FlError):
+            fb.Guide(ctx, **bad)
