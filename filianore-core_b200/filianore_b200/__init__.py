@@ -20,6 +20,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.environ.get("FILIANORE_B200_LIB", os.path.join(PKG_DIR, "lib", "libfilianore_b200.so"))
 ROOT = os.path.dirname(PKG_DIR)
 TABLES_PATH = os.path.join(ROOT, "tests", "golden", "spectral_tables.npz")
+METALS_PATH = os.path.join(ROOT, "tests", "golden", "metal_tables.npz")
 
 EXPORTED = [
     "fl_context_create", "fl_context_destroy", "fl_status_string", "fl_last_error", "fl_context_binned_tables",
@@ -101,9 +102,18 @@ def check(status, ctx=None):
         raise FlError(status, f"{lib().fl_status_string(status).decode()}: {buf.value.decode()}")
 
 
-def reference_tables(path: str = TABLES_PATH) -> dict:
-    """The reference's spectral data (color/cie.h) as stored by tests/golden/make_golden.py."""
-    return dict(np.load(path))
+def reference_tables(path: str = TABLES_PATH, measured_metals: bool = False) -> dict:
+    """The reference's spectral data (color/cie.h) as stored by tests/golden/make_golden.py.
+    measured_metals adds the metal eta / k curves of color/metallurgy.h ("metal_lambda_m",
+    "metal_eta_m", "metal_k_m" for the nine metals). Without them the measured-metal Fresnel
+    sees eta = k = 0, as the reference does (it never calls InitializeForge)."""
+    t = dict(np.load(path))
+    if measured_metals:
+        m = np.load(METALS_PATH)
+        for i in range(9):
+            for key in ("lambda", "eta", "k"):
+                t[f"metal_{key}_{i}"] = m[f"{key}_{i}"]
+    return t
 
 
 def _tables_struct(t: dict):
@@ -120,7 +130,8 @@ def _tables_struct(t: dict):
     for b in range(7):
         s.refl[b] = fp(refl[b])
         s.illum[b] = fp(illum[b])
-    return s, (keep, refl, illum)
+    metals = T.set_metal_tables(s, t, fp)
+    return s, (keep, refl, illum, metals)
 
 
 # Handles still open at interpreter exit are closed children first (guides and servers,

@@ -121,8 +121,10 @@ def _quad(p0, p1, p2, p3):
     return [list(p0) + list(p1) + list(p2), list(p0) + list(p2) + list(p3)]
 
 
-def _box(cx, cz, sx, sy, sz, angle_deg):
-    """axis box of size (sx, sy, sz) standing on y = 0, centred at (cx, cz), rotated about y."""
+def _box(cx, cz, sx, sy, sz, angle_deg, outward=False):
+    """axis box of size (sx, sy, sz) standing on y = 0, centred at (cx, cz), rotated about y.
+    The faces' geometric normals (Triangle::intersect's cross(v1 - v3, v2 - v3)) point into
+    the box; outward=True reverses the winding so that they point out."""
     a = math.radians(angle_deg)
     ca, sa = math.cos(a), math.sin(a)
 
@@ -138,14 +140,14 @@ def _box(cx, cz, sx, sy, sz, angle_deg):
     faces = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (2, 3, 7, 6), (1, 2, 6, 5), (3, 0, 4, 7)]
     tris = []
     for f in faces:
-        tris += _quad(*(c[i] for i in f))
+        tris += _quad(*(c[i] for i in (f[::-1] if outward else f)))
     return tris
 
 
 def cornell(width=256, height=256, variant="lambert") -> Scene:
     """Cornell-style box of 36 triangles (unit-cube room open at z = 0, two rotated boxes,
     0.25 x 0.25 ceiling light at y = 0.999 facing down with constant spectral radiance 10).
-    variant "lambert": every surface Lambertian; "standard" / "standard2": the boxes are
+    variant "lambert": every surface Lambertian; "standard" / "standard2" / "standard3": the boxes are
     StandardSurface materials (see below); "materials": short box GGX conductor
     (roughness 0.3, eta 0.2, k 3.9), tall box rough dielectric (roughness 0.25, IOR 1.5);
     "glass": short box conductor (roughness 0.05), tall box smooth glass (IOR 1.5)."""
@@ -160,8 +162,11 @@ def cornell(width=256, height=256, variant="lambert") -> Scene:
     tris += _quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)); mats += [RED] * 2
     tris += _quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)); mats += [GREEN] * 2
     # short box (front, image right), tall box (back, image left)
-    tris += _box(0.66, 0.37, 0.3, 0.3, 0.3, -17.0); mats += [SHORT] * 12
-    tris += _box(0.33, 0.67, 0.3, 0.6, 0.3, 17.0); mats += [TALL] * 12
+    # ("standard3": outward normals, so that the thin film and the thin walls see their
+    # outside from the room)
+    out = variant == "standard3"
+    tris += _box(0.66, 0.37, 0.3, 0.3, 0.3, -17.0, out); mats += [SHORT] * 12
+    tris += _box(0.33, 0.67, 0.3, 0.6, 0.3, 17.0, out); mats += [TALL] * 12
     # light quad, normal (0, -1, 0)
     h, lo, hi = 0.999, 0.375, 0.625
     light_first = len(tris)
@@ -195,6 +200,18 @@ def cornell(width=256, height=256, variant="lambert") -> Scene:
                       {"standard": {"ks": (1.0, 1.0, 1.0), "ks_weight": 1.0, "ks_ior": 1.5, "ks_roughness": 0.2,
                                     "kt": (0.9, 0.95, 1.0), "kt_weight": 1.0, "sheen_color": (1.0, 0.8, 0.8),
                                     "sheen_weight": 0.3, "sheen_roughness": 0.5}}]
+    elif variant == "standard3":
+        # StandardSurface: thin-walled diffuse transmission with sheen; measured copper (Oren-Nayar
+        # diffuse, anisotropic GGX conductor) under a thin film and a clear coat
+        materials += [{"standard": {"kd": (0.3, 0.7, 0.4), "kd_weight": 1.0, "kd_roughness": 0.6, "thin_walled": 1,
+                                    "sheen_color": (0.8, 0.8, 1.0), "sheen_weight": 0.5, "sheen_roughness": 0.3}},
+                      {"standard": {"kd": (0.5, 0.5, 0.5), "kd_weight": 0.4, "kd_roughness": 0.5,
+                                    "ks": (1.0, 1.0, 1.0), "ks_weight": 0.9, "ks_roughness": 0.3,
+                                    "ks_anisotropic": 0.2, "ks_ior": 1.8,
+                                    "fresnel_type": T.FL_FRESNEL_MEASURED_METAL, "metal_type": 1,
+                                    "thin_film_thickness": 350.0, "thin_film_ior": 1.33,
+                                    "coat_color": (1.0, 1.0, 1.0), "coat_weight": 0.3, "coat_ior": 1.5,
+                                    "coat_gloss": 0.8}}]
     lights = [{"type": T.FL_LIGHT_TRIANGLE, "tri": light_first + k, "radiance": 10.0} for k in range(2)]
     cam = {"position": (0.5, 0.5, -1.4), "look_at": (0.5, 0.5, 0.0), "up": (0.0, 1.0, 0.0), "vfov": 40.0,
            "width": width, "height": height}

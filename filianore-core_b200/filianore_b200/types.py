@@ -1,6 +1,8 @@
 """ctypes mirrors of the structs in include/filianore_gpu.h (the C ABI)."""
 import ctypes as C
 
+import numpy as np
+
 FL_OK = 0
 FL_ERR_INVALID = -1
 FL_ERR_OOM = -2
@@ -35,6 +37,8 @@ FL_RENDER_CORRECTED_GGX = 4
 FL_MAT_STANDARD = 4
 FL_FRESNEL_DIELECTRIC = 0
 FL_FRESNEL_METALLIC = 1
+FL_FRESNEL_MEASURED_METAL = 2
+METALS = ("gold", "copper", "silver", "aluminium", "beryllium", "chromium", "mercury", "iridium", "lithium")
 
 FL_SERVE_SHORTEST_FIRST = 0
 FL_SERVE_FIRST_COME = 1
@@ -55,6 +59,11 @@ class fl_spectral_tables(C.Structure):
         ("n_rgb2spec", C.c_int32),
         ("refl", C.POINTER(C.c_float) * 7),
         ("illum", C.POINTER(C.c_float) * 7),
+        ("n_metals", C.c_int32),
+        ("metal_n", C.c_int32 * 9),
+        ("metal_lambda", C.POINTER(C.c_float) * 9),
+        ("metal_eta", C.POINTER(C.c_float) * 9),
+        ("metal_k", C.POINTER(C.c_float) * 9),
     ]
 
 
@@ -86,7 +95,7 @@ class fl_standard_surface(C.Structure):
     _fields_ = [
         ("kd", C.c_float * 3), ("kd_weight", C.c_float), ("kd_roughness", C.c_float),
         ("ks", C.c_float * 3), ("ks_weight", C.c_float), ("ks_roughness", C.c_float), ("ks_anisotropic", C.c_float),
-        ("ks_ior", C.c_float), ("fresnel_type", C.c_int32),
+        ("ks_ior", C.c_float), ("fresnel_type", C.c_int32), ("metal_type", C.c_int32),
         ("kt", C.c_float * 3), ("kt_weight", C.c_float),
         ("sheen_color", C.c_float * 3), ("sheen_weight", C.c_float), ("sheen_roughness", C.c_float),
         ("coat_color", C.c_float * 3), ("coat_weight", C.c_float), ("coat_ior", C.c_float), ("coat_gloss", C.c_float),
@@ -215,3 +224,18 @@ FL_GUIDE_TRAIN = 2
 FL_GUIDE_PARAMS = 19968
 FL_GUIDE_RECORD_FLOATS = 20
 
+
+def set_metal_tables(s, t: dict, fp):
+    """fills the metal fields of an fl_spectral_tables from a tables dict; returns the arrays
+    the struct points to (keep them alive)"""
+    if "metal_lambda_0" not in t:
+        s.n_metals = 0
+        return []
+    keep = []
+    s.n_metals = 9
+    for i in range(9):
+        arrs = [np.ascontiguousarray(t[f"metal_{key}_{i}"], np.float32) for key in ("lambda", "eta", "k")]
+        keep += arrs
+        s.metal_n[i] = arrs[0].shape[0]
+        s.metal_lambda[i], s.metal_eta[i], s.metal_k[i] = (fp(a) for a in arrs)
+    return keep

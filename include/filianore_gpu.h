@@ -82,6 +82,17 @@ typedef struct {
     int32_t n_rgb2spec;      /* 32 in the reference */
     const float *refl[7];
     const float *illum[7];
+    /* Measured metal eta / k curves as the reference holds them in color/metallurgy.h
+     * (Gold_Lambda, Gold_Eta, Gold_K, Gold_nSamples, ...), in GetMetalCoefficientsFromForge's
+     * order: gold, copper, silver, aluminium, beryllium, chromium, mercury, iridium, lithium.
+     * The library bins them as InitializeForge does (color/metallurgy.cpp:7-39). n_metals = 0
+     * leaves every metal at eta = k = 0, which is what the reference renders: nothing in it
+     * calls InitializeForge, so its metal spectra stay zero (a conductor Fresnel of 1). */
+    int32_t n_metals;        /* 0 or 9 */
+    int32_t metal_n[9];
+    const float *metal_lambda[9];
+    const float *metal_eta[9];
+    const float *metal_k[9];
 } fl_spectral_tables;
 
 /* ------------------------------------------------------------------------- */
@@ -116,27 +127,36 @@ enum {
 };
 
 enum {
-    FL_FRESNEL_DIELECTRIC = 0,   /* FresnelType::Dielectric: Schlick with r0 from the specular IOR */
-    FL_FRESNEL_METALLIC = 1      /* FresnelType::Metallic: Schlick with r0 = the specular colour */
+    FL_FRESNEL_DIELECTRIC = 0,      /* FresnelType::Dielectric: Schlick with r0 from the specular IOR */
+    FL_FRESNEL_METALLIC = 1,        /* FresnelType::Metallic: Schlick with r0 = the specular colour */
+    FL_FRESNEL_MEASURED_METAL = 2   /* FresnelType::WavelengthDependentMetallic: FresnelConductor with
+                                       the measured eta / k of metal_type (fl_spectral_tables) */
 };
 
 /* The StandardSurfaceMaterial's parameters with constant textures. Colours are upsampled
- * with from_reflectance_rgb. The lobes follow compute_scattering_functions: Oren-Nayar
- * diffuse (sigma = 90 * kd_roughness) when there is no specular weight; otherwise a Fresnel-
- * blended diffuse + GGX specular lobe (or, with kt_weight > 0, FresnelSpecular with R = ks,
- * T = kt); then an Estevez sheen lobe and a GTR1 clear coat when their weights are > 0.
- * Not supported (fl_scene_create rejects them): thin-film interference, the measured-metal
- * Fresnel (FresnelType::WavelengthDependentMetallic), thin-walled diffuse transmission and
- * bump maps. */
+ * with from_reflectance_rgb. The lobes follow compute_scattering_functions, in its order:
+ *   - Oren-Nayar diffuse (sigma = 90 kd_roughness) when kd_weight > 0 and either ks_weight
+ *     <= 0 or the measured-metal Fresnel; thin_walled turns it into diffuse transmission
+ *     (DiffuseTransmission: the same Oren-Nayar lobe, sampled on the far side);
+ *   - with ks_weight > 0: FresnelSpecular with R = ks, T = kt when kt_weight > 0; else GGX
+ *     (alphas from ks_roughness and ks_anisotropic) with the measured-metal conductor
+ *     Fresnel, or the Fresnel-blended diffuse + specular lobe (Schlick dielectric/metallic);
+ *   - with thin_film_thickness > 0: GGX with the thin-film interference Fresnel
+ *     (ThinFilmInteference(thin_film_ior, thickness in nm, ks_ior));
+ *   - an Estevez sheen lobe and a GTR1 clear coat when their weights are > 0.
+ * Not supported: bump maps. */
 typedef struct {
     float kd[3], kd_weight, kd_roughness;
     float ks[3], ks_weight, ks_roughness, ks_anisotropic, ks_ior;
-    int32_t fresnel_type;        /* FL_FRESNEL_* */
+    int32_t fresnel_type;        /* FL_FRESNEL_* (other values are rejected) */
+    int32_t metal_type;          /* FL_FRESNEL_MEASURED_METAL: 0 gold, 1 copper, 2 silver, 3 aluminium,
+                                    4 beryllium, 5 chromium, 6 mercury, 7 iridium, 8 lithium; other
+                                    values gold, as GetMetalCoefficientsFromForge does */
     float kt[3], kt_weight;
     float sheen_color[3], sheen_weight, sheen_roughness;
     float coat_color[3], coat_weight, coat_ior, coat_gloss;
-    float thin_film_thickness, thin_film_ior;  /* thickness must be 0 */
-    int32_t thin_walled;                       /* must be 0 */
+    float thin_film_thickness, thin_film_ior;
+    int32_t thin_walled;
 } fl_standard_surface;
 
 typedef struct {

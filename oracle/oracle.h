@@ -64,6 +64,9 @@ typedef struct {
     /* 60-bin tables built as InitializeSpectrals does (color/spectruminits.cpp:6-64) */
     float X[ORC_NBINS], Y[ORC_NBINS], Z[ORC_NBINS];
     float brefl[7][ORC_NBINS], billum[7][ORC_NBINS];
+    /* measured metals binned as InitializeForge does (color/metallurgy.cpp:7-39): eta, k;
+     * zero without metal curves (the reference never calls InitializeForge) */
+    float metal[9][2][ORC_NBINS];
 } orc_tables;
 
 int orc_tables_init(orc_tables *t, const fl_spectral_tables *src);
@@ -71,6 +74,8 @@ int orc_tables_init(orc_tables *t, const fl_spectral_tables *src);
 float orc_average_spectrum_samples(const float *lambda, const float *vals, int n, float l0, float l1);
 /* 17*60 floats: X, Y, Z, refl[7], illum[7] */
 void orc_tables_binned(const orc_tables *t, float *out);
+/* the binned metal spectra: 9 metals x (eta, k) x 60 */
+void orc_tables_metals(const orc_tables *t, float *out);
 
 /* ---------------------------------------------------------------- render */
 typedef struct {

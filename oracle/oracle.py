@@ -130,6 +130,11 @@ class Tables:
         lib().orc_tables_binned(self.buf, _fp(out))
         return out.reshape(17, 60)
 
+    def metals(self):
+        out = np.zeros(9 * 2 * 60, np.float32)
+        lib().orc_tables_metals(self.buf, _fp(out))
+        return out.reshape(9, 2, 60)
+
     def reflectance(self, rgb, mode=T.FL_SPECTRAL_BINS60, lambdas=None):
         rgb = np.asarray(rgb, np.float32)
         lam = np.asarray(lambdas if lambdas is not None else np.zeros(4), np.float32)
@@ -154,7 +159,8 @@ def spectral_tables_struct(t: dict):
     for b in range(7):
         s.refl[b] = _fp(rows_r[b])
         s.illum[b] = _fp(rows_i[b])
-    return s, (keep, rows_r, rows_i)
+    metals = T.set_metal_tables(s, t, _fp)
+    return s, (keep, rows_r, rows_i, metals)
 
 
 # ----------------------------------------------------------------------------- render
@@ -213,13 +219,32 @@ def write_scene_file(path, scene, params, nthreads=0, pixels=None, width=None, h
         f.write(bytes(stds)[: C.sizeof(T.fl_standard_surface) * n_std])
 
 
-def run_reference(scene_path, out_path, W, H):
-    """runs the compiled reference integrator; returns (film (H, W, 3) float64, info dict)"""
+def run_reference(scene_path, out_path, W, H, forge=False):
+    """runs the compiled reference integrator; returns (film (H, W, 3) float64, info dict).
+    forge: call InitializeForge first (the reference itself never does)."""
     import json
-    r = subprocess.run([REF_BIN, scene_path, out_path], check=True, capture_output=True, text=True)
+    r = subprocess.run([REF_BIN, scene_path, out_path] + (["--forge"] if forge else []), check=True,
+                       capture_output=True, text=True)
     info = json.loads(r.stdout.strip().splitlines()[-1])
     film = np.fromfile(out_path, dtype=np.float64).reshape(H, W, 3)
     return film, info
+
+
+def load_metals_dump(path):
+    """parses `ref_render --metals` output: per metal m (GetMetalCoefficientsFromForge order)
+    lambda_m, eta_m, k_m (the raw curves) and the binned eta60 / k60 (9 x 60)."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    n = np.frombuffer(raw[:36], np.int32).copy()
+    f = np.frombuffer(raw[36:], np.float32)
+    out, o = {"n": n}, 0
+    for m in range(9):
+        for key in ("lambda", "eta", "k"):
+            out[f"{key}_{m}"] = f[o:o + n[m]].copy()
+            o += n[m]
+    binned = f[o:o + 1080].reshape(9, 2, 60)  # per metal: eta, then k
+    out["eta60"] = binned[:, 0].copy()
+    out["k60"] = binned[:, 1].copy()
+    return out
 
 
 def load_tables_dump(path):

@@ -154,8 +154,11 @@ typedef struct {
     int corrected;   /* FL_RENDER_CORRECTED_GGX */
     /* StandardSurfaceMaterial (FL_MAT_STANDARD): the lobes in the order
      * compute_scattering_functions adds them and their parameters */
-    int std_n, std_lobes[4];
+    int std_n, std_lobes[5];
     spec kd, ks, kt, sheen, coat;
+    spec metal_eta, metal_k;         /* measured metal (lobe 9) */
+    float tf_ior, tf_thickness;      /* thin film (lobe 10) over a medium of IOR mat_eta */
+    float wl[NL_MAX];                /* the path's wavelengths (bin starts in the 60-bin mode) */
     float kd_weight, on_A, on_B;     /* OrenNayarBRDF(kd, kdweight, 90 * kdrough) */
     float fb_A, fb_B;                /* the blended lobe's OrenNayarBRDF(kd, kdweight, kdrough) */
     float ks_weight, ro;
@@ -271,14 +274,16 @@ static float fr_conductor(float cosI, float etaT_, float k_) {
 /* lobes: 0 Lambert, 1 GGX microfacet reflection, 2 GGX microfacet transmission,
  * 3 FresnelSpecular (R = T = the material colour), and the StandardSurface lobes
  * 4 Oren-Nayar, 5 Fresnel-blended diffuse + specular, 6 Estevez sheen, 7 GTR1 clear coat,
- * 8 FresnelSpecular with R = ks, T = kt */
+ * 8 FresnelSpecular with R = ks, T = kt, 9 GGX with the measured-metal conductor Fresnel,
+ * 10 GGX with the thin-film Fresnel, 11 diffuse transmission */
 static int lobe_type(int lobe) {
     switch (lobe) {
     case 0: return BSDF_REFLECTION | BSDF_DIFFUSE;
     case 1: return BSDF_REFLECTION | BSDF_GLOSSY;
     case 2: return BSDF_TRANSMISSION | BSDF_GLOSSY;
     case 4: return BSDF_REFLECTION | BSDF_DIFFUSE;
-    case 5: case 6: case 7: return BSDF_REFLECTION | BSDF_GLOSSY;
+    case 5: case 6: case 7: case 9: case 10: return BSDF_REFLECTION | BSDF_GLOSSY;
+    case 11: return BSDF_TRANSMISSION | BSDF_DIFFUSE;
     default: return BSDF_REFLECTION | BSDF_TRANSMISSION | BSDF_SPECULAR;
     }
 }
@@ -362,6 +367,42 @@ static float smith_g_ggx(float cosTheta, float alpha) {
 }
 static int matches(int type, int flags) { return (type & flags) == type; }
 
+/* ThinFilmInteference::evaluate (fresnel/thinfilm.cpp:8-58) with extIOR 1 and the amplitude
+ * coefficients of fresnel/fresnel.h:9-23, at the path's wavelengths. The reference's
+ * sin^2 ratios divide a quotient by itself, so both equal 1 - cos^2 (kept). */
+static void thin_film_fresnel(const bsdf_t *b, float cosThetaI, spec *F) {
+    const float extIOR = 1.f, tfIOR = b->tf_ior, mIOR = b->mat_eta, thickness = b->tf_thickness;
+    float sinSqrd1 = ((extIOR / tfIOR) / (extIOR / tfIOR)) * (1 - cosThetaI * cosThetaI);
+    float sinSqrd2 = ((extIOR / mIOR) / (extIOR / mIOR)) * (1 - cosThetaI * cosThetaI);
+    if ((sinSqrd1 > 1) || (sinSqrd2 > 1)) { sp_set(F, b->nl, 1.f); return; }
+    float cos1 = sqrtf(1 - sinSqrd1);
+    float cos2 = sqrtf(1 - sinSqrd2);
+#define SP_R(n1, n2, ci, ct) (((n1) * (ci) - (n2) * (ct)) / ((n1) * (ci) + (n2) * (ct)))
+#define SP_T(n1, n2, ci, ct) ((2.f * (n1) * (ci)) / ((n1) * (ci) + (n2) * (ct)))
+#define PP_R(n1, n2, ci, ct) (((n2) * (ci) - (n1) * (ct)) / ((n1) * (ct) + (n2) * (ci)))
+#define PP_T(n1, n2, ci, ct) ((2.f * (n1) * (ci)) / ((n1) * (ct) + (n2) * (ci)))
+    float alphaSP = SP_R(tfIOR, extIOR, cos1, cosThetaI) * SP_R(mIOR, tfIOR, cos1, cos2);
+    float alphaPP = PP_R(tfIOR, extIOR, cos1, cosThetaI) * PP_R(mIOR, tfIOR, cos1, cos2);
+    float betaSP = SP_T(extIOR, tfIOR, cosThetaI, cos1) * SP_T(tfIOR, mIOR, cos1, cos2);
+    float betaPP = PP_T(extIOR, tfIOR, cosThetaI, cos1) * PP_T(tfIOR, mIOR, cos1, cos2);
+#undef SP_R
+#undef SP_T
+#undef PP_R
+#undef PP_T
+    float delta10 = tfIOR < extIOR ? ORC_PI : 0.f;
+    float delta12 = tfIOR < mIOR ? ORC_PI : 0.f;
+    float delta = delta10 + delta12;
+    float beamRatio = (mIOR * cos2) / (extIOR * cosThetaI);
+    for (int i = 0; i < b->nl; ++i) {
+        float wavelength = b->wl[i];
+        float phi = (2.f * ORC_PI / wavelength) * (2.f * tfIOR * thickness * cos1) + delta;
+        float cp = cosf(phi);
+        float ts = (betaSP * betaSP) / ((alphaSP * alphaSP) - (2.f * alphaSP * cp) + 1.f);
+        float tp = (betaPP * betaPP) / ((alphaPP * alphaPP) - (2.f * alphaPP * cp) + 1.f);
+        F->c[i] = 1.f - (ts + tp) * 0.5f * beamRatio;
+    }
+}
+
 /* lobe evaluate (spectrum) */
 static void lobe_eval(const bsdf_t *b, int lobe, v3 wo, v3 wi, spec *out) {
     int nl = b->nl;
@@ -443,6 +484,25 @@ static void lobe_eval(const bsdf_t *b, int lobe, v3 wo, v3 wi, spec *out) {
         for (int i = 0; i < nl; ++i) out->c[i] = b->sheen.c[i] * b->sheen_weight * D * G * 1.f / den;
         return;
     }
+    if (lobe == 9 || lobe == 10) {
+        /* MicrofacetReflectionBRDF::evaluate (microfacetreflection.cpp:13-32) with R = 1 and the
+         * measured-metal FresnelConductor (weight ks_weight) or the thin film (weight 1) */
+        float cosThetaO = fabsf(wo.z), cosThetaI = fabsf(wi.z);
+        v3 wh = v3_add(wi, wo);
+        if (cosThetaI == 0 || cosThetaO == 0 || (wh.x == 0 && wh.y == 0 && wh.z == 0)) { sp_set(out, nl, 0.f); return; }
+        wh = v3_norm(wh);
+        v3 whf = v3_dot(wh, v3m(0.f, 0.f, 1.f)) < 0.f ? v3_neg(wh) : wh;
+        float cF = v3_dot(wi, whf);
+        spec F;
+        if (lobe == 9) for (int i = 0; i < nl; ++i) F.c[i] = fr_conductor(cF, b->metal_eta.c[i], b->metal_k.c[i]);
+        else thin_film_fresnel(b, cF, &F);
+        float weight = lobe == 9 ? b->ks_weight : 1.f;
+        float D = ggx_D(b, wh), G = ggx_G(b, wo, wi);
+        float den = 4.f * cosThetaO * cosThetaI;
+        for (int i = 0; i < nl; ++i) out->c[i] = 1.f * weight * D * G * F.c[i] / den;
+        return;
+    }
+    if (lobe == 11) { oren_nayar_eval(&b->kd, b->kd_weight, b->on_A, b->on_B, wo, wi, nl, out); return; }
     if (lobe == 7) {
         /* ClearcoatReflectionBRDF::evaluate (clearcoat.cpp:28-41) */
         v3 wh = v3_add(wi, wo);
@@ -487,6 +547,13 @@ static float lobe_pdf(const bsdf_t *b, int lobe, v3 wo, v3 wi) {
         v3 wh = v3_norm(v3_add(wo, wi));
         return est_D(b->sheen_rough, wh) * fabsf(wh.z) / (4.f * v3_dot(wo, wh));
     }
+    if (lobe == 9 || lobe == 10) {
+        if (!same_hemi(wo, wi)) return 0.f;
+        v3 wh = v3_norm(v3_add(wo, wi));
+        return ggx_pdf(b, wo, wh) / (4.f * v3_dot(wo, wh));
+    }
+    /* DiffuseTransmission::pdf (bxdfs/diffusetransmission.cpp:29-31) */
+    if (lobe == 11) return !same_hemi(wo, wi) ? fabsf(wi.z) * ORC_INV_PI : 0.f;
     if (lobe == 7) {
         /* clearcoat.cpp:70-80 */
         if (!same_hemi(wo, wi)) return 0;
@@ -583,6 +650,26 @@ static void lobe_sample(const bsdf_t *b, int lobe, v3 wo, v3 *wi, float ux, floa
         lobe_eval(b, 6, wo, *wi, f);
         return;
     }
+    if (lobe == 9 || lobe == 10) {
+        /* MicrofacetReflectionBRDF::sample (microfacetreflection.cpp:34-56) */
+        if (wo.z == 0) { sp_set(f, nl, 0.f); return; }
+        v3 wh = ggx_sample_wh(b, wo, ux, uy);
+        if (v3_dot(wo, wh) < 0) { sp_set(f, nl, 0.f); return; }
+        *wi = reflect_wh(wo, wh);
+        if (!same_hemi(wo, *wi)) { sp_set(f, nl, 0.f); return; }
+        *pdf = ggx_pdf(b, wo, wh) / (4.f * v3_dot(wo, wh));
+        lobe_eval(b, lobe, wo, *wi, f);
+        return;
+    }
+    if (lobe == 11) {
+        /* DiffuseTransmission::sample (bxdfs/diffusetransmission.cpp:16-27): a cosine-weighted
+         * direction on the side away from wo */
+        *wi = cos_hemi(v3m(0.f, 0.f, 1.f), ux, uy);
+        if (wo.z > 0) wi->z *= -1.f;
+        *pdf = lobe_pdf(b, 11, wo, *wi);
+        lobe_eval(b, 11, wo, *wi, f);
+        return;
+    }
     if (lobe == 7) {
         /* clearcoat.cpp:43-68 */
         if (wo.z == 0) { sp_set(f, nl, 0.f); return; }
@@ -634,7 +721,7 @@ static void lobe_sample(const bsdf_t *b, int lobe, v3 wo, v3 *wi, float ux, floa
 }
 
 static int bsdf_num_components(const bsdf_t *b, int flags) {
-    int lobes[4], n = bsdf_lobes(b, lobes), c = 0;
+    int lobes[5], n = bsdf_lobes(b, lobes), c = 0;
     for (int i = 0; i < n; ++i) if (matches(lobe_type(lobes[i]), flags)) ++c;
     return c;
 }
@@ -645,7 +732,7 @@ static void bsdf_eval(const bsdf_t *b, v3 woW, v3 wiW, int flags, spec *out) {
     sp_set(out, b->nl, 0.f);
     if (wo.z == 0) return;
     int reflect = v3_dot(wiW, b->ng) * v3_dot(woW, b->ng) > 0;
-    int lobes[4], n = bsdf_lobes(b, lobes);
+    int lobes[5], n = bsdf_lobes(b, lobes);
     for (int i = 0; i < n; ++i) {
         int ty = lobe_type(lobes[i]);
         if (matches(ty, flags) && ((reflect && (ty & BSDF_REFLECTION)) || (!reflect && (ty & BSDF_TRANSMISSION)))) {
@@ -658,7 +745,7 @@ static void bsdf_eval(const bsdf_t *b, v3 woW, v3 wiW, int flags, spec *out) {
 
 /* BSDF::pdf, bsdf.cpp:127-151 */
 static float bsdf_pdf(const bsdf_t *b, v3 woW, v3 wiW, int flags) {
-    int lobes[4], n = bsdf_lobes(b, lobes);
+    int lobes[5], n = bsdf_lobes(b, lobes);
     if (n == 0) return 0.f;
     v3 wi = to_local(b, wiW), wo = to_local(b, woW);
     if (wo.z == 0) return 0.f;
@@ -672,7 +759,7 @@ static float bsdf_pdf(const bsdf_t *b, v3 woW, v3 wiW, int flags) {
 /* BSDF::sample, bsdf.cpp:52-125. Returns 0 when *pdf was left untouched (wo.z == 0). */
 static void bsdf_sample(const bsdf_t *b, v3 woW, v3 *wiW, float ux, float uy, float *pdf, int flags, int *sampledType,
                         spec *f) {
-    int lobes[4], n = bsdf_lobes(b, lobes);
+    int lobes[5], n = bsdf_lobes(b, lobes);
     int mc = 0;
     for (int i = 0; i < n; ++i) if (matches(lobe_type(lobes[i]), flags)) ++mc;
     sp_set(f, b->nl, 0.f);
@@ -737,8 +824,7 @@ static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda
     }
     if (m->type == FL_MAT_STANDARD) {
         /* StandardSurfaceMaterial::compute_scattering_functions (standardsurface.cpp:72-159)
-         * with constant textures; thin film, measured metals and thin walls are rejected
-         * by the GPU's fl_scene_create and never reach here */
+         * with constant textures */
         const fl_standard_surface *p = &S->sc->standard_surfaces[m->standard];
         b->eta = (p->ks_weight > 0 && p->kt_weight > 0) ? p->ks_ior : 1.f;
         b->mat_eta = p->ks_ior;
@@ -762,9 +848,29 @@ static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda
         b->coat_weight = p->coat_weight;
         b->coat_ior = p->coat_ior;
         b->coat_gloss = (1.f - p->coat_gloss) * .1f + p->coat_gloss * .001f;  /* lerp(gloss, .1, .001) */
+        const int measured = p->fresnel_type == FL_FRESNEL_MEASURED_METAL;
+        const int metal = (p->metal_type >= 0 && p->metal_type <= 8) ? p->metal_type : 0;  /* default: gold */
+        for (int i = 0; i < b->nl; ++i) {
+            if (S->mode == FL_SPECTRAL_BINS60) {
+                b->metal_eta.c[i] = S->tab->metal[metal][0][i];
+                b->metal_k.c[i] = S->tab->metal[metal][1][i];
+                b->wl[i] = (float)(400 + 5 * i);
+            } else {
+                /* hero wavelengths read the 5 nm bin they fall in, clamped to 400..700 nm */
+                int bin = (int)floorf((lambda[i] - 400.f) / 5.f);
+                bin = bin < 0 ? 0 : (bin > ORC_NBINS - 1 ? ORC_NBINS - 1 : bin);
+                b->metal_eta.c[i] = S->tab->metal[metal][0][bin];
+                b->metal_k.c[i] = S->tab->metal[metal][1][bin];
+                b->wl[i] = lambda[i];
+            }
+        }
+        b->tf_ior = p->thin_film_ior;
+        b->tf_thickness = p->thin_film_thickness;
         b->std_n = 0;
-        if (p->kd_weight > 0 && p->ks_weight <= 0) b->std_lobes[b->std_n++] = 4;
-        if (p->ks_weight > 0) b->std_lobes[b->std_n++] = p->kt_weight > 0 ? 8 : 5;
+        if ((p->kd_weight > 0 && p->ks_weight <= 0) || (p->kd_weight > 0 && p->ks_weight > 0 && measured))
+            b->std_lobes[b->std_n++] = p->thin_walled ? 11 : 4;
+        if (p->ks_weight > 0) b->std_lobes[b->std_n++] = p->kt_weight > 0 ? 8 : (measured ? 9 : 5);
+        if (p->thin_film_thickness > 0) b->std_lobes[b->std_n++] = 10;
         if (p->sheen_weight > 0) b->std_lobes[b->std_n++] = 6;
         if (p->coat_weight > 0) b->std_lobes[b->std_n++] = 7;
     }

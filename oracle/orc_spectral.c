@@ -83,6 +83,9 @@ float orc_average_spectrum_samples(const float *wl, const float *vals, int n, fl
 
 int orc_tables_init(orc_tables *t, const fl_spectral_tables *s) {
     if (!s || s->n_cie <= 1 || s->n_cie > 512 || s->n_rgb2spec <= 1 || s->n_rgb2spec > 64) return -1;
+    if (s->n_metals != 0 && s->n_metals != 9) return -1;
+    for (int m = 0; m < s->n_metals; ++m)
+        if (s->metal_n[m] < 1 || !s->metal_lambda[m] || !s->metal_eta[m] || !s->metal_k[m]) return -1;
     memset(t, 0, sizeof(*t));
     t->n_cie = s->n_cie;
     t->n_rgb = s->n_rgb2spec;
@@ -106,9 +109,15 @@ int orc_tables_init(orc_tables *t, const fl_spectral_tables *s) {
             t->brefl[b][i] = orc_average_spectrum_samples(t->rgb_lambda, t->refl[b], t->n_rgb, wl0, wl1);
             t->billum[b][i] = orc_average_spectrum_samples(t->rgb_lambda, t->illum[b], t->n_rgb, wl0, wl1);
         }
+        for (int m = 0; m < s->n_metals && m < 9; ++m) {
+            t->metal[m][0][i] = orc_average_spectrum_samples(s->metal_lambda[m], s->metal_eta[m], s->metal_n[m], wl0, wl1);
+            t->metal[m][1][i] = orc_average_spectrum_samples(s->metal_lambda[m], s->metal_k[m], s->metal_n[m], wl0, wl1);
+        }
     }
     return 0;
 }
+
+void orc_tables_metals(const orc_tables *t, float *out) { memcpy(out, t->metal, sizeof(t->metal)); }
 
 void orc_tables_binned(const orc_tables *t, float *out) {
     memcpy(out, t->X, sizeof(float) * ORC_NBINS);

@@ -25,11 +25,17 @@
  *
  * Usage:
  *   ref_render SCENE.bin OUT.bin     render a scene file written by tests/golden/scenefile.py
+ *   ref_render SCENE.bin OUT.bin --forge   the same after InitializeForge (color/metallurgy.cpp:7-39),
+ *                                    which nothing in the reference calls: without it the
+ *                                    measured-metal spectra stay zero
  *   ref_render --tables OUT.bin      dump the raw and 60-bin spectral tables
+ *   ref_render --metals OUT.bin      dump the measured metal curves (color/metallurgy.h) and the
+ *                                    60-bin spectra InitializeForge makes of them
  *   ref_render --pcg OUT.bin         dump pcg32 known-answer sequences
  */
 #include "filianore/cameras/physical.h"
 #include "filianore/color/cie.h"
+#include "filianore/color/metallurgy.h"
 #include "filianore/color/spectruminits.h"
 #include "filianore/color/spectrumoperations.h"
 #include "filianore/core/interaction.h"
@@ -192,6 +198,36 @@ int dump_tables(const char *out) {
     return 0;
 }
 
+// the raw curves in GetMetalCoefficientsFromForge's order, then InitializeForge's 60-bin eta / k
+int dump_metals(const char *out) {
+    FILE *f = fopen(out, "wb");
+    if (!f) return 2;
+    const int ns[9] = {Gold_nSamples, Copper_nSamples, Silver_nSamples, Aluminium_nSamples, Beryllium_nSamples,
+                       Chromium_nSamples, Mercury_nSamples, Iridium_nSamples, Lithium_nSamples};
+    const float *lam[9] = {Gold_Lambda, Copper_Lambda, Silver_Lambda, Aluminium_Lambda, Beryllium_Lambda,
+                           Chromium_Lambda, Mercury_Lambda, Iridium_Lambda, Lithium_Lambda};
+    const float *eta[9] = {Gold_Eta, Copper_Eta, Silver_Eta, Aluminium_Eta, Beryllium_Eta,
+                           Chromium_Eta, Mercury_Eta, Iridium_Eta, Lithium_Eta};
+    const float *kk[9] = {Gold_K, Copper_K, Silver_K, Aluminium_K, Beryllium_K,
+                          Chromium_K, Mercury_K, Iridium_K, Lithium_K};
+    int32_t n9[9];
+    for (int m = 0; m < 9; ++m) n9[m] = ns[m];
+    fwrite(n9, sizeof(int32_t), 9, f);
+    for (int m = 0; m < 9; ++m) {
+        fwrite(lam[m], sizeof(float), ns[m], f);
+        fwrite(eta[m], sizeof(float), ns[m], f);
+        fwrite(kk[m], sizeof(float), ns[m], f);
+    }
+    InitializeForge();
+    for (int m = 0; m < 9; ++m) {
+        const std::pair<PrincipalSpectrum, PrincipalSpectrum> p = GetMetalCoefficientsFromForge(m);
+        fwrite(p.first.c, sizeof(float), nSpectralSamples, f);
+        fwrite(p.second.c, sizeof(float), nSpectralSamples, f);
+    }
+    fclose(f);
+    return 0;
+}
+
 int dump_pcg(const char *out) {
     FILE *f = fopen(out, "wb");
     if (!f) return 2;
@@ -218,7 +254,7 @@ int dump_pcg(const char *out) {
     return 0;
 }
 
-int render(const char *scene_path, const char *out_path) {
+int render(const char *scene_path, const char *out_path, bool forge) {
     FILE *f = fopen(scene_path, "rb");
     if (!f) { fprintf(stderr, "cannot open %s\n", scene_path); return 2; }
     SceneFileHeader h;
@@ -244,6 +280,7 @@ int render(const char *scene_path, const char *out_path) {
     }
 
     InitializeSpectrals();
+    if (forge) InitializeForge();
 
     std::vector<std::shared_ptr<Material>> materials;
     for (const auto &m : mats) {
@@ -267,7 +304,7 @@ int render(const char *scene_path, const char *out_path) {
             auto flt = [](float v) { return std::make_shared<ConstantTexture<float>>(v); };
             materials.push_back(std::make_shared<StandardSurfaceMaterial>(
                 p.kd_weight, spec(p.kd), flt(p.kd_roughness), p.ks_weight, spec(p.ks), flt(p.ks_roughness),
-                flt(p.ks_anisotropic), p.fresnel_type, p.ks_ior, 0, p.sheen_weight, spec(p.sheen_color),
+                flt(p.ks_anisotropic), p.fresnel_type, p.ks_ior, p.metal_type, p.sheen_weight, spec(p.sheen_color),
                 flt(p.sheen_roughness), p.kt_weight, spec(p.kt), p.coat_weight, spec(p.coat_color), p.coat_ior,
                 p.coat_gloss, p.thin_film_thickness, p.thin_film_ior, p.thin_walled != 0, nullptr));
         } else {
@@ -390,7 +427,9 @@ int render(const char *scene_path, const char *out_path) {
 int main(int argc, char **argv) {
     if (argc == 3 && strcmp(argv[1], "--tables") == 0) return dump_tables(argv[2]);
     if (argc == 3 && strcmp(argv[1], "--pcg") == 0) return dump_pcg(argv[2]);
-    if (argc == 3) return render(argv[1], argv[2]);
-    fprintf(stderr, "usage: ref_render SCENE.bin OUT.bin | --tables OUT.bin | --pcg OUT.bin\n");
+    if (argc == 3 && strcmp(argv[1], "--metals") == 0) return dump_metals(argv[2]);
+    if (argc == 3) return render(argv[1], argv[2], false);
+    if (argc == 4 && strcmp(argv[3], "--forge") == 0) return render(argv[1], argv[2], true);
+    fprintf(stderr, "usage: ref_render SCENE.bin OUT.bin [--forge] | --tables OUT.bin | --metals OUT.bin | --pcg OUT.bin\n");
     return 1;
 }

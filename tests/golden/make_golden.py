@@ -16,10 +16,16 @@ reference sources with oracle/Makefile). Outputs:
                         point, spot and directional lights added: 64x64 at 4 spp (float64)
   cornell_standard_ref.npz  the Cornell box with StandardSurfaceMaterial boxes ("standard":
                         Oren-Nayar + sheen, Fresnel-blended anisotropic GGX + clear coat;
-                        "standard2": Schlick-metallic blend, specular R/T glass + sheen):
-                        64x64 at 4 spp (float64)
+                        "standard2": Schlick-metallic blend, specular R/T glass + sheen;
+                        "standard3": thin-walled diffuse transmission + sheen, measured copper
+                        with Oren-Nayar diffuse + thin film + clear coat), 64x64 at 4 spp
+                        (float64); "standard3" twice: as the reference renders it (no
+                        InitializeForge: zero metal spectra) and after InitializeForge
+  metal_tables.npz      the measured metal curves of color/metallurgy.h (wavelengths, eta, k
+                        per metal) and the 60-bin spectra InitializeForge makes of them
 Usage: python tests/golden/make_golden.py [part ...]   (parts: tables pcg cornell materials
-       delta standard; default all)
+       delta metals standard; default all)
+Scratch files go to oracle/_ref/tmp.
 """
 import os
 import sys
@@ -105,28 +111,39 @@ def delta(tmp):
     np.savez_compressed(os.path.join(HERE, "cornell_delta_ref.npz"), **out)
 
 
+def metals(tmp):
+    """the measured metal curves and InitializeForge's 60-bin spectra"""
+    import subprocess
+    path = os.path.join(tmp, "metals.bin")
+    subprocess.run([oracle.REF_BIN, "--metals", path], check=True)
+    np.savez_compressed(os.path.join(HERE, "metal_tables.npz"), **oracle.load_metals_dump(path))
+
+
 def standard(tmp):
     """the box with StandardSurfaceMaterial boxes"""
     out = {}
-    for variant in ("standard", "standard2"):
+    for variant, forge in (("standard", False), ("standard2", False), ("standard3", False), ("standard3", True)):
         sc = scenes.cornell(64, 64, variant)
         p = scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60)
-        spath = os.path.join(tmp, f"{variant}.scene")
-        fpath = os.path.join(tmp, f"{variant}.film")
+        key = variant + ("_forge" if forge else "")
+        spath = os.path.join(tmp, f"{key}.scene")
+        fpath = os.path.join(tmp, f"{key}.film")
         oracle.write_scene_file(spath, sc, p)
-        film, info = oracle.run_reference(spath, fpath, 64, 64)
-        out[f"{variant}_xyz"] = film.astype(np.float64)
-        print(variant, info)
+        film, info = oracle.run_reference(spath, fpath, 64, 64, forge=forge)
+        out[f"{key}_xyz"] = film.astype(np.float64)
+        print(key, info)
     np.savez_compressed(os.path.join(HERE, "cornell_standard_ref.npz"), **out)
 
 
 PARTS = {"tables": tables, "pcg": pcg, "cornell": cornell, "materials": materials, "delta": delta,
-         "standard": standard}
+         "metals": metals, "standard": standard}
 
 
 def main(parts):
     oracle.build(ref=True)
-    tmp = tempfile.mkdtemp()
+    scratch = os.path.join(ROOT, "oracle", "_ref", "tmp")
+    os.makedirs(scratch, exist_ok=True)
+    tmp = tempfile.mkdtemp(dir=scratch)
     for name in parts or list(PARTS):
         PARTS[name](tmp)
 

@@ -4,6 +4,7 @@ import os
 
 import numpy as np
 
+import filianore_b200 as fb
 import oracle
 from filianore_b200 import scenes, types as T
 
@@ -87,8 +88,26 @@ def test_oracle_standard_surface_equal_reference(orc_tables):
     Fresnel, Estevez sheen, GTR1 clear coat, specular R/T glass) in the Cornell box: the
     restatement is bit-exact at 64x64 x 4 spp."""
     g = np.load(os.path.join(GOLDEN, "cornell_standard_ref.npz"))
-    for variant in ("standard", "standard2"):
+    for variant in ("standard", "standard2", "standard3"):
         sc = scenes.cornell(64, 64, variant)
         film, _ = oracle.render(sc, orc_tables, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60))
         assert np.array_equal(film, g[f"{variant}_xyz"]), (variant, np.abs(film - g[f"{variant}_xyz"]).max())
         assert film.mean() > 0
+
+
+def test_oracle_measured_metals_equal_reference():
+    """Measured-metal eta / k binned from the curves of color/metallurgy.h as InitializeForge
+    does, bit-exact against the reference's own binning; without curves every metal is zero
+    (the reference never calls InitializeForge). The "standard3" box (thin-walled diffuse
+    transmission, measured copper with a thin film and a clear coat) after InitializeForge
+    is bit-exact against the reference run with InitializeForge."""
+    m = np.load(os.path.join(GOLDEN, "metal_tables.npz"))
+    tab = oracle.Tables(fb.reference_tables(measured_metals=True))
+    got = tab.metals()
+    assert np.array_equal(got[:, 0], m["eta60"]) and np.array_equal(got[:, 1], m["k60"])
+    assert (m["eta60"] > 0).all() and (m["k60"] > 0).all()
+    assert not oracle.Tables(fb.reference_tables()).metals().any()
+    g = np.load(os.path.join(GOLDEN, "cornell_standard_ref.npz"))
+    film, _ = oracle.render(scenes.cornell(64, 64, "standard3"), tab, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60))
+    assert np.array_equal(film, g["standard3_forge_xyz"])
+    assert not np.array_equal(film, g["standard3_xyz"])
