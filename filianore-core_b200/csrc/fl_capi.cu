@@ -151,9 +151,14 @@ static StandardDev standard_dev(const fl_standard_surface &P) {
     d.coat_weight = P.coat_weight;
     d.coat_ior = P.coat_ior;
     d.coat_gloss = (1.f - P.coat_gloss) * .1f + P.coat_gloss * .001f;  // lerp(gloss, .1, .001)
+    d.tf_ior = P.thin_film_ior;
+    d.tf_thickness = P.thin_film_thickness;
+    const bool measured = P.fresnel_type == FL_FRESNEL_MEASURED_METAL;
     d.n_lobes = 0;
-    if (P.kd_weight > 0 && P.ks_weight <= 0) d.lobes[d.n_lobes++] = 4;
-    if (P.ks_weight > 0) d.lobes[d.n_lobes++] = P.kt_weight > 0 ? 8 : 5;
+    if ((P.kd_weight > 0 && P.ks_weight <= 0) || (P.kd_weight > 0 && P.ks_weight > 0 && measured))
+        d.lobes[d.n_lobes++] = P.thin_walled ? 11 : 4;  // DiffuseTransmission or OrenNayarBRDF
+    if (P.ks_weight > 0) d.lobes[d.n_lobes++] = P.kt_weight > 0 ? 8 : (measured ? 9 : 5);
+    if (P.thin_film_thickness > 0) d.lobes[d.n_lobes++] = 10;
     if (P.sheen_weight > 0) d.lobes[d.n_lobes++] = 6;
     if (P.coat_weight > 0) d.lobes[d.n_lobes++] = 7;
     const float *rgb[5] = {P.kd, P.ks, P.kt, P.sheen_color, P.coat_color};
@@ -208,6 +213,15 @@ fl_status fl_context_create(int32_t device, const fl_spectral_tables *t, fl_cont
             set_error(nullptr, "missing RGB-to-spectrum basis");
             return FL_ERR_INVALID;
         }
+    if (t->n_metals != 0 && t->n_metals != 9) {
+        set_error(nullptr, "n_metals must be 0 or 9");
+        return FL_ERR_INVALID;
+    }
+    for (int m = 0; m < t->n_metals; ++m)
+        if (t->metal_n[m] < 1 || t->metal_n[m] > 4096 || !t->metal_lambda[m] || !t->metal_eta[m] || !t->metal_k[m]) {
+            set_error(nullptr, "incomplete metal curve");
+            return FL_ERR_INVALID;
+        }
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) {
@@ -237,8 +251,10 @@ fl_status fl_context_create(int32_t device, const fl_spectral_tables *t, fl_cont
     CTX_TRY(cudaMalloc(&ctx->d_error, sizeof(int) * 4));
     CTX_TRY(cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * 8));
 
-    // 60-bin tables as InitializeSpectrals builds them (color/spectruminits.cpp:6-64)
+    // 60-bin tables as InitializeSpectrals builds them (color/spectruminits.cpp:6-64), and
+    // the metals as InitializeForge does (color/metallurgy.cpp:7-39)
     ctx->binned_host.assign(17 * 60, 0.f);
+    ctx->metal60.assign(9 * 120, 0.f);
     for (int i = 0; i < 60; ++i) {
         const float wl0 = lerp_ref((float)i / 60.f, 400.f, 700.f);
         const float wl1 = lerp_ref((float)(i + 1) / 60.f, 400.f, 700.f);
@@ -250,6 +266,11 @@ fl_status fl_context_create(int32_t device, const fl_spectral_tables *t, fl_cont
                 average_spectrum_samples(t->rgb2spec_lambda, t->refl[b], t->n_rgb2spec, wl0, wl1);
             ctx->binned_host[600 + 60 * b + i] =
                 average_spectrum_samples(t->rgb2spec_lambda, t->illum[b], t->n_rgb2spec, wl0, wl1);
+        }
+        for (int m = 0; m < t->n_metals; ++m) {
+            ctx->metal60[120 * m + i] = average_spectrum_samples(t->metal_lambda[m], t->metal_eta[m], t->metal_n[m], wl0, wl1);
+            ctx->metal60[120 * m + 60 + i] =
+                average_spectrum_samples(t->metal_lambda[m], t->metal_k[m], t->metal_n[m], wl0, wl1);
         }
     }
     SpectralTablesDev &T = ctx->tables;
@@ -307,6 +328,7 @@ fl_status fl_context_binned_tables(const fl_context *ctx_h, float *out, size_t n
     const Context *ctx = reinterpret_cast<const Context *>(ctx_h);
     if (!ctx || !out || n < 17 * 60) return FL_ERR_INVALID;
     std::memcpy(out, ctx->binned_host.data(), sizeof(float) * 17 * 60);
+    if (n >= 17 * 60 + 9 * 120) std::memcpy(out + 17 * 60, ctx->metal60.data(), sizeof(float) * 9 * 120);
     return FL_OK;
 }
 
@@ -333,16 +355,9 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
     }
     for (uint32_t i = 0; d->standard_surfaces && i < d->n_standard_surfaces; ++i) {
         const fl_standard_surface &P = d->standard_surfaces[i];
-        if (P.fresnel_type != FL_FRESNEL_DIELECTRIC && P.fresnel_type != FL_FRESNEL_METALLIC) {
-            set_error(ctx, "standard surface: unsupported fresnel_type (the measured-metal Fresnel is not implemented)");
-            return FL_ERR_INVALID;
-        }
-        if (P.thin_film_thickness != 0.f) {
-            set_error(ctx, "standard surface: thin-film interference is not implemented (thickness must be 0)");
-            return FL_ERR_INVALID;
-        }
-        if (P.thin_walled != 0) {
-            set_error(ctx, "standard surface: thin-walled transmission is not implemented");
+        if (P.fresnel_type != FL_FRESNEL_DIELECTRIC && P.fresnel_type != FL_FRESNEL_METALLIC &&
+            P.fresnel_type != FL_FRESNEL_MEASURED_METAL) {
+            set_error(ctx, "standard surface: unknown fresnel_type");
             return FL_ERR_INVALID;
         }
     }
@@ -466,12 +481,18 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
         SC_TRY(cudaMemcpy(s->mat_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
     }
     SC_TRY(cudaMalloc(&s->standard, sizeof(StandardDev) * (n_std ? n_std : 1)));
-    SC_TRY(cudaMalloc(&s->std_refl60, sizeof(float) * 300 * (n_std ? n_std : 1)));
+    const size_t std_floats = (size_t)kStdSpectra * 60;
+    SC_TRY(cudaMalloc(&s->std_refl60, sizeof(float) * std_floats * (n_std ? n_std : 1)));
     if (n_std) {
-        std::vector<float> refl((size_t)300 * n_std);
-        for (uint32_t m = 0; m < n_std; ++m)
-            for (int c = 0; c < 5; ++c)
-                refl60(ctx->binned_host, std_host[m].basis[c], std_host[m].w[c], &refl[(size_t)m * 300 + 60 * c]);
+        std::vector<float> refl(std_floats * n_std);
+        for (uint32_t m = 0; m < n_std; ++m) {
+            float *row = &refl[(size_t)m * std_floats];
+            for (int c = 0; c < 5; ++c) refl60(ctx->binned_host, std_host[m].basis[c], std_host[m].w[c], row + 60 * c);
+            // GetMetalCoefficientsFromForge (color/metallurgy.cpp:42-74): unknown types are gold
+            const int mt = d->standard_surfaces[m].metal_type;
+            const int metal = (mt >= 0 && mt <= 8) ? mt : 0;
+            std::memcpy(row + 300, &ctx->metal60[120 * (size_t)metal], sizeof(float) * 120);
+        }
         SC_TRY(cudaMemcpy(s->standard, std_host.data(), sizeof(StandardDev) * n_std, cudaMemcpyHostToDevice));
         SC_TRY(cudaMemcpy(s->std_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
     }

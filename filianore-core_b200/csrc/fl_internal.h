@@ -34,6 +34,7 @@ struct Context {
     std::mutex mu;
     std::string last_error;
     std::vector<float> binned_host;  // 17 * 60
+    std::vector<float> metal60;      // 9 metals x (eta, k) x 60 bins (zero without metal curves)
     SpectralTablesDev tables{};
     // grow-only scratch owned by the context (render wavefront state, trace staging)
     void *scratch = nullptr;
@@ -65,10 +66,14 @@ struct MaterialDev {
 // StandardSurfaceMaterial with constant textures, reduced on the host to what
 // compute_scattering_functions (materials/standardsurface.cpp:72-159) hands its BxDFs.
 // Lobe ids: 4 Oren-Nayar, 5 Fresnel-blended diffuse + specular, 6 Estevez sheen,
-// 7 GTR1 clear coat, 8 FresnelSpecular with R = ks and T = kt.
+// 7 GTR1 clear coat, 8 FresnelSpecular with R = ks and T = kt, 9 GGX with the measured-metal
+// conductor Fresnel, 10 GGX with the thin-film Fresnel, 11 diffuse transmission.
+// Its spectra (kStdSpectra rows of 60 bins in Scene::std_refl60): kd, ks, kt, sheen colour,
+// coat colour, metal eta, metal k.
+constexpr int kStdSpectra = 7;
 struct StandardDev {
     int n_lobes;
-    int lobes[4];         // in the order the material adds them
+    int lobes[5];         // in the order the material adds them
     float eta;            // BSDF::eta: ks_ior with both specular and transmission weights, else 1
     float ior;            // ks_ior (FresnelSpecular, Schlick r0)
     float ax, ay;         // GGX alphas with the anisotropic aspect
@@ -78,6 +83,7 @@ struct StandardDev {
     int fresnel_type;     // FL_FRESNEL_*
     float sheen_weight, sheen_rough;
     float coat_weight, coat_ior, coat_gloss;  // coat_gloss = lerp(gloss, .1, .001)
+    float tf_ior, tf_thickness;                // thin film over a medium of IOR ior
     int basis[5][3];      // Smits terms of kd, ks, kt, sheen colour, coat colour
     float w[5][3];
 };
@@ -109,7 +115,7 @@ struct Scene {
     MaterialDev *materials = nullptr;
     float *mat_refl60 = nullptr;      // n_materials x 60: from_reflectance_rgb in the 60 bins
     StandardDev *standard = nullptr;  // n_standard StandardSurface records
-    float *std_refl60 = nullptr;      // n_standard x 5 x 60: their five colours in the 60 bins
+    float *std_refl60 = nullptr;      // n_standard x kStdSpectra x 60: their spectra in the 60 bins
     uint32_t n_standard = 0;
     uint32_t n_materials = 0;
     LightDev *lights = nullptr;

@@ -311,7 +311,7 @@ __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const Sm
         b.mat_eta = sd->ior;
         b.ax = sd->ax;
         b.ay = sd->ay;
-        b.std60 = A.std_refl60 + 300 * (size_t)m.standard;
+        b.std60 = A.std_refl60 + kStdSpectra * 60 * (size_t)m.standard;
         b.bases = sm.bases;
         b.rgb_l0 = tab.rgb_lambda0;
         b.rgb_l1 = tab.rgb_lambda1;

@@ -212,10 +212,22 @@ struct Bsdf {
     float lambda0;
 };
 
-enum : int { kStdKd = 0, kStdKs = 1, kStdKt = 2, kStdSheen = 3, kStdCoat = 4 };
+enum : int { kStdKd = 0, kStdKs = 1, kStdKt = 2, kStdSheen = 3, kStdCoat = 4, kStdEta = 5, kStdK = 6 };
+// the wavelength of spectral sample i: the bin start 400 + 5 i nm (the loop of
+// ThinFilmInteference::evaluate) or the hero wavelength
+template <int NL>
+__device__ inline float std_wavelength(const Bsdf<NL> &b, int i) {
+    return NL == 60 ? (float)(400 + 5 * i) : hero_lambda(b.lambda0, i);
+}
 template <int NL>
 __device__ inline float std_color(const Bsdf<NL> &b, int c, int i) {
     if (NL == 60) return __ldg(b.std60 + 60 * c + i);
+    if (c >= kStdEta) {
+        // measured metal: hero wavelengths read the 5 nm bin they fall in, clamped to 400..700 nm
+        int bin = (int)floorf((hero_lambda(b.lambda0, i) - 400.f) / 5.f);
+        bin = bin < 0 ? 0 : (bin > 59 ? 59 : bin);
+        return __ldg(b.std60 + 60 * c + bin);
+    }
     // from_reflectance_rgb at hero wavelength i (color/spectrumoperations.cpp:113-147)
     const float l = hero_lambda(b.lambda0, i);
     float r = 0.f;
@@ -338,7 +350,7 @@ __device__ inline float fr_conductor(float cosI, float etaT, float k) {
 // lobes: 0 Lambert, 1 microfacet reflection, 2 microfacet transmission, 3 Fresnel specular,
 // and the StandardSurface lobes 4 Oren-Nayar, 5 Fresnel-blended diffuse + specular,
 // 6 Estevez sheen, 7 GTR1 clear coat, 8 Fresnel specular with R = ks, T = kt
-constexpr int kMaxLobes = 4;
+constexpr int kMaxLobes = 5;
 // The BSDF routines are compiled twice: STD = false for the Lambert, GGX and glass
 // materials (lobes 0..3), STD = true for the StandardSurface (lobes 4..8), which the
 // shading kernels' StandardSurface instances call. Kept apart, the StandardSurface code
@@ -351,8 +363,9 @@ __device__ inline int lobe_type(int lobe) {
                                      : lobe == 2 ? (kBsdfTransmission | kBsdfGlossy)
                                                  : (kBsdfReflection | kBsdfTransmission | kBsdfSpecular);
     return lobe == 4 ? (kBsdfReflection | kBsdfDiffuse)
-                     : lobe == 8 ? (kBsdfReflection | kBsdfTransmission | kBsdfSpecular)
-                                 : (kBsdfReflection | kBsdfGlossy);
+                     : lobe == 11 ? (kBsdfTransmission | kBsdfDiffuse)
+                                  : lobe == 8 ? (kBsdfReflection | kBsdfTransmission | kBsdfSpecular)
+                                              : (kBsdfReflection | kBsdfGlossy);
 }
 template <bool STD, int NL>
 __device__ inline int mat_lobes(const Bsdf<NL> &b, int *lobes) {
@@ -440,7 +453,40 @@ __device__ inline float smith_g_ggx(float cosTheta, float alpha) {
 }
 __device__ inline bool matches(int type, int flags) { return (type & flags) == type; }
 
-// StandardSurface lobes 4..7, out of line: they are the rarely run part of the shading
+// ThinFilmInteference::evaluate (fresnel/thinfilm.cpp:8-58) with extIOR 1 and the amplitude
+// coefficients of fresnel/fresnel.h:9-23, at the path's wavelengths. The reference's sin^2
+// ratios divide a quotient by itself, so both equal 1 - cos^2 (kept).
+template <int NL>
+__device__ inline void thin_film_fresnel(const Bsdf<NL> &b, float cosThetaI, Spec<NL> &F) {
+    const float extIOR = 1.f, tfIOR = b.sd->tf_ior, mIOR = b.mat_eta, thickness = b.sd->tf_thickness;
+    const float sinSqrd1 = ((extIOR / tfIOR) / (extIOR / tfIOR)) * (1 - cosThetaI * cosThetaI);
+    const float sinSqrd2 = ((extIOR / mIOR) / (extIOR / mIOR)) * (1 - cosThetaI * cosThetaI);
+    if ((sinSqrd1 > 1) || (sinSqrd2 > 1)) { F.set(1.f); return; }
+    const float cos1 = sqrtf(1 - sinSqrd1);
+    const float cos2 = sqrtf(1 - sinSqrd2);
+    auto sp_r = [](float n1, float n2, float ci, float ct) { return (n1 * ci - n2 * ct) / (n1 * ci + n2 * ct); };
+    auto sp_t = [](float n1, float n2, float ci, float ct) { return (2.f * n1 * ci) / (n1 * ci + n2 * ct); };
+    auto pp_r = [](float n1, float n2, float ci, float ct) { return (n2 * ci - n1 * ct) / (n1 * ct + n2 * ci); };
+    auto pp_t = [](float n1, float n2, float ci, float ct) { return (2.f * n1 * ci) / (n1 * ct + n2 * ci); };
+    const float alphaSP = sp_r(tfIOR, extIOR, cos1, cosThetaI) * sp_r(mIOR, tfIOR, cos1, cos2);
+    const float alphaPP = pp_r(tfIOR, extIOR, cos1, cosThetaI) * pp_r(mIOR, tfIOR, cos1, cos2);
+    const float betaSP = sp_t(extIOR, tfIOR, cosThetaI, cos1) * sp_t(tfIOR, mIOR, cos1, cos2);
+    const float betaPP = pp_t(extIOR, tfIOR, cosThetaI, cos1) * pp_t(tfIOR, mIOR, cos1, cos2);
+    const float delta10 = tfIOR < extIOR ? kPi : 0.f;
+    const float delta12 = tfIOR < mIOR ? kPi : 0.f;
+    const float delta = delta10 + delta12;
+    const float beamRatio = (mIOR * cos2) / (extIOR * cosThetaI);
+    for (int i = 0; i < NL; ++i) {
+        const float wavelength = std_wavelength(b, i);
+        const float phi = (2.f * kPi / wavelength) * (2.f * tfIOR * thickness * cos1) + delta;
+        const float cp = fl_cos(phi);
+        const float ts = (betaSP * betaSP) / ((alphaSP * alphaSP) - (2.f * alphaSP * cp) + 1.f);
+        const float tp = (betaPP * betaPP) / ((alphaPP * alphaPP) - (2.f * alphaPP * cp) + 1.f);
+        F.c[i] = 1.f - (ts + tp) * 0.5f * beamRatio;
+    }
+}
+
+// StandardSurface lobes 4..7 and 9..11, out of line: they are the rarely run part of the shading
 // kernels, and kept apart their registers do not weigh on the Lambert and GGX code.
 template <int NL>
 __device__ __noinline__ void std_lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec<NL> &out) {
@@ -503,6 +549,29 @@ __device__ __noinline__ void std_lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v
         for (int i = 0; i < NL; ++i) out.c[i] = std_color(b, kStdCoat, i) * Fr * w * Gr * Dr / 4;
         return;
     }
+    if (lobe == 9 || lobe == 10) {
+        // MicrofacetReflectionBRDF::evaluate (bxdfs/microfacetreflection.cpp:13-32) with R = 1 and
+        // the measured-metal FresnelConductor (weight ks_weight) or the thin film (weight 1)
+        const float cosThetaO = fabsf(wo.z), cosThetaI = fabsf(wi.z);
+        v3 wh = add(wi, wo);
+        if (cosThetaI == 0 || cosThetaO == 0 || (wh.x == 0 && wh.y == 0 && wh.z == 0)) { out.set(0.f); return; }
+        wh = normalize(wh);
+        const v3 whf = dot(wh, mk(0.f, 0.f, 1.f)) < 0.f ? neg(wh) : wh;
+        const float cF = dot(wi, whf);
+        if (lobe == 9) {
+#pragma unroll 4
+            for (int i = 0; i < NL; ++i) out.c[i] = fr_conductor(cF, std_color(b, kStdEta, i), std_color(b, kStdK, i));
+        } else {
+            thin_film_fresnel(b, cF, out);
+        }
+        const float weight = lobe == 9 ? b.sd->ks_weight : 1.f;
+        const float D = ggx_D(b, wh), G = ggx_G(b, wo, wi);
+        const float den = 4.f * cosThetaO * cosThetaI;
+#pragma unroll 4
+        for (int i = 0; i < NL; ++i) out.c[i] = 1.f * weight * D * G * out.c[i] / den;
+        return;
+    }
+    if (lobe == 11) { oren_nayar_eval(b, b.sd->on_A, b.sd->on_B, wo, wi, out); return; }
     out.set(0.f);
 }
 
@@ -531,6 +600,13 @@ __device__ __noinline__ float std_lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v
         const float Dr = gtr1(fabsf(wh.z), b.sd->coat_gloss);
         return Dr * fabsf(wh.z) / (4 * dot(wo, wh));
     }
+    if (lobe == 9 || lobe == 10) {
+        if (!same_hemi(wo, wi)) return 0.f;
+        const v3 wh = normalize(add(wo, wi));
+        return ggx_pdf(b, wo, wh) / (4.f * dot(wo, wh));
+    }
+    // DiffuseTransmission::pdf (bxdfs/diffusetransmission.cpp:29-31)
+    if (lobe == 11) return !same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.f;
     return 0.f;
 }
 
@@ -588,6 +664,26 @@ __device__ __noinline__ void std_lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo,
         std_lobe_eval(b, 7, wo, wi, f);
         return;
     }
+    if (lobe == 9 || lobe == 10) {
+        // MicrofacetReflectionBRDF::sample (bxdfs/microfacetreflection.cpp:34-56)
+        if (wo.z == 0) { f.set(0.f); return; }
+        const v3 wh = ggx_sample_wh(b, wo, ux, uy);
+        if (dot(wo, wh) < 0) { f.set(0.f); return; }
+        wi = reflect_wh(wo, wh);
+        if (!same_hemi(wo, wi)) { f.set(0.f); return; }
+        pdf = ggx_pdf(b, wo, wh) / (4.f * dot(wo, wh));
+        std_lobe_eval(b, lobe, wo, wi, f);
+        return;
+    }
+    if (lobe == 11) {
+        // DiffuseTransmission::sample (bxdfs/diffusetransmission.cpp:16-27): a cosine-weighted
+        // direction on the side away from wo
+        wi = cos_hemi(mk(0.f, 0.f, 1.f), ux, uy);
+        if (wo.z > 0) wi.z *= -1.f;
+        pdf = std_lobe_pdf(b, 11, wo, wi);
+        std_lobe_eval(b, 11, wo, wi, f);
+        return;
+    }
     f.set(0.f);
 }
 
@@ -595,7 +691,7 @@ __device__ __noinline__ void std_lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo,
 template <bool STD, int NL>
 __device__ inline void lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec<NL> &out) {
     if (STD) {
-        if (lobe >= 4 && lobe <= 7) std_lobe_eval(b, lobe, wo, wi, out);
+        if (lobe != 8) std_lobe_eval(b, lobe, wo, wi, out);
         else out.set(0.f);
         return;
     }
@@ -640,7 +736,7 @@ __device__ inline void lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec
 
 template <bool STD, int NL>
 __device__ inline float lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi) {
-    if (STD) return (lobe >= 4 && lobe <= 7) ? std_lobe_pdf(b, lobe, wo, wi) : 0.f;
+    if (STD) return lobe != 8 ? std_lobe_pdf(b, lobe, wo, wi) : 0.f;
     if (lobe == 0) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.f;
     if (lobe == 1) {
         if (!same_hemi(wo, wi)) return 0.f;
@@ -695,7 +791,7 @@ __device__ inline void lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo, v3 &wi, f
         lobe_eval<false>(b, 2, wo, wi, f);
         return;
     }
-    if (STD && lobe >= 4 && lobe <= 7) { std_lobe_sample(b, lobe, wo, wi, ux, uy, pdf, f); return; }
+    if (STD && lobe != 8) { std_lobe_sample(b, lobe, wo, wi, ux, uy, pdf, f); return; }
     // FresnelSpecularBXDF: lobe 3 with R = T = the material colour, lobe 8 with R = ks, T = kt
     const float F = fr_dielectric(wo.z, 1.f, b.mat_eta);
     if (ux < F) {

@@ -189,6 +189,12 @@ class Context:
         check(lib().fl_context_binned_tables(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size), self.h)
         return out.reshape(17, 60)
 
+    def binned_metals(self):
+        """the measured metals' 60-bin eta and k: (9, 2, 60)"""
+        out = np.zeros(17 * 60 + 9 * 120, np.float32)
+        check(lib().fl_context_binned_tables(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size), self.h)
+        return out[17 * 60:].reshape(9, 2, 60)
+
     def scene(self, scene_obj):
         return SceneHandle(self, scene_obj)
 

@@ -109,7 +109,8 @@ FL_API const char *fl_status_string(fl_status status);
 FL_API fl_status fl_last_error(const fl_context *ctx, char *buf, size_t buf_len);
 
 /* The 60-bin tables the library derived from the caller's tables, for inspection:
- * out has room for 17*60 floats in the order X, Y, Z, refl[0..6], illum[0..6]. */
+ * out has room for 17*60 floats in the order X, Y, Z, refl[0..6], illum[0..6]; with room for
+ * 17*60 + 9*120 floats the binned metals follow (per metal: eta, then k). */
 FL_API fl_status fl_context_binned_tables(const fl_context *ctx, float *out, size_t n_floats);
 
 /* ------------------------------------------------------------------------- */

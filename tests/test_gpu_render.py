@@ -152,41 +152,66 @@ def test_delta_lights_match_reference_integrator(ctx, variant):
     assert abs(xyz.mean() / ref.mean() - 1) < 2e-3
 
 
-@pytest.mark.parametrize("variant", ["standard", "standard2"])
-def test_standard_surface_matches_reference_material(ctx, variant):
+@pytest.fixture(scope="module")
+def ctx_metals():
+    """a context with the measured metal curves (the reference after InitializeForge)"""
+    c = fb.Context(0, tables=fb.reference_tables(measured_metals=True))
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("variant", ["standard", "standard2", "standard3", "standard3_forge"])
+def test_standard_surface_matches_reference_material(ctx, ctx_metals, variant):
     """StandardSurfaceMaterial boxes (Oren-Nayar, Fresnel-blended anisotropic GGX with Schlick
-    dielectric and metallic Fresnel, Estevez sheen, GTR1 clear coat, specular R/T glass),
-    60-bin parity build, against the reference's own material (fixture made by the reference
-    build). The near-specular glass chain amplifies last-ulp differences, so the bound is 99%
+    dielectric and metallic Fresnel, Estevez sheen, GTR1 clear coat, specular R/T glass,
+    thin-walled diffuse transmission, measured copper under a thin film: with zero metal
+    spectra as the reference renders it, and after InitializeForge), 60-bin parity build,
+    against the reference's own material (fixture made by the reference build). The near-specular glass chain amplifies last-ulp differences, so the bound is 99%
     of pixels within 1e-4 relative (or 1e-6 absolute) and the image mean within 2e-3."""
     g = np.load(os.path.join(GOLDEN, "cornell_standard_ref.npz"))
     ref = g[f"{variant}_xyz"]
-    sc = scenes.cornell(64, 64, variant)
-    xyz, _, stats = render_xyz(ctx, sc, scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60))
+    forge = variant.endswith("_forge")
+    sc = scenes.cornell(64, 64, variant.replace("_forge", ""))
+    xyz, _, stats = render_xyz(ctx_metals if forge else ctx, sc, scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60))
     assert stats["paths"] == 64 * 64 * 4 and stats["traversal_errors"] == 0
     assert close_fraction(xyz, ref, 1e-4, 1e-6) >= 0.99
     assert abs(xyz.mean() / ref.mean() - 1) < 2e-3
 
 
-@pytest.mark.parametrize("variant", ["standard", "standard2"])
-def test_standard_surface_hero_matches_oracle(ctx, orc_tables, variant):
+@pytest.mark.parametrize("variant", ["standard", "standard2", "standard3_forge"])
+def test_standard_surface_hero_matches_oracle(ctx, ctx_metals, orc_tables, variant):
     """The same boxes in the hero-wavelength build (FMA contraction, single-precision pow,
     exp, log) against the oracle's hero mode: >= 99% of pixels within 1e-3 relative and the
-    image mean within 2e-3."""
-    sc = scenes.cornell(64, 64, variant)
+    image mean within 2e-3. The thin-walled box of "standard3" sends paths through its inside,
+    from one face to a neighbouring one near their shared edges, where the contracted build
+    rounds intersections differently from the CPU: there ~2.5% of the pixels hold a path that
+    went another way at 8 spp (errors of 0.2-30%; 99.9% agree in the uncontracted 60-bin
+    build), so its bound is 96% of pixels and the image mean within 1e-3."""
+    forge = variant.endswith("_forge")
+    sc = scenes.cornell(64, 64, variant.replace("_forge", ""))
     p = scenes.render_params(8, 8, fb.FL_SPECTRAL_HERO4)
-    xyz, _, stats = render_xyz(ctx, sc, p)
-    cpu, cnt = oracle.render(sc, orc_tables, p)
+    xyz, _, stats = render_xyz(ctx_metals if forge else ctx, sc, p)
+    tab = oracle.Tables(fb.reference_tables(measured_metals=True)) if forge else orc_tables
+    cpu, cnt = oracle.render(sc, tab, p)
     assert stats["paths"] == cnt["paths"]
-    assert close_fraction(xyz, cpu, 1e-3, 1e-5) >= 0.99
-    assert abs(xyz.mean() / cpu.mean() - 1) < 2e-3
+    thin_walled = variant.startswith("standard3")
+    assert close_fraction(xyz, cpu, 1e-3, 1e-5) >= (0.96 if thin_walled else 0.99)
+    assert abs(xyz.mean() / cpu.mean() - 1) < (1e-3 if thin_walled else 2e-3)
 
 
-@pytest.mark.parametrize("bad", [{"thin_film_thickness": 400.0}, {"thin_walled": 1}, {"fresnel_type": 2},
-                                 {"fresnel_type": -1}])
-def test_standard_surface_rejects_unsupported_parts(ctx, bad):
-    """Thin-film interference, thin-walled transmission and the measured-metal Fresnel are
-    refused by fl_scene_create with FL_ERR_INVALID and a message, never rendered wrongly."""
+def test_binned_metals_equal_initializeforge(ctx, ctx_metals):
+    """The library bins the metal curves as InitializeForge does: bit-exact against the
+    reference's own binning; without curves every metal spectrum is zero."""
+    m = np.load(os.path.join(GOLDEN, "metal_tables.npz"))
+    got = ctx_metals.binned_metals()
+    assert np.array_equal(got[:, 0], m["eta60"]) and np.array_equal(got[:, 1], m["k60"])
+    assert not ctx.binned_metals().any()
+
+
+@pytest.mark.parametrize("bad", [{"fresnel_type": 3}, {"fresnel_type": -1}])
+def test_standard_surface_rejects_unknown_fresnel(ctx, bad):
+    """An unknown Fresnel type is refused by fl_scene_create with FL_ERR_INVALID and a
+    message (the reference's switch would silently add no specular lobe)."""
     sc = scenes.cornell(8, 8, "standard")
     mats = [dict(m) for m in sc.materials]
     mats[-1] = {"standard": dict(mats[-1]["standard"], **bad)}
