@@ -93,6 +93,14 @@ struct Illuminant {
     float cone_angle = 0.f, penumbra_angle = 0.f;  // spot, radians from the axis
 };
 
+// StandardSurfaceMaterial: its parameters are standard_surfaces[index] of the Scene
+inline fl_material StandardSurfaceMaterial(int32_t index) {
+    fl_material m{};
+    m.type = FL_MAT_STANDARD;
+    m.standard = index;
+    return m;
+}
+
 inline fl_material LambertMaterial(float r, float g, float b) {
     fl_material m{};
     m.type = FL_MAT_LAMBERT;
@@ -156,7 +164,8 @@ public:
         tri_material_.push_back(material);
     }
     // Builds the device BVH (embree's rtcCommitScene). Returns false on failure.
-    bool finalise(const std::vector<fl_material> &materials, const std::vector<fl_light> &lights) {
+    bool finalise(const std::vector<fl_material> &materials, const std::vector<fl_light> &lights,
+                  const std::vector<fl_standard_surface> &standard_surfaces = {}) {
         clean_up();
         if (!ctx_ || !ctx_->ok()) {
             error_ = "BVH::finalise without a valid context";
@@ -170,6 +179,8 @@ public:
         d.n_materials = (uint32_t)materials.size();
         d.lights = lights.data();
         d.n_lights = (uint32_t)lights.size();
+        d.standard_surfaces = standard_surfaces.empty() ? nullptr : standard_surfaces.data();
+        d.n_standard_surfaces = (uint32_t)standard_surfaces.size();
         const fl_status st = fl_scene_create(ctx_->get(), &d, &scene_);
         if (st != FL_OK) {
             error_ = status_text(ctx_->get(), st);
@@ -243,7 +254,7 @@ private:
 class Scene {
 public:
     Scene(Context &ctx, const SceneGeometry &geometry, const std::vector<fl_material> &materials,
-          const std::vector<Illuminant> &illuminants)
+          const std::vector<Illuminant> &illuminants, const std::vector<fl_standard_surface> &standard_surfaces = {})
         : illuminants(illuminants) {
         bvh.initialize(ctx);
         bvh.initialize_scene_geometry(geometry);
@@ -264,7 +275,7 @@ public:
             l.penumbra_angle = il.penumbra_angle;
             lights.push_back(l);
         }
-        ok_ = bvh.finalise(materials, lights);
+        ok_ = bvh.finalise(materials, lights, standard_surfaces);
     }
     ~Scene() { bvh.clean_up(); }
     bool ok() const { return ok_; }

@@ -43,6 +43,7 @@ int main(int argc, char **argv) {
     fl_spectral_tables t{};
     std::vector<fl_material> mats;
     std::vector<fl_light> lights_raw;
+    std::vector<fl_standard_surface> standard;
     fl_camera cam{};
     SceneGeometry geometry;
     int spp = 0, depth = 0, mode = 0;
@@ -67,6 +68,7 @@ int main(int argc, char **argv) {
         spp = r.get<int32_t>(), depth = r.get<int32_t>(), mode = r.get<int32_t>();
         const uint32_t n_rays = r.get<uint32_t>();
         const std::vector<float> org = r.arr<float>(4 * (size_t)n_rays), dir = r.arr<float>(4 * (size_t)n_rays);
+        standard = r.arr<fl_standard_surface>(r.get<uint32_t>());
         // one mesh per triangle keeps the per-triangle materials and the soup order
         for (uint32_t i = 0; i < n_tri; ++i) {
             auto mesh = std::make_shared<TriangleMesh>();
@@ -107,7 +109,7 @@ int main(int argc, char **argv) {
     }
     int rc = 0;
     {
-        Scene scene(ctx, geometry, mats, illuminants);
+        Scene scene(ctx, geometry, mats, illuminants, standard);
         if (!scene.ok()) {
             std::fprintf(stderr, "scene: %s\n", scene.bvh.last_error().c_str());
             return 1;

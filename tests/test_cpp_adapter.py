@@ -55,12 +55,15 @@ def write_input(path, sc, params, org, dirs):
         f.write(np.uint32(org.shape[0]).tobytes())
         f.write(np.ascontiguousarray(org, np.float32).tobytes())
         f.write(np.ascontiguousarray(dirs, np.float32).tobytes())
+        stds, n_std = sc.standard_array()
+        f.write(np.uint32(n_std).tobytes())
+        f.write(bytes(stds)[: n_std * C.sizeof(fb.fl_standard_surface)])
 
 
 @pytest.mark.gpu
 def test_adapter_matches_c_abi(tmp_path):
     exe = build(str(tmp_path))
-    sc = scenes.cornell_delta(48, 48)   # area, point, spot and directional lights
+    sc = scenes.cornell_delta(48, 48, "standard")   # area, point, spot and directional lights; StandardSurface boxes
     params = scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60)
     rng = np.random.default_rng(3)
     n = 4096
