@@ -561,8 +561,7 @@ static fl_status check_render_args(Context *ctx, Scene *s, const fl_camera *came
         return FL_ERR_INVALID;
     }
     const fl_render_params &p = *params;
-    if (camera->width <= 0 || camera->height <= 0 || (uint64_t)camera->width * camera->height > (1ull << 31) ||
-        p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 || p.spectral_mode != FL_SPECTRAL_HERO4 ||
+    if (!camera_ok(*camera) || p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 || p.spectral_mode != FL_SPECTRAL_HERO4 ||
         (memory != FL_MEM_HOST && memory != FL_MEM_DEVICE)) {
         set_error(ctx, "invalid guided render parameters (hero wavelengths only)");
         return FL_ERR_INVALID;

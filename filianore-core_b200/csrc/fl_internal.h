@@ -150,6 +150,12 @@ fl_status launch_trace(Scene *s, const float4 *org_tmin, const float4 *dir_tmax,
 fl_status ensure_scratch(Context *ctx, size_t bytes, void **out);
 fl_status ensure_film_scratch(Context *ctx, size_t bytes, void **out);
 
+// camera resolution within 2^31 pixels and a finite, non-negative aperture
+inline bool camera_ok(const fl_camera &c) {
+    return c.width > 0 && c.height > 0 && (uint64_t)c.width * c.height <= (1ull << 31) && c.aperture >= 0.f &&
+           c.aperture <= 3.0e38f;
+}
+
 // Smits terms of from_reflectance_rgb (basis ids and weights, in the reference's order)
 void smits_terms(const float rgb[3], int basis[3], float w[3]);
 

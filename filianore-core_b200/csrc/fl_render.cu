@@ -36,6 +36,7 @@ CamDev camera_basis_of(const fl_camera &c) {
     d.vertical = mul(mul(mul(v, 2.f), halfHeight), focusDistance);
     d.W = c.width;
     d.H = c.height;
+    d.lens_radius = c.aperture / 2.f;
     return d;
 }
 }  // namespace fl
@@ -53,8 +54,7 @@ extern "C" fl_status fl_render(fl_scene *scene_h, const fl_camera *camera, const
         return FL_ERR_INVALID;
     }
     const fl_render_params p = *params;
-    if (camera->width <= 0 || camera->height <= 0 || (uint64_t)camera->width * camera->height > (1ull << 31) ||
-        p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 ||
+    if (!camera_ok(*camera) || p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 ||
         (p.spectral_mode != FL_SPECTRAL_HERO4 && p.spectral_mode != FL_SPECTRAL_BINS60) ||
         (memory != FL_MEM_HOST && memory != FL_MEM_DEVICE)) {
         set_error(ctx, "invalid render parameters");

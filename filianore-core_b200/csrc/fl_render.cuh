@@ -91,6 +91,7 @@ struct RenderProfile {
 struct CamDev {
     v3 origin, lower_left, horizontal, vertical, u, v;
     int W, H;
+    float lens_radius;  // PhysicalCamera::lensRadius = aperture / 2 (0: pinhole)
 };
 
 // Everything one render job needs: its scene, camera, parameters and film. A wave's paths
@@ -351,9 +352,17 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
         const uint32_t px = pix % (uint32_t)J.cam.W, py = pix / (uint32_t)J.cam.W;
         const float sx = __fdiv_rn(__fadd_rn((float)px, ux), (float)J.cam.W);
         const float sy = __fdiv_rn(__fadd_rn((float)((uint32_t)J.cam.H - 1u - py), uy), (float)J.cam.H);
-        // PhysicalCamera::awaken_ray with lens sample (0.5, 0.5) and lensRadius 0
-        const v3 lp = sub(mul(mk(0.5f, 0.5f, 0.f), 2.f), mk(1.f, 1.f, 0.f));
-        const v3 rd = mul(lp, 0.f);
+        // PhysicalCamera::awaken_ray (cameras/physical.cpp:12-22): a pinhole takes the lens
+        // sample (0.5, 0.5); a lens draws two numbers and maps them with the concentric disk
+        v3 rd;
+        if (J.cam.lens_radius > 0.f) {
+            const float lx = rng.nextf(), ly = rng.nextf();
+            const v3 lp = concentric_disk(lx, ly);
+            rd = mul(lp, J.cam.lens_radius);
+        } else {
+            const v3 lp = sub(mul(mk(0.5f, 0.5f, 0.f), 2.f), mk(1.f, 1.f, 0.f));
+            rd = mul(lp, 0.f);
+        }
         const v3 offset = add(mul(J.cam.u, rd.x), mul(J.cam.v, rd.y));
         const v3 o = add(J.cam.origin, offset);
         const v3 dir = sub(sub(add(add(J.cam.lower_left, mul(J.cam.horizontal, sx)), mul(J.cam.vertical, sy)),

@@ -58,8 +58,7 @@ extern "C" fl_status fl_render_noalloc(fl_scene *scene_h, const fl_camera *camer
         return FL_ERR_INVALID;
     }
     const fl_render_params p = *params;
-    if (camera->width <= 0 || camera->height <= 0 || (uint64_t)camera->width * camera->height > (1ull << 31) ||
-        p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 ||
+    if (!camera_ok(*camera) || p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 ||
         (p.spectral_mode != FL_SPECTRAL_HERO4 && p.spectral_mode != FL_SPECTRAL_BINS60) || s->n_lights > 64) {
         set_error(ctx, "invalid render parameters");
         return FL_ERR_INVALID;

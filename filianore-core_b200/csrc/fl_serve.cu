@@ -377,7 +377,7 @@ fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job
     if (!S || !job || !job_id) return FL_ERR_INVALID;
     const fl_camera &c = job->camera;
     const fl_render_params &p = job->params;
-    if (c.width <= 0 || c.height <= 0 || (uint64_t)c.width * c.height > (1ull << 31) || p.spp <= 0 ||
+    if (!camera_ok(c) || p.spp <= 0 ||
         p.max_depth < 0 || p.max_depth > S->cfg.max_depth || p.spectral_mode != FL_SPECTRAL_HERO4) {
         set_error(S->ctx, "invalid job (hero-wavelength mode, depth within the server's max_depth)");
         return FL_ERR_INVALID;

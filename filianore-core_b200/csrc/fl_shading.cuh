@@ -401,18 +401,19 @@ __device__ inline void oren_nayar_eval(const Bsdf<NL> &b, float A, float B, v3 w
 #pragma unroll
     for (int i = 0; i < NL; ++i) out.c[i] = std_color(b, kStdKd, i) * kInvPi * v * weight;
 }
+// concentric_sample_disk (core/shadingcore.h:65-80), as (x, y, 0)
+__device__ inline v3 concentric_disk(float ux, float uy) {
+    const float ox = ux * 2.f - 1.f, oy = uy * 2.f - 1.f;
+    if (ox == 0 && oy == 0) return mk(0.f, 0.f, 0.f);
+    float theta, r;
+    if (fabsf(ox) > fabsf(oy)) { r = ox; theta = kPiOver4 * (oy / ox); }
+    else { r = oy; theta = kPiOver2 - kPiOver4 * (ox / oy); }
+    return mk(r * fl_cos(theta), r * fl_sin(theta), 0.f);
+}
 // cosine_hemisphere_sample over concentric_sample_disk (core/shadingcore.h:65-89), on wo's side
 __device__ inline v3 cos_hemi(v3 wo, float ux, float uy) {
-    const float ox = ux * 2.f - 1.f, oy = uy * 2.f - 1.f;
-    float dx, dy;
-    if (ox == 0 && oy == 0) { dx = 0.f; dy = 0.f; }
-    else {
-        float theta, r;
-        if (fabsf(ox) > fabsf(oy)) { r = ox; theta = kPiOver4 * (oy / ox); }
-        else { r = oy; theta = kPiOver2 - kPiOver4 * (ox / oy); }
-        dx = r * fl_cos(theta);
-        dy = r * fl_sin(theta);
-    }
+    const v3 dsk = concentric_disk(ux, uy);
+    const float dx = dsk.x, dy = dsk.y;
     const float zz = 1.f - dx * dx - dy * dy;
     v3 wi = mk(dx, dy, sqrtf(zz > 0.f ? zz : 0.f));
     if (wo.z < 0) wi.z *= -1.f;

@@ -99,6 +99,7 @@ class Scene:
         cam.vfov_deg = c["vfov"]
         cam.width = width or c["width"]
         cam.height = height or c["height"]
+        cam.aperture = c.get("aperture", 0.0)
         return cam
 
 

@@ -140,6 +140,7 @@ class fl_camera(C.Structure):
         ("vfov_deg", C.c_float),
         ("width", C.c_int32),
         ("height", C.c_int32),
+        ("aperture", C.c_float),
     ]
 
 

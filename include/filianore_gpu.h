@@ -263,6 +263,13 @@ typedef struct {
     float up[3];
     float vfov_deg;
     int32_t width, height;
+    /* PhysicalCamera's aperture: the lens diameter (lensRadius = aperture / 2), focused at
+     * the look-at distance; 0 is a pinhole. With a lens, each sample draws two more numbers
+     * after (ux, uy, u_lambda) and maps them to the lens with concentric_sample_disk
+     * (core/shadingcore.h:65-80). The reference's random_point_on_lens
+     * (cameras/physical.cpp:4-10) rejects points outside the disk without drawing new ones,
+     * so it never returns for 21% of lens samples. */
+    float aperture;
 } fl_camera;
 
 enum {

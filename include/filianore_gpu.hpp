@@ -78,6 +78,7 @@ struct PhysicalCamera {
     Vector3f position, lookAt, up{0.f, 1.f, 0.f};
     float fov = 40.f;  // vertical, degrees
     int xRes = 256, yRes = 256;
+    float aperture = 0.f;  // lens diameter, focused at lookAt (0: pinhole)
 };
 
 // An illuminant: a triangle of the soup (DiffuseAreaIlluminant), a point, spot or
@@ -311,6 +312,7 @@ public:
         cam.look_at[0] = camera.lookAt.x, cam.look_at[1] = camera.lookAt.y, cam.look_at[2] = camera.lookAt.z;
         cam.up[0] = camera.up.x, cam.up[1] = camera.up.y, cam.up[2] = camera.up.z;
         cam.vfov_deg = camera.fov;
+        cam.aperture = camera.aperture;
         cam.width = camera.xRes;
         cam.height = camera.yRes;
         fl_render_params p{};

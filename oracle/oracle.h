@@ -94,7 +94,7 @@ int orc_render(const fl_scene_desc *scene, const orc_tables *tables, const fl_ca
                orc_render_counts *counts);
 
 /* camera basis exactly as PhysicalCamera::PhysicalCamera (cameras/physical.h:11-43) */
-typedef struct { v3 origin, lower_left, horizontal, vertical, u, v; } orc_camera;
+typedef struct { v3 origin, lower_left, horizontal, vertical, u, v; float lens_radius; } orc_camera;
 void orc_camera_init(const fl_camera *c, orc_camera *out);
 /* one camera ray for (pixel, sample) plus the hero-wavelength draw; returns 3 floats used */
 void orc_camera_ray(const orc_camera *cam, const fl_camera *c, uint32_t pixel, orc_pcg32 *rng,

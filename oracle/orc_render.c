@@ -1235,6 +1235,7 @@ void orc_camera_init(const fl_camera *c, orc_camera *out) {
                              v3_mul(w, focusDistance));
     out->horizontal = v3_mul(v3_mul(v3_mul(u, 2.f), halfWidth), focusDistance);
     out->vertical = v3_mul(v3_mul(v3_mul(v, 2.f), halfHeight), focusDistance);
+    out->lens_radius = c->aperture / 2.f;  /* lensRadius = aperture / 2 (physical.h:20) */
 }
 
 /* The render loop the reference lacks: sample (s, t) of pixel p, PhysicalCamera::awaken_ray
@@ -1246,9 +1247,24 @@ void orc_camera_ray(const orc_camera *cam, const fl_camera *c, uint32_t pixel, o
     uint32_t px = pixel % (uint32_t)c->width, py = pixel / (uint32_t)c->width;
     float sx = ((float)px + ux) / (float)c->width;
     float sy = ((float)((uint32_t)c->height - 1u - py) + uy) / (float)c->height;
-    /* random_point_on_lens((0.5, 0.5)) * lensRadius with lensRadius = 0 */
-    v3 p = v3_sub(v3_mul(v3m(0.5f, 0.5f, 0.f), 2.f), v3m(1.f, 1.f, 0.f));
-    v3 rd = v3_mul(p, 0.f);
+    v3 rd;
+    if (cam->lens_radius > 0.f) {
+        /* a lens: two more numbers, mapped with concentric_sample_disk (shadingcore.h:65-80)
+         * in place of random_point_on_lens, whose rejection loop never draws a new sample */
+        float lx = orc_pcg32_nextf(rng), ly = orc_pcg32_nextf(rng);
+        float ox = lx * 2.f - 1.f, oy = ly * 2.f - 1.f, dx = 0.f, dy = 0.f;
+        if (!(ox == 0 && oy == 0)) {
+            float theta, r;
+            if (fabsf(ox) > fabsf(oy)) { r = ox; theta = ORC_PI_OVER_4 * (oy / ox); }
+            else { r = oy; theta = ORC_PI_OVER_2 - ORC_PI_OVER_4 * (ox / oy); }
+            dx = cosf(theta) * r; dy = sinf(theta) * r;
+        }
+        rd = v3_mul(v3m(dx, dy, 0.f), cam->lens_radius);
+    } else {
+        /* random_point_on_lens((0.5, 0.5)) * lensRadius with lensRadius = 0 */
+        v3 p = v3_sub(v3_mul(v3m(0.5f, 0.5f, 0.f), 2.f), v3m(1.f, 1.f, 0.f));
+        rd = v3_mul(p, 0.f);
+    }
     v3 offset = v3_add(v3_mul(cam->u, rd.x), v3_mul(cam->v, rd.y));
     *o = v3_add(cam->origin, offset);
     v3 dir = v3_sub(v3_sub(v3_add(v3_add(cam->lower_left, v3_mul(cam->horizontal, sx)), v3_mul(cam->vertical, sy)),

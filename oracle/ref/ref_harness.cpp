@@ -366,6 +366,12 @@ int render(const char *scene_path, const char *out_path, bool forge) {
     Scene scene(geom, illuminants);
 
     const fl_camera &c = h.cam;
+    if (c.aperture != 0.f) {
+        // random_point_on_lens (cameras/physical.cpp:4-10) never returns for lens samples
+        // outside the unit disk: the reference can only render a pinhole here
+        fprintf(stderr, "the reference's lens sampler does not terminate: aperture must be 0\n");
+        return 2;
+    }
     PhysicalCamera camera(Vector3f(c.position[0], c.position[1], c.position[2]),
                           Vector3f(c.look_at[0], c.look_at[1], c.look_at[2]), c.width, c.height, c.vfov_deg, 0.f, 0.f,
                           0.f, Vector3f(c.up[0], c.up[1], c.up[2]), true);

@@ -220,3 +220,28 @@ def test_standard_surface_rejects_unknown_fresnel(ctx, bad):
         ctx.scene(bad_scene)
     assert e.value.status == fb.FL_ERR_INVALID
     assert "standard surface" in str(e.value)
+
+
+@pytest.mark.parametrize("mode", [fb.FL_SPECTRAL_BINS60, fb.FL_SPECTRAL_HERO4])
+def test_thin_lens_matches_oracle(ctx, orc_tables, mode):
+    """Thin-lens depth of field (PhysicalCamera's aperture, focused at the look-at distance,
+    lens points from concentric_sample_disk) against the oracle: >= 99% of pixels within 1e-4
+    (60-bin) / 1e-3 (hero) and the image mean within 2e-3; the defocused image differs from
+    the pinhole one, and a negative or non-finite aperture is refused."""
+    base = scenes.cornell(64, 64)
+    sc = scenes.Scene(base.verts, base.tri_material, base.materials, base.lights, dict(base.camera, aperture=0.15))
+    p = scenes.render_params(8, 8, mode)
+    xyz, _, stats = render_xyz(ctx, sc, p)
+    cpu, cnt = oracle.render(sc, orc_tables, p)
+    assert stats["paths"] == cnt["paths"]
+    tol = 1e-4 if mode == fb.FL_SPECTRAL_BINS60 else 1e-3
+    assert close_fraction(xyz, cpu, tol, 1e-5) >= 0.99
+    assert abs(xyz.mean() / cpu.mean() - 1) < 2e-3
+    pin, _, _ = render_xyz(ctx, base, p)
+    assert not np.allclose(xyz, pin, rtol=1e-2)
+    for bad in (-0.1, float("nan"), float("inf")):
+        bad_sc = scenes.Scene(base.verts, base.tri_material, base.materials, base.lights, dict(base.camera, aperture=bad))
+        s = ctx.scene(bad_sc)
+        with pytest.raises(fb.FlError):
+            s.render(p)
+        s.close()
