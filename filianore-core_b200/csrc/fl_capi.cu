@@ -93,23 +93,6 @@ float average_spectrum_samples(const float *wl, const float *vals, int n, float 
     return sum / (we - ws);
 }
 
-// Smits terms of from_reflectance_rgb (color/spectrumoperations.cpp:113-147): basis ids
-// (0 white, 1 cyan, 2 magenta, 3 yellow, 4 red, 5 green, 6 blue) and weights, in its order.
-void smits_terms(const float rgb[3], int basis[3], float w[3]) {
-    if (rgb[0] <= rgb[1] && rgb[0] <= rgb[2]) {
-        basis[0] = 0; w[0] = rgb[0];
-        if (rgb[1] <= rgb[2]) { basis[1] = 1; w[1] = rgb[1] - rgb[0]; basis[2] = 6; w[2] = rgb[2] - rgb[1]; }
-        else { basis[1] = 1; w[1] = rgb[2] - rgb[0]; basis[2] = 5; w[2] = rgb[1] - rgb[2]; }
-    } else if (rgb[1] <= rgb[0] && rgb[1] <= rgb[2]) {
-        basis[0] = 0; w[0] = rgb[1];
-        if (rgb[0] <= rgb[2]) { basis[1] = 2; w[1] = rgb[0] - rgb[1]; basis[2] = 6; w[2] = rgb[2] - rgb[0]; }
-        else { basis[1] = 2; w[1] = rgb[2] - rgb[1]; basis[2] = 4; w[2] = rgb[0] - rgb[2]; }
-    } else {
-        basis[0] = 0; w[0] = rgb[2];
-        if (rgb[0] <= rgb[1]) { basis[1] = 3; w[1] = rgb[0] - rgb[2]; basis[2] = 5; w[2] = rgb[1] - rgb[0]; }
-        else { basis[1] = 3; w[1] = rgb[1] - rgb[2]; basis[2] = 4; w[2] = rgb[0] - rgb[1]; }
-    }
-}
 
 // from_reflectance_rgb (color/spectrumoperations.cpp:113-147) over the 60 bins, clamped
 // at zero (spectrum_clamp) from the Smits terms
@@ -352,12 +335,27 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
             set_error(ctx, "standard surface index out of range");
             return FL_ERR_INVALID;
         }
+        if (M.texture < 0 || (M.texture > 0 && (!d->images || (uint32_t)M.texture > d->n_images))) {
+            set_error(ctx, "material texture index out of range");
+            return FL_ERR_INVALID;
+        }
+    }
+    for (uint32_t i = 0; d->images && i < d->n_images; ++i) {
+        const fl_image &im = d->images[i];
+        if (im.width <= 0 || im.height <= 0 || !im.rgb || (uint64_t)im.width * im.height > (1ull << 28)) {
+            set_error(ctx, "invalid image (needs pixels, at most 2^28 of them)");
+            return FL_ERR_INVALID;
+        }
     }
     for (uint32_t i = 0; d->standard_surfaces && i < d->n_standard_surfaces; ++i) {
         const fl_standard_surface &P = d->standard_surfaces[i];
         if (P.fresnel_type != FL_FRESNEL_DIELECTRIC && P.fresnel_type != FL_FRESNEL_METALLIC &&
             P.fresnel_type != FL_FRESNEL_MEASURED_METAL) {
             set_error(ctx, "standard surface: unknown fresnel_type");
+            return FL_ERR_INVALID;
+        }
+        if (P.kd_texture < 0 || (P.kd_texture > 0 && (!d->images || (uint32_t)P.kd_texture > d->n_images))) {
+            set_error(ctx, "standard surface: kd texture index out of range");
             return FL_ERR_INVALID;
         }
     }
@@ -446,12 +444,18 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
         md.k = M.k;
         smits_terms(M.rgb, md.basis, md.w);
         md.standard = M.type == FL_MAT_STANDARD ? M.standard : 0;
+        md.texture = M.type == FL_MAT_LAMBERT ? M.texture - 1 : -1;
         s->materials_host.push_back(md);
     }
     const uint32_t n_std = d->standard_surfaces ? d->n_standard_surfaces : 0;
     std::vector<StandardDev> std_host;
-    for (uint32_t i = 0; i < n_std; ++i) std_host.push_back(standard_dev(d->standard_surfaces[i]));
+    for (uint32_t i = 0; i < n_std; ++i) {
+        std_host.push_back(standard_dev(d->standard_surfaces[i]));
+        std_host.back().kd_texture = d->standard_surfaces[i].kd_texture - 1;
+    }
     s->n_standard = n_std;
+    s->ext_kernels = n_std > 0;
+    for (const MaterialDev &md : s->materials_host) s->ext_kernels |= md.texture >= 0;
     s->n_lights = d->n_lights;
     s->n_materials = d->n_materials;
 
@@ -479,6 +483,26 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
         for (uint32_t m = 0; m < d->n_materials; ++m)
             refl60(ctx->binned_host, s->materials_host[m].basis, s->materials_host[m].w, &refl[(size_t)m * 60]);
         SC_TRY(cudaMemcpy(s->mat_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
+    }
+    if (d->uvs && d->n_tri) {
+        SC_TRY(cudaMalloc(&s->uvs, sizeof(float) * 6 * (size_t)d->n_tri));
+        SC_TRY(cudaMemcpy(s->uvs, d->uvs, sizeof(float) * 6 * (size_t)d->n_tri, cudaMemcpyHostToDevice));
+    }
+    if (d->images && d->n_images) {
+        std::vector<ImageDev> info(d->n_images);
+        unsigned long long total = 0;
+        for (uint32_t i = 0; i < d->n_images; ++i) {
+            info[i] = ImageDev{total, d->images[i].width, d->images[i].height};
+            total += 3ull * (unsigned long long)d->images[i].width * (unsigned long long)d->images[i].height;
+        }
+        SC_TRY(cudaMalloc(&s->pixels, total));
+        SC_TRY(cudaMalloc(&s->images, sizeof(ImageDev) * d->n_images));
+        for (uint32_t i = 0; i < d->n_images; ++i)
+            SC_TRY(cudaMemcpy(s->pixels + info[i].offset, d->images[i].rgb,
+                              3ull * (unsigned long long)d->images[i].width * (unsigned long long)d->images[i].height,
+                              cudaMemcpyHostToDevice));
+        SC_TRY(cudaMemcpy(s->images, info.data(), sizeof(ImageDev) * d->n_images, cudaMemcpyHostToDevice));
+        s->n_images = d->n_images;
     }
     SC_TRY(cudaMalloc(&s->standard, sizeof(StandardDev) * (n_std ? n_std : 1)));
     const size_t std_floats = (size_t)kStdSpectra * 60;
@@ -535,6 +559,9 @@ fl_status fl_scene_destroy(fl_scene *scene) {
     cudaFree(s->mat_refl60);
     cudaFree(s->standard);
     cudaFree(s->std_refl60);
+    cudaFree(s->uvs);
+    cudaFree(s->pixels);
+    cudaFree(s->images);
     if (s->counted) s->ctx->children--;
     delete s;
     return FL_OK;

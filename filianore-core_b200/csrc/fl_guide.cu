@@ -539,7 +539,7 @@ static fl_status guide_pass(Guide *G, Scene *s, const CamDev &cam, const fl_rend
         d.seg[0] = WaveSeg{0u, 0u, d.n_wave, 0u, wb, 0ull};
         FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
         if (train) FL_CUDA_TRY(ctx, cudaMemsetAsync(G->rec_count, 0, sizeof(uint32_t), st));
-        enqueue_wave<4, true>(W, p.max_depth, false, &prof, sms, st, s->n_standard > 0);
+        enqueue_wave<4, true>(W, p.max_depth, false, &prof, sms, st, s->ext_kernels);
         FL_CUDA_TRY(ctx, cudaGetLastError());
         if (train) {
             FL_CUDA_TRY(ctx, cudaMemcpyAsync(G->h_count, G->rec_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));

@@ -61,6 +61,13 @@ struct MaterialDev {
     int basis[3];       // Smits basis indices of from_reflectance_rgb
     float w[3];         // and their weights
     int standard;       // FL_MAT_STANDARD: index into Scene::standard
+    int texture;        // FL_MAT_LAMBERT: image of its reflectance, -1: rgb
+};
+
+// An ImageMapTexture's pixels in Scene::pixels: RGB bytes, rows from the top.
+struct ImageDev {
+    unsigned long long offset;  // first byte
+    int width, height;
 };
 
 // StandardSurfaceMaterial with constant textures, reduced on the host to what
@@ -84,6 +91,7 @@ struct StandardDev {
     float sheen_weight, sheen_rough;
     float coat_weight, coat_ior, coat_gloss;  // coat_gloss = lerp(gloss, .1, .001)
     float tf_ior, tf_thickness;                // thin film over a medium of IOR ior
+    int kd_texture;                            // image of kd, -1: the constant kd
     int basis[5][3];      // Smits terms of kd, ks, kt, sheen colour, coat colour
     float w[5][3];
 };
@@ -117,6 +125,11 @@ struct Scene {
     StandardDev *standard = nullptr;  // n_standard StandardSurface records
     float *std_refl60 = nullptr;      // n_standard x kStdSpectra x 60: their spectra in the 60 bins
     uint32_t n_standard = 0;
+    float *uvs = nullptr;             // 6 per triangle, soup order (null: every hit has uv (0, 0))
+    unsigned char *pixels = nullptr;  // the images' RGB bytes
+    ImageDev *images = nullptr;
+    uint32_t n_images = 0;
+    bool ext_kernels = false;         // StandardSurface or image-textured materials: their kernel instances run
     uint32_t n_materials = 0;
     LightDev *lights = nullptr;
     uint32_t n_lights = 0;
@@ -156,7 +169,22 @@ inline bool camera_ok(const fl_camera &c) {
            c.aperture <= 3.0e38f;
 }
 
-// Smits terms of from_reflectance_rgb (basis ids and weights, in the reference's order)
-void smits_terms(const float rgb[3], int basis[3], float w[3]);
+// Smits terms of from_reflectance_rgb (color/spectrumoperations.cpp:113-147): basis ids
+// (0 white, 1 cyan, 2 magenta, 3 yellow, 4 red, 5 green, 6 blue) and weights, in its order.
+__host__ __device__ inline void smits_terms(const float rgb[3], int basis[3], float w[3]) {
+    if (rgb[0] <= rgb[1] && rgb[0] <= rgb[2]) {
+        basis[0] = 0; w[0] = rgb[0];
+        if (rgb[1] <= rgb[2]) { basis[1] = 1; w[1] = rgb[1] - rgb[0]; basis[2] = 6; w[2] = rgb[2] - rgb[1]; }
+        else { basis[1] = 1; w[1] = rgb[2] - rgb[0]; basis[2] = 5; w[2] = rgb[1] - rgb[2]; }
+    } else if (rgb[1] <= rgb[0] && rgb[1] <= rgb[2]) {
+        basis[0] = 0; w[0] = rgb[1];
+        if (rgb[0] <= rgb[2]) { basis[1] = 2; w[1] = rgb[0] - rgb[1]; basis[2] = 6; w[2] = rgb[2] - rgb[0]; }
+        else { basis[1] = 2; w[1] = rgb[2] - rgb[1]; basis[2] = 4; w[2] = rgb[0] - rgb[2]; }
+    } else {
+        basis[0] = 0; w[0] = rgb[2];
+        if (rgb[0] <= rgb[1]) { basis[1] = 3; w[1] = rgb[0] - rgb[2]; basis[2] = 5; w[2] = rgb[1] - rgb[0]; }
+        else { basis[1] = 3; w[1] = rgb[1] - rgb[2]; basis[2] = 4; w[2] = rgb[0] - rgb[1]; }
+    }
+}
 
 }  // namespace fl

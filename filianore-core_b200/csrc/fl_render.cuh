@@ -31,8 +31,8 @@
 namespace fl {
 
 // 0: miss, 1 + material type (Lambert, conductor, rough / smooth dielectric, standard
-// surface), and with guiding on, kClassLambertLate: Lambert vertices past the guided ones
-// (no inference)
+// surface; image-textured Lambert joins the standard surfaces), and with guiding on,
+// kClassLambertLate: Lambert vertices past the guided ones (no inference)
 constexpr int kShadeClasses = 7;
 constexpr int kClassStandard = 1 + FL_MAT_STANDARD;
 constexpr int kClassLambertLate = 6;
@@ -108,6 +108,9 @@ struct JobDev {
     const float *mat_refl60;
     const StandardDev *standard;
     const float *std_refl60;
+    const float *uvs;              // 6 per triangle, or null
+    const unsigned char *pixels;   // image bytes
+    const ImageDev *images;
     const LightDev *lights;
     int n_lights;
     int any_hit_ok;
@@ -270,6 +273,8 @@ __device__ inline Hit make_hit(const JobDev &A, float4 o4, float4 d4, int4 h) {
     r.p = add(o, mul(d, t));
     r.wo = normalize(neg(d));
     r.prim = h.x;
+    r.b1 = __int_as_float(h.z);
+    r.b2 = __int_as_float(h.w);
     if (h.x >= 0) {
         const v3 v0 = tri_v(A.soup, (uint32_t)h.x, 0), v1 = tri_v(A.soup, (uint32_t)h.x, 1),
                  v2 = tri_v(A.soup, (uint32_t)h.x, 2);
@@ -285,6 +290,48 @@ __device__ inline int prim_light(const JobDev &A, int prim) {
     if (prim >= 0) return A.tri_light[prim];
     if (prim <= -2) return -2 - prim;
     return -1;
+}
+
+// The hit's texture coordinates uv0 (1 - b1 - b2) + uv1 b1 + uv2 b2, each operation rounded
+// on its own in both builds; (0, 0) without uvs, as BVH::intersect (bvh/bvh.cpp:69-71) leaves them.
+__device__ inline void hit_uv(const JobDev &A, const Hit &h, float &u, float &v) {
+    u = v = 0.f;
+    if (!A.uvs || h.prim < 0) return;
+    const float *t = A.uvs + 6 * (size_t)h.prim;
+    const float w = __fsub_rn(__fsub_rn(1.f, h.b1), h.b2);
+    u = __fadd_rn(__fadd_rn(__fmul_rn(__ldg(t + 0), w), __fmul_rn(__ldg(t + 2), h.b1)), __fmul_rn(__ldg(t + 4), h.b2));
+    v = __fadd_rn(__fadd_rn(__fmul_rn(__ldg(t + 1), w), __fmul_rn(__ldg(t + 3), h.b1)), __fmul_rn(__ldg(t + 5), h.b2));
+}
+
+// ImageMapTexture::evaluate (shading/textures/imagemap.cpp:36-62): the nearest texel, then
+// from_reflectance_rgb of it / 255, at the path's spectral samples. For j past the last row
+// the reference sets i = height - 1 and reads outside the image; here j is clamped too.
+template <int NL>
+__device__ inline void image_reflectance(const JobDev &A, const TablesArg &tab, const SmemTables &sm, int img, float u,
+                                         float v, float lambda0, Spec<NL> &out) {
+    const ImageDev im = A.images[img];
+    int i = (int)__fmul_rn(u, (float)im.width);
+    int j = (int)__fsub_rn(__fmul_rn(__fsub_rn(1.f, v), (float)im.height), 0.001f);
+    if (i < 0) i = 0;
+    if (j < 0) j = 0;
+    if (i > im.width - 1) i = im.width - 1;
+    if (j > im.height - 1) { i = im.height - 1; j = im.height - 1; }
+    if (i > im.width - 1) i = im.width - 1;
+    const unsigned char *px = A.pixels + im.offset + 3ull * ((unsigned long long)j * (unsigned)im.width + (unsigned)i);
+    const float rgb[3] = {(float)(int)px[0] / 255.f, (float)(int)px[1] / 255.f, (float)(int)px[2] / 255.f};
+    int basis[3];
+    float w[3];
+    smits_terms(rgb, basis, w);
+    for (int k = 0; k < NL; ++k) {
+        if (NL == 60) {
+            float r = 0.f;
+            for (int q = 0; q < 3; ++q) r += sm.binned[180 + 60 * basis[q] + k] * w[q];
+            r *= 0.94f;
+            out.c[k] = r < 0.f ? 0.f : r;
+        } else {
+            out.c[k] = smits_at(sm, tab, basis, w, hero_lambda(lambda0, k));
+        }
+    }
 }
 
 template <int NL, bool STD>
@@ -303,6 +350,13 @@ __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const Sm
     b.ay = m.ay;
     b.eta = (m.type == FL_MAT_ROUGH_DIELECTRIC || m.type == FL_MAT_SMOOTH_DIELECTRIC) ? m.eta : 1.f;
     b.corrected = A.corrected_ggx;
+    if (STD && m.type == FL_MAT_LAMBERT) {
+        // LambertMaterial with an ImageMapTexture (materials/lambert.cpp:8-15)
+        float u, v;
+        hit_uv(A, h, u, v);
+        image_reflectance<NL>(A, tab, sm, m.texture, u, v, lambda0, b.R);
+        return;
+    }
     if (STD) {
         // StandardSurfaceMaterial::compute_scattering_functions (materials/standardsurface.cpp:72-159)
         // from the host-reduced record
@@ -318,10 +372,19 @@ __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const Sm
         b.rgb_l1 = tab.rgb_lambda1;
         b.n_rgb = tab.n_rgb;
         b.lambda0 = lambda0;
+        b.kd_tex = sd->kd_texture >= 0;
+        if (b.kd_tex) {
+            float u, v;
+            hit_uv(A, h, u, v);
+            image_reflectance<NL>(A, tab, sm, sd->kd_texture, u, v, lambda0, b.R);
+        }
         return;
     }
-    if (m.type == FL_MAT_LAMBERT) reflectance<NL>(sm, tab, m, A.mat_refl60 + 60 * (size_t)mi, lambda0, b.R);
-    else b.R.set(1.f);
+    if (m.type == FL_MAT_LAMBERT) {
+        reflectance<NL>(sm, tab, m, A.mat_refl60 + 60 * (size_t)mi, lambda0, b.R);
+    } else {
+        b.R.set(1.f);
+    }
 }
 
 // ------------------------------------------------------------------------------ kernels
@@ -452,7 +515,8 @@ struct PathTraceItem {
         int cls = 0;
         if (res.id != -1) {
             const uint32_t mi = res.id >= 0 ? J->tri_material[res.id] : 0u;
-            cls = 1 + J->materials[mi].type;
+            const MaterialDev &m = J->materials[mi];
+            cls = (m.type == FL_MAT_LAMBERT && m.texture >= 0) ? kClassStandard : 1 + m.type;
             if (cls == 1 + FL_MAT_LAMBERT && A->g.select > 0.f && lambert_count(A->flags[slot]) >= kGuidedVertices)
                 cls = kClassLambertLate;
         }
@@ -840,7 +904,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             const float *gm = nullptr;
             float c_sel = 0.f, u_sel = 1.f;
             if constexpr (GUIDE) {
-                if (b.type == FL_MAT_LAMBERT && A.g.select > 0.f && lambert_count(fl) < kGuidedVertices) {
+                if (!STD && b.type == FL_MAT_LAMBERT && A.g.select > 0.f && lambert_count(fl) < kGuidedVertices) {
                     gm = A.g.mix + (size_t)slot * kMixFloats;
                     if (gm[0] >= 0.f) {
                         c_sel = A.g.select;
@@ -870,7 +934,8 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
 #pragma unroll
                 for (int k = 0; k < NL; ++k) beta.c[k] *= f.c[k] * ad / pdf;
                 if constexpr (GUIDE && NL == 4) {
-                    if (A.g.record && b.type == FL_MAT_LAMBERT) guide_record(A, slot, hr, lambda0, wi, pdf, beta, L);
+                    if (!STD && A.g.record && b.type == FL_MAT_LAMBERT)
+                        guide_record(A, slot, hr, lambda0, wi, pdf, beta, L);
                 }
                 const bool spec_b = (sflags & kBsdfSpecular) != 0;
                 float etaScale = A.eta_scale[slot];
@@ -897,7 +962,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                     A.eta_scale[slot] = etaScale;
                     uint32_t nfl = (bounce + 1u) | (spec_b ? 0x100u : 0u);
                     if constexpr (GUIDE) {
-                        const uint32_t lc = lambert_count(fl) + (b.type == FL_MAT_LAMBERT ? 1u : 0u);
+                        const uint32_t lc = lambert_count(fl) + (!STD && b.type == FL_MAT_LAMBERT ? 1u : 0u);
                         nfl |= (lc < 3u ? lc : 3u) << 9;
                     }
                     A.flags[slot] = nfl;
@@ -1081,6 +1146,9 @@ inline JobDev job_of(const Scene *s, const CamDev &cam, const fl_render_params &
     j.mat_refl60 = s->mat_refl60;
     j.standard = s->standard;
     j.std_refl60 = s->std_refl60;
+    j.uvs = s->uvs;
+    j.pixels = s->pixels;
+    j.images = s->images;
     j.lights = s->lights;
     j.n_lights = (int)s->n_lights;
     j.any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
@@ -1118,7 +1186,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_jobs, &j, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(W.A.cnt, 0, sizeof(WaveCounters), st));
     const bool count = (p.flags & FL_RENDER_COUNT) != 0;
-    const bool standard = s->n_standard > 0;
+    const bool standard = s->ext_kernels;
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
     const size_t desc_bytes = offsetof(WaveDesc, seg) + sizeof(WaveSeg);
     // Replay one captured graph per wave: a depth-16 wave is ~85 launches, and its late

@@ -35,6 +35,10 @@ struct HostScene {
     std::vector<uint32_t> tri_material;
     std::vector<fl_material> materials;
     std::vector<fl_light> lights;
+    std::vector<fl_standard_surface> standard;
+    std::vector<float> uvs;
+    std::vector<std::vector<uint8_t>> pixels;  // one buffer per image
+    std::vector<fl_image> images;              // pointing into pixels
     Scene *dev = nullptr;
     uint64_t bytes = 0;
 };
@@ -122,6 +126,11 @@ fl_status make_scene(Server *S, HostScene &h) {
     d.n_materials = (uint32_t)h.materials.size();
     d.lights = h.lights.data();
     d.n_lights = (uint32_t)h.lights.size();
+    d.standard_surfaces = h.standard.empty() ? nullptr : h.standard.data();
+    d.n_standard_surfaces = (uint32_t)h.standard.size();
+    d.uvs = h.uvs.empty() ? nullptr : h.uvs.data();
+    d.images = h.images.empty() ? nullptr : h.images.data();
+    d.n_images = (uint32_t)h.images.size();
     fl_scene *out = nullptr;
     fl_status rc = fl_scene_create(reinterpret_cast<fl_context *>(S->ctx), &d, &out);
     if (rc == FL_OK) h.dev = reinterpret_cast<Scene *>(out);
@@ -363,7 +372,22 @@ fl_status fl_server_add_scene(fl_server *srv, const fl_scene_desc *d, uint64_t *
     else h.tri_material.assign(d->n_tri, 0u);
     h.materials.assign(d->materials, d->materials + d->n_materials);
     if (d->n_lights) h.lights.assign(d->lights, d->lights + d->n_lights);
-    h.bytes = scene_bytes_estimate(d->n_tri, d->n_materials);
+    if (d->standard_surfaces && d->n_standard_surfaces)
+        h.standard.assign(d->standard_surfaces, d->standard_surfaces + d->n_standard_surfaces);
+    if (d->uvs) h.uvs.assign(d->uvs, d->uvs + 6 * (size_t)d->n_tri);
+    for (uint32_t i = 0; d->images && i < d->n_images; ++i) {
+        const fl_image &im = d->images[i];
+        if (im.width <= 0 || im.height <= 0 || !im.rgb || (uint64_t)im.width * im.height > (1ull << 28)) {
+            set_error(S->ctx, "invalid image");
+            return FL_ERR_INVALID;
+        }
+        h.pixels.emplace_back(im.rgb, im.rgb + 3 * (size_t)im.width * im.height);
+    }
+    for (size_t i = 0; i < h.pixels.size(); ++i)
+        h.images.push_back(fl_image{d->images[i].width, d->images[i].height, h.pixels[i].data()});
+    h.bytes = scene_bytes_estimate(d->n_tri, d->n_materials) + 4 * h.uvs.size() +
+              (uint64_t)h.standard.size() * (sizeof(StandardDev) + sizeof(float) * kStdSpectra * 60);
+    for (const auto &px : h.pixels) h.bytes += px.size();
     std::lock_guard<std::mutex> lock(S->mu);
     const uint64_t id = S->next_scene++;
     S->sched.add_scene(id, h.bytes);

@@ -210,6 +210,7 @@ struct Bsdf {
     float rgb_l0, rgb_l1;
     int n_rgb;
     float lambda0;
+    int kd_tex;     // kd is an image texture, evaluated at the hit into R
 };
 
 enum : int { kStdKd = 0, kStdKs = 1, kStdKt = 2, kStdSheen = 3, kStdCoat = 4, kStdEta = 5, kStdK = 6 };
@@ -221,6 +222,7 @@ __device__ inline float std_wavelength(const Bsdf<NL> &b, int i) {
 }
 template <int NL>
 __device__ inline float std_color(const Bsdf<NL> &b, int c, int i) {
+    if (c == kStdKd && b.kd_tex) return b.R.c[i];
     if (NL == 60) return __ldg(b.std60 + 60 * c + i);
     if (c >= kStdEta) {
         // measured metal: hero wavelengths read the 5 nm bin they fall in, clamped to 400..700 nm
@@ -352,9 +354,9 @@ __device__ inline float fr_conductor(float cosI, float etaT, float k) {
 // 6 Estevez sheen, 7 GTR1 clear coat, 8 Fresnel specular with R = ks, T = kt
 constexpr int kMaxLobes = 5;
 // The BSDF routines are compiled twice: STD = false for the Lambert, GGX and glass
-// materials (lobes 0..3), STD = true for the StandardSurface (lobes 4..8), which the
-// shading kernels' StandardSurface instances call. Kept apart, the StandardSurface code
-// adds no calls, registers or branches to the other materials' kernels.
+// materials (lobes 0..3), STD = true for the StandardSurface (lobes 4..11) and the
+// image-textured Lambert (lobe 0), which the shading kernels' StandardSurface instances
+// call. Kept apart, this code adds no calls, registers or branches to the other kernels.
 template <bool STD>
 __device__ inline int lobe_type(int lobe) {
     if (!STD)
@@ -362,7 +364,7 @@ __device__ inline int lobe_type(int lobe) {
                          : lobe == 1 ? (kBsdfReflection | kBsdfGlossy)
                                      : lobe == 2 ? (kBsdfTransmission | kBsdfGlossy)
                                                  : (kBsdfReflection | kBsdfTransmission | kBsdfSpecular);
-    return lobe == 4 ? (kBsdfReflection | kBsdfDiffuse)
+    return (lobe == 0 || lobe == 4) ? (kBsdfReflection | kBsdfDiffuse)
                      : lobe == 11 ? (kBsdfTransmission | kBsdfDiffuse)
                                   : lobe == 8 ? (kBsdfReflection | kBsdfTransmission | kBsdfSpecular)
                                               : (kBsdfReflection | kBsdfGlossy);
@@ -370,6 +372,7 @@ __device__ inline int lobe_type(int lobe) {
 template <bool STD, int NL>
 __device__ inline int mat_lobes(const Bsdf<NL> &b, int *lobes) {
     if (STD) {
+        if (b.type == FL_MAT_LAMBERT) { lobes[0] = 0; return 1; }  // image-textured Lambert
 #pragma unroll
         for (int i = 0; i < kMaxLobes; ++i) lobes[i] = b.sd->lobes[i];
         return b.sd->n_lobes;
@@ -691,7 +694,7 @@ __device__ __noinline__ void std_lobe_sample(const Bsdf<NL> &b, int lobe, v3 wo,
 // lobe evaluate into out (reference multiplication order)
 template <bool STD, int NL>
 __device__ inline void lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec<NL> &out) {
-    if (STD) {
+    if (STD && lobe != 0) {
         if (lobe != 8) std_lobe_eval(b, lobe, wo, wi, out);
         else out.set(0.f);
         return;
@@ -737,7 +740,7 @@ __device__ inline void lobe_eval(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi, Spec
 
 template <bool STD, int NL>
 __device__ inline float lobe_pdf(const Bsdf<NL> &b, int lobe, v3 wo, v3 wi) {
-    if (STD) return lobe != 8 ? std_lobe_pdf(b, lobe, wo, wi) : 0.f;
+    if (STD && lobe != 0) return lobe != 8 ? std_lobe_pdf(b, lobe, wo, wi) : 0.f;
     if (lobe == 0) return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.f;
     if (lobe == 1) {
         if (!same_hemi(wo, wi)) return 0.f;
@@ -918,6 +921,7 @@ __device__ __noinline__ void bsdf_sample(const Bsdf<NL> &b, v3 woW, v3 &wiW, flo
 struct Hit {
     v3 p, n, wo;   // pError is 0 for every hit (BVH::intersect computes gamma<int>(5) == 0)
     int prim;      // triangle id, or -2 - light for a sphere light
+    float b1, b2;  // barycentrics of the triangle's second and third vertex
 };
 
 // offset_point_origin (core/interaction.h:11-31) with pError = 0: the origin is p itself

@@ -21,6 +21,8 @@ class Scene:
     materials: list = field(default_factory=list)   # dicts: type, rgb, roughness, eta, k
     lights: list = field(default_factory=list)      # dicts: type, tri, radiance, radius, center
     camera: dict | None = None             # position, look_at, up, vfov, width, height
+    uvs: np.ndarray | None = None          # (n, 6) float32: (u, v) of each triangle's vertices
+    images: list = field(default_factory=list)      # (H, W, 3) uint8 arrays, rows from the top
 
     @property
     def n_tri(self) -> int:
@@ -35,6 +37,7 @@ class Scene:
             arr[i].eta = m.get("eta", 1.5)
             arr[i].k = m.get("k", 0.0)
             arr[i].standard = -1
+            arr[i].texture = m.get("texture", -1) + 1
         # StandardSurfaceMaterial parameters: materials with "standard" get consecutive indices
         k = 0
         for i, m in enumerate(self.materials):
@@ -56,7 +59,18 @@ class Scene:
                         getattr(arr[i], name)[:] = list(v)
                     else:
                         setattr(arr[i], name, v)
+            arr[i].kd_texture = p.get("kd_texture", -1) + 1
         return arr, len(stds)
+
+    def images_array(self):
+        """fl_image records of self.images plus the contiguous pixel buffers they point to"""
+        pix = [np.ascontiguousarray(im, np.uint8) for im in self.images]
+        arr = (T.fl_image * max(1, len(pix)))()
+        for i, p in enumerate(pix):
+            assert p.ndim == 3 and p.shape[2] == 3
+            arr[i].height, arr[i].width = p.shape[0], p.shape[1]
+            arr[i].rgb = p.ctypes.data_as(C.POINTER(C.c_uint8))
+        return arr, pix
 
     def lights_array(self):
         arr = (T.fl_light * max(1, len(self.lights)))()
@@ -88,7 +102,14 @@ class Scene:
         stds, n_std = self.standard_array()
         d.standard_surfaces = C.cast(stds, C.POINTER(T.fl_standard_surface))
         d.n_standard_surfaces = n_std
-        return d, (verts, tm, mats, lights, stds)
+        uvs = None
+        if self.uvs is not None:
+            uvs = np.ascontiguousarray(self.uvs, np.float32).reshape(self.n_tri, 6)
+            d.uvs = uvs.ctypes.data_as(C.POINTER(C.c_float))
+        imgs, pix = self.images_array()
+        d.images = C.cast(imgs, C.POINTER(T.fl_image))
+        d.n_images = len(self.images)
+        return d, (verts, tm, mats, lights, stds, uvs, imgs, pix)
 
     def camera_struct(self, width=None, height=None):
         c = self.camera
@@ -397,3 +418,47 @@ def caustic(width=1024, height=1024, slices=256, stacks=129) -> Scene:
     cam = {"position": (0.0, 3.0, -2.9), "look_at": (0.0, 1.0, 0.5), "up": (0.0, 1.0, 0.0), "vfov": 60.0,
            "width": width, "height": height}
     return Scene(verts, mats, materials, lights, cam)
+
+
+def texture_images(seed=11):
+    """two seeded RGB images: a 48 x 32 checkerboard of random colours (6 x 4 cells) and a
+    37 x 29 image of smooth colour ramps with noise (odd sizes exercise the texel rule)"""
+    rng = np.random.default_rng(seed)
+    cells = rng.integers(20, 236, size=(4, 6, 3))
+    checker = np.repeat(np.repeat(cells, 8, axis=0), 8, axis=1).astype(np.uint8)
+    y, x = np.mgrid[0:29, 0:37]
+    ramp = np.stack([x * 255 / 36, y * 255 / 28, (x + y) * 255 / 64], axis=-1)
+    ramp = np.clip(ramp + rng.normal(0, 12, ramp.shape), 0, 255).astype(np.uint8)
+    return [checker, ramp]
+
+
+def quad_uvs(n_tri):
+    """uvs of the _quad triangles (p0, p1, p2), (p0, p2, p3): the quad maps onto [0, 1]^2"""
+    one = np.array([[0, 0, 1, 0, 1, 1], [0, 0, 1, 1, 0, 1]], np.float32)
+    return np.tile(one, (n_tri // 2, 1))
+
+
+def cornell_textured(width=64, height=64) -> Scene:
+    """The Cornell box with image textures (ImageMapTexture): the back wall and the tall box
+    are Lambert with the checkerboard, the floor Lambert with the ramp image, the short box a
+    StandardSurface (Oren-Nayar diffuse + sheen) whose kd is the ramp image. Every quad maps
+    onto [0, 1]^2; on the box faces u runs over [-0.15, 1.15] and v over [0, 1.15], so that
+    the texel rule's clamps are reached. (v < 0 would send the reference past its image:
+    for a row past the last it resets the column instead of the row.)"""
+    sc = cornell(width, height, "lambert")
+    CHECKER, RAMP, STD = len(sc.materials), len(sc.materials) + 1, len(sc.materials) + 2
+    mats = list(sc.materials) + [
+        {"type": T.FL_MAT_LAMBERT, "texture": 0},
+        {"type": T.FL_MAT_LAMBERT, "texture": 1},
+        {"standard": {"kd_texture": 1, "kd_weight": 1.0, "kd_roughness": 0.4,
+                      "sheen_color": (0.9, 0.9, 1.0), "sheen_weight": 0.4, "sheen_roughness": 0.3}},
+    ]
+    tm = np.array(sc.tri_material, np.uint32)
+    tm[0:2] = RAMP       # floor
+    tm[4:6] = CHECKER    # back wall
+    tm[10:22] = STD      # short box
+    tm[22:34] = CHECKER  # tall box
+    uvs = quad_uvs(sc.n_tri)
+    uvs[10:34, 0::2] = uvs[10:34, 0::2] * 1.3 - 0.15   # u in [-0.15, 1.15]
+    uvs[10:34, 1::2] = uvs[10:34, 1::2] * 1.15          # v in [0, 1.15]
+    return Scene(sc.verts, tm, mats, sc.lights, sc.camera, uvs=uvs, images=texture_images())

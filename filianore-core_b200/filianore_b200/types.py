@@ -75,6 +75,15 @@ class fl_material(C.Structure):
         ("eta", C.c_float),
         ("k", C.c_float),
         ("standard", C.c_int32),
+        ("texture", C.c_int32),
+    ]
+
+
+class fl_image(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("rgb", C.POINTER(C.c_uint8)),
     ]
 
 
@@ -100,6 +109,7 @@ class fl_standard_surface(C.Structure):
         ("sheen_color", C.c_float * 3), ("sheen_weight", C.c_float), ("sheen_roughness", C.c_float),
         ("coat_color", C.c_float * 3), ("coat_weight", C.c_float), ("coat_ior", C.c_float), ("coat_gloss", C.c_float),
         ("thin_film_thickness", C.c_float), ("thin_film_ior", C.c_float), ("thin_walled", C.c_int32),
+        ("kd_texture", C.c_int32),
     ]
 
 
@@ -114,6 +124,9 @@ class fl_scene_desc(C.Structure):
         ("n_lights", C.c_uint32),
         ("standard_surfaces", C.POINTER(fl_standard_surface)),
         ("n_standard_surfaces", C.c_uint32),
+        ("uvs", C.POINTER(C.c_float)),
+        ("images", C.POINTER(fl_image)),
+        ("n_images", C.c_uint32),
     ]
 
 

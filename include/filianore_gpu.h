@@ -158,6 +158,7 @@ typedef struct {
     float coat_color[3], coat_weight, coat_ior, coat_gloss;
     float thin_film_thickness, thin_film_ior;
     int32_t thin_walled;
+    int32_t kd_texture;          /* 1 + index into fl_scene_desc.images: kd is that ImageMapTexture; 0: kd */
 } fl_standard_surface;
 
 typedef struct {
@@ -168,7 +169,20 @@ typedef struct {
     float eta;          /* dielectric IOR, or conductor eta */
     float k;            /* conductor absorption */
     int32_t standard;   /* FL_MAT_STANDARD: index into fl_scene_desc.standard_surfaces */
+    int32_t texture;    /* FL_MAT_LAMBERT: 1 + index into fl_scene_desc.images, the reflectance is that
+                           ImageMapTexture; 0: rgb */
 } fl_material;
+
+/* An RGB image for ImageMapTexture (shading/textures/imagemap.cpp:24-62): width x height
+ * pixels of 3 bytes, rows from the top, as stbi_load returns them. Looked up at the hit's
+ * uv by the reference's nearest-texel rule: i = int(u * width), j = int((1 - v) * height -
+ * 0.001), each clamped to the image (where the reference, for j past the last row, sets i
+ * to height - 1 and reads outside the image, the library clamps j as well), then
+ * from_reflectance_rgb of the texel / 255. */
+typedef struct {
+    int32_t width, height;
+    const uint8_t *rgb;
+} fl_image;
 
 enum {
     FL_LIGHT_TRIANGLE = 0, /* DiffuseAreaIlluminant over one scene triangle (illuminants/diffusearea.cpp) */
@@ -205,6 +219,12 @@ typedef struct {
     uint32_t n_lights;
     const fl_standard_surface *standard_surfaces;  /* for FL_MAT_STANDARD materials (nullable) */
     uint32_t n_standard_surfaces;
+    /* Texture coordinates: 6 floats per triangle, (u, v) of its three vertices (nullable).
+     * A hit at barycentrics (b1, b2) has uv = uv0 (1 - b1 - b2) + uv1 b1 + uv2 b2. The
+     * reference's BVH::intersect leaves uv at (0, 0); without uvs every hit has that uv. */
+    const float *uvs;
+    const fl_image *images;         /* textures (nullable) */
+    uint32_t n_images;
 } fl_scene_desc;
 
 typedef struct {

@@ -217,6 +217,15 @@ def write_scene_file(path, scene, params, nthreads=0, pixels=None, width=None, h
         stds, n_std = scene.standard_array()
         f.write(np.uint32(n_std).tobytes())
         f.write(bytes(stds)[: C.sizeof(T.fl_standard_surface) * n_std])
+        # texture coordinates and images
+        f.write(np.uint32(0 if scene.uvs is None else 1).tobytes())
+        if scene.uvs is not None:
+            f.write(np.ascontiguousarray(scene.uvs, np.float32).reshape(scene.n_tri, 6).tobytes())
+        f.write(np.uint32(len(scene.images)).tobytes())
+        for im in scene.images:
+            im = np.ascontiguousarray(im, np.uint8)
+            f.write(np.array([im.shape[1], im.shape[0]], np.int32).tobytes())
+            f.write(im.tobytes())
 
 
 def run_reference(scene_path, out_path, W, H, forge=False):

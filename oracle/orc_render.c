@@ -80,6 +80,7 @@ typedef struct {
     float t;
     v3 p, pError, wo, n, ns;
     int32_t prim;   /* triangle id, or -2 - light index for a sphere-light hit */
+    float b1, b2;   /* barycentrics of the triangle's second and third vertex */
 } isect_t;
 
 static float sphere_hit(const fl_light *L, const ray3 *r) {
@@ -132,8 +133,36 @@ static int scene_intersect(const scene_ctx *S, const ray3 *r, isect_t *is, uint6
         is->n = v3_norm(v3_cross(v3_sub(v1, v0), v3_sub(v2, v0)));
         is->prim = id;
     }
+    is->b1 = sphere >= 0 ? 0.f : u;
+    is->b2 = sphere >= 0 ? 0.f : v;
     is->ns = is->n;
     return 1;
+}
+
+/* The hit's texture coordinates uv0 (1 - b1 - b2) + uv1 b1 + uv2 b2 in this order; (0, 0)
+ * without uvs, as BVH::intersect (bvh/bvh.cpp:69-71) leaves them */
+static void hit_uv(const scene_ctx *S, const isect_t *is, float *u, float *v) {
+    *u = *v = 0.f;
+    if (!S->sc->uvs || is->prim < 0) return;
+    const float *t = S->sc->uvs + 6 * (size_t)is->prim;
+    float w = 1.f - is->b1 - is->b2;
+    *u = t[0] * w + t[2] * is->b1 + t[4] * is->b2;
+    *v = t[1] * w + t[3] * is->b1 + t[5] * is->b2;
+}
+
+/* ImageMapTexture::evaluate (shading/textures/imagemap.cpp:36-62): the nearest texel's RGB;
+ * for j past the last row the reference sets i = height - 1 and reads outside the image,
+ * here j is clamped too */
+static void image_texel(const fl_image *im, float u, float v, float rgb[3]) {
+    int i = (int)(u * (float)im->width);
+    int j = (int)((1.f - v) * (float)im->height - 0.001f);
+    if (i < 0) i = 0;
+    if (j < 0) j = 0;
+    if (i > im->width - 1) i = im->width - 1;
+    if (j > im->height - 1) { i = im->height - 1; j = im->height - 1; }
+    if (i > im->width - 1) i = im->width - 1;
+    const uint8_t *px = im->rgb + 3 * (size_t)i + 3 * (size_t)im->width * (size_t)j;
+    for (int k = 0; k < 3; ++k) rgb[k] = (float)(int)px[k] / 255.f;
 }
 
 static int32_t prim_light(const scene_ctx *S, int32_t prim) {
@@ -816,7 +845,13 @@ static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda
     b->ay = b->ax;
     b->eta = (m->type == FL_MAT_ROUGH_DIELECTRIC || m->type == FL_MAT_SMOOTH_DIELECTRIC) ? m->eta : 1.f;
     b->corrected = S->corrected;
-    if (m->type == FL_MAT_LAMBERT) {
+    if (m->type == FL_MAT_LAMBERT && m->texture > 0) {
+        /* LambertMaterial with an ImageMapTexture (materials/lambert.cpp:8-15) */
+        float u, v, rgb[3];
+        hit_uv(S, is, &u, &v);
+        image_texel(&S->sc->images[m->texture - 1], u, v, rgb);
+        orc_reflectance(S->tab, rgb, S->mode, lambda, b->R.c);
+    } else if (m->type == FL_MAT_LAMBERT) {
         if (S->mode == FL_SPECTRAL_BINS60) b->R = S->mat_refl60[mi];
         else orc_reflectance(S->tab, m->rgb, S->mode, lambda, b->R.c);
     } else {
@@ -828,7 +863,14 @@ static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda
         const fl_standard_surface *p = &S->sc->standard_surfaces[m->standard];
         b->eta = (p->ks_weight > 0 && p->kt_weight > 0) ? p->ks_ior : 1.f;
         b->mat_eta = p->ks_ior;
-        orc_reflectance(S->tab, p->kd, S->mode, lambda, b->kd.c);
+        if (p->kd_texture > 0) {
+            float u, v, rgb[3];
+            hit_uv(S, is, &u, &v);
+            image_texel(&S->sc->images[p->kd_texture - 1], u, v, rgb);
+            orc_reflectance(S->tab, rgb, S->mode, lambda, b->kd.c);
+        } else {
+            orc_reflectance(S->tab, p->kd, S->mode, lambda, b->kd.c);
+        }
         orc_reflectance(S->tab, p->ks, S->mode, lambda, b->ks.c);
         orc_reflectance(S->tab, p->kt, S->mode, lambda, b->kt.c);
         orc_reflectance(S->tab, p->sheen_color, S->mode, lambda, b->sheen.c);

@@ -6,7 +6,10 @@
  * pError = abs(p) * gamma<int>(5) (which is 0), n = normalize(Ng), and ray.tMax shrinks.
  * Two fields the reference leaves unset are filled in, without which it cannot render:
  *  - isect->primitive, from a geomID -> Primitive table the harness registers;
- *  - Shading.n = n (the reference's constructor call leaves it NaN).
+ *  - Shading.n = n (the reference's constructor call leaves it NaN);
+ *  - uv, from the triangle's vertex uvs and the hit's barycentrics (b1, b2) as
+ *    uv0 (1 - b1 - b2) + uv1 b1 + uv2 b2, when the harness registers uvs (it stays (0, 0)
+ *    otherwise, as BVH::intersect leaves it).
  * Ng = cross(v1 - v0, v2 - v0), the orientation Triangle::sample uses (triangle.cpp:146),
  * so one-sided area lights face the same way for NEE and for BSDF hits.
  * Test infrastructure only.
@@ -20,6 +23,7 @@
 
 namespace ref_shim {
 std::vector<const filianore::Primitive *> g_primitives;
+std::vector<float> g_uvs;  // 6 per triangle, or empty
 }
 
 void rtcReleaseScene(RTCScene scene) {
@@ -75,6 +79,11 @@ bool BVH::intersect(const Ray &ray, SurfaceInteraction *isect) const {
     isect->Shading.n = isect->n;
     coordinate_system(isect->n, &isect->dpdu, &isect->dpdv);
     isect->primitive = ref_shim::g_primitives[id];
+    if (!ref_shim::g_uvs.empty()) {
+        const float *q = ref_shim::g_uvs.data() + 6 * (size_t)id;
+        const float w = 1.f - u - v;
+        isect->uv = Vector2f(q[0] * w + q[2] * u + q[4] * v, q[1] * w + q[3] * u + q[5] * v);
+    }
     ray.tMax = isect->t;
     return true;
 }

@@ -57,6 +57,7 @@
 #include "filianore/shading/materials/standardsurface.h"
 #include "filianore/shading/microfacets/ggx.h"
 #include "filianore/shading/textures/constant.h"
+#include "filianore/shading/textures/imagemap.h"
 #include "filianore/shapes/triangle.h"
 #include "ext/pcg32.h"
 #include "../../include/filianore_gpu.h"
@@ -71,6 +72,7 @@
 
 namespace ref_shim {
 extern std::vector<const filianore::Primitive *> g_primitives;
+extern std::vector<float> g_uvs;
 }
 
 using namespace filianore;
@@ -272,8 +274,33 @@ int render(const char *scene_path, const char *out_path, bool forge) {
     std::vector<fl_standard_surface> stds;
     uint32_t n_std = 0;
     if (ok && fread(&n_std, sizeof(n_std), 1, f) == 1) ok = read_n(f, stds, n_std);
+    // optional: texture coordinates (6 per triangle) and RGB images, each written out as a
+    // binary PPM for the reference's own ImageMapTexture (stbi_load) to read
+    uint32_t has_uvs = 0, n_img = 0;
+    std::vector<std::string> image_paths;
+    if (ok && fread(&has_uvs, sizeof(has_uvs), 1, f) == 1) {
+        if (has_uvs) ok = read_n(f, ref_shim::g_uvs, (size_t)h.n_tri * 6);
+        if (ok && fread(&n_img, sizeof(n_img), 1, f) == 1) {
+            for (uint32_t i = 0; ok && i < n_img; ++i) {
+                int32_t wh[2];
+                std::vector<uint8_t> px;
+                ok = fread(wh, sizeof(int32_t), 2, f) == 2 && wh[0] > 0 && wh[1] > 0 &&
+                     read_n(f, px, (size_t)wh[0] * wh[1] * 3);
+                if (!ok) break;
+                const std::string path = std::string(out_path) + ".tex" + std::to_string(i) + ".ppm";
+                FILE *o = fopen(path.c_str(), "wb");
+                if (!o) { ok = false; break; }
+                fprintf(o, "P6\n%d %d\n255\n", wh[0], wh[1]);
+                fwrite(px.data(), 1, px.size(), o);
+                fclose(o);
+                image_paths.push_back(path);
+            }
+        }
+    }
     fclose(f);
     if (!ok) { fprintf(stderr, "truncated scene file\n"); return 2; }
+    std::vector<std::shared_ptr<Texture<PrincipalSpectrum>>> images;
+    for (const std::string &p : image_paths) images.push_back(std::make_shared<ImageMapTexture>(p.c_str()));
     if (h.spectral_mode != FL_SPECTRAL_BINS60) {
         fprintf(stderr, "the reference integrator only has 60-bin spectra\n");
         return 2;
@@ -285,7 +312,9 @@ int render(const char *scene_path, const char *out_path, bool forge) {
     std::vector<std::shared_ptr<Material>> materials;
     for (const auto &m : mats) {
         const float alpha = m.roughness * m.roughness;
-        if (m.type == FL_MAT_LAMBERT) {
+        if (m.type == FL_MAT_LAMBERT && m.texture > 0 && (size_t)m.texture <= images.size()) {
+            materials.push_back(std::make_shared<LambertMaterial>(images[m.texture - 1]));
+        } else if (m.type == FL_MAT_LAMBERT) {
             PrincipalSpectrum r = from_reflectance_rgb(Vector3f(m.rgb[0], m.rgb[1], m.rgb[2]));
             materials.push_back(
                 std::make_shared<LambertMaterial>(std::make_shared<ConstantTexture<PrincipalSpectrum>>(r)));
@@ -303,7 +332,9 @@ int render(const char *scene_path, const char *out_path, bool forge) {
             };
             auto flt = [](float v) { return std::make_shared<ConstantTexture<float>>(v); };
             materials.push_back(std::make_shared<StandardSurfaceMaterial>(
-                p.kd_weight, spec(p.kd), flt(p.kd_roughness), p.ks_weight, spec(p.ks), flt(p.ks_roughness),
+                p.kd_weight,
+                (p.kd_texture > 0 && (size_t)p.kd_texture <= images.size()) ? images[p.kd_texture - 1] : spec(p.kd),
+                flt(p.kd_roughness), p.ks_weight, spec(p.ks), flt(p.ks_roughness),
                 flt(p.ks_anisotropic), p.fresnel_type, p.ks_ior, p.metal_type, p.sheen_weight, spec(p.sheen_color),
                 flt(p.sheen_roughness), p.kt_weight, spec(p.kt), p.coat_weight, spec(p.coat_color), p.coat_ior,
                 p.coat_gloss, p.thin_film_thickness, p.thin_film_ior, p.thin_walled != 0, nullptr));

@@ -23,8 +23,12 @@ reference sources with oracle/Makefile). Outputs:
                         InitializeForge: zero metal spectra) and after InitializeForge
   metal_tables.npz      the measured metal curves of color/metallurgy.h (wavelengths, eta, k
                         per metal) and the 60-bin spectra InitializeForge makes of them
+  cornell_textured_ref.npz  the Cornell box with ImageMapTexture materials (Lambert and a
+                        StandardSurface kd) at 64x64 x 4 spp (float64): with texture
+                        coordinates ("uv") and without (every hit at uv (0, 0), as the
+                        reference's BVH::intersect leaves it: "nouv")
 Usage: python tests/golden/make_golden.py [part ...]   (parts: tables pcg cornell materials
-       delta metals standard; default all)
+       delta metals standard textures; default all)
 Scratch files go to oracle/_ref/tmp.
 """
 import os
@@ -135,8 +139,25 @@ def standard(tmp):
     np.savez_compressed(os.path.join(HERE, "cornell_standard_ref.npz"), **out)
 
 
+def textures(tmp):
+    """the box with image textures, with and without texture coordinates"""
+    out = {}
+    for key in ("uv", "nouv"):
+        sc = scenes.cornell_textured(64, 64)
+        if key == "nouv":
+            sc.uvs = None
+        p = scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60)
+        spath = os.path.join(tmp, f"tex_{key}.scene")
+        fpath = os.path.join(tmp, f"tex_{key}.film")
+        oracle.write_scene_file(spath, sc, p)
+        film, info = oracle.run_reference(spath, fpath, 64, 64)
+        out[f"{key}_xyz"] = film.astype(np.float64)
+        print("textured", key, info)
+    np.savez_compressed(os.path.join(HERE, "cornell_textured_ref.npz"), **out)
+
+
 PARTS = {"tables": tables, "pcg": pcg, "cornell": cornell, "materials": materials, "delta": delta,
-         "metals": metals, "standard": standard}
+         "metals": metals, "standard": standard, "textures": textures}
 
 
 def main(parts):

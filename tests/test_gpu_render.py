@@ -245,3 +245,33 @@ def test_thin_lens_matches_oracle(ctx, orc_tables, mode):
         with pytest.raises(fb.FlError):
             s.render(p)
         s.close()
+
+
+@pytest.mark.parametrize("key", ["uv", "nouv"])
+def test_image_textures_match_reference(ctx, orc_tables, key):
+    """ImageMapTexture on Lambert and StandardSurface kd: 60-bin parity build against the
+    reference's film (fixture), with and without texture coordinates, and the hero build
+    against the oracle; bounds as for the Lambert box (99.9% of pixels within 1e-4, mean
+    within 1e-4; hero 99% within 1e-3)."""
+    g = np.load(os.path.join(GOLDEN, "cornell_textured_ref.npz"))
+    sc = scenes.cornell_textured(64, 64)
+    if key == "nouv":
+        sc.uvs = None
+    xyz, _, stats = render_xyz(ctx, sc, scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60))
+    ref = g[f"{key}_xyz"]
+    assert close_fraction(xyz, ref, 1e-4, 1e-6) >= 0.999
+    assert abs(xyz.mean() / ref.mean() - 1) < 1e-4
+    p = scenes.render_params(8, 8, fb.FL_SPECTRAL_HERO4)
+    xh, _, _ = render_xyz(ctx, sc, p)
+    cpu, _ = oracle.render(sc, orc_tables, p)
+    assert close_fraction(xh, cpu, 1e-3, 1e-5) >= 0.99
+    assert abs(xh.mean() / cpu.mean() - 1) < 2e-3
+
+
+def test_texture_indices_are_validated(ctx):
+    sc = scenes.cornell_textured(8, 8)
+    for mats in ([dict(m) for m in sc.materials[:-1]] + [{"type": fb.FL_MAT_LAMBERT, "texture": 2}],
+                 [dict(m) for m in sc.materials[:-1]] + [{"standard": {"kd_texture": 5}}]):
+        bad = scenes.Scene(sc.verts, sc.tri_material, mats, sc.lights, sc.camera, uvs=sc.uvs, images=sc.images)
+        with pytest.raises(fb.FlError):
+            ctx.scene(bad)

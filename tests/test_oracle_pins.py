@@ -111,3 +111,18 @@ def test_oracle_measured_metals_equal_reference():
     film, _ = oracle.render(scenes.cornell(64, 64, "standard3"), tab, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60))
     assert np.array_equal(film, g["standard3_forge_xyz"])
     assert not np.array_equal(film, g["standard3_xyz"])
+
+
+def test_oracle_image_textures_equal_reference(orc_tables):
+    """ImageMapTexture (the reference's own class, reading the images through stbi_load) on
+    Lambert materials and a StandardSurface kd: bit-exact with texture coordinates (u over
+    [-0.15, 1.15] on the boxes, so the texel clamps are reached) and without them (every hit
+    at uv (0, 0), as the reference's BVH::intersect leaves it)."""
+    g = np.load(os.path.join(GOLDEN, "cornell_textured_ref.npz"))
+    for key in ("uv", "nouv"):
+        sc = scenes.cornell_textured(64, 64)
+        if key == "nouv":
+            sc.uvs = None
+        film, _ = oracle.render(sc, orc_tables, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60))
+        assert np.array_equal(film, g[f"{key}_xyz"]), (key, np.abs(film - g[f"{key}_xyz"]).max())
+    assert not np.array_equal(g["uv_xyz"], g["nouv_xyz"])
