@@ -354,8 +354,9 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
             set_error(ctx, "standard surface: unknown fresnel_type");
             return FL_ERR_INVALID;
         }
-        if (P.kd_texture < 0 || (P.kd_texture > 0 && (!d->images || (uint32_t)P.kd_texture > d->n_images))) {
-            set_error(ctx, "standard surface: kd texture index out of range");
+        if (P.kd_texture < 0 || (P.kd_texture > 0 && (!d->images || (uint32_t)P.kd_texture > d->n_images)) ||
+            P.bump_texture < 0 || (P.bump_texture > 0 && (!d->images || (uint32_t)P.bump_texture > d->n_images))) {
+            set_error(ctx, "standard surface: texture index out of range");
             return FL_ERR_INVALID;
         }
     }
@@ -452,6 +453,7 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
     for (uint32_t i = 0; i < n_std; ++i) {
         std_host.push_back(standard_dev(d->standard_surfaces[i]));
         std_host.back().kd_texture = d->standard_surfaces[i].kd_texture - 1;
+        std_host.back().bump_texture = d->standard_surfaces[i].bump_texture - 1;
     }
     s->n_standard = n_std;
     s->ext_kernels = n_std > 0;

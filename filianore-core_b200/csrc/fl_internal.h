@@ -92,6 +92,7 @@ struct StandardDev {
     float coat_weight, coat_ior, coat_gloss;  // coat_gloss = lerp(gloss, .1, .001)
     float tf_ior, tf_thickness;                // thin film over a medium of IOR ior
     int kd_texture;                            // image of kd, -1: the constant kd
+    int bump_texture;                          // bump map image (red channel), -1: none
     int basis[5][3];      // Smits terms of kd, ks, kt, sheen colour, coat colour
     float w[5][3];
 };

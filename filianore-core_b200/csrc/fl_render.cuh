@@ -306,9 +306,7 @@ __device__ inline void hit_uv(const JobDev &A, const Hit &h, float &u, float &v)
 // ImageMapTexture::evaluate (shading/textures/imagemap.cpp:36-62): the nearest texel, then
 // from_reflectance_rgb of it / 255, at the path's spectral samples. For j past the last row
 // the reference sets i = height - 1 and reads outside the image; here j is clamped too.
-template <int NL>
-__device__ inline void image_reflectance(const JobDev &A, const TablesArg &tab, const SmemTables &sm, int img, float u,
-                                         float v, float lambda0, Spec<NL> &out) {
+__device__ inline const unsigned char *image_texel(const JobDev &A, int img, float u, float v) {
     const ImageDev im = A.images[img];
     int i = (int)__fmul_rn(u, (float)im.width);
     int j = (int)__fsub_rn(__fmul_rn(__fsub_rn(1.f, v), (float)im.height), 0.001f);
@@ -317,7 +315,13 @@ __device__ inline void image_reflectance(const JobDev &A, const TablesArg &tab, 
     if (i > im.width - 1) i = im.width - 1;
     if (j > im.height - 1) { i = im.height - 1; j = im.height - 1; }
     if (i > im.width - 1) i = im.width - 1;
-    const unsigned char *px = A.pixels + im.offset + 3ull * ((unsigned long long)j * (unsigned)im.width + (unsigned)i);
+    return A.pixels + im.offset + 3ull * ((unsigned long long)j * (unsigned)im.width + (unsigned)i);
+}
+
+template <int NL>
+__device__ inline void image_reflectance(const JobDev &A, const TablesArg &tab, const SmemTables &sm, int img, float u,
+                                         float v, float lambda0, Spec<NL> &out) {
+    const unsigned char *px = image_texel(A, img, u, v);
     const float rgb[3] = {(float)(int)px[0] / 255.f, (float)(int)px[1] / 255.f, (float)(int)px[2] / 255.f};
     int basis[3];
     float w[3];
@@ -332,6 +336,40 @@ __device__ inline void image_reflectance(const JobDev &A, const TablesArg &tab, 
             out.c[k] = smits_at(sm, tab, basis, w, hero_lambda(lambda0, k));
         }
     }
+}
+
+// Material::bump_evaluate (materials/material.cpp:8-31) with the bump map's red channel as
+// height: the shading normal of a hit on triangle h.prim. dpdu, dpdv follow
+// Triangle::intersect (shapes/triangle.cpp:33-52) over the vertex uvs (all zero without uvs).
+static __device__ __noinline__ v3 bump_normal(const JobDev &A, const Hit &h, int img) {
+    const v3 p1 = tri_v(A.soup, (uint32_t)h.prim, 0), p2 = tri_v(A.soup, (uint32_t)h.prim, 1),
+             p3 = tri_v(A.soup, (uint32_t)h.prim, 2);
+    float uv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (A.uvs)
+        for (int k = 0; k < 6; ++k) uv[k] = __ldg(A.uvs + 6 * (size_t)h.prim + k);
+    const float duv02x = __fsub_rn(uv[0], uv[4]), duv02y = __fsub_rn(uv[1], uv[5]);
+    const float duv12x = __fsub_rn(uv[2], uv[4]), duv12y = __fsub_rn(uv[3], uv[5]);
+    const v3 dp02 = sub(p1, p3), dp12 = sub(p2, p3);
+    const float determinant = __fsub_rn(__fmul_rn(duv02x, duv12y), __fmul_rn(duv02y, duv12x));
+    const bool degenerate = fabs((double)determinant) < 1e-8;
+    v3 dpdu = mk(0.f, 0.f, 0.f), dpdv = mk(0.f, 0.f, 0.f);
+    if (!degenerate) {
+        const float invDet = __fdiv_rn(1.f, determinant);
+        dpdu = mul(sub(mul(dp02, duv12y), mul(dp12, duv02y)), invDet);
+        dpdv = mul(add(mul(dp02, -duv12x), mul(dp12, duv02x)), invDet);
+    }
+    if (degenerate || len2(cross(dpdu, dpdv)) == 0.f) coordinate_system(cross(sub(p2, p1), sub(p3, p1)), &dpdu, &dpdv);
+    float u, v;
+    hit_uv(A, h, u, v);
+    const float du = 0.0005f, dv = 0.0005f;
+    const float uDisplace = (float)(int)image_texel(A, img, __fadd_rn(u, du), v)[0] / 255.f;
+    const float vDisplace = (float)(int)image_texel(A, img, u, __fadd_rn(v, dv))[0] / 255.f;
+    const float displace = (float)(int)image_texel(A, img, u, v)[0] / 255.f;
+    const v3 bu = add(dpdu, mul(mul(h.n, __fdiv_rn(__fsub_rn(uDisplace, displace), du)), 4.f));
+    const v3 bv = add(dpdv, mul(mul(h.n, __fdiv_rn(__fsub_rn(vDisplace, displace), dv)), 4.f));
+    // set_shading_geometry (core/interaction.cpp:20-33): normal of (bu, bv) on n's side
+    const v3 ns = normalize(cross(bu, bv));
+    return dot(ns, h.n) < 0.f ? neg(ns) : ns;
 }
 
 template <int NL, bool STD>
@@ -373,6 +411,11 @@ __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const Sm
         b.n_rgb = tab.n_rgb;
         b.lambda0 = lambda0;
         b.kd_tex = sd->kd_texture >= 0;
+        if (sd->bump_texture >= 0 && h.prim >= 0) {
+            b.ns = bump_normal(A, h, sd->bump_texture);
+            coordinate_system(b.ns, &b.s, &b.t);
+            b.s = normalize(b.s);
+        }
         if (b.kd_tex) {
             float u, v;
             hit_uv(A, h, u, v);

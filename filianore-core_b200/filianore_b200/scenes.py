@@ -60,6 +60,7 @@ class Scene:
                     else:
                         setattr(arr[i], name, v)
             arr[i].kd_texture = p.get("kd_texture", -1) + 1
+            arr[i].bump_texture = p.get("bump_texture", -1) + 1
         return arr, len(stds)
 
     def images_array(self):
@@ -438,13 +439,15 @@ def quad_uvs(n_tri):
     return np.tile(one, (n_tri // 2, 1))
 
 
-def cornell_textured(width=64, height=64) -> Scene:
+def cornell_textured(width=64, height=64, bump=False) -> Scene:
     """The Cornell box with image textures (ImageMapTexture): the back wall and the tall box
     are Lambert with the checkerboard, the floor Lambert with the ramp image, the short box a
     StandardSurface (Oren-Nayar diffuse + sheen) whose kd is the ramp image. Every quad maps
     onto [0, 1]^2; on the box faces u runs over [-0.15, 1.15] and v over [0, 1.15], so that
     the texel rule's clamps are reached. (v < 0 would send the reference past its image:
-    for a row past the last it resets the column instead of the row.)"""
+    for a row past the last it resets the column instead of the row.) bump: the short box
+    also takes the ramp image's red channel as its bump map, and the tall box becomes a
+    bumped StandardSurface over the checkerboard (Fresnel-blended GGX)."""
     sc = cornell(width, height, "lambert")
     CHECKER, RAMP, STD = len(sc.materials), len(sc.materials) + 1, len(sc.materials) + 2
     mats = list(sc.materials) + [
@@ -458,6 +461,11 @@ def cornell_textured(width=64, height=64) -> Scene:
     tm[4:6] = CHECKER    # back wall
     tm[10:22] = STD      # short box
     tm[22:34] = CHECKER  # tall box
+    if bump:
+        mats[STD] = {"standard": dict(mats[STD]["standard"], bump_texture=1)}
+        mats.append({"standard": {"kd_texture": 0, "kd_weight": 0.8, "kd_roughness": 0.2, "ks": (0.9, 0.9, 0.9),
+                                  "ks_weight": 0.7, "ks_roughness": 0.3, "ks_ior": 1.5, "bump_texture": 0}})
+        tm[22:34] = len(mats) - 1
     uvs = quad_uvs(sc.n_tri)
     uvs[10:34, 0::2] = uvs[10:34, 0::2] * 1.3 - 0.15   # u in [-0.15, 1.15]
     uvs[10:34, 1::2] = uvs[10:34, 1::2] * 1.15          # v in [0, 1.15]

@@ -110,6 +110,7 @@ class fl_standard_surface(C.Structure):
         ("coat_color", C.c_float * 3), ("coat_weight", C.c_float), ("coat_ior", C.c_float), ("coat_gloss", C.c_float),
         ("thin_film_thickness", C.c_float), ("thin_film_ior", C.c_float), ("thin_walled", C.c_int32),
         ("kd_texture", C.c_int32),
+        ("bump_texture", C.c_int32),
     ]
 
 

@@ -159,6 +159,11 @@ typedef struct {
     float thin_film_thickness, thin_film_ior;
     int32_t thin_walled;
     int32_t kd_texture;          /* 1 + index into fl_scene_desc.images: kd is that ImageMapTexture; 0: kd */
+    int32_t bump_texture;        /* 1 + index into fl_scene_desc.images: the bump map, its height the red
+                                    byte / 255 of the texel (ImageMapTexture's rule); 0: none. The
+                                    shading normal follows Material::bump_evaluate (materials/
+                                    material.cpp:8-31) over dpdu, dpdv from the vertex uvs as
+                                    Triangle::intersect computes them (shapes/triangle.cpp:33-52) */
 } fl_standard_surface;
 
 typedef struct {

@@ -827,6 +827,43 @@ static void bsdf_sample(const bsdf_t *b, v3 woW, v3 *wiW, float ux, float uy, fl
     }
 }
 
+/* Material::bump_evaluate (materials/material.cpp:8-31) with the bump map's red channel as
+ * height: the shading normal of a triangle hit. dpdu, dpdv follow Triangle::intersect
+ * (shapes/triangle.cpp:33-52) over the vertex uvs (all zero without uvs). */
+static v3 bump_normal(const scene_ctx *S, const isect_t *is, const fl_image *im) {
+    const float *tv = S->sc->verts + 9 * (size_t)is->prim;
+    v3 p1 = v3m(tv[0], tv[1], tv[2]), p2 = v3m(tv[3], tv[4], tv[5]), p3 = v3m(tv[6], tv[7], tv[8]);
+    float uv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (S->sc->uvs) memcpy(uv, S->sc->uvs + 6 * (size_t)is->prim, sizeof(uv));
+    float duv02x = uv[0] - uv[4], duv02y = uv[1] - uv[5];
+    float duv12x = uv[2] - uv[4], duv12y = uv[3] - uv[5];
+    v3 dp02 = v3_sub(p1, p3), dp12 = v3_sub(p2, p3);
+    float determinant = duv02x * duv12y - duv02y * duv12x;
+    int degenerate = fabs((double)determinant) < 1e-8;
+    v3 dpdu = v3m(0.f, 0.f, 0.f), dpdv = v3m(0.f, 0.f, 0.f);
+    if (!degenerate) {
+        float invDet = 1.f / determinant;
+        dpdu = v3_mul(v3_sub(v3_mul(dp02, duv12y), v3_mul(dp12, duv02y)), invDet);
+        dpdv = v3_mul(v3_add(v3_mul(dp02, -duv12x), v3_mul(dp12, duv02x)), invDet);
+    }
+    if (degenerate || v3_len2(v3_cross(dpdu, dpdv)) == 0.f)
+        orc_coordinate_system(v3_cross(v3_sub(p2, p1), v3_sub(p3, p1)), &dpdu, &dpdv);
+    float u, v, rgb[3];
+    hit_uv(S, is, &u, &v);
+    const float du = 0.0005f, dv = 0.0005f;
+    image_texel(im, u + du, v, rgb);
+    float uDisplace = rgb[0];
+    image_texel(im, u, v + dv, rgb);
+    float vDisplace = rgb[0];
+    image_texel(im, u, v, rgb);
+    float displace = rgb[0];
+    v3 bu = v3_add(dpdu, v3_mul(v3_mul(is->n, (uDisplace - displace) / du), 4.f));
+    v3 bv = v3_add(dpdv, v3_mul(v3_mul(is->n, (vDisplace - displace) / dv), 4.f));
+    /* set_shading_geometry (core/interaction.cpp:20-33): the normal of (bu, bv) on n's side */
+    v3 ns = v3_norm(v3_cross(bu, bv));
+    return v3_dot(ns, is->n) < 0.f ? v3_neg(ns) : ns;
+}
+
 /* Material::compute_scattering_functions for the supported materials */
 static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda, bsdf_t *b) {
     b->nl = S->nl;
@@ -905,6 +942,11 @@ static void make_bsdf(const scene_ctx *S, const isect_t *is, const float *lambda
                 b->metal_k.c[i] = S->tab->metal[metal][1][bin];
                 b->wl[i] = lambda[i];
             }
+        }
+        if (p->bump_texture > 0 && is->prim >= 0) {
+            b->ns = bump_normal(S, is, &S->sc->images[p->bump_texture - 1]);
+            orc_coordinate_system(b->ns, &b->s, &b->t);
+            b->s = v3_norm(b->s);
         }
         b->tf_ior = p->thin_film_ior;
         b->tf_thickness = p->thin_film_thickness;
@@ -1208,6 +1250,7 @@ static void path_Li(const scene_ctx *S, const fl_render_params *P, v3 o, v3 d, f
         ++cn->bounces;
         bsdf_t b;
         make_bsdf(S, &is, lambda, &b);
+        is.ns = b.ns;  /* a bump map changed the shading normal (isect->Shading.n) */
         if (bsdf_num_components(&b, BSDF_ALL & ~BSDF_SPECULAR) > 0) {
             spec Ls;
             sp_set(&Ls, nl, 0.f);

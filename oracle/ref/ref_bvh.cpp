@@ -9,7 +9,10 @@
  *  - Shading.n = n (the reference's constructor call leaves it NaN);
  *  - uv, from the triangle's vertex uvs and the hit's barycentrics (b1, b2) as
  *    uv0 (1 - b1 - b2) + uv1 b1 + uv2 b2, when the harness registers uvs (it stays (0, 0)
- *    otherwise, as BVH::intersect leaves it).
+ *    otherwise, as BVH::intersect leaves it);
+ *  - dpdu, dpdv (and Shading.dpdu, Shading.dpdv) as Triangle::intersect computes them
+ *    (shapes/triangle.cpp:33-52) from the vertex uvs (all zero without uvs). Only the bump
+ *    map reads them.
  * Ng = cross(v1 - v0, v2 - v0), the orientation Triangle::sample uses (triangle.cpp:146),
  * so one-sided area lights face the same way for NEE and for BSDF hits.
  * Test infrastructure only.
@@ -77,7 +80,26 @@ bool BVH::intersect(const Ray &ray, SurfaceInteraction *isect) const {
     Vector3f v0(tv[0], tv[1], tv[2]), v1(tv[3], tv[4], tv[5]), v2(tv[6], tv[7], tv[8]);
     isect->n = normalize(cross(v1 - v0, v2 - v0));
     isect->Shading.n = isect->n;
-    coordinate_system(isect->n, &isect->dpdu, &isect->dpdv);
+    {
+        float q[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (!ref_shim::g_uvs.empty())
+            for (int k = 0; k < 6; ++k) q[k] = ref_shim::g_uvs[6 * (size_t)id + k];
+        const Vector2f duv02 = Vector2f(q[0], q[1]) - Vector2f(q[4], q[5]);
+        const Vector2f duv12 = Vector2f(q[2], q[3]) - Vector2f(q[4], q[5]);
+        const Vector3f dp02 = v0 - v2, dp12 = v1 - v2;
+        const float determinant = duv02.x * duv12.y - duv02.y * duv12.x;
+        const bool degenerate = std::abs(determinant) < 1e-8;
+        Vector3f dpdu(0.f), dpdv(0.f);
+        if (!degenerate) {
+            const float invDet = 1.f / determinant;
+            dpdu = (dp02 * duv12.y - dp12 * duv02.y) * invDet;
+            dpdv = (dp02 * -duv12.x + dp12 * duv02.x) * invDet;
+        }
+        if (degenerate || cross(dpdu, dpdv).length_squared() == 0)
+            coordinate_system(cross(v1 - v0, v2 - v0), &dpdu, &dpdv);
+        isect->dpdu = isect->Shading.dpdu = dpdu;
+        isect->dpdv = isect->Shading.dpdv = dpdv;
+    }
     isect->primitive = ref_shim::g_primitives[id];
     if (!ref_shim::g_uvs.empty()) {
         const float *q = ref_shim::g_uvs.data() + 6 * (size_t)id;

@@ -79,6 +79,27 @@ using namespace filianore;
 
 namespace {
 
+// The bump map's height: the red byte / 255 of the nearest texel, by ImageMapTexture's rule
+// (shading/textures/imagemap.cpp:36-62). The reference has no float image texture.
+class RedChannelTexture : public Texture<float> {
+public:
+    RedChannelTexture(int w, int h, std::vector<uint8_t> px) : w_(w), h_(h), px_(std::move(px)) {}
+    float evaluate(const SurfaceInteraction &isect) const {
+        int i = int(isect.uv.x * w_);
+        int j = int((1.f - isect.uv.y) * h_ - 0.001f);
+        if (i < 0) i = 0;
+        if (j < 0) j = 0;
+        if (i > w_ - 1) i = w_ - 1;
+        if (j > h_ - 1) { i = h_ - 1; j = h_ - 1; }
+        if (i > w_ - 1) i = w_ - 1;
+        return int(px_[3 * i + 3 * w_ * j]) / 255.f;
+    }
+
+private:
+    int w_, h_;
+    std::vector<uint8_t> px_;
+};
+
 class PCG32Sampler : public Sampler {
 public:
     void reset(uint64_t pixel, uint64_t sample) {
@@ -278,6 +299,7 @@ int render(const char *scene_path, const char *out_path, bool forge) {
     // binary PPM for the reference's own ImageMapTexture (stbi_load) to read
     uint32_t has_uvs = 0, n_img = 0;
     std::vector<std::string> image_paths;
+    std::vector<std::shared_ptr<Texture<float>>> heights;
     if (ok && fread(&has_uvs, sizeof(has_uvs), 1, f) == 1) {
         if (has_uvs) ok = read_n(f, ref_shim::g_uvs, (size_t)h.n_tri * 6);
         if (ok && fread(&n_img, sizeof(n_img), 1, f) == 1) {
@@ -294,6 +316,7 @@ int render(const char *scene_path, const char *out_path, bool forge) {
                 fwrite(px.data(), 1, px.size(), o);
                 fclose(o);
                 image_paths.push_back(path);
+                heights.push_back(std::make_shared<RedChannelTexture>(wh[0], wh[1], std::move(px)));
             }
         }
     }
@@ -337,7 +360,9 @@ int render(const char *scene_path, const char *out_path, bool forge) {
                 flt(p.kd_roughness), p.ks_weight, spec(p.ks), flt(p.ks_roughness),
                 flt(p.ks_anisotropic), p.fresnel_type, p.ks_ior, p.metal_type, p.sheen_weight, spec(p.sheen_color),
                 flt(p.sheen_roughness), p.kt_weight, spec(p.kt), p.coat_weight, spec(p.coat_color), p.coat_ior,
-                p.coat_gloss, p.thin_film_thickness, p.thin_film_ior, p.thin_walled != 0, nullptr));
+                p.coat_gloss, p.thin_film_thickness, p.thin_film_ior, p.thin_walled != 0,
+                (p.bump_texture > 0 && (size_t)p.bump_texture <= heights.size()) ? heights[p.bump_texture - 1]
+                                                                                   : nullptr));
         } else {
             fprintf(stderr, "unknown material type\n");
             return 2;

@@ -26,7 +26,8 @@ reference sources with oracle/Makefile). Outputs:
   cornell_textured_ref.npz  the Cornell box with ImageMapTexture materials (Lambert and a
                         StandardSurface kd) at 64x64 x 4 spp (float64): with texture
                         coordinates ("uv") and without (every hit at uv (0, 0), as the
-                        reference's BVH::intersect leaves it: "nouv")
+                        reference's BVH::intersect leaves it: "nouv"); the same with bump
+                        maps ("bump", "bump_nouv")
 Usage: python tests/golden/make_golden.py [part ...]   (parts: tables pcg cornell materials
        delta metals standard textures; default all)
 Scratch files go to oracle/_ref/tmp.
@@ -142,9 +143,9 @@ def standard(tmp):
 def textures(tmp):
     """the box with image textures, with and without texture coordinates"""
     out = {}
-    for key in ("uv", "nouv"):
-        sc = scenes.cornell_textured(64, 64)
-        if key == "nouv":
+    for key in ("uv", "nouv", "bump", "bump_nouv"):
+        sc = scenes.cornell_textured(64, 64, bump=key.startswith("bump"))
+        if key.endswith("nouv"):
             sc.uvs = None
         p = scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60)
         spath = os.path.join(tmp, f"tex_{key}.scene")

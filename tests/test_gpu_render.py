@@ -247,15 +247,15 @@ def test_thin_lens_matches_oracle(ctx, orc_tables, mode):
         s.close()
 
 
-@pytest.mark.parametrize("key", ["uv", "nouv"])
+@pytest.mark.parametrize("key", ["uv", "nouv", "bump", "bump_nouv"])
 def test_image_textures_match_reference(ctx, orc_tables, key):
-    """ImageMapTexture on Lambert and StandardSurface kd: 60-bin parity build against the
-    reference's film (fixture), with and without texture coordinates, and the hero build
-    against the oracle; bounds as for the Lambert box (99.9% of pixels within 1e-4, mean
-    within 1e-4; hero 99% within 1e-3)."""
+    """ImageMapTexture on Lambert and StandardSurface kd, and bump maps: 60-bin parity build
+    against the reference's film (fixture), with and without texture coordinates, and the
+    hero build against the oracle; bounds as for the Lambert box (99.9% of pixels within
+    1e-4, mean within 1e-4; hero 99% within 1e-3)."""
     g = np.load(os.path.join(GOLDEN, "cornell_textured_ref.npz"))
-    sc = scenes.cornell_textured(64, 64)
-    if key == "nouv":
+    sc = scenes.cornell_textured(64, 64, bump=key.startswith("bump"))
+    if key.endswith("nouv"):
         sc.uvs = None
     xyz, _, stats = render_xyz(ctx, sc, scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60))
     ref = g[f"{key}_xyz"]

@@ -117,11 +117,12 @@ def test_oracle_image_textures_equal_reference(orc_tables):
     """ImageMapTexture (the reference's own class, reading the images through stbi_load) on
     Lambert materials and a StandardSurface kd: bit-exact with texture coordinates (u over
     [-0.15, 1.15] on the boxes, so the texel clamps are reached) and without them (every hit
-    at uv (0, 0), as the reference's BVH::intersect leaves it)."""
+    at uv (0, 0), as the reference's BVH::intersect leaves it); and with bump maps, which run
+    the reference's own Material::bump_evaluate and set_shading_geometry."""
     g = np.load(os.path.join(GOLDEN, "cornell_textured_ref.npz"))
-    for key in ("uv", "nouv"):
-        sc = scenes.cornell_textured(64, 64)
-        if key == "nouv":
+    for key in ("uv", "nouv", "bump", "bump_nouv"):
+        sc = scenes.cornell_textured(64, 64, bump=key.startswith("bump"))
+        if key.endswith("nouv"):
             sc.uvs = None
         film, _ = oracle.render(sc, orc_tables, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60))
         assert np.array_equal(film, g[f"{key}_xyz"]), (key, np.abs(film - g[f"{key}_xyz"]).max())
