@@ -221,13 +221,23 @@ __device__ inline uint32_t load_count(const uint32_t *p) { return *(volatile con
 
 template <int NL>
 __device__ inline void load_spec(const float *a, uint32_t cap, uint32_t slot, Spec<NL> &s) {
+    // a slot's NL samples are contiguous (16-byte aligned): the shading kernels visit slots
+    // in material order, so one path's spectrum is one or a few sectors, not NL of them
+    static_assert(NL % 4 == 0, "spectra are stored as float4 groups");
+    (void)cap;
+    const float4 *p = reinterpret_cast<const float4 *>(a + (size_t)slot * NL);
 #pragma unroll
-    for (int k = 0; k < NL; ++k) s.c[k] = a[(size_t)k * cap + slot];
+    for (int k = 0; k < NL / 4; ++k) {
+        const float4 v = p[k];
+        s.c[4 * k] = v.x; s.c[4 * k + 1] = v.y; s.c[4 * k + 2] = v.z; s.c[4 * k + 3] = v.w;
+    }
 }
 template <int NL>
 __device__ inline void store_spec(float *a, uint32_t cap, uint32_t slot, const Spec<NL> &s) {
+    (void)cap;
+    float4 *p = reinterpret_cast<float4 *>(a + (size_t)slot * NL);
 #pragma unroll
-    for (int k = 0; k < NL; ++k) a[(size_t)k * cap + slot] = s.c[k];
+    for (int k = 0; k < NL / 4; ++k) p[k] = make_float4(s.c[4 * k], s.c[4 * k + 1], s.c[4 * k + 2], s.c[4 * k + 3]);
 }
 
 template <int NL>
@@ -481,11 +491,11 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
         A.lambda0[k] = 380.f + ul * 340.f;
         A.eta_scale[k] = 1.f;
         A.flags[k] = 0u;
-#pragma unroll
-        for (int c = 0; c < NL; ++c) {
-            A.beta[(size_t)c * A.cap + k] = 1.f;
-            A.L[(size_t)c * A.cap + k] = 0.f;
-        }
+        Spec<NL> one, zero;
+        one.set(1.f);
+        zero.set(0.f);
+        store_spec<NL>(A.beta, A.cap, k, one);
+        store_spec<NL>(A.L, A.cap, k, zero);
         A.ray_o[k] = make_float4(o.x, o.y, o.z, 0.f);
         A.ray_d[k] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
         A.q_trace[k] = k;
