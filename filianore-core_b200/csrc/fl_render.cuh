@@ -138,21 +138,31 @@ struct WaveDesc {
     WaveSeg seg[kMaxSegs];
 };
 
+// A path's scalar state in one 32-byte record, so that a shading kernel, which visits
+// slots in material order, reads it from one sector.
+struct alignas(32) PathHead {
+    unsigned long long rng;  // PCG32 state (increment 3)
+    float lambda0;           // hero wavelength
+    uint32_t flags;          // bits 0..7 bounce, bit 8 specular, bits 9..10 Lambert vertices (guiding)
+    uint32_t pixel;
+    uint32_t job;
+    float eta_scale;
+    uint32_t pad;
+};
+static_assert(sizeof(PathHead) == 32, "one sector per path");
+
 struct RenderArgs {
     TablesArg tab;
     const JobDev *jobs;      // device, kMaxJobs entries
     const WaveDesc *wave;    // device
     int nl;                  // pending-term slots per path: the most lights of any job
     uint32_t cap;            // paths per wave
-    // path state (slot-indexed, component-major for spectra: x[k * cap + slot])
-    uint32_t *pixel;
-    uint16_t *job;
-    unsigned long long *rng;
-    float *beta, *L, *lambda0, *eta_scale;
-    uint32_t *flags;  // bits 0..7 bounce, bit 8 specular
+    // path state, slot-indexed; a slot's spectra are contiguous: x[slot * NL + k]
+    PathHead *head;
+    float *beta, *L;
     float4 *ray_o, *ray_d;
     int4 *hit;
-    // pending NEE terms: C*[(li * NL + k) * cap + slot], pflags[li * cap + slot]
+    // pending NEE terms: C*[(li * cap + slot) * NL + k], pflags[li * cap + slot]
     float *CL, *CS;
     uint32_t *pflags;
     // shadow / MIS rays
@@ -244,8 +254,8 @@ template <int NL>
 __device__ inline void finish_path(const RenderArgs &A, const JobDev &J, const SmemTables &sm, uint32_t slot,
                                    const Spec<NL> &L) {
     double xyz[3];
-    spectrum_xyz<NL>(sm, A.tab, A.lambda0[slot], L, xyz);
-    const uint32_t pix = A.pixel[slot];
+    spectrum_xyz<NL>(sm, A.tab, A.head[slot].lambda0, L, xyz);
+    const uint32_t pix = A.head[slot].pixel;
     atomicAdd(&J.film[3 * (size_t)pix + 0], xyz[0]);
     atomicAdd(&J.film[3 * (size_t)pix + 1], xyz[1]);
     atomicAdd(&J.film[3 * (size_t)pix + 2], xyz[2]);
@@ -485,12 +495,15 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
                                J.cam.origin),
                            offset);
         const v3 d = normalize(dir);
-        A.pixel[k] = pix;
-        A.job[k] = (uint16_t)sg.job;
-        A.rng[k] = rng.state;
-        A.lambda0[k] = 380.f + ul * 340.f;
-        A.eta_scale[k] = 1.f;
-        A.flags[k] = 0u;
+        PathHead ph;
+        ph.rng = rng.state;
+        ph.lambda0 = 380.f + ul * 340.f;
+        ph.flags = 0u;
+        ph.pixel = pix;
+        ph.job = sg.job;
+        ph.eta_scale = 1.f;
+        ph.pad = 0u;
+        A.head[k] = ph;
         Spec<NL> one, zero;
         one.set(1.f);
         zero.set(0.f);
@@ -551,7 +564,7 @@ struct PathTraceItem {
     TravState st;
     __device__ bool begin(uint32_t q) {
         slot = A->q_trace[q];
-        J = &A->jobs[A->job[slot]];
+        J = &A->jobs[A->head[slot].job];
         nodes = J->nodes;
         n_nodes = J->n_nodes;
         tris = J->tris;
@@ -570,7 +583,7 @@ struct PathTraceItem {
             const uint32_t mi = res.id >= 0 ? J->tri_material[res.id] : 0u;
             const MaterialDev &m = J->materials[mi];
             cls = (m.type == FL_MAT_LAMBERT && m.texture >= 0) ? kClassStandard : 1 + m.type;
-            if (cls == 1 + FL_MAT_LAMBERT && A->g.select > 0.f && lambert_count(A->flags[slot]) >= kGuidedVertices)
+            if (cls == 1 + FL_MAT_LAMBERT && A->g.select > 0.f && lambert_count(A->head[slot].flags) >= kGuidedVertices)
                 cls = kClassLambertLate;
         }
         const uint32_t pos = coalesced_append_class(A->cnt->n_class, cls);
@@ -616,9 +629,9 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
             int c = 0;
             while (q >= off[c + 1]) ++c;
             slot = A.q_class[(size_t)c * A.cap + (q - off[c])];
-            const JobDev &J = A.jobs[A.job[slot]];
+            const JobDev &J = A.jobs[A.head[slot].job];
             const int4 h = A.hit[slot];
-            const uint32_t fl = A.flags[slot];
+            const uint32_t fl = A.head[slot].flags;
             const uint32_t bounce = fl & 0xffu;
             const bool specular = (fl >> 8) & 1u;
             const float4 o4 = A.ray_o[slot], d4 = A.ray_d[slot];
@@ -648,12 +661,12 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                 ++shaded;
                 alive = true;
                 store_spec<NL>(A.L, A.cap, slot, L);
-                const float lambda0 = A.lambda0[slot];
+                const float lambda0 = A.head[slot].lambda0;
                 Bsdf<NL> b;
                 make_bsdf<NL, STD>(J, A.tab, sm, hr, lambda0, b);
                 if (bsdf_num_components<STD>(b, kBsdfAll & ~kBsdfSpecular) > 0) {
                     Pcg32 rng;
-                    rng.state = A.rng[slot];
+                    rng.state = A.head[slot].rng;
                     rng.inc = 3u;
                     const int bsdfFlags = kBsdfAll & ~kBsdfSpecular;
                     for (int li = 0; li < J.n_lights; ++li) {
@@ -744,7 +757,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                         if (pf & kHasCL) store_spec<NL>(A.CL + (size_t)li * NL * A.cap, A.cap, slot, CL);
                         if (pf & kHasCS) store_spec<NL>(A.CS + (size_t)li * NL * A.cap, A.cap, slot, CS);
                     }
-                    A.rng[slot] = rng.state;
+                    A.head[slot].rng = rng.state;
                 }
             }
         }
@@ -770,7 +783,7 @@ struct NeeRayItem {
         const uint32_t tag = A->stag[q];
         kind = tag & 1u;
         sl = tag >> 1;  // li * cap + slot
-        J = &A->jobs[A->job[sl % A->cap]];
+        J = &A->jobs[A->head[sl % A->cap].job];
         nodes = J->nodes;
         n_nodes = J->n_nodes;
         tris = J->tris;
@@ -874,13 +887,13 @@ __global__ void __launch_bounds__(32 * kInferWarps, 3) k_guide_infer(RenderArgs 
         __half *row = X + (lane & 15) * kLdIn;
         if (valid) {
             slot = q[i];
-            const JobDev &J = A.jobs[A.job[slot]];
+            const JobDev &J = A.jobs[A.head[slot].job];
             const Hit hr = make_hit(J, A.ray_o[slot], A.ray_d[slot], A.hit[slot]);
             const v3 nf = dot(hr.n, hr.wo) < 0.f ? neg(hr.n) : hr.n;
             float pn[3];
             guide_normalise(A.g.bmin, A.g.binv, hr.p, pn);
             const float nn[3] = {nf.x, nf.y, nf.z};
-            guide_encode_part(pn, nn, (A.lambda0[slot] - 380.f) * (1.f / 340.f), lane >> 4, row);
+            guide_encode_part(pn, nn, (A.head[slot].lambda0 - 380.f) * (1.f / 340.f), lane >> 4, row);
         } else {
             uint4 *d = reinterpret_cast<uint4 *>(row + 40 * (lane >> 4));
 #pragma unroll
@@ -905,13 +918,13 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
         uint32_t slot = 0;
         if (active) {
             slot = A.q_cont[STD ? A.cap - 1 - q : q];
-            const JobDev &J = A.jobs[A.job[slot]];
+            const JobDev &J = A.jobs[A.head[slot].job];
             const int4 h = A.hit[slot];
-            const uint32_t fl = A.flags[slot];
+            const uint32_t fl = A.head[slot].flags;
             const uint32_t bounce = fl & 0xffu;
             const float4 o4 = A.ray_o[slot], d4 = A.ray_d[slot];
             const Hit hr = make_hit(J, o4, d4, h);
-            const float lambda0 = A.lambda0[slot];
+            const float lambda0 = A.head[slot].lambda0;
             Bsdf<NL> b;
             make_bsdf<NL, STD>(J, A.tab, sm, hr, lambda0, b);
             Spec<NL> beta, L;
@@ -945,7 +958,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             }
             // continuation (pathintegrator.cpp:46-84)
             Pcg32 rng;
-            rng.state = A.rng[slot];
+            rng.state = A.head[slot].rng;
             rng.inc = 3u;
             const v3 wo = mk(-d4.x, -d4.y, -d4.z);
             v3 wi = mk(0.f, 0.f, 0.f);
@@ -991,7 +1004,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                         guide_record(A, slot, hr, lambda0, wi, pdf, beta, L);
                 }
                 const bool spec_b = (sflags & kBsdfSpecular) != 0;
-                float etaScale = A.eta_scale[slot];
+                float etaScale = A.head[slot].eta_scale;
                 if ((sflags & kBsdfSpecular) && (sflags & kBsdfTransmission)) {
                     const float eta = b.eta;
                     etaScale *= (dot(wo, hr.n) > 0) ? (eta * eta) : 1.f / (eta * eta);
@@ -1012,18 +1025,18 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                 if (!stop) {
                     alive = true;
                     store_spec<NL>(A.beta, A.cap, slot, beta);
-                    A.eta_scale[slot] = etaScale;
+                    A.head[slot].eta_scale = etaScale;
                     uint32_t nfl = (bounce + 1u) | (spec_b ? 0x100u : 0u);
                     if constexpr (GUIDE) {
                         const uint32_t lc = lambert_count(fl) + (!STD && b.type == FL_MAT_LAMBERT ? 1u : 0u);
                         nfl |= (lc < 3u ? lc : 3u) << 9;
                     }
-                    A.flags[slot] = nfl;
+                    A.head[slot].flags = nfl;
                     A.ray_o[slot] = make_float4(no.x, no.y, no.z, kShadowEpsilon);
                     A.ray_d[slot] = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
                 }
             }
-            A.rng[slot] = rng.state;
+            A.head[slot].rng = rng.state;
             if (alive) store_spec<NL>(A.L, A.cap, slot, L);
             else finish_path<NL>(A, J, sm, slot, L);
         }
@@ -1050,7 +1063,7 @@ inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // bytes of wave state per path slot
 inline size_t wave_bytes_per_slot(int NL, int nl) {
-    return 94 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
+    return 100 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
 }
 
 // The device buffers of a wavefront: job table, wave descriptor, path state and queues.
@@ -1084,9 +1097,7 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
     auto take = [&](size_t bytes) { size_t o = off; off += align_up(bytes ? bytes : 1); return o; };
     const size_t o_cnt = take(sizeof(WaveCounters)), o_jobs = take(sizeof(JobDev) * kMaxJobs),
                  o_wave = take(sizeof(WaveDesc));
-    const size_t o_pixel = take(4 * cap), o_job = take(2 * cap), o_rng = take(8 * cap), o_beta = take(4 * NL * cap),
-                 o_L = take(4 * NL * cap);
-    const size_t o_lam = take(4 * cap), o_eta = take(4 * cap), o_flags = take(4 * cap);
+    const size_t o_head = take(sizeof(PathHead) * cap), o_beta = take(4 * NL * cap), o_L = take(4 * NL * cap);
     const size_t o_ro = take(16 * cap), o_rd = take(16 * cap), o_hit = take(16 * cap);
     const size_t o_CL = take(4 * (size_t)NL * nl * cap), o_CS = take(4 * (size_t)NL * nl * cap);
     const size_t o_pf = take(4 * (size_t)nl * cap);
@@ -1115,14 +1126,9 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
     A.cap = (uint32_t)cap;
     A.scap = (uint32_t)scap;
     A.cnt = reinterpret_cast<WaveCounters *>(B + o_cnt);
-    A.pixel = reinterpret_cast<uint32_t *>(B + o_pixel);
-    A.job = reinterpret_cast<uint16_t *>(B + o_job);
-    A.rng = reinterpret_cast<unsigned long long *>(B + o_rng);
+    A.head = reinterpret_cast<PathHead *>(B + o_head);
     A.beta = reinterpret_cast<float *>(B + o_beta);
     A.L = reinterpret_cast<float *>(B + o_L);
-    A.lambda0 = reinterpret_cast<float *>(B + o_lam);
-    A.eta_scale = reinterpret_cast<float *>(B + o_eta);
-    A.flags = reinterpret_cast<uint32_t *>(B + o_flags);
     A.ray_o = reinterpret_cast<float4 *>(B + o_ro);
     A.ray_d = reinterpret_cast<float4 *>(B + o_rd);
     A.hit = reinterpret_cast<int4 *>(B + o_hit);
