@@ -593,7 +593,7 @@ struct PathTraceItem {
 
 // camera and continuation rays: closest hit (persistent, lanes refilled as rays finish)
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_trace_paths(RenderArgs A) {
+__global__ void __launch_bounds__(128, 7) k_trace_paths(RenderArgs A) {
     const uint32_t n = load_count(&A.cnt->n_trace);
     bool err = false;
     TraceStats st;
@@ -821,7 +821,7 @@ struct NeeRayItem {
 
 // shadow rays (kind 0) and MIS rays (kind 1), persistent
 template <bool COUNT>
-__global__ void __launch_bounds__(128) k_trace_rays2(RenderArgs A) {
+__global__ void __launch_bounds__(128, 7) k_trace_rays2(RenderArgs A) {
     const uint32_t n = min(load_count(&A.cnt->n_shadow), A.scap);
     bool err = false;
     TraceStats st;
