@@ -287,8 +287,8 @@ class Guide:
     """Learned path guide (fl_guide_*): an MLP proposal for continuation directions at Lambert
     vertices, trained online on the renderer's own samples."""
 
-    def __init__(self, ctx: Context, seed: int = 1, learning_rate: float = 1e-2, select_prob: float = 0.5,
-                 batch: int = 16384, max_records: int = 1 << 20, steps_per_wave: int = 16,
+    def __init__(self, ctx: Context, seed: int = 1, learning_rate: float = 1e-3, select_prob: float = 0.5,
+                 batch: int = 32768, max_records: int = 1 << 20, steps_per_wave: int = 16,
                  position_scale: float = 1.0 / 16, weight_average: float = 0.99):
         self.ctx = ctx
         self.h = None

@@ -89,12 +89,13 @@ def test_untrained_guide_is_unbiased(ctx):
 
 def test_trained_guide_lowers_caustic_error(ctx):
     """Caustic scene (glass sphere under a tiny, bright sphere light), 256 x 256: after online
-    training (48 passes of 4 spp, rendering with the weight average), the guided render's
-    mean squared error against a 4096-spp plain render is below the plain render's at the
-    same 64 samples per pixel: below 0.92 x over the image and 0.85 x in the caustic (the
-    brightest 3% of the reference). Errors are averaged over six renders per estimator, and
-    the guided one over two independently trained guides: training order varies from run to
-    run (atomics), and single guides measured 0.72-0.87 x over the image."""
+    training (48 passes of 4 spp; Adam lr 1e-3, batches of 32 K records; rendering with the
+    weight average), the guided render's mean squared error against a 4096-spp plain render
+    is below the plain render's at the same 64 samples per pixel: below 0.85 x over the image
+    and 0.75 x in the caustic (the brightest 3% of the reference). Errors are averaged over
+    six renders per estimator, and the guided one over two independently trained guides:
+    training order varies from run to run (atomics). Six single guides measured 0.48-0.67 x
+    over the image and 0.43-0.57 x in the caustic."""
     R = 256
     sc = scenes.caustic(R, R, slices=128, stacks=65)
     s = ctx.scene(sc)
@@ -116,8 +117,8 @@ def test_trained_guide_lowers_caustic_error(ctx):
                                                film_xyz64=f))
     e_guided = []
     for seed in (5, 6):
-        g = fb.Guide(ctx, seed=seed, select_prob=0.5, batch=16384, max_records=1 << 19, steps_per_wave=32,
-                     weight_average=0.99)
+        g = fb.Guide(ctx, seed=seed, learning_rate=1e-3, select_prob=0.5, batch=32768, max_records=1 << 19,
+                     steps_per_wave=32, weight_average=0.99)
         for k in range(48):
             flags = fb.FL_GUIDE_TRAIN | (fb.FL_GUIDE_SAMPLE if k > 0 else 0)
             g.render(s, scenes.render_params(4, 8, fb.FL_SPECTRAL_HERO4, sample_offset=(1 << 16) + 4 * k), flags)
@@ -126,7 +127,7 @@ def test_trained_guide_lowers_caustic_error(ctx):
             s, scenes.render_params(64, 8, fb.FL_SPECTRAL_HERO4, sample_offset=off), fb.FL_GUIDE_SAMPLE, film_xyz64=f)))
         g.close()
     ratio = np.mean(e_guided, axis=0) / e_plain
-    assert ratio[0] < 0.92 and ratio[1] < 0.85, (ratio, e_guided, e_plain)
+    assert ratio[0] < 0.85 and ratio[1] < 0.75, (ratio, e_guided, e_plain)
     s.close()
 
 
