@@ -37,3 +37,30 @@ def test_status_strings_and_no_device_error():
     # null tables are rejected before any device work
     h = ctypes.c_void_p()
     assert lib.fl_context_create(0, None, ctypes.byref(h)) == fb.FL_ERR_INVALID
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """Every ctypes mirror in filianore_b200.types has the C struct's size and field offsets:
+    a C program built against include/filianore_gpu.h prints them (gcc, no GPU)."""
+    import subprocess
+
+    from filianore_b200 import types as T
+    structs = [(name, cls) for name, cls in vars(T).items()
+               if isinstance(cls, type) and issubclass(cls, ctypes.Structure) and name.startswith("fl_")]
+    assert len(structs) >= 10
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "filianore_gpu.h"', "int main(void) {"]
+    for name, cls in structs:
+        lines.append(f'    printf("{name} %zu\\n", sizeof({name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'    printf("{name}.{field} %zu\\n", offsetof({name}, {field}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                                text=True).stdout.splitlines())
+    for name, cls in structs:
+        assert int(got[name]) == ctypes.sizeof(cls), name
+        for field, _ in cls._fields_:
+            assert int(got[f"{name}.{field}"]) == getattr(cls, field).offset, (name, field)
