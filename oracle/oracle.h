@@ -106,6 +106,8 @@ void orc_xyz_from_spectrum(const orc_tables *t, int mode, const float *lambda, c
 
 /* f(wo, wi) |cos theta_i| of a non-Lambert material in its local frame, n directions */
 void orc_bsdf_fcos(const fl_material *m, const float wo[3], uint32_t n, const float *wi, int corrected, float *out);
+/* ImageMapTexture's texel rule (RGB / 255) at n uv pairs */
+void orc_image_texels(const fl_image *im, const float *uv, uint32_t n, float *rgb);
 
 /* ---------------------------------------------------------------- guiding (orc_guide.c) */
 /* 1: evaluate without the GPU's FP16 roundings (for finite-difference checks) */

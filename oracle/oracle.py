@@ -60,6 +60,7 @@ def lib():
         L.orc_guide_gradient.restype = C.c_float
         L.orc_guide_set_exact.argtypes = [C.c_int]
         L.orc_bsdf_fcos.argtypes = [P(T.fl_material), P(C.c_float), C.c_uint32, P(C.c_float), C.c_int, P(C.c_float)]
+        L.orc_image_texels.argtypes = [P(T.fl_image), P(C.c_float), C.c_uint32, P(C.c_float)]
         _lib = L
     return _lib
 
@@ -318,3 +319,13 @@ def bsdf_fcos(material, wo, wi, corrected=False):
     lib().orc_bsdf_fcos(C.byref(material), _fp(o), w.shape[0], _fp(w), 1 if corrected else 0, _fp(out))
     return out
 
+
+
+def image_texels(image, uv):
+    """the oracle's ImageMapTexture texel (RGB / 255) at each (u, v) row of uv"""
+    im = np.ascontiguousarray(image, np.uint8)
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    rec = T.fl_image(im.shape[1], im.shape[0], im.ctypes.data_as(C.POINTER(C.c_uint8)))
+    out = np.zeros((uv.shape[0], 3), np.float32)
+    lib().orc_image_texels(C.byref(rec), _fp(uv), uv.shape[0], _fp(out))
+    return out

@@ -827,6 +827,11 @@ static void bsdf_sample(const bsdf_t *b, v3 woW, v3 *wiW, float ux, float uy, fl
     }
 }
 
+/* the texel rule for n uv pairs (tests) */
+void orc_image_texels(const fl_image *im, const float *uv, uint32_t n, float *rgb) {
+    for (uint32_t i = 0; i < n; ++i) image_texel(im, uv[2 * i], uv[2 * i + 1], rgb + 3 * (size_t)i);
+}
+
 /* Material::bump_evaluate (materials/material.cpp:8-31) with the bump map's red channel as
  * height: the shading normal of a triangle hit. dpdu, dpdv follow Triangle::intersect
  * (shapes/triangle.cpp:33-52) over the vertex uvs (all zero without uvs). */

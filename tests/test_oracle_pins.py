@@ -127,3 +127,22 @@ def test_oracle_image_textures_equal_reference(orc_tables):
         film, _ = oracle.render(sc, orc_tables, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60))
         assert np.array_equal(film, g[f"{key}_xyz"]), (key, np.abs(film - g[f"{key}_xyz"]).max())
     assert not np.array_equal(g["uv_xyz"], g["nouv_xyz"])
+
+
+def test_texel_rule_edges():
+    """ImageMapTexture's nearest-texel rule (shading/textures/imagemap.cpp:36-62) on a 5 x 3
+    image whose texels encode their column and row: i = int(u * width) and j = int((1 - v) *
+    height - 0.001), truncated toward zero and clamped to the image. For a row past the last
+    (v < 0) the reference sets i = height - 1 and reads outside the image; the oracle (like
+    the library) clamps j as well and returns the texel (min(height - 1, width - 1), last row)."""
+    W, H = 5, 3
+    img = np.zeros((H, W, 3), np.uint8)
+    for j in range(H):
+        for i in range(W):
+            img[j, i] = (10 * i, 10 * j, 7)
+    cases = [((0.0, 0.0), (0, 2)), ((0.99, 0.99), (4, 0)), ((0.5, 0.5), (2, 1)), ((-0.3, 0.5), (0, 1)),
+             ((1.7, 0.5), (4, 1)), ((0.5, 1.8), (2, 0)), ((0.2, 2 / 3), (1, 0)), ((0.2, 0.3333), (1, 1)),
+             ((0.9, -0.2), (2, 2)), ((0.1, -5.0), (2, 2))]
+    got = oracle.image_texels(img, np.array([c[0] for c in cases], np.float32))
+    for (uv, (i, j)), rgb in zip(cases, got):
+        assert np.array_equal(rgb, img[j, i] / np.float32(255.0)), (uv, i, j, rgb * 255)
