@@ -434,3 +434,6 @@ class Server:
         st = T.fl_server_stats()
         lib().fl_server_get_stats(self.h, C.byref(st))
         return {k: getattr(st, k) for k, _ in T.fl_server_stats._fields_}
+
+
+from . import scenes  # noqa: E402,F401  (scene generators: fb.scenes.cornell, ...)
