@@ -84,3 +84,28 @@ def test_job_too_large_is_rejected():
     assert e.value.status == fb.FL_ERR_CAPACITY
     srv.close()
     ctx.close()
+
+
+def test_served_standard_surface_and_textures_equal_plain_render():
+    """Scenes with StandardSurface materials (thin walls, measured copper under a thin film,
+    with the measured metal curves), image textures and bump maps, served in one mix: the
+    server keeps its own copies of the StandardSurface records, texture coordinates and
+    images, and each job's image equals fl_render's."""
+    ctx = fb.Context(0, tables=fb.reference_tables(measured_metals=True))
+    srv = fb.Server(ctx, budget_bytes=2 << 30, max_depth=8, max_jobs=8, max_lights=4, wave_paths=1 << 16)
+    scs = [scenes.cornell_textured(48, 48, bump=True), scenes.cornell(40, 40, "standard3"),
+           scenes.cornell(40, 40, "standard")]
+    ids = [srv.add_scene(sc) for sc in scs]   # the scene objects' buffers may go after this
+    jobs = []
+    for sid, sc, spp in zip(ids, scs, (8, 6, 4)):
+        cam = sc.camera_struct()
+        p = scenes.render_params(spp, 8, fb.FL_SPECTRAL_HERO4)
+        jobs.append((srv.submit(sid, cam, p), sc, cam, p))
+    for jid, sc, cam, p in jobs:
+        rgb, xyz, _ = srv.wait(jid, timeout_ms=60000, want_xyz=True)
+        want_rgb, want_xyz = alone(ctx, sc, cam, p)
+        assert want_xyz.mean() > 0
+        np.testing.assert_allclose(xyz, want_xyz, rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(rgb, want_rgb, rtol=1e-5, atol=1e-6)
+    srv.close()
+    ctx.close()
