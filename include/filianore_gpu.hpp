@@ -36,8 +36,14 @@ struct Vector3f {
     float x = 0.f, y = 0.f, z = 0.f;
 };
 
+struct Vector2f {
+    float x = 0.f, y = 0.f;
+};
+
+// A triangle of the soup, with the texture coordinates of its vertices (TriangleEntity::uv).
 struct BasicTriangle {
     Vector3f v1, v2, v3;
+    Vector2f uv1, uv2, uv3;
 };
 
 // One mesh of the soup. `material` indexes Scene's materials (the reference attaches a
@@ -163,10 +169,15 @@ public:
         const float v[9] = {t.v1.x, t.v1.y, t.v1.z, t.v2.x, t.v2.y, t.v2.z, t.v3.x, t.v3.y, t.v3.z};
         soup_.insert(soup_.end(), v, v + 9);
         tri_material_.push_back(material);
+        const float uv[6] = {t.uv1.x, t.uv1.y, t.uv2.x, t.uv2.y, t.uv3.x, t.uv3.y};
+        uvs_.insert(uvs_.end(), uv, uv + 6);
+        for (float c : uv) has_uvs_ = has_uvs_ || c != 0.f;
     }
-    // Builds the device BVH (embree's rtcCommitScene). Returns false on failure.
+    // Builds the device BVH (embree's rtcCommitScene). Returns false on failure. `images`
+    // are the ImageMapTextures the materials name (their pixels are copied during the call).
     bool finalise(const std::vector<fl_material> &materials, const std::vector<fl_light> &lights,
-                  const std::vector<fl_standard_surface> &standard_surfaces = {}) {
+                  const std::vector<fl_standard_surface> &standard_surfaces = {},
+                  const std::vector<fl_image> &images = {}) {
         clean_up();
         if (!ctx_ || !ctx_->ok()) {
             error_ = "BVH::finalise without a valid context";
@@ -182,6 +193,9 @@ public:
         d.n_lights = (uint32_t)lights.size();
         d.standard_surfaces = standard_surfaces.empty() ? nullptr : standard_surfaces.data();
         d.n_standard_surfaces = (uint32_t)standard_surfaces.size();
+        d.uvs = has_uvs_ ? uvs_.data() : nullptr;  // all zero: every hit at uv (0, 0) either way
+        d.images = images.empty() ? nullptr : images.data();
+        d.n_images = (uint32_t)images.size();
         const fl_status st = fl_scene_create(ctx_->get(), &d, &scene_);
         if (st != FL_OK) {
             error_ = status_text(ctx_->get(), st);
@@ -248,6 +262,8 @@ private:
     fl_scene *scene_ = nullptr;
     std::vector<float> soup_;
     std::vector<uint32_t> tri_material_;
+    std::vector<float> uvs_;  // 6 per triangle
+    bool has_uvs_ = false;
     std::string error_;
 };
 
@@ -255,7 +271,8 @@ private:
 class Scene {
 public:
     Scene(Context &ctx, const SceneGeometry &geometry, const std::vector<fl_material> &materials,
-          const std::vector<Illuminant> &illuminants, const std::vector<fl_standard_surface> &standard_surfaces = {})
+          const std::vector<Illuminant> &illuminants, const std::vector<fl_standard_surface> &standard_surfaces = {},
+          const std::vector<fl_image> &images = {})
         : illuminants(illuminants) {
         bvh.initialize(ctx);
         bvh.initialize_scene_geometry(geometry);
@@ -276,7 +293,7 @@ public:
             l.penumbra_angle = il.penumbra_angle;
             lights.push_back(l);
         }
-        ok_ = bvh.finalise(materials, lights, standard_surfaces);
+        ok_ = bvh.finalise(materials, lights, standard_surfaces, images);
     }
     ~Scene() { bvh.clean_up(); }
     bool ok() const { return ok_; }

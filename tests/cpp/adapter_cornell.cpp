@@ -44,6 +44,8 @@ int main(int argc, char **argv) {
     std::vector<fl_material> mats;
     std::vector<fl_light> lights_raw;
     std::vector<fl_standard_surface> standard;
+    std::vector<std::vector<uint8_t>> pixels;
+    std::vector<fl_image> images;
     fl_camera cam{};
     SceneGeometry geometry;
     int spp = 0, depth = 0, mode = 0;
@@ -69,12 +71,23 @@ int main(int argc, char **argv) {
         const uint32_t n_rays = r.get<uint32_t>();
         const std::vector<float> org = r.arr<float>(4 * (size_t)n_rays), dir = r.arr<float>(4 * (size_t)n_rays);
         standard = r.arr<fl_standard_surface>(r.get<uint32_t>());
+        // texture coordinates (6 per triangle, all zero when the scene has none) and images
+        const std::vector<float> uvs = r.arr<float>(6 * (size_t)n_tri);
+        const uint32_t n_img = r.get<uint32_t>();
+        for (uint32_t i = 0; i < n_img; ++i) {
+            const int32_t w = r.get<int32_t>(), h = r.get<int32_t>();
+            pixels.push_back(r.arr<uint8_t>(3 * (size_t)w * (size_t)h));
+            images.push_back(fl_image{w, h, nullptr});
+        }
+        for (size_t i = 0; i < images.size(); ++i) images[i].rgb = pixels[i].data();
         // one mesh per triangle keeps the per-triangle materials and the soup order
         for (uint32_t i = 0; i < n_tri; ++i) {
             auto mesh = std::make_shared<TriangleMesh>();
             auto tri = std::make_shared<BasicTriangle>();
             const float *v = &soup[9 * (size_t)i];
             tri->v1 = {v[0], v[1], v[2]}, tri->v2 = {v[3], v[4], v[5]}, tri->v3 = {v[6], v[7], v[8]};
+            const float *q = &uvs[6 * (size_t)i];
+            tri->uv1 = {q[0], q[1]}, tri->uv2 = {q[2], q[3]}, tri->uv3 = {q[4], q[5]};
             mesh->triangles.push_back(tri);
             mesh->material = tri_mat[i];
             geometry.triangleMeshes.push_back(mesh);
@@ -109,7 +122,7 @@ int main(int argc, char **argv) {
     }
     int rc = 0;
     {
-        Scene scene(ctx, geometry, mats, illuminants, standard);
+        Scene scene(ctx, geometry, mats, illuminants, standard, images);
         if (!scene.ok()) {
             std::fprintf(stderr, "scene: %s\n", scene.bvh.last_error().c_str());
             return 1;

@@ -58,12 +58,22 @@ def write_input(path, sc, params, org, dirs):
         stds, n_std = sc.standard_array()
         f.write(np.uint32(n_std).tobytes())
         f.write(bytes(stds)[: n_std * C.sizeof(fb.fl_standard_surface)])
+        uvs = np.zeros((sc.n_tri, 6), np.float32) if sc.uvs is None else sc.uvs
+        f.write(np.ascontiguousarray(uvs, np.float32).tobytes())
+        f.write(np.uint32(len(sc.images)).tobytes())
+        for im in sc.images:
+            im = np.ascontiguousarray(im, np.uint8)
+            f.write(np.array([im.shape[1], im.shape[0]], np.int32).tobytes())
+            f.write(im.tobytes())
 
 
 @pytest.mark.gpu
 def test_adapter_matches_c_abi(tmp_path):
     exe = build(str(tmp_path))
-    sc = scenes.cornell_delta(48, 48, "standard")   # area, point, spot and directional lights; StandardSurface boxes
+    # area, point, spot and directional lights; image textures, a bump-mapped StandardSurface
+    tex = scenes.cornell_textured(48, 48, bump=True)
+    sc = scenes.Scene(tex.verts, tex.tri_material, tex.materials, list(tex.lights) + scenes.delta_lights(),
+                      tex.camera, uvs=tex.uvs, images=tex.images)
     params = scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60)
     rng = np.random.default_rng(3)
     n = 4096
