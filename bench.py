@@ -10,9 +10,12 @@ Workloads (all inputs synthetic and seeded, FP32 geometry):
            1920x1080, 64 spp, max depth 16, 4 hero wavelengths. One step = one frame.
            The working set (path state ~0.8 GB per wave, BVH ~60 MB, film 50 MB) is
            larger than the 126 MB L2, so no flush is needed between steps.
-  raycast  8,388,608-triangle soup (centroids U[0,1]^3, edges N(0, 0.002^2)) and
-           16,777,216 incoherent rays (origins U[-0.1,1.1]^3, directions uniform on the
-           sphere, tmax inf); one step = one closest-hit batch. Inputs exceed L2.
+           The render line also carries a "raycast" object: the ray-cast workload below,
+           measured in the same run (both ray sets, roofline, end to end).
+  raycast  8,388,608-triangle soup (centroids U[0,1]^3, edges N(0, 0.002^2)) and two ray
+           sets: 16,777,216 incoherent rays (origins U[-0.1,1.1]^3, directions uniform on
+           the sphere, tmax inf) and 4096 x 4096 pinhole primary rays towards the cube's
+           centre; one step = one closest-hit batch. Inputs exceed L2.
 `--impl reference` times the CPU implementation of the same workload on the host cores
 (rank 0 only): the CPU oracle, a restatement of the reference's integrator pinned
 bit-exact against the reference's own build, on a bounded sample of pixels or rays.
@@ -50,7 +53,8 @@ RENDER = {"width": 1920, "height": 1080, "spp": 64, "depth": 16}
 #   raycast: one k_trace launch over the full 16,777,216 rays: 32.73 + 1.21 GB
 #   render:  k_trace_paths + k_trace_rays2 over the first 8 of the frame's 64 waves
 #            (272 launches): 5.762 + 0.368 GB, times 8 for the frame
-TRAFFIC = {"raycast": 33.94e9, "render": 49.04e9}
+TRAFFIC = {"raycast_incoherent": 33.94e9, "render": 49.04e9}
+COHERENT_SIDE = 4096
 
 
 def load_peaks():
@@ -376,7 +380,8 @@ def config_of(workload, world):
                             "max depth 16, 4 hero wavelengths",
                 "n_tri": 1048578, "width": W, "height": H, "spp": spp, "max_depth": 16,
                 "l2": "working set larger than L2 (no flush)", "parallelism": f"sample split x{world}"}
-    return {"workload": f"raycast: 8,388,608-triangle soup, {N_RAYS:,} incoherent rays, closest hit",
+    return {"workload": f"raycast: 8,388,608-triangle soup, {N_RAYS:,} incoherent rays (value) and "
+                        f"{COHERENT_SIDE}x{COHERENT_SIDE} coherent primary rays, closest hit",
             "n_tri": N_TRI, "rays_per_gpu": N_RAYS, "l2": "inputs larger than L2 (no flush)",
             "parallelism": f"replicas x{world}"}
 
@@ -487,79 +492,107 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
                     "bytes": info["bvh_bytes"]}}
     scene.close()
     ctx.close()
+    if not args.no_raycast:
+        # the 8,388,608-triangle ray-cast workload (both ray sets), measured in the same run
+        line["raycast"] = measure_raycast(args, world, rank, local, barrier, reduce_max, max(3, args.steps))
     return line
 
 
-def gpu_raycast(args, world, rank, local, barrier, reduce_max):
+def measure_raycast(args, world, rank, local, barrier, reduce_max, steps):
+    """The ray-cast workload on one GPU: the 8,388,608-triangle soup, its BVH built on the
+    device, and both ray sets (16,777,216 incoherent rays; 4096 x 4096 pinhole primary rays),
+    each timed per launch with CUDA events on the launching stream. Returns per-set throughput,
+    the traversal roofline (algorithmic bytes from the device visit counters of the same rays),
+    and the end-to-end rate through the C ABI with host buffers."""
     import torch
     import filianore_b200 as fb
     from filianore_b200 import scenes
     tris, org, dirs = raycast_inputs(rank)
     sc = scenes.Scene(tris, np.zeros(N_TRI, np.uint32), [{"type": 0, "rgb": (0.5, 0.5, 0.5)}], [], None)
+    side = COHERENT_SIDE if N_RAYS == 1 << 24 else max(64, int(N_RAYS ** 0.5))
+    sets = {"incoherent": (org, dirs), "coherent": scenes.coherent_rays(side, side)}
     ctx = fb.Context(local)
     scene = ctx.scene(sc)
     info = scene.info()
-    d_org = torch.from_numpy(org).cuda()
-    d_dir = torch.from_numpy(dirs).cuda()
-    d_hits = torch.empty((N_RAYS, 4), dtype=torch.int32, device="cuda")
-    stream = torch.cuda.current_stream().cuda_stream
-    nodes, trisv = scene.trace_count(d_org, d_dir)
-    alg_bytes = N_RAYS * (RAY_BYTES + HIT_BYTES) + NODE_BYTES * nodes + TRI_BYTES * trisv
-    for _ in range(args.warmup):
-        scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
-    clocks = ClockSampler(local)
-    barrier()
-    clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    torch.cuda.nvtx.range_push("timed")
-    t_start.record()
-    for k in range(args.steps):
-        ev[k][0].record()
-        scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
-        ev[k][1].record()
-    t_end.record()
-    torch.cuda.nvtx.range_pop()
-    barrier()
-    clk = clocks.stop()
-    total_ms = reduce_max(t_start.elapsed_time(t_end))
-    per_launch = [a.elapsed_time(b) for a, b in ev]
-    value = world * N_RAYS * args.steps / (total_ms / 1e3) / 1e6
-    h_org = torch.from_numpy(org).pin_memory()
-    h_dir = torch.from_numpy(dirs).pin_memory()
-    h_hits = torch.empty((N_RAYS, 4), dtype=torch.int32).pin_memory()
-    L = fb.lib()
-    e2e_steps = max(2, args.steps // 2)
-
-    def host_call():
-        fb.check(L.fl_trace_closest(scene.h, C.c_void_p(h_org.data_ptr()), C.c_void_p(h_dir.data_ptr()), N_RAYS,
-                                    C.c_void_p(h_hits.data_ptr()), fb.FL_MEM_HOST, None), ctx.h)
-    host_call()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        host_call()
-    barrier()
-    e2e_s = reduce_max((time.perf_counter() - t0) / e2e_steps)
-    e2e = {"value": round(world * N_RAYS / e2e_s / 1e6, 3), "unit": "Mrays/s",
-           "h2d_bytes_per_step": N_RAYS * RAY_BYTES, "d2h_bytes_per_step": N_RAYS * HIT_BYTES}
     peaks = load_peaks()
-    launch_ms = statistics.mean(per_launch)
-    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved / peaks["hbm_gbs"], 4),
-                "traffic": TRAFFIC["raycast"] if N_RAYS == 1 << 24 else None, "traffic_unit": "bytes per launch (ncu)",
-                "peak_src": peaks["src"], "kernel": "k_trace<closest>", "alg_bytes_per_launch": int(alg_bytes),
-                "nodes_per_ray": round(nodes / N_RAYS, 2), "tris_per_ray": round(trisv / N_RAYS, 2)}
-    line = {"metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_of("raycast", world), "roofline": roofline, "e2e": e2e, "gpu_launches": args.steps,
-            "clocks": clk, "bvh": {"nodes": info["n_nodes"], "depth": info["max_depth"],
+    stream = torch.cuda.current_stream().cuda_stream
+    L = fb.lib()
+    out = {"n_tri": N_TRI, "bvh": {"nodes": info["n_nodes"], "depth": info["max_depth"],
                                    "build_ms": round(info["build_ms"], 2), "bytes": info["bvh_bytes"]}}
+    e2e_rays, e2e_s = 0, 0.0
+    clocks = ClockSampler(local)
+    clocks.start()
+    for name, (o, d) in sets.items():
+        n = o.shape[0]
+        d_org = torch.from_numpy(o).cuda()
+        d_dir = torch.from_numpy(d).cuda()
+        d_hits = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+        nodes, trisv = scene.trace_count(d_org, d_dir)
+        alg_bytes = n * (RAY_BYTES + HIT_BYTES) + NODE_BYTES * nodes + TRI_BYTES * trisv
+        for _ in range(args.warmup):
+            scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
+        barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            ev[k][0].record()
+            scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
+            ev[k][1].record()
+        barrier()
+        launch_ms = reduce_max(statistics.mean(a.elapsed_time(b) for a, b in ev))
+        achieved = alg_bytes / (launch_ms / 1e3) / 1e9
+        mrays = n / (launch_ms / 1e3) / 1e6
+        out[name] = {
+            "rays": n, "mrays_s": round(world * mrays, 3), "ms_per_launch": round(launch_ms, 4),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_src": peaks["src"],
+                         "kernel": "k_trace<closest>", "alg_bytes_per_launch": int(alg_bytes),
+                         "traffic": TRAFFIC.get(f"raycast_{name}") if N_RAYS == 1 << 24 else None,
+                         "traffic_unit": "bytes per launch (ncu)",
+                         # layout-independent floor: only the ray read and the hit write
+                         "floor_bytes_per_ray": RAY_BYTES + HIT_BYTES,
+                         "floor_frac": round(n * (RAY_BYTES + HIT_BYTES) / (launch_ms / 1e3) / 1e9 / peaks["hbm_gbs"], 4)},
+            "nodes_per_ray": round(nodes / n, 2), "tris_per_ray": round(trisv / n, 2)}
+        # end to end through the C ABI with pinned host buffers: H2D of the rays, the trace,
+        # D2H of the hits, every call
+        h_org = torch.from_numpy(o).pin_memory()
+        h_dir = torch.from_numpy(d).pin_memory()
+        h_hits = torch.empty((n, 4), dtype=torch.int32).pin_memory()
+
+        def host_call():
+            fb.check(L.fl_trace_closest(scene.h, C.c_void_p(h_org.data_ptr()), C.c_void_p(h_dir.data_ptr()), n,
+                                        C.c_void_p(h_hits.data_ptr()), fb.FL_MEM_HOST, None), ctx.h)
+        host_call()
+        e_steps = max(2, steps // 2)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            host_call()
+        barrier()
+        dt = reduce_max((time.perf_counter() - t0) / e_steps)
+        out[name]["e2e_mrays_s"] = round(world * n / dt / 1e6, 3)
+        e2e_rays += n
+        e2e_s += dt
+        del d_org, d_dir, d_hits, h_org, h_dir, h_hits
+    out["clocks"] = clocks.stop()
+    out["e2e"] = {"value": round(world * e2e_rays / e2e_s / 1e6, 3), "unit": "Mrays/s",
+                  "h2d_bytes_per_step": e2e_rays * RAY_BYTES, "d2h_bytes_per_step": e2e_rays * HIT_BYTES,
+                  "note": "one step = both ray sets through fl_trace_closest with pinned host buffers"}
     scene.close()
     ctx.close()
+    return out
+
+
+def gpu_raycast(args, world, rank, local, barrier, reduce_max):
+    rc = measure_raycast(args, world, rank, local, barrier, reduce_max, args.steps)
+    inc = rc["incoherent"]
+    line = {"metric": "Mrays/s", "value": inc["mrays_s"], "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": inc["ms_per_launch"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of("raycast", world), "roofline": inc["roofline"],
+            "e2e": {"value": inc["e2e_mrays_s"], "unit": "Mrays/s", "h2d_bytes_per_step": inc["rays"] * RAY_BYTES,
+                    "d2h_bytes_per_step": inc["rays"] * HIT_BYTES},
+            "gpu_launches": args.steps, "clocks": rc["clocks"], "coherent": rc["coherent"], "bvh": rc["bvh"],
+            "nodes_per_ray": inc["nodes_per_ray"], "tris_per_ray": inc["tris_per_ray"]}
     return line
 
 
@@ -571,6 +604,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve", "guide"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-raycast", action="store_true", help="render: skip the ray-cast sub-measurement")
     ap.add_argument("--size", default=None, help="render: WxH (smaller cases for profiling)")
     ap.add_argument("--spp", type=int, default=None, help="render: samples per pixel")
     ap.add_argument("--rays", type=int, default=None, help="raycast: rays per batch")

@@ -20,10 +20,14 @@
 //
 // Set-up: host code cannot use the array's name as a device address (on the host it names a
 // shadow variable). The first call on each device, with that device current, asks the runtime
-// for the array's device address with cudaGetSymbolAddress and keeps it; make that first call
-// before any stream capture.
+// for the array's device address with cudaGetSymbolAddress and keeps it. With CUDA's lazy
+// module loading that first call is also when the driver loads the device code holding the
+// array, which reserves its 32 MiB and may synchronise the device: make the first call during
+// set-up, before any stream capture and before the caller's memory budget is fixed. Later
+// calls allocate nothing.
 #include <chrono>
 #include <mutex>
+#include <string>
 
 #include "fl_render.cuh"
 
@@ -63,7 +67,10 @@ extern "C" fl_status fl_render_noalloc(fl_scene *scene_h, const fl_camera *camer
         set_error(ctx, "invalid render parameters");
         return FL_ERR_INVALID;
     }
-    if (ctx->device < 0 || ctx->device >= kMaxDevices) return FL_ERR_INVALID;
+    if (ctx->device < 0 || ctx->device >= kMaxDevices) {
+        set_error(ctx, "fl_render_noalloc supports device indices 0.." + std::to_string(kMaxDevices - 1));
+        return FL_ERR_INVALID;
+    }
     FL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     void *scratch = nullptr;
     {
@@ -88,21 +95,30 @@ extern "C" fl_status fl_render_noalloc(fl_scene *scene_h, const fl_camera *camer
     fl_render_params q = p;
     q.wave_paths = (int32_t)std::min<size_t>(p.wave_paths > 0 ? (size_t)p.wave_paths : ((size_t)1 << 30),
                                              (kNoAllocScratchBytes - fixed_overhead) / per_slot);
-    q.wave_paths &= ~127;
+    q.wave_paths = std::max<int32_t>(128, q.wave_paths & ~127);  // never 0, which would mean "the default"
     q.flags = p.flags & FL_RENDER_COUNT;  // no event timing: events would be allocated
     cudaStream_t st = ctx->stream;
     const CamDev cam = camera_basis_of(*camera);
     const size_t n_pix = (size_t)camera->width * camera->height;
     const auto t0 = std::chrono::steady_clock::now();
-    FL_CUDA_TRY(ctx, cudaMemsetAsync(film_xyz64, 0, n_pix * 3 * sizeof(double), st));
+    // On an error, wait for the kernels already queued before returning: they may still be
+    // writing the shared array, and the next call (from any context on this device) must
+    // not overlap them.
+    auto fail = [&](fl_status code) {
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+        return code;
+    };
+    cudaError_t ce = cudaMemsetAsync(film_xyz64, 0, n_pix * 3 * sizeof(double), st);
+    if (ce != cudaSuccess) return fail(cuda_status(ctx, ce, "film clear"));
     WaveCounters hc{};
     RenderProfile prof;  // off: records nothing
     fl_status rc = NL == 60 ? render_waves<60>(s, cam, q, film_xyz64, &hc, &prof, st, scratch, kNoAllocScratchBytes)
                             : render_waves<4>(s, cam, q, film_xyz64, &hc, &prof, st, scratch, kNoAllocScratchBytes);
-    if (rc) return rc;
+    if (rc) return fail(rc);
     k_resolve<<<(uint32_t)std::min<size_t>((n_pix + 255) / 256, (size_t)ctx->sm_count * 8), 256, 0, st>>>(
         film_xyz64, (uint32_t)n_pix, 1.0 / (double)p.spp, film_rgb);
-    FL_CUDA_TRY(ctx, cudaGetLastError());
+    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_status(ctx, ce, "resolve launch"));
     FL_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (stats) {
         *stats = fl_render_stats{};

@@ -68,7 +68,9 @@ public:
             JobState &js = jobs_[j];
             SceneState &sc = scenes_[js.scene];
             const uint64_t need = js.film_bytes + (sc.resident ? 0 : sc.bytes);
-            if (need > budget_) {  // can never fit, even with every scene evicted
+            // The job holds its scene and its film for as long as it runs, so scene + film
+            // beyond the budget can never fit, whether or not the scene is resident now.
+            if (js.film_bytes + sc.bytes > budget_) {
                 a.rejected.push_back(j);
                 pending_.pop_front();
                 jobs_.erase(j);

@@ -415,8 +415,11 @@ FL_API fl_status fl_server_get_stats(fl_server *srv, fl_server_stats *stats);
  * FL_ERR_CAPACITY. film_rgb (width*height*3 floats) and film_xyz64 (width*height*3 doubles,
  * the FP64 XYZ sums, cleared by the call) are caller-owned DEVICE buffers. All calls share
  * the fixed array: calls whose GPU work overlaps race and give wrong images. The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress); make it before
- * any stream capture. stats->ms is host wall time of the call. */
+ * on a device looks up the array's device address (cudaGetSymbolAddress); under CUDA's lazy
+ * module loading that is when the driver loads the library code holding the array, which
+ * reserves its 32 MiB on the device and may synchronise it. So make the first call during
+ * set-up, before any stream capture; later calls allocate nothing. stats->ms is host wall
+ * time of the call. */
 FL_API fl_status fl_render_noalloc(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
                                    float *film_rgb, double *film_xyz64, fl_render_stats *stats);
 

@@ -80,5 +80,19 @@ int main() {
             q.finish_wave();
         }
     }
+    // a resident, idle scene whose bytes plus the job's film exceed the budget: the job can
+    // never run (it holds both), so it is rejected instead of waiting forever at the head
+    {
+        ServeScheduler q(100, 4);
+        q.add_scene(1, 60);
+        q.submit(40, 1, 30, 10);  // fits: 60 + 30
+        print_adm("B1", q.admit());
+        q.plan_wave(64);
+        q.finish_wave();
+        q.submit(41, 1, 50, 10);  // 60 + 50 > 100 with the scene already resident
+        q.submit(42, 1, 20, 10);  // behind it, fits
+        print_adm("B2", q.admit());
+        std::printf("pending %d running %d\n", (int)q.pending(), (int)q.running());
+    }
     return 0;
 }

@@ -58,3 +58,12 @@ def test_response_ratio_bounds_waiting():
     assert out[6] == "R6 30:256"
     assert out[7] == "R7 30:56 37:200"
 
+
+def test_resident_scene_plus_film_over_budget_is_rejected():
+    """Budget 100, scene 60: after a job with a 30-byte film finished, the scene stays
+    resident and idle. A job with a 50-byte film can never run (it needs both, 110 bytes), so
+    it is rejected rather than left blocking the queue; the job behind it is admitted."""
+    out = run_driver()[25:]
+    assert out[0] == "B1 admitted 40 | build 1 | evict | rejected"
+    assert out[1] == "B2 admitted 42 | build | evict | rejected 41"
+    assert out[2] == "pending 0 running 1"
