@@ -447,12 +447,24 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
     host_film = torch.zeros((H, W, 3), dtype=torch.float32).pin_memory()
     e2e_steps = max(2, args.steps // 2)
 
+    parts = {"scene_create_ms": 0.0, "render_call_ms": 0.0, "render_device_ms": 0.0, "scene_destroy_ms": 0.0}
+
     def e2e_step():
+        t0 = time.perf_counter()
         h = ctx.scene(pinned)
+        t1 = time.perf_counter()
         _, st = h.render(params(offset=fdist.rank_sample_offset(rank, RENDER["spp"])), film_rgb=host_film.numpy(), memory=fb.FL_MEM_HOST)
+        t2 = time.perf_counter()
         h.close()
+        t3 = time.perf_counter()
+        parts["scene_create_ms"] += (t1 - t0) * 1e3
+        parts["render_call_ms"] += (t2 - t1) * 1e3
+        parts["render_device_ms"] += st["ms"]
+        parts["scene_destroy_ms"] += (t3 - t2) * 1e3
         return st
     e2e_step()
+    for k in parts:
+        parts[k] = 0.0
     barrier()
     t0 = time.perf_counter()
     e_rays = 0
@@ -464,7 +476,8 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
            "samples_per_s": round(world * e2e_steps * W * H * RENDER["spp"] / e2e_s, 1),
            "h2d_bytes_per_step": int(pinned.verts.nbytes + pinned.tri_material.nbytes),
            "d2h_bytes_per_step": W * H * 3 * 4,
-           "note": "per step: scene upload from pinned host memory + BVH build + render + film readback"}
+           "note": "per step: scene upload from pinned host memory + BVH build + render + film readback",
+           "breakdown_ms_per_step": {k: round(v / e2e_steps, 2) for k, v in parts.items()}}
 
     peaks = load_peaks()
     prof = stats[-1]

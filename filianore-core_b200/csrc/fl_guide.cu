@@ -539,8 +539,12 @@ static fl_status guide_pass(Guide *G, Scene *s, const CamDev &cam, const fl_rend
         d.seg[0] = WaveSeg{0u, 0u, d.n_wave, 0u, wb, 0ull};
         FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
         if (train) FL_CUDA_TRY(ctx, cudaMemsetAsync(G->rec_count, 0, sizeof(uint32_t), st));
-        enqueue_wave<4, true>(W, p.max_depth, false, &prof, sms, st, s->ext_kernels);
+        enqueue_wave<4, true>(W, deepest_depth(p), false, &prof, sms, st, s->ext_kernels);
         FL_CUDA_TRY(ctx, cudaGetLastError());
+        if (!depths_equal(p)) {
+            rc = run_tail<4, true>(ctx, W, deepest_depth(p) + 1, false, &prof, sms, st, s->ext_kernels);
+            if (rc) return rc;
+        }
         if (train) {
             FL_CUDA_TRY(ctx, cudaMemcpyAsync(G->h_count, G->rec_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             FL_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -561,7 +565,7 @@ static fl_status check_render_args(Context *ctx, Scene *s, const fl_camera *came
         return FL_ERR_INVALID;
     }
     const fl_render_params &p = *params;
-    if (!camera_ok(*camera) || p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 || p.spectral_mode != FL_SPECTRAL_HERO4 ||
+    if (!camera_ok(*camera) || p.spp <= 0 || !depths_ok(p) || p.spectral_mode != FL_SPECTRAL_HERO4 ||
         (memory != FL_MEM_HOST && memory != FL_MEM_DEVICE)) {
         set_error(ctx, "invalid guided render parameters (hero wavelengths only)");
         return FL_ERR_INVALID;
@@ -613,6 +617,7 @@ static void add_stats(fl_render_stats *stats, const WaveCounters &hc) {
     stats->shadow_rays += hc.shadow_rays;
     stats->bounces += hc.bounces;
     stats->traversal_errors += (uint32_t)hc.err;
+    stats->paths_cut += hc.cut;
 }
 
 }  // namespace fl
@@ -744,11 +749,7 @@ extern "C" fl_status fl_guide_render(fl_guide *g_h, fl_scene *scene_h, const fl_
         add_stats(stats, hc);
         stats->ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
-    if (hc.err) {
-        set_error(ctx, std::to_string(hc.err) + " traversal or queue bound hits during the render");
-        return FL_ERR_TRAVERSAL;
-    }
-    return FL_OK;
+    return render_bounds_status(ctx, hc);
 }
 
 extern "C" fl_status fl_guide_render_timed(fl_guide *g_h, fl_scene *scene_h, const fl_camera *camera,
@@ -794,11 +795,10 @@ extern "C" fl_status fl_guide_render_timed(fl_guide *g_h, fl_scene *scene_h, con
         *stats = acc;
         stats->ms = elapsed();
     }
-    if (acc.traversal_errors) {
-        set_error(ctx, std::to_string(acc.traversal_errors) + " traversal or queue bound hits during the render");
-        return FL_ERR_TRAVERSAL;
-    }
-    return FL_OK;
+    WaveCounters total{};
+    total.err = (int)acc.traversal_errors;
+    total.cut = (uint32_t)acc.paths_cut;
+    return render_bounds_status(ctx, total);
 }
 
 extern "C" fl_status fl_guide_get_weights(fl_guide *g_h, float *weights) {

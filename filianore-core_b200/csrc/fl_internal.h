@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <mutex>
@@ -163,6 +164,40 @@ fl_status launch_trace(Scene *s, const float4 *org_tmin, const float4 *dir_tmax,
 // context scratch: returns a device buffer of at least `bytes` (grow-only)
 fl_status ensure_scratch(Context *ctx, size_t bytes, void **out);
 fl_status ensure_film_scratch(Context *ctx, size_t bytes, void **out);
+
+// RenderParams' three depths (core/renderparams.h:5-10) in the order diffuse, reflection
+// (specular and glossy), transmission: the params' own with FL_RENDER_LOBE_DEPTHS, else
+// max_depth for all three.
+inline void lobe_depths(const fl_render_params &p, int d[3]) {
+    if (p.flags & FL_RENDER_LOBE_DEPTHS) {
+        d[0] = p.diffuse_depth;
+        d[1] = p.reflection_depth;
+        d[2] = p.transmission_depth;
+    } else {
+        d[0] = d[1] = d[2] = p.max_depth;
+    }
+}
+// every depth a bounce index below FL_MAX_BOUNCES
+inline bool depths_ok(const fl_render_params &p) {
+    int d[3];
+    lobe_depths(p, d);
+    for (int k = 0; k < 3; ++k)
+        if (d[k] < 0 || d[k] >= FL_MAX_BOUNCES) return false;
+    return true;
+}
+// Equal depths end every path at that bounce (a sampled lobe is always diffuse, glossy or
+// specular); unequal ones let paths run on (fl_render.cuh, run_tail).
+inline bool depths_equal(const fl_render_params &p) {
+    int d[3];
+    lobe_depths(p, d);
+    return d[0] == d[1] && d[1] == d[2];
+}
+// the bounces a wave's fixed launch sequence covers: 0..deepest depth
+inline int deepest_depth(const fl_render_params &p) {
+    int d[3];
+    lobe_depths(p, d);
+    return std::max(d[0], std::max(d[1], d[2]));
+}
 
 // camera resolution within 2^31 pixels and a finite, non-negative aperture
 inline bool camera_ok(const fl_camera &c) {

@@ -51,7 +51,8 @@ struct WaveCounters {
     unsigned long long rays, shadow_rays, bounces, paths;
     unsigned long long nodes, tris;  // FL_RENDER_COUNT
     int err;
-    int pad[3];
+    uint32_t cut;                    // paths ended at the job's bounce cap
+    int pad[2];
 };
 
 // FL_RENDER_PROFILE: CUDA events bracketing every launch, grouped by kernel class. The
@@ -94,6 +95,17 @@ struct CamDev {
     float lens_radius;  // PhysicalCamera::lensRadius = aperture / 2 (0: pinhole)
 };
 
+// fl_li: a batch of caller rays in place of the camera's. Ray i is "pixel" i of a 1-spp
+// job; it starts from the caller's PCG32 state (increment 3) and hero wavelength, and its
+// radiance spectrum and final generator state are written back.
+struct LiRays {
+    const float4 *org, *dir;            // (o, tmin), (d, tmax)
+    const unsigned long long *rng;      // PCG32 state per ray
+    const float *lambda0;               // hero wavelength per ray (hero mode)
+    float *L;                           // NL floats per ray
+    unsigned long long *rng_out;        // generator state when the path ended (nullable)
+};
+
 // Everything one render job needs: its scene, camera, parameters and film. A wave's paths
 // may belong to different jobs (serving); every kernel looks its path's job up.
 struct JobDev {
@@ -118,12 +130,15 @@ struct JobDev {
     int has_spheres;
     float env_radiance;
     CamDev cam;
-    int spp, max_depth;
+    int spp;
+    int depth[3];       // RenderParams: diffuse, reflection (specular + glossy), transmission
+    int bounce_cap;     // paths alive after bounce bounce_cap - 1 are cut (FL_MAX_BOUNCES)
     float rr_threshold;
     uint32_t sample_offset;
     uint32_t n_pix;
     double *film;  // FP64 XYZ sums, 3 per pixel
     int corrected_ggx;  // FL_RENDER_CORRECTED_GGX
+    LiRays li;          // fl_li batches (li.org == nullptr for camera jobs)
 };
 
 // A wave is a list of sample ranges: slots [slot_begin, slot_begin + count) render the
@@ -259,6 +274,11 @@ __device__ inline void finish_path(const RenderArgs &A, const JobDev &J, const S
     atomicAdd(&J.film[3 * (size_t)pix + 0], xyz[0]);
     atomicAdd(&J.film[3 * (size_t)pix + 1], xyz[1]);
     atomicAdd(&J.film[3 * (size_t)pix + 2], xyz[2]);
+    if (J.li.L) {
+        // Integrator::Li's return value and the sampler's state after the path
+        store_spec<NL>(J.li.L, 0, pix, L);
+        if (J.li.rng_out) J.li.rng_out[pix] = A.head[slot].rng;
+    }
     if constexpr (NL == 4) {
         // guiding: the radiance gathered after each recorded vertex, divided by the
         // throughput it was scaled by, estimates the incident radiance along the
@@ -470,6 +490,31 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
         const unsigned long long g = sg.sample_base + (k - sg.slot_begin);
         const uint32_t pix = (uint32_t)(g % J.n_pix);
         const unsigned long long s = g / J.n_pix;
+        if (J.li.org) {
+            // fl_li: the caller's ray, generator state and wavelength
+            PathHead ph;
+            ph.rng = J.li.rng[pix];
+            ph.lambda0 = J.li.lambda0 ? J.li.lambda0[pix] : 380.f;
+            ph.flags = 0u;
+            ph.pixel = pix;
+            ph.job = sg.job;
+            ph.eta_scale = 1.f;
+            ph.pad = 0u;
+            A.head[k] = ph;
+            Spec<NL> one, zero;
+            one.set(1.f);
+            zero.set(0.f);
+            store_spec<NL>(A.beta, A.cap, k, one);
+            store_spec<NL>(A.L, A.cap, k, zero);
+            A.ray_o[k] = J.li.org[pix];
+            A.ray_d[k] = J.li.dir[pix];
+            A.q_trace[k] = k;
+            if (A.g.rec_idx) {
+                A.g.rec_idx[k] = kNoRecord;
+                A.g.rec_idx[(size_t)A.cap + k] = kNoRecord;
+            }
+            continue;
+        }
         Pcg32 rng;
         rng.seed(pix, 1u);
         const unsigned long long sidx = (unsigned long long)J.sample_offset + s;
@@ -600,7 +645,8 @@ __global__ void __launch_bounds__(128, 7) k_trace_paths(RenderArgs A) {
     PathTraceItem it;
     it.A = &A;
     it.any_hit = false;
-    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, err, st);
+    __shared__ uint2 stack[trav_stack_smem_bytes(128) / sizeof(uint2)];
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, err, st, stack);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->rays, (unsigned long long)n);
     if (COUNT) {
         warp_count(&A.cnt->nodes, st.nodes);
@@ -827,7 +873,8 @@ __global__ void __launch_bounds__(128, 7) k_trace_rays2(RenderArgs A) {
     TraceStats st;
     NeeRayItem it;
     it.A = &A;
-    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, err, st);
+    __shared__ uint2 stack[trav_stack_smem_bytes(128) / sizeof(uint2)];
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, err, st, stack);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&A.cnt->shadow_rays, (unsigned long long)n);
         atomicAdd(&A.cnt->rays, (unsigned long long)n);
@@ -990,11 +1037,13 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
             if (GUIDE && c_sel > 0.f && !(f.black() || pdf == 0))
                 pdf = c_sel * guide_mixture_pdf(gm, wi) + (1.f - c_sel) * pdf;
             bool stop = f.black() || pdf == 0;
-            const int depth = J.max_depth;
+            // the depth of the sampled lobe's kind ends the path at exactly that bounce
+            // (pathintegrator.cpp:55-65)
             const int bi = (int)bounce;
-            if (!stop && depth == bi && (sflags & kBsdfDiffuse)) stop = true;
-            if (!stop && ((depth == bi && (sflags & kBsdfSpecular)) || (depth == bi && (sflags & kBsdfGlossy)))) stop = true;
-            if (!stop && depth == bi && (sflags & kBsdfTransmission)) stop = true;
+            if (!stop && J.depth[0] == bi && (sflags & kBsdfDiffuse)) stop = true;
+            if (!stop && ((J.depth[1] == bi && (sflags & kBsdfSpecular)) || (J.depth[1] == bi && (sflags & kBsdfGlossy))))
+                stop = true;
+            if (!stop && J.depth[2] == bi && (sflags & kBsdfTransmission)) stop = true;
             if (!stop) {
                 const float ad = absdot(wi, b.ns);
 #pragma unroll
@@ -1021,6 +1070,11 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
 #pragma unroll
                         for (int k = 0; k < NL; ++k) beta.c[k] /= 1.f - qq;
                     }
+                }
+                if (!stop && bi + 1 >= J.bounce_cap) {
+                    // unequal lobe depths: a path still going at the bounce bound is cut
+                    stop = true;
+                    atomicAdd(&A.cnt->cut, 1u);
                 }
                 if (!stop) {
                     alive = true;
@@ -1146,23 +1200,19 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
     return FL_OK;
 }
 
-// Enqueues one wave (camera rays of the samples in *W.d_wave, then max_depth + 1 bounces)
-// on `st`. Launch shapes do not depend on the wave's content, so the sequence can be
-// captured once into a CUDA graph and replayed for every wave.
-// `standard`: the wave may hold StandardSurface materials, shaded by their own kernel instances.
+// Enqueues bounces [b_begin, b_end) of a wave on `st`. Bounce b reads the trace queue of
+// parity b (qa for even b) and appends survivors to the other one. Launch shapes do not
+// depend on the wave's content (kernels read their counts from device memory).
 template <int NL, bool GUIDE = false>
-void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile *prof, int sms, cudaStream_t st,
-                  bool standard) {
+void enqueue_bounces(const WaveBuffers &W, int b_begin, int b_end, bool count, RenderProfile *prof, int sms,
+                     cudaStream_t st, bool standard) {
     RenderArgs A = W.A;
-    A.q_trace = W.qa;
-    A.q_next = W.qb;
     const int g_trace = sms * 16, g_shade = sms * 8;
-    k_raygen<NL><<<std::min<uint32_t>(((uint32_t)W.cap + 127) / 128, (uint32_t)sms * 32), 128, 0, st>>>(A);
-    prof->launches += 1;
-    for (int b = 0; b <= max_depth; ++b) {
+    for (int b = b_begin; b < b_end; ++b) {
+        A.q_trace = (b & 1) ? W.qb : W.qa;
+        A.q_next = (b & 1) ? W.qa : W.qb;
         if (b > 0) {
             k_advance<<<1, 1, 0, st>>>(A.cnt);
-            std::swap(A.q_trace, A.q_next);
             prof->launches += 1;
         }
         prof->mark(0, st);
@@ -1191,6 +1241,50 @@ void enqueue_wave(const WaveBuffers &W, int max_depth, bool count, RenderProfile
     }
 }
 
+// Enqueues one wave: camera rays of the samples in *W.d_wave, then bounces 0..depth. The
+// sequence can be captured once into a CUDA graph and replayed for every wave.
+// `standard`: the wave may hold StandardSurface materials, shaded by their own kernel instances.
+template <int NL, bool GUIDE = false>
+void enqueue_wave(const WaveBuffers &W, int depth, bool count, RenderProfile *prof, int sms, cudaStream_t st,
+                  bool standard) {
+    RenderArgs A = W.A;
+    A.q_trace = W.qa;
+    A.q_next = W.qb;
+    k_raygen<NL><<<std::min<uint32_t>(((uint32_t)W.cap + 127) / 128, (uint32_t)sms * 32), 128, 0, st>>>(A);
+    prof->launches += 1;
+    enqueue_bounces<NL, GUIDE>(W, 0, depth + 1, count, prof, sms, st, standard);
+}
+
+// With unequal lobe depths a path is ended only by the depth of the lobe kind it samples,
+// at that exact bounce, so it can outlive the deepest depth. After a wave's fixed bounces
+// 0..first_bounce - 1 the paths still alive run further bounces, kTailBounces per check of
+// the live count, until none is left; k_continue cuts what reaches FL_MAX_BOUNCES.
+constexpr int kTailBounces = 4;
+template <int NL, bool GUIDE = false>
+fl_status run_tail(Context *ctx, const WaveBuffers &W, int first_bounce, bool count, RenderProfile *prof, int sms,
+                   cudaStream_t st, bool standard) {
+    for (int b = first_bounce; b < FL_MAX_BOUNCES; b += kTailBounces) {
+        uint32_t live = 0;
+        FL_CUDA_TRY(ctx, cudaMemcpyAsync(&live, &W.A.cnt->n_next, sizeof(live), cudaMemcpyDeviceToHost, st));
+        FL_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        if (live == 0) break;
+        enqueue_bounces<NL, GUIDE>(W, b, std::min(b + kTailBounces, FL_MAX_BOUNCES), count, prof, sms, st, standard);
+        FL_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    return FL_OK;
+}
+
+// FL_ERR_TRAVERSAL when a traversal, queue or bounce bound was hit during a render (the
+// image holds everything else), with the counts in the context's message.
+inline fl_status render_bounds_status(Context *ctx, const WaveCounters &hc) {
+    if (!hc.err && !hc.cut) return FL_OK;
+    std::string m;
+    if (hc.err) m = std::to_string(hc.err) + " traversal or queue bound hits during the render";
+    if (hc.cut) m += (m.empty() ? "" : "; ") + std::to_string(hc.cut) + " paths still alive at FL_MAX_BOUNCES were cut";
+    set_error(ctx, m);
+    return FL_ERR_TRAVERSAL;
+}
+
 // The job record of one scene + camera + parameters (fl_render's single job).
 inline JobDev job_of(const Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film) {
     JobDev j{};
@@ -1217,7 +1311,9 @@ inline JobDev job_of(const Scene *s, const CamDev &cam, const fl_render_params &
     for (const auto &l : s->lights_host) j.has_spheres |= (l.type == FL_LIGHT_SPHERE) ? 1 : 0;
     j.cam = cam;
     j.spp = p.spp;
-    j.max_depth = p.max_depth;
+    lobe_depths(p, j.depth);
+    // equal depths end every path by bounce depth (no cut); unequal ones run to the bound
+    j.bounce_cap = depths_equal(p) ? j.depth[0] + 1 : FL_MAX_BOUNCES;
     j.rr_threshold = p.rr_threshold;
     j.sample_offset = p.sample_offset;
     j.n_pix = (uint32_t)((uint64_t)cam.W * (uint64_t)cam.H);
@@ -1232,7 +1328,7 @@ inline JobDev job_of(const Scene *s, const CamDev &cam, const fl_render_params &
 template <int NL>
 fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, double *d_film,
                        WaveCounters *h_cnt, RenderProfile *prof, cudaStream_t st, void *fixed_scratch = nullptr,
-                       size_t fixed_bytes = 0) {
+                       size_t fixed_bytes = 0, const LiRays *li = nullptr) {
     Context *ctx = s->ctx;
     const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
     const unsigned long long total = n_pix * (unsigned long long)p.spp;
@@ -1241,19 +1337,23 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     WaveBuffers W;
     fl_status rc = wave_buffers(ctx, NL, (int)s->n_lights, cap_req, fixed_scratch, fixed_bytes, W);
     if (rc) return rc;
-    const JobDev j = job_of(s, cam, p, d_film);
+    JobDev j = job_of(s, cam, p, d_film);
+    if (li) j.li = *li;
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_jobs, &j, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(W.A.cnt, 0, sizeof(WaveCounters), st));
     const bool count = (p.flags & FL_RENDER_COUNT) != 0;
     const bool standard = s->ext_kernels;
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
     const size_t desc_bytes = offsetof(WaveDesc, seg) + sizeof(WaveSeg);
+    const int depth = deepest_depth(p);
+    const bool tail = !depths_equal(p);
     // Replay one captured graph per wave: a depth-16 wave is ~85 launches, and its late
     // bounces have so few paths that launching dominates. Not used by the allocation-free
-    // path (instantiating a graph allocates) nor when every launch is timed with events.
-    const bool use_graph = !fixed_scratch && !prof->on;
+    // path (instantiating a graph allocates), when every launch is timed with events, nor by
+    // fl_li (its small batches would replace the render's graph with one of their own size).
+    const bool use_graph = !fixed_scratch && !prof->on && !li;
     if (use_graph && (!ctx->wave_graph || ctx->graph_base != W.A.cnt || ctx->graph_cap != W.cap ||
-                      ctx->graph_depth != p.max_depth || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count ||
+                      ctx->graph_depth != depth || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count ||
                       ctx->graph_std != (int)standard)) {
         if (ctx->wave_graph) {
             cudaGraphExecDestroy(ctx->wave_graph);
@@ -1262,7 +1362,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         cudaGraph_t g = nullptr;
         RenderProfile off;
         FL_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        enqueue_wave<NL>(W, p.max_depth, count, &off, sms, st, standard);
+        enqueue_wave<NL>(W, depth, count, &off, sms, st, standard);
         FL_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
         cudaError_t e = cudaGraphInstantiate(&ctx->wave_graph, g, 0);
         cudaGraphDestroy(g);
@@ -1272,7 +1372,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         }
         ctx->graph_base = W.A.cnt;
         ctx->graph_cap = W.cap;
-        ctx->graph_depth = p.max_depth;
+        ctx->graph_depth = depth;
         ctx->graph_nl_mode = NL;
         ctx->graph_count = (int)count;
         ctx->graph_std = (int)standard;
@@ -1286,11 +1386,15 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
         if (use_graph) {
             FL_CUDA_TRY(ctx, cudaGraphLaunch(ctx->wave_graph, st));
-            prof->launches += 1 + (standard ? 7 : 5) * (uint32_t)p.max_depth + (standard ? 6 : 4);
+            prof->launches += 1 + (standard ? 7 : 5) * (uint32_t)depth + (standard ? 6 : 4);
         } else {
-            enqueue_wave<NL>(W, p.max_depth, count, prof, sms, st, standard);
+            enqueue_wave<NL>(W, depth, count, prof, sms, st, standard);
         }
         FL_CUDA_TRY(ctx, cudaGetLastError());
+        if (tail) {
+            const fl_status rc2 = run_tail<NL>(ctx, W, depth + 1, count, prof, sms, st, standard);
+            if (rc2) return rc2;
+        }
     }
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, W.A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
     return FL_OK;

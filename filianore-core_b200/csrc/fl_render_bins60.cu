@@ -5,5 +5,5 @@
 
 namespace fl {
 template fl_status render_waves<60>(Scene *, const CamDev &, const fl_render_params &, double *, WaveCounters *, RenderProfile *,
-                                    cudaStream_t, void *, size_t);
+                                    cudaStream_t, void *, size_t, const LiRays *);
 }

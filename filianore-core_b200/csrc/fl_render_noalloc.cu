@@ -33,9 +33,11 @@
 
 namespace fl {
 extern template fl_status render_waves<4>(Scene *, const CamDev &, const fl_render_params &, double *,
-                                          WaveCounters *, RenderProfile *, cudaStream_t, void *, size_t);
+                                          WaveCounters *, RenderProfile *, cudaStream_t, void *, size_t,
+                                          const LiRays *);
 extern template fl_status render_waves<60>(Scene *, const CamDev &, const fl_render_params &, double *,
-                                           WaveCounters *, RenderProfile *, cudaStream_t, void *, size_t);
+                                           WaveCounters *, RenderProfile *, cudaStream_t, void *, size_t,
+                                           const LiRays *);
 CamDev camera_basis_of(const fl_camera &c);
 
 namespace {
@@ -62,7 +64,7 @@ extern "C" fl_status fl_render_noalloc(fl_scene *scene_h, const fl_camera *camer
         return FL_ERR_INVALID;
     }
     const fl_render_params p = *params;
-    if (!camera_ok(*camera) || p.spp <= 0 || p.max_depth < 0 || p.max_depth > 250 ||
+    if (!camera_ok(*camera) || p.spp <= 0 || !depths_ok(p) ||
         (p.spectral_mode != FL_SPECTRAL_HERO4 && p.spectral_mode != FL_SPECTRAL_BINS60) || s->n_lights > 64) {
         set_error(ctx, "invalid render parameters");
         return FL_ERR_INVALID;
@@ -131,10 +133,7 @@ extern "C" fl_status fl_render_noalloc(fl_scene *scene_h, const fl_camera *camer
         stats->launches = prof.launches + 1;
         stats->nodes_visited = hc.nodes;
         stats->tris_tested = hc.tris;
+        stats->paths_cut = hc.cut;
     }
-    if (hc.err) {
-        set_error(ctx, std::to_string(hc.err) + " traversal or queue bound hits during the render");
-        return FL_ERR_TRAVERSAL;
-    }
-    return FL_OK;
+    return render_bounds_status(ctx, hc);
 }

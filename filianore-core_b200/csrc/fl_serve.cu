@@ -235,6 +235,15 @@ void worker_loop(Server *S) {
                 const auto w0 = std::chrono::steady_clock::now();
                 cudaGraphLaunch(S->graph, S->stream);
                 cudaError_t e = cudaStreamSynchronize(S->stream);
+                // jobs with unequal lobe depths may have paths alive past the wave's bounces
+                if (e == cudaSuccess) {
+                    RenderProfile tprof;
+                    if (run_tail<4>(S->ctx, S->W, S->cfg.max_depth + 1, false, &tprof,
+                                    S->ctx->sm_count > 0 ? S->ctx->sm_count : 148, S->stream, true) != FL_OK)
+                        e = cudaErrorUnknown;
+                    else
+                        e = cudaStreamSynchronize(S->stream);
+                }
                 const double wave_ms =
                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
                 std::lock_guard<std::mutex> lock(S->mu);
@@ -401,9 +410,9 @@ fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job
     if (!S || !job || !job_id) return FL_ERR_INVALID;
     const fl_camera &c = job->camera;
     const fl_render_params &p = job->params;
-    if (!camera_ok(c) || p.spp <= 0 ||
-        p.max_depth < 0 || p.max_depth > S->cfg.max_depth || p.spectral_mode != FL_SPECTRAL_HERO4) {
-        set_error(S->ctx, "invalid job (hero-wavelength mode, depth within the server's max_depth)");
+    if (!camera_ok(c) || p.spp <= 0 || !depths_ok(p) || deepest_depth(p) > S->cfg.max_depth ||
+        p.spectral_mode != FL_SPECTRAL_HERO4) {
+        set_error(S->ctx, "invalid job (hero-wavelength mode, depths within the server's max_depth)");
         return FL_ERR_INVALID;
     }
     auto hj = std::make_unique<HostJob>();

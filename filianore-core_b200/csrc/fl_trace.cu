@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restric
     TraceStats st;
     bool error = false;
     uint32_t *fetch = reinterpret_cast<uint32_t *>(counters + 4);
-    persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, error, st);
+    __shared__ uint2 stack[trav_stack_smem_bytes(kTraceBlock) / sizeof(uint2)];
+    persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, error, st, stack);
     if (KIND == kTraceCount) {
         warp_add_u64(&counters[0], st.nodes);
         warp_add_u64(&counters[1], st.tris);

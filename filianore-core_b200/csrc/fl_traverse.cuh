@@ -59,10 +59,45 @@ __device__ __forceinline__ void trav_init(TravState &s, const RayPre &r) {
     s.res.v = 0.f;
 }
 
+// Per-lane traversal stack: the first kSmemStack entries live in shared memory (a column per
+// lane: entry k of thread t at sm[k * stride + t], so lanes pushing at the same depth hit
+// consecutive words), deeper ones in a local-memory spill array that a typical ray never
+// touches. Entries are node groups (internal-child hit bits 24..31 set) or postponed
+// triangle groups (hit bits 0..23 only).
+#ifndef FL_SMEM_STACK
+#define FL_SMEM_STACK 8
+#endif
+constexpr int kSmemStack = FL_SMEM_STACK;
+static_assert(kSmemStack > 0 && kSmemStack < kTraversalStack, "shared part of the traversal stack");
+struct TravStack {
+    uint2 *sm;         // this lane's column
+    uint32_t stride;   // threads per block
+    uint2 spill[kTraversalStack - kSmemStack];
+    __device__ __forceinline__ void put(int k, uint2 v) {
+        if (k < kSmemStack) sm[k * stride] = v;
+        else spill[k - kSmemStack] = v;
+    }
+    __device__ __forceinline__ uint2 get(int k) const { return k < kSmemStack ? sm[k * stride] : spill[k - kSmemStack]; }
+};
+// shared memory a block of `threads` traversal threads needs for its stacks
+constexpr size_t trav_stack_smem_bytes(int threads) { return (size_t)threads * kSmemStack * sizeof(uint2); }
+__device__ __forceinline__ void trav_stack_bind(TravStack &st, uint2 *smem) {
+    st.sm = smem + threadIdx.x;
+    st.stride = blockDim.x;
+}
+
+// Triangle groups are tested when at least this many lanes of the warp test triangles;
+// with fewer, the group is pushed and the lanes keep traversing nodes, so that triangle
+// tests run with more lanes active (Ylitie, Karras and Laine, HPG 2017). 0 disables it.
+#ifndef FL_POSTPONE_LANES
+#define FL_POSTPONE_LANES 0
+#endif
+constexpr int kPostponeLanes = FL_POSTPONE_LANES;
+
 // One traversal step: visit the next node (if any) and test its triangles, then pop.
 // Returns true when the ray is finished (no work left, any-hit found, or a bound hit).
 template <bool COUNT>
-__device__ __forceinline__ bool trav_step(TravState &s, uint2 *stack, const WideNode *__restrict__ nodes,
+__device__ __forceinline__ bool trav_step(TravState &s, TravStack &stack, const WideNode *__restrict__ nodes,
                                           uint32_t n_nodes, const float4 *__restrict__ tris, uint32_t n_tris,
                                           const RayPre &r, bool any_hit, bool &error, TraceStats &stats) {
     if (++s.iter > kTraversalIterLimit) {
@@ -80,7 +115,7 @@ __device__ __forceinline__ bool trav_step(TravState &s, uint2 *stack, const Wide
             return true;
         }
         if (s.ng.y > 0x00ffffffu) {
-            if (s.sp < kTraversalStack) stack[s.sp++] = s.ng;
+            if (s.sp < kTraversalStack) stack.put(s.sp++, s.ng);
             else { error = true; return true; }
         }
         const uint4 *np = reinterpret_cast<const uint4 *>(nodes + ni);
@@ -127,6 +162,12 @@ __device__ __forceinline__ bool trav_step(TravState &s, uint2 *stack, const Wide
         s.tg = make_uint2(w1.y, hitmask & 0x00ffffffu);
     }
     while (s.tg.y) {
+        if (kPostponeLanes > 0 && __popc(__activemask()) < kPostponeLanes && s.ng.y > 0x00ffffffu &&
+            s.sp < kTraversalStack) {
+            stack.put(s.sp++, s.tg);  // test these with more lanes after the next nodes
+            s.tg.y = 0u;
+            break;
+        }
         const int b = __ffs(s.tg.y) - 1;
         s.tg.y &= s.tg.y - 1u;
         const uint32_t ti = s.tg.x + (uint32_t)b;
@@ -152,7 +193,9 @@ __device__ __forceinline__ bool trav_step(TravState &s, uint2 *stack, const Wide
     }
     if (s.ng.y <= 0x00ffffffu) {
         if (s.sp == 0) return true;
-        s.ng = stack[--s.sp];
+        const uint2 e = stack.get(--s.sp);
+        if (e.y > 0x00ffffffu) s.ng = e;     // a node group
+        else { s.tg = e; s.ng.y = 0u; }      // a postponed triangle group
     }
     return false;
 }
@@ -161,11 +204,10 @@ __device__ __forceinline__ bool trav_step(TravState &s, uint2 *stack, const Wide
 template <bool ANY_HIT, bool COUNT>
 __device__ __forceinline__ TraceResult traverse(const WideNode *__restrict__ nodes, uint32_t n_nodes,
                                                 const float4 *__restrict__ tris, uint32_t n_tris, const RayPre &r,
-                                                bool &error, TraceStats &stats) {
+                                                TravStack &stack, bool &error, TraceStats &stats) {
     TravState s;
     trav_init(s, r);
     if (!r.valid || n_nodes == 0) return s.res;
-    uint2 stack[kTraversalStack];
     while (!trav_step<COUNT>(s, stack, nodes, n_nodes, tris, n_tris, r, ANY_HIT, error, stats)) {
     }
     return s.res;
@@ -176,10 +218,12 @@ __device__ __forceinline__ TraceResult traverse(const WideNode *__restrict__ nod
 // begin(q) -> bool (false: nothing to trace, already finished), finish(), the traversal
 // state (st, ray, any_hit) and the acceleration structure it traverses (nodes, n_nodes,
 // tris, n_tris), which begin() may choose per item. Call with all 32 lanes of the warp.
+// `smem` holds the block's traversal stacks (trav_stack_smem_bytes(blockDim.x)).
 template <int STEPS, bool COUNT, class Item>
 __device__ __forceinline__ void persistent_trace(Item &it, uint32_t *fetch_counter, uint32_t n, bool &error,
-                                                 TraceStats &stats) {
-    uint2 stack[kTraversalStack];
+                                                 TraceStats &stats, uint2 *smem) {
+    TravStack stack;
+    trav_stack_bind(stack, smem);
     bool has = false;
     bool exhausted = false;
     const int lane = threadIdx.x & 31;

@@ -25,7 +25,7 @@ METALS_PATH = os.path.join(ROOT, "tests", "golden", "metal_tables.npz")
 EXPORTED = [
     "fl_context_create", "fl_context_destroy", "fl_status_string", "fl_last_error", "fl_context_binned_tables",
     "fl_scene_create", "fl_scene_destroy", "fl_scene_get_info", "fl_trace_closest", "fl_trace_occluded",
-    "fl_trace_count", "fl_render", "fl_render_noalloc", "fl_server_create", "fl_server_destroy",
+    "fl_trace_count", "fl_render", "fl_li", "fl_render_noalloc", "fl_server_create", "fl_server_destroy",
     "fl_server_add_scene", "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_get_stats",
     "fl_guide_create", "fl_guide_destroy", "fl_guide_render", "fl_guide_render_timed", "fl_guide_get_weights",
     "fl_guide_set_weights", "fl_guide_get_info", "fl_guide_gradient", "fl_guide_eval", "fl_guide_get_records",
@@ -68,6 +68,7 @@ def lib():
         L.fl_trace_count.argtypes = [vp, vp, vp, C.c_uint32, C.c_int32, P(C.c_uint64), P(C.c_uint64)]
         L.fl_render.argtypes = [vp, P(T.fl_camera), P(T.fl_render_params), vp, vp, C.c_int32, P(T.fl_render_stats)]
         L.fl_render_noalloc.argtypes = [vp, P(T.fl_camera), P(T.fl_render_params), vp, vp, P(T.fl_render_stats)]
+        L.fl_li.argtypes = [vp, P(T.fl_render_params), vp, vp, vp, vp, C.c_uint32, vp, vp, vp, C.c_int32]
         L.fl_server_create.argtypes = [vp, P(T.fl_server_config), P(vp)]
         L.fl_server_destroy.argtypes = [vp]
         L.fl_server_add_scene.argtypes = [vp, P(T.fl_scene_desc), P(C.c_uint64)]
@@ -281,6 +282,23 @@ class SceneHandle:
         check(lib().fl_render(self.h, C.byref(cam), C.byref(params), _ptr(film_rgb), xyz, mem, C.byref(stats)),
               self.ctx.h)
         return film_rgb, {k: getattr(stats, k) for k, _ in T.fl_render_stats._fields_}
+
+
+def li(scene: "SceneHandle", params, org, dirs, rng_state, lambda0=None):
+    """Integrator::Li for a batch of host rays (fl_li): returns (radiance (n, NL) float32,
+    generator states after the paths (n,) uint64, XYZ (n, 3) float64)."""
+    n = org.shape[0]
+    nl = 60 if params.spectral_mode == T.FL_SPECTRAL_BINS60 else 4
+    org = np.ascontiguousarray(org, np.float32)
+    dirs = np.ascontiguousarray(dirs, np.float32)
+    rng = np.ascontiguousarray(rng_state, np.uint64)
+    lam = None if lambda0 is None else np.ascontiguousarray(lambda0, np.float32)
+    L = np.zeros((n, nl), np.float32)
+    rng_out = np.zeros(n, np.uint64)
+    xyz = np.zeros((n, 3), np.float64)
+    check(lib().fl_li(scene.h, C.byref(params), _ptr(org), _ptr(dirs), _ptr(rng), _ptr(lam) if lam is not None else None,
+                      n, _ptr(L), _ptr(rng_out), _ptr(xyz), T.FL_MEM_HOST), scene.ctx.h)
+    return L, rng_out, xyz
 
 
 class Guide:

@@ -125,11 +125,17 @@ class Scene:
         return cam
 
 
-def render_params(spp, max_depth, mode=T.FL_SPECTRAL_HERO4, rr=1.0, wave_paths=0, sample_offset=0, flags=0):
+def render_params(spp, max_depth, mode=T.FL_SPECTRAL_HERO4, rr=1.0, wave_paths=0, sample_offset=0, flags=0,
+                  depths=None):
+    """fl_render_params; depths=(diffuse, reflection, transmission) sets RenderParams' three
+    depths (FL_RENDER_LOBE_DEPTHS) in place of max_depth for all three."""
     p = T.fl_render_params()
     p.flags = flags
     p.spp = spp
     p.max_depth = max_depth
+    if depths is not None:
+        p.flags |= T.FL_RENDER_LOBE_DEPTHS
+        p.diffuse_depth, p.reflection_depth, p.transmission_depth = (int(d) for d in depths)
     p.rr_threshold = rr
     p.spectral_mode = mode
     p.wave_paths = wave_paths

@@ -34,6 +34,8 @@ FL_SPECTRAL_BINS60 = 1
 FL_RENDER_PROFILE = 1
 FL_RENDER_COUNT = 2
 FL_RENDER_CORRECTED_GGX = 4
+FL_RENDER_LOBE_DEPTHS = 8
+FL_MAX_BOUNCES = 250
 FL_MAT_STANDARD = 4
 FL_FRESNEL_DIELECTRIC = 0
 FL_FRESNEL_METALLIC = 1
@@ -168,6 +170,10 @@ class fl_render_params(C.Structure):
         ("sample_offset", C.c_uint32),
         ("flags", C.c_int32),
         ("reserved", C.c_int32),
+        ("diffuse_depth", C.c_int32),
+        ("reflection_depth", C.c_int32),
+        ("transmission_depth", C.c_int32),
+        ("reserved2", C.c_int32),
     ]
 
 
@@ -186,6 +192,7 @@ class fl_render_stats(C.Structure):
         ("ms_continue", C.c_double),
         ("nodes_visited", C.c_uint64),
         ("tris_tested", C.c_uint64),
+        ("paths_cut", C.c_uint64),
     ]
 
 

@@ -305,20 +305,38 @@ enum {
 enum {
     FL_RENDER_PROFILE = 1,  /* time each kernel class with CUDA events (fl_render_stats.ms_*) */
     FL_RENDER_COUNT = 2,    /* count BVH nodes and triangles visited (instrumented traversal) */
-    FL_RENDER_CORRECTED_GGX = 4 /* corrected GGX: the density of the visible normals the sampler draws,
+    FL_RENDER_CORRECTED_GGX = 4, /* corrected GGX: the density of the visible normals the sampler draws,
                                    sampled on wo's side (the reference keeps D |cos| and the upper
                                    hemisphere, microfacet.cpp:14-16, ggx.cpp:32-57) */
+    FL_RENDER_LOBE_DEPTHS = 8    /* depths per sampled lobe kind (diffuse_depth, reflection_depth,
+                                   transmission_depth) instead of max_depth for all three */
 };
+
+/* The most bounces a path can take (bounce indices 0..FL_MAX_BOUNCES-1). With unequal lobe
+ * depths a path is ended only by the depth of the lobe kind it samples, at that exact
+ * bounce, so it can outlive the deepest of them until Russian roulette ends it; a path
+ * still going at this bound is cut, counted in fl_render_stats.paths_cut, and the call
+ * returns FL_ERR_TRAVERSAL (the image holds everything else). */
+#define FL_MAX_BOUNCES 250
 
 typedef struct {
     int32_t spp;            /* samples per pixel */
-    int32_t max_depth;      /* RenderParams diffuse = reflection = transmission depth (core/renderparams.h:5-10) */
+    int32_t max_depth;      /* RenderParams diffuse = reflection = transmission depth (core/renderparams.h:5-10),
+                               0..249; ignored with FL_RENDER_LOBE_DEPTHS */
     float rr_threshold;     /* PathIntegrator rrThreshold (pathintegrator.h:11-12), 1 by default */
     int32_t spectral_mode;  /* FL_SPECTRAL_* */
     int32_t wave_paths;     /* paths in flight per wavefront (0 = library default) */
     uint32_t sample_offset; /* first sample index (progressive / multi-GPU sample split) */
     int32_t flags;          /* FL_RENDER_* */
     int32_t reserved;
+    /* FL_RENDER_LOBE_DEPTHS: RenderParams' three depths (core/renderparams.h:5-10), each 0..249.
+     * PathIntegrator::Li (integrators/pathintegrator.cpp:55-65) ends a path at bounce b when
+     * the lobe it sampled there is diffuse and b == diffuse_depth, specular or glossy and
+     * b == reflection_depth, or a transmission and b == transmission_depth. */
+    int32_t diffuse_depth;
+    int32_t reflection_depth;
+    int32_t transmission_depth;
+    int32_t reserved2;
 } fl_render_params;
 
 typedef struct {
@@ -337,6 +355,7 @@ typedef struct {
     /* FL_RENDER_COUNT: traversal work of all rays */
     uint64_t nodes_visited;
     uint64_t tris_tested;
+    uint64_t paths_cut;      /* paths ended at FL_MAX_BOUNCES (only with unequal lobe depths) */
 } fl_render_stats;
 
 /* Renders the image: for pixel p and sample s the PCG32 stream is seeded with
@@ -346,6 +365,26 @@ typedef struct {
  * film_xyz64 (nullable) receives the FP64 XYZ sums (not divided by spp). */
 FL_API fl_status fl_render(fl_scene *scene, const fl_camera *camera, const fl_render_params *params,
                     float *film_rgb, double *film_xyz64, int32_t memory, fl_render_stats *stats);
+
+/* Integrator::Li (integrators/integrator.h:17-18; PathIntegrator::Li,
+ * integrators/pathintegrator.cpp:12-87) for a batch of n rays: the radiance each ray brings
+ * back. Path i draws its random numbers from its own PCG32 generator (src/ext/pcg32.h) whose
+ * 64-bit state the caller passes in rng_state[i], on the reference sampler's default stream
+ * (initseq 1, increment 3), in the reference's order (per light: uLight, uScatter; then the
+ * BSDF sample; then Russian roulette): the Sampler argument of Li. params: spectral_mode, the
+ * depths, rr_threshold and FL_RENDER_CORRECTED_GGX as for fl_render (spp, wave_paths,
+ * sample_offset and the other flags are not used). Rays as for fl_trace_closest (the ray's
+ * tMin is the third constructor argument of the reference's Ray). lambda0: each ray's hero
+ * wavelength in [380, 720) (FL_SPECTRAL_HERO4; ignored, nullable, with 60 bins). Outputs:
+ *   radiance  n * 60 floats (FL_SPECTRAL_BINS60, the PrincipalSpectrum Li returns) or n * 4
+ *             (the hero wavelengths' samples)
+ *   rng_out   the generator state after the path (nullable): the sampler after Li returns
+ *   xyz       to_xyz of each radiance (nullable), n * 3 doubles, what fl_render's film adds
+ * All pointers are host or device memory according to `memory`. The per-ray form of the
+ * reference is this call with n = 1 (slow: one launch sequence per call). */
+FL_API fl_status fl_li(fl_scene *scene, const fl_render_params *params, const float *org_tmin, const float *dir_tmax,
+                       const uint64_t *rng_state, const float *lambda0, uint32_t n, float *radiance,
+                       uint64_t *rng_out, double *xyz, int32_t memory);
 
 /* ------------------------------------------------------------------------- */
 /* Serving: continuous batching of render jobs (no counterpart in the reference) */

@@ -9,16 +9,19 @@
 //   Scene (geometry + illuminants, owns its BVH)   src/filianore/core/scene.h:12-27
 //   RenderParams                                    src/filianore/core/renderparams.h:5-10
 //   PathIntegrator(RenderParams, rrThreshold)       src/filianore/integrators/pathintegrator.h:9-22
+//     with Li(ray, scene, sampler, depth)           src/filianore/integrators/integrator.h:17-18
 //   PhysicalCamera (position, look-at, up, fov)     src/filianore/cameras/physical.h:11-43
+//     with awaken_ray                               src/filianore/cameras/physical.cpp:12-22
+//   PCG32Sampler (a Sampler over pcg32)             src/filianore/sampling/sampler.h:10-19, src/ext/pcg32.h
 // The types are this library's own (plain structs), not the reference's: a maintainer
 // converts at the boundary, as shown in the integration notes.
 //
 // Conventions kept from the reference: intersect / intersect_p return bool (hit or not)
 // and shrink ray.tMax on a hit; nothing throws. A failure of the library (no device, out of
 // memory) makes the call report a miss or false and leaves the message in last_error().
-// The GPU's granularity differs in one place: PathIntegrator renders whole images
-// (render), the replacement of the application's loop over Integrator::Li, instead of one
-// camera ray at a time.
+// The GPU's granularity: PathIntegrator renders whole images (render), the replacement of
+// the application's loop over Integrator::Li; Li itself is there for single rays and batches
+// (one device launch sequence per call, so slow per ray).
 #ifndef FILIANORE_GPU_HPP
 #define FILIANORE_GPU_HPP
 
@@ -80,11 +83,122 @@ struct RenderParams {
     int transmissionRayDepth = 8;
 };
 
+// The reference's 60-bin spectrum (color/principalspectrum.h:7-21), as Li returns it.
+struct PrincipalSpectrum {
+    float c[60] = {};
+};
+
+// A Sampler over O'Neill's PCG32 (the generator of src/ext/pcg32.h), the sampler the GPU
+// renders with: seed(pixel, 1) per pixel, get_1d = nextFloat, get_2d = (get_1d, get_1d).
+// Li continues the sampler's stream on the device, which supports the default stream
+// (initseq 1) only.
+class PCG32Sampler {
+public:
+    uint64_t state = 0x853c49e6748fea9bULL, inc = 0xda3e39cb94b95bdbULL;
+    void seed(uint64_t initstate, uint64_t initseq = 1u) {
+        state = 0u;
+        inc = (initseq << 1u) | 1u;
+        next_uint();
+        state += initstate;
+        next_uint();
+    }
+    uint32_t next_uint() {
+        const uint64_t old = state;
+        state = old * 0x5851f42d4c957f2dULL + inc;
+        const uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+        const uint32_t rot = (uint32_t)(old >> 59u);
+        return (xorshifted >> rot) | (xorshifted << ((~rot + 1u) & 31));
+    }
+    float get_1d() {
+        union {
+            uint32_t u;
+            float f;
+        } x;
+        x.u = (next_uint() >> 9) | 0x3f800000u;
+        return x.f - 1.0f;
+    }
+    Vector2f get_2d() {
+        const float a = get_1d();
+        const float b = get_1d();
+        return Vector2f{a, b};
+    }
+    // jump ahead by delta draws (Brown's method, as pcg32::advance)
+    void advance(uint64_t delta) {
+        uint64_t cur_mult = 0x5851f42d4c957f2dULL, cur_plus = inc, acc_mult = 1u, acc_plus = 0u;
+        while (delta > 0) {
+            if (delta & 1) {
+                acc_mult *= cur_mult;
+                acc_plus = acc_plus * cur_mult + cur_plus;
+            }
+            cur_plus = (cur_mult + 1) * cur_plus;
+            cur_mult *= cur_mult;
+            delta /= 2;
+        }
+        state = acc_mult * state + acc_plus;
+    }
+};
+
 struct PhysicalCamera {
     Vector3f position, lookAt, up{0.f, 1.f, 0.f};
     float fov = 40.f;  // vertical, degrees
     int xRes = 256, yRes = 256;
     float aperture = 0.f;  // lens diameter, focused at lookAt (0: pinhole)
+
+    // PhysicalCamera::awaken_ray (cameras/physical.cpp:12-22) for a pinhole, with the
+    // constructor's basis (physical.h:11-43, flipCameraDirection = true) in the reference's
+    // operation order: the ray the device renders for camera sample s (x, y in [0, 1]).
+    Ray awaken_ray(const Vector2f &s) const {
+        const Vector3f pos = position;
+        const float focusDistance = length(sub(pos, lookAt));
+        const float theta = fov * 3.14159265358979323846f / 180.f;
+        const float halfHeight = std::tan(theta / 2.f);
+        const float aspect = (float)xRes / (float)yRes;
+        const float halfWidth = aspect * halfHeight;
+        Vector3f w = normalize(sub(pos, lookAt));
+        w = mul(w, -1.f);
+        const Vector3f u = normalize(cross(up, w));
+        const Vector3f v = cross(w, u);
+        w = mul(w, -1.f);
+        const Vector3f lowerLeft =
+            sub(sub(sub(pos, mul(mul(u, halfWidth), focusDistance)), mul(mul(v, focusDistance), halfHeight)),
+                mul(w, focusDistance));
+        const Vector3f horizontal = mul(mul(mul(u, 2.f), halfWidth), focusDistance);
+        const Vector3f vertical = mul(mul(mul(v, 2.f), halfHeight), focusDistance);
+        // random_point_on_lens((0.5, 0.5)) * lensRadius with lensRadius 0 for a pinhole
+        const Vector3f rd = mul(sub(mul(Vector3f{0.5f, 0.5f, 0.f}, 2.f), Vector3f{1.f, 1.f, 0.f}), 0.f);
+        const Vector3f offset = add(mul(u, rd.x), mul(v, rd.y));
+        Ray r;
+        r.origin = add(pos, offset);
+        r.dir = normalize(sub(sub(add(add(lowerLeft, mul(horizontal, s.x)), mul(vertical, s.y)), pos), offset));
+        r.tMin = 0.f;  // time0 + s.x (time1 - time0) with no shutter interval
+        return r;
+    }
+    // The render loop's camera ray of pixel (px, py), row 0 at the top: the sampler draws
+    // (ux, uy) and then the hero wavelength's number, as the device does.
+    Ray pixel_ray(int px, int py, PCG32Sampler &sampler, float *u_lambda = nullptr) const {
+        const float ux = sampler.get_1d(), uy = sampler.get_1d();
+        const float ul = sampler.get_1d();
+        if (u_lambda) *u_lambda = ul;
+        const float sx = ((float)px + ux) / (float)xRes;
+        const float sy = ((float)(yRes - 1 - py) + uy) / (float)yRes;
+        return awaken_ray(Vector2f{sx, sy});
+    }
+
+private:
+    // maths/geometry.h's operations: products as s * x, cross in double, normalize by the
+    // reciprocal of the length
+    static Vector3f add(Vector3f a, Vector3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+    static Vector3f sub(Vector3f a, Vector3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+    static Vector3f mul(Vector3f a, float s) { return {s * a.x, s * a.y, s * a.z}; }
+    static float length(Vector3f a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+    static Vector3f normalize(Vector3f a) {
+        const float inv = 1.f / length(a);
+        return {a.x * inv, a.y * inv, a.z * inv};
+    }
+    static Vector3f cross(Vector3f a, Vector3f b) {
+        const double ax = a.x, ay = a.y, az = a.z, bx = b.x, by = b.y, bz = b.z;
+        return {(float)((ay * bz) - (az * by)), (float)((az * bx) - (ax * bz)), (float)((ax * by) - (ay * bx))};
+    }
 };
 
 // An illuminant: a triangle of the soup (DiffuseAreaIlluminant), a point, spot or
@@ -307,8 +421,10 @@ private:
     bool ok_ = false;
 };
 
-// The path tracer. Its depths follow RenderParams; the device path uses one maximum depth,
-// so the three depths must be equal (the reference configurations set them equal).
+// The path tracer, with RenderParams' three depths: a path ends at bounce b when the lobe
+// it samples there is diffuse and b == diffuseRayDepth, specular or glossy and
+// b == reflectionRayDepth, or a transmission and b == transmissionRayDepth
+// (pathintegrator.cpp:55-65).
 class PathIntegrator {
 public:
     explicit PathIntegrator(const RenderParams &renderParams, float rrThreshold = 1.f)
@@ -319,11 +435,6 @@ public:
     // Returns false (message in last_error()) when the library fails.
     bool render(const Scene &scene, const PhysicalCamera &camera, std::vector<float> &rgb,
                 int spectral_mode = FL_SPECTRAL_BINS60, fl_render_stats *stats = nullptr) const {
-        if (renderParams.diffuseRayDepth != renderParams.reflectionRayDepth ||
-            renderParams.diffuseRayDepth != renderParams.transmissionRayDepth) {
-            error_ = "the device path traces with one depth: diffuse, reflection and transmission depths must match";
-            return false;
-        }
         fl_camera cam{};
         cam.position[0] = camera.position.x, cam.position[1] = camera.position.y, cam.position[2] = camera.position.z;
         cam.look_at[0] = camera.lookAt.x, cam.look_at[1] = camera.lookAt.y, cam.look_at[2] = camera.lookAt.z;
@@ -332,11 +443,8 @@ public:
         cam.aperture = camera.aperture;
         cam.width = camera.xRes;
         cam.height = camera.yRes;
-        fl_render_params p{};
+        fl_render_params p = params(spectral_mode);
         p.spp = renderParams.samples;
-        p.max_depth = renderParams.diffuseRayDepth;
-        p.rr_threshold = rrThreshold;
-        p.spectral_mode = spectral_mode;
         rgb.assign((size_t)camera.xRes * camera.yRes * 3, 0.f);
         const fl_status st = fl_render(scene.bvh.get(), &cam, &p, rgb.data(), nullptr, FL_MEM_HOST, stats);
         if (st != FL_OK) {
@@ -345,12 +453,67 @@ public:
         }
         return true;
     }
+
+    // Integrator::Li (integrators/integrator.h:18): the radiance along `ray`, the path drawing
+    // its numbers from `sampler`, which is left where the path stopped drawing. `depth` is
+    // unused, as in the reference. 60 bins; xyz (nullable) receives to_xyz of the result.
+    // A miss (no scene, a library failure) returns black and sets last_error().
+    PrincipalSpectrum Li(const Ray &ray, const Scene &scene, PCG32Sampler &sampler, int depth = 0,
+                         double xyz[3] = nullptr) const {
+        PrincipalSpectrum L;
+        Li(&ray, 1, scene, &sampler, &L, depth, xyz);
+        return L;
+    }
+    // Li for n rays in one device call: rays[i] with samplers[i] into out[i] (xyz: 3 per ray).
+    bool Li(const Ray *rays, uint32_t n, const Scene &scene, PCG32Sampler *samplers, PrincipalSpectrum *out,
+            int depth = 0, double *xyz = nullptr) const {
+        (void)depth;
+        if (!scene.bvh.get()) {
+            error_ = "Li without a scene";
+            return false;
+        }
+        std::vector<float> o(4 * (size_t)n), d(4 * (size_t)n);
+        std::vector<uint64_t> rng(n), rng_out(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            if (samplers[i].inc != 3u) {
+                error_ = "the device continues the default PCG32 stream (initseq 1) only";
+                return false;
+            }
+            const Ray &r = rays[i];
+            o[4 * i] = r.origin.x, o[4 * i + 1] = r.origin.y, o[4 * i + 2] = r.origin.z, o[4 * i + 3] = r.tMin;
+            d[4 * i] = r.dir.x, d[4 * i + 1] = r.dir.y, d[4 * i + 2] = r.dir.z, d[4 * i + 3] = r.tMax;
+            rng[i] = samplers[i].state;
+        }
+        const fl_render_params p = params(FL_SPECTRAL_BINS60);
+        const fl_status st = fl_li(scene.bvh.get(), &p, o.data(), d.data(), rng.data(), nullptr, n,
+                                   reinterpret_cast<float *>(out), rng_out.data(), xyz, FL_MEM_HOST);
+        static_assert(sizeof(PrincipalSpectrum) == 60 * sizeof(float), "60 packed floats");
+        if (st != FL_OK) {
+            error_ = std::string(fl_status_string(st));
+            for (uint32_t i = 0; i < n; ++i) out[i] = PrincipalSpectrum{};
+            return false;
+        }
+        for (uint32_t i = 0; i < n; ++i) samplers[i].state = rng_out[i];
+        return true;
+    }
     const std::string &last_error() const { return error_; }
 
     const RenderParams renderParams;
     const float rrThreshold;
 
 private:
+    fl_render_params params(int spectral_mode) const {
+        fl_render_params p{};
+        p.spp = 1;
+        p.max_depth = renderParams.diffuseRayDepth;
+        p.rr_threshold = rrThreshold;
+        p.spectral_mode = spectral_mode;
+        p.flags = FL_RENDER_LOBE_DEPTHS;
+        p.diffuse_depth = renderParams.diffuseRayDepth;
+        p.reflection_depth = renderParams.reflectionRayDepth;
+        p.transmission_depth = renderParams.transmissionRayDepth;
+        return p;
+    }
     mutable std::string error_;
 };
 

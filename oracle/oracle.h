@@ -99,6 +99,11 @@ void orc_camera_init(const fl_camera *c, orc_camera *out);
 /* one camera ray for (pixel, sample) plus the hero-wavelength draw; returns 3 floats used */
 void orc_camera_ray(const orc_camera *cam, const fl_camera *c, uint32_t pixel, orc_pcg32 *rng,
                     v3 *o, v3 *d, float *u_lambda);
+void orc_camera_rays(const fl_camera *cam, const uint32_t *pixels, uint32_t n, uint32_t sample, float *org_tmin,
+                     float *dir_tmax, uint64_t *rng_state, float *lambda0);
+int orc_li(const fl_scene_desc *sc, const orc_tables *tab, const fl_render_params *P, uint32_t n,
+           const float *org_tmin, const float *dir_tmax, const uint64_t *rng_state, const float *lambda0,
+           float *radiance, uint64_t *rng_out, double *xyz);
 
 /* spectral upsampling used by materials: 60 bins or hero wavelengths */
 void orc_reflectance(const orc_tables *t, const float rgb[3], int mode, const float *lambda, float *out);

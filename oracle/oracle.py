@@ -24,8 +24,10 @@ REF_BIN = os.path.join(HERE, "_ref", "ref_render")
 _lib = None
 
 
-def build(ref: bool = False) -> None:
-    targets = ["all"] + (["ref"] if ref else [])
+def build(ref: bool = False, ref_dir: str | None = None) -> None:
+    """liboracle.so; with ref, also _ref/ref_render from the reference tree ref_dir (default:
+    $FL_REFERENCE_DIR)."""
+    targets = ["all"] + (["ref"] if ref else []) + ([f"REF={ref_dir}"] if ref and ref_dir else [])
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
@@ -54,6 +56,11 @@ def lib():
         L.orc_render.argtypes = [P(T.fl_scene_desc), C.c_void_p, P(T.fl_camera), P(T.fl_render_params), C.c_void_p,
                                  P(C.c_double), C.c_void_p]
         L.orc_render.restype = C.c_int
+        L.orc_camera_rays.argtypes = [P(T.fl_camera), P(C.c_uint32), C.c_uint32, C.c_uint32, P(C.c_float),
+                                      P(C.c_float), P(C.c_uint64), P(C.c_float)]
+        L.orc_li.argtypes = [P(T.fl_scene_desc), C.c_void_p, P(T.fl_render_params), C.c_uint32, P(C.c_float),
+                             P(C.c_float), P(C.c_uint64), P(C.c_float), P(C.c_float), P(C.c_uint64), P(C.c_double)]
+        L.orc_li.restype = C.c_int
         L.orc_guide_eval.argtypes = [P(C.c_float), P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float)]
         L.orc_guide_gradient.argtypes = [P(C.c_float), P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float),
                                          P(C.c_float)]
@@ -194,9 +201,44 @@ def render(scene, tables: Tables, params, nthreads=None, pixels=None, width=None
                                    "bounces": cnt.bounces}
 
 
+def camera_rays(scene, pixels, sample=0, width=None, height=None):
+    """the render loop's camera rays of `sample` for the given pixels: (org_tmin (n, 4),
+    dir_tmax (n, 4), generator state after the camera's draws (n,) uint64, hero wavelength (n,))"""
+    cam = scene.camera_struct(width, height)
+    px = np.ascontiguousarray(pixels, np.uint32)
+    n = px.shape[0]
+    org = np.zeros((n, 4), np.float32)
+    dirs = np.zeros((n, 4), np.float32)
+    rng = np.zeros(n, np.uint64)
+    lam = np.zeros(n, np.float32)
+    lib().orc_camera_rays(C.byref(cam), px.ctypes.data_as(C.POINTER(C.c_uint32)), n, sample, _fp(org), _fp(dirs),
+                          rng.ctypes.data_as(C.POINTER(C.c_uint64)), _fp(lam))
+    return org, dirs, rng, lam
+
+
+def li(scene, tables: Tables, params, org, dirs, rng_state, lambda0):
+    """PathIntegrator::Li of the oracle for n given rays: (radiance (n, NL), generator
+    state after each path (n,), XYZ (n, 3))"""
+    desc, keep = scene.desc()
+    n = org.shape[0]
+    nl = 60 if params.spectral_mode == T.FL_SPECTRAL_BINS60 else 4
+    org = np.ascontiguousarray(org, np.float32)
+    dirs = np.ascontiguousarray(dirs, np.float32)
+    rng = np.ascontiguousarray(rng_state, np.uint64)
+    lam = np.ascontiguousarray(lambda0, np.float32)
+    L = np.zeros((n, nl), np.float32)
+    rng_out = np.zeros(n, np.uint64)
+    xyz = np.zeros((n, 3), np.float64)
+    rc = lib().orc_li(C.byref(desc), tables.buf, C.byref(params), n, _fp(org), _fp(dirs),
+                      rng.ctypes.data_as(C.POINTER(C.c_uint64)), _fp(lam), _fp(L),
+                      rng_out.ctypes.data_as(C.POINTER(C.c_uint64)), xyz.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rc == 0, "orc_li failed"
+    return L, rng_out, xyz
+
+
 # ----------------------------------------------------------------------------- reference binary
 
-SCENE_MAGIC = b"FLSCENE1"
+SCENE_MAGIC = b"FLSCENE2"
 
 
 def write_scene_file(path, scene, params, nthreads=0, pixels=None, width=None, height=None):
@@ -204,8 +246,13 @@ def write_scene_file(path, scene, params, nthreads=0, pixels=None, width=None, h
     cam = scene.camera_struct(width, height)
     px = np.ascontiguousarray(pixels if pixels is not None else np.zeros(0), np.uint32)
     hdr = bytearray(SCENE_MAGIC)
+    if params.flags & T.FL_RENDER_LOBE_DEPTHS:
+        depths = [params.diffuse_depth, params.reflection_depth, params.transmission_depth]
+    else:
+        depths = [params.max_depth] * 3
     hdr += np.array([scene.n_tri, len(scene.materials), len(scene.lights), params.spp, params.max_depth,
-                     params.spectral_mode, params.sample_offset, nthreads, px.shape[0]], np.uint32).tobytes()
+                     params.spectral_mode, params.sample_offset, nthreads, px.shape[0]] + depths,
+                    np.uint32).tobytes()
     hdr += np.array([params.rr_threshold], np.float32).tobytes()
     hdr += bytes(cam)
     with open(path, "wb") as f:

@@ -1225,16 +1225,22 @@ static void estimate_direct(const scene_ctx *S, const isect_t *it, const bsdf_t 
 }
 
 /* PathIntegrator::Li, pathintegrator.cpp:12-87 */
-static void path_Li(const scene_ctx *S, const fl_render_params *P, v3 o, v3 d, float tmin, const float *lambda,
-                    orc_pcg32 *rng, spec *L, counters *cn) {
+static void path_Li(const scene_ctx *S, const fl_render_params *P, v3 o, v3 d, float tmin, float tmax,
+                    const float *lambda, orc_pcg32 *rng, spec *L, counters *cn) {
     const int nl = S->nl;
     spec beta;
     sp_set(L, nl, 0.f);
     sp_set(&beta, nl, 1.f);
-    ray3 ray = {o, d, tmin, INF_F};
+    ray3 ray = {o, d, tmin, tmax};
     int specularBounce = 0;
     float etaScale = 1.f;
-    const int depth = P->max_depth;
+    /* RenderParams (core/renderparams.h:5-10): diffuse, reflection, transmission depth */
+    int depth[3] = {P->max_depth, P->max_depth, P->max_depth};
+    if (P->flags & FL_RENDER_LOBE_DEPTHS) {
+        depth[0] = P->diffuse_depth;
+        depth[1] = P->reflection_depth;
+        depth[2] = P->transmission_depth;
+    }
     const float rrThreshold = P->rr_threshold;
     for (int bounces = 0;; ++bounces) {
         isect_t is;
@@ -1275,9 +1281,10 @@ static void path_Li(const scene_ctx *S, const fl_render_params *P, v3 o, v3 d, f
         float ux = orc_pcg32_nextf(rng), uy = orc_pcg32_nextf(rng);
         bsdf_sample(&b, wo, &wi, ux, uy, &pdf, BSDF_ALL, &flags, &f);
         if (sp_black(&f, nl) || pdf == 0) break;
-        if (depth == bounces && (flags & BSDF_DIFFUSE)) break;
-        if ((depth == bounces && (flags & BSDF_SPECULAR)) || (depth == bounces && (flags & BSDF_GLOSSY))) break;
-        if (depth == bounces && (flags & BSDF_TRANSMISSION)) break;
+        /* pathintegrator.cpp:55-65: the sampled lobe's own depth, tested with == */
+        if (depth[0] == bounces && (flags & BSDF_DIFFUSE)) break;
+        if ((depth[1] == bounces && (flags & BSDF_SPECULAR)) || (depth[1] == bounces && (flags & BSDF_GLOSSY))) break;
+        if (depth[2] == bounces && (flags & BSDF_TRANSMISSION)) break;
         float ad = v3_absdot(wi, is.ns);
         for (int i = 0; i < nl; ++i) beta.c[i] *= f.c[i] * ad / pdf;
         specularBounce = (flags & BSDF_SPECULAR) != 0;
@@ -1363,6 +1370,14 @@ void orc_camera_ray(const orc_camera *cam, const fl_camera *c, uint32_t pixel, o
     *d = v3_norm(dir);
 }
 
+/* hero wavelengths of lambda0: rotation by 85 nm, wrapped into [380, 720) */
+static void hero_lambdas(float l0, float lambda[4]) {
+    for (int j = 0; j < 4; ++j) {
+        float l = l0 + 85.f * (float)j;
+        lambda[j] = l >= 720.f ? l - 340.f : l;
+    }
+}
+
 /* ---------------------------------------------------------------- driver */
 typedef struct {
     const scene_ctx *S;
@@ -1397,15 +1412,9 @@ static void *render_worker(void *argp) {
                 float ul;
                 orc_camera_ray(a->oc, a->cam, pixel, &rng, &o, &d, &ul);
                 float lambda[4];
-                if (S->mode == FL_SPECTRAL_HERO4) {
-                    float l0 = 380.f + ul * 340.f;
-                    for (int j = 0; j < 4; ++j) {
-                        float l = l0 + 85.f * (float)j;
-                        lambda[j] = l >= 720.f ? l - 340.f : l;
-                    }
-                }
+                if (S->mode == FL_SPECTRAL_HERO4) hero_lambdas(380.f + ul * 340.f, lambda);
                 spec L;
-                path_Li(S, a->P, o, d, 0.f, lambda, &rng, &L, &a->cn);
+                path_Li(S, a->P, o, d, 0.f, INF_F, lambda, &rng, &L, &a->cn);
                 double xyz[3];
                 orc_xyz_from_spectrum(S->tab, S->mode, lambda, L.c, xyz);
                 (void)nl;
@@ -1420,9 +1429,7 @@ static void *render_worker(void *argp) {
     return NULL;
 }
 
-int orc_render(const fl_scene_desc *sc, const orc_tables *tab, const fl_camera *cam, const fl_render_params *P,
-               const orc_render_opts *opts, double *film, orc_render_counts *counts) {
-    if (!sc || !tab || !cam || !P || !film || cam->width <= 0 || cam->height <= 0 || P->spp <= 0) return -1;
+static void scene_ctx_init(scene_ctx *Sp, const fl_scene_desc *sc, const orc_tables *tab, const fl_render_params *P) {
     scene_ctx S;
     memset(&S, 0, sizeof(S));
     S.sc = sc;
@@ -1443,7 +1450,20 @@ int orc_render(const fl_scene_desc *sc, const orc_tables *tab, const fl_camera *
     S.mat_refl60 = (spec *)malloc(sizeof(spec) * (sc->n_materials ? sc->n_materials : 1));
     for (uint32_t m = 0; m < sc->n_materials; ++m)
         orc_reflectance(tab, sc->materials[m].rgb, FL_SPECTRAL_BINS60, NULL, S.mat_refl60[m].c);
+    *Sp = S;
+}
 
+static void scene_ctx_free(scene_ctx *S) {
+    orc_bvh_free(S->bvh);
+    free(S->tri_light);
+    free(S->mat_refl60);
+}
+
+int orc_render(const fl_scene_desc *sc, const orc_tables *tab, const fl_camera *cam, const fl_render_params *P,
+               const orc_render_opts *opts, double *film, orc_render_counts *counts) {
+    if (!sc || !tab || !cam || !P || !film || cam->width <= 0 || cam->height <= 0 || P->spp <= 0) return -1;
+    scene_ctx S;
+    scene_ctx_init(&S, sc, tab, P);
     orc_camera oc;
     orc_camera_init(cam, &oc);
     uint32_t total = opts && opts->pixels ? opts->n_pixels : (uint32_t)cam->width * (uint32_t)cam->height;
@@ -1467,9 +1487,57 @@ int orc_render(const fl_scene_desc *sc, const orc_tables *tab, const fl_camera *
         c.bounces += args[k].cn.bounces;
     }
     if (counts) *counts = c;
-    orc_bvh_free(S.bvh);
-    free(S.tri_light);
-    free(S.mat_refl60);
+    scene_ctx_free(&S);
+    return 0;
+}
+
+/* The camera rays of sample `sample` of the given pixels, as the render loop makes them:
+ * (o, tmin 0), (d, tmax inf), the generator state after the camera's draws and the hero
+ * wavelength 380 + 340 u. */
+void orc_camera_rays(const fl_camera *cam, const uint32_t *pixels, uint32_t n, uint32_t sample, float *org_tmin,
+                     float *dir_tmax, uint64_t *rng_state, float *lambda0) {
+    orc_camera oc;
+    orc_camera_init(cam, &oc);
+    for (uint32_t i = 0; i < n; ++i) {
+        orc_pcg32 rng;
+        orc_pcg32_seed(&rng, pixels[i], 1u);
+        if (sample) orc_pcg32_advance(&rng, (int64_t)((uint64_t)sample << 16));
+        v3 o, d;
+        float ul;
+        orc_camera_ray(&oc, cam, pixels[i], &rng, &o, &d, &ul);
+        org_tmin[4 * i] = o.x; org_tmin[4 * i + 1] = o.y; org_tmin[4 * i + 2] = o.z; org_tmin[4 * i + 3] = 0.f;
+        dir_tmax[4 * i] = d.x; dir_tmax[4 * i + 1] = d.y; dir_tmax[4 * i + 2] = d.z; dir_tmax[4 * i + 3] = INF_F;
+        rng_state[i] = rng.state;
+        lambda0[i] = 380.f + ul * 340.f;
+    }
+}
+
+/* PathIntegrator::Li (pathintegrator.cpp:12-87) for n given rays: ray i starts from
+ * generator state rng_state[i] (increment 3) and hero wavelength lambda0[i]; writes its
+ * radiance (NL floats: 60 bins or 4 hero samples), the generator state after the path and
+ * to_xyz of the radiance. The first ray's tmin and tmax are the given ones (Li copies
+ * its ray argument). */
+int orc_li(const fl_scene_desc *sc, const orc_tables *tab, const fl_render_params *P, uint32_t n,
+           const float *org_tmin, const float *dir_tmax, const uint64_t *rng_state, const float *lambda0,
+           float *radiance, uint64_t *rng_out, double *xyz) {
+    if (!sc || !tab || !P) return -1;
+    scene_ctx S;
+    scene_ctx_init(&S, sc, tab, P);
+    counters cn;
+    memset(&cn, 0, sizeof(cn));
+    for (uint32_t i = 0; i < n; ++i) {
+        orc_pcg32 rng = {rng_state[i], 3u};
+        float lambda[4] = {0.f, 0.f, 0.f, 0.f};
+        if (S.mode == FL_SPECTRAL_HERO4) hero_lambdas(lambda0[i], lambda);
+        spec L;
+        v3 o = v3m(org_tmin[4 * i], org_tmin[4 * i + 1], org_tmin[4 * i + 2]);
+        v3 d = v3m(dir_tmax[4 * i], dir_tmax[4 * i + 1], dir_tmax[4 * i + 2]);
+        path_Li(&S, P, o, d, org_tmin[4 * i + 3], dir_tmax[4 * i + 3], lambda, &rng, &L, &cn);
+        for (int k = 0; k < S.nl; ++k) radiance[(size_t)i * S.nl + k] = L.c[k];
+        rng_out[i] = rng.state;
+        orc_xyz_from_spectrum(S.tab, S.mode, lambda, L.c, xyz + 3 * (size_t)i);
+    }
+    scene_ctx_free(&S);
     return 0;
 }
 

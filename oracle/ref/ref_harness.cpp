@@ -121,6 +121,7 @@ private:
 struct SceneFileHeader {
     char magic[8];
     uint32_t n_tri, n_mat, n_light, spp, max_depth, spectral_mode, sample_offset, nthreads, n_pixels;
+    uint32_t diffuse_depth, reflection_depth, transmission_depth;  // RenderParams' three depths
     float rr_threshold;
     fl_camera cam;
 };
@@ -281,7 +282,7 @@ int render(const char *scene_path, const char *out_path, bool forge) {
     FILE *f = fopen(scene_path, "rb");
     if (!f) { fprintf(stderr, "cannot open %s\n", scene_path); return 2; }
     SceneFileHeader h;
-    if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, "FLSCENE1", 8) != 0) {
+    if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, "FLSCENE2", 8) != 0) {
         fprintf(stderr, "bad scene file\n");
         return 2;
     }
@@ -431,7 +432,7 @@ int render(const char *scene_path, const char *out_path, bool forge) {
     PhysicalCamera camera(Vector3f(c.position[0], c.position[1], c.position[2]),
                           Vector3f(c.look_at[0], c.look_at[1], c.look_at[2]), c.width, c.height, c.vfov_deg, 0.f, 0.f,
                           0.f, Vector3f(c.up[0], c.up[1], c.up[2]), true);
-    RenderParams rp{(int)h.spp, (int)h.max_depth, (int)h.max_depth, (int)h.max_depth};
+    RenderParams rp{(int)h.spp, (int)h.diffuse_depth, (int)h.reflection_depth, (int)h.transmission_depth};
     PathIntegrator integrator(rp, h.rr_threshold);
 
     const uint32_t W = (uint32_t)c.width, H = (uint32_t)c.height;

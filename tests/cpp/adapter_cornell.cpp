@@ -1,13 +1,18 @@
 // Drives the C++ adapter (include/filianore_gpu.hpp) the way code written against the
 // reference's classes would: SceneGeometry of BasicTriangles -> Scene (owning its BVH) ->
-// BVH::intersect per ray and BVH::trace in a batch -> PathIntegrator::render. Inputs and
-// outputs are raw little-endian files written and read by tests/test_cpp_adapter.py:
+// BVH::intersect per ray and BVH::trace in a batch -> PathIntegrator::render, and
+// PathIntegrator::Li on the camera rays of PhysicalCamera::awaken_ray with a PCG32Sampler
+// per pixel. Inputs and outputs are raw little-endian files written and read by
+// tests/test_cpp_adapter.py:
 //   adapter_cornell <input> <output>
 // input:  spectral tables (n_cie, y integral, lambda/x/y/z, n_rgb, lambda, refl[7], illum[7]),
 //         soup (n_tri, 9 floats per triangle, material per triangle), materials, lights,
-//         camera, samples, depth, spectral mode, rays (n, origin/tmin and direction/tmax)
+//         camera, samples, the diffuse / reflection / transmission depths, spectral mode,
+//         rays (n, origin/tmin and direction/tmax)
 // output: the image (width * height * 3 floats), then per ray: intersect's (hit, id, t,
-//         tMax after the call) and trace's (id, t)
+//         tMax after the call) and trace's (id, t); then for every pixel, sample 0 (the
+//         sampler seeded with the pixel index): Li's XYZ (3 doubles) from one batch call, and
+//         for the first 16 pixels the XYZ of single-ray Li calls and the sampler state after.
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -48,7 +53,7 @@ int main(int argc, char **argv) {
     std::vector<fl_image> images;
     fl_camera cam{};
     SceneGeometry geometry;
-    int spp = 0, depth = 0, mode = 0;
+    int spp = 0, depth_d = 0, depth_r = 0, depth_t = 0, mode = 0;
     std::vector<Ray> rays;
     try {
         const int n_cie = r.get<int32_t>();
@@ -67,7 +72,8 @@ int main(int argc, char **argv) {
         mats = r.arr<fl_material>(r.get<uint32_t>());
         lights_raw = r.arr<fl_light>(r.get<uint32_t>());
         cam = r.get<fl_camera>();
-        spp = r.get<int32_t>(), depth = r.get<int32_t>(), mode = r.get<int32_t>();
+        spp = r.get<int32_t>(), depth_d = r.get<int32_t>(), depth_r = r.get<int32_t>(), depth_t = r.get<int32_t>();
+        mode = r.get<int32_t>();
         const uint32_t n_rays = r.get<uint32_t>();
         const std::vector<float> org = r.arr<float>(4 * (size_t)n_rays), dir = r.arr<float>(4 * (size_t)n_rays);
         standard = r.arr<fl_standard_surface>(r.get<uint32_t>());
@@ -129,7 +135,9 @@ int main(int argc, char **argv) {
         }
         RenderParams params;
         params.samples = spp;
-        params.diffuseRayDepth = params.reflectionRayDepth = params.transmissionRayDepth = depth;
+        params.diffuseRayDepth = depth_d;
+        params.reflectionRayDepth = depth_r;
+        params.transmissionRayDepth = depth_t;
         PathIntegrator integrator(params);
         PhysicalCamera camera;
         camera.position = {cam.position[0], cam.position[1], cam.position[2]};
@@ -154,6 +162,36 @@ int main(int argc, char **argv) {
             std::fwrite(rec, sizeof(float), 4, out);
             const float b[2] = {(float)batch[i].primitive, batch[i].t};
             std::fwrite(b, sizeof(float), 2, out);
+        }
+        // Integrator::Li on every pixel's camera ray (sample 0), in one batch ...
+        const int W = camera.xRes, H = camera.yRes;
+        std::vector<Ray> cam_rays;
+        std::vector<PCG32Sampler> samplers;
+        for (int p = 0; p < W * H; ++p) {
+            PCG32Sampler sm;
+            sm.seed((uint64_t)p, 1u);
+            cam_rays.push_back(camera.pixel_ray(p % W, p / W, sm));
+            samplers.push_back(sm);
+        }
+        std::vector<PrincipalSpectrum> Ls(cam_rays.size());
+        std::vector<double> xyz(3 * cam_rays.size());
+        if (!integrator.Li(cam_rays.data(), (uint32_t)cam_rays.size(), scene, samplers.data(), Ls.data(), 0,
+                           xyz.data())) {
+            std::fprintf(stderr, "Li: %s\n", integrator.last_error().c_str());
+            rc = 1;
+        }
+        std::fwrite(xyz.data(), sizeof(double), xyz.size(), out);
+        // ... and one ray at a time for the first pixels (the reference's per-ray call)
+        for (int p = 0; p < 16 && p < W * H; ++p) {
+            PCG32Sampler sm;
+            sm.seed((uint64_t)p, 1u);
+            const Ray ray = camera.pixel_ray(p % W, p / W, sm);
+            double one[3] = {0, 0, 0};
+            const PrincipalSpectrum L = integrator.Li(ray, scene, sm, 0, one);
+            std::fwrite(one, sizeof(double), 3, out);
+            const int same_spectrum = std::memcmp(L.c, Ls[p].c, sizeof(L.c)) == 0;
+            const uint64_t rec2[2] = {sm.state, (uint64_t)same_spectrum};
+            std::fwrite(rec2, sizeof(uint64_t), 2, out);
         }
         std::fclose(out);
     }

@@ -12,6 +12,9 @@ reference sources with oracle/Makefile). Outputs:
   cornell_materials_ref.npz  the same with GGX conductor + rough dielectric boxes
                         ("materials") and conductor + smooth glass boxes ("glass"):
                         64x64 at 4 spp (float64) and 128x128 at 16 spp (float32)
+  cornell_depths_ref.npz  RenderParams with unequal depths per lobe kind: the "materials"
+                        box at (diffuse, reflection, transmission) = (3, 6, 5) and the "glass"
+                        box at (5, 3, 6), 64x64 at 4 spp (float64)
   cornell_delta_ref.npz the Cornell box ("lambert" and "materials") with the reference's
                         point, spot and directional lights added: 64x64 at 4 spp (float64)
   cornell_standard_ref.npz  the Cornell box with StandardSurfaceMaterial boxes ("standard":
@@ -29,7 +32,7 @@ reference sources with oracle/Makefile). Outputs:
                         reference's BVH::intersect leaves it: "nouv"); the same with bump
                         maps ("bump", "bump_nouv")
 Usage: python tests/golden/make_golden.py [part ...]   (parts: tables pcg cornell materials
-       delta metals standard textures; default all)
+       depths delta metals standard textures; default all)
 Scratch files go to oracle/_ref/tmp.
 """
 import os
@@ -101,6 +104,23 @@ def materials(tmp):
     np.savez_compressed(os.path.join(HERE, "cornell_materials_ref.npz"), **out)
 
 
+def depths(tmp):
+    """RenderParams with three different depths: the materials box at depths (3, 6, 5) and
+    the glass box at (5, 3, 6) (diffuse, reflection, transmission), 64x64 at 4 spp"""
+    out = {}
+    for variant, ds in (("materials", (3, 6, 5)), ("glass", (5, 3, 6))):
+        sc = scenes.cornell(64, 64, variant)
+        p = scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60, depths=ds)
+        spath = os.path.join(tmp, f"depths_{variant}.scene")
+        fpath = os.path.join(tmp, f"depths_{variant}.film")
+        oracle.write_scene_file(spath, sc, p)
+        film, info = oracle.run_reference(spath, fpath, 64, 64)
+        out[f"{variant}_xyz"] = film.astype(np.float64)
+        out[f"{variant}_depths"] = np.array(ds, np.int32)
+        print("depths", variant, ds, info)
+    np.savez_compressed(os.path.join(HERE, "cornell_depths_ref.npz"), **out)
+
+
 def delta(tmp):
     """the box with the reference's point, spot and directional lights added"""
     out = {}
@@ -157,12 +177,16 @@ def textures(tmp):
     np.savez_compressed(os.path.join(HERE, "cornell_textured_ref.npz"), **out)
 
 
-PARTS = {"tables": tables, "pcg": pcg, "cornell": cornell, "materials": materials, "delta": delta,
+PARTS = {"tables": tables, "pcg": pcg, "cornell": cornell, "materials": materials, "depths": depths, "delta": delta,
          "metals": metals, "standard": standard, "textures": textures}
 
 
 def main(parts):
-    oracle.build(ref=True)
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import reference_dir
+    if reference_dir() is None:
+        sys.exit("the reference source tree is needed: set FL_REFERENCE_DIR")
+    oracle.build(ref=True, ref_dir=reference_dir())
     scratch = os.path.join(ROOT, "oracle", "_ref", "tmp")
     os.makedirs(scratch, exist_ok=True)
     tmp = tempfile.mkdtemp(dir=scratch)

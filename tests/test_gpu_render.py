@@ -75,6 +75,108 @@ def test_bins60_materials_match_reference_bxdfs(ctx, variant):
         assert abs(xyz.mean() / ref.mean() - 1) < 2e-3
 
 
+@pytest.mark.parametrize("variant", ["materials", "glass"])
+def test_lobe_depths_match_reference_integrator(ctx, variant):
+    """RenderParams with a different depth per lobe kind (pathintegrator.cpp:55-65): each
+    depth ends a path only when the lobe sampled at exactly that bounce is of its kind, so
+    paths outlive the deepest depth and the device runs bounces past the wave's fixed ones.
+    60-bin mode against the reference integrator's film (fixture made by the reference):
+    >= 99% of pixels within 1e-4 relative, image mean within 2e-3, no path cut."""
+    g = np.load(os.path.join(GOLDEN, "cornell_depths_ref.npz"))
+    ds = tuple(int(d) for d in g[f"{variant}_depths"])
+    sc = scenes.cornell(64, 64, variant)
+    xyz, _, stats = render_xyz(ctx, sc, scenes.render_params(4, 8, fb.FL_SPECTRAL_BINS60, depths=ds))
+    ref = g[f"{variant}_xyz"]
+    frac = close_fraction(xyz, ref, 1e-4, 1e-6)
+    assert frac >= 0.99, (variant, frac)
+    assert abs(xyz.mean() / ref.mean() - 1) < 2e-3
+    assert stats["paths_cut"] == 0
+
+
+def test_lobe_depths_hero_match_oracle(ctx, orc_tables):
+    """hero mode with depths (2, 7, 4) against the oracle: >= 99% of pixels within 1e-3, the
+    image mean within 1e-3, and more path vertices than an equal-depth-2 render"""
+    sc = scenes.cornell(64, 64, "materials")
+    p = scenes.render_params(8, 8, fb.FL_SPECTRAL_HERO4, depths=(2, 7, 4))
+    xyz, _, stats = render_xyz(ctx, sc, p)
+    cpu, cnt = oracle.render(sc, orc_tables, p)
+    assert stats["paths"] == cnt["paths"]
+    assert stats["bounces"] == pytest.approx(cnt["bounces"], rel=2e-3)
+    frac = close_fraction(xyz, cpu, 1e-3, 1e-5)
+    assert frac >= 0.99, frac
+    assert abs(xyz.mean() / cpu.mean() - 1) < 1e-3
+    _, _, st2 = render_xyz(ctx, sc, scenes.render_params(8, 2, fb.FL_SPECTRAL_HERO4))
+    assert stats["bounces"] > st2["bounces"]
+
+
+def closed_room():
+    """the Cornell box closed at z = 0 with the camera inside: no path escapes"""
+    sc = scenes.cornell(32, 32, "glass")
+    front = np.asarray(scenes._quad((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)), np.float32)
+    verts = np.concatenate([sc.verts, front])
+    mats = np.concatenate([sc.tri_material, np.zeros(2, np.uint32)])
+    cam = dict(sc.camera, position=(0.5, 0.5, 0.05), look_at=(0.5, 0.5, 1.0))
+    return scenes.Scene(verts, mats, sc.materials, sc.lights, cam)
+
+
+def test_paths_cut_at_the_bounce_bound(ctx):
+    """Without Russian roulette (threshold 0) in a closed room, a path whose lobe kinds miss
+    their depths never ends: it is cut at FL_MAX_BOUNCES and the call reports it
+    (FL_ERR_TRAVERSAL, with the count in the message); equal depths cut nothing."""
+    sc = closed_room()
+    s = ctx.scene(sc)
+    p = scenes.render_params(2, 8, fb.FL_SPECTRAL_HERO4, rr=0.0, depths=(1, 2, 2))
+    with pytest.raises(fb.FlError) as e:
+        s.render(p)
+    assert e.value.status == fb.FL_ERR_TRAVERSAL and "FL_MAX_BOUNCES" in str(e.value)
+    _, st = s.render(scenes.render_params(2, 6, fb.FL_SPECTRAL_HERO4, rr=0.0))
+    assert st["paths_cut"] == 0 and st["traversal_errors"] == 0
+    s.close()
+
+
+@pytest.mark.parametrize("mode", [fb.FL_SPECTRAL_BINS60, fb.FL_SPECTRAL_HERO4])
+def test_li_on_camera_rays_equals_one_spp_film(ctx, mode):
+    """fl_li (Integrator::Li for a batch) on the render loop's camera rays of sample 0 (made
+    by the oracle's restatement of the camera, with the generator state after the camera's
+    draws) equals the 1-spp film pixel for pixel: the same path, one sample per pixel"""
+    sc = scenes.cornell(32, 24, "materials")
+    s = ctx.scene(sc)
+    p = scenes.render_params(1, 8, mode, depths=(3, 6, 5))
+    film = np.zeros((24, 32, 3), np.float64)
+    s.render(p, film_xyz64=film)
+    o, d, r, lam = oracle.camera_rays(sc, np.arange(32 * 24))
+    L, r_out, xyz = fb.li(s, p, o, d, r, lam)
+    s.close()
+    assert L.shape == (32 * 24, 60 if mode == fb.FL_SPECTRAL_BINS60 else 4)
+    assert np.array_equal(xyz.reshape(24, 32, 3), film)
+    assert np.any(r_out != r)  # paths that hit draw numbers (misses draw none)
+
+
+def test_li_matches_oracle_on_arbitrary_rays(ctx, orc_tables):
+    """fl_li on rays from random points inside the box in random directions, with random
+    generator states, against the oracle's PathIntegrator::Li: 60 bins, >= 99% of rays with
+    every bin within 1e-4 relative (1e-6 absolute) and the same generator state after"""
+    sc = scenes.cornell(8, 8, "materials")
+    rng = np.random.default_rng(11)
+    n = 4096
+    o = np.zeros((n, 4), np.float32)
+    o[:, :3] = rng.uniform(0.05, 0.95, (n, 3))
+    v = rng.normal(size=(n, 3))
+    d = np.zeros((n, 4), np.float32)
+    d[:, :3] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    d[:, 3] = np.inf
+    state = rng.integers(0, 2 ** 63, n, dtype=np.uint64)
+    lam = rng.uniform(380, 720, n).astype(np.float32)
+    p = scenes.render_params(1, 8, fb.FL_SPECTRAL_BINS60, depths=(4, 6, 5))
+    s = ctx.scene(sc)
+    L, r_out, _ = fb.li(s, p, o, d, state, lam)
+    s.close()
+    Lc, rc, _ = oracle.li(sc, orc_tables, p, o, d, state, lam)
+    ok = np.all(np.abs(L - Lc) <= np.maximum(1e-4 * np.abs(Lc), 1e-6), axis=1)
+    assert ok.mean() >= 0.99, ok.mean()
+    assert np.mean(r_out == rc) >= 0.99
+
+
 def test_hero_matches_oracle(ctx, orc_tables):
     sc = scenes.cornell(64, 64)
     p = scenes.render_params(8, 8, fb.FL_SPECTRAL_HERO4)

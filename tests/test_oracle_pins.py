@@ -70,6 +70,21 @@ def test_oracle_materials_equal_reference_bxdfs(orc_tables):
         np.testing.assert_allclose(film, g[f"{variant}_full_xyz"].astype(np.float64), rtol=2e-7, atol=1e-12)
 
 
+def test_oracle_lobe_depths_equal_reference(orc_tables):
+    """RenderParams with a different depth per lobe kind (pathintegrator.cpp:55-65: each an
+    exact == test on the sampled lobe's kind, so paths run past the deepest one until
+    Russian roulette ends them): bit-exact against the reference integrator at 64x64 x 4 spp,
+    and different from the equal-depth render."""
+    g = np.load(os.path.join(GOLDEN, "cornell_depths_ref.npz"))
+    for variant in ("materials", "glass"):
+        ds = tuple(int(d) for d in g[f"{variant}_depths"])
+        sc = scenes.cornell(64, 64, variant)
+        film, _ = oracle.render(sc, orc_tables, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60, depths=ds))
+        assert np.array_equal(film, g[f"{variant}_xyz"]), variant
+        same, _ = oracle.render(sc, orc_tables, scenes.render_params(4, max(ds), T.FL_SPECTRAL_BINS60))
+        assert not np.array_equal(same, film)
+
+
 def test_oracle_delta_lights_equal_reference(orc_tables):
     """The reference's PointIlluminant, SpotIlluminant and DirectionalIlluminant (unweighted
     NEE, no BSDF-sampled MIS ray, d^2 decay) in the Cornell box beside its area light,
@@ -146,3 +161,17 @@ def test_texel_rule_edges():
     got = oracle.image_texels(img, np.array([c[0] for c in cases], np.float32))
     for (uv, (i, j)), rgb in zip(cases, got):
         assert np.array_equal(rgb, img[j, i] / np.float32(255.0)), (uv, i, j, rgb * 255)
+
+
+def test_oracle_li_on_camera_rays_equals_render(orc_tables):
+    """The oracle's per-ray PathIntegrator::Li (orc_li) on the render loop's camera rays of
+    sample 0 adds up to the 1-spp film of orc_render exactly, in both spectral modes and with
+    unequal lobe depths: the per-ray entry point and the image loop are the same estimator."""
+    sc = scenes.cornell(24, 16, "glass")
+    o, d, r, lam = oracle.camera_rays(sc, np.arange(24 * 16))
+    for mode in (T.FL_SPECTRAL_BINS60, T.FL_SPECTRAL_HERO4):
+        p = scenes.render_params(1, 8, mode, depths=(5, 3, 6))
+        film, _ = oracle.render(sc, orc_tables, p)
+        _, r_out, xyz = oracle.li(sc, orc_tables, p, o, d, r, lam)
+        assert np.array_equal(xyz.reshape(16, 24, 3), film)
+        assert np.any(r_out != r)  # paths that hit draw numbers (misses draw none)
