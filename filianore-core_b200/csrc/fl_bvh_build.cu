@@ -7,8 +7,9 @@
 //   2. 63-bit Morton codes of the centroids, radix sort (CUB) of (code, triangle)
 //   3. binary radix tree over the sorted codes (Karras, HPG 2012), ties broken by index
 //   4. bottom-up bounds (one climbing thread per leaf, second arrival merges)
-//   5. level-parallel collapse into 8-wide nodes: each wide node greedily opens its
-//      largest-area binary children until it has 8 or all remaining hold <= 3 triangles;
+//   5. SAH costs of every way to group each binary subtree into up to 8 child slots
+//      (dynamic programme, bottom-up like the bounds)
+//   6. level-parallel collapse into 8-wide nodes following the programme's choices;
 //      children are placed in the slot matching the ray octant that should visit them
 //      first; child boxes are quantised to 8 bits per axis, rounded outwards.
 // Triangles are rewritten in leaf order as three float4 (v0.w = soup index).
@@ -157,6 +158,79 @@ __global__ void k_refit(const float *__restrict__ trib, const uint32_t *__restri
     }
 }
 
+// 4b. SAH-optimal grouping of the binary tree into 8-wide nodes (the dynamic programme of
+// Ylitie, Karras and Laine, HPG 2017). For binary node n and i in 1..8, C(n, i) is the
+// least SAH cost of representing n's subtree with at most i child slots of a wide node:
+//   C(n, 1) = min(leaf: A(n) c_tri count (count <= 3), internal: A(n) c_node + D(n, 8))
+//   C(n, i) = min(C(n, i - 1), D(n, i)),   D(n, j) = min_k C(left, k) + C(right, j - k)
+// A binary leaf (one triangle) costs A c_tri for every i. dec[8 n + i - 1] records the choice:
+// for i = 1, 0 = leaf and k > 0 = internal with its 8 slots split k / 8 - k; for i > 1, 0 =
+// take C(n, i - 1) and k > 0 = split k / i - k between the children. Costs climb the tree like
+// the bounds (second arrival computes).
+#ifndef FL_SAH_TRI_COST
+#define FL_SAH_TRI_COST 0.3f
+#endif
+constexpr float kCostNode = 1.0f;             // a wide node visit
+constexpr float kCostTri = FL_SAH_TRI_COST;   // a triangle test, relative to a node visit
+
+__device__ inline float half_area6(const float *b) {
+    const float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_sah_costs(int n, const uint32_t *__restrict__ child, const uint2 *__restrict__ range,
+                            const int *__restrict__ parent_int, const int *__restrict__ parent_leaf,
+                            const float *__restrict__ leafbox, const float *__restrict__ nodebox, float *cost,
+                            uint8_t *dec, int *flags) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || n < 2) return;
+    int node = parent_leaf[i];
+    int guard = 0;
+    while (node >= 0 && node < n - 1 && guard++ < n) {
+        __threadfence();
+        if (atomicAdd(&flags[node], 1) == 0) return;
+        float cc[2][8];
+        for (int c = 0; c < 2; ++c) {
+            const uint32_t ref = child[2 * node + c];
+            if (ref & kLeafBit) {
+                if ((ref & ~kLeafBit) >= (uint32_t)n) return;
+                const float a = kCostTri * half_area6(leafbox + 6 * (size_t)(ref & ~kLeafBit));
+                for (int k = 0; k < 8; ++k) cc[c][k] = a;
+            } else {
+                if (ref >= (uint32_t)(n - 1)) return;
+                for (int k = 0; k < 8; ++k) cc[c][k] = __ldcg(cost + 8 * (size_t)ref + k);
+            }
+        }
+        // D(node, j) for j = 2..8 and the split that gives it
+        float D[9];
+        uint8_t split[9];
+        for (int j = 2; j <= 8; ++j) {
+            D[j] = INFINITY;
+            split[j] = 1;
+            for (int k = 1; k < j; ++k) {
+                const float v = cc[0][k - 1] + cc[1][j - k - 1];
+                if (v < D[j]) { D[j] = v; split[j] = (uint8_t)k; }
+            }
+        }
+        const float A = half_area6(nodebox + 6 * (size_t)node);
+        const uint2 r = range[node];
+        const uint32_t count = r.y - r.x + 1;
+        const float c_internal = kCostNode * A + D[8];
+        const float c_leaf = count <= (uint32_t)kMaxLeafTris ? kCostTri * A * (float)count : INFINITY;
+        float C = c_leaf <= c_internal ? c_leaf : c_internal;
+        uint8_t d0 = c_leaf <= c_internal ? 0 : split[8];
+        __stcg(cost + 8 * (size_t)node, C);
+        __stcg(dec + 8 * (size_t)node, d0);
+        for (int j = 2; j <= 8; ++j) {
+            uint8_t dj = 0;
+            if (D[j] < C) { C = D[j]; dj = split[j]; }
+            __stcg(cost + 8 * (size_t)node + j - 1, C);
+            __stcg(dec + 8 * (size_t)node + j - 1, dj);
+        }
+        node = parent_int[node];
+    }
+}
+
 struct BuildCounters {
     uint32_t node_count;
     uint32_t tri_count;
@@ -176,57 +250,62 @@ __device__ inline uint32_t ref_count(uint32_t ref, const uint2 *range) {
 __device__ inline uint32_t ref_first(uint32_t ref, const uint2 *range) {
     return (ref & kLeafBit) ? (ref & ~kLeafBit) : range[ref].x;
 }
-__device__ inline float half_area(const float *b) {
-    float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
-    return dx * dy + dy * dz + dz * dx;
-}
 
 // 5. collapse one level: frontier item (binary ref, wide node index)
 __global__ void k_collapse(const uint2 *__restrict__ frontier, uint32_t n_items, uint2 *__restrict__ next,
                            const uint32_t *__restrict__ child, const uint2 *__restrict__ range,
                            const float *__restrict__ leafbox, const float *__restrict__ nodebox,
-                           const uint32_t *__restrict__ vals, const float *__restrict__ soup,
-                           WideNode *__restrict__ nodes, float4 *__restrict__ tris, BuildCounters *cnt,
-                           uint32_t cap) {
+                           const uint8_t *__restrict__ dec, const uint32_t *__restrict__ vals,
+                           const float *__restrict__ soup, WideNode *__restrict__ nodes, float4 *__restrict__ tris,
+                           BuildCounters *cnt, uint32_t cap) {
     uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item >= n_items) return;
     const uint32_t ref = frontier[item].x;
     const uint32_t widx = frontier[item].y;
 
     uint32_t c[8];
-    int count;
+    int count = 0;
     auto valid = [&](uint32_t r) { return (r & kLeafBit) ? (r & ~kLeafBit) < cap : r + 1 < cap; };
     if (!valid(ref)) {
         atomicOr(&cnt->overflow, 2u);
         return;
     }
-    if ((ref & kLeafBit) || ref_count(ref, range) <= (uint32_t)kMaxLeafTris) {
-        c[0] = ref;
+    // a child slot is a leaf when it is one triangle or the programme chose a leaf for it
+    auto is_leaf = [&](uint32_t r) { return (r & kLeafBit) || dec[8 * (size_t)r] == 0; };
+    if (is_leaf(ref)) {
+        c[0] = ref;  // the whole tree fits one leaf: a root with a single leaf child
         count = 1;
     } else {
-        c[0] = child[2 * ref];
-        c[1] = child[2 * ref + 1];
-        count = 2;
-        if (!valid(c[0]) || !valid(c[1])) {
-            atomicOr(&cnt->overflow, 2u);
-            return;
-        }
-        while (count < 8) {
-            int best = -1;
-            float best_area = -1.f;
-            for (int k = 0; k < count; ++k) {
-                if ((c[k] & kLeafBit) || ref_count(c[k], range) <= (uint32_t)kMaxLeafTris) continue;
-                float a = half_area(ref_box(c[k], leafbox, nodebox));
-                if (a > best_area) { best_area = a; best = k; }
-            }
-            if (best < 0) break;
-            uint32_t r = c[best];
-            if (!valid(child[2 * r]) || !valid(child[2 * r + 1])) {
+        // expand the programme's choices: (binary node, slots) pairs until each is one slot
+        uint32_t st_ref[16];
+        uint8_t st_slots[16];
+        int sp = 0;
+        const uint8_t k0 = dec[8 * (size_t)ref];
+        st_ref[sp] = child[2 * ref + 1], st_slots[sp++] = (uint8_t)(8 - k0);
+        st_ref[sp] = child[2 * ref], st_slots[sp++] = k0;
+        while (sp > 0) {
+            const uint32_t m = st_ref[--sp];
+            uint8_t i = st_slots[sp];
+            if (!valid(m) || count >= 8) {
                 atomicOr(&cnt->overflow, 2u);
                 return;
             }
-            c[best] = child[2 * r];
-            c[count++] = child[2 * r + 1];
+            if ((m & kLeafBit) || i <= 1) {
+                c[count++] = m;
+                continue;
+            }
+            while (i > 1 && dec[8 * (size_t)m + i - 1] == 0) --i;  // fewer slots were as cheap
+            if (i <= 1) {
+                c[count++] = m;
+                continue;
+            }
+            const uint8_t k = dec[8 * (size_t)m + i - 1];
+            if (sp + 2 > 16 || k == 0 || k >= i) {
+                atomicOr(&cnt->overflow, 2u);
+                return;
+            }
+            st_ref[sp] = child[2 * m + 1], st_slots[sp++] = (uint8_t)(i - k);
+            st_ref[sp] = child[2 * m], st_slots[sp++] = k;
         }
     }
 
@@ -274,9 +353,8 @@ __global__ void k_collapse(const uint2 *__restrict__ frontier, uint32_t n_items,
 
     uint32_t n_inner = 0, n_leaf_tris = 0, n_leaves = 0;
     for (int k = 0; k < count; ++k) {
-        uint32_t m = ref_count(c[k], range);
-        if (m > (uint32_t)kMaxLeafTris) ++n_inner;
-        else { n_leaf_tris += m; ++n_leaves; }
+        if (!is_leaf(c[k])) ++n_inner;
+        else { n_leaf_tris += ref_count(c[k], range); ++n_leaves; }
     }
     uint32_t child_base = n_inner ? atomicAdd(&cnt->node_count, n_inner) : 0;
     uint32_t tri_base = n_leaf_tris ? atomicAdd(&cnt->tri_count, n_leaf_tris) : 0;
@@ -326,7 +404,7 @@ __global__ void k_collapse(const uint2 *__restrict__ frontier, uint32_t n_items,
         nd.qlox[s] = qlo[0]; nd.qloy[s] = qlo[1]; nd.qloz[s] = qlo[2];
         nd.qhix[s] = qhi[0]; nd.qhiy[s] = qhi[1]; nd.qhiz[s] = qhi[2];
         uint32_t m = ref_count(c[k], range);
-        if (m > (uint32_t)kMaxLeafTris) {
+        if (!is_leaf(c[k])) {
             imask |= (uint8_t)(1u << s);
             nd.meta[s] = (uint8_t)((1u << 5) | (24u + (uint32_t)s));
             next[next_base + inner_rank] = make_uint2(c[k], child_base + inner_rank);
@@ -350,26 +428,17 @@ __global__ void k_collapse(const uint2 *__restrict__ frontier, uint32_t n_items,
     nodes[widx] = nd;
 }
 
-template <typename T>
-fl_status dalloc(Context *ctx, T **p, size_t count) {
-    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        cudaGetLastError();
-        set_error(ctx, std::string("device allocation failed: ") + cudaGetErrorString(e));
-        return FL_ERR_OOM;
-    }
-    return FL_OK;
-}
-
+// build temporaries from the context's pool, returned to it in stream order
 struct Tmp {
+    Context *ctx;
     std::vector<void *> ptrs;
+    explicit Tmp(Context *c) : ctx(c) {}
     ~Tmp() {
-        for (void *p : ptrs) cudaFree(p);
+        for (void *p : ptrs) dev_free(ctx, p);
     }
     template <typename T>
-    fl_status get(Context *ctx, T **p, size_t count) {
-        fl_status st = dalloc(ctx, p, count);
+    fl_status get(T **p, size_t count) {
+        fl_status st = dev_alloc_n(ctx, p, count);
         if (st == FL_OK) ptrs.push_back(*p);
         return st;
     }
@@ -394,7 +463,7 @@ fl_status build_bvh(Scene *s) {
     FL_CUDA_TRY(ctx, cudaEventCreate(&ev1));
     FL_CUDA_TRY(ctx, cudaEventRecord(ev0, st));
 
-    Tmp tmp;
+    Tmp tmp(ctx);
     fl_status rc;
     float *trib, *leafbox, *nodebox;
     uint32_t *cbounds, *vals_a, *vals_b, *child;
@@ -404,15 +473,15 @@ fl_status build_bvh(Scene *s) {
     BuildCounters *cnt;
     WideNode *nodes_big;
     const size_t ni = n > 1 ? n - 1 : 1;
-    if ((rc = tmp.get(ctx, &trib, 6 * (size_t)n)) || (rc = tmp.get(ctx, &leafbox, 6 * (size_t)n)) ||
-        (rc = tmp.get(ctx, &nodebox, 6 * ni)) || (rc = tmp.get(ctx, &cbounds, 6)) ||
-        (rc = tmp.get(ctx, &vals_a, n)) || (rc = tmp.get(ctx, &vals_b, n)) || (rc = tmp.get(ctx, &child, 2 * ni)) ||
-        (rc = tmp.get(ctx, &keys_a, n)) || (rc = tmp.get(ctx, &keys_b, n)) || (rc = tmp.get(ctx, &range, ni)) ||
-        (rc = tmp.get(ctx, &front_a, n)) || (rc = tmp.get(ctx, &front_b, n)) ||
-        (rc = tmp.get(ctx, &parent_int, ni)) || (rc = tmp.get(ctx, &parent_leaf, n)) ||
-        (rc = tmp.get(ctx, &flags, ni)) || (rc = tmp.get(ctx, &cnt, 1)) || (rc = tmp.get(ctx, &nodes_big, n)))
+    if ((rc = tmp.get(&trib, 6 * (size_t)n)) || (rc = tmp.get(&leafbox, 6 * (size_t)n)) ||
+        (rc = tmp.get(&nodebox, 6 * ni)) || (rc = tmp.get(&cbounds, 6)) ||
+        (rc = tmp.get(&vals_a, n)) || (rc = tmp.get(&vals_b, n)) || (rc = tmp.get(&child, 2 * ni)) ||
+        (rc = tmp.get(&keys_a, n)) || (rc = tmp.get(&keys_b, n)) || (rc = tmp.get(&range, ni)) ||
+        (rc = tmp.get(&front_a, n)) || (rc = tmp.get(&front_b, n)) ||
+        (rc = tmp.get(&parent_int, ni)) || (rc = tmp.get(&parent_leaf, n)) ||
+        (rc = tmp.get(&flags, ni)) || (rc = tmp.get(&cnt, 1)) || (rc = tmp.get(&nodes_big, n)))
         return rc;
-    if ((rc = dalloc(ctx, &s->tris, 3 * (size_t)n))) return rc;
+    if ((rc = dev_alloc_n(ctx, &s->tris, 3 * (size_t)n))) return rc;
 
     const int bs = 256;
     const uint32_t grid_n = (n + bs - 1) / bs;
@@ -427,7 +496,7 @@ fl_status build_bvh(Scene *s) {
     size_t temp_bytes = 0;
     FL_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dkeys, dvals, (int)n, 0, 63, st));
     void *temp;
-    if ((rc = tmp.get(ctx, (char **)&temp, temp_bytes))) return rc;
+    if ((rc = tmp.get((char **)&temp, temp_bytes))) return rc;
     FL_CUDA_TRY(ctx, cub::DeviceRadixSort::SortPairs(temp, temp_bytes, dkeys, dvals, (int)n, 0, 63, st));
     const uint64_t *keys = dkeys.Current();
     const uint32_t *vals = dvals.Current();
@@ -441,6 +510,14 @@ fl_status build_bvh(Scene *s) {
         k_karras<<<(uint32_t)((ni + bs - 1) / bs), bs, 0, st>>>(keys, (int)n, child, range, parent_int, parent_leaf);
     }
     k_refit<<<grid_n, bs, 0, st>>>(trib, vals, (int)n, child, parent_int, parent_leaf, leafbox, nodebox, flags);
+    float *cost = nullptr;
+    uint8_t *dec = nullptr;
+    if ((rc = tmp.get(&cost, 8 * ni)) || (rc = tmp.get(&dec, 8 * ni))) return rc;
+    if (n >= 2) {
+        FL_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(int) * ni, st));
+        k_sah_costs<<<grid_n, bs, 0, st>>>((int)n, child, range, parent_int, parent_leaf, leafbox, nodebox, cost, dec,
+                                           flags);
+    }
 
     // collapse, one launch per wide level
     BuildCounters c0 = {1u, 0u, 0u, 0u, 0u};
@@ -456,8 +533,8 @@ fl_status build_bvh(Scene *s) {
             return FL_ERR_INVALID;
         }
         FL_CUDA_TRY(ctx, cudaMemsetAsync(&cnt->next_count, 0, sizeof(uint32_t), st));
-        k_collapse<<<(items + 127) / 128, 128, 0, st>>>(front_a, items, front_b, child, range, leafbox, nodebox, vals,
-                                                        s->soup, nodes_big, s->tris, cnt, n);
+        k_collapse<<<(items + 127) / 128, 128, 0, st>>>(front_a, items, front_b, child, range, leafbox, nodebox, dec,
+                                                        vals, s->soup, nodes_big, s->tris, cnt, n);
         FL_CUDA_TRY(ctx, cudaMemcpyAsync(&hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
         FL_CUDA_TRY(ctx, cudaStreamSynchronize(st));
         FL_CUDA_TRY(ctx, cudaGetLastError());
@@ -475,7 +552,7 @@ fl_status build_bvh(Scene *s) {
     s->n_nodes = hc.node_count;
     s->n_leaves = hc.leaf_count;
     s->max_depth = depth;
-    if ((rc = dalloc(ctx, &s->nodes, s->n_nodes))) return rc;
+    if ((rc = dev_alloc_n(ctx, &s->nodes, s->n_nodes))) return rc;
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(s->nodes, nodes_big, sizeof(WideNode) * s->n_nodes, cudaMemcpyDeviceToDevice, st));
     FL_CUDA_TRY(ctx, cudaEventRecord(ev1, st));
     FL_CUDA_TRY(ctx, cudaEventSynchronize(ev1));

@@ -32,6 +32,26 @@ fl_status cuda_status(Context *ctx, cudaError_t e, const char *what) {
     return FL_ERR_CUDA;
 }
 
+// the emissive-triangle table: triangle -> its light (the rest stay -1)
+__global__ void k_tri_light(const LightDev *__restrict__ lights, uint32_t n_lights, int32_t *__restrict__ tri_light) {
+    const uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < n_lights && lights[l].type == FL_LIGHT_TRIANGLE) tri_light[lights[l].tri] = (int32_t)l;
+}
+
+fl_status dev_alloc(Context *ctx, void **p, size_t bytes) {
+    *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, ctx->pool, ctx->stream);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_status(ctx, e, "device allocation");
+    }
+    return FL_OK;
+}
+
+void dev_free(Context *ctx, void *p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
+}
+
 fl_status ensure_scratch(Context *ctx, size_t bytes, void **out) {
     if (bytes > ctx->scratch_bytes) {
         if (ctx->wave_graph) {  // captured against the old buffer
@@ -41,6 +61,7 @@ fl_status ensure_scratch(Context *ctx, size_t bytes, void **out) {
         }
         if (ctx->scratch) {
             cudaStreamSynchronize(ctx->stream);
+            if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
             cudaFree(ctx->scratch);
             ctx->scratch = nullptr;
             ctx->scratch_bytes = 0;
@@ -231,6 +252,17 @@ fl_status fl_context_create(int32_t device, const fl_spectral_tables *t, fl_cont
     CTX_TRY(cudaSetDevice(device));
     CTX_TRY(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
     CTX_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        CTX_TRY(cudaMemPoolCreate(&ctx->pool, &props));
+        uint64_t keep = kPoolKeepBytes;
+        CTX_TRY(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    CTX_TRY(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    CTX_TRY(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
     CTX_TRY(cudaMalloc(&ctx->d_error, sizeof(int) * 4));
     CTX_TRY(cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * 8));
 
@@ -302,6 +334,14 @@ fl_status fl_context_destroy(fl_context *ctx_h) {
     cudaFree(ctx->tables.cie_xyz);
     cudaFree(ctx->tables.rgb_bases);
     cudaFree(ctx->tables.binned);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    if (ctx->stream2) {
+        cudaStreamSynchronize(ctx->stream2);
+        cudaStreamDestroy(ctx->stream2);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return FL_OK;
@@ -366,7 +406,6 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
                 set_error(ctx, "triangle material index out of range");
                 return FL_ERR_INVALID;
             }
-    std::vector<int32_t> tri_light(d->n_tri, -1);
     Scene *s = new Scene();
     s->ctx = ctx;
     s->n_tri = d->n_tri;
@@ -387,7 +426,6 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
                 set_error(ctx, "light triangle index out of range");
                 return FL_ERR_INVALID;
             }
-            tri_light[L.tri] = (int32_t)l;
             s->n_emissive_tris++;
         } else if (L.type == FL_LIGHT_ENV) {
             s->has_env = 1;
@@ -471,24 +509,29 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
         e = (call);                                             \
         if (e != cudaSuccess) return fail(cuda_status(ctx, e, #call)); \
     } while (0)
+#define SC_TRY_RC(call)                                         \
+    do {                                                        \
+        const fl_status r_ = (call);                            \
+        if (r_ != FL_OK) return fail(r_);                       \
+    } while (0)
     SC_TRY(cudaSetDevice(ctx->device));
     const size_t nt = d->n_tri ? d->n_tri : 1;
-    SC_TRY(cudaMalloc(&s->soup, sizeof(float) * 9 * nt));
-    SC_TRY(cudaMalloc(&s->tri_material, sizeof(uint32_t) * nt));
-    SC_TRY(cudaMalloc(&s->tri_light, sizeof(int32_t) * nt));
-    SC_TRY(cudaMalloc(&s->materials, sizeof(MaterialDev) * d->n_materials));
-    SC_TRY(cudaMalloc(&s->lights, sizeof(LightDev) * (d->n_lights ? d->n_lights : 1)));
-    SC_TRY(cudaMalloc(&s->mat_refl60, sizeof(float) * 60 * d->n_materials));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->soup, 9 * nt));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->tri_material, nt));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->tri_light, nt));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->materials, d->n_materials));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->lights, d->n_lights));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->mat_refl60, 60 * (size_t)d->n_materials));
     {
         // from_reflectance_rgb (color/spectrumoperations.cpp:113-147) over the 60 bins
         std::vector<float> refl((size_t)60 * d->n_materials);
         for (uint32_t m = 0; m < d->n_materials; ++m)
             refl60(ctx->binned_host, s->materials_host[m].basis, s->materials_host[m].w, &refl[(size_t)m * 60]);
-        SC_TRY(cudaMemcpy(s->mat_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
+        SC_TRY(cudaMemcpyAsync(s->mat_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
     if (d->uvs && d->n_tri) {
-        SC_TRY(cudaMalloc(&s->uvs, sizeof(float) * 6 * (size_t)d->n_tri));
-        SC_TRY(cudaMemcpy(s->uvs, d->uvs, sizeof(float) * 6 * (size_t)d->n_tri, cudaMemcpyHostToDevice));
+        SC_TRY_RC(dev_alloc_n(ctx, &s->uvs, 6 * (size_t)d->n_tri));
+        SC_TRY(cudaMemcpyAsync(s->uvs, d->uvs, sizeof(float) * 6 * (size_t)d->n_tri, cudaMemcpyHostToDevice, ctx->stream));
     }
     if (d->images && d->n_images) {
         std::vector<ImageDev> info(d->n_images);
@@ -497,18 +540,19 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
             info[i] = ImageDev{total, d->images[i].width, d->images[i].height};
             total += 3ull * (unsigned long long)d->images[i].width * (unsigned long long)d->images[i].height;
         }
-        SC_TRY(cudaMalloc(&s->pixels, total));
-        SC_TRY(cudaMalloc(&s->images, sizeof(ImageDev) * d->n_images));
+        SC_TRY_RC(dev_alloc_n(ctx, &s->pixels, total));
+        SC_TRY_RC(dev_alloc_n(ctx, &s->images, d->n_images));
         for (uint32_t i = 0; i < d->n_images; ++i)
-            SC_TRY(cudaMemcpy(s->pixels + info[i].offset, d->images[i].rgb,
-                              3ull * (unsigned long long)d->images[i].width * (unsigned long long)d->images[i].height,
-                              cudaMemcpyHostToDevice));
-        SC_TRY(cudaMemcpy(s->images, info.data(), sizeof(ImageDev) * d->n_images, cudaMemcpyHostToDevice));
+            SC_TRY(cudaMemcpyAsync(s->pixels + info[i].offset, d->images[i].rgb,
+                                   3ull * (unsigned long long)d->images[i].width * (unsigned long long)d->images[i].height,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+        SC_TRY(cudaMemcpyAsync(s->images, info.data(), sizeof(ImageDev) * d->n_images, cudaMemcpyHostToDevice,
+                               ctx->stream));
         s->n_images = d->n_images;
     }
-    SC_TRY(cudaMalloc(&s->standard, sizeof(StandardDev) * (n_std ? n_std : 1)));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->standard, n_std));
     const size_t std_floats = (size_t)kStdSpectra * 60;
-    SC_TRY(cudaMalloc(&s->std_refl60, sizeof(float) * std_floats * (n_std ? n_std : 1)));
+    SC_TRY_RC(dev_alloc_n(ctx, &s->std_refl60, std_floats * (n_std ? n_std : 1)));
     if (n_std) {
         std::vector<float> refl(std_floats * n_std);
         for (uint32_t m = 0; m < n_std; ++m) {
@@ -519,8 +563,10 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
             const int metal = (mt >= 0 && mt <= 8) ? mt : 0;
             std::memcpy(row + 300, &ctx->metal60[120 * (size_t)metal], sizeof(float) * 120);
         }
-        SC_TRY(cudaMemcpy(s->standard, std_host.data(), sizeof(StandardDev) * n_std, cudaMemcpyHostToDevice));
-        SC_TRY(cudaMemcpy(s->std_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice));
+        SC_TRY(cudaMemcpyAsync(s->standard, std_host.data(), sizeof(StandardDev) * n_std, cudaMemcpyHostToDevice,
+                               ctx->stream));
+        SC_TRY(cudaMemcpyAsync(s->std_refl60, refl.data(), sizeof(float) * refl.size(), cudaMemcpyHostToDevice,
+                               ctx->stream));
     }
     if (d->n_tri) {
         SC_TRY(cudaMemcpyAsync(s->soup, d->verts, sizeof(float) * 9 * d->n_tri, cudaMemcpyHostToDevice, ctx->stream));
@@ -529,15 +575,21 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
                                    cudaMemcpyHostToDevice, ctx->stream));
         else
             SC_TRY(cudaMemsetAsync(s->tri_material, 0, sizeof(uint32_t) * d->n_tri, ctx->stream));
-        SC_TRY(cudaMemcpyAsync(s->tri_light, tri_light.data(), sizeof(int32_t) * d->n_tri, cudaMemcpyHostToDevice,
-                               ctx->stream));
+        // no triangle emits but the lights' own (set on the device below)
+        SC_TRY(cudaMemsetAsync(s->tri_light, 0xff, sizeof(int32_t) * d->n_tri, ctx->stream));
     }
     SC_TRY(cudaMemcpyAsync(s->materials, s->materials_host.data(), sizeof(MaterialDev) * d->n_materials,
                            cudaMemcpyHostToDevice, ctx->stream));
-    if (d->n_lights)
+    if (d->n_lights) {
         SC_TRY(cudaMemcpyAsync(s->lights, lights_dev.data(), sizeof(LightDev) * d->n_lights, cudaMemcpyHostToDevice,
                                ctx->stream));
+        if (s->n_emissive_tris) {
+            k_tri_light<<<(d->n_lights + 127) / 128, 128, 0, ctx->stream>>>(s->lights, d->n_lights, s->tri_light);
+            SC_TRY(cudaGetLastError());
+        }
+    }
 #undef SC_TRY
+#undef SC_TRY_RC
     fl_status rc = build_bvh(s);
     if (rc != FL_OK) return fail(rc);
     ctx->children++;
@@ -549,21 +601,14 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
 fl_status fl_scene_destroy(fl_scene *scene) {
     Scene *s = reinterpret_cast<Scene *>(scene);
     if (!s) return FL_ERR_INVALID;
-    cudaSetDevice(s->ctx->device);
-    cudaStreamSynchronize(s->ctx->stream);
-    cudaFree(s->nodes);
-    cudaFree(s->tris);
-    cudaFree(s->soup);
-    cudaFree(s->tri_material);
-    cudaFree(s->tri_light);
-    cudaFree(s->materials);
-    cudaFree(s->lights);
-    cudaFree(s->mat_refl60);
-    cudaFree(s->standard);
-    cudaFree(s->std_refl60);
-    cudaFree(s->uvs);
-    cudaFree(s->pixels);
-    cudaFree(s->images);
+    // every entry point returns with its work finished, so nothing in flight reads the
+    // scene; the arrays go back to the context's pool in stream order
+    Context *ctx = s->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    void *arrays[] = {s->nodes, s->tris, s->soup, s->tri_material, s->tri_light, s->materials, s->lights,
+                      s->mat_refl60, s->standard, s->std_refl60, s->uvs, s->pixels, s->images};
+    for (void *p : arrays) dev_free(ctx, p);
     if (s->counted) s->ctx->children--;
     delete s;
     return FL_OK;

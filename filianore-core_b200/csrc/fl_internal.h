@@ -51,7 +51,16 @@ struct Context {
     std::atomic<int> children{0};       // live scenes, guides and servers made from this context
     int *d_error = nullptr;             // traversal error counter
     unsigned long long *d_counters = nullptr;  // 8 x u64 statistics
+    // Stream-ordered pool for scene arrays and BVH build temporaries: allocations and frees
+    // are ordered on `stream` without device synchronisation, and freed blocks stay cached
+    // for the next scene (up to kPoolKeepBytes).
+    cudaMemPool_t pool = nullptr;
+    // a second stream for host-memory trace batches (copies of one chunk overlap the
+    // traversal of another), and the events that fork it from and join it to the caller's
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
+constexpr uint64_t kPoolKeepBytes = (uint64_t)8 << 30;
 
 // Device material record (constant over the render).
 struct MaterialDev {
@@ -158,8 +167,18 @@ fl_status build_bvh(Scene *s);
 
 // traversal launches (fl_trace.cu); arrays are device pointers.
 enum TraceKind { kTraceClosest = 0, kTraceOccluded = 1, kTraceCount = 2 };
+// fetch_slot (0 or 1) picks the launch's work counter: launches that may run at the same
+// time on different streams use different slots.
 fl_status launch_trace(Scene *s, const float4 *org_tmin, const float4 *dir_tmax, uint32_t n, fl_hit *hits,
-                       uint8_t *occluded, int kind, cudaStream_t stream);
+                       uint8_t *occluded, int kind, cudaStream_t stream, int fetch_slot);
+
+// device memory from the context's pool, ordered on ctx->stream
+fl_status dev_alloc(Context *ctx, void **p, size_t bytes);
+void dev_free(Context *ctx, void *p);
+template <typename T>
+fl_status dev_alloc_n(Context *ctx, T **p, size_t count) {
+    return dev_alloc(ctx, reinterpret_cast<void **>(p), sizeof(T) * (count ? count : 1));
+}
 
 // context scratch: returns a device buffer of at least `bytes` (grow-only)
 fl_status ensure_scratch(Context *ctx, size_t bytes, void **out);

@@ -594,7 +594,15 @@ __device__ inline void add_spheres(const JobDev &A, const RayPre &r, TraceResult
     }
 }
 
-constexpr int kRenderTraceSteps = 8;
+#ifndef FL_TRACE_STEPS
+#define FL_TRACE_STEPS 8
+#endif
+constexpr int kRenderTraceSteps = FL_TRACE_STEPS;  // traversal steps between refills of finished lanes
+// resident blocks per SM the render's traversal kernels are compiled for (caps registers)
+#ifndef FL_RENDER_TRACE_BLOCKS
+#define FL_RENDER_TRACE_BLOCKS 7
+#endif
+constexpr int kRenderTraceBlocks = FL_RENDER_TRACE_BLOCKS;
 
 struct PathTraceItem {
     const RenderArgs *A;
@@ -638,7 +646,7 @@ struct PathTraceItem {
 
 // camera and continuation rays: closest hit (persistent, lanes refilled as rays finish)
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 7) k_trace_paths(RenderArgs A) {
+__global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_paths(RenderArgs A) {
     const uint32_t n = load_count(&A.cnt->n_trace);
     bool err = false;
     TraceStats st;
@@ -867,7 +875,7 @@ struct NeeRayItem {
 
 // shadow rays (kind 0) and MIS rays (kind 1), persistent
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 7) k_trace_rays2(RenderArgs A) {
+__global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_rays2(RenderArgs A) {
     const uint32_t n = min(load_count(&A.cnt->n_shadow), A.scap);
     bool err = false;
     TraceStats st;

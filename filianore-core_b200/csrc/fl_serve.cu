@@ -41,6 +41,7 @@ struct HostScene {
     std::vector<fl_image> images;              // pointing into pixels
     Scene *dev = nullptr;
     uint64_t bytes = 0;
+    bool removed = false;  // fl_server_remove_scene: release once no job uses it
 };
 
 struct HostJob {
@@ -77,6 +78,7 @@ struct Server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     bool stop = false;
+    int removals = 0;  // scenes removed by the caller and not yet released
     std::thread worker;
     ServeScheduler sched;
     std::map<uint64_t, HostScene> scenes;
@@ -167,7 +169,7 @@ void worker_loop(Server *S) {
         std::vector<ServeScheduler::Seg> segs;
         {
             std::unique_lock<std::mutex> lock(S->mu);
-            S->cv_work.wait(lock, [&] { return S->stop || !S->sched.idle(); });
+            S->cv_work.wait(lock, [&] { return S->stop || !S->sched.idle() || S->removals > 0; });
             if (S->stop) break;
             adm = S->sched.admit();
             // scenes: release, then build
@@ -274,6 +276,22 @@ void worker_loop(Server *S) {
             }
         }
         if (!done.empty()) S->cv_done.notify_all();
+        // scenes removed by the caller that no job uses any more
+        std::vector<Scene *> drop;
+        {
+            std::lock_guard<std::mutex> lock(S->mu);
+            for (auto it = S->scenes.begin(); it != S->scenes.end();) {
+                if (it->second.removed && S->sched.scene_unused(it->first)) {
+                    S->sched.forget_scene(it->first);
+                    S->removals--;
+                    if (it->second.dev) drop.push_back(it->second.dev);
+                    it = S->scenes.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        }
+        for (Scene *sc : drop) fl_scene_destroy(reinterpret_cast<fl_scene *>(sc));
     }
 }
 
@@ -289,7 +307,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     if (!ctx || !cfg || !out) return FL_ERR_INVALID;
     *out = nullptr;
     if (cfg->memory_budget_bytes == 0 || cfg->max_jobs <= 0 || cfg->max_jobs > kMaxJobs || cfg->max_depth < 0 ||
-        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64 || cfg->policy < 0 || cfg->policy > 4) {
+        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64 || cfg->policy < 0 || cfg->policy > 5) {
         set_error(ctx, "invalid server configuration");
         return FL_ERR_INVALID;
     }
@@ -405,6 +423,23 @@ fl_status fl_server_add_scene(fl_server *srv, const fl_scene_desc *d, uint64_t *
     return FL_OK;
 }
 
+fl_status fl_server_remove_scene(fl_server *srv, uint64_t scene_id) {
+    Server *S = reinterpret_cast<Server *>(srv);
+    if (!S) return FL_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        auto it = S->scenes.find(scene_id);
+        if (it == S->scenes.end() || it->second.removed) {
+            set_error(S->ctx, "unknown scene id");
+            return FL_ERR_INVALID;
+        }
+        it->second.removed = true;
+        S->removals++;
+    }
+    S->cv_work.notify_one();
+    return FL_OK;
+}
+
 fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job_id) {
     Server *S = reinterpret_cast<Server *>(srv);
     if (!S || !job || !job_id) return FL_ERR_INVALID;
@@ -423,8 +458,9 @@ fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job
     const uint64_t samples = (uint64_t)c.width * c.height * (uint64_t)p.spp;
     {
         std::lock_guard<std::mutex> lock(S->mu);
-        if (!S->sched.has_scene(job->scene_id)) {
-            set_error(S->ctx, "unknown scene id");
+        auto sc = S->scenes.find(job->scene_id);
+        if (!S->sched.has_scene(job->scene_id) || sc == S->scenes.end() || sc->second.removed) {
+            set_error(S->ctx, "unknown or removed scene id");
             return FL_ERR_INVALID;
         }
         const uint64_t id = S->next_job++;

@@ -15,8 +15,9 @@
 //    reserved share for the oldest job, at both the median and the 99th percentile.)
 //    The other policies are first come, first served packing, equal sharing
 //    (water-filling), shortest-remaining-first with a quarter of every wave reserved for
-//    the oldest running job, and highest response ratio next ((waves waited + waves
-//    needed) / waves needed). Each job gets one contiguous sample range per wave, so its
+//    the oldest running job, highest response ratio next ((waves waited + waves needed) /
+//    waves needed), and earliest deadline first (deadline = submission + 2 x the waves the
+//    job needs alone + 1). Each job gets one contiguous sample range per wave, so its
 //    per-sample random streams do not depend on how it was batched.
 //  - A job is complete when all its samples were dispatched and the wave that carried its
 //    last samples has finished.
@@ -44,7 +45,19 @@ public:
         std::vector<uint64_t> rejected;  // jobs that can never fit the budget
     };
 
-    enum Policy { kShortestFirst = 0, kFirstCome = 1, kFairShare = 2, kShortestFirstAged = 3, kResponseRatio = 4 };
+    enum Policy {
+        kShortestFirst = 0,
+        kFirstCome = 1,
+        kFairShare = 2,
+        kShortestFirstAged = 3,
+        kResponseRatio = 4,
+        kDeadline = 5
+    };
+    // kDeadline: a job's deadline is its submission (in planned waves) plus kDeadlineSlack times
+    // the waves it needs alone, plus one; waves go to the earliest deadlines first. Small jobs
+    // get near deadlines and pass large ones, but a large job's deadline does not move, so
+    // once it is the earliest it is served ahead of every later arrival.
+    static constexpr double kDeadlineSlack = 2.0;
 
     ServeScheduler(uint64_t budget_bytes, int max_jobs, int policy = kShortestFirst)
         : budget_(budget_bytes), max_jobs_(max_jobs), policy_(policy) {}
@@ -142,7 +155,16 @@ public:
                 want[0].first -= g;
                 if (want[0].first == 0) want.erase(want.begin());
             }
-            if (policy_ == kResponseRatio) {
+            if (policy_ == kDeadline) {
+                auto deadline = [&](const std::pair<uint64_t, uint64_t> &w) {
+                    const JobState &js = jobs_[w.second];
+                    return (double)js.submit_wave + 1.0 + kDeadlineSlack * (double)js.total / (double)cap;
+                };
+                std::stable_sort(want.begin(), want.end(),
+                                 [&](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
+                                     return deadline(a) < deadline(b);
+                                 });
+            } else if (policy_ == kResponseRatio) {
                 // highest response ratio next: (waves waited, this one included, + waves still
                 // needed) / waves still needed, so short jobs go first and a long job's
                 // priority grows while it waits
@@ -198,6 +220,26 @@ public:
             }
         }
         return done;
+    }
+
+    // A scene no pending or running job uses (it may still be resident): can be forgotten.
+    bool scene_unused(uint64_t id) const {
+        auto it = scenes_.find(id);
+        if (it == scenes_.end() || it->second.users != 0) return false;
+        for (uint64_t j : pending_) {
+            auto jt = jobs_.find(j);
+            if (jt != jobs_.end() && jt->second.scene == id) return false;
+        }
+        return true;
+    }
+    // Forgets an unused scene; returns whether it was resident (its memory is released).
+    bool forget_scene(uint64_t id) {
+        auto it = scenes_.find(id);
+        if (it == scenes_.end()) return false;
+        const bool resident = it->second.resident;
+        if (resident) used_ -= it->second.bytes;
+        scenes_.erase(it);
+        return resident;
     }
 
     uint64_t used() const { return used_; }

@@ -17,7 +17,14 @@ __device__ inline void warp_add_u64(unsigned long long *dst, uint32_t v) {
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
 }
 
-constexpr int kTraceSteps = 8;
+// traversal steps a lane takes between the warp's refills of finished lanes
+#ifndef FL_TRACE_STEPS
+#define FL_TRACE_STEPS 8
+#endif
+constexpr int kTraceSteps = FL_TRACE_STEPS;
+// rays per chunk of a host-memory batch: large enough to fill the GPU, small enough that
+// a batch of 2^24 rays overlaps copies and traversal over eight chunks
+constexpr uint32_t kHostChunk = 1u << 21;
 
 template <int KIND>
 struct TraceItem {
@@ -57,12 +64,16 @@ struct TraceItem {
 
 // persistent kernel: warps refill finished lanes with new rays (fl_traverse.cuh)
 template <int KIND>
-__global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restrict__ nodes, uint32_t n_nodes,
+#ifndef FL_TRACE_MIN_BLOCKS
+#define FL_TRACE_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kTraceBlock, FL_TRACE_MIN_BLOCKS) k_trace(const WideNode *__restrict__ nodes, uint32_t n_nodes,
                                                        const float4 *__restrict__ tris, uint32_t n_tris,
                                                        const int32_t *__restrict__ tri_light, int any_hit_ok,
                                                        const float4 *__restrict__ org, const float4 *__restrict__ dir,
                                                        uint32_t n, int4 *__restrict__ hits, uint8_t *__restrict__ occ,
-                                                       int *__restrict__ err, unsigned long long *__restrict__ counters) {
+                                                       int *__restrict__ err, unsigned long long *__restrict__ counters,
+                                                       unsigned long long *__restrict__ fetch_counter) {
     TraceItem<KIND> it;
     it.org = org;
     it.dir = dir;
@@ -76,7 +87,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restric
     it.any_hit = KIND == kTraceOccluded && any_hit_ok;
     TraceStats st;
     bool error = false;
-    uint32_t *fetch = reinterpret_cast<uint32_t *>(counters + 4);
+    uint32_t *fetch = reinterpret_cast<uint32_t *>(fetch_counter);
     __shared__ uint2 stack[trav_stack_smem_bytes(kTraceBlock) / sizeof(uint2)];
     persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, error, st, stack);
     if (KIND == kTraceCount) {
@@ -89,28 +100,30 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const WideNode *__restric
 }  // namespace
 
 fl_status launch_trace(Scene *s, const float4 *org, const float4 *dir, uint32_t n, fl_hit *hits, uint8_t *occluded,
-                       int kind, cudaStream_t stream) {
+                       int kind, cudaStream_t stream, int fetch_slot) {
     if (n == 0) return FL_OK;
     // persistent grid: up to 16 blocks of 128 threads per SM, never more than the rays need
     const uint32_t grid = std::min<uint32_t>((n + kTraceBlock - 1) / kTraceBlock, (uint32_t)s->ctx->sm_count * 16u);
-    FL_CUDA_TRY(s->ctx, cudaMemsetAsync(s->ctx->d_counters + 4, 0, sizeof(unsigned long long), stream));
+    // the work counter of this launch (launches in flight on different streams use different ones)
+    unsigned long long *counters = s->ctx->d_counters + fetch_slot;
+    FL_CUDA_TRY(s->ctx, cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), stream));
     const int any_hit_ok = s->n_emissive_tris == 0 ? 1 : 0;
     int4 *h = reinterpret_cast<int4 *>(hits);
     switch (kind) {
     case kTraceClosest:
         k_trace<kTraceClosest><<<grid, kTraceBlock, 0, stream>>>(s->nodes, s->n_nodes, s->tris, s->n_tri, s->tri_light,
                                                                  any_hit_ok, org, dir, n, h, occluded,
-                                                                 s->ctx->d_error, s->ctx->d_counters);
+                                                                 s->ctx->d_error, s->ctx->d_counters, counters + 4);
         break;
     case kTraceOccluded:
         k_trace<kTraceOccluded><<<grid, kTraceBlock, 0, stream>>>(s->nodes, s->n_nodes, s->tris, s->n_tri, s->tri_light,
                                                                   any_hit_ok, org, dir, n, h, occluded,
-                                                                  s->ctx->d_error, s->ctx->d_counters);
+                                                                  s->ctx->d_error, s->ctx->d_counters, counters + 4);
         break;
     default:
         k_trace<kTraceCount><<<grid, kTraceBlock, 0, stream>>>(s->nodes, s->n_nodes, s->tris, s->n_tri, s->tri_light,
                                                                any_hit_ok, org, dir, n, h, occluded, s->ctx->d_error,
-                                                               s->ctx->d_counters);
+                                                               s->ctx->d_counters, counters + 4);
         break;
     }
     return cuda_status(s->ctx, cudaGetLastError(), "trace launch");
@@ -145,26 +158,45 @@ fl_status trace_common(fl_scene *scene_h, const float *org_tmin, const float *di
     fl_status rc = FL_OK;
     if (memory == FL_MEM_DEVICE) {
         rc = launch_trace(s, reinterpret_cast<const float4 *>(org_tmin), reinterpret_cast<const float4 *>(dir_tmax), n,
-                          hits, occluded, kind, st);
+                          hits, occluded, kind, st, 0);
         if (rc) return rc;
     } else {
-        const uint32_t chunk = std::min<uint32_t>(n, 1u << 24);
+        // Host buffers: the batch goes through in chunks on two streams that take turns, so
+        // the copies of one chunk overlap the traversal of the other (each stream has its
+        // own staging buffers and work counter).
+        const uint32_t chunk = std::min<uint32_t>(n, kHostChunk);
         const size_t per_ray = 32 + 16 + 1;
+        const size_t half = ((size_t)chunk * per_ray + 255) & ~(size_t)255;
+        const int lanes = n > chunk ? 2 : 1;
         void *scratch = nullptr;
-        if ((rc = ensure_scratch(ctx, (size_t)chunk * per_ray + 256, &scratch))) return rc;
-        float4 *d_org = reinterpret_cast<float4 *>(scratch);
-        float4 *d_dir = d_org + chunk;
-        fl_hit *d_hits = reinterpret_cast<fl_hit *>(d_dir + chunk);
-        uint8_t *d_occ = reinterpret_cast<uint8_t *>(d_hits + chunk);
-        for (uint32_t off = 0; off < n; off += chunk) {
+        if ((rc = ensure_scratch(ctx, half * lanes, &scratch))) return rc;
+        if (lanes > 1 && !ctx->stream2) FL_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+        cudaStream_t ss[2] = {st, lanes > 1 ? ctx->stream2 : st};
+        if (lanes > 1) {  // the second stream starts after the work already queued on st
+            FL_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, st));
+            FL_CUDA_TRY(ctx, cudaStreamWaitEvent(ss[1], ctx->ev_fork, 0));
+        }
+        uint32_t k = 0;
+        for (uint32_t off = 0; off < n; off += chunk, ++k) {
+            const int l = (int)(k & 1u) % lanes;
+            cudaStream_t q = ss[l];
+            char *base = static_cast<char *>(scratch) + half * l;
+            float4 *d_org = reinterpret_cast<float4 *>(base);
+            float4 *d_dir = d_org + chunk;
+            fl_hit *d_hits = reinterpret_cast<fl_hit *>(d_dir + chunk);
+            uint8_t *d_occ = reinterpret_cast<uint8_t *>(d_hits + chunk);
             const uint32_t m = std::min(chunk, n - off);
-            FL_CUDA_TRY(ctx, cudaMemcpyAsync(d_org, org_tmin + 4 * (size_t)off, 16 * (size_t)m, cudaMemcpyHostToDevice, st));
-            FL_CUDA_TRY(ctx, cudaMemcpyAsync(d_dir, dir_tmax + 4 * (size_t)off, 16 * (size_t)m, cudaMemcpyHostToDevice, st));
-            if ((rc = launch_trace(s, d_org, d_dir, m, d_hits, d_occ, kind, st))) return rc;
+            FL_CUDA_TRY(ctx, cudaMemcpyAsync(d_org, org_tmin + 4 * (size_t)off, 16 * (size_t)m, cudaMemcpyHostToDevice, q));
+            FL_CUDA_TRY(ctx, cudaMemcpyAsync(d_dir, dir_tmax + 4 * (size_t)off, 16 * (size_t)m, cudaMemcpyHostToDevice, q));
+            if ((rc = launch_trace(s, d_org, d_dir, m, d_hits, d_occ, kind, q, l))) return rc;
             if (kind == kTraceClosest)
-                FL_CUDA_TRY(ctx, cudaMemcpyAsync(hits + off, d_hits, 16 * (size_t)m, cudaMemcpyDeviceToHost, st));
+                FL_CUDA_TRY(ctx, cudaMemcpyAsync(hits + off, d_hits, 16 * (size_t)m, cudaMemcpyDeviceToHost, q));
             else if (kind == kTraceOccluded)
-                FL_CUDA_TRY(ctx, cudaMemcpyAsync(occluded + off, d_occ, m, cudaMemcpyDeviceToHost, st));
+                FL_CUDA_TRY(ctx, cudaMemcpyAsync(occluded + off, d_occ, m, cudaMemcpyDeviceToHost, q));
+        }
+        if (lanes > 1) {  // st waits for the second stream's chunks
+            FL_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_join, ss[1]));
+            FL_CUDA_TRY(ctx, cudaStreamWaitEvent(st, ctx->ev_join, 0));
         }
     }
     int err = 0;

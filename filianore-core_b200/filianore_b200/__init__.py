@@ -72,6 +72,7 @@ def lib():
         L.fl_server_create.argtypes = [vp, P(T.fl_server_config), P(vp)]
         L.fl_server_destroy.argtypes = [vp]
         L.fl_server_add_scene.argtypes = [vp, P(T.fl_scene_desc), P(C.c_uint64)]
+        L.fl_server_remove_scene.argtypes = [vp, C.c_uint64]
         L.fl_server_submit.argtypes = [vp, P(T.fl_job_desc), P(C.c_uint64)]
         L.fl_server_poll.argtypes = [vp, C.c_uint64, vp, vp, P(T.fl_job_stats)]
         L.fl_server_wait.argtypes = [vp, C.c_uint64, C.c_int32, vp, vp, P(T.fl_job_stats)]
@@ -428,6 +429,10 @@ class Server:
         sid = C.c_uint64()
         check(lib().fl_server_add_scene(self.h, C.byref(desc), C.byref(sid)), self.ctx.h)
         return sid.value
+
+    def remove_scene(self, scene_id: int) -> None:
+        """no more jobs for the scene; its memory is released once no submitted job uses it"""
+        check(lib().fl_server_remove_scene(self.h, scene_id), self.ctx.h)
 
     def submit(self, scene_id: int, camera, params) -> int:
         job = T.fl_job_desc(scene_id, camera, params)

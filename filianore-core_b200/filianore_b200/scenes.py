@@ -389,6 +389,56 @@ def procedural_spheres(n_spheres=64, slices=128, stacks=65, width=1920, height=1
     return Scene(verts, np.concatenate(mats), materials, lights, cam)
 
 
+def sphere_library(slices: int, stacks: int, n: int = 8, seed: int = 3) -> np.ndarray:
+    """n unit UV spheres (2 * slices * (stacks - 1) triangles each), each radially displaced by
+    its own value noise of amplitude 0.05: (n, triangles, 9) float32, to be scaled and placed."""
+    flat = uv_sphere(slices, stacks).reshape(-1, 3)
+    out = []
+    for k in range(n):
+        disp = 1.0 + 0.05 * value_noise(flat, seed * 1000 + k)
+        out.append((flat * disp[:, None]).reshape(-1, 9).astype(np.float32))
+    return np.stack(out)
+
+
+def request_scene(n_tri_target: float, seed: int, width: int, height: int, libraries: dict) -> Scene:
+    """A procedural scene of the procedural_spheres kind with about n_tri_target triangles, fast
+    enough to make per request: spheres of 16,384 triangles (1,024 below 131,072 triangles)
+    taken from a library of pre-displaced unit spheres (`libraries[(slices, stacks)]`, from
+    sphere_library), radii U[0.2, 1], centres U[-e, e]^2 with e growing as the square root of
+    the sphere count, the same material mix, a ground plane, an environment and a sphere light."""
+    rng = np.random.default_rng(seed)
+    key = (128, 65) if n_tri_target >= 16384 * 8 else (32, 17)
+    lib = libraries[key]
+    per = lib.shape[1]
+    n_sph = max(1, int(round(n_tri_target / per)))
+    extent = max(3.0, 10.0 * (n_sph / 64) ** 0.5)
+    pick = rng.integers(0, lib.shape[0], n_sph)
+    r = rng.uniform(0.2, 1.0, n_sph).astype(np.float32)
+    c = np.zeros((n_sph, 3), np.float32)
+    c[:, 0] = rng.uniform(-extent, extent, n_sph)
+    c[:, 1] = r
+    c[:, 2] = rng.uniform(-extent, extent, n_sph)
+    sph = (lib[pick].reshape(n_sph, per, 3, 3) * r[:, None, None, None] + c[:, None, None, :]).reshape(-1, 9)
+    g = 2.0 * extent
+    ground = np.array([[-g, 0, -g, -g, 0, g, g, 0, g], [-g, 0, -g, g, 0, g, g, 0, -g]], np.float32)
+    verts = np.concatenate([ground, sph]).astype(np.float32)
+    materials = [{"type": 0, "rgb": (0.5, 0.5, 0.5)}]
+    u = rng.uniform(size=n_sph)
+    for k in range(n_sph):
+        if u[k] < 0.4:
+            a = rng.uniform(0.1, 0.9)
+            materials.append({"type": 0, "rgb": (a, a, a)})
+        elif u[k] < 0.8:
+            materials.append({"type": 1, "roughness": rng.uniform(0.05, 0.8), "eta": 0.2, "k": 3.9})
+        else:
+            materials.append({"type": 2, "roughness": rng.uniform(0.0, 0.3), "eta": 1.5})
+    mats = np.concatenate([np.zeros(2, np.uint32), np.repeat(np.arange(1, n_sph + 1, dtype=np.uint32), per)])
+    lights = [{"type": 1, "radiance": 40.0, "radius": 0.5, "center": (0.0, 6.0, 0.0)}, {"type": 2, "radiance": 0.5}]
+    cam = {"position": (0.0, 0.7 * extent, -2.1 * extent), "look_at": (0.0, 0.5, 0.0), "up": (0.0, 1.0, 0.0),
+           "vfov": 40.0, "width": width, "height": height}
+    return Scene(verts, mats, materials, lights, cam)
+
+
 def delta_lights():
     """A point light, a spot light (30 degree cone, 20 degree full-intensity core, tilted down
     the box) and a directional light entering through the open side of the Cornell box."""

@@ -47,6 +47,7 @@ FL_SERVE_FIRST_COME = 1
 FL_SERVE_FAIR_SHARE = 2
 FL_SERVE_SHORTEST_FIRST_AGED = 3
 FL_SERVE_RESPONSE_RATIO = 4
+FL_SERVE_DEADLINE = 5
 
 
 class fl_spectral_tables(C.Structure):

@@ -410,7 +410,10 @@ enum {
     FL_SERVE_FIRST_COME = 1,      /* arrival order */
     FL_SERVE_FAIR_SHARE = 2,      /* equal shares (water-filling) */
     FL_SERVE_SHORTEST_FIRST_AGED = 3, /* shortest first, oldest job keeps a quarter of each wave */
-    FL_SERVE_RESPONSE_RATIO = 4   /* highest (waves waited + waves needed) / waves needed first */
+    FL_SERVE_RESPONSE_RATIO = 4,  /* highest (waves waited + waves needed) / waves needed first */
+    FL_SERVE_DEADLINE = 5         /* earliest deadline first, deadline = submission + 2 x the waves the job
+                                     needs alone + 1 wave: small jobs pass large ones, a large job's
+                                     deadline does not move while it waits */
 };
 
 typedef struct {
@@ -434,6 +437,9 @@ FL_API fl_status fl_server_create(fl_context *ctx, const fl_server_config *cfg, 
 FL_API fl_status fl_server_destroy(fl_server *srv);
 /* copies the scene description; the scene is built on the device when a job needs it */
 FL_API fl_status fl_server_add_scene(fl_server *srv, const fl_scene_desc *desc, uint64_t *scene_id);
+/* The scene takes no more jobs; once no submitted job uses it, its host copy and device
+ * arrays are released (for requests that each bring their own scene). */
+FL_API fl_status fl_server_remove_scene(fl_server *srv, uint64_t scene_id);
 FL_API fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job_id);
 /* FL_OK and the films (host buffers, nullable) once the job is done, FL_ERR_NOT_READY before;
  * FL_ERR_CAPACITY for a job that can never fit the budget. Results are handed out once. */

@@ -94,5 +94,38 @@ int main() {
         print_adm("B2", q.admit());
         std::printf("pending %d running %d\n", (int)q.pending(), (int)q.running());
     }
+    // earliest deadline first: job 50 (2000 samples, deadline 0 + 1 + 2 x 2000/256 = 16.6)
+    // waits behind short jobs arriving each wave (deadline w + 1 + 2 x 200/256 = w + 2.6)
+    // until their deadlines pass its own, then takes whole waves
+    {
+        ServeScheduler q(1 << 20, 8, ServeScheduler::kDeadline);
+        q.add_scene(1, 100);
+        q.submit(50, 1, 10, 2000);
+        q.admit();
+        uint64_t next = 51;
+        for (int w = 0; w < 18; ++w) {
+            q.submit(next++, 1, 10, 200);
+            q.admit();
+            auto p = q.plan_wave(256);
+            std::printf("D%d", w);
+            for (auto &sg : p) std::printf(" %llu:%u", (unsigned long long)sg.job, sg.count);
+            std::printf("\n");
+            q.finish_wave();
+        }
+    }
+    // forgetting a scene: only once no pending or running job uses it; its bytes are released
+    {
+        ServeScheduler q(1000, 4);
+        q.add_scene(1, 300);
+        q.submit(60, 1, 10, 10);
+        q.admit();
+        std::printf("F unused %d used %llu\n", (int)q.scene_unused(1), (unsigned long long)q.used());
+        q.plan_wave(64);
+        q.finish_wave();
+        std::printf("F unused %d\n", (int)q.scene_unused(1));
+        const int was_resident = (int)q.forget_scene(1);
+        std::printf("F resident %d used %llu known %d\n", was_resident, (unsigned long long)q.used(),
+                    (int)q.has_scene(1));
+    }
     return 0;
 }

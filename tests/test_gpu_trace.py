@@ -121,13 +121,15 @@ def test_traversal_counts(ctx):
 
 
 def test_raycast_microbenchmark_agreement(ctx):
-    """The ray-cast workload (8,388,608-triangle soup, incoherent and coherent rays): hit-id
-    agreement >= 99.999% with the oracle on a 2^17-ray sample of each set, hit distance
-    within 1e-6 relative; plus size-independent checks on all rays."""
+    """The ray-cast workload at its configured size (8,388,608-triangle soup; 16,777,216
+    incoherent rays and 4096 x 4096 coherent primary rays): hit-id agreement >= 99.999% with
+    the oracle on a 2^17-ray sample of each set, hit distance within 1e-6 relative; plus
+    size-independent checks on all rays (every hit lies on its triangle at distance t with
+    valid barycentrics)."""
     tris = scenes.triangle_soup(1 << 23, seed=1)
     s = ctx.scene(soup_scene(tris))
     cpu_bvh = oracle.CpuBVH(tris)
-    for org, dirs in (scenes.incoherent_rays(1 << 22, seed=2), scenes.coherent_rays(2048, 2048)):
+    for org, dirs in (scenes.incoherent_rays(1 << 24, seed=2), scenes.coherent_rays(4096, 4096)):
         h = s.trace_closest(org, dirs)
         rng = np.random.default_rng(0)
         idx = rng.choice(org.shape[0], 1 << 17, replace=False)
@@ -137,11 +139,15 @@ def test_raycast_microbenchmark_agreement(ctx):
         both = (h["id"][idx] == cpu["id"]) & (cpu["id"] >= 0)
         rel = np.abs(h["t"][idx][both] - cpu["t"][both]) / np.maximum(cpu["t"][both], 1e-30)
         assert rel.max() <= 1e-6
-        # every reported hit lies on its triangle at distance t
-        hit = h["id"] >= 0
-        tv = tris[h["id"][hit]].reshape(-1, 3, 3).astype(np.float64)
-        u, v = h["u"][hit].astype(np.float64), h["v"][hit].astype(np.float64)
-        p_tri = tv[:, 0] * (1 - u - v)[:, None] + tv[:, 1] * u[:, None] + tv[:, 2] * v[:, None]
-        p_ray = org[hit, :3].astype(np.float64) + dirs[hit, :3].astype(np.float64) * h["t"][hit][:, None]
-        assert np.max(np.abs(p_tri - p_ray)) < 1e-4
-        assert np.all((u >= 0) & (v >= 0) & (u + v <= 1 + 1e-6))
+        # every reported hit lies on its triangle at distance t (in chunks of 2^22 rays)
+        assert (h["id"] >= 0).mean() > 0.5
+        for c0 in range(0, org.shape[0], 1 << 22):
+            sl = slice(c0, c0 + (1 << 22))
+            hc, oc, dc = h[sl], org[sl], dirs[sl]
+            hit = hc["id"] >= 0
+            tv = tris[hc["id"][hit]].reshape(-1, 3, 3).astype(np.float64)
+            u, v = hc["u"][hit].astype(np.float64), hc["v"][hit].astype(np.float64)
+            p_tri = tv[:, 0] * (1 - u - v)[:, None] + tv[:, 1] * u[:, None] + tv[:, 2] * v[:, None]
+            p_ray = oc[hit, :3].astype(np.float64) + dc[hit, :3].astype(np.float64) * hc["t"][hit][:, None]
+            assert np.max(np.abs(p_tri - p_ray)) < 1e-4
+            assert np.all((u >= 0) & (v >= 0) & (u + v <= 1 + 1e-6))

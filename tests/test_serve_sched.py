@@ -67,3 +67,20 @@ def test_resident_scene_plus_film_over_budget_is_rejected():
     assert out[0] == "B1 admitted 40 | build 1 | evict | rejected"
     assert out[1] == "B2 admitted 42 | build | evict | rejected 41"
     assert out[2] == "pending 0 running 1"
+
+
+def test_deadline_policy_serves_a_long_job_once_its_deadline_is_earliest():
+    """Earliest deadline first: a 2000-sample job (deadline 1 + 2 x 2000 / 256 = 16.6 waves)
+    shares each wave with a short job arriving every wave (deadline w + 1 + 2 x 200 / 256)
+    while the short ones' deadlines are earlier, then takes whole waves: its wait is bounded
+    by its own size, not by the arrivals behind it."""
+    out = run_driver()[28:]
+    assert out[:15] == [f"D{w} 50:56 {51 + w}:200" for w in range(15)]
+    assert out[15:18] == [f"D{w} 50:256" for w in (15, 16, 17)]
+
+
+def test_removed_scene_is_forgotten_only_when_unused():
+    out = run_driver()[46:]
+    assert out[0] == "F unused 0 used 310"      # a running job holds it
+    assert out[1] == "F unused 1"               # the job is done
+    assert out[2] == "F resident 1 used 0 known 0"
