@@ -26,7 +26,7 @@ EXPORTED = [
     "fl_context_create", "fl_context_destroy", "fl_status_string", "fl_last_error", "fl_context_binned_tables",
     "fl_scene_create", "fl_scene_destroy", "fl_scene_get_info", "fl_trace_closest", "fl_trace_occluded",
     "fl_trace_count", "fl_render", "fl_li", "fl_render_noalloc", "fl_server_create", "fl_server_destroy",
-    "fl_server_add_scene", "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_get_stats",
+    "fl_server_add_scene", "fl_server_remove_scene", "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_get_stats",
     "fl_guide_create", "fl_guide_destroy", "fl_guide_render", "fl_guide_render_timed", "fl_guide_get_weights",
     "fl_guide_set_weights", "fl_guide_get_info", "fl_guide_gradient", "fl_guide_eval", "fl_guide_get_records",
 ]
