@@ -527,6 +527,7 @@ static fl_status guide_pass(Guide *G, Scene *s, const CamDev &cam, const fl_rend
         ga.binv[a] = binv[a];
     }
     const JobDev j = job_of(s, cam, p, d_film);
+    W.A.job0 = W.d_jobs;  // one job: every path's scene is job 0's
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_jobs, &j, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(W.A.cnt, 0, sizeof(WaveCounters), st));
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;

@@ -169,6 +169,7 @@ static_assert(sizeof(PathHead) == 32, "one sector per path");
 struct RenderArgs {
     TablesArg tab;
     const JobDev *jobs;      // device, kMaxJobs entries
+    const JobDev *job0;      // &jobs[0] when every path of the wave belongs to job 0 (no per-path lookup), else null
     const WaveDesc *wave;    // device
     int nl;                  // pending-term slots per path: the most lights of any job
     uint32_t cap;            // paths per wave
@@ -192,6 +193,12 @@ struct RenderArgs {
 };
 
 enum : uint32_t { kHasCL = 1u, kHasCS = 2u, kVisOK = 4u, kMisOK = 8u };
+
+// A shadow / MIS ray's tag: its path slot (< 2^25), light (< 64) and kind (0 shadow, 1 MIS)
+constexpr uint32_t kMaxWaveSlots = 1u << 25;
+__device__ __forceinline__ uint32_t shadow_tag(uint32_t slot, uint32_t li, uint32_t kind) {
+    return (slot << 7) | (li << 1) | kind;
+}
 
 // queue append from divergent code: one atomic per group of converged lanes
 __device__ inline uint32_t coalesced_append(uint32_t *counter, bool pred) {
@@ -615,13 +622,22 @@ struct PathTraceItem {
     bool any_hit;
     RayPre ray;
     TravState st;
-    __device__ bool begin(uint32_t q) {
-        slot = A->q_trace[q];
-        J = &A->jobs[A->head[slot].job];
+    __device__ void bind_job0() {  // every path in job 0: its scene once, not per ray
+        J = A->job0;
         nodes = J->nodes;
         n_nodes = J->n_nodes;
         tris = J->tris;
         n_tris = J->n_tri;
+    }
+    __device__ bool begin(uint32_t q) {
+        slot = A->q_trace[q];
+        if (!A->job0) {
+            J = &A->jobs[A->head[slot].job];
+            nodes = J->nodes;
+            n_nodes = J->n_nodes;
+            tris = J->tris;
+            n_tris = J->n_tri;
+        }
         ray = ray_precompute(A->ray_o[slot], A->ray_d[slot]);
         trav_init(st, ray);
         return true;
@@ -653,6 +669,7 @@ __global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_paths(RenderA
     PathTraceItem it;
     it.A = &A;
     it.any_hit = false;
+    if (A.job0) it.bind_job0();
     __shared__ uint2 stack[trav_stack_smem_bytes(128) / sizeof(uint2)];
     persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, err, st, stack);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->rays, (unsigned long long)n);
@@ -766,7 +783,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                                 if (pos < A.scap) {
                                     A.sray_o[pos] = so;
                                     A.sray_d[pos] = sd;
-                                    A.stag[pos] = (((uint32_t)li * A.cap + slot) << 1) | 0u;
+                                    A.stag[pos] = shadow_tag(slot, (uint32_t)li, 0u);
                                 } else {
                                     atomicAdd(&A.cnt->err, 1);
                                 }
@@ -800,7 +817,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
                                     if (pos < A.scap) {
                                         A.sray_o[pos] = make_float4(oo.x, oo.y, oo.z, kShadowEpsilon);
                                         A.sray_d[pos] = make_float4(wi.x, wi.y, wi.z, __int_as_float(0x7f800000));
-                                        A.stag[pos] = (((uint32_t)li * A.cap + slot) << 1) | 1u;
+                                        A.stag[pos] = shadow_tag(slot, (uint32_t)li, 1u);
                                     } else {
                                         atomicAdd(&A.cnt->err, 1);
                                     }
@@ -828,29 +845,39 @@ struct NeeRayItem {
     uint32_t n_nodes;
     const float4 *tris;
     uint32_t n_tris;
-    uint32_t q, kind, sl;
+    uint32_t q, kind, slot, li;
     bool any_hit;
     RayPre ray;
     TravState st;
-    __device__ bool begin(uint32_t qq) {
-        q = qq;
-        const uint32_t tag = A->stag[q];
-        kind = tag & 1u;
-        sl = tag >> 1;  // li * cap + slot
-        J = &A->jobs[A->head[sl % A->cap].job];
+    __device__ void bind_job0() {  // every path in job 0: its scene once, not per ray
+        J = A->job0;
         nodes = J->nodes;
         n_nodes = J->n_nodes;
         tris = J->tris;
         n_tris = J->n_tri;
+    }
+    __device__ bool begin(uint32_t qq) {
+        q = qq;
+        const uint32_t tag = A->stag[q];
+        kind = tag & 1u;
+        li = (tag >> 1) & 63u;
+        slot = tag >> 7;
+        if (!A->job0) {
+            J = &A->jobs[A->head[slot].job];
+            nodes = J->nodes;
+            n_nodes = J->n_nodes;
+            tris = J->tris;
+            n_tris = J->n_tri;
+        }
         ray = ray_precompute(A->sray_o[q], A->sray_d[q]);
         // shadow rays stop at the first hit when no triangle emits; a MIS ray towards the
         // environment only asks whether it escapes, so any triangle hit ends it as well
-        any_hit = kind == 0 ? J->any_hit_ok != 0 : J->lights[sl / A->cap].type == FL_LIGHT_ENV;
+        any_hit = kind == 0 ? J->any_hit_ok != 0 : J->lights[li].type == FL_LIGHT_ENV;
         trav_init(st, ray);
         return true;
     }
     __device__ void finish() {
-        const uint32_t li = sl / A->cap;
+        const uint32_t sl = li * A->cap + slot;
         TraceResult res = st.res;
         uint32_t bit = 0;
         if (kind == 0) {
@@ -881,6 +908,7 @@ __global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_rays2(RenderA
     TraceStats st;
     NeeRayItem it;
     it.A = &A;
+    if (A.job0) it.bind_job0();
     __shared__ uint2 stack[trav_stack_smem_bytes(128) / sizeof(uint2)];
     persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, err, st, stack);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1150,7 +1178,7 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
     }
     size_t cap = std::min(cap_request, (budget - head - 32 * 256) / per_slot);
     cap = std::max<size_t>(128, cap & ~(size_t)127);
-    if (cap * (size_t)std::max(nl, 1) >= ((size_t)1 << 31)) {
+    if (cap >= kMaxWaveSlots || cap * (size_t)std::max(nl, 1) >= ((size_t)1 << 31) || nl > 64) {
         set_error(ctx, "wave too large for the shadow-ray tags");
         return FL_ERR_INVALID;
     }
@@ -1347,6 +1375,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     if (rc) return rc;
     JobDev j = job_of(s, cam, p, d_film);
     if (li) j.li = *li;
+    W.A.job0 = W.d_jobs;  // one job: every path's scene is job 0's
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_jobs, &j, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     FL_CUDA_TRY(ctx, cudaMemsetAsync(W.A.cnt, 0, sizeof(WaveCounters), st));
     const bool count = (p.flags & FL_RENDER_COUNT) != 0;
