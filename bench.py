@@ -339,7 +339,7 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
     runs = []
     for frac in (1 / 3, 1 / 2, 1.0):
         g = fb.Guide(ctx, seed=5, learning_rate=1e-3, select_prob=0.5, batch=32768, max_records=1 << 21,
-                     steps_per_wave=64, weight_average=0.99)
+                     steps_per_wave=64, weight_average=0.99, learn_select=args.learn_select)
         img = np.zeros((R, R, 3), np.float64)
         t0 = time.perf_counter()
         _, gst = g.render_timed(s, scenes.render_params(4, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20),
@@ -373,8 +373,9 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
             "steps": len(runs), "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 render, f16 weights / f32 accumulate", "data": "synthetic",
             "config": {"workload": f"guide: caustic scene {R}x{R}, glass sphere 65,536 tris, sphere light r 0.02 "
-                                   f"L 5e3, depth {depth}; MLP 80-64x4-40 (8 vMF lobes), Adam lr 1e-3 on batches "
-                                   "of 32 K records, weight average 0.99, one-sample MIS c 0.5, training in the first "
+                                   f"L 5e3, depth {depth}; MLP 80-64x4-41 (8 vMF lobes + selection logit), Adam lr "
+                                   "1e-3 on batches of 32 K records, weight average 0.99, one-sample MIS with "
+                                   + ("c learned per point" if args.learn_select else "c 0.5") + ", training in the first "
                                    "25% of each budget",
                        "reference_spp": n_ref, "parallelism": "1 GPU"},
             "plain": dict(spp=n_plain, wall_ms=round(t_plain, 1), device_ms=round(pst["ms"], 1), **e_plain),
@@ -628,6 +629,7 @@ def main():
     ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve", "guide"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-raycast", action="store_true", help="render: skip the ray-cast sub-measurement")
+    ap.add_argument("--learn-select", action="store_true", help="guide: learn the selection probability per point")
     ap.add_argument("--size", default=None, help="render: WxH (smaller cases for profiling)")
     ap.add_argument("--spp", type=int, default=None, help="render: samples per pixel")
     ap.add_argument("--rays", type=int, default=None, help="raycast: rays per batch")

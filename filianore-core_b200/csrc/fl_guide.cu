@@ -50,6 +50,7 @@ struct TrainArgs {
     float bmin[3], binv[3];
     const float *cdf;          // resampling: inclusive prefix sum of the record weights (null: in order)
     uint32_t seed;             // resampling: stratification jitter of this batch
+    int learned;               // fit the selection probability with the mixture (loss -log f)
 };
 
 __device__ inline float hash01(uint32_t a, uint32_t b) {
@@ -71,8 +72,12 @@ __device__ inline float record_weight(const float *R) {
     return isfinite(w) ? w : 0.f;
 }
 
-// d(-log q(w))/d(head) for one point (FP32); returns -log q(w).
-__device__ inline float guide_head_grad(const float *h, v3 w, float *dh) {
+// d(loss)/d(head) for one point (FP32); returns the loss. Without a learned selection the
+// loss is -log q(w). With it (learned = true) the loss is -log f(w) of the one-sample MIS
+// density f = c q + (1 - c) pb, c = guide_select(h[40]) and pb the BSDF's density of w: the
+// mixture and c are fitted together, so c grows where the guide explains the incident
+// radiance better than the BSDF does and shrinks where it does not.
+__device__ inline float guide_head_grad(const float *h, v3 w, float *dh, float pb, bool learned) {
     float mx = h[0];
 #pragma unroll
     for (int j = 1; j < 8; ++j) mx = fmaxf(mx, h[j]);
@@ -116,7 +121,27 @@ __device__ inline float guide_head_grad(const float *h, v3 w, float *dh) {
         dh[32 + j] = -r * (1.f - 2.f * k / expm1f(2.f * k) + k * (dp[j] - 1.f)) *
                      (kLogKappaMax - kLogKappaMin) * sg * (1.f - sg);
     }
-    return -lse;
+    dh[40] = 0.f;
+    if (!learned) return -lse;
+    // f = c q + (1 - c) pb in logs: d(-log f)/dh_k = (c q / f) d(-log q)/dh_k for the mixture
+    // outputs, and d(-log f)/ds = -(q - pb) / f dc/ds for the selection logit s = h[40]
+    const float sg = 1.f / (1.f + expf(-h[40]));
+    const float c = kSelectMin + (kSelectMax - kSelectMin) * sg;
+    const float a = logf(c) + lse;                                   // log(c q)
+    const float b = pb > 0.f ? logf((1.f - c) * pb) : -INFINITY;     // log((1 - c) pb)
+    const float m = fmaxf(a, b);
+    const float lf = m + logf(expf(a - m) + expf(b - m));            // log f
+    const float rq = expf(a - lf);                                   // c q / f
+#pragma unroll
+    for (int k = 0; k < 40; ++k) dh[k] *= rq;
+    dh[40] = -(expf(lse - lf) - pb * expf(-lf)) * (kSelectMax - kSelectMin) * sg * (1.f - sg);
+    return -lf;
+}
+
+// the Lambert BSDF's density of a record's direction (normal facing the viewer): cos / pi
+__device__ inline float record_bsdf_pdf(const float *R) {
+    const float c = R[3] * R[7] + R[4] * R[8] + R[5] * R[9];
+    return c > 0.f ? c * kInvPi : 0.f;
 }
 
 // dW^T (in x out) += S^T D over the CTA's 128 rows: S rows = records (ld ldS, Mt 16-col
@@ -229,16 +254,17 @@ __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
     __syncwarp();
     // head gradient of the weighted loss, one lane per record, scaled into FP16 range
     if (lane < 16) {
-        float dh[kGuideOut];
+        float dh[kGuideOut + 1];  // even count: written as FP16 pairs
 #pragma unroll
-        for (int k = 0; k < kGuideOut; ++k) dh[k] = 0.f;
+        for (int k = 0; k <= kGuideOut; ++k) dh[k] = 0.f;
         float loss = 0.f;
         if (valid) {
             const float wmean = T.wstat[0] / fmaxf(T.wstat[1], 1.f);
             const float wr = record_weight(R);
             const float wn = T.cdf ? (wr > 0.f ? 1.f : 0.f) : fminf(wr / wmean, kWeightClamp);
             if (wn > 0.f) {
-                const float nl = guide_head_grad(Head + (r0 + lane) * kHeadLd, mk(R[7], R[8], R[9]), dh);
+                const float nl = guide_head_grad(Head + (r0 + lane) * kHeadLd, mk(R[7], R[8], R[9]), dh,
+                                                 record_bsdf_pdf(R), T.learned != 0);
                 loss = wn * nl;
 #pragma unroll
                 for (int k = 0; k < kGuideOut; ++k) dh[k] *= wn * kLossScale;
@@ -248,7 +274,7 @@ __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
 #pragma unroll
         for (int k = 0; k < kGuideOut; k += 2) *reinterpret_cast<uint32_t *>(drow + k) = pack_h2(dh[k], dh[k + 1], false);
 #pragma unroll
-        for (int k = kGuideOut; k < kHeadRowsPad; k += 2) *reinterpret_cast<uint32_t *>(drow + k) = 0u;
+        for (int k = kGuideOut + 1; k < kHeadRowsPad; k += 2) *reinterpret_cast<uint32_t *>(drow + k) = 0u;
         // batch loss (one atomic per warp)
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) loss += __shfl_down_sync(0x0000ffffu, loss, o, 16);
@@ -256,7 +282,7 @@ __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
     }
     __syncthreads();
     // head: dW^T = Act4^T dZ, then dZ of hidden layer 4
-    guide_dw(Act + 3 * actS, kLdH, 4, DzA, 5, T.grad + guide_woff(4), 64, 40);
+    guide_dw(Act + 3 * actS, kLdH, 4, DzA, 6, T.grad + guide_woff(4), 64, kGuideOut);
     guide_back_warp(DzA + r0 * kLdH, 3, sw + guide_sm_off(4), Act + 3 * actS + r0 * kLdH, DzB + r0 * kLdH);
     __syncthreads();
     guide_dw(Act + 2 * actS, kLdH, 4, DzB, 8, T.grad + guide_woff(3), 64, 64);
@@ -465,6 +491,7 @@ static fl_status guide_train(Guide *G, uint32_t n, const float bmin[3], const fl
         }
         T.cdf = G->cdf;
         T.seed = (uint32_t)G->steps;
+        T.learned = G->cfg.learn_select;
         k_guide_train<<<(B + kTrainRows - 1) / kTrainRows, 32 * kTrainWarps, kTrainSmem, st>>>(T);
         G->steps += 1;
         AdamArgs a{};
@@ -521,6 +548,7 @@ static fl_status guide_pass(Guide *G, Scene *s, const CamDev &cam, const fl_rend
     ga.rec_count = G->rec_count;
     ga.rec_cap = (uint32_t)G->cfg.max_records;
     ga.select = (flags & FL_GUIDE_SAMPLE) ? G->cfg.select_prob : 0.f;
+    ga.learned_select = G->cfg.learn_select;
     ga.record = train ? 1 : 0;
     for (int a = 0; a < 3; ++a) {
         ga.bmin[a] = s->bmin[a];
@@ -634,7 +662,7 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     if (!(c.learning_rate > 0.f) || !(c.select_prob >= 0.f && c.select_prob < 1.f) || c.batch < 128 ||
         c.batch > 65536 || c.batch % 128 != 0 || c.max_records < c.batch || c.max_records > (1 << 26) ||
         c.steps_per_wave < 1 || !(c.position_scale >= 0.f && c.position_scale <= 1.f) ||
-        !(c.weight_average >= 0.f && c.weight_average < 1.f)) {
+        !(c.weight_average >= 0.f && c.weight_average < 1.f) || (c.learn_select != 0 && c.learn_select != 1)) {
         set_error(ctx, "invalid guide configuration");
         return FL_ERR_INVALID;
     }
@@ -869,6 +897,7 @@ extern "C" fl_status fl_guide_gradient(fl_guide *g_h, const float *records, uint
     T.batch_size = n;
     T.wstat = G->wstat;
     T.loss = G->loss;
+    T.learned = G->cfg.learn_select;
     for (int a = 0; a < 3; ++a) {
         T.bmin[a] = bmin[a];
         T.binv[a] = binv[a];

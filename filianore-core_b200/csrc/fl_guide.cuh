@@ -6,9 +6,10 @@
 //                hero wavelength mapped to [0, 1] (1), a constant 1 that acts as the first
 //                layer's bias (1), and 3 zeros
 //   hidden       4 layers of width 64 with ReLU, no biases
-//   head   (40)  8 von Mises-Fisher lobes: mixture logits (8), unnormalised mean directions
-//                (8 x 3), log concentrations (8)
-// Weights are FP16 (row-major [out][in], packed layer after layer, 19,968 values) and every
+//   head   (41)  8 von Mises-Fisher lobes: mixture logits (8), unnormalised mean directions
+//                (8 x 3), log concentrations (8); and the logit of the point's selection
+//                probability c (used when the guide learns it, fl_guide_config.learn_select)
+// Weights are FP16 (row-major [out][in], packed layer after layer, 20,032 values) and every
 // product accumulates in FP32 on the tensor cores (mma.sync m16n8k16, operands staged in
 // shared memory and loaded with ldmatrix). One warp evaluates 16 points at a time; the
 // output of one layer stays in registers as the A operand of the next.
@@ -28,9 +29,9 @@ namespace fl {
 
 constexpr int kGuideIn = 80;
 constexpr int kGuideHidden = 64;
-constexpr int kGuideOut = 40;
+constexpr int kGuideOut = 41;
 constexpr int kGuideLobes = 8;
-constexpr int kGuideParams = 64 * 80 + 3 * 64 * 64 + 40 * 64;  // 19,968
+constexpr int kGuideParams = 64 * 80 + 3 * 64 * 64 + 41 * 64;  // 20,032
 constexpr int kGuideLayers = 5;
 // shared-memory copy of the weights: rows padded to 88 (layer 1) or 72 halves so that the
 // eight rows read by one ldmatrix fall into distinct banks; the head gets 8 zero rows so
@@ -41,12 +42,17 @@ constexpr int kHeadLd = 44;                                  // floats per head 
 // log concentration = min + (max - min) * sigmoid(s - shift): bounded, with a gradient
 // everywhere (a clamp would freeze a lobe that overshoots), about 0.4 at s = 0
 constexpr float kLogKappaMin = -2.f, kLogKappaMax = 7.f, kLogKappaShift = 2.f;
-constexpr int kMixFloats = 48;  // per path slot: pi[8], mu[8][3], kappa[8], log(pi * vMF normalisation)[8]
+// per path slot: pi[8], mu[8][3], kappa[8], log(pi * vMF normalisation)[8], c, 3 unused
+constexpr int kMixFloats = 52;
+constexpr int kMixSelect = 48;
+// learned selection probability c = min + (max - min) * sigmoid(s): kept inside (0, 1), so
+// both techniques of the one-sample MIS keep a positive density
+constexpr float kSelectMin = 0.05f, kSelectMax = 0.95f;
 constexpr int kRecFloats = 20;  // training record, see GuideArgs
 constexpr uint32_t kNoRecord = 0xffffffffu;
 
 __host__ __device__ constexpr int guide_in(int l) { return l == 0 ? 80 : 64; }
-__host__ __device__ constexpr int guide_out(int l) { return l == 4 ? 40 : 64; }
+__host__ __device__ constexpr int guide_out(int l) { return l == 4 ? 41 : 64; }
 __host__ __device__ constexpr int guide_woff(int l) { return l == 0 ? 0 : 5120 + (l - 1) * 4096; }
 __host__ __device__ constexpr int guide_sm_off(int l) { return l == 0 ? 0 : 5632 + (l - 1) * 4608; }
 __host__ __device__ constexpr int guide_sm_ld(int l) { return l == 0 ? kLdIn : kLdH; }
@@ -63,7 +69,8 @@ struct GuideArgs {
     float *rec;           // records
     uint32_t *rec_count;  // records written this wave
     uint32_t rec_cap;
-    float select;         // c: probability of sampling the mixture at a Lambert vertex
+    float select;         // c: probability of sampling the mixture at a Lambert vertex (0: guiding off)
+    int learned_select;   // take c from the network's output per point instead of `select`
     int record;           // write training records
     float bmin[3], binv[3];  // position normalisation to [0, 1]^3
 };
@@ -258,14 +265,14 @@ __device__ inline void guide_forward_warp(const __half *sw, const __half *X, __h
             *reinterpret_cast<uint32_t *>(A + (g + 8) * kLdH + kt * 16 + 8 + 2 * t) = h[kt][3];
         }
     }
-    // head (N = 40: n-tiles 0..4), linear
+    // head (N = 41: n-tiles 0..5, the last holding output 40 and seven zero rows), linear
     {
-        float acc[5][4];
+        float acc[6][4];
 #pragma unroll
-        for (int n = 0; n < 5; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+        for (int n = 0; n < 6; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
         const __half *W = sw + guide_sm_off(4);
 #pragma unroll
-        for (int np = 0; np < 2; ++np)
+        for (int np = 0; np < 3; ++np)
 #pragma unroll
             for (int kt = 0; kt < 4; ++kt) {
                 uint32_t b[4];
@@ -274,17 +281,17 @@ __device__ inline void guide_forward_warp(const __half *sw, const __half *X, __h
                 mma16816(acc[2 * np + 1], h[kt], b[2], b[3]);
             }
 #pragma unroll
-        for (int kt = 0; kt < 4; ++kt) {
-            uint32_t b[2];
-            ldsm_x2(b, W + (32 + (lane & 7)) * kLdH + kt * 16 + ((lane >> 3) & 1) * 8);
-            mma16816(acc[4], h[kt], b[0], b[1]);
-        }
-#pragma unroll
         for (int n = 0; n < 5; ++n) {
             head[g * kHeadLd + n * 8 + 2 * t] = acc[n][0];
             head[g * kHeadLd + n * 8 + 2 * t + 1] = acc[n][1];
             head[(g + 8) * kHeadLd + n * 8 + 2 * t] = acc[n][2];
             head[(g + 8) * kHeadLd + n * 8 + 2 * t + 1] = acc[n][3];
+        }
+        if (t < 2) {  // columns 40..43 of the 44 a head row holds
+            head[g * kHeadLd + 40 + 2 * t] = acc[5][0];
+            head[g * kHeadLd + 41 + 2 * t] = acc[5][1];
+            head[(g + 8) * kHeadLd + 40 + 2 * t] = acc[5][2];
+            head[(g + 8) * kHeadLd + 41 + 2 * t] = acc[5][3];
         }
     }
 }
@@ -298,8 +305,11 @@ __device__ inline float guide_kappa(float s) { return expf(guide_log_kappa(s)); 
 __device__ inline float vmf_log_norm(float k) { return logf(k) - 1.8378770664f - logf(-expm1f(-2.f * k)); }
 __device__ inline float vmf_log_norm2(float k, float logk) { return logk - 1.8378770664f - log1pf(-expf(-2.f * k)); }
 
-// Mixture parameters of one point from its 40 head outputs: pi (softmax), mu (unit), kappa,
-// and with `lognorm` also log(pi_j * C(kappa_j)) in out[40..47] for the density.
+__device__ inline float guide_select(float s) { return kSelectMin + (kSelectMax - kSelectMin) / (1.f + expf(-s)); }
+
+// Mixture parameters of one point from its 41 head outputs: pi (softmax), mu (unit), kappa
+// and the selection probability c (out[40]); with `lognorm` (the per-slot layout of
+// kMixFloats) log(pi_j * C(kappa_j)) goes to out[40..47] and c to out[kMixSelect].
 // Returns false (and marks pi[0] = -1) when the outputs are not finite.
 __device__ inline bool guide_mixture(const float *h, float *out, bool lognorm = false) {
     float mx = h[0];
@@ -326,6 +336,8 @@ __device__ inline bool guide_mixture(const float *h, float *out, bool lognorm = 
         if (lognorm) out[40 + j] = (h[j] - mx) - logf(sum) + vmf_log_norm2(out[32 + j], lk);
         ok = ok && isfinite(len) && len > 1e-6f && isfinite(h[32 + j]);
     }
+    out[lognorm ? kMixSelect : 40] = guide_select(h[40]);
+    ok = ok && isfinite(h[40]);
     if (!ok) out[0] = -1.f;
     return ok;
 }

@@ -1056,7 +1056,7 @@ __global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
                 if (!STD && b.type == FL_MAT_LAMBERT && A.g.select > 0.f && lambert_count(fl) < kGuidedVertices) {
                     gm = A.g.mix + (size_t)slot * kMixFloats;
                     if (gm[0] >= 0.f) {
-                        c_sel = A.g.select;
+                        c_sel = A.g.learned_select ? gm[kMixSelect] : A.g.select;
                         u_sel = rng.nextf();
                     }
                 }

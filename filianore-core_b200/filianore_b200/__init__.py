@@ -308,11 +308,11 @@ class Guide:
 
     def __init__(self, ctx: Context, seed: int = 1, learning_rate: float = 1e-3, select_prob: float = 0.5,
                  batch: int = 32768, max_records: int = 1 << 20, steps_per_wave: int = 16,
-                 position_scale: float = 1.0 / 16, weight_average: float = 0.99):
+                 position_scale: float = 1.0 / 16, weight_average: float = 0.99, learn_select: bool = False):
         self.ctx = ctx
         self.h = None
         cfg = T.fl_guide_config(seed, learning_rate, select_prob, batch, max_records, steps_per_wave, position_scale,
-                                weight_average)
+                                weight_average, int(learn_select))
         h = C.c_void_p()
         check(lib().fl_guide_create(ctx.h, C.byref(cfg), C.byref(h)), ctx.h)
         self.h = h
@@ -388,7 +388,7 @@ class Guide:
 
     def eval(self, records, bmin, bmax):
         r = np.ascontiguousarray(records, np.float32)
-        out = np.zeros((r.shape[0], 40), np.float32)
+        out = np.zeros((r.shape[0], 41), np.float32)  # pi[8], mu[8][3], kappa[8], c
         bn = np.asarray(bmin, np.float32)
         bx = np.asarray(bmax, np.float32)
         check(lib().fl_guide_eval(self.h, r.ctypes.data_as(C.POINTER(C.c_float)), r.shape[0],

@@ -238,7 +238,7 @@ class fl_guide_config(C.Structure):
         ("steps_per_wave", C.c_int32),
         ("position_scale", C.c_float),
         ("weight_average", C.c_float),
-        ("reserved", C.c_int32),
+        ("learn_select", C.c_int32),
     ]
 
 

@@ -495,7 +495,10 @@ typedef struct {
     float weight_average;    /* beta in [0, 1): rendering samples from the exponential moving average
                                 (decay beta per Adam step, bias-corrected) of the weights Adam
                                 produces; 0 renders with Adam's current weights */
-    int32_t reserved;
+    int32_t learn_select;    /* 1: the network also outputs each point's selection probability c, in
+                                [0.05, 0.95], fitted with the mixture by minimising -log of the
+                                one-sample MIS density c q + (1 - c) p_bsdf; select_prob > 0 still
+                                switches guided sampling on. 0: c = select_prob everywhere */
 } fl_guide_config;
 
 enum {
@@ -503,7 +506,7 @@ enum {
     FL_GUIDE_TRAIN = 2    /* record training samples and take Adam steps after every wave */
 };
 
-#define FL_GUIDE_PARAMS 19968   /* weights: [64][80], 3 x [64][64], [40][64], row-major [out][in] */
+#define FL_GUIDE_PARAMS 20032   /* weights: [64][80], 3 x [64][64], [41][64], row-major [out][in] */
 #define FL_GUIDE_RECORD_FLOATS 20
 
 FL_API fl_status fl_guide_create(fl_context *ctx, const fl_guide_config *cfg, fl_guide **out);
@@ -527,7 +530,8 @@ FL_API fl_status fl_guide_get_info(fl_guide *guide, int64_t *adam_steps, float *
 /* Training loss and its gradient on n host records (FL_GUIDE_RECORD_FLOATS floats each:
  * position 3, normal 3, wavelength, direction 3, density, incident radiance, then 8 unused)
  * in the bounds [bmin, bmax]: grad (FL_GUIDE_PARAMS floats) = d/dweights of
- * mean_i w_i * -log q(direction_i) with w_i = L_i cos_i / density_i / mean(w). Weights are
+ * mean_i w_i * -log q(direction_i) with w_i = L_i cos_i / density_i / mean(w) (with learn_select,
+ * -log(c q + (1 - c) cos_i / pi) in place of -log q). Weights are
  * unchanged. n <= max_records. */
 FL_API fl_status fl_guide_gradient(fl_guide *guide, const float *records, uint32_t n, const float bmin[3],
                                    const float bmax[3], float *grad, float *loss);
@@ -536,8 +540,8 @@ FL_API fl_status fl_guide_gradient(fl_guide *guide, const float *records, uint32
  * density, incident radiance estimate, path throughput after the vertex [4], radiance
  * gathered before it [4]. */
 FL_API fl_status fl_guide_get_records(fl_guide *guide, float *records, uint32_t max_n, uint32_t *n);
-/* Mixture parameters (40 floats per record: pi[8], mu[8][3], kappa[8]) for the points of n
- * host records in the bounds [bmin, bmax]. */
+/* Mixture parameters (41 floats per record: pi[8], mu[8][3], kappa[8], the learned selection
+ * probability c) for the points of n host records in the bounds [bmin, bmax]. */
 FL_API fl_status fl_guide_eval(fl_guide *guide, const float *records, uint32_t n, const float bmin[3],
                                const float bmax[3], float *mixture);
 

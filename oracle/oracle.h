@@ -122,7 +122,7 @@ void orc_guide_eval(const float *w32, const float *rec, uint32_t n, const float 
                     float *mix);
 /* gradient of the weighted training loss (FL_GUIDE_PARAMS floats); returns the mean loss */
 float orc_guide_gradient(const float *w32, const float *rec, uint32_t n, const float bmin[3], const float bmax[3],
-                         float *grad);
+                         float *grad, int learned);
 
 #ifdef __cplusplus
 }

@@ -63,7 +63,7 @@ def lib():
         L.orc_li.restype = C.c_int
         L.orc_guide_eval.argtypes = [P(C.c_float), P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float), P(C.c_float)]
         L.orc_guide_gradient.argtypes = [P(C.c_float), P(C.c_float), C.c_uint32, P(C.c_float), P(C.c_float),
-                                         P(C.c_float)]
+                                         P(C.c_float), C.c_int]
         L.orc_guide_gradient.restype = C.c_float
         L.orc_guide_set_exact.argtypes = [C.c_int]
         L.orc_bsdf_fcos.argtypes = [P(T.fl_material), P(C.c_float), C.c_uint32, P(C.c_float), C.c_int, P(C.c_float)]
@@ -334,10 +334,11 @@ def load_tables_dump(path):
 # ----------------------------------------------------------------------------- guiding
 
 def guide_eval(weights, records, bmin, bmax):
-    """mixture parameters (n, 40) of the guide network for the records' points"""
+    """mixture parameters (n, 41) of the guide network for the records' points: pi[8], mu[8][3],
+    kappa[8], the selection probability c"""
     w = np.ascontiguousarray(weights, dtype=np.float32)
     r = np.ascontiguousarray(records, dtype=np.float32)
-    out = np.zeros((r.shape[0], 40), np.float32)
+    out = np.zeros((r.shape[0], 41), np.float32)
     lib().orc_guide_eval(_fp(w), _fp(r), r.shape[0], _fp(np.asarray(bmin, np.float32)),
                          _fp(np.asarray(bmax, np.float32)), _fp(out))
     return out
@@ -348,13 +349,14 @@ def guide_set_exact(on: bool):
     lib().orc_guide_set_exact(1 if on else 0)
 
 
-def guide_gradient(weights, records, bmin, bmax):
-    """(gradient, mean loss) of the weighted training loss"""
+def guide_gradient(weights, records, bmin, bmax, learned=False):
+    """(gradient, mean loss) of the weighted training loss (learned: the one-sample MIS
+    mixture loss that also fits the selection probability)"""
     w = np.ascontiguousarray(weights, dtype=np.float32)
     r = np.ascontiguousarray(records, dtype=np.float32)
     g = np.zeros(w.shape[0], np.float32)
     loss = lib().orc_guide_gradient(_fp(w), _fp(r), r.shape[0], _fp(np.asarray(bmin, np.float32)),
-                                    _fp(np.asarray(bmax, np.float32)), _fp(g))
+                                    _fp(np.asarray(bmax, np.float32)), _fp(g), 1 if learned else 0)
     return g, float(loss)
 
 

@@ -16,14 +16,16 @@
 
 #define G_IN 80
 #define G_H 64
-#define G_OUT 40
-#define G_PARAMS 19968
+#define G_OUT 41
+#define G_PARAMS 20032
 #define G_REC 20
 #define G_LOSS_SCALE (1.0 / 64.0)
 #define G_WCLAMP 4096.0
 #define G_LKMIN -2.0
 #define G_LKMAX 7.0
 #define G_LKSHIFT 2.0
+#define G_SELMIN 0.05
+#define G_SELMAX 0.95
 
 static int g_exact = 0; /* 1: no FP16 rounding (finite-difference checks of the gradient) */
 void orc_guide_set_exact(int on) { g_exact = on; }
@@ -35,7 +37,7 @@ static float h16(double x) {
     return (float)(_Float16)(float)x;
 }
 static int w_in(int l) { return l == 0 ? 80 : 64; }
-static int w_out(int l) { return l == 4 ? 40 : 64; }
+static int w_out(int l) { return l == 4 ? 41 : 64; }
 static int w_off(int l) { return l == 0 ? 0 : 5120 + (l - 1) * 4096; }
 
 /* features of a record: sin/cos(2^k pi x) per axis and band, normal, wavelength, 1, zeros */
@@ -83,8 +85,11 @@ static double sigm(double s) { return 1.0 / (1.0 + exp(-(s - G_LKSHIFT))); }
 static double kappa_of(double s) { return exp(G_LKMIN + (G_LKMAX - G_LKMIN) * sigm(s)); }
 static double vmf_log_norm(double k) { return log(k) - log(2.0 * M_PI) - log(-expm1(-2.0 * k)); }
 
-/* d(-log q(d))/d(head); returns -log q(d) */
-static double head_grad(const double h[G_OUT], const double d[3], double dh[G_OUT]) {
+static double select_of(double s) { return G_SELMIN + (G_SELMAX - G_SELMIN) / (1.0 + exp(-s)); }
+
+/* d(loss)/d(head); returns the loss: -log q(d), or with a learned selection -log f(d) of the
+ * one-sample MIS density f = c q + (1 - c) pb, c = select_of(h[40]) */
+static double head_grad(const double h[G_OUT], const double d[3], double dh[G_OUT], double pb, int learned) {
     double mx = h[0];
     for (int j = 1; j < 8; ++j) mx = h[j] > mx ? h[j] : mx;
     double se = 0.0;
@@ -118,7 +123,21 @@ static double head_grad(const double h[G_OUT], const double d[3], double dh[G_OU
         const double sg = sigm(h[32 + j]), k = kap[j];
         dh[32 + j] = -r * (1.0 - 2.0 * k / expm1(2.0 * k) + k * (dp[j] - 1.0)) * (G_LKMAX - G_LKMIN) * sg * (1.0 - sg);
     }
-    return -lse;
+    dh[40] = 0.0;
+    if (!learned) return -lse;
+    const double sg = 1.0 / (1.0 + exp(-h[40]));
+    const double c = G_SELMIN + (G_SELMAX - G_SELMIN) * sg;
+    const double q = exp(lse);
+    const double f = c * q + (1.0 - c) * pb;
+    for (int k = 0; k < 40; ++k) dh[k] *= c * q / f;
+    dh[40] = -(q - pb) / f * (G_SELMAX - G_SELMIN) * sg * (1.0 - sg);
+    return -log(f);
+}
+
+/* the Lambert BSDF's density of a record's direction (normal facing the viewer) */
+static double record_bsdf_pdf(const float *R) {
+    const double c = (double)R[3] * R[7] + (double)R[4] * R[8] + (double)R[5] * R[9];
+    return c > 0.0 ? c / M_PI : 0.0;
 }
 
 static double record_weight(const float *R) {
@@ -161,12 +180,14 @@ void orc_guide_eval(const float *w32, const float *rec, uint32_t n, const float 
             for (int a = 0; a < 3; ++a) m[8 + 3 * j + a] = (float)(h[8 + 3 * j + a] / len);
             m[32 + j] = (float)kappa_of(h[32 + j]);
         }
+        m[40] = (float)select_of(h[40]);
     }
 }
 
-/* grad = d/dw of mean_r wn_r * -log q_r, wn = min(w / mean(w), clamp); returns the mean loss */
+/* grad = d/dw of mean_r wn_r * loss_r, wn = min(w / mean(w), clamp), loss_r = -log q_r (or, with
+ * learned != 0, -log of the one-sample MIS density); returns the mean loss */
 float orc_guide_gradient(const float *w32, const float *rec, uint32_t n, const float bmin[3], const float bmax[3],
-                         float *grad) {
+                         float *grad, int learned) {
     static float w[G_PARAMS];
     static double gacc[G_PARAMS];
     round_weights(w32, w);
@@ -187,7 +208,7 @@ float orc_guide_gradient(const float *w32, const float *rec, uint32_t n, const f
         features(R, bmin, binv, x);
         forward(w, x, acts, h);
         const double d[3] = {R[7], R[8], R[9]};
-        loss += wn * head_grad(h, d, dh);
+        loss += wn * head_grad(h, d, dh, record_bsdf_pdf(R), learned);
         /* back-propagation with the GPU's FP16 roundings */
         float dz[G_H], dprev[G_H];
         for (int o = 0; o < G_OUT; ++o) dz[o] = h16(dh[o] * wn * G_LOSS_SCALE);

@@ -32,7 +32,7 @@ def records(n, seed=0):
 def weights(seed=0, scale=1.0):
     """He-uniform hidden layers, Xavier head (the guide's own initialisation scheme)"""
     rng = np.random.default_rng(seed)
-    shapes = [(64, 80), (64, 64), (64, 64), (64, 64), (40, 64)]
+    shapes = [(64, 80), (64, 64), (64, 64), (64, 64), (41, 64)]
     out = []
     for l, (o, i) in enumerate(shapes):
         lim = np.sqrt(6.0 / i) if l < 4 else np.sqrt(6.0 / (i + o))

@@ -12,7 +12,7 @@ from filianore_b200 import scenes
 
 pytestmark = pytest.mark.gpu
 
-LAYER = [(0, 5120), (5120, 9216), (9216, 13312), (13312, 17408), (17408, 19968)]
+LAYER = [(0, 5120), (5120, 9216), (9216, 13312), (13312, 17408), (17408, 20032)]
 
 
 @pytest.fixture(scope="module")
@@ -22,15 +22,17 @@ def ctx():
     c.close()
 
 
-def test_gradient_matches_oracle(ctx):
+@pytest.mark.parametrize("learned", [False, True])
+def test_gradient_matches_oracle(ctx, learned):
     """FP16 tensor-core forward + backward against the oracle (same FP16 roundings, double
-    accumulation): relative L2 error of every layer's gradient below 1e-2."""
-    g = fb.Guide(ctx, max_records=8192, batch=1024)
+    accumulation): relative L2 error of every layer's gradient below 1e-2; with the learned
+    selection probability, the loss of the one-sample MIS density as well."""
+    g = fb.Guide(ctx, max_records=8192, batch=1024, learn_select=learned)
     w = gr.weights(seed=11)
     g.set_weights(w)
     rec = gr.records(3000, seed=12)
     gg, lg = g.gradient(rec, gr.BMIN, gr.BMAX)
-    gc, lc = oracle.guide_gradient(w, rec, gr.BMIN, gr.BMAX)
+    gc, lc = oracle.guide_gradient(w, rec, gr.BMIN, gr.BMAX, learned)
     assert np.isfinite(gg).all()
     assert abs(lg / lc - 1) < 1e-3, (lg, lc)
     for lo, hi in LAYER:
@@ -47,7 +49,8 @@ def test_mixture_matches_oracle(ctx):
     mg = g.eval(rec, gr.BMIN, gr.BMAX)
     mc = oracle.guide_eval(w, rec, gr.BMIN, gr.BMAX)
     assert np.abs(mg[:, :32] - mc[:, :32]).max() < 5e-3
-    assert np.abs(mg[:, 32:] / mc[:, 32:] - 1).max() < 5e-3
+    assert np.abs(mg[:, 32:40] / mc[:, 32:40] - 1).max() < 5e-3
+    assert np.abs(mg[:, 40] - mc[:, 40]).max() < 5e-3  # selection probability
     g.close()
 
 
@@ -67,15 +70,17 @@ def test_unguided_pass_equals_plain_render(ctx):
     s.close()
 
 
-def test_untrained_guide_is_unbiased(ctx):
-    """One-sample MIS with an arbitrary (untrained) mixture: the image converges to the
-    plain render's. 1024 spp; tolerances are several standard errors."""
+@pytest.mark.parametrize("learn_select", [False, True])
+def test_untrained_guide_is_unbiased(ctx, learn_select):
+    """One-sample MIS with an arbitrary (untrained) mixture, and with c fixed or taken per
+    point from the network: the image converges to the plain render's. 1024 spp; tolerances
+    are several standard errors."""
     sc = scenes.cornell(32, 32)
     s = ctx.scene(sc)
     p = scenes.render_params(1024, 8, fb.FL_SPECTRAL_HERO4)
     plain = np.zeros((32, 32, 3), np.float64)
     s.render(p, film_xyz64=plain)
-    g = fb.Guide(ctx, seed=3, select_prob=0.5)
+    g = fb.Guide(ctx, seed=3, select_prob=0.5, learn_select=learn_select)
     guided = np.zeros((32, 32, 3), np.float64)
     g.render(s, scenes.render_params(1024, 8, fb.FL_SPECTRAL_HERO4, sample_offset=5000), fb.FL_GUIDE_SAMPLE,
              film_xyz64=guided)
@@ -132,6 +137,7 @@ def test_trained_guide_lowers_caustic_error(ctx):
 
 
 def test_guide_config_is_validated(ctx):
-    for bad in ({"weight_average": 1.0}, {"weight_average": -0.1}, {"batch": 100}, {"select_prob": 1.0}):
+    for bad in ({"weight_average": 1.0}, {"weight_average": -0.1}, {"batch": 100}, {"select_prob": 1.0},
+                {"learn_select": 2}):
         with pytest.raises(fb.FlError):
             fb.Guide(ctx, **bad)

@@ -4,6 +4,7 @@ import os
 import sys
 
 import numpy as np
+import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
@@ -12,15 +13,22 @@ sys.path.insert(0, HERE)
 import oracle  # noqa: E402
 import guide_records as gr  # noqa: E402
 
-LAYER = [(0, 5120), (5120, 9216), (9216, 13312), (13312, 17408), (17408, 19968)]
+LAYER = [(0, 5120), (5120, 9216), (9216, 13312), (13312, 17408), (17408, 20032)]
 
 
-def test_gradient_matches_finite_differences():
+@pytest.mark.parametrize("learned", [False, True])
+def test_gradient_matches_finite_differences(learned):
+    """learned: the loss of the one-sample MIS density c q + (1 - c) p_bsdf, whose gradient
+    also reaches the selection output (head row 40, the last 64 weights)"""
     rec = gr.records(64, seed=3)
     w = gr.weights(seed=4).astype(np.float64)
     oracle.guide_set_exact(True)
     try:
-        g, loss = oracle.guide_gradient(w.astype(np.float32), rec, gr.BMIN, gr.BMAX)
+        g, loss = oracle.guide_gradient(w.astype(np.float32), rec, gr.BMIN, gr.BMAX, learned)
+        if learned:
+            assert np.abs(g[-64:]).max() > 0
+        else:
+            assert np.all(g[-64:] == 0)
         assert np.isfinite(loss) and loss != 0.0
         rng = np.random.default_rng(5)
         for lo, hi in LAYER:
@@ -32,8 +40,8 @@ def test_gradient_matches_finite_differences():
                 wp[i] += h
                 wm = w.copy()
                 wm[i] -= h
-                _, lp = oracle.guide_gradient(wp.astype(np.float32), rec, gr.BMIN, gr.BMAX)
-                _, lm = oracle.guide_gradient(wm.astype(np.float32), rec, gr.BMIN, gr.BMAX)
+                _, lp = oracle.guide_gradient(wp.astype(np.float32), rec, gr.BMIN, gr.BMAX, learned)
+                _, lm = oracle.guide_gradient(wm.astype(np.float32), rec, gr.BMIN, gr.BMAX, learned)
                 fd = (lp - lm) / (2 * h)
                 assert abs(fd - g[i]) <= 2e-2 * max(abs(g[i]), 1e-2 * np.abs(g[lo:hi]).max()) + 1e-4, (i, fd, g[i])
     finally:
@@ -46,4 +54,5 @@ def test_mixture_is_normalised():
     assert np.allclose(m[:, :8].sum(axis=1), 1.0, atol=1e-5)
     mu = m[:, 8:32].reshape(-1, 8, 3)
     assert np.allclose(np.linalg.norm(mu, axis=2), 1.0, atol=1e-5)
-    assert np.all(m[:, 32:] >= np.exp(-2.0) * 0.999) and np.all(m[:, 32:] <= np.exp(7.0) * 1.001)
+    assert np.all(m[:, 32:40] >= np.exp(-2.0) * 0.999) and np.all(m[:, 32:40] <= np.exp(7.0) * 1.001)
+    assert np.all((m[:, 40] >= 0.05) & (m[:, 40] <= 0.95))
