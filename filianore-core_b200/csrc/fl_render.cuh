@@ -671,7 +671,9 @@ __global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_paths(RenderA
     it.any_hit = false;
     if (A.job0) it.bind_job0();
     __shared__ uint2 stack[trav_stack_smem_bytes(128) / sizeof(uint2)];
-    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, err, st, stack);
+    __shared__ uint4 top[kSmemNodeWords];
+    const uint32_t n_top = trav_stage_top(top, A.job0 ? it.nodes : nullptr, A.job0 ? it.n_nodes : 0u);
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_trace, n, err, st, stack, top, n_top);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->rays, (unsigned long long)n);
     if (COUNT) {
         warp_count(&A.cnt->nodes, st.nodes);
@@ -910,7 +912,9 @@ __global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_rays2(RenderA
     it.A = &A;
     if (A.job0) it.bind_job0();
     __shared__ uint2 stack[trav_stack_smem_bytes(128) / sizeof(uint2)];
-    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, err, st, stack);
+    __shared__ uint4 top[kSmemNodeWords];
+    const uint32_t n_top = trav_stage_top(top, A.job0 ? it.nodes : nullptr, A.job0 ? it.n_nodes : 0u);
+    persistent_trace<kRenderTraceSteps, COUNT>(it, &A.cnt->fetch_rays2, n, err, st, stack, top, n_top);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&A.cnt->shadow_rays, (unsigned long long)n);
         atomicAdd(&A.cnt->rays, (unsigned long long)n);

@@ -89,7 +89,9 @@ __global__ void __launch_bounds__(kTraceBlock, FL_TRACE_MIN_BLOCKS) k_trace(cons
     bool error = false;
     uint32_t *fetch = reinterpret_cast<uint32_t *>(fetch_counter);
     __shared__ uint2 stack[trav_stack_smem_bytes(kTraceBlock) / sizeof(uint2)];
-    persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, error, st, stack);
+    __shared__ uint4 top[kSmemNodeWords];
+    const uint32_t n_top = trav_stage_top(top, nodes, n_nodes);
+    persistent_trace<kTraceSteps, KIND == kTraceCount>(it, fetch, n, error, st, stack, top, n_top);
     if (KIND == kTraceCount) {
         warp_add_u64(&counters[0], st.nodes);
         warp_add_u64(&counters[1], st.tris);

@@ -72,6 +72,8 @@ static_assert(kSmemStack > 0 && kSmemStack < kTraversalStack, "shared part of th
 struct TravStack {
     uint2 *sm;         // this lane's column
     uint32_t stride;   // threads per block
+    const uint4 *top;  // the first n_top wide nodes (the top of the tree), staged in shared memory
+    uint32_t n_top;
     uint2 spill[kTraversalStack - kSmemStack];
     __device__ __forceinline__ void put(int k, uint2 v) {
         if (k < kSmemStack) sm[k * stride] = v;
@@ -84,6 +86,26 @@ constexpr size_t trav_stack_smem_bytes(int threads) { return (size_t)threads * k
 __device__ __forceinline__ void trav_stack_bind(TravStack &st, uint2 *smem) {
     st.sm = smem + threadIdx.x;
     st.stride = blockDim.x;
+    st.top = nullptr;
+    st.n_top = 0;
+}
+
+// The top of the tree in shared memory: the collapse numbers wide nodes level by level, so
+// the first kSmemNodes nodes are the root and the levels under it, which every ray visits.
+// A block stages them once (all its threads call this, with the same arguments) and reads
+// them from there instead of through L1.
+#ifndef FL_SMEM_NODES
+#define FL_SMEM_NODES 0
+#endif
+constexpr int kSmemNodes = FL_SMEM_NODES;
+constexpr int kSmemNodeWords = kSmemNodes > 0 ? kSmemNodes * 5 : 1;
+__device__ __forceinline__ uint32_t trav_stage_top(uint4 *smem_nodes, const WideNode *__restrict__ nodes,
+                                                   uint32_t n_nodes) {
+    const uint32_t n_top = nodes ? min((uint32_t)kSmemNodes, n_nodes) : 0u;
+    const uint4 *src = reinterpret_cast<const uint4 *>(nodes);
+    for (uint32_t i = threadIdx.x; i < n_top * 5u; i += blockDim.x) smem_nodes[i] = __ldg(src + i);
+    __syncthreads();
+    return n_top;
 }
 
 // Triangle groups are tested when at least this many lanes of the warp test triangles;
@@ -118,12 +140,14 @@ __device__ __forceinline__ bool trav_step(TravState &s, TravStack &stack, const 
             if (s.sp < kTraversalStack) stack.put(s.sp++, s.ng);
             else { error = true; return true; }
         }
-        const uint4 *np = reinterpret_cast<const uint4 *>(nodes + ni);
-        const uint4 w0 = __ldg(np + 0);
-        const uint4 w1 = __ldg(np + 1);
-        const uint4 w2 = __ldg(np + 2);
-        const uint4 w3 = __ldg(np + 3);
-        const uint4 w4 = __ldg(np + 4);
+        uint4 w0, w1, w2, w3, w4;
+        if (kSmemNodes > 0 && ni < stack.n_top) {
+            const uint4 *np = stack.top + 5 * ni;
+            w0 = np[0], w1 = np[1], w2 = np[2], w3 = np[3], w4 = np[4];
+        } else {
+            const uint4 *np = reinterpret_cast<const uint4 *>(nodes + ni);
+            w0 = __ldg(np + 0), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+        }
         if (COUNT) stats.nodes++;
         const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
         const float sx = __uint_as_float((w0.w & 0xffu) << 23);
@@ -219,11 +243,16 @@ __device__ __forceinline__ TraceResult traverse(const WideNode *__restrict__ nod
 // state (st, ray, any_hit) and the acceleration structure it traverses (nodes, n_nodes,
 // tris, n_tris), which begin() may choose per item. Call with all 32 lanes of the warp.
 // `smem` holds the block's traversal stacks (trav_stack_smem_bytes(blockDim.x)).
+// top / n_top: the top of the tree staged by trav_stage_top (n_top 0: none), valid for
+// every item the kernel traces (one scene).
 template <int STEPS, bool COUNT, class Item>
 __device__ __forceinline__ void persistent_trace(Item &it, uint32_t *fetch_counter, uint32_t n, bool &error,
-                                                 TraceStats &stats, uint2 *smem) {
+                                                 TraceStats &stats, uint2 *smem, const uint4 *top = nullptr,
+                                                 uint32_t n_top = 0) {
     TravStack stack;
     trav_stack_bind(stack, smem);
+    stack.top = top;
+    stack.n_top = n_top;
     bool has = false;
     bool exhausted = false;
     const int lane = threadIdx.x & 31;
