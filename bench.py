@@ -557,10 +557,12 @@ def measure_raycast(args, world, rank, local, barrier, reduce_max, steps):
             scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
         barrier()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.nvtx.range_push(f"timed_{name}")
         for k in range(steps):
             ev[k][0].record()
             scene.trace_closest(d_org, d_dir, out=d_hits, stream=stream)
             ev[k][1].record()
+        torch.cuda.nvtx.range_pop()
         barrier()
         launch_ms = reduce_max(statistics.mean(a.elapsed_time(b) for a, b in ev))
         achieved = alg_bytes / (launch_ms / 1e3) / 1e9
