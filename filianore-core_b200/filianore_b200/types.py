@@ -244,7 +244,7 @@ class fl_guide_config(C.Structure):
 
 FL_GUIDE_SAMPLE = 1
 FL_GUIDE_TRAIN = 2
-FL_GUIDE_PARAMS = 19968
+FL_GUIDE_PARAMS = 20032
 FL_GUIDE_RECORD_FLOATS = 20
 
 
