@@ -64,3 +64,22 @@ def test_ctypes_structs_match_the_header(tmp_path):
         assert int(got[name]) == ctypes.sizeof(cls), name
         for field, _ in cls._fields_:
             assert int(got[f"{name}.{field}"]) == getattr(cls, field).offset, (name, field)
+
+
+def test_constants_match_the_header():
+    """Every #define and enum constant of include/filianore_gpu.h has the same value in the
+    ctypes binding (filianore_b200.types), where the binding names it."""
+    from filianore_b200 import types as T
+    text = open(os.path.join(ROOT, "include", "filianore_gpu.h")).read()
+    consts = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(FL_\w+)\s+(-?\d+)\b", text)}
+    for body in re.findall(r"enum\s*\{([^}]*)\}", text):
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        for m in re.finditer(r"(FL_\w+)\s*=\s*(-?\d+)", body):
+            consts[m.group(1)] = int(m.group(2))
+    assert "FL_GUIDE_PARAMS" in consts and "FL_RENDER_LOBE_DEPTHS" in consts
+    checked = 0
+    for name, value in consts.items():
+        if hasattr(T, name):
+            assert getattr(T, name) == value, name
+            checked += 1
+    assert checked >= 20
