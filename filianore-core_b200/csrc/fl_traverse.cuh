@@ -33,6 +33,17 @@ struct TraceStats {
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int b) { return (w >> (8 * b)) & 0xffu; }
 
+// Byte b of w as a float. FL_PRMT_CVT 1: one byte permute builds the float 2^23 + byte
+// (exponent 150, the byte as mantissa) and one subtraction of 2^23 leaves the byte exactly,
+// with integer and FP32 instructions only; 0: an integer-to-float conversion.
+#ifndef FL_PRMT_CVT
+#define FL_PRMT_CVT 0
+#endif
+__device__ __forceinline__ float byte_float(uint32_t w, int b) {
+    if (FL_PRMT_CVT) return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)b)) - 8388608.f;
+    return (float)byte_of(w, b);
+}
+
 struct TravState {
     uint2 ng, tg;
     int sp;
@@ -167,12 +178,12 @@ __device__ __forceinline__ bool trav_step(TravState &s, TravStack &stack, const 
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int bsel = i & 3;
-            const uint32_t qlx = byte_of(i < 4 ? lox0 : lox1, bsel), qhx = byte_of(i < 4 ? hix0 : hix1, bsel);
-            const uint32_t qly = byte_of(i < 4 ? loy0 : loy1, bsel), qhy = byte_of(i < 4 ? hiy0 : hiy1, bsel);
-            const uint32_t qlz = byte_of(i < 4 ? loz0 : loz1, bsel), qhz = byte_of(i < 4 ? hiz0 : hiz1, bsel);
-            const float tlx = fmaf((float)qlx, aix, aox), thx = fmaf((float)qhx, aix, aox);
-            const float tly = fmaf((float)qly, aiy, aoy), thy = fmaf((float)qhy, aiy, aoy);
-            const float tlz = fmaf((float)qlz, aiz, aoz), thz = fmaf((float)qhz, aiz, aoz);
+            const float qlx = byte_float(i < 4 ? lox0 : lox1, bsel), qhx = byte_float(i < 4 ? hix0 : hix1, bsel);
+            const float qly = byte_float(i < 4 ? loy0 : loy1, bsel), qhy = byte_float(i < 4 ? hiy0 : hiy1, bsel);
+            const float qlz = byte_float(i < 4 ? loz0 : loz1, bsel), qhz = byte_float(i < 4 ? hiz0 : hiz1, bsel);
+            const float tlx = fmaf(qlx, aix, aox), thx = fmaf(qhx, aix, aox);
+            const float tly = fmaf(qly, aiy, aoy), thy = fmaf(qhy, aiy, aoy);
+            const float tlz = fmaf(qlz, aiz, aoz), thz = fmaf(qhz, aiz, aoz);
             const float tn = fmaxf(fmaxf(tlx, tly), fmaxf(tlz, r.tmin));
             const float tf = fminf(fminf(thx, thy), fminf(thz, s.res.t)) * far_scale;
             if (tn <= tf) {
