@@ -16,6 +16,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <cfloat>
+#include <cstring>
 
 #include "fl_internal.h"
 
@@ -33,10 +34,12 @@ __device__ inline float float_unflip(uint32_t u) {
     return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }
 
-// 1. triangle bounds + centroid bounds (as order-preserving uint for atomicMin/Max)
+// 1. triangle bounds, centroid bounds (cbounds[0..5]) and scene bounds (cbounds[6..11]), the
+// last two as order-preserving uints for atomicMin/Max
 __global__ void k_tri_bounds(const float *__restrict__ soup, uint32_t n, float *__restrict__ box,
                              uint32_t *__restrict__ cbounds) {
     float cmin[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, cmax[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float smin[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, smax[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float *v = soup + 9 * (size_t)i;
         for (int a = 0; a < 3; ++a) {
@@ -47,20 +50,34 @@ __global__ void k_tri_bounds(const float *__restrict__ soup, uint32_t n, float *
             float c = 0.5f * (lo + hi);
             cmin[a] = fminf(cmin[a], c);
             cmax[a] = fmaxf(cmax[a], c);
+            smin[a] = fminf(smin[a], lo);
+            smax[a] = fmaxf(smax[a], hi);
         }
     }
     for (int a = 0; a < 3; ++a) {
         for (int o = 16; o > 0; o >>= 1) {
             cmin[a] = fminf(cmin[a], __shfl_xor_sync(0xffffffffu, cmin[a], o));
             cmax[a] = fmaxf(cmax[a], __shfl_xor_sync(0xffffffffu, cmax[a], o));
+            smin[a] = fminf(smin[a], __shfl_xor_sync(0xffffffffu, smin[a], o));
+            smax[a] = fmaxf(smax[a], __shfl_xor_sync(0xffffffffu, smax[a], o));
         }
     }
     if ((threadIdx.x & 31) == 0) {
         for (int a = 0; a < 3; ++a) {
             atomicMin(&cbounds[a], float_flip(cmin[a]));
             atomicMax(&cbounds[3 + a], float_flip(cmax[a]));
+            atomicMin(&cbounds[6 + a], float_flip(smin[a]));
+            atomicMax(&cbounds[9 + a], float_flip(smax[a]));
         }
     }
+}
+
+// the host side of float_flip's order-preserving map
+inline float host_float_unflip(uint32_t u) {
+    const uint32_t b = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    float f;
+    std::memcpy(&f, &b, sizeof f);
+    return f;
 }
 
 __device__ inline uint64_t spread3_21(uint32_t v) {
@@ -474,7 +491,7 @@ fl_status build_bvh(Scene *s) {
     WideNode *nodes_big;
     const size_t ni = n > 1 ? n - 1 : 1;
     if ((rc = tmp.get(&trib, 6 * (size_t)n)) || (rc = tmp.get(&leafbox, 6 * (size_t)n)) ||
-        (rc = tmp.get(&nodebox, 6 * ni)) || (rc = tmp.get(&cbounds, 6)) ||
+        (rc = tmp.get(&nodebox, 6 * ni)) || (rc = tmp.get(&cbounds, 12)) ||
         (rc = tmp.get(&vals_a, n)) || (rc = tmp.get(&vals_b, n)) || (rc = tmp.get(&child, 2 * ni)) ||
         (rc = tmp.get(&keys_a, n)) || (rc = tmp.get(&keys_b, n)) || (rc = tmp.get(&range, ni)) ||
         (rc = tmp.get(&front_a, n)) || (rc = tmp.get(&front_b, n)) ||
@@ -485,7 +502,8 @@ fl_status build_bvh(Scene *s) {
 
     const int bs = 256;
     const uint32_t grid_n = (n + bs - 1) / bs;
-    uint32_t init_bounds[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    uint32_t init_bounds[12] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u,
+                                0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(cbounds, init_bounds, sizeof(init_bounds), cudaMemcpyHostToDevice, st));
     uint32_t grid_b = std::min<uint32_t>(grid_n, (uint32_t)ctx->sm_count * 8u);
     k_tri_bounds<<<grid_b, bs, 0, st>>>(s->soup, n, trib, cbounds);
@@ -554,8 +572,14 @@ fl_status build_bvh(Scene *s) {
     s->max_depth = depth;
     if ((rc = dev_alloc_n(ctx, &s->nodes, s->n_nodes))) return rc;
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(s->nodes, nodes_big, sizeof(WideNode) * s->n_nodes, cudaMemcpyDeviceToDevice, st));
+    uint32_t sb[6];
+    FL_CUDA_TRY(ctx, cudaMemcpyAsync(sb, cbounds + 6, sizeof(sb), cudaMemcpyDeviceToHost, st));
     FL_CUDA_TRY(ctx, cudaEventRecord(ev1, st));
     FL_CUDA_TRY(ctx, cudaEventSynchronize(ev1));
+    for (int a = 0; a < 3; ++a) {  // the scene's bounds (for guiding's position encoding)
+        s->bmin[a] = host_float_unflip(sb[a]);
+        s->bmax[a] = host_float_unflip(sb[3 + a]);
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     s->build_ms = ms;

@@ -409,15 +409,7 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
     Scene *s = new Scene();
     s->ctx = ctx;
     s->n_tri = d->n_tri;
-    for (int a = 0; a < 3; ++a) {
-        s->bmin[a] = d->n_tri ? INFINITY : 0.f;
-        s->bmax[a] = d->n_tri ? -INFINITY : 0.f;
-    }
-    for (size_t i = 0; i < 3 * (size_t)d->n_tri; ++i)
-        for (int a = 0; a < 3; ++a) {
-            s->bmin[a] = std::min(s->bmin[a], d->verts[3 * i + a]);
-            s->bmax[a] = std::max(s->bmax[a], d->verts[3 * i + a]);
-        }
+    for (int a = 0; a < 3; ++a) s->bmin[a] = s->bmax[a] = 0.f;  // the BVH build sets them
     for (uint32_t l = 0; l < d->n_lights; ++l) {
         const fl_light &L = d->lights[l];
         if (L.type == FL_LIGHT_TRIANGLE) {
