@@ -62,11 +62,15 @@ struct TraceItem {
     }
 };
 
-// persistent kernel: warps refill finished lanes with new rays (fl_traverse.cuh)
-template <int KIND>
+// persistent kernel: warps refill finished lanes with new rays (fl_traverse.cuh). Compiled for
+// 10 resident blocks per SM (at most 48 registers): the ray-cast is latency-bound, and the
+// extra warps took the 8.4 M-triangle soup from 599 to 1015 Mrays/s (incoherent) and from
+// 1251 to 1805 (coherent) against the compiler's own choice (64 registers, 8 blocks), A/B on
+// one B200.
 #ifndef FL_TRACE_MIN_BLOCKS
-#define FL_TRACE_MIN_BLOCKS 1
+#define FL_TRACE_MIN_BLOCKS 10
 #endif
+template <int KIND>
 __global__ void __launch_bounds__(kTraceBlock, FL_TRACE_MIN_BLOCKS) k_trace(const WideNode *__restrict__ nodes, uint32_t n_nodes,
                                                        const float4 *__restrict__ tris, uint32_t n_tris,
                                                        const int32_t *__restrict__ tri_light, int any_hit_ok,

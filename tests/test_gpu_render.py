@@ -288,7 +288,7 @@ def test_standard_surface_hero_matches_oracle(ctx, ctx_metals, orc_tables, varia
     from one face to a neighbouring one near their shared edges, where the contracted build
     rounds intersections differently from the CPU: there ~2.5% of the pixels hold a path that
     went another way at 8 spp (errors of 0.2-30%; 99.9% agree in the uncontracted 60-bin
-    build), so its bound is 96% of pixels and the image mean within 1e-3."""
+    build), so its bound is 97% of pixels (97.5% measured) and the image mean within 1e-3."""
     forge = variant.endswith("_forge")
     sc = scenes.cornell(64, 64, variant.replace("_forge", ""))
     p = scenes.render_params(8, 8, fb.FL_SPECTRAL_HERO4)
@@ -297,7 +297,7 @@ def test_standard_surface_hero_matches_oracle(ctx, ctx_metals, orc_tables, varia
     cpu, cnt = oracle.render(sc, tab, p)
     assert stats["paths"] == cnt["paths"]
     thin_walled = variant.startswith("standard3")
-    assert close_fraction(xyz, cpu, 1e-3, 1e-5) >= (0.96 if thin_walled else 0.99)
+    assert close_fraction(xyz, cpu, 1e-3, 1e-5) >= (0.97 if thin_walled else 0.99)
     assert abs(xyz.mean() / cpu.mean() - 1) < (1e-3 if thin_walled else 2e-3)
 
 

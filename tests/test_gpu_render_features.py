@@ -36,7 +36,10 @@ def small_procedural():
                                      sphere_light=(0.0, 4.0, 0.0, 0.5, 40.0))
 
 
-@pytest.mark.parametrize("mode,rtol,frac_min", [(fb.FL_SPECTRAL_HERO4, 1e-3, 0.97), (fb.FL_SPECTRAL_BINS60, 1e-4, 0.97)])
+# Measured on a B200: hero 99.85% of pixels within 1e-3 (99.69% within 1e-4), 60 bins 100%
+# within 1e-4. The hero build contracts into FMAs and evaluates sin / cos in single
+# precision, so a path can rarely take another discrete decision.
+@pytest.mark.parametrize("mode,rtol,frac_min", [(fb.FL_SPECTRAL_HERO4, 1e-3, 0.995), (fb.FL_SPECTRAL_BINS60, 1e-4, 0.999)])
 def test_procedural_scene_matches_oracle(ctx, orc_tables, mode, rtol, frac_min):
     sc = small_procedural()
     p = scenes.render_params(4, 8, mode)
@@ -49,8 +52,13 @@ def test_procedural_scene_matches_oracle(ctx, orc_tables, mode, rtol, frac_min):
 
 def test_caustic_scene_matches_oracle(ctx, orc_tables):
     """Glass sphere + tiny sphere light: per pixel in the 60-bin parity build (no FMA,
-    correctly rounded sin/cos); the hero build contracts into FMAs, which the long
-    specular chains turn into different paths, so it is compared on the image mean."""
+    correctly rounded sin/cos), >= 99% of pixels within 1e-4. The hero build contracts into
+    FMAs, which the long specular chains turn into different paths in some pixels, so its
+    per-pixel bound has two parts: >= 88% of pixels within 1e-3 relative (91.0% measured),
+    and the per-pixel differences of the rest no larger than Monte Carlo noise: their 99th
+    percentile at most a quarter of the 99th percentile of the difference between two oracle
+    renders with independent samples (0.12 of it measured), their maximum below the noise's
+    maximum; the image mean within 1e-2."""
     sc = scenes.caustic(64, 64, slices=32, stacks=17)
     p = scenes.render_params(8, 8, fb.FL_SPECTRAL_BINS60)
     xyz, _ = gpu_xyz(ctx, sc, p)
@@ -59,6 +67,12 @@ def test_caustic_scene_matches_oracle(ctx, orc_tables):
     p = scenes.render_params(16, 8, fb.FL_SPECTRAL_HERO4)
     xyz, _ = gpu_xyz(ctx, sc, p)
     cpu, _ = oracle.render(sc, orc_tables, p)
+    cpu2, _ = oracle.render(sc, orc_tables, scenes.render_params(16, 8, fb.FL_SPECTRAL_HERO4, sample_offset=1000))
+    assert close_fraction(xyz, cpu, 1e-3, 1e-5) >= 0.88
+    diff = np.abs(xyz - cpu).max(axis=-1)
+    noise = np.abs(cpu2 - cpu).max(axis=-1)
+    assert np.quantile(diff, 0.99) <= 0.25 * np.quantile(noise, 0.99), (np.quantile(diff, 0.99), np.quantile(noise, 0.99))
+    assert diff.max() <= noise.max()
     assert abs(xyz.mean() / cpu.mean() - 1) < 1e-2
 
 
