@@ -184,11 +184,12 @@ __global__ void k_refit(const float *__restrict__ trib, const uint32_t *__restri
 // for i = 1, 0 = leaf and k > 0 = internal with its 8 slots split k / 8 - k; for i > 1, 0 =
 // take C(n, i - 1) and k > 0 = split k / i - k between the children. Costs climb the tree like
 // the bounds (second arrival computes).
-// Triangle-test cost against a node visit: 0.5 measured faster than 0.3 on the 8.4 M-triangle
-// soup (709 against 599 Mrays/s incoherent; 5.3 against 8.0 triangles and 22.0 against 21.0
-// nodes per ray), the render unchanged (A/B on one B200).
+// Triangle-test cost against a node visit, A/B on one B200: 0.3 -> 0.5 -> 0.8 took the
+// 8.4 M-triangle soup from 8.0 to 5.3 to 4.4 triangles per incoherent ray (21.0, 22.0, 22.5
+// nodes) and from 599 to 709 Mrays/s (0.5, with 64 registers) and 1157 to 1208 (0.8, with
+// 48), the render from 888 to 898 Mrays/s.
 #ifndef FL_SAH_TRI_COST
-#define FL_SAH_TRI_COST 0.5f
+#define FL_SAH_TRI_COST 0.8f
 #endif
 constexpr float kCostNode = 1.0f;             // a wide node visit
 constexpr float kCostTri = FL_SAH_TRI_COST;   // a triangle test, relative to a node visit

@@ -105,10 +105,15 @@ def materials(tmp):
 
 
 def depths(tmp):
-    """RenderParams with three different depths: the materials box at depths (3, 6, 5) and
-    the glass box at (5, 3, 6) (diffuse, reflection, transmission), 64x64 at 4 spp"""
+    """RenderParams with three different depths (diffuse, reflection, transmission): the
+    materials box at (3, 6, 5), the glass box at (5, 3, 6), and the StandardSurface boxes
+    "standard2" at (5, 3, 6) and "standard3" at (3, 6, 5), 64x64 at 4 spp. (The materials
+    box's GGX lobes are seen from below their normals, where the reference's sampler fails,
+    so there only the diffuse depth matters; the glass and StandardSurface boxes exercise the
+    specular, glossy and transmission depths.)"""
     out = {}
-    for variant, ds in (("materials", (3, 6, 5)), ("glass", (5, 3, 6))):
+    for variant, ds in (("materials", (3, 6, 5)), ("glass", (5, 3, 6)), ("standard2", (5, 3, 6)),
+                        ("standard3", (3, 6, 5))):
         sc = scenes.cornell(64, 64, variant)
         p = scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60, depths=ds)
         spath = os.path.join(tmp, f"depths_{variant}.scene")

@@ -76,13 +76,16 @@ def test_oracle_lobe_depths_equal_reference(orc_tables):
     Russian roulette ends them): bit-exact against the reference integrator at 64x64 x 4 spp,
     and different from the equal-depth render."""
     g = np.load(os.path.join(GOLDEN, "cornell_depths_ref.npz"))
-    for variant in ("materials", "glass"):
+    for variant in ("materials", "glass", "standard2", "standard3"):
         ds = tuple(int(d) for d in g[f"{variant}_depths"])
         sc = scenes.cornell(64, 64, variant)
         film, _ = oracle.render(sc, orc_tables, scenes.render_params(4, 8, T.FL_SPECTRAL_BINS60, depths=ds))
         assert np.array_equal(film, g[f"{variant}_xyz"]), variant
-        same, _ = oracle.render(sc, orc_tables, scenes.render_params(4, max(ds), T.FL_SPECTRAL_BINS60))
-        assert not np.array_equal(same, film)
+        deepest, _ = oracle.render(sc, orc_tables, scenes.render_params(4, max(ds), T.FL_SPECTRAL_BINS60))
+        assert not np.array_equal(deepest, film)
+        if variant != "materials":  # the materials box's GGX lobes never sample (seen from below)
+            shallow, _ = oracle.render(sc, orc_tables, scenes.render_params(4, ds[0], T.FL_SPECTRAL_BINS60))
+            assert not np.array_equal(shallow, film), variant
 
 
 def test_oracle_delta_lights_equal_reference(orc_tables):
