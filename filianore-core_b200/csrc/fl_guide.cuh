@@ -46,8 +46,15 @@ constexpr float kLogKappaMin = -2.f, kLogKappaMax = 7.f, kLogKappaShift = 2.f;
 constexpr int kMixFloats = 52;
 constexpr int kMixSelect = 48;
 // learned selection probability c = min + (max - min) * sigmoid(s): kept inside (0, 1), so
-// both techniques of the one-sample MIS keep a positive density
-constexpr float kSelectMin = 0.05f, kSelectMax = 0.95f;
+// both techniques of the one-sample MIS keep a positive density; the upper bound also bounds
+// the weight of radiance the BSDF part finds where the mixture is sharp (1 / (1 - max))
+#ifndef FL_SELECT_MIN
+#define FL_SELECT_MIN 0.05f
+#endif
+#ifndef FL_SELECT_MAX
+#define FL_SELECT_MAX 0.95f
+#endif
+constexpr float kSelectMin = FL_SELECT_MIN, kSelectMax = FL_SELECT_MAX;
 constexpr int kRecFloats = 20;  // training record, see GuideArgs
 constexpr uint32_t kNoRecord = 0xffffffffu;
 
