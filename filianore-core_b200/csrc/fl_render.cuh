@@ -610,6 +610,10 @@ constexpr int kRenderTraceSteps = FL_TRACE_STEPS;  // traversal steps between re
 #define FL_RENDER_TRACE_BLOCKS 7
 #endif
 constexpr int kRenderTraceBlocks = FL_RENDER_TRACE_BLOCKS;
+#ifndef FL_RENDER_RAYS2_BLOCKS
+#define FL_RENDER_RAYS2_BLOCKS 7
+#endif
+constexpr int kRenderRays2Blocks = FL_RENDER_RAYS2_BLOCKS;  // the same for the shadow / MIS ray kernel
 
 struct PathTraceItem {
     const RenderArgs *A;
@@ -904,7 +908,7 @@ struct NeeRayItem {
 
 // shadow rays (kind 0) and MIS rays (kind 1), persistent
 template <bool COUNT>
-__global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_rays2(RenderArgs A) {
+__global__ void __launch_bounds__(128, kRenderRays2Blocks) k_trace_rays2(RenderArgs A) {
     const uint32_t n = min(load_count(&A.cnt->n_shadow), A.scap);
     bool err = false;
     TraceStats st;
