@@ -339,7 +339,7 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
     runs = []
     for frac in (1 / 3, 1 / 2, 1.0):
         g = fb.Guide(ctx, seed=5, learning_rate=1e-3, select_prob=0.5, batch=32768, max_records=1 << 21,
-                     steps_per_wave=64, weight_average=0.99, learn_select=args.learn_select)
+                     steps_per_wave=64, weight_average=0.99, learn_select=not args.fixed_select)
         img = np.zeros((R, R, 3), np.float64)
         t0 = time.perf_counter()
         _, gst = g.render_timed(s, scenes.render_params(4, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20),
@@ -375,7 +375,8 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
             "config": {"workload": f"guide: caustic scene {R}x{R}, glass sphere 65,536 tris, sphere light r 0.02 "
                                    f"L 5e3, depth {depth}; MLP 80-64x4-41 (8 vMF lobes + selection logit), Adam lr "
                                    "1e-3 on batches of 32 K records, weight average 0.99, one-sample MIS with "
-                                   + ("c learned per point" if args.learn_select else "c 0.5") + ", training in the first "
+                                   + ("c 0.5" if args.fixed_select else "c learned per point in [0.2, 0.7]")
+                                   + ", training in the first "
                                    "25% of each budget",
                        "reference_spp": n_ref, "parallelism": "1 GPU"},
             "plain": dict(spp=n_plain, wall_ms=round(t_plain, 1), device_ms=round(pst["ms"], 1), **e_plain),
@@ -631,7 +632,8 @@ def main():
     ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve", "guide"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-raycast", action="store_true", help="render: skip the ray-cast sub-measurement")
-    ap.add_argument("--learn-select", action="store_true", help="guide: learn the selection probability per point")
+    ap.add_argument("--fixed-select", action="store_true",
+                    help="guide: a fixed selection probability c = 0.5 instead of the learned one")
     ap.add_argument("--size", default=None, help="render: WxH (smaller cases for profiling)")
     ap.add_argument("--spp", type=int, default=None, help="render: samples per pixel")
     ap.add_argument("--rays", type=int, default=None, help="raycast: rays per batch")

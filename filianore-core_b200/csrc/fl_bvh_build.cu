@@ -187,9 +187,9 @@ __global__ void k_refit(const float *__restrict__ trib, const uint32_t *__restri
 // Triangle-test cost against a node visit, A/B on one B200: 0.3 -> 0.5 -> 0.8 took the
 // 8.4 M-triangle soup from 8.0 to 5.3 to 4.4 triangles per incoherent ray (21.0, 22.0, 22.5
 // nodes) and from 599 to 709 Mrays/s (0.5, with 64 registers) and 1157 to 1208 (0.8, with
-// 48), the render from 888 to 898 Mrays/s.
+// 48), the render from 888 to 898 Mrays/s; 1.3 measured 1,230 Mrays/s (4.15 / 22.75).
 #ifndef FL_SAH_TRI_COST
-#define FL_SAH_TRI_COST 0.8f
+#define FL_SAH_TRI_COST 1.3f
 #endif
 constexpr float kCostNode = 1.0f;             // a wide node visit
 constexpr float kCostTri = FL_SAH_TRI_COST;   // a triangle test, relative to a node visit

@@ -48,11 +48,13 @@ constexpr int kMixSelect = 48;
 // learned selection probability c = min + (max - min) * sigmoid(s): kept inside (0, 1), so
 // both techniques of the one-sample MIS keep a positive density; the upper bound also bounds
 // the weight of radiance the BSDF part finds where the mixture is sharp (1 / (1 - max))
+// (measured on the 1024^2 caustic: bounds [0.05, 0.95] made the equal-time error 3.7x
+// worse than a fixed c = 0.5, [0.2, 0.7] 1.13x better)
 #ifndef FL_SELECT_MIN
-#define FL_SELECT_MIN 0.05f
+#define FL_SELECT_MIN 0.2f
 #endif
 #ifndef FL_SELECT_MAX
-#define FL_SELECT_MAX 0.95f
+#define FL_SELECT_MAX 0.7f
 #endif
 constexpr float kSelectMin = FL_SELECT_MIN, kSelectMax = FL_SELECT_MAX;
 constexpr int kRecFloats = 20;  // training record, see GuideArgs

@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
         const v3 d = normalize(dir);
         PathHead ph;
         ph.rng = rng.state;
-        ph.lambda0 = 380.f + ul * 340.f;
+        ph.lambda0 = __fadd_rn(380.f, __fmul_rn(ul, 340.f));  // not contracted: the oracle rounds twice
         ph.flags = 0u;
         ph.pixel = pix;
         ph.job = sg.job;

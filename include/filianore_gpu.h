@@ -496,7 +496,7 @@ typedef struct {
                                 (decay beta per Adam step, bias-corrected) of the weights Adam
                                 produces; 0 renders with Adam's current weights */
     int32_t learn_select;    /* 1: the network also outputs each point's selection probability c, in
-                                [0.05, 0.95], fitted with the mixture by minimising -log of the
+                                [0.2, 0.7], fitted with the mixture by minimising -log of the
                                 one-sample MIS density c q + (1 - c) p_bsdf; select_prob > 0 still
                                 switches guided sampling on. 0: c = select_prob everywhere */
 } fl_guide_config;

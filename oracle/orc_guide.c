@@ -24,8 +24,8 @@
 #define G_LKMIN -2.0
 #define G_LKMAX 7.0
 #define G_LKSHIFT 2.0
-#define G_SELMIN 0.05
-#define G_SELMAX 0.95
+#define G_SELMIN 0.2
+#define G_SELMAX 0.7
 
 static int g_exact = 0; /* 1: no FP16 rounding (finite-difference checks of the gradient) */
 void orc_guide_set_exact(int on) { g_exact = on; }

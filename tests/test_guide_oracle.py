@@ -55,4 +55,4 @@ def test_mixture_is_normalised():
     mu = m[:, 8:32].reshape(-1, 8, 3)
     assert np.allclose(np.linalg.norm(mu, axis=2), 1.0, atol=1e-5)
     assert np.all(m[:, 32:40] >= np.exp(-2.0) * 0.999) and np.all(m[:, 32:40] <= np.exp(7.0) * 1.001)
-    assert np.all((m[:, 40] >= 0.05) & (m[:, 40] <= 0.95))
+    assert np.all((m[:, 40] >= 0.2) & (m[:, 40] <= 0.7))
