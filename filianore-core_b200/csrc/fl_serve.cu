@@ -3,10 +3,12 @@
 // A worker thread owns one GPU stream and a fixed set of wave buffers. Each iteration it
 //   1. admits queued jobs in arrival order while their films (and their scene, when it is
 //      not resident) fit the memory budget, evicting idle scenes least recently used first
-//      and building newly needed scenes on the device (fl_serve_sched.h has the policy);
-//   2. plans one wave: the path slots are split over all running jobs (water-filling), each
-//      job contributing one contiguous range of its samples, so several scenes' paths run
-//      in the same kernels;
+//      (fl_serve_sched.h has the policy); newly needed scenes are handed to a builder thread,
+//      which uploads them and builds their BVHs on the context's stream while the worker's
+//      waves run, and a job takes part in waves from the first wave after its scene is built;
+//   2. plans one wave: the path slots are split over the running jobs whose scenes are
+//      ready (by the server's packing policy), each job contributing one contiguous range
+//      of its samples, so several scenes' paths run in the same kernels;
 //   3. uploads the job table and the wave's sample ranges and replays the wave as a CUDA
 //      graph captured once at start-up (the launch sequence never changes; the kernels
 //      read what to do from device memory);
@@ -18,6 +20,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <thread>
@@ -55,7 +58,16 @@ struct HostJob {
     std::vector<double> xyz;
     fl_status status = FL_ERR_NOT_READY;
     fl_status fail = FL_OK;  // set when admission could not give the job a film; reported when it completes
+    bool bound = false;      // its job table entry points at its (built) scene
     double submit_ms = 0, start_ms = 0, done_ms = 0;
+};
+
+// Work for the builder thread, done in order: build a scene, or release an evicted or
+// removed one (releases queue behind the builds issued before them, so memory is freed in
+// the order the scheduler accounted for it).
+struct BuildTask {
+    uint64_t scene = 0;       // build this scene
+    Scene *release = nullptr; // or destroy this one
 };
 
 uint64_t scene_bytes_estimate(uint32_t n_tri, uint32_t n_mat) {
@@ -79,7 +91,11 @@ struct Server {
     std::condition_variable cv_work, cv_done;
     bool stop = false;
     int removals = 0;  // scenes removed by the caller and not yet released
+    uint64_t events = 0;  // submissions, removals and finished builds: the worker looks again
     std::thread worker;
+    std::thread builder;
+    std::deque<BuildTask> build_q;
+    std::condition_variable cv_build;
     ServeScheduler sched;
     std::map<uint64_t, HostScene> scenes;
     std::map<uint64_t, std::unique_ptr<HostJob>> jobs;
@@ -111,7 +127,9 @@ struct Server {
         else cudaFree(p);
     }
 
-    Server(uint64_t budget, int max_jobs, int policy) : sched(budget, max_jobs, policy) {}
+    Server(uint64_t budget, int max_jobs, int policy) : sched(budget, max_jobs, policy) {
+        sched.set_async_builds(true);
+    }
     double now_ms() const {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
@@ -119,7 +137,7 @@ struct Server {
 
 namespace {
 
-fl_status make_scene(Server *S, HostScene &h) {
+fl_status make_scene(Server *S, const HostScene &h, Scene **out_scene) {
     fl_scene_desc d{};
     d.verts = h.verts.data();
     d.n_tri = (uint32_t)(h.verts.size() / 9);
@@ -135,8 +153,43 @@ fl_status make_scene(Server *S, HostScene &h) {
     d.n_images = (uint32_t)h.images.size();
     fl_scene *out = nullptr;
     fl_status rc = fl_scene_create(reinterpret_cast<fl_context *>(S->ctx), &d, &out);
-    if (rc == FL_OK) h.dev = reinterpret_cast<Scene *>(out);
+    *out_scene = rc == FL_OK ? reinterpret_cast<Scene *>(out) : nullptr;
     return rc;
+}
+
+// Builds and releases scenes in the order the worker queued them. A scene whose build
+// failed is still marked built; its jobs then fail with FL_ERR_OOM when they are bound.
+void builder_loop(Server *S) {
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lock(S->mu);
+    while (true) {
+        S->cv_build.wait(lock, [&] { return S->stop || !S->build_q.empty(); });
+        if (S->stop) break;  // fl_server_destroy releases what is left
+        const BuildTask t = S->build_q.front();
+        S->build_q.pop_front();
+        if (t.release) {
+            lock.unlock();
+            fl_scene_destroy(reinterpret_cast<fl_scene *>(t.release));
+            lock.lock();
+            continue;
+        }
+        auto it = S->scenes.find(t.scene);
+        if (it == S->scenes.end()) continue;
+        // the map node stays: a job that waits for this scene holds it until the scene is built
+        const HostScene *h = &it->second;
+        Scene *dev = h->dev;
+        fl_status rc = FL_OK;
+        if (!dev) {
+            lock.unlock();
+            rc = make_scene(S, *h, &dev);
+            lock.lock();
+        }
+        it->second.dev = dev;
+        if (rc == FL_OK) S->stats.builds++;
+        S->sched.scene_built(t.scene);
+        S->events++;
+        S->cv_work.notify_one();
+    }
 }
 
 void finish_job(Server *S, uint64_t jid, HostJob &job) {
@@ -164,38 +217,39 @@ void finish_job(Server *S, uint64_t jid, HostJob &job) {
 void worker_loop(Server *S) {
     cudaSetDevice(S->ctx->device);
     const size_t desc_head = offsetof(WaveDesc, seg);
+    uint64_t seen = 0;
+    bool progressed = true;  // the last iteration ran a wave or completed jobs
     while (true) {
         ServeScheduler::Admission adm;
         std::vector<ServeScheduler::Seg> segs;
         {
             std::unique_lock<std::mutex> lock(S->mu);
-            S->cv_work.wait(lock, [&] { return S->stop || !S->sched.idle() || S->removals > 0; });
+            // with nothing to run (every running job waits for its scene) wait for news
+            S->cv_work.wait(lock, [&] { return S->stop || S->events != seen || (progressed && !S->sched.idle()); });
             if (S->stop) break;
+            seen = S->events;
             adm = S->sched.admit();
-            // scenes: release, then build
+            // scenes: release, then build, in this order on the builder thread
             for (uint64_t sid : adm.evict) {
                 HostScene &h = S->scenes[sid];
-                if (h.dev) fl_scene_destroy(reinterpret_cast<fl_scene *>(h.dev));
+                if (h.dev) S->build_q.push_back(BuildTask{0, h.dev});
                 h.dev = nullptr;
                 S->stats.evictions++;
             }
+            for (uint64_t sid : adm.build) S->build_q.push_back(BuildTask{sid, nullptr});
             for (uint64_t jid : adm.rejected) {
                 auto it = S->jobs.find(jid);
                 if (it != S->jobs.end()) it->second->status = FL_ERR_CAPACITY;
             }
         }
+        if (!adm.evict.empty() || !adm.build.empty()) S->cv_build.notify_one();
         if (!adm.rejected.empty()) S->cv_done.notify_all();
-        for (uint64_t sid : adm.build) {
-            HostScene &h = S->scenes[sid];
-            if (!h.dev && make_scene(S, h) == FL_OK) S->stats.builds++;
-        }
         {
             std::lock_guard<std::mutex> lock(S->mu);
             for (uint64_t jid : adm.admitted) {
                 HostJob &job = *S->jobs[jid];
                 const size_t n_pix = (size_t)job.cam.width * job.cam.height;
-                HostScene &h = S->scenes[job.scene];
-                bool ok = h.dev != nullptr && !S->free_slots.empty();
+                bool ok = !S->free_slots.empty();
                 if (ok) job.d_film = static_cast<double *>(S->acquire(n_pix * 3 * sizeof(double)));
                 if (ok) job.d_rgb = static_cast<float *>(S->acquire(n_pix * 3 * sizeof(float)));
                 if (!job.d_film || !job.d_rgb) ok = false;
@@ -210,11 +264,30 @@ void worker_loop(Server *S) {
                 cudaMemsetAsync(job.d_film, 0, n_pix * 3 * sizeof(double), S->stream);
                 job.slot = S->free_slots.back();
                 S->free_slots.pop_back();
+            }
+            // jobs whose scenes are now built join this wave; a failed build fails its jobs
+            for (uint64_t jid : S->sched.running_jobs()) {
+                HostJob &job = *S->jobs[jid];
+                if (job.bound || job.slot < 0 || !S->sched.scene_ready(job.scene)) continue;
+                const HostScene &h = S->scenes[job.scene];
+                job.bound = true;
                 job.start_ms = S->now_ms();
-                S->table[job.slot] = job_of(h.dev, camera_basis_of(job.cam), job.params, job.d_film);
+                if (h.dev) {
+                    S->table[job.slot] = job_of(h.dev, camera_basis_of(job.cam), job.params, job.d_film);
+                } else {
+                    const size_t n_pix = (size_t)job.cam.width * job.cam.height;
+                    S->release(job.d_film, n_pix * 3 * sizeof(double));
+                    S->release(job.d_rgb, n_pix * 3 * sizeof(float));
+                    job.d_film = nullptr;
+                    job.d_rgb = nullptr;
+                    job.fail = FL_ERR_OOM;
+                    S->free_slots.push_back(job.slot);
+                    job.slot = -1;
+                }
             }
             segs = S->sched.plan_wave((uint32_t)S->W.cap);
         }
+        progressed = !segs.empty();
         if (!segs.empty()) {
             WaveDesc d{};
             uint32_t slot_begin = 0;
@@ -275,23 +348,29 @@ void worker_loop(Server *S) {
                 job->slot = -1;
             }
         }
-        if (!done.empty()) S->cv_done.notify_all();
+        if (!done.empty()) {
+            progressed = true;
+            S->cv_done.notify_all();
+        }
         // scenes removed by the caller that no job uses any more
-        std::vector<Scene *> drop;
+        bool dropped = false;
         {
             std::lock_guard<std::mutex> lock(S->mu);
-            for (auto it = S->scenes.begin(); it != S->scenes.end();) {
+            for (auto it = S->scenes.begin(); S->removals > 0 && it != S->scenes.end();) {
                 if (it->second.removed && S->sched.scene_unused(it->first)) {
                     S->sched.forget_scene(it->first);
                     S->removals--;
-                    if (it->second.dev) drop.push_back(it->second.dev);
+                    if (it->second.dev) {
+                        S->build_q.push_back(BuildTask{0, it->second.dev});
+                        dropped = true;
+                    }
                     it = S->scenes.erase(it);
                 } else {
                     ++it;
                 }
             }
         }
-        for (Scene *sc : drop) fl_scene_destroy(reinterpret_cast<fl_scene *>(sc));
+        if (dropped) S->cv_build.notify_one();
     }
 }
 
@@ -307,7 +386,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     if (!ctx || !cfg || !out) return FL_ERR_INVALID;
     *out = nullptr;
     if (cfg->memory_budget_bytes == 0 || cfg->max_jobs <= 0 || cfg->max_jobs > kMaxJobs || cfg->max_depth < 0 ||
-        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64 || cfg->policy < 0 || cfg->policy > 5) {
+        cfg->max_depth > 250 || cfg->max_lights < 0 || cfg->max_lights > 64 || cfg->policy < 0 || cfg->policy > 6) {
         set_error(ctx, "invalid server configuration");
         return FL_ERR_INVALID;
     }
@@ -354,6 +433,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     Server *raw = S.release();
     ctx->children++;
     raw->worker = std::thread(worker_loop, raw);
+    raw->builder = std::thread(builder_loop, raw);
     *out = reinterpret_cast<fl_server *>(raw);
     return FL_OK;
 }
@@ -366,9 +446,13 @@ fl_status fl_server_destroy(fl_server *srv) {
         S->stop = true;
     }
     S->cv_work.notify_all();
+    S->cv_build.notify_all();
     if (S->worker.joinable()) S->worker.join();
+    if (S->builder.joinable()) S->builder.join();
     cudaSetDevice(S->ctx->device);
     cudaStreamSynchronize(S->stream);
+    for (const BuildTask &t : S->build_q)
+        if (t.release) fl_scene_destroy(reinterpret_cast<fl_scene *>(t.release));
     for (auto &kv : S->jobs) {
         cudaFree(kv.second->d_film);
         cudaFree(kv.second->d_rgb);
@@ -435,6 +519,7 @@ fl_status fl_server_remove_scene(fl_server *srv, uint64_t scene_id) {
         }
         it->second.removed = true;
         S->removals++;
+        S->events++;
     }
     S->cv_work.notify_one();
     return FL_OK;
@@ -468,6 +553,7 @@ fl_status fl_server_submit(fl_server *srv, const fl_job_desc *job, uint64_t *job
         S->jobs[id] = std::move(hj);
         S->sched.submit(id, job->scene_id, film, samples);
         S->stats.jobs_submitted++;
+        S->events++;
         *job_id = id;
     }
     S->cv_work.notify_one();

@@ -16,8 +16,9 @@
 //    The other policies are first come, first served packing, equal sharing
 //    (water-filling), shortest-remaining-first with a quarter of every wave reserved for
 //    the oldest running job, highest response ratio next ((waves waited + waves needed) /
-//    waves needed), and earliest deadline first (deadline = submission + 2 x the waves the
-//    job needs alone + 1). Each job gets one contiguous sample range per wave, so its
+//    waves needed), earliest deadline first (deadline = submission + 2 x the waves the job
+//    needs alone + 1), and arrival order with an eighth of each wave reserved for small
+//    jobs, shortest first. Each job gets one contiguous sample range per wave, so its
 //    per-sample random streams do not depend on how it was batched.
 //  - A job is complete when all its samples were dispatched and the wave that carried its
 //    last samples has finished.
@@ -51,8 +52,14 @@ public:
         kFairShare = 2,
         kShortestFirstAged = 3,
         kResponseRatio = 4,
-        kDeadline = 5
+        kDeadline = 5,
+        kFirstComeLane = 6
     };
+    // kFirstComeLane: an eighth of every wave is a lane for small jobs (those that need no
+    // more than the lane), shortest first; the rest of the wave goes to the running jobs in
+    // arrival order. A large job then runs at seven eighths of the GPU at least, in arrival
+    // order, while small jobs do not queue behind it.
+    static constexpr uint32_t kLaneDivisor = 8;
     // kDeadline: a job's deadline is its submission (in planned waves) plus kDeadlineSlack times
     // the waves it needs alone, plus one; waves go to the earliest deadlines first. Small jobs
     // get near deadlines and pass large ones, but a large job's deadline does not move, so
@@ -62,7 +69,20 @@ public:
     ServeScheduler(uint64_t budget_bytes, int max_jobs, int policy = kShortestFirst)
         : budget_(budget_bytes), max_jobs_(max_jobs), policy_(policy) {}
 
-    void add_scene(uint64_t id, uint64_t bytes) { scenes_[id] = SceneState{bytes, false, 0, 0}; }
+    void add_scene(uint64_t id, uint64_t bytes) { scenes_[id] = SceneState{bytes, false, 0, 0, false}; }
+    // With asynchronous builds a scene that admission makes resident is not ready until
+    // scene_built(id): its jobs are admitted (their memory is reserved) but get no samples
+    // until then, while jobs whose scenes are ready keep the waves full. Without them a
+    // resident scene is ready at once (the caller builds it before the next wave).
+    void set_async_builds(bool on) { async_builds_ = on; }
+    void scene_built(uint64_t id) {
+        auto it = scenes_.find(id);
+        if (it != scenes_.end() && it->second.resident) it->second.built = true;
+    }
+    bool scene_ready(uint64_t id) const {
+        auto it = scenes_.find(id);
+        return it != scenes_.end() && it->second.resident && it->second.built;
+    }
     bool has_scene(uint64_t id) const { return scenes_.count(id) != 0; }
     bool scene_resident(uint64_t id) const {
         auto it = scenes_.find(id);
@@ -103,12 +123,14 @@ public:
                     if (used_ + need <= budget_) break;
                     SceneState &ev = scenes_[p.second];
                     ev.resident = false;
+                    ev.built = false;
                     used_ -= ev.bytes;
                     a.evict.push_back(p.second);
                 }
             }
             if (!sc.resident) {
                 sc.resident = true;
+                sc.built = !async_builds_;
                 used_ += sc.bytes;
                 a.build.push_back(js.scene);
             }
@@ -123,12 +145,13 @@ public:
         return a;
     }
 
-    // Splits `cap` slots over running jobs that still have samples to dispatch.
+    // Splits `cap` slots over running jobs that still have samples to dispatch and whose
+    // scenes are ready.
     std::vector<Seg> plan_wave(uint32_t cap) {
         std::vector<std::pair<uint64_t, uint64_t>> want;  // (remaining, job)
         for (uint64_t j : running_) {
             const JobState &js = jobs_[j];
-            if (js.dispatched < js.total) want.push_back({js.total - js.dispatched, j});
+            if (js.dispatched < js.total && scene_ready(js.scene)) want.push_back({js.total - js.dispatched, j});
         }
         std::vector<Seg> segs;
         uint64_t left = cap;
@@ -155,7 +178,31 @@ public:
                 want[0].first -= g;
                 if (want[0].first == 0) want.erase(want.begin());
             }
-            if (policy_ == kDeadline) {
+            if (policy_ == kFirstComeLane) {
+                std::vector<std::pair<uint64_t, uint64_t>> small;
+                const uint64_t lane = cap / kLaneDivisor;
+                for (auto &w : want)
+                    if (w.first <= lane) small.push_back(w);
+                std::stable_sort(small.begin(), small.end(),
+                                 [](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
+                                     return a.first < b.first;
+                                 });
+                uint64_t lane_left = lane;
+                for (auto &w : small) {
+                    if (lane_left == 0) break;
+                    const uint64_t g = std::min<uint64_t>(w.first, lane_left);
+                    JobState &js = jobs_[w.second];
+                    segs.push_back(Seg{w.second, (uint32_t)g, js.dispatched});
+                    js.dispatched += g;
+                    lane_left -= g;
+                    left -= g;
+                }
+                for (auto &w : want) w.first = jobs_[w.second].total - jobs_[w.second].dispatched;
+                want.erase(std::remove_if(want.begin(), want.end(),
+                                          [](const std::pair<uint64_t, uint64_t> &w) { return w.first == 0; }),
+                           want.end());
+                // the rest in arrival order (want follows running_, which is in arrival order)
+            } else if (policy_ == kDeadline) {
                 auto deadline = [&](const std::pair<uint64_t, uint64_t> &w) {
                     const JobState &js = jobs_[w.second];
                     return (double)js.submit_wave + 1.0 + kDeadlineSlack * (double)js.total / (double)cap;
@@ -176,7 +223,7 @@ public:
                                  [&](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
                                      return ratio(a) > ratio(b);
                                  });
-            } else if (policy_ != kFirstCome) {
+            } else if (policy_ != kFirstCome && policy_ != kFirstComeLane) {
                 // shortest remaining first (first come first served keeps running_'s arrival order)
                 std::stable_sort(want.begin(), want.end(),
                                  [](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
@@ -254,6 +301,7 @@ private:
         bool resident;
         uint64_t last_use;
         int users;
+        bool built;  // resident and ready for rendering
     };
     struct JobState {
         uint64_t scene, film_bytes, total, dispatched;
@@ -270,6 +318,7 @@ private:
     uint64_t used_ = 0;
     uint64_t clock_ = 0;
     uint64_t waves_ = 0;
+    bool async_builds_ = false;
     std::map<uint64_t, SceneState> scenes_;
     std::map<uint64_t, JobState> jobs_;
     std::deque<uint64_t> pending_;

@@ -48,6 +48,7 @@ FL_SERVE_FAIR_SHARE = 2
 FL_SERVE_SHORTEST_FIRST_AGED = 3
 FL_SERVE_RESPONSE_RATIO = 4
 FL_SERVE_DEADLINE = 5
+FL_SERVE_FIRST_COME_LANE = 6
 
 
 class fl_spectral_tables(C.Structure):

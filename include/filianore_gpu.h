@@ -411,9 +411,12 @@ enum {
     FL_SERVE_FAIR_SHARE = 2,      /* equal shares (water-filling) */
     FL_SERVE_SHORTEST_FIRST_AGED = 3, /* shortest first, oldest job keeps a quarter of each wave */
     FL_SERVE_RESPONSE_RATIO = 4,  /* highest (waves waited + waves needed) / waves needed first */
-    FL_SERVE_DEADLINE = 5         /* earliest deadline first, deadline = submission + 2 x the waves the job
+    FL_SERVE_DEADLINE = 5,        /* earliest deadline first, deadline = submission + 2 x the waves the job
                                      needs alone + 1 wave: small jobs pass large ones, a large job's
                                      deadline does not move while it waits */
+    FL_SERVE_FIRST_COME_LANE = 6  /* arrival order, with an eighth of each wave reserved for jobs that fit
+                                     in it (shortest first): large jobs keep 7/8 of the GPU in arrival
+                                     order, small ones do not queue behind them */
 };
 
 typedef struct {

@@ -113,6 +113,48 @@ int main() {
             q.finish_wave();
         }
     }
+    // arrival order with a small-job lane: job 70 (2000 samples) and job 71 (200) arrive with
+    // job 72 (10); a 20-sample job arrives every later wave. The small jobs take the lane (an
+    // eighth of 256 = 32), the rest of each wave goes to 70 until it is done, then to 71.
+    {
+        ServeScheduler q(1 << 20, 16, ServeScheduler::kFirstComeLane);
+        q.add_scene(1, 100);
+        q.submit(70, 1, 10, 2000);
+        q.submit(71, 1, 10, 200);
+        q.submit(72, 1, 10, 10);
+        uint64_t next = 73;
+        for (int w = 0; w < 9; ++w) {
+            if (w > 0) q.submit(next++, 1, 10, 20);
+            q.admit();
+            auto p = q.plan_wave(256);
+            std::printf("L%d", w);
+            for (auto &sg : p) std::printf(" %llu:%u", (unsigned long long)sg.job, sg.count);
+            std::printf("\n");
+            q.finish_wave();
+        }
+    }
+    // asynchronous builds: a job whose scene is still being built gets no samples; jobs with
+    // ready scenes take the wave meanwhile
+    {
+        ServeScheduler q(1 << 20, 8, ServeScheduler::kFirstCome);
+        q.set_async_builds(true);
+        q.add_scene(1, 100);
+        q.add_scene(2, 100);
+        q.submit(80, 1, 10, 100);
+        auto a = q.admit();
+        auto p = q.plan_wave(256);
+        std::printf("G1 build %d planned %d ready %d\n", (int)a.build.size(), (int)p.size(), (int)q.scene_ready(1));
+        q.finish_wave();
+        q.scene_built(1);
+        q.submit(81, 2, 10, 100);
+        a = q.admit();
+        print_plan("G2", q.plan_wave(256));
+        q.finish_wave();
+        q.scene_built(2);
+        q.submit(82, 2, 10, 50);
+        q.admit();
+        print_plan("G3", q.plan_wave(256));
+    }
     // forgetting a scene: only once no pending or running job uses it; its bytes are released
     {
         ServeScheduler q(1000, 4);

@@ -80,7 +80,28 @@ def test_deadline_policy_serves_a_long_job_once_its_deadline_is_earliest():
 
 
 def test_removed_scene_is_forgotten_only_when_unused():
-    out = run_driver()[46:]
+    out = run_driver()[58:]
     assert out[0] == "F unused 0 used 310"      # a running job holds it
     assert out[1] == "F unused 1"               # the job is done
     assert out[2] == "F resident 1 used 0 known 0"
+
+
+def test_first_come_lane_keeps_small_jobs_out_of_the_queue():
+    """Arrival order with an eighth of each wave (32 of 256) reserved for jobs that fit in it:
+    the small jobs finish in the wave they arrive, the 2000-sample job takes the other 7/8 in
+    arrival order, and the 200-sample job (too large for the lane) waits behind it."""
+    out = run_driver()[46:55]
+    # (segments are listed in arrival order)
+    assert out[0] == "L0 70:246 72:10"
+    assert out[1:8] == [f"L{w} 70:236 {72 + w}:20" for w in range(1, 8)]
+    assert out[8] == "L8 70:102 71:134 80:20"
+
+
+def test_async_builds_hold_jobs_until_their_scene_is_built():
+    """With asynchronous builds a job takes part in waves only once its scene is built: the
+    first wave is empty while scene 1 builds; then job 80 renders alone while scene 2 builds;
+    then 81 and 82 (scene 2, already resident and built: no new build) join."""
+    out = run_driver()[55:58]
+    assert out[0] == "G1 build 1 planned 0 ready 0"
+    assert out[1] == "G2 80:100@0"
+    assert out[2] == "G3 81:100@0 82:50@0"
