@@ -190,8 +190,9 @@ def serve_requests(n_req=200, seed=5):
 def gpu_serve(args, world, rank, local, barrier, reduce_max):
     """200 requests at 80% of the measured one-job-at-a-time capacity (Poisson arrivals), each
     with its own scene: the continuous-batching server against the plain GPU path serving one
-    job at a time (scene upload + BVH build + render per request, as the server must)."""
-    import queue
+    job at a time (scene upload + BVH build + render per request, as the server must). The
+    requests' scenes are made on the host before the clock starts (a client brings its scene
+    with its request); the server's own work from fl_server_add_scene on is timed."""
     import threading
     import filianore_b200 as fb
     from filianore_b200 import scenes
@@ -199,19 +200,16 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
     reqs = serve_requests()
     n_req = len(reqs)
     libs = {(128, 65): scenes.sphere_library(128, 65), (32, 17): scenes.sphere_library(32, 17)}
-
-    def make(i):
-        target, res, _, sd = reqs[i]
-        return scenes.request_scene(target, sd, res, res, libs)
+    made = [scenes.request_scene(target, sd, res, res, libs) for (target, res, _, sd) in reqs]
     ctx = fb.Context(local)
     # plain GPU path, one job at a time: service time of every request (upload, build, render)
-    warm = ctx.scene(make(0))
+    warm = ctx.scene(made[0])
     warm.render(scenes.render_params(1, 16), camera=warm.src.camera_struct(64, 64))
     warm.close()
     service, tris = [], []
     samples = 0
     for i, (target, res, spp, _) in enumerate(reqs):
-        sc = make(i)
+        sc = made[i]
         tris.append(sc.n_tri)
         t0 = time.perf_counter()
         h = ctx.scene(sc)
@@ -232,23 +230,20 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
     serial_makespan = t
     budget = 12 << 30
     p = lambda v, q: float(np.percentile(np.asarray(v) * 1e3, q))  # noqa: E731
+    detail = {"arrival_ms": [round(a * 1e3, 2) for a in arrivals], "service_ms": [round(x * 1e3, 2) for x in service],
+              "serial_tti_ms": [round(x * 1e3, 2) for x in serial_tti], "samples": [r * r * k for (_, r, k, _) in reqs],
+              "tris": tris, "policies": {}}
 
-    def run_server(policy):
+    def run_server(name, policy):
         srv = fb.Server(ctx, budget_bytes=budget, max_depth=16, max_jobs=64, max_lights=4, policy=policy)
-        ready = queue.Queue(maxsize=12)
-
-        def producer():  # scenes are made ahead of their arrival
-            for i in range(n_req):
-                ready.put(make(i))
         job_ids = [None] * n_req
+        submitted = [threading.Event() for _ in range(n_req)]
         late = [0.0] * n_req
-        pt = threading.Thread(target=producer)
-        pt.start()
         t_start = time.perf_counter()
 
         def submitter():
             for i, (_, res, spp, _) in enumerate(reqs):
-                sc = ready.get()
+                sc = made[i]
                 delay = arrivals[i] - (time.perf_counter() - t_start)
                 if delay > 0:
                     time.sleep(delay)
@@ -256,22 +251,23 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
                 sid = srv.add_scene(sc)
                 job_ids[i] = srv.submit(sid, sc.camera_struct(res, res), scenes.render_params(spp, 16, fb.FL_SPECTRAL_HERO4))
                 srv.remove_scene(sid)  # released once its job is done
+                submitted[i].set()
         th = threading.Thread(target=submitter)
         th.start()
         tti, rows = [], []
         last_done, first_submit = 0.0, None
         for i in range(n_req):
-            while job_ids[i] is None:
-                time.sleep(0.0005)
+            submitted[i].wait()
             _, _, st = srv.wait(job_ids[i], timeout_ms=600000)
             tti.append((st["done_ms"] - st["submit_ms"]) / 1e3 + late[i])  # from the scheduled arrival
             rows.append((tti[-1], i, st))
             last_done = max(last_done, st["done_ms"])
             first_submit = st["submit_ms"] if first_submit is None else min(first_submit, st["submit_ms"])
         th.join()
-        pt.join()
         sstats = srv.stats()
         srv.close()
+        detail["policies"][name] = {"tti_ms": [round(x * 1e3, 2) for x in tti], "late_ms": [round(x * 1e3, 2) for x in late],
+                                    "queued_ms": [round(st["start_ms"] - st["submit_ms"], 2) for _, _, st in rows]}
         rows.sort(key=lambda r: -r[0])
         slowest = [{"req": i, "samples": st["samples"], "tris": tris[i], "res": reqs[i][1], "spp": reqs[i][2],
                     "queued_ms": round(st["start_ms"] - st["submit_ms"], 1), "tti_ms": round(t_ * 1e3, 1),
@@ -284,8 +280,11 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
     policies = (("response_ratio", fb.FL_SERVE_RESPONSE_RATIO), ("first_come_lane", fb.FL_SERVE_FIRST_COME_LANE),
                 ("deadline", fb.FL_SERVE_DEADLINE), ("shortest_first", fb.FL_SERVE_SHORTEST_FIRST),
                 ("first_come", fb.FL_SERVE_FIRST_COME))
-    results = {name: run_server(pol) for name, pol in policies}
+    results = {name: run_server(name, pol) for name, pol in policies}
     ctx.close()
+    if args.serve_detail:
+        with open(args.serve_detail, "w") as f:
+            json.dump(detail, f)
     best = results["response_ratio"]
     return {"metric": "p99 time-to-image", "value": best["p99_ms"], "unit": "ms", "n_gpus": world,
             "steps": n_req, "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -633,6 +632,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="render", choices=["render", "raycast", "serve", "guide"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-detail", default=None, help="serve: write per-request times to this JSON file")
     ap.add_argument("--no-raycast", action="store_true", help="render: skip the ray-cast sub-measurement")
     ap.add_argument("--fixed-select", action="store_true",
                     help="guide: a fixed selection probability c = 0.5 instead of the learned one")

@@ -614,6 +614,23 @@ constexpr int kRenderTraceBlocks = FL_RENDER_TRACE_BLOCKS;
 #define FL_RENDER_RAYS2_BLOCKS 7
 #endif
 constexpr int kRenderRays2Blocks = FL_RENDER_RAYS2_BLOCKS;  // the same for the shadow / MIS ray kernel
+// resident blocks per SM that k_shade and k_continue are compiled for (0: no bound)
+#ifndef FL_RENDER_SHADE_BLOCKS
+#define FL_RENDER_SHADE_BLOCKS 0
+#endif
+#ifndef FL_RENDER_CONT_BLOCKS
+#define FL_RENDER_CONT_BLOCKS 0
+#endif
+#if FL_RENDER_SHADE_BLOCKS > 0
+#define FL_SHADE_BOUNDS __launch_bounds__(128, FL_RENDER_SHADE_BLOCKS)
+#else
+#define FL_SHADE_BOUNDS __launch_bounds__(128)
+#endif
+#if FL_RENDER_CONT_BLOCKS > 0
+#define FL_CONT_BOUNDS __launch_bounds__(128, FL_RENDER_CONT_BLOCKS)
+#else
+#define FL_CONT_BOUNDS __launch_bounds__(128)
+#endif
 
 struct PathTraceItem {
     const RenderArgs *A;
@@ -689,7 +706,7 @@ __global__ void __launch_bounds__(128, kRenderTraceBlocks) k_trace_paths(RenderA
 // STD: the StandardSurface instance, over the StandardSurface class alone; the other
 // instance takes every other class
 template <int NL, bool STD = false>
-__global__ void __launch_bounds__(128) k_shade(RenderArgs A) {
+__global__ void FL_SHADE_BOUNDS k_shade(RenderArgs A) {
     __shared__ SmemTables sm;
     stage_tables(sm, A.tab, NL != 60);
     uint32_t off[kShadeClasses + 1];
@@ -999,7 +1016,7 @@ __global__ void __launch_bounds__(32 * kInferWarps, 3) k_guide_infer(RenderArgs 
 }
 
 template <int NL, bool GUIDE = false, bool STD = false>
-__global__ void __launch_bounds__(128) k_continue(RenderArgs A) {
+__global__ void FL_CONT_BOUNDS k_continue(RenderArgs A) {
     __shared__ SmemTables sm;
     stage_tables(sm, A.tab, NL != 60);
     const uint32_t n = load_count(STD ? &A.cnt->n_cont_std : &A.cnt->n_cont);

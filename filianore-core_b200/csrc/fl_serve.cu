@@ -181,8 +181,12 @@ void builder_loop(Server *S) {
         fl_status rc = FL_OK;
         if (!dev) {
             lock.unlock();
+            const auto b0 = std::chrono::steady_clock::now();
             rc = make_scene(S, *h, &dev);
+            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - b0).count();
             lock.lock();
+            S->stats.build_ms += ms;
+            S->stats.build_max_ms = std::max(S->stats.build_max_ms, ms);
         }
         it->second.dev = dev;
         if (rc == FL_OK) S->stats.builds++;
@@ -193,6 +197,7 @@ void builder_loop(Server *S) {
 }
 
 void finish_job(Server *S, uint64_t jid, HostJob &job) {
+    const auto f0 = std::chrono::steady_clock::now();
     const size_t n_pix = (size_t)job.cam.width * job.cam.height;
     k_resolve<<<(uint32_t)std::min<size_t>((n_pix + 255) / 256, (size_t)S->ctx->sm_count * 8), 256, 0, S->stream>>>(
         job.d_film, (uint32_t)n_pix, 1.0 / (double)job.params.spp, job.d_rgb);
@@ -208,6 +213,7 @@ void finish_job(Server *S, uint64_t jid, HostJob &job) {
     job.d_rgb = nullptr;
     job.status = e == cudaSuccess ? FL_OK : FL_ERR_CUDA;
     job.done_ms = S->now_ms();
+    S->stats.finish_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - f0).count();
     if (job.slot >= 0) S->free_slots.push_back(job.slot);
     job.slot = -1;
     S->stats.jobs_done++;
@@ -225,7 +231,9 @@ void worker_loop(Server *S) {
         {
             std::unique_lock<std::mutex> lock(S->mu);
             // with nothing to run (every running job waits for its scene) wait for news
+            const auto i0 = std::chrono::steady_clock::now();
             S->cv_work.wait(lock, [&] { return S->stop || S->events != seen || (progressed && !S->sched.idle()); });
+            S->stats.idle_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - i0).count();
             if (S->stop) break;
             seen = S->events;
             adm = S->sched.admit();
@@ -323,6 +331,7 @@ void worker_loop(Server *S) {
                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
                 std::lock_guard<std::mutex> lock(S->mu);
                 S->stats.busy_ms += wave_ms;
+                S->stats.wave_max_ms = std::max(S->stats.wave_max_ms, wave_ms);
                 S->stats.waves++;
                 S->stats.paths += d.n_wave;
                 if (e != cudaSuccess) S->error = cudaGetErrorString(e);

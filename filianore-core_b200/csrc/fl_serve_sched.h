@@ -75,6 +75,12 @@ public:
     // until then, while jobs whose scenes are ready keep the waves full. Without them a
     // resident scene is ready at once (the caller builds it before the next wave).
     void set_async_builds(bool on) { async_builds_ = on; }
+    // kFirstComeLane's lane (share of a wave) and the largest job it takes (in waves);
+    // 0 keeps the defaults (an eighth of the wave, for jobs that fit in it)
+    void set_lane(double share, double small_waves) {
+        lane_share_ = share;
+        lane_small_waves_ = small_waves;
+    }
     void scene_built(uint64_t id) {
         auto it = scenes_.find(id);
         if (it != scenes_.end() && it->second.resident) it->second.built = true;
@@ -180,9 +186,10 @@ public:
             }
             if (policy_ == kFirstComeLane) {
                 std::vector<std::pair<uint64_t, uint64_t>> small;
-                const uint64_t lane = cap / kLaneDivisor;
+                const uint64_t lane = lane_share_ > 0.0 ? (uint64_t)(lane_share_ * cap) : cap / kLaneDivisor;
+                const uint64_t small_max = lane_small_waves_ > 0.0 ? (uint64_t)(lane_small_waves_ * cap) : lane;
                 for (auto &w : want)
-                    if (w.first <= lane) small.push_back(w);
+                    if (w.first <= small_max) small.push_back(w);
                 std::stable_sort(small.begin(), small.end(),
                                  [](const std::pair<uint64_t, uint64_t> &a, const std::pair<uint64_t, uint64_t> &b) {
                                      return a.first < b.first;
@@ -319,6 +326,7 @@ private:
     uint64_t clock_ = 0;
     uint64_t waves_ = 0;
     bool async_builds_ = false;
+    double lane_share_ = 0.0, lane_small_waves_ = 0.0;
     std::map<uint64_t, SceneState> scenes_;
     std::map<uint64_t, JobState> jobs_;
     std::deque<uint64_t> pending_;

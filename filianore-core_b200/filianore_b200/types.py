@@ -226,6 +226,8 @@ class fl_server_stats(C.Structure):
         ("jobs_submitted", C.c_uint64), ("jobs_done", C.c_uint64), ("waves", C.c_uint64), ("paths", C.c_uint64),
         ("builds", C.c_uint64), ("evictions", C.c_uint64), ("resident_bytes", C.c_uint64),
         ("running", C.c_uint32), ("pending", C.c_uint32), ("busy_ms", C.c_double),
+        ("wave_max_ms", C.c_double), ("build_ms", C.c_double), ("build_max_ms", C.c_double),
+        ("finish_ms", C.c_double), ("idle_ms", C.c_double),
     ]
 
 

@@ -434,6 +434,10 @@ typedef struct {
     uint64_t jobs_submitted, jobs_done, waves, paths, builds, evictions, resident_bytes;
     uint32_t running, pending;
     double busy_ms;               /* host wall time of the waves (launch to completion) */
+    double wave_max_ms;           /* the longest wave */
+    double build_ms, build_max_ms; /* scene builds on the builder thread: total and longest */
+    double finish_ms;             /* resolving and copying out finished films (worker thread) */
+    double idle_ms;               /* worker time spent waiting for submissions or builds */
 } fl_server_stats;
 
 FL_API fl_status fl_server_create(fl_context *ctx, const fl_server_config *cfg, fl_server **out);
