@@ -234,7 +234,18 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
               "serial_tti_ms": [round(x * 1e3, 2) for x in serial_tti], "samples": [r * r * k for (_, r, k, _) in reqs],
               "tris": tris, "policies": {}}
 
+    def mem_available_kb():
+        try:
+            with open("/proc/meminfo") as f:
+                return int(next(l for l in f if l.startswith("MemAvailable")).split()[1])
+        except (OSError, StopIteration, ValueError):
+            return None
+
+    if args.serve_detail:
+        os.environ["FL_SERVE_TRACE"] = args.serve_detail + ".trace.csv"
+
     def run_server(name, policy):
+        mem0 = mem_available_kb()
         srv = fb.Server(ctx, budget_bytes=budget, max_depth=16, max_jobs=64, max_lights=4, policy=policy)
         job_ids = [None] * n_req
         submitted = [threading.Event() for _ in range(n_req)]
@@ -267,7 +278,8 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
         sstats = srv.stats()
         srv.close()
         detail["policies"][name] = {"tti_ms": [round(x * 1e3, 2) for x in tti], "late_ms": [round(x * 1e3, 2) for x in late],
-                                    "queued_ms": [round(st["start_ms"] - st["submit_ms"], 2) for _, _, st in rows]}
+                                    "queued_ms": [round(st["start_ms"] - st["submit_ms"], 2) for _, _, st in rows],
+                                    "mem_available_kb": [mem0, mem_available_kb()]}
         rows.sort(key=lambda r: -r[0])
         slowest = [{"req": i, "samples": st["samples"], "tris": tris[i], "res": reqs[i][1], "spp": reqs[i][2],
                     "queued_ms": round(st["start_ms"] - st["submit_ms"], 1), "tti_ms": round(t_ * 1e3, 1),

@@ -12,13 +12,17 @@
 //   3. uploads the job table and the wave's sample ranges and replays the wave as a CUDA
 //      graph captured once at start-up (the launch sequence never changes; the kernels
 //      read what to do from device memory);
-//   4. after the wave, resolves the films of jobs that are complete and copies them to the
-//      host, where fl_server_poll / fl_server_wait pick them up.
+//   4. after the wave, resolves the films of jobs that are complete and queues their copies
+//      to pinned host buffers; a read-out thread waits for each copy and marks the job done,
+//      so the worker goes on with the next wave meanwhile. fl_server_poll / fl_server_wait
+//      copy the films out of the pinned buffers.
 // Jobs that arrive while others run join at the next wave. Per-sample random streams depend
 // only on (pixel, sample index), so a job's image is the same alone and in any mix, up to
 // the order of the FP64 film additions.
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -54,12 +58,19 @@ struct HostJob {
     int slot = -1;
     double *d_film = nullptr;
     float *d_rgb = nullptr;
-    std::vector<float> rgb;
-    std::vector<double> xyz;
+    float *h_rgb = nullptr;    // pinned host copies of the finished films
+    double *h_xyz = nullptr;
     fl_status status = FL_ERR_NOT_READY;
     fl_status fail = FL_OK;  // set when admission could not give the job a film; reported when it completes
     bool bound = false;      // its job table entry points at its (built) scene
     double submit_ms = 0, start_ms = 0, done_ms = 0;
+};
+
+// A finished job whose film copies to pinned host memory are in flight.
+struct Readback {
+    uint64_t job;
+    cudaEvent_t done;  // recorded after the copies
+    double t0;         // when they were queued
 };
 
 // Work for the builder thread, done in order: build a scene, or release an evicted or
@@ -81,6 +92,8 @@ struct Server {
     Context *ctx = nullptr;
     fl_server_config cfg{};
     cudaStream_t stream = nullptr;
+    cudaStream_t rstream = nullptr;       // film read-outs
+    cudaEvent_t ev_resolved = nullptr;    // a finished film is resolved (read-outs wait on it)
     void *wave_mem = nullptr;
     size_t wave_bytes = 0;
     WaveBuffers W{};
@@ -96,6 +109,23 @@ struct Server {
     std::thread builder;
     std::deque<BuildTask> build_q;
     std::condition_variable cv_build;
+    std::thread reader;
+    std::deque<Readback> read_q;
+    std::condition_variable cv_read;
+    std::vector<cudaEvent_t> free_events;
+    // pinned host buffers for finished films, kept by size for the next jobs
+    std::multimap<size_t, void *> pinned_pool;
+    // FL_SERVE_TRACE=<file>: one line per wave, build and film read-out, appended at destroy
+    bool tracing = false;
+    std::string trace_path;
+    std::vector<std::string> trace;
+    void trace_event(const char *kind, double t0, double ms, uint64_t id, uint64_t n) {
+        if (!tracing) return;
+        char b[160];
+        std::snprintf(b, sizeof(b), "%s,%.3f,%.3f,%llu,%llu", kind, t0, ms, (unsigned long long)id,
+                      (unsigned long long)n);
+        trace.emplace_back(b);
+    }
     ServeScheduler sched;
     std::map<uint64_t, HostScene> scenes;
     std::map<uint64_t, std::unique_ptr<HostJob>> jobs;
@@ -125,6 +155,25 @@ struct Server {
         if (!p) return;
         if (buffer_pool.count(bytes) < 8) buffer_pool.insert({bytes, p});
         else cudaFree(p);
+    }
+    void *acquire_pinned(size_t bytes) {
+        auto it = pinned_pool.find(bytes);
+        if (it != pinned_pool.end()) {
+            void *p = it->second;
+            pinned_pool.erase(it);
+            return p;
+        }
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return p;
+    }
+    void release_pinned(void *p, size_t bytes) {
+        if (!p) return;
+        if (pinned_pool.count(bytes) < 8) pinned_pool.insert({bytes, p});
+        else cudaFreeHost(p);
     }
 
     Server(uint64_t budget, int max_jobs, int policy) : sched(budget, max_jobs, policy) {
@@ -181,12 +230,13 @@ void builder_loop(Server *S) {
         fl_status rc = FL_OK;
         if (!dev) {
             lock.unlock();
-            const auto b0 = std::chrono::steady_clock::now();
+            const double b0 = S->now_ms();
             rc = make_scene(S, *h, &dev);
-            const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - b0).count();
+            const double ms = S->now_ms() - b0;
             lock.lock();
             S->stats.build_ms += ms;
             S->stats.build_max_ms = std::max(S->stats.build_max_ms, ms);
+            S->trace_event("build", b0, ms, t.scene, h->verts.size() / 9);
         }
         it->second.dev = dev;
         if (rc == FL_OK) S->stats.builds++;
@@ -196,28 +246,79 @@ void builder_loop(Server *S) {
     }
 }
 
+// Resolves a finished job's film and queues its copies to pinned host memory; the read-out
+// thread completes the job when they have arrived. Called by the worker without the lock.
 void finish_job(Server *S, uint64_t jid, HostJob &job) {
-    const auto f0 = std::chrono::steady_clock::now();
+    const double t0 = S->now_ms();
     const size_t n_pix = (size_t)job.cam.width * job.cam.height;
     k_resolve<<<(uint32_t)std::min<size_t>((n_pix + 255) / 256, (size_t)S->ctx->sm_count * 8), 256, 0, S->stream>>>(
         job.d_film, (uint32_t)n_pix, 1.0 / (double)job.params.spp, job.d_rgb);
-    job.rgb.resize(n_pix * 3);
-    job.xyz.resize(n_pix * 3);
-    cudaMemcpyAsync(job.rgb.data(), job.d_rgb, n_pix * 3 * sizeof(float), cudaMemcpyDeviceToHost, S->stream);
-    cudaMemcpyAsync(job.xyz.data(), job.d_film, n_pix * 3 * sizeof(double), cudaMemcpyDeviceToHost, S->stream);
-    cudaError_t e = cudaStreamSynchronize(S->stream);
+    // the copies run on the read-out stream, after the resolve, while the next waves run
+    cudaEvent_t ev = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(S->mu);
+        job.h_rgb = static_cast<float *>(S->acquire_pinned(n_pix * 3 * sizeof(float)));
+        job.h_xyz = static_cast<double *>(S->acquire_pinned(n_pix * 3 * sizeof(double)));
+        if (!S->free_events.empty()) {
+            ev = S->free_events.back();
+            S->free_events.pop_back();
+        }
+    }
+    cudaError_t e = job.h_rgb && job.h_xyz ? cudaSuccess : cudaErrorMemoryAllocation;
+    if (e == cudaSuccess && !ev) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(S->ev_resolved, S->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(S->rstream, S->ev_resolved, 0);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(job.h_rgb, job.d_rgb, n_pix * 3 * sizeof(float), cudaMemcpyDeviceToHost, S->rstream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(job.h_xyz, job.d_film, n_pix * 3 * sizeof(double), cudaMemcpyDeviceToHost, S->rstream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, S->rstream);
     std::lock_guard<std::mutex> lock(S->mu);
-    S->release(job.d_film, n_pix * 3 * sizeof(double));
-    S->release(job.d_rgb, n_pix * 3 * sizeof(float));
-    job.d_film = nullptr;
-    job.d_rgb = nullptr;
-    job.status = e == cudaSuccess ? FL_OK : FL_ERR_CUDA;
-    job.done_ms = S->now_ms();
-    S->stats.finish_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - f0).count();
-    if (job.slot >= 0) S->free_slots.push_back(job.slot);
+    if (job.slot >= 0) S->free_slots.push_back(job.slot);  // no later wave uses its table entry
     job.slot = -1;
-    S->stats.jobs_done++;
-    (void)jid;
+    if (e == cudaSuccess) {
+        S->read_q.push_back(Readback{jid, ev, t0});
+        S->cv_read.notify_one();
+    } else {
+        cudaGetLastError();
+        if (ev) S->free_events.push_back(ev);
+        S->release(job.d_film, n_pix * 3 * sizeof(double));
+        S->release(job.d_rgb, n_pix * 3 * sizeof(float));
+        job.d_film = nullptr;
+        job.d_rgb = nullptr;
+        job.status = e == cudaErrorMemoryAllocation ? FL_ERR_OOM : FL_ERR_CUDA;
+        job.done_ms = S->now_ms();
+        S->stats.jobs_done++;
+        S->cv_done.notify_all();
+    }
+    S->stats.finish_ms += S->now_ms() - t0;
+}
+
+// Waits for the queued film copies in order and completes their jobs.
+void reader_loop(Server *S) {
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lock(S->mu);
+    while (true) {
+        S->cv_read.wait(lock, [&] { return S->stop || !S->read_q.empty(); });
+        if (S->read_q.empty()) break;  // stopping, with nothing in flight
+        const Readback r = S->read_q.front();
+        S->read_q.pop_front();
+        lock.unlock();
+        const cudaError_t e = cudaEventSynchronize(r.done);
+        lock.lock();
+        S->free_events.push_back(r.done);
+        HostJob &job = *S->jobs[r.job];
+        const size_t n_pix = (size_t)job.cam.width * job.cam.height;
+        S->release(job.d_film, n_pix * 3 * sizeof(double));
+        S->release(job.d_rgb, n_pix * 3 * sizeof(float));
+        job.d_film = nullptr;
+        job.d_rgb = nullptr;
+        job.status = e == cudaSuccess ? FL_OK : FL_ERR_CUDA;
+        job.done_ms = S->now_ms();
+        S->stats.jobs_done++;
+        S->trace_event("readout", r.t0, job.done_ms - r.t0, r.job, n_pix);
+        S->cv_done.notify_all();
+    }
 }
 
 void worker_loop(Server *S) {
@@ -316,6 +417,7 @@ void worker_loop(Server *S) {
                 cudaMemcpyAsync(S->W.d_wave, &d, desc_head + sizeof(WaveSeg) * d.n_seg, cudaMemcpyHostToDevice,
                                 S->stream);
                 const auto w0 = std::chrono::steady_clock::now();
+                const double w0_ms = S->now_ms();
                 cudaGraphLaunch(S->graph, S->stream);
                 cudaError_t e = cudaStreamSynchronize(S->stream);
                 // jobs with unequal lobe depths may have paths alive past the wave's bounces
@@ -332,6 +434,7 @@ void worker_loop(Server *S) {
                 std::lock_guard<std::mutex> lock(S->mu);
                 S->stats.busy_ms += wave_ms;
                 S->stats.wave_max_ms = std::max(S->stats.wave_max_ms, wave_ms);
+                S->trace_event("wave", w0_ms, wave_ms, d.n_seg, d.n_wave);
                 S->stats.waves++;
                 S->stats.paths += d.n_wave;
                 if (e != cudaSuccess) S->error = cudaGetErrorString(e);
@@ -355,6 +458,7 @@ void worker_loop(Server *S) {
                 job->status = job->fail != FL_OK ? job->fail : FL_ERR_OOM;
                 if (job->slot >= 0) S->free_slots.push_back(job->slot);
                 job->slot = -1;
+                S->stats.jobs_done++;
             }
         }
         if (!done.empty()) {
@@ -403,20 +507,42 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     S->ctx = ctx;
     S->cfg = *cfg;
     S->t0 = std::chrono::steady_clock::now();
+    if (const char *tp = std::getenv("FL_SERVE_TRACE")) {
+        S->tracing = tp[0] != 0;
+        S->trace_path = tp;
+    }
     FL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    // scene memory the budget allows stays cached in the context's pool between builds
+    if (ctx->pool) {
+        uint64_t cur = 0, keep = std::max<uint64_t>(kPoolKeepBytes, cfg->memory_budget_bytes);
+        if (cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && keep > cur)
+            cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     FL_CUDA_TRY(ctx, cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    cudaError_t es = cudaStreamCreateWithFlags(&S->rstream, cudaStreamNonBlocking);
+    if (es == cudaSuccess) es = cudaEventCreateWithFlags(&S->ev_resolved, cudaEventDisableTiming);
+    if (es != cudaSuccess) {
+        if (S->rstream) cudaStreamDestroy(S->rstream);
+        cudaStreamDestroy(S->stream);
+        return cuda_status(ctx, es, "server streams");
+    }
+    auto drop_streams = [&] {
+        cudaEventDestroy(S->ev_resolved);
+        cudaStreamDestroy(S->rstream);
+        cudaStreamDestroy(S->stream);
+    };
     const size_t cap = cfg->wave_paths > 0 ? (size_t)cfg->wave_paths : ((size_t)1 << 21);
     const size_t per_slot = wave_bytes_per_slot(4, cfg->max_lights);
     S->wave_bytes = cap * per_slot + (1 << 20);
     cudaError_t e = cudaMalloc(&S->wave_mem, S->wave_bytes);
     if (e != cudaSuccess) {
-        cudaStreamDestroy(S->stream);
+        drop_streams();
         return cuda_status(ctx, e, "server wave buffers");
     }
     fl_status rc = wave_buffers(ctx, 4, cfg->max_lights, cap, S->wave_mem, S->wave_bytes, S->W);
     if (rc) {
         cudaFree(S->wave_mem);
-        cudaStreamDestroy(S->stream);
+        drop_streams();
         return rc;
     }
     S->table.assign(kMaxJobs, JobDev{});
@@ -435,7 +561,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     if (g) cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         cudaFree(S->wave_mem);
-        cudaStreamDestroy(S->stream);
+        drop_streams();
         return cuda_status(ctx, e, "wave graph capture");
     }
     cudaStreamSynchronize(S->stream);
@@ -443,6 +569,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     ctx->children++;
     raw->worker = std::thread(worker_loop, raw);
     raw->builder = std::thread(builder_loop, raw);
+    raw->reader = std::thread(reader_loop, raw);
     *out = reinterpret_cast<fl_server *>(raw);
     return FL_OK;
 }
@@ -458,6 +585,15 @@ fl_status fl_server_destroy(fl_server *srv) {
     S->cv_build.notify_all();
     if (S->worker.joinable()) S->worker.join();
     if (S->builder.joinable()) S->builder.join();
+    S->cv_read.notify_all();
+    if (S->reader.joinable()) S->reader.join();  // finishes the read-outs in flight
+    if (S->tracing) {
+        if (FILE *f = std::fopen(S->trace_path.c_str(), "a")) {
+            std::fprintf(f, "# server policy %d\n", S->cfg.policy);
+            for (const auto &l : S->trace) std::fprintf(f, "%s\n", l.c_str());
+            std::fclose(f);
+        }
+    }
     cudaSetDevice(S->ctx->device);
     cudaStreamSynchronize(S->stream);
     for (const BuildTask &t : S->build_q)
@@ -465,12 +601,19 @@ fl_status fl_server_destroy(fl_server *srv) {
     for (auto &kv : S->jobs) {
         cudaFree(kv.second->d_film);
         cudaFree(kv.second->d_rgb);
+        cudaFreeHost(kv.second->h_rgb);
+        cudaFreeHost(kv.second->h_xyz);
     }
     for (auto &kv : S->buffer_pool) cudaFree(kv.second);
+    for (auto &kv : S->pinned_pool) cudaFreeHost(kv.second);
+    for (cudaEvent_t e : S->free_events) cudaEventDestroy(e);
     for (auto &kv : S->scenes)
         if (kv.second.dev) fl_scene_destroy(reinterpret_cast<fl_scene *>(kv.second.dev));
     if (S->graph) cudaGraphExecDestroy(S->graph);
     cudaFree(S->wave_mem);
+    cudaStreamSynchronize(S->rstream);
+    cudaEventDestroy(S->ev_resolved);
+    cudaStreamDestroy(S->rstream);
     cudaStreamDestroy(S->stream);
     S->ctx->children--;
     delete S;
@@ -581,10 +724,13 @@ static fl_status collect(Server *S, uint64_t job_id, float *film_rgb, double *fi
         st->samples = (uint64_t)j.cam.width * j.cam.height * (uint64_t)j.params.spp;
     }
     const fl_status rc = j.status;
+    const size_t n_pix = (size_t)j.cam.width * j.cam.height;
     if (rc == FL_OK) {
-        if (film_rgb) std::memcpy(film_rgb, j.rgb.data(), j.rgb.size() * sizeof(float));
-        if (film_xyz64) std::memcpy(film_xyz64, j.xyz.data(), j.xyz.size() * sizeof(double));
+        if (film_rgb) std::memcpy(film_rgb, j.h_rgb, n_pix * 3 * sizeof(float));
+        if (film_xyz64) std::memcpy(film_xyz64, j.h_xyz, n_pix * 3 * sizeof(double));
     }
+    S->release_pinned(j.h_rgb, n_pix * 3 * sizeof(float));
+    S->release_pinned(j.h_xyz, n_pix * 3 * sizeof(double));
     S->jobs.erase(it);  // results are handed out once
     return rc;
 }
