@@ -52,7 +52,11 @@ struct WaveCounters {
     unsigned long long nodes, tris;  // FL_RENDER_COUNT
     int err;
     uint32_t cut;                    // paths ended at the job's bounce cap
-    int pad[2];
+    // streaming waves (path regeneration): free path slots, paths of the wave started so
+    // far, and this iteration's new paths (the regen_n lowest free slots take wave paths
+    // regen_base, +regen_n and are queued at q_trace[regen_dst, +regen_n))
+    uint32_t n_free, next_path;
+    uint32_t regen_n, regen_dst, regen_base, pad3;
 };
 
 // FL_RENDER_PROFILE: CUDA events bracketing every launch, grouped by kernel class. The
@@ -188,6 +192,10 @@ struct RenderArgs {
     // queues
     uint32_t *q_trace, *q_cont, *q_next;
     uint32_t *q_class;  // kShadeClasses x cap: traced paths grouped by what shades them
+    // streaming waves (null for fixed waves): 1 marks a slot whose path has ended, and per
+    // chunk of kFreeChunk slots their count and the exclusive prefix of the counts
+    uint8_t *slot_free;
+    uint32_t *free_count, *free_off;
     WaveCounters *cnt;
     GuideArgs g;        // learned guiding (zero when off)
 };
@@ -278,6 +286,7 @@ __device__ inline void finish_path(const RenderArgs &A, const JobDev &J, const S
     double xyz[3];
     spectrum_xyz<NL>(sm, A.tab, A.head[slot].lambda0, L, xyz);
     const uint32_t pix = A.head[slot].pixel;
+    if (A.slot_free) A.slot_free[slot] = 1;  // streaming: the slot takes a new path
     atomicAdd(&J.film[3 * (size_t)pix + 0], xyz[0]);
     atomicAdd(&J.film[3 * (size_t)pix + 1], xyz[1]);
     atomicAdd(&J.film[3 * (size_t)pix + 2], xyz[2]);
@@ -479,77 +488,23 @@ __device__ inline void make_bsdf(const JobDev &A, const TablesArg &tab, const Sm
 
 // ------------------------------------------------------------------------------ kernels
 
+// Starts path q of the wave (its segment gives the job and the sample index) in slot k: the
+// camera ray (or fl_li's ray) and the initial path state. The caller queues the slot.
 template <int NL>
-__global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
-    const uint32_t n_wave = A.wave->n_wave;
+__device__ inline void init_path(const RenderArgs &A, uint32_t k, uint32_t q) {
     const uint32_t n_seg = A.wave->n_seg;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        A.cnt->n_trace = n_wave;
-        A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = A.cnt->n_cont_std = 0;
-        A.cnt->fetch_trace = A.cnt->fetch_rays2 = 0;
-        for (int c = 0; c < kShadeClasses; ++c) A.cnt->n_class[c] = 0;
-    }
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_wave; k += gridDim.x * blockDim.x) {
-        uint32_t si = 0;
-        while (si + 1 < n_seg && k >= A.wave->seg[si + 1].slot_begin) ++si;
-        const WaveSeg sg = A.wave->seg[si];
-        const JobDev &J = A.jobs[sg.job];
-        const unsigned long long g = sg.sample_base + (k - sg.slot_begin);
-        const uint32_t pix = (uint32_t)(g % J.n_pix);
-        const unsigned long long s = g / J.n_pix;
-        if (J.li.org) {
-            // fl_li: the caller's ray, generator state and wavelength
-            PathHead ph;
-            ph.rng = J.li.rng[pix];
-            ph.lambda0 = J.li.lambda0 ? J.li.lambda0[pix] : 380.f;
-            ph.flags = 0u;
-            ph.pixel = pix;
-            ph.job = sg.job;
-            ph.eta_scale = 1.f;
-            ph.pad = 0u;
-            A.head[k] = ph;
-            Spec<NL> one, zero;
-            one.set(1.f);
-            zero.set(0.f);
-            store_spec<NL>(A.beta, A.cap, k, one);
-            store_spec<NL>(A.L, A.cap, k, zero);
-            A.ray_o[k] = J.li.org[pix];
-            A.ray_d[k] = J.li.dir[pix];
-            A.q_trace[k] = k;
-            if (A.g.rec_idx) {
-                A.g.rec_idx[k] = kNoRecord;
-                A.g.rec_idx[(size_t)A.cap + k] = kNoRecord;
-            }
-            continue;
-        }
-        Pcg32 rng;
-        rng.seed(pix, 1u);
-        const unsigned long long sidx = (unsigned long long)J.sample_offset + s;
-        if (sidx) rng.advance(sidx << 16);
-        const float ux = rng.nextf(), uy = rng.nextf(), ul = rng.nextf();
-        const uint32_t px = pix % (uint32_t)J.cam.W, py = pix / (uint32_t)J.cam.W;
-        const float sx = __fdiv_rn(__fadd_rn((float)px, ux), (float)J.cam.W);
-        const float sy = __fdiv_rn(__fadd_rn((float)((uint32_t)J.cam.H - 1u - py), uy), (float)J.cam.H);
-        // PhysicalCamera::awaken_ray (cameras/physical.cpp:12-22): a pinhole takes the lens
-        // sample (0.5, 0.5); a lens draws two numbers and maps them with the concentric disk
-        v3 rd;
-        if (J.cam.lens_radius > 0.f) {
-            const float lx = rng.nextf(), ly = rng.nextf();
-            const v3 lp = concentric_disk(lx, ly);
-            rd = mul(lp, J.cam.lens_radius);
-        } else {
-            const v3 lp = sub(mul(mk(0.5f, 0.5f, 0.f), 2.f), mk(1.f, 1.f, 0.f));
-            rd = mul(lp, 0.f);
-        }
-        const v3 offset = add(mul(J.cam.u, rd.x), mul(J.cam.v, rd.y));
-        const v3 o = add(J.cam.origin, offset);
-        const v3 dir = sub(sub(add(add(J.cam.lower_left, mul(J.cam.horizontal, sx)), mul(J.cam.vertical, sy)),
-                               J.cam.origin),
-                           offset);
-        const v3 d = normalize(dir);
+    uint32_t si = 0;
+    while (si + 1 < n_seg && q >= A.wave->seg[si + 1].slot_begin) ++si;
+    const WaveSeg sg = A.wave->seg[si];
+    const JobDev &J = A.jobs[sg.job];
+    const unsigned long long g = sg.sample_base + (q - sg.slot_begin);
+    const uint32_t pix = (uint32_t)(g % J.n_pix);
+    const unsigned long long s = g / J.n_pix;
+    if (J.li.org) {
+        // fl_li: the caller's ray, generator state and wavelength
         PathHead ph;
-        ph.rng = rng.state;
-        ph.lambda0 = __fadd_rn(380.f, __fmul_rn(ul, 340.f));  // not contracted: the oracle rounds twice
+        ph.rng = J.li.rng[pix];
+        ph.lambda0 = J.li.lambda0 ? J.li.lambda0[pix] : 380.f;
         ph.flags = 0u;
         ph.pixel = pix;
         ph.job = sg.job;
@@ -561,15 +516,222 @@ __global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
         zero.set(0.f);
         store_spec<NL>(A.beta, A.cap, k, one);
         store_spec<NL>(A.L, A.cap, k, zero);
-        A.ray_o[k] = make_float4(o.x, o.y, o.z, 0.f);
-        A.ray_d[k] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
-        A.q_trace[k] = k;
+        A.ray_o[k] = J.li.org[pix];
+        A.ray_d[k] = J.li.dir[pix];
         if (A.g.rec_idx) {
             A.g.rec_idx[k] = kNoRecord;
             A.g.rec_idx[(size_t)A.cap + k] = kNoRecord;
         }
+        return;
+    }
+    Pcg32 rng;
+    rng.seed(pix, 1u);
+    const unsigned long long sidx = (unsigned long long)J.sample_offset + s;
+    if (sidx) rng.advance(sidx << 16);
+    const float ux = rng.nextf(), uy = rng.nextf(), ul = rng.nextf();
+    const uint32_t px = pix % (uint32_t)J.cam.W, py = pix / (uint32_t)J.cam.W;
+    const float sx = __fdiv_rn(__fadd_rn((float)px, ux), (float)J.cam.W);
+    const float sy = __fdiv_rn(__fadd_rn((float)((uint32_t)J.cam.H - 1u - py), uy), (float)J.cam.H);
+    // PhysicalCamera::awaken_ray (cameras/physical.cpp:12-22): a pinhole takes the lens
+    // sample (0.5, 0.5); a lens draws two numbers and maps them with the concentric disk
+    v3 rd;
+    if (J.cam.lens_radius > 0.f) {
+        const float lx = rng.nextf(), ly = rng.nextf();
+        const v3 lp = concentric_disk(lx, ly);
+        rd = mul(lp, J.cam.lens_radius);
+    } else {
+        const v3 lp = sub(mul(mk(0.5f, 0.5f, 0.f), 2.f), mk(1.f, 1.f, 0.f));
+        rd = mul(lp, 0.f);
+    }
+    const v3 offset = add(mul(J.cam.u, rd.x), mul(J.cam.v, rd.y));
+    const v3 o = add(J.cam.origin, offset);
+    const v3 dir = sub(sub(add(add(J.cam.lower_left, mul(J.cam.horizontal, sx)), mul(J.cam.vertical, sy)),
+                           J.cam.origin),
+                       offset);
+    const v3 d = normalize(dir);
+    PathHead ph;
+    ph.rng = rng.state;
+    ph.lambda0 = __fadd_rn(380.f, __fmul_rn(ul, 340.f));  // not contracted: the oracle rounds twice
+    ph.flags = 0u;
+    ph.pixel = pix;
+    ph.job = sg.job;
+    ph.eta_scale = 1.f;
+    ph.pad = 0u;
+    A.head[k] = ph;
+    Spec<NL> one, zero;
+    one.set(1.f);
+    zero.set(0.f);
+    store_spec<NL>(A.beta, A.cap, k, one);
+    store_spec<NL>(A.L, A.cap, k, zero);
+    A.ray_o[k] = make_float4(o.x, o.y, o.z, 0.f);
+    A.ray_d[k] = make_float4(d.x, d.y, d.z, __int_as_float(0x7f800000));
+    if (A.g.rec_idx) {
+        A.g.rec_idx[k] = kNoRecord;
+        A.g.rec_idx[(size_t)A.cap + k] = kNoRecord;
+    }
+}
+
+template <int NL>
+__global__ void __launch_bounds__(128) k_raygen(RenderArgs A) {
+    const uint32_t n_wave = A.wave->n_wave;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        A.cnt->n_trace = n_wave;
+        A.cnt->n_cont = A.cnt->n_next = A.cnt->n_shadow = A.cnt->n_cont_std = 0;
+        A.cnt->fetch_trace = A.cnt->fetch_rays2 = 0;
+        for (int c = 0; c < kShadeClasses; ++c) A.cnt->n_class[c] = 0;
+    }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_wave; k += gridDim.x * blockDim.x) {
+        init_path<NL>(A, k, k);
+        A.q_trace[k] = k;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.cnt->paths, (unsigned long long)n_wave);
+}
+
+// Streaming waves (path regeneration). The wave descriptor lists more paths than there are
+// slots; a path that ends frees its slot (finish_path), and every iteration starts as many
+// new paths as there are free slots, so the late bounces of early paths run alongside the
+// first bounces of later ones and the slots stay full until the descriptor's paths run out.
+// New paths take the lowest free slots in slot order, so the paths started together sit in
+// neighbouring slots and the kernels read and write their state in whole sectors.
+constexpr uint32_t kFreeChunk = 4096;      // slots per block of the free-slot scan
+constexpr uint32_t kMaxFreeChunks = 8192;  // covers kMaxWaveSlots
+__host__ __device__ inline uint32_t free_chunks(size_t cap) { return (uint32_t)((cap + kFreeChunk - 1) / kFreeChunk); }
+
+static __global__ void __launch_bounds__(128) k_stream_init(RenderArgs A) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < A.cap; i += gridDim.x * blockDim.x)
+        A.slot_free[i] = 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        WaveCounters *c = A.cnt;
+        c->n_free = A.cap;
+        c->next_path = 0;
+        c->n_next = 0;
+        c->n_trace = 0;
+        c->regen_n = c->regen_dst = c->regen_base = 0;
+    }
+}
+
+// Free slots per chunk (one block of 256 threads per chunk, 16 flags per thread).
+static __global__ void __launch_bounds__(256) k_free_count(RenderArgs A) {
+    const uint32_t c0 = blockIdx.x * kFreeChunk;
+    uint32_t n = 0;
+    for (uint32_t i = c0 + threadIdx.x; i < min(c0 + kFreeChunk, A.cap); i += 256) n += A.slot_free[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    __shared__ uint32_t w[8];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int k = 0; k < 8; ++k) t += w[k];
+        A.free_count[blockIdx.x] = t;
+    }
+}
+
+// Iteration start (one block of 1024 threads): the prefix of the chunk counts, then the
+// survivors of the last iteration head this iteration's trace queue and new paths follow.
+static __global__ void __launch_bounds__(1024) k_stream_step(RenderArgs A) {
+    const uint32_t nc = free_chunks(A.cap);
+    constexpr int kPer = kMaxFreeChunks / 1024;
+    uint32_t v[kPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const uint32_t i = threadIdx.x * kPer + k;
+        v[k] = i < nc ? A.free_count[i] : 0u;
+        sum += v[k];
+    }
+    // exclusive scan of the per-thread sums over the block
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    __shared__ uint32_t wsum[32];
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t x = wsum[lane], xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= o) xi += y;
+        }
+        wsum[lane] = xi - x;  // exclusive prefix of the warp sums
+    }
+    __syncthreads();
+    uint32_t run = wsum[warp] + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const uint32_t i = threadIdx.x * kPer + k;
+        if (i < nc) A.free_off[i] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 1023) {
+        WaveCounters *c = A.cnt;
+        const uint32_t n_free = run;  // the total
+        // every slot is free or holds a survivor (checked, so that a broken count can only
+        // stop the wave early, never index outside the buffers)
+        uint32_t surv = c->n_next;
+        uint32_t avail = n_free;
+        if (surv > A.cap || avail > A.cap - surv) {
+            c->err += 1;
+            surv = min(surv, A.cap);
+            avail = min(avail, A.cap - surv);
+        }
+        const uint32_t n_wave = A.wave->n_wave;
+        const uint32_t remaining = n_wave > c->next_path ? n_wave - c->next_path : 0u;
+        const uint32_t nn = min(avail, remaining);
+        c->n_free = n_free;
+        c->regen_n = nn;
+        c->regen_dst = surv;
+        c->regen_base = c->next_path;
+        c->next_path += nn;
+        c->n_trace = surv + nn;
+        c->n_next = 0;
+        c->n_cont = 0;
+        c->n_cont_std = 0;
+        c->n_shadow = 0;
+        c->fetch_trace = 0;
+        c->fetch_rays2 = 0;
+        for (int k = 0; k < kShadeClasses; ++k) c->n_class[k] = 0;
+    }
+}
+
+// New paths into the regen_n lowest free slots (one block of 256 threads per chunk): the
+// r-th free slot of the wave starts path regen_base + r and is queued at regen_dst + r.
+template <int NL>
+__global__ void __launch_bounds__(256) k_regen(RenderArgs A) {
+    const uint32_t nn = load_count(&A.cnt->regen_n);
+    const uint32_t off = A.free_off[blockIdx.x];
+    if (off >= nn) return;  // every free slot of this chunk stays free
+    const uint32_t dst = A.cnt->regen_dst, base = A.cnt->regen_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ uint32_t wcnt[8];
+    uint32_t rank0 = off;  // rank of the first free slot of this round
+    const uint32_t c0 = blockIdx.x * kFreeChunk, c1 = min(c0 + kFreeChunk, A.cap);
+    for (uint32_t r0 = c0; r0 < c1 && rank0 < nn; r0 += 256) {
+        const uint32_t slot = r0 + threadIdx.x;
+        const bool fr = slot < c1 && A.slot_free[slot] != 0;
+        const uint32_t m = __ballot_sync(0xffffffffu, fr);
+        if (lane == 0) wcnt[warp] = __popc(m);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            before += k < warp ? wcnt[k] : 0u;
+            total += wcnt[k];
+        }
+        const uint32_t rank = rank0 + before + __popc(m & ((1u << lane) - 1u));
+        if (fr && rank < nn) {
+            A.slot_free[slot] = 0;
+            init_path<NL>(A, slot, base + rank);
+            A.q_trace[dst + rank] = slot;
+        }
+        rank0 += total;
+        __syncthreads();  // wcnt is reused
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && nn) atomicAdd(&A.cnt->paths, (unsigned long long)nn);
 }
 
 static __global__ void __launch_bounds__(128) k_advance(WaveCounters *cnt) {
@@ -1177,14 +1339,28 @@ static __global__ void k_resolve(const double *__restrict__ film, uint32_t n_pix
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // bytes of wave state per path slot
+// Iterations per graph replay of a streaming wave, and the most paths one descriptor lists.
+constexpr int kStreamIters = 8;
+constexpr unsigned long long kStreamDescPaths = 1ull << 31;
+// Default paths per wave. A wave runs every bounce up to the deepest depth, and its late
+// bounces hold few paths (their launches cost about the same as full ones), so large waves
+// amortise that tail: the 1,048,578-triangle procedural frame (1920x1080, 64 spp, depth 16)
+// measured 915 Mrays/s with waves of 2^21 paths, 1,209 with 2^22 and 1,424 with 2^23.
+constexpr size_t kWavePathsHero = (size_t)1 << 23;
+constexpr size_t kWavePathsBins60 = (size_t)1 << 21;
+// The wave state of a render lives in the context scratch, at most this many bytes.
+constexpr size_t kWaveScratchBytes = (size_t)16 << 30;
 inline size_t wave_bytes_per_slot(int NL, int nl) {
-    return 100 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
+    return 101 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
 }
 
 // The device buffers of a wavefront: job table, wave descriptor, path state and queues.
 struct WaveBuffers {
     RenderArgs A;
     uint32_t *qa, *qb;
+    // streaming waves set A.slot_free / free_count / free_off to these
+    uint8_t *slot_free;
+    uint32_t *free_count, *free_off;
     JobDev *d_jobs;
     WaveDesc *d_wave;
     size_t cap;
@@ -1196,7 +1372,7 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
                               WaveBuffers &W) {
     const size_t per_slot = wave_bytes_per_slot(NL, nl);
     const size_t head = align_up(sizeof(WaveCounters)) + align_up(sizeof(JobDev) * kMaxJobs) + align_up(sizeof(WaveDesc));
-    const size_t budget = fixed ? fixed_bytes : (size_t)3 << 30;
+    const size_t budget = fixed ? fixed_bytes : kWaveScratchBytes;
     if (budget < head + 32 * 256 + 128 * per_slot) {
         set_error(ctx, "render state does not fit the fixed scratch buffer");
         return FL_ERR_CAPACITY;
@@ -1219,6 +1395,7 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
     const size_t o_so = take(16 * scap), o_sd = take(16 * scap), o_st = take(4 * scap);
     const size_t o_qa = take(4 * cap), o_qb = take(4 * cap), o_qc = take(4 * cap);
     const size_t o_qk = take(4 * cap * kShadeClasses);
+    const size_t o_free = take(cap), o_fc = take(4 * (size_t)free_chunks(cap)), o_fo = take(4 * (size_t)free_chunks(cap));
     void *base = fixed;
     if (!fixed) {
         fl_status rc = ensure_scratch(ctx, off, &base);
@@ -1255,6 +1432,9 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
     A.stag = reinterpret_cast<uint32_t *>(B + o_st);
     A.q_cont = reinterpret_cast<uint32_t *>(B + o_qc);
     A.q_class = reinterpret_cast<uint32_t *>(B + o_qk);
+    W.slot_free = reinterpret_cast<uint8_t *>(B + o_free);
+    W.free_count = reinterpret_cast<uint32_t *>(B + o_fc);
+    W.free_off = reinterpret_cast<uint32_t *>(B + o_fo);
     W.qa = reinterpret_cast<uint32_t *>(B + o_qa);
     W.qb = reinterpret_cast<uint32_t *>(B + o_qb);
     W.cap = cap;
@@ -1266,13 +1446,20 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
 // depend on the wave's content (kernels read their counts from device memory).
 template <int NL, bool GUIDE = false>
 void enqueue_bounces(const WaveBuffers &W, int b_begin, int b_end, bool count, RenderProfile *prof, int sms,
-                     cudaStream_t st, bool standard) {
+                     cudaStream_t st, bool standard, bool stream = false) {
     RenderArgs A = W.A;
     const int g_trace = sms * 16, g_shade = sms * 8;
     for (int b = b_begin; b < b_end; ++b) {
         A.q_trace = (b & 1) ? W.qb : W.qa;
         A.q_next = (b & 1) ? W.qa : W.qb;
-        if (b > 0) {
+        if (stream) {
+            // streaming: survivors plus new paths in the lowest free slots
+            const uint32_t nc = free_chunks(A.cap);
+            k_free_count<<<nc, 256, 0, st>>>(A);
+            k_stream_step<<<1, 1024, 0, st>>>(A);
+            k_regen<NL><<<nc, 256, 0, st>>>(A);
+            prof->launches += 3;
+        } else if (b > 0) {
             k_advance<<<1, 1, 0, st>>>(A.cnt);
             prof->launches += 1;
         }
@@ -1393,7 +1580,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     Context *ctx = s->ctx;
     const unsigned long long n_pix = (unsigned long long)cam.W * (unsigned long long)cam.H;
     const unsigned long long total = n_pix * (unsigned long long)p.spp;
-    size_t cap_req = p.wave_paths > 0 ? (size_t)p.wave_paths : (NL == 60 ? (size_t)1 << 19 : (size_t)1 << 21);
+    size_t cap_req = p.wave_paths > 0 ? (size_t)p.wave_paths : (NL == 60 ? kWavePathsBins60 : kWavePathsHero);
     cap_req = std::min<size_t>(cap_req, (size_t)total);
     WaveBuffers W;
     fl_status rc = wave_buffers(ctx, NL, (int)s->n_lights, cap_req, fixed_scratch, fixed_bytes, W);
@@ -1407,15 +1594,20 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     const bool standard = s->ext_kernels;
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
     const size_t desc_bytes = offsetof(WaveDesc, seg) + sizeof(WaveSeg);
-    const int depth = deepest_depth(p);
-    const bool tail = !depths_equal(p);
-    // Replay one captured graph per wave: a depth-16 wave is ~85 launches, and its late
-    // bounces have so few paths that launching dominates. Not used by the allocation-free
+    const int bounce_cap = j.bounce_cap;
+    // Streaming waves: slots of ended paths take the descriptor's next paths every
+    // iteration, so the wave stays full until its paths run out and the late bounces of a
+    // few long paths are paid once per descriptor, not once per wave of cap paths. The
+    // host looks at the counters after every kStreamIters iterations (one graph replay).
+    W.A.slot_free = W.slot_free;
+    W.A.free_count = W.free_count;
+    W.A.free_off = W.free_off;
+    // Replay one captured graph per kStreamIters iterations. Not used by the allocation-free
     // path (instantiating a graph allocates), when every launch is timed with events, nor by
     // fl_li (its small batches would replace the render's graph with one of their own size).
     const bool use_graph = !fixed_scratch && !prof->on && !li;
     if (use_graph && (!ctx->wave_graph || ctx->graph_base != W.A.cnt || ctx->graph_cap != W.cap ||
-                      ctx->graph_depth != depth || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count ||
+                      ctx->graph_depth != kStreamIters || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count ||
                       ctx->graph_std != (int)standard)) {
         if (ctx->wave_graph) {
             cudaGraphExecDestroy(ctx->wave_graph);
@@ -1424,7 +1616,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         cudaGraph_t g = nullptr;
         RenderProfile off;
         FL_CUDA_TRY(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        enqueue_wave<NL>(W, depth, count, &off, sms, st, standard);
+        enqueue_bounces<NL>(W, 0, kStreamIters, count, &off, sms, st, standard, true);
         FL_CUDA_TRY(ctx, cudaStreamEndCapture(st, &g));
         cudaError_t e = cudaGraphInstantiate(&ctx->wave_graph, g, 0);
         cudaGraphDestroy(g);
@@ -1434,28 +1626,40 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
         }
         ctx->graph_base = W.A.cnt;
         ctx->graph_cap = W.cap;
-        ctx->graph_depth = depth;
+        ctx->graph_depth = kStreamIters;
         ctx->graph_nl_mode = NL;
         ctx->graph_count = (int)count;
         ctx->graph_std = (int)standard;
     }
-    for (unsigned long long wb = 0; wb < total; wb += W.cap) {
+    const uint32_t per_iter = standard ? 9u : 7u;  // launches per iteration
+    for (unsigned long long wb = 0; wb < total; wb += kStreamDescPaths) {
         WaveDesc d;
-        d.n_wave = (uint32_t)std::min<unsigned long long>(W.cap, total - wb);
+        d.n_wave = (uint32_t)std::min<unsigned long long>(kStreamDescPaths, total - wb);
         d.n_seg = 1;
         d.seg[0] = WaveSeg{0u, 0u, d.n_wave, 0u, wb, 0ull};
         // pageable source: the copy is staged before the call returns, so `d` may be reused
         FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
-        if (use_graph) {
-            FL_CUDA_TRY(ctx, cudaGraphLaunch(ctx->wave_graph, st));
-            prof->launches += 1 + (standard ? 7 : 5) * (uint32_t)depth + (standard ? 6 : 4);
-        } else {
-            enqueue_wave<NL>(W, depth, count, prof, sms, st, standard);
-        }
-        FL_CUDA_TRY(ctx, cudaGetLastError());
-        if (tail) {
-            const fl_status rc2 = run_tail<NL>(ctx, W, depth + 1, count, prof, sms, st, standard);
-            if (rc2) return rc2;
+        k_stream_init<<<std::min<uint32_t>(((uint32_t)W.cap + 127) / 128, (uint32_t)sms * 8), 128, 0, st>>>(W.A);
+        prof->launches += 1;
+        // every path ends within bounce_cap bounces, so each run of bounce_cap + 1 iterations
+        // frees every slot that was busy at its start
+        const unsigned long long max_iters =
+            ((unsigned long long)d.n_wave / W.cap + 2ull) * (unsigned long long)(bounce_cap + 2);
+        for (unsigned long long it = 0;; it += kStreamIters) {
+            if (it > max_iters) {
+                set_error(ctx, "streaming wave did not drain within its iteration bound");
+                return FL_ERR_TRAVERSAL;
+            }
+            if (use_graph) {
+                FL_CUDA_TRY(ctx, cudaGraphLaunch(ctx->wave_graph, st));
+                prof->launches += per_iter * kStreamIters;
+            } else {
+                enqueue_bounces<NL>(W, 0, kStreamIters, count, prof, sms, st, standard, true);
+            }
+            FL_CUDA_TRY(ctx, cudaGetLastError());
+            FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, W.A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+            FL_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+            if (h_cnt->n_next == 0 && h_cnt->next_path >= d.n_wave) break;
         }
     }
     FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, W.A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
