@@ -355,6 +355,20 @@ fl_status fl_context_binned_tables(const fl_context *ctx_h, float *out, size_t n
     return FL_OK;
 }
 
+// Frees a scene (the caller holds ctx->mu). Every entry point returns with its work
+// finished, so nothing in flight reads the scene; the arrays go back to the context's pool
+// in stream order.
+static void scene_release(Scene *s) {
+    Context *ctx = s->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    void *arrays[] = {s->nodes, s->tris, s->soup, s->tri_material, s->tri_light, s->materials, s->lights,
+                      s->mat_refl60, s->standard, s->std_refl60, s->uvs, s->pixels, s->images};
+    for (void *p : arrays) dev_free(ctx, p);
+    if (s->counted) s->ctx->children--;
+    delete s;
+}
+
 fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **out) {
     Context *ctx = reinterpret_cast<Context *>(ctx_h);
     if (!ctx || !d || !out) return FL_ERR_INVALID;
@@ -492,7 +506,7 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
     s->n_materials = d->n_materials;
 
     auto fail = [&](fl_status rc) {
-        fl_scene_destroy(reinterpret_cast<fl_scene *>(s));
+        scene_release(s);  // ctx->mu is held
         return rc;
     };
     cudaError_t e;
@@ -593,16 +607,10 @@ fl_status fl_scene_create(fl_context *ctx_h, const fl_scene_desc *d, fl_scene **
 fl_status fl_scene_destroy(fl_scene *scene) {
     Scene *s = reinterpret_cast<Scene *>(scene);
     if (!s) return FL_ERR_INVALID;
-    // every entry point returns with its work finished, so nothing in flight reads the
-    // scene; the arrays go back to the context's pool in stream order
-    Context *ctx = s->ctx;
-    cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    void *arrays[] = {s->nodes, s->tris, s->soup, s->tri_material, s->tri_light, s->materials, s->lights,
-                      s->mat_refl60, s->standard, s->std_refl60, s->uvs, s->pixels, s->images};
-    for (void *p : arrays) dev_free(ctx, p);
-    if (s->counted) s->ctx->children--;
-    delete s;
+    // The context's lock: its stream may be capturing a render's graph on another thread,
+    // and neither the synchronisation nor the frees may enter that capture.
+    std::lock_guard<std::mutex> lock(s->ctx->mu);
+    scene_release(s);
     return FL_OK;
 }
 

@@ -196,6 +196,7 @@ struct RenderArgs {
     // chunk of kFreeChunk slots their count and the exclusive prefix of the counts
     uint8_t *slot_free;
     uint32_t *free_count, *free_off;
+    unsigned long long *job_done;  // streaming server: finished paths per job table entry (else null)
     WaveCounters *cnt;
     GuideArgs g;        // learned guiding (zero when off)
 };
@@ -287,6 +288,11 @@ __device__ inline void finish_path(const RenderArgs &A, const JobDev &J, const S
     spectrum_xyz<NL>(sm, A.tab, A.head[slot].lambda0, L, xyz);
     const uint32_t pix = A.head[slot].pixel;
     if (A.slot_free) A.slot_free[slot] = 1;  // streaming: the slot takes a new path
+    if (A.job_done) {  // one atomic per job among the converged lanes
+        const uint32_t job = A.head[slot].job;
+        const uint32_t peers = __match_any_sync(__activemask(), job);
+        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&A.job_done[job], (unsigned long long)__popc(peers));
+    }
     atomicAdd(&J.film[3 * (size_t)pix + 0], xyz[0]);
     atomicAdd(&J.film[3 * (size_t)pix + 1], xyz[1]);
     atomicAdd(&J.film[3 * (size_t)pix + 2], xyz[2]);

@@ -88,6 +88,20 @@ uint64_t scene_bytes_estimate(uint32_t n_tri, uint32_t n_mat) {
 
 }  // namespace
 
+// Streaming iterations per replay of the server's graph: the worker looks at the counters
+// (finished jobs, the descriptor's unstarted paths) after each replay. The descriptor is
+// topped up while fewer than kServeLookahead / 2 waves (of wave_paths) of its paths are
+// unstarted: fewer keeps a new job's samples closer to the front, more keeps every slot
+// busy between two looks.
+#ifndef FL_SERVE_ITERS
+#define FL_SERVE_ITERS 2
+#endif
+#ifndef FL_SERVE_LOOKAHEAD
+#define FL_SERVE_LOOKAHEAD 4
+#endif
+constexpr int kServeIters = FL_SERVE_ITERS;
+constexpr uint32_t kServeLookahead = FL_SERVE_LOOKAHEAD;
+
 struct Server {
     Context *ctx = nullptr;
     fl_server_config cfg{};
@@ -97,8 +111,12 @@ struct Server {
     void *wave_mem = nullptr;
     size_t wave_bytes = 0;
     WaveBuffers W{};
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;  // kServeIters streaming iterations
     std::vector<JobDev> table;  // kMaxJobs
+    WaveDesc desc{};            // the device descriptor's host copy
+    unsigned long long *d_job_done = nullptr;  // finished paths per job table entry
+    unsigned long long *h_done = nullptr;      // pinned copies of the counters
+    WaveCounters *h_cnt = nullptr;
     std::vector<int> free_slots;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -321,19 +339,45 @@ void reader_loop(Server *S) {
     }
 }
 
+// Completes the running jobs whose paths have all finished on the device (or that have no
+// film: their samples were skipped), in the worker without the lock held.
+void complete_jobs(Server *S, const std::vector<uint64_t> &done) {
+    for (uint64_t jid : done) {
+        HostJob *job;
+        {
+            std::lock_guard<std::mutex> lock(S->mu);
+            job = S->jobs[jid].get();
+        }
+        if (job->d_film) finish_job(S, jid, *job);
+        else {
+            std::lock_guard<std::mutex> lock(S->mu);
+            job->done_ms = S->now_ms();
+            job->status = job->fail != FL_OK ? job->fail : FL_ERR_OOM;
+            if (job->slot >= 0) S->free_slots.push_back(job->slot);
+            job->slot = -1;
+            S->stats.jobs_done++;
+        }
+    }
+    if (!done.empty()) S->cv_done.notify_all();
+}
+
 void worker_loop(Server *S) {
     cudaSetDevice(S->ctx->device);
     const size_t desc_head = offsetof(WaveDesc, seg);
+    const uint32_t cap = (uint32_t)S->W.cap;
     uint64_t seen = 0;
-    bool progressed = true;  // the last iteration ran a wave or completed jobs
+    bool progressed = true;   // the last iteration ran device work or completed jobs
+    bool busy = false;        // paths in flight or not yet started on the device
+    WaveCounters &hc = *S->h_cnt;
     while (true) {
         ServeScheduler::Admission adm;
-        std::vector<ServeScheduler::Seg> segs;
         {
             std::unique_lock<std::mutex> lock(S->mu);
             // with nothing to run (every running job waits for its scene) wait for news
             const auto i0 = std::chrono::steady_clock::now();
-            S->cv_work.wait(lock, [&] { return S->stop || S->events != seen || (progressed && !S->sched.idle()); });
+            S->cv_work.wait(lock, [&] {
+                return S->stop || S->events != seen || (progressed && (busy || !S->sched.idle()));
+            });
             S->stats.idle_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - i0).count();
             if (S->stop) break;
             seen = S->events;
@@ -353,6 +397,8 @@ void worker_loop(Server *S) {
         }
         if (!adm.evict.empty() || !adm.build.empty()) S->cv_build.notify_one();
         if (!adm.rejected.empty()) S->cv_done.notify_all();
+        std::vector<uint64_t> done;
+        bool table_changed = false, desc_changed = false;
         {
             std::lock_guard<std::mutex> lock(S->mu);
             for (uint64_t jid : adm.admitted) {
@@ -374,7 +420,7 @@ void worker_loop(Server *S) {
                 job.slot = S->free_slots.back();
                 S->free_slots.pop_back();
             }
-            // jobs whose scenes are now built join this wave; a failed build fails its jobs
+            // jobs whose scenes are now built join; a failed build fails its jobs
             for (uint64_t jid : S->sched.running_jobs()) {
                 HostJob &job = *S->jobs[jid];
                 if (job.bound || job.slot < 0 || !S->sched.scene_ready(job.scene)) continue;
@@ -383,6 +429,9 @@ void worker_loop(Server *S) {
                 job.start_ms = S->now_ms();
                 if (h.dev) {
                     S->table[job.slot] = job_of(h.dev, camera_basis_of(job.cam), job.params, job.d_film);
+                    cudaMemsetAsync(S->d_job_done + job.slot, 0, sizeof(unsigned long long), S->stream);
+                    S->h_done[job.slot] = 0;
+                    table_changed = true;
                 } else {
                     const size_t n_pix = (size_t)job.cam.width * job.cam.height;
                     S->release(job.d_film, n_pix * 3 * sizeof(double));
@@ -394,77 +443,90 @@ void worker_loop(Server *S) {
                     job.slot = -1;
                 }
             }
-            segs = S->sched.plan_wave((uint32_t)S->W.cap);
-        }
-        progressed = !segs.empty();
-        if (!segs.empty()) {
-            WaveDesc d{};
-            uint32_t slot_begin = 0;
-            {
-                std::lock_guard<std::mutex> lock(S->mu);
-                for (const auto &sg : segs) {
-                    HostJob &job = *S->jobs[sg.job];
-                    if (job.slot < 0) continue;  // failed admission: its samples are skipped
-                    d.seg[d.n_seg++] = WaveSeg{(uint32_t)job.slot, slot_begin, sg.count, 0u, sg.sample_base, 0ull};
-                    slot_begin += sg.count;
-                    if (d.n_seg == kMaxSegs) break;
+            // Top the descriptor up while fewer than two waves of its paths are unstarted:
+            // its unstarted remainder, then the scheduler's next plan of samples.
+            const uint32_t started = busy ? hc.next_path : S->desc.n_wave;
+            const uint32_t unstarted = S->desc.n_wave - std::min(started, S->desc.n_wave);
+            const uint32_t ahead = (uint32_t)(((uint64_t)cap * kServeLookahead) / 2);
+            if (unstarted < ahead) {
+                WaveDesc nd{};
+                uint32_t pos = 0;
+                for (uint32_t k = 0; k < S->desc.n_seg; ++k) {  // the remainder
+                    const WaveSeg &sg = S->desc.seg[k];
+                    const uint32_t b = std::max(sg.slot_begin, started), e = sg.slot_begin + sg.count;
+                    if (b >= e) continue;
+                    nd.seg[nd.n_seg++] = WaveSeg{sg.job, pos, e - b, 0u, sg.sample_base + (b - sg.slot_begin), 0ull};
+                    pos += e - b;
+                }
+                // a plan adds at most one range per running job
+                if (nd.n_seg + (uint32_t)S->sched.running() <= (uint32_t)kMaxSegs) {
+                    for (const auto &sg : S->sched.plan_wave(ahead - unstarted)) {
+                        HostJob &job = *S->jobs[sg.job];
+                        S->stats.paths += sg.count;
+                        if (job.slot < 0) continue;  // failed admission: its samples are skipped
+                        WaveSeg *last = nd.n_seg ? &nd.seg[nd.n_seg - 1] : nullptr;
+                        if (last && last->job == (uint32_t)job.slot &&
+                            last->sample_base + last->count == sg.sample_base)
+                            last->count += sg.count;  // the same job's next samples
+                        else
+                            nd.seg[nd.n_seg++] = WaveSeg{(uint32_t)job.slot, pos, sg.count, 0u, sg.sample_base, 0ull};
+                        pos += sg.count;
+                    }
+                    S->stats.waves++;
+                }
+                nd.n_wave = pos;
+                if (pos > unstarted) {  // new samples: the device goes on with nd from its start
+                    S->desc = nd;
+                    desc_changed = true;
                 }
             }
-            d.n_wave = slot_begin;
-            if (d.n_wave > 0) {
-                cudaMemcpyAsync(S->W.d_jobs, S->table.data(), sizeof(JobDev) * kMaxJobs, cudaMemcpyHostToDevice,
-                                S->stream);
-                cudaMemcpyAsync(S->W.d_wave, &d, desc_head + sizeof(WaveSeg) * d.n_seg, cudaMemcpyHostToDevice,
-                                S->stream);
-                const auto w0 = std::chrono::steady_clock::now();
-                const double w0_ms = S->now_ms();
-                cudaGraphLaunch(S->graph, S->stream);
-                cudaError_t e = cudaStreamSynchronize(S->stream);
-                // jobs with unequal lobe depths may have paths alive past the wave's bounces
-                if (e == cudaSuccess) {
-                    RenderProfile tprof;
-                    if (run_tail<4>(S->ctx, S->W, S->cfg.max_depth + 1, false, &tprof,
-                                    S->ctx->sm_count > 0 ? S->ctx->sm_count : 148, S->stream, true) != FL_OK)
-                        e = cudaErrorUnknown;
-                    else
-                        e = cudaStreamSynchronize(S->stream);
-                }
-                const double wave_ms =
-                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
-                std::lock_guard<std::mutex> lock(S->mu);
-                S->stats.busy_ms += wave_ms;
-                S->stats.wave_max_ms = std::max(S->stats.wave_max_ms, wave_ms);
-                S->trace_event("wave", w0_ms, wave_ms, d.n_seg, d.n_wave);
-                S->stats.waves++;
-                S->stats.paths += d.n_wave;
-                if (e != cudaSuccess) S->error = cudaGetErrorString(e);
+            // jobs without a film whose samples are all dispatched complete now
+            for (uint64_t jid : S->sched.running_jobs()) {
+                const HostJob &job = *S->jobs[jid];
+                if (job.slot < 0 && S->sched.dispatched_all(jid)) done.push_back(jid);
             }
+            for (uint64_t jid : done) S->sched.complete(jid);
         }
-        std::vector<uint64_t> done;
-        {
-            std::lock_guard<std::mutex> lock(S->mu);
-            done = S->sched.finish_wave();
+        if (table_changed)
+            cudaMemcpyAsync(S->W.d_jobs, S->table.data(), sizeof(JobDev) * kMaxJobs, cudaMemcpyHostToDevice, S->stream);
+        if (desc_changed) {
+            cudaMemcpyAsync(S->W.d_wave, &S->desc, desc_head + sizeof(WaveSeg) * S->desc.n_seg, cudaMemcpyHostToDevice,
+                            S->stream);
+            cudaMemsetAsync(&S->W.A.cnt->next_path, 0, sizeof(uint32_t), S->stream);
+            hc.next_path = 0;
         }
-        for (uint64_t jid : done) {
-            HostJob *job;
-            {
-                std::lock_guard<std::mutex> lock(S->mu);
-                job = S->jobs[jid].get();
-            }
-            if (job->d_film) finish_job(S, jid, *job);
-            else {
-                std::lock_guard<std::mutex> lock(S->mu);
-                job->done_ms = S->now_ms();
-                job->status = job->fail != FL_OK ? job->fail : FL_ERR_OOM;
-                if (job->slot >= 0) S->free_slots.push_back(job->slot);
-                job->slot = -1;
-                S->stats.jobs_done++;
-            }
-        }
-        if (!done.empty()) {
+        busy = busy || S->desc.n_wave > 0;
+        progressed = !done.empty();
+        if (busy) {
+            // a few iterations, then the counters: live paths, started paths, finished paths per job
+            const double w0 = S->now_ms();
+            cudaGraphLaunch(S->graph, S->stream);
+            cudaMemcpyAsync(S->h_cnt, S->W.A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, S->stream);
+            cudaMemcpyAsync(S->h_done, S->d_job_done, sizeof(unsigned long long) * kMaxJobs, cudaMemcpyDeviceToHost,
+                            S->stream);
+            const cudaError_t e = cudaStreamSynchronize(S->stream);
+            const double ms = S->now_ms() - w0;
+            busy = e == cudaSuccess && !(hc.n_next == 0 && hc.next_path >= S->desc.n_wave);
             progressed = true;
-            S->cv_done.notify_all();
+            std::vector<uint64_t> fin;
+            {
+                std::lock_guard<std::mutex> lock(S->mu);
+                S->stats.busy_ms += ms;
+                S->stats.wave_max_ms = std::max(S->stats.wave_max_ms, ms);
+                S->trace_event("iters", w0, ms, hc.n_next, hc.next_path);
+                if (e != cudaSuccess) S->error = cudaGetErrorString(e);
+                if (hc.err) S->error = "traversal or queue bound hit in a server wave";
+                for (uint64_t jid : S->sched.running_jobs()) {
+                    const HostJob &job = *S->jobs[jid];
+                    if (job.slot < 0 || !job.bound || !S->sched.dispatched_all(jid)) continue;
+                    const uint64_t total = (uint64_t)job.cam.width * job.cam.height * (uint64_t)job.params.spp;
+                    if (S->h_done[job.slot] >= total || e != cudaSuccess) fin.push_back(jid);
+                }
+                for (uint64_t jid : fin) S->sched.complete(jid);
+            }
+            done.insert(done.end(), fin.begin(), fin.end());
         }
+        complete_jobs(S, done);
         // scenes removed by the caller that no job uses any more
         bool dropped = false;
         {
@@ -547,19 +609,43 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     }
     S->table.assign(kMaxJobs, JobDev{});
     for (int i = cfg->max_jobs - 1; i >= 0; --i) S->free_slots.push_back(i);
+    e = cudaMalloc(&S->d_job_done, sizeof(unsigned long long) * kMaxJobs);
+    if (e == cudaSuccess) e = cudaHostAlloc(&S->h_done, sizeof(unsigned long long) * kMaxJobs, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(&S->h_cnt, sizeof(WaveCounters), cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaFree(S->d_job_done);
+        cudaFreeHost(S->h_done);
+        cudaFree(S->wave_mem);
+        drop_streams();
+        return cuda_status(ctx, e, "server counters");
+    }
+    std::memset(S->h_done, 0, sizeof(unsigned long long) * kMaxJobs);
+    std::memset(S->h_cnt, 0, sizeof(WaveCounters));
+    const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    // streaming waves: every slot free, an empty descriptor, finished paths counted per job
+    S->W.A.slot_free = S->W.slot_free;
+    S->W.A.free_count = S->W.free_count;
+    S->W.A.free_off = S->W.free_off;
+    S->W.A.job_done = S->d_job_done;
     cudaMemsetAsync(S->W.A.cnt, 0, sizeof(WaveCounters), S->stream);
-    // capture the launch sequence of one wave once; every wave replays it
+    cudaMemsetAsync(S->W.d_wave, 0, offsetof(WaveDesc, seg), S->stream);
+    cudaMemsetAsync(S->d_job_done, 0, sizeof(unsigned long long) * kMaxJobs, S->stream);
+    k_stream_init<<<std::min<uint32_t>(((uint32_t)S->W.cap + 127) / 128, (uint32_t)sms * 8), 128, 0, S->stream>>>(S->W.A);
+    // capture kServeIters streaming iterations once; the worker replays them
     RenderProfile prof;
     cudaGraph_t g = nullptr;
     e = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
         // the server's waves may carry any scene: include the StandardSurface kernels
-        enqueue_wave<4>(S->W, cfg->max_depth, false, &prof, ctx->sm_count > 0 ? ctx->sm_count : 148, S->stream, true);
+        enqueue_bounces<4>(S->W, 0, kServeIters, false, &prof, sms, S->stream, true, true);
         e = cudaStreamEndCapture(S->stream, &g);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&S->graph, g, 0);
     if (g) cudaGraphDestroy(g);
     if (e != cudaSuccess) {
+        cudaFree(S->d_job_done);
+        cudaFreeHost(S->h_done);
+        cudaFreeHost(S->h_cnt);
         cudaFree(S->wave_mem);
         drop_streams();
         return cuda_status(ctx, e, "wave graph capture");
@@ -610,6 +696,9 @@ fl_status fl_server_destroy(fl_server *srv) {
     for (auto &kv : S->scenes)
         if (kv.second.dev) fl_scene_destroy(reinterpret_cast<fl_scene *>(kv.second.dev));
     if (S->graph) cudaGraphExecDestroy(S->graph);
+    cudaFree(S->d_job_done);
+    cudaFreeHost(S->h_done);
+    cudaFreeHost(S->h_cnt);
     cudaFree(S->wave_mem);
     cudaStreamSynchronize(S->rstream);
     cudaEventDestroy(S->ev_resolved);

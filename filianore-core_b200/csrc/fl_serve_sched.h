@@ -276,6 +276,28 @@ public:
         return done;
     }
 
+    // Completes one running job whose samples were all dispatched and have all finished
+    // (the streaming server learns that from the device): releases its film and its hold
+    // on the scene. Returns false for a job that is not running or has samples left.
+    bool complete(uint64_t job) {
+        auto it = std::find(running_.begin(), running_.end(), job);
+        if (it == running_.end()) return false;
+        JobState &js = jobs_[job];
+        if (js.dispatched < js.total) return false;
+        used_ -= js.film_bytes;
+        SceneState &sc = scenes_[js.scene];
+        sc.users -= 1;
+        sc.last_use = ++clock_;
+        jobs_.erase(job);
+        running_.erase(it);
+        return true;
+    }
+    // whether every sample of a running job has been dispatched
+    bool dispatched_all(uint64_t job) const {
+        auto it = jobs_.find(job);
+        return it != jobs_.end() && it->second.dispatched >= it->second.total;
+    }
+
     // A scene no pending or running job uses (it may still be resident): can be forgotten.
     bool scene_unused(uint64_t id) const {
         auto it = scenes_.find(id);
