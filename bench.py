@@ -206,17 +206,18 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
     warm = ctx.scene(made[0])
     warm.render(scenes.render_params(1, 16), camera=warm.src.camera_struct(64, 64))
     warm.close()
-    service, tris = [], []
-    samples = 0
-    for i, (target, res, spp, _) in enumerate(reqs):
-        sc = made[i]
-        tris.append(sc.n_tri)
-        t0 = time.perf_counter()
-        h = ctx.scene(sc)
-        h.render(scenes.render_params(spp, 16, fb.FL_SPECTRAL_HERO4))
-        h.close()
-        service.append(time.perf_counter() - t0)
-        samples += res * res * spp
+    # each request's service time is the shorter of two measurements (a one-off stall, such
+    # as the first use of a pool block, does not count against the serial path)
+    service = [float("inf")] * n_req
+    tris = [sc.n_tri for sc in made]
+    samples = sum(res * res * spp for (_, res, spp, _) in reqs)
+    for _ in range(2):
+        for i, (target, res, spp, _) in enumerate(reqs):
+            t0 = time.perf_counter()
+            h = ctx.scene(made[i])
+            h.render(scenes.render_params(spp, 16, fb.FL_SPECTRAL_HERO4))
+            h.close()
+            service[i] = min(service[i], time.perf_counter() - t0)
     mean_s = float(np.mean(service))
     lam = 0.8 / mean_s
     arrivals = np.cumsum(rng.exponential(1.0 / lam, n_req))
@@ -270,7 +271,7 @@ def gpu_serve(args, world, rank, local, barrier, reduce_max):
         last_done, first_submit = 0.0, None
         for i in range(n_req):
             submitted[i].wait()
-            _, _, st = srv.wait(job_ids[i], timeout_ms=600000)
+            _, _, st = srv.wait(job_ids[i], timeout_ms=120000)
             tti.append((st["done_ms"] - st["submit_ms"]) / 1e3 + late[i])  # from the scheduled arrival
             rows.append((tti[-1], i, st))
             last_done = max(last_done, st["done_ms"])

@@ -561,6 +561,36 @@ static fl_status guide_pass(Guide *G, Scene *s, const CamDev &cam, const fl_rend
     const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
     const size_t desc_bytes = offsetof(WaveDesc, seg) + sizeof(WaveSeg);
     RenderProfile prof;
+    if (!train) {
+        // sampling only: streaming waves, as fl_render's (no records to close per wave)
+        W.A.slot_free = W.slot_free;
+        W.A.free_count = W.free_count;
+        W.A.free_off = W.free_off;
+        for (unsigned long long wb = 0; wb < total; wb += kStreamDescPaths) {
+            WaveDesc d;
+            d.n_wave = (uint32_t)std::min<unsigned long long>(kStreamDescPaths, total - wb);
+            d.n_seg = 1;
+            d.seg[0] = WaveSeg{0u, 0u, d.n_wave, 0u, wb, 0ull};
+            FL_CUDA_TRY(ctx, cudaMemcpyAsync(W.d_wave, &d, desc_bytes, cudaMemcpyHostToDevice, st));
+            k_stream_init<<<std::min<uint32_t>(((uint32_t)W.cap + 127) / 128, (uint32_t)sms * 8), 128, 0, st>>>(W.A);
+            const unsigned long long max_iters =
+                ((unsigned long long)d.n_wave / W.cap + 2ull) * (unsigned long long)(j.bounce_cap + 2);
+            for (unsigned long long it = 0;; it += kStreamIters) {
+                if (it > max_iters) {
+                    set_error(ctx, "streaming wave did not drain within its iteration bound");
+                    return FL_ERR_TRAVERSAL;
+                }
+                enqueue_bounces<4, true>(W, 0, kStreamIters, false, &prof, sms, st, s->ext_kernels, true);
+                FL_CUDA_TRY(ctx, cudaGetLastError());
+                FL_CUDA_TRY(ctx, cudaMemcpyAsync(h_cnt, W.A.cnt, sizeof(WaveCounters), cudaMemcpyDeviceToHost, st));
+                FL_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+                if (h_cnt->n_next == 0 && h_cnt->next_path >= d.n_wave) break;
+            }
+        }
+        return FL_OK;
+    }
+    // Training: fixed waves, so that every path of a wave has ended, and closed its records,
+    // when they train the guide after the wave.
     for (unsigned long long wb = 0; wb < total; wb += W.cap) {
         WaveDesc d;
         d.n_wave = (uint32_t)std::min<unsigned long long>(W.cap, total - wb);

@@ -1347,6 +1347,7 @@ inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 // bytes of wave state per path slot
 // Iterations per graph replay of a streaming wave, and the most paths one descriptor lists.
 constexpr int kStreamIters = 8;
+static_assert(kStreamIters % 2 == 0, "a replay starts at queue parity 0");
 constexpr unsigned long long kStreamDescPaths = 1ull << 31;
 // Default paths per wave. A wave runs every bounce up to the deepest depth, and its late
 // bounces hold few paths (their launches cost about the same as full ones), so large waves

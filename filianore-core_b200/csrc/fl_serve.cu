@@ -100,6 +100,8 @@ uint64_t scene_bytes_estimate(uint32_t n_tri, uint32_t n_mat) {
 #define FL_SERVE_LOOKAHEAD 4
 #endif
 constexpr int kServeIters = FL_SERVE_ITERS;
+// the trace queues alternate by iteration parity and a replay always starts at parity 0
+static_assert(kServeIters > 0 && kServeIters % 2 == 0, "an even number of iterations per replay");
 constexpr uint32_t kServeLookahead = FL_SERVE_LOOKAHEAD;
 
 struct Server {
@@ -151,28 +153,18 @@ struct Server {
     std::chrono::steady_clock::time_point t0;
     fl_server_stats stats{};
     std::string error;
-    // device buffers of finished jobs, kept by size for the next jobs: cudaFree and
-    // cudaMalloc synchronise the device, which would stall the wave pipeline per job
-    std::multimap<size_t, void *> buffer_pool;
-
+    // Film buffers come from the context's stream-ordered pool on the server's stream:
+    // cudaMalloc / cudaFree would synchronise the device and stall the waves per job.
     void *acquire(size_t bytes) {
-        auto it = buffer_pool.find(bytes);
-        if (it != buffer_pool.end()) {
-            void *p = it->second;
-            buffer_pool.erase(it);
-            return p;
-        }
         void *p = nullptr;
-        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        if (cudaMallocFromPoolAsync(&p, bytes, ctx->pool, stream) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
         return p;
     }
-    void release(void *p, size_t bytes) {
-        if (!p) return;
-        if (buffer_pool.count(bytes) < 8) buffer_pool.insert({bytes, p});
-        else cudaFree(p);
+    void release(void *p, size_t) {
+        if (p) cudaFreeAsync(p, stream);
     }
     void *acquire_pinned(size_t bytes) {
         auto it = pinned_pool.find(bytes);
@@ -189,9 +181,7 @@ struct Server {
         return p;
     }
     void release_pinned(void *p, size_t bytes) {
-        if (!p) return;
-        if (pinned_pool.count(bytes) < 8) pinned_pool.insert({bytes, p});
-        else cudaFreeHost(p);
+        if (p) pinned_pool.insert({bytes, p});  // kept until the server is destroyed (cudaFreeHost synchronises)
     }
 
     Server(uint64_t budget, int max_jobs, int policy) : sched(budget, max_jobs, policy) {
@@ -685,12 +675,12 @@ fl_status fl_server_destroy(fl_server *srv) {
     for (const BuildTask &t : S->build_q)
         if (t.release) fl_scene_destroy(reinterpret_cast<fl_scene *>(t.release));
     for (auto &kv : S->jobs) {
-        cudaFree(kv.second->d_film);
-        cudaFree(kv.second->d_rgb);
+        if (kv.second->d_film) cudaFreeAsync(kv.second->d_film, S->stream);
+        if (kv.second->d_rgb) cudaFreeAsync(kv.second->d_rgb, S->stream);
         cudaFreeHost(kv.second->h_rgb);
         cudaFreeHost(kv.second->h_xyz);
     }
-    for (auto &kv : S->buffer_pool) cudaFree(kv.second);
+    cudaStreamSynchronize(S->stream);
     for (auto &kv : S->pinned_pool) cudaFreeHost(kv.second);
     for (cudaEvent_t e : S->free_events) cudaEventDestroy(e);
     for (auto &kv : S->scenes)
