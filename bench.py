@@ -53,7 +53,10 @@ RENDER = {"width": 1920, "height": 1080, "spp": 64, "depth": 16}
 #   raycast: one k_trace launch over the full 16,777,216 rays: 32.73 + 1.21 GB
 #   render:  k_trace_paths + k_trace_rays2 over the first 8 of the frame's 64 waves
 #            (272 launches): 5.762 + 0.368 GB, times 8 for the frame
-TRAFFIC = {"raycast_incoherent": 33.94e9, "render": 49.04e9}
+# DRAM bytes (read + write) of the roofline kernels from ncu captures of this code: the
+# render's traversal kernels over one whole timed frame (48 streaming iterations), and one
+# k_trace launch of 2^21 incoherent rays scaled by 8 to the 2^24 rays of a bench launch
+TRAFFIC = {"raycast_incoherent": 27.79e9, "render": 45.89e9}
 COHERENT_SIDE = 4096
 
 
@@ -518,7 +521,7 @@ def gpu_render(args, world, rank, local, barrier, reduce_max):
     full = RENDER["width"] == 1920 and RENDER["height"] == 1080 and RENDER["spp"] == 64
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": TRAFFIC["render"] if full else None,
-                "traffic_unit": "bytes per frame (ncu, 8 of 64 waves x 8)", "peak_src": peaks["src"],
+                "traffic_unit": "bytes per frame (ncu, every traversal launch of one frame)", "peak_src": peaks["src"],
                 "kernel": "BVH traversal (k_trace_paths + k_trace_rays2)",
                 "alg_bytes_per_frame": int(alg_bytes), "traversal_ms_per_frame": round(trav_ms, 3),
                 "profiled_frame_ms": round(prof["ms"], 3),
@@ -591,7 +594,7 @@ def measure_raycast(args, world, rank, local, barrier, reduce_max, steps):
                          "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_src": peaks["src"],
                          "kernel": "k_trace<closest>", "alg_bytes_per_launch": int(alg_bytes),
                          "traffic": TRAFFIC.get(f"raycast_{name}") if N_RAYS == 1 << 24 else None,
-                         "traffic_unit": "bytes per launch (ncu)",
+                         "traffic_unit": "bytes per launch (ncu: 2^21 rays, x 8)",
                          # layout-independent floor: only the ray read and the hit write
                          "floor_bytes_per_ray": RAY_BYTES + HIT_BYTES,
                          "floor_frac": round(n * (RAY_BYTES + HIT_BYTES) / (launch_ms / 1e3) / 1e9 / peaks["hbm_gbs"], 4)},
