@@ -1344,19 +1344,19 @@ static __global__ void k_resolve(const double *__restrict__ film, uint32_t n_pix
 
 inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// bytes of wave state per path slot
 // Iterations per graph replay of a streaming wave, and the most paths one descriptor lists.
 constexpr int kStreamIters = 8;
 static_assert(kStreamIters % 2 == 0, "a replay starts at queue parity 0");
 constexpr unsigned long long kStreamDescPaths = 1ull << 31;
-// Default paths per wave. A wave runs every bounce up to the deepest depth, and its late
-// bounces hold few paths (their launches cost about the same as full ones), so large waves
-// amortise that tail: the 1,048,578-triangle procedural frame (1920x1080, 64 spp, depth 16)
-// measured 915 Mrays/s with waves of 2^21 paths, 1,209 with 2^22 and 1,424 with 2^23.
+// Default path slots of a streaming wave. More slots give each iteration's kernels more
+// rays to share the GPU: the 1,048,578-triangle procedural frame (1920x1080, 64 spp, depth
+// 16) measured 1,430 Mrays/s with 2^20 slots, 1,582 with 2^21, 1,668 with 2^22 and 1,685
+// with 2^23 (3.3 GB of state with two lights). The 60-bin mode has 15x the spectra per slot.
 constexpr size_t kWavePathsHero = (size_t)1 << 23;
 constexpr size_t kWavePathsBins60 = (size_t)1 << 21;
 // The wave state of a render lives in the context scratch, at most this many bytes.
 constexpr size_t kWaveScratchBytes = (size_t)16 << 30;
+// bytes of wave state per path slot
 inline size_t wave_bytes_per_slot(int NL, int nl) {
     return 101 + 4 * kShadeClasses + 8 * (size_t)NL + 8 * (size_t)NL * nl + 4 * (size_t)nl + 72 * (size_t)nl;
 }

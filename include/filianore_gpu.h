@@ -325,7 +325,8 @@ typedef struct {
                                0..249; ignored with FL_RENDER_LOBE_DEPTHS */
     float rr_threshold;     /* PathIntegrator rrThreshold (pathintegrator.h:11-12), 1 by default */
     int32_t spectral_mode;  /* FL_SPECTRAL_* */
-    int32_t wave_paths;     /* paths in flight per wavefront (0 = library default) */
+    int32_t wave_paths;     /* path slots of the streaming wave (0 = library default: 2^23 with hero
+                               wavelengths, 2^21 with 60 bins); a frame's paths stream through them */
     uint32_t sample_offset; /* first sample index (progressive / multi-GPU sample split) */
     int32_t flags;          /* FL_RENDER_* */
     int32_t reserved;
@@ -391,18 +392,20 @@ FL_API fl_status fl_li(fl_scene *scene, const fl_render_params *params, const fl
 /* ------------------------------------------------------------------------- */
 /* A server keeps registered scenes resident in HBM under a memory budget (least recently
  * used idle scenes are evicted and rebuilt on demand), admits jobs in arrival order as
- * films and scenes fit, and renders the running jobs' samples together: every wave's path
- * slots are split over the running jobs and run through the same kernels. A job's image is
- * the one fl_render gives for the same scene, camera and parameters (hero mode). */
+ * films and scenes fit, and renders the running jobs' samples together: one streaming wave
+ * runs continuously, the scheduler appends each plan of samples (about a wave of
+ * wave_paths, split over the running jobs by the policy) to it, and a job completes when
+ * all its paths have finished. A job's image is the one fl_render gives for the same
+ * scene, camera and parameters (hero mode). */
 typedef struct fl_server fl_server;
 
 typedef struct {
     uint64_t memory_budget_bytes; /* resident scenes + films of running jobs */
-    int32_t wave_paths;           /* path slots per wave shared by running jobs (0 = 2^21) */
-    int32_t max_depth;            /* deepest job accepted; each wave runs this many bounces */
+    int32_t wave_paths;           /* path slots of the streaming wave shared by running jobs (0 = 2^21) */
+    int32_t max_depth;            /* deepest job accepted */
     int32_t max_jobs;             /* jobs running at once, 1..64 */
     int32_t max_lights;           /* most lights any scene may have, 0..64 */
-    int32_t policy;               /* FL_SERVE_* wave packing */
+    int32_t policy;               /* FL_SERVE_*: how each plan of samples is split over the jobs */
 } fl_server_config;
 
 enum {
@@ -432,11 +435,12 @@ typedef struct {
 
 typedef struct {
     uint64_t jobs_submitted, jobs_done, waves, paths, builds, evictions, resident_bytes;
+    /* waves: plans of samples appended to the streaming wave; paths: samples planned */
     uint32_t running, pending;
-    double busy_ms;               /* host wall time of the waves (launch to completion) */
-    double wave_max_ms;           /* the longest wave */
+    double busy_ms;               /* host wall time of the graph replays (launch to completion) */
+    double wave_max_ms;           /* the longest replay */
     double build_ms, build_max_ms; /* scene builds on the builder thread: total and longest */
-    double finish_ms;             /* resolving and copying out finished films (worker thread) */
+    double finish_ms;             /* queueing finished films' resolve and read-out (worker thread) */
     double idle_ms;               /* worker time spent waiting for submissions or builds */
 } fl_server_stats;
 
