@@ -155,6 +155,23 @@ int main() {
         q.admit();
         print_plan("G3", q.plan_wave(256));
     }
+    // completing single jobs (the streaming server): only a running job with every sample
+    // dispatched completes; its film and its hold on the scene are released
+    {
+        ServeScheduler q(1000, 4, ServeScheduler::kFirstCome);
+        q.add_scene(1, 300);
+        q.submit(90, 1, 50, 100);
+        q.submit(91, 1, 50, 300);
+        q.admit();
+        q.plan_wave(256);  // 90: 100, 91: 156 of 300
+        const int a90 = q.dispatched_all(90), a91 = q.dispatched_all(91);
+        const int c91 = q.complete(91), c90 = q.complete(90);
+        std::printf("H1 %d %d %d %d used %llu\n", a90, a91, c91, c90, (unsigned long long)q.used());
+        q.plan_wave(256);  // 91: the other 144
+        const int b91 = q.dispatched_all(91), d91 = q.complete(91);
+        std::printf("H2 %d %d running %d used %llu unused %d\n", b91, d91, (int)q.running(),
+                    (unsigned long long)q.used(), (int)q.scene_unused(1));
+    }
     // forgetting a scene: only once no pending or running job uses it; its bytes are released
     {
         ServeScheduler q(1000, 4);

@@ -80,7 +80,7 @@ def test_deadline_policy_serves_a_long_job_once_its_deadline_is_earliest():
 
 
 def test_removed_scene_is_forgotten_only_when_unused():
-    out = run_driver()[58:]
+    out = run_driver()[60:]
     assert out[0] == "F unused 0 used 310"      # a running job holds it
     assert out[1] == "F unused 1"               # the job is done
     assert out[2] == "F resident 1 used 0 known 0"
@@ -105,3 +105,13 @@ def test_async_builds_hold_jobs_until_their_scene_is_built():
     assert out[0] == "G1 build 1 planned 0 ready 0"
     assert out[1] == "G2 80:100@0"
     assert out[2] == "G3 81:100@0 82:50@0"
+
+
+def test_complete_releases_a_job_once_all_its_samples_are_dispatched():
+    """The streaming server completes jobs one at a time when the device has finished their
+    paths: a job with samples still to dispatch is not completed; a completed one releases
+    its film (used 400 = scene 300 + the other film) and, with the last job, the scene's
+    hold (the scene stays resident and becomes unused)."""
+    out = run_driver()[58:60]
+    assert out[0] == "H1 1 0 0 1 used 350"
+    assert out[1] == "H2 1 1 running 0 used 300 unused 1"
