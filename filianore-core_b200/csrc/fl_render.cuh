@@ -773,13 +773,16 @@ __device__ inline void add_spheres(const JobDev &A, const RayPre &r, TraceResult
 #define FL_TRACE_STEPS 8
 #endif
 constexpr int kRenderTraceSteps = FL_TRACE_STEPS;  // traversal steps between refills of finished lanes
-// resident blocks per SM the render's traversal kernels are compiled for (caps registers)
+// Resident blocks per SM the render's traversal kernels are compiled for (caps registers).
+// With streaming waves every launch has a full queue, and more warps per SM pay: the
+// 1,048,578-triangle frame measured 1,632 Mrays/s at 6 blocks, 1,670 at 7, 1,697 at 8 and
+// 1,695 at 9 (A/B on one B200).
 #ifndef FL_RENDER_TRACE_BLOCKS
-#define FL_RENDER_TRACE_BLOCKS 7
+#define FL_RENDER_TRACE_BLOCKS 8
 #endif
 constexpr int kRenderTraceBlocks = FL_RENDER_TRACE_BLOCKS;
 #ifndef FL_RENDER_RAYS2_BLOCKS
-#define FL_RENDER_RAYS2_BLOCKS 7
+#define FL_RENDER_RAYS2_BLOCKS 8
 #endif
 constexpr int kRenderRays2Blocks = FL_RENDER_RAYS2_BLOCKS;  // the same for the shadow / MIS ray kernel
 // resident blocks per SM that k_shade and k_continue are compiled for (0: no bound)
