@@ -56,7 +56,7 @@ RENDER = {"width": 1920, "height": 1080, "spp": 64, "depth": 16}
 # DRAM bytes (read + write) of the roofline kernels from ncu captures of this code: the
 # render's traversal kernels over one whole timed frame (48 streaming iterations), and one
 # k_trace launch of 2^21 incoherent rays scaled by 8 to the 2^24 rays of a bench launch
-TRAFFIC = {"raycast_incoherent": 27.79e9, "render": 45.89e9}
+TRAFFIC = {"raycast_incoherent": 27.79e9, "render": 47.01e9}
 COHERENT_SIDE = 4096
 
 
