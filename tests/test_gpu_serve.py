@@ -109,3 +109,26 @@ def test_served_standard_surface_and_textures_equal_plain_render():
         np.testing.assert_allclose(rgb, want_rgb, rtol=1e-5, atol=1e-6)
     srv.close()
     ctx.close()
+
+
+def test_unequal_lobe_depths_and_many_refills_equal_alone():
+    """Jobs with unequal lobe depths (paths may outlive the deepest depth) on a server of 2,048
+    path slots, so that every job's paths stream through the slots over many iterations and
+    share them with the other jobs: the images equal fl_render's for each job alone."""
+    ctx = fb.Context(0)
+    srv = fb.Server(ctx, budget_bytes=2 << 30, max_depth=8, max_jobs=8, max_lights=4, wave_paths=2048)
+    sc_a = scenes.cornell(48, 40, "standard2")
+    sc_b = scenes.cornell(32, 32, "materials")
+    ia, ib = srv.add_scene(sc_a), srv.add_scene(sc_b)
+    jobs = []
+    for sid, sc, spp, depths in ((ia, sc_a, 6, (5, 3, 6)), (ib, sc_b, 4, (3, 6, 5)), (ia, sc_a, 2, (2, 7, 4))):
+        cam = sc.camera_struct()
+        p = scenes.render_params(spp, 8, fb.FL_SPECTRAL_HERO4, depths=depths)
+        jobs.append((srv.submit(sid, cam, p), sc, cam, p))
+    for jid, sc, cam, p in jobs:
+        _, xyz, _ = srv.wait(jid, timeout_ms=60000, want_xyz=True)
+        _, want = alone(ctx, sc, cam, p)
+        np.testing.assert_allclose(xyz, want, rtol=1e-9, atol=1e-12)
+    assert srv.stats()["jobs_done"] == 3
+    srv.close()
+    ctx.close()
