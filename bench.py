@@ -359,7 +359,8 @@ def gpu_guide(args, world, rank, local, barrier, reduce_max):
     runs = []
     for frac in (1 / 3, 1 / 2, 1.0):
         g = fb.Guide(ctx, seed=5, learning_rate=1e-3, select_prob=0.5, batch=32768, max_records=1 << 21,
-                     steps_per_wave=64, weight_average=0.99, learn_select=not args.fixed_select)
+                     steps_per_wave=64, weight_average=0.99, learn_select=not args.fixed_select,
+                     train_kernel=fb.FL_GUIDE_TRAIN_TCGEN05 if args.guide_tcgen05 else fb.FL_GUIDE_TRAIN_MMA_SYNC)
         img = np.zeros((R, R, 3), np.float64)
         t0 = time.perf_counter()
         _, gst = g.render_timed(s, scenes.render_params(4, depth, fb.FL_SPECTRAL_HERO4, sample_offset=1 << 20),
@@ -655,6 +656,7 @@ def main():
     ap.add_argument("--serve-wave-paths", type=int, default=0, help="serve: the server's path slots (0: its default)")
     ap.add_argument("--serve-policies", default=None, help="serve: comma-separated subset of the policies")
     ap.add_argument("--no-raycast", action="store_true", help="render: skip the ray-cast sub-measurement")
+    ap.add_argument("--guide-tcgen05", action="store_true", help="guide: train with the tcgen05 kernel")
     ap.add_argument("--fixed-select", action="store_true",
                     help="guide: a fixed selection probability c = 0.5 instead of the learned one")
     ap.add_argument("--size", default=None, help="render: WxH (smaller cases for profiling)")

@@ -51,6 +51,7 @@ struct TrainArgs {
     const float *cdf;          // resampling: inclusive prefix sum of the record weights (null: in order)
     uint32_t seed;             // resampling: stratification jitter of this batch
     int learned;               // fit the selection probability with the mixture (loss -log f)
+    int *err;                  // counts tensor-core products that did not complete (nullable)
 };
 
 __device__ inline float hash01(uint32_t a, uint32_t b) {
@@ -297,6 +298,303 @@ __global__ void __launch_bounds__(256, 1) k_guide_train(TrainArgs T) {
     guide_dw(X, kLdIn, 5, DzA, 8, T.grad + guide_woff(0), 80, 64);
 }
 
+
+// ----------------------------------------------------------------- tcgen05 training kernel
+//
+// The same step as k_guide_train with its nine 128-row products on the 5th-generation tensor
+// cores: the forward layers (X W0^T, ..., A4 Wh^T) and the backward products dZ W of the
+// layers past the first run as tcgen05.mma (M = 128 records, N = 64 or 48, K = 16 per
+// instruction) from shared memory into a 64-column TMEM accumulator, issued by one thread
+// and completed through an mbarrier; the epilogues read the accumulator back with
+// tcgen05.ld (each warp its 32 TMEM lanes, a warp pair splitting the columns), apply ReLU or
+// the ReLU mask and write FP16 operands for the next product. The weight gradients (64 or 80
+// input rows, summed over the records) stay on mma.sync and overlap the tensor-core product
+// of the same level. Operands use the canonical K-major layout without swizzle: 8-row x 16-byte
+// core matrices, the next one along K 128 bytes on, the next 8 rows K x 16 bytes on.
+
+// element (r, k) of an R x K operand in the canonical layout, in halves
+__device__ __forceinline__ int tc_canon(int r, int k, int K) { return (r >> 3) * (K * 8) + (k >> 3) * 64 + (r & 7) * 8 + (k & 7); }
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    // start, leading and stride byte offsets, descriptor version 1, no swizzle
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// FP32 accumulator, FP16 A and B, A K-major, B K-major or (b_mn) MN-major, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int n, bool b_mn) {
+    return (1u << 4) | (b_mn ? 1u << 16 : 0u) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+// D (TMEM) = A (128 x K, K-major) * B, one thread issues, the mbarrier receives the commit.
+// B is W (N rows x K, K-major) for the forward products, or, for the backward ones, the same
+// forward copy of W read as an MN-major K x N operand (its 8-row groups along K 16 * Kw
+// bytes apart, Kw its own row length), which makes dZ W without a transposed copy.
+__device__ inline void tc_gemm(uint32_t tmem, const __half *A, const __half *B, int K, int n, bool b_mn, int Kw,
+                               uint64_t *mbar) {
+    const uint32_t a0 = smem_u32(A), b0 = smem_u32(B), sbo = (uint32_t)K * 16u, idesc = tc_idesc(n, b_mn);
+    const uint32_t b_lbo = b_mn ? (uint32_t)Kw * 16u : 128u, b_sbo = b_mn ? 128u : sbo;
+    const uint32_t b_step = b_mn ? 2u * (uint32_t)Kw * 16u : 256u;  // bytes per 16 of K
+    for (int s = 0; s < K / 16; ++s) {
+        const uint64_t da = tc_sdesc(a0 + 256u * s, 128u, sbo), db = tc_sdesc(b0 + b_step * s, b_lbo, b_sbo);
+        const uint32_t acc = s > 0 ? 1u : 0u;
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                     "l"(da), "l"(db), "r"(idesc), "r"(acc));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                 : "memory");
+}
+// every writer of an operand calls this before the barrier that precedes the product
+__device__ __forceinline__ void tc_operands_written() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+// bounded wait for the product's commit (phase `ph`); false if it did not arrive
+__device__ inline bool tc_wait(uint64_t *mbar, uint32_t ph) {
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 24) && !done; ++it)
+        asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(smem_u32(mbar)), "r"(ph));
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return done != 0;
+}
+// 16 / 32 consecutive accumulator columns of this thread's TMEM lane
+__device__ inline void tc_ld16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ inline void tc_ld32(uint32_t taddr, float v[32]) {
+    tc_ld16(taddr, v);
+    tc_ld16(taddr + 16u, v + 16);
+}
+// 32 accumulator columns of row m (from c0) through ReLU, or through the mask of the
+// activations `mask` (same layout), into the 64-wide canonical operand `out`
+__device__ inline void tc_store_row32(const float v[32], int m, int c0, __half *out, const __half *mask) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t h[4];
+        const int c = c0 + 8 * q;
+        uint4 mk4 = make_uint4(0, 0, 0, 0);
+        if (mask) mk4 = *reinterpret_cast<const uint4 *>(mask + tc_canon(m, c, 64));
+        const uint32_t mw[4] = {mk4.x, mk4.y, mk4.z, mk4.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float a = v[8 * q + 2 * j], b = v[8 * q + 2 * j + 1];
+            if (mask) {
+                const float2 am = __half22float2(*reinterpret_cast<const __half2 *>(&mw[j]));
+                a = am.x > 0.f ? a : 0.f;
+                b = am.y > 0.f ? b : 0.f;
+            }
+            h[j] = pack_h2(a, b, mask == nullptr);
+        }
+        *reinterpret_cast<uint4 *>(out + tc_canon(m, c, 64)) = make_uint4(h[0], h[1], h[2], h[3]);
+    }
+}
+// weight gradient of one layer, as guide_dw, from canonical operands: S (records x in, Ks
+// wide) and D (records x out, Kd wide)
+__device__ inline void tc_dw(const __half *S, int Ks, int Mt, const __half *D, int Kd, int Nt, float *grad, int in_dim,
+                             int out_valid) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    for (int tile = warp; tile < Mt * Nt; tile += kTrainWarps) {
+        const int m0 = (tile / Nt) * 16, n0 = (tile % Nt) * 8;
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k0 = 0; k0 < kTrainRows; k0 += 16) {
+            uint32_t a[4], b[2];
+            ldsm_x4_t(a, S + tc_canon(k0 + (lane & 7) + ((lane >> 4) << 3), m0 + ((lane >> 3) & 1) * 8, Ks));
+            ldsm_x2_t(b, D + tc_canon(k0 + (lane & 15), n0, Kd));
+            mma16816(acc, a, b[0], b[1]);
+        }
+        const int o = n0 + 2 * t, i = m0 + g;
+        if (o < out_valid) {
+            atomicAdd(&grad[o * in_dim + i], acc[0]);
+            atomicAdd(&grad[o * in_dim + i + 8], acc[2]);
+        }
+        if (o + 1 < out_valid) {
+            atomicAdd(&grad[(o + 1) * in_dim + i], acc[1]);
+            atomicAdd(&grad[(o + 1) * in_dim + i + 8], acc[3]);
+        }
+    }
+}
+
+// shared memory of k_guide_train_tc (byte offsets)
+constexpr int kTcW0 = 0, kTcW1 = 10240, kTcWh = 34816, kTcX = 40960, kTcAct = 61440, kTcDzA = 126976,
+              kTcDzB = 143360, kTcMisc = 159744;
+constexpr size_t kTrainSmemTc = (size_t)kTcMisc + 1024;
+
+__global__ void __launch_bounds__(256, 1) k_guide_train_tc(TrainArgs T) {
+    extern __shared__ __align__(16) unsigned char tsm[];  // every operand offset is a multiple of 1024
+    const uint32_t n_total = min(*T.rec_count, T.rec_cap);
+    const uint32_t begin = T.cdf ? blockIdx.x * kTrainRows : T.batch_begin + blockIdx.x * kTrainRows;
+    const uint32_t end = T.cdf ? (n_total ? T.batch_size : 0u) : min(T.batch_begin + T.batch_size, n_total);
+    if (begin >= end || !(T.wstat[0] > 0.f)) return;
+    const float total = T.cdf ? T.cdf[n_total - 1] : 0.f;
+    if (T.cdf && !(total > 0.f)) return;
+    __half *Wc[4] = {reinterpret_cast<__half *>(tsm + kTcW0), reinterpret_cast<__half *>(tsm + kTcW1),
+                     reinterpret_cast<__half *>(tsm + kTcW1 + 8192), reinterpret_cast<__half *>(tsm + kTcW1 + 16384)};
+    __half *Wch = reinterpret_cast<__half *>(tsm + kTcWh);
+    __half *Xc = reinterpret_cast<__half *>(tsm + kTcX);
+    __half *Act[4] = {reinterpret_cast<__half *>(tsm + kTcAct), reinterpret_cast<__half *>(tsm + kTcAct + 16384),
+                      reinterpret_cast<__half *>(tsm + kTcAct + 32768), reinterpret_cast<__half *>(tsm + kTcAct + 49152)};
+    __half *DzA = reinterpret_cast<__half *>(tsm + kTcDzA);
+    __half *DzB = reinterpret_cast<__half *>(tsm + kTcDzB);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(tsm + kTcMisc);
+    uint32_t *taddr_s = reinterpret_cast<uint32_t *>(tsm + kTcMisc + 8);
+    uint32_t *rid = reinterpret_cast<uint32_t *>(tsm + kTcMisc + 64);  // record of each row (~0u: none)
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // TMEM: 64 columns for the accumulator (warp 0 allocates and frees)
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_s)), "r"(64));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    // weights W_l [out][in], canonical K-major (rows = outputs), 8 halves per copy; the head's
+    // rows 41..47 are zero
+    for (int l = 0; l < kGuideLayers; ++l) {
+        const int in = guide_in(l), out = guide_out(l), rows = l == 4 ? kHeadRowsPad : out, per_row = in / 8;
+        const __half *w = T.w + guide_woff(l);
+        __half *F = l == 4 ? Wch : Wc[l];
+        for (int e = tid; e < rows * per_row; e += blockDim.x) {
+            const int o = e / per_row, c8 = e % per_row;
+            const uint4 v = o < out ? *reinterpret_cast<const uint4 *>(w + o * in + 8 * c8) : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4 *>(F + tc_canon(o, 8 * c8, in)) = v;
+        }
+    }
+    // the rows' records (stratified resampling as k_guide_train), then their features
+    if (tid < kTrainRows) {
+        uint32_t i = begin + tid;
+        const bool valid = i < end;
+        if (T.cdf && valid) {
+            const float u = ((float)i + hash01(T.seed, i)) / (float)T.batch_size * total;
+            uint32_t lo = 0, hi = n_total - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (T.cdf[mid] > u) hi = mid;
+                else lo = mid + 1;
+            }
+            i = lo;
+        }
+        rid[tid] = valid ? i : ~0u;
+    }
+    __syncthreads();
+    {
+        const int m = tid >> 1, part = tid & 1;
+        uint32_t h[20];
+        if (rid[m] != ~0u) {
+            const float *R = T.rec + (size_t)rid[m] * kRecFloats;
+            float pn[3];
+            guide_normalise(T.bmin, T.binv, mk(R[0], R[1], R[2]), pn);
+            const float nf[3] = {R[3], R[4], R[5]};
+            guide_encode_pairs(pn, nf, (R[6] - 380.f) * (1.f / 340.f), part, h);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 20; ++k) h[k] = 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+            *reinterpret_cast<uint4 *>(Xc + tc_canon(m, 40 * part + 8 * q, kGuideIn)) =
+                make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
+    }
+    tc_operands_written();
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *taddr_s;
+    const int q4 = warp & 3, chalf = warp >> 2;       // TMEM lane quarter and column half of this warp
+    const int row = 32 * q4 + lane;                     // the accumulator row (record) this thread reads
+    const uint32_t tl = tmem + ((uint32_t)(32 * q4) << 16);
+    uint32_t ph = 0;
+    bool ok = true;
+    // forward: 4 hidden layers (ReLU) and the head
+    for (int l = 0; l < 5; ++l) {
+        if (tid == 0) tc_gemm(tmem, l == 0 ? Xc : Act[l - 1], l == 4 ? Wch : Wc[l], l == 0 ? kGuideIn : 64,
+                              l == 4 ? kHeadRowsPad : 64, false, 0, mbar);
+        ok = tc_wait(mbar, ph) && ok;
+        ph ^= 1u;
+        if (l < 4) {
+            float v[32];
+            tc_ld32(tl + 32u * chalf, v);
+            tc_store_row32(v, row, 32 * chalf, Act[l], nullptr);
+        } else if (warp < 4) {
+            // head gradient of the weighted loss, one thread per record, scaled into FP16 range
+            float hrow[kHeadRowsPad];
+            tc_ld32(tl, hrow);
+            tc_ld16(tl + 32u, hrow + 32);
+            float dh[kHeadRowsPad];
+#pragma unroll
+            for (int k = 0; k < kHeadRowsPad; ++k) dh[k] = 0.f;
+            float loss = 0.f;
+            if (rid[row] != ~0u) {
+                const float *R = T.rec + (size_t)rid[row] * kRecFloats;
+                const float wmean = T.wstat[0] / fmaxf(T.wstat[1], 1.f);
+                const float wr = record_weight(R);
+                const float wn = T.cdf ? (wr > 0.f ? 1.f : 0.f) : fminf(wr / wmean, kWeightClamp);
+                if (wn > 0.f) {
+                    const float nl = guide_head_grad(hrow, mk(R[7], R[8], R[9]), dh, record_bsdf_pdf(R), T.learned != 0);
+                    loss = wn * nl;
+#pragma unroll
+                    for (int k = 0; k < kGuideOut; ++k) dh[k] *= wn * kLossScale;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kHeadRowsPad / 8; ++q) {
+                uint32_t h[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int k = 8 * q + 2 * j;
+                    h[j] = k < kGuideOut + 1 ? pack_h2(dh[k], dh[k + 1], false) : 0u;
+                }
+                *reinterpret_cast<uint4 *>(DzA + tc_canon(row, 8 * q, kHeadRowsPad)) = make_uint4(h[0], h[1], h[2], h[3]);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
+            if (lane == 0 && loss != 0.f) atomicAdd(T.loss, loss);
+        }
+        tc_operands_written();
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    // backward: per level, the product dZ W on the tensor cores (issued first) and the
+    // weight gradient on mma.sync meanwhile; then the masked dZ of the layer below
+    const __half *dz = DzA;
+    __half *dzn = DzB;
+    for (int l = 4; l >= 1; --l) {
+        const int kz = l == 4 ? kHeadRowsPad : 64;  // width of this level's dZ
+        if (tid == 0) tc_gemm(tmem, dz, l == 4 ? Wch : Wc[l], kz, 64, true, 64, mbar);
+        tc_dw(Act[l - 1], 64, 4, dz, kz, l == 4 ? 6 : 8, T.grad + guide_woff(l), 64, guide_out(l));
+        ok = tc_wait(mbar, ph) && ok;
+        ph ^= 1u;
+        float v[32];
+        tc_ld32(tl + 32u * chalf, v);
+        tc_store_row32(v, row, 32 * chalf, dzn, Act[l - 1]);
+        tc_operands_written();
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const __half *t2 = dzn;
+        dzn = const_cast<__half *>(dz);
+        dz = t2;
+    }
+    tc_dw(Xc, kGuideIn, 5, dz, 64, 8, T.grad + guide_woff(0), kGuideIn, 64);
+    if (!ok && tid == 0 && T.err) atomicAdd(T.err, 1);
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
+}
+
+// one training step's forward + backward over the records of T, on the kernel the guide's
+// configuration names (fl_guide_config.train_kernel)
+static void launch_train(const TrainArgs &T, uint32_t blocks, cudaStream_t st, int kernel) {
+    if (kernel == FL_GUIDE_TRAIN_TCGEN05) k_guide_train_tc<<<blocks, 32 * kTrainWarps, kTrainSmemTc, st>>>(T);
+    else k_guide_train<<<blocks, 32 * kTrainWarps, kTrainSmem, st>>>(T);
+}
+
 // sum and count of the record weights of this wave (and the weights themselves, when asked)
 __global__ void k_guide_stats(const float *rec, const uint32_t *rec_count, uint32_t rec_cap, float *wstat,
                               float *weights) {
@@ -492,7 +790,8 @@ static fl_status guide_train(Guide *G, uint32_t n, const float bmin[3], const fl
         T.cdf = G->cdf;
         T.seed = (uint32_t)G->steps;
         T.learned = G->cfg.learn_select;
-        k_guide_train<<<(B + kTrainRows - 1) / kTrainRows, 32 * kTrainWarps, kTrainSmem, st>>>(T);
+        T.err = ctx->d_error;
+        launch_train(T, (B + kTrainRows - 1) / kTrainRows, st, G->cfg.train_kernel);
         G->steps += 1;
         AdamArgs a{};
         a.w32 = G->w32;
@@ -692,12 +991,14 @@ extern "C" fl_status fl_guide_create(fl_context *ctx_h, const fl_guide_config *c
     if (!(c.learning_rate > 0.f) || !(c.select_prob >= 0.f && c.select_prob < 1.f) || c.batch < 128 ||
         c.batch > 65536 || c.batch % 128 != 0 || c.max_records < c.batch || c.max_records > (1 << 26) ||
         c.steps_per_wave < 1 || !(c.position_scale >= 0.f && c.position_scale <= 1.f) ||
-        !(c.weight_average >= 0.f && c.weight_average < 1.f) || (c.learn_select != 0 && c.learn_select != 1)) {
+        !(c.weight_average >= 0.f && c.weight_average < 1.f) || (c.learn_select != 0 && c.learn_select != 1) ||
+        (c.train_kernel != FL_GUIDE_TRAIN_MMA_SYNC && c.train_kernel != FL_GUIDE_TRAIN_TCGEN05)) {
         set_error(ctx, "invalid guide configuration");
         return FL_ERR_INVALID;
     }
     FL_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     FL_CUDA_TRY(ctx, cudaFuncSetAttribute(k_guide_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
+    FL_CUDA_TRY(ctx, cudaFuncSetAttribute(k_guide_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmemTc));
     FL_CUDA_TRY(ctx, cudaFuncSetAttribute(k_guide_infer<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)guide_infer_smem_bytes()));
     FL_CUDA_TRY(ctx, cudaFuncSetAttribute(k_guide_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -932,7 +1233,8 @@ extern "C" fl_status fl_guide_gradient(fl_guide *g_h, const float *records, uint
         T.bmin[a] = bmin[a];
         T.binv[a] = binv[a];
     }
-    k_guide_train<<<(n + kTrainRows - 1) / kTrainRows, 32 * kTrainWarps, kTrainSmem, st>>>(T);
+    T.err = ctx->d_error;
+    launch_train(T, (n + kTrainRows - 1) / kTrainRows, st, G->cfg.train_kernel);
     FL_CUDA_TRY(ctx, cudaGetLastError());
     std::vector<float> g(kGuideParams);
     float l = 0.f;

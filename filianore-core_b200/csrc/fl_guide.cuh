@@ -154,8 +154,7 @@ __device__ inline void guide_stage_weights(__half *sw, const __half *__restrict_
 // to `row` + 40 * part. pn is the position normalised to [0, 1]^3. Feature 2 (12 a + k) + {0, 1}
 // is sin / cos(2^k pi pn[a]); both halves of a warp run the same loop over their 20
 // (axis, band) pairs, so the two parts do not serialise.
-__device__ inline void guide_encode_part(const float pn[3], const float nf[3], float lam01, int part, __half *row) {
-    uint32_t h[20];  // feature pairs as packed FP16
+__device__ inline void guide_encode_pairs(const float pn[3], const float nf[3], float lam01, int part, uint32_t h[20]) {
 #pragma unroll
     for (int i = 0; i < 20; ++i) {
         const int pair = 20 * part + i;  // (axis, band) = (pair / 12, pair % 12); pairs >= 36 are not sines
@@ -172,6 +171,10 @@ __device__ inline void guide_encode_part(const float pn[3], const float nf[3], f
         h[18] = pack_h2(1.f, 0.f, false);
         h[19] = 0u;
     }
+}
+__device__ inline void guide_encode_part(const float pn[3], const float nf[3], float lam01, int part, __half *row) {
+    uint32_t h[20];  // feature pairs as packed FP16
+    guide_encode_pairs(pn, nf, lam01, part, h);
     uint4 *dst = reinterpret_cast<uint4 *>(row + 40 * part);
 #pragma unroll
     for (int q = 0; q < 5; ++q) dst[q] = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);

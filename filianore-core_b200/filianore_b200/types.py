@@ -49,6 +49,8 @@ FL_SERVE_SHORTEST_FIRST_AGED = 3
 FL_SERVE_RESPONSE_RATIO = 4
 FL_SERVE_DEADLINE = 5
 FL_SERVE_FIRST_COME_LANE = 6
+FL_GUIDE_TRAIN_MMA_SYNC = 0
+FL_GUIDE_TRAIN_TCGEN05 = 1
 
 
 class fl_spectral_tables(C.Structure):
@@ -242,6 +244,7 @@ class fl_guide_config(C.Structure):
         ("position_scale", C.c_float),
         ("weight_average", C.c_float),
         ("learn_select", C.c_int32),
+        ("train_kernel", C.c_int32),
     ]
 
 

@@ -510,7 +510,13 @@ typedef struct {
                                 [0.2, 0.7], fitted with the mixture by minimising -log of the
                                 one-sample MIS density c q + (1 - c) p_bsdf; select_prob > 0 still
                                 switches guided sampling on. 0: c = select_prob everywhere */
+    int32_t train_kernel;    /* FL_GUIDE_TRAIN_*: the kernel of a training step (same gradients) */
 } fl_guide_config;
+
+enum {
+    FL_GUIDE_TRAIN_MMA_SYNC = 0,  /* warp-level mma.sync (the default: faster at 128 records per CTA) */
+    FL_GUIDE_TRAIN_TCGEN05 = 1    /* tcgen05.mma into TMEM for the 128-row products */
+};
 
 enum {
     FL_GUIDE_SAMPLE = 1,  /* sample continuations from the guide (one-sample MIS) */

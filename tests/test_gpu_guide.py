@@ -22,12 +22,14 @@ def ctx():
     c.close()
 
 
+@pytest.mark.parametrize("kernel", [fb.FL_GUIDE_TRAIN_MMA_SYNC, fb.FL_GUIDE_TRAIN_TCGEN05])
 @pytest.mark.parametrize("learned", [False, True])
-def test_gradient_matches_oracle(ctx, learned):
+def test_gradient_matches_oracle(ctx, learned, kernel):
     """FP16 tensor-core forward + backward against the oracle (same FP16 roundings, double
-    accumulation): relative L2 error of every layer's gradient below 1e-2; with the learned
-    selection probability, the loss of the one-sample MIS density as well."""
-    g = fb.Guide(ctx, max_records=8192, batch=1024, learn_select=learned)
+    accumulation), on the mma.sync training kernel and on the tcgen05 one: relative L2 error
+    of every layer's gradient below 1e-2; with the learned selection probability, the loss of
+    the one-sample MIS density as well."""
+    g = fb.Guide(ctx, max_records=8192, batch=1024, learn_select=learned, train_kernel=kernel)
     w = gr.weights(seed=11)
     g.set_weights(w)
     rec = gr.records(3000, seed=12)
