@@ -466,8 +466,8 @@ FL_API fl_status fl_server_get_stats(fl_server *srv, fl_server_stats *stats);
  * trigger the implicit device synchronisation of cudaMalloc). It has no counterpart in the
  * reference. It allocates nothing: no cudaMalloc/cudaFree, no events, no allocating library
  * call. The path state lives in a fixed 32 MiB device array inside the library (held by
- * every GPU that loads the library until exit); frames are rendered in waves that fit it,
- * and a scene whose per-path state cannot fit even a minimal wave is rejected with
+ * every GPU that loads the library until exit); frames stream through as many path slots as
+ * fit it, and a scene whose per-path state cannot fit even 128 slots is rejected with
  * FL_ERR_CAPACITY. film_rgb (width*height*3 floats) and film_xyz64 (width*height*3 doubles,
  * the FP64 XYZ sums, cleared by the call) are caller-owned DEVICE buffers. All calls share
  * the fixed array: calls whose GPU work overlaps race and give wrong images. The first call
