@@ -1454,11 +1454,39 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
 // Enqueues bounces [b_begin, b_end) of a wave on `st`. Bounce b reads the trace queue of
 // parity b (qa for even b) and appends survivors to the other one. Launch shapes do not
 // depend on the wave's content (kernels read their counts from device memory).
+// Blocks per SM of the grid-stride shading kernels: as many as are resident at once, so
+// that every block of a launch runs from the start (a grid of more blocks than fit leaves a
+// second, partial round of blocks that starts late and ends the launch alone).
+// FL_SHADE_GRID_OCC 0: 8 per SM whatever fits.
+#ifndef FL_SHADE_GRID_OCC
+#define FL_SHADE_GRID_OCC 1
+#endif
+struct ShadeShapes {
+    int shade, shade_std, cont, cont_std;
+};
+template <class K>
+inline int resident_blocks(K kernel) {
+    int b = 0;
+    if (!FL_SHADE_GRID_OCC || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 128, 0) != cudaSuccess || b <= 0) {
+        cudaGetLastError();
+        b = 8;
+    }
+    return b;
+}
+// computed on first use; call it before a stream capture of the bounces
+template <int NL, bool GUIDE>
+const ShadeShapes &shade_shapes() {
+    static const ShadeShapes s{resident_blocks(k_shade<NL>), resident_blocks(k_shade<NL, true>),
+                               resident_blocks(k_continue<NL, GUIDE>), resident_blocks(k_continue<NL, GUIDE, true>)};
+    return s;
+}
+
 template <int NL, bool GUIDE = false>
 void enqueue_bounces(const WaveBuffers &W, int b_begin, int b_end, bool count, RenderProfile *prof, int sms,
                      cudaStream_t st, bool standard, bool stream = false) {
     RenderArgs A = W.A;
-    const int g_trace = sms * 16, g_shade = sms * 8;
+    const ShadeShapes &sh = shade_shapes<NL, GUIDE>();
+    const int g_trace = sms * 16;
     for (int b = b_begin; b < b_end; ++b) {
         A.q_trace = (b & 1) ? W.qb : W.qa;
         A.q_next = (b & 1) ? W.qa : W.qb;
@@ -1478,8 +1506,8 @@ void enqueue_bounces(const WaveBuffers &W, int b_begin, int b_end, bool count, R
         else k_trace_paths<false><<<g_trace, 128, 0, st>>>(A);
         prof->mark(0, st);
         prof->mark(1, st);
-        k_shade<NL><<<g_shade, 128, 0, st>>>(A);
-        if (standard) k_shade<NL, true><<<g_shade, 128, 0, st>>>(A);
+        k_shade<NL><<<sms * sh.shade, 128, 0, st>>>(A);
+        if (standard) k_shade<NL, true><<<sms * sh.shade_std, 128, 0, st>>>(A);
         prof->mark(1, st);
         prof->mark(2, st);
         if (count) k_trace_rays2<true><<<g_trace, 128, 0, st>>>(A);
@@ -1492,8 +1520,8 @@ void enqueue_bounces(const WaveBuffers &W, int b_begin, int b_end, bool count, R
                 prof->launches += 1;
             }
         }
-        k_continue<NL, GUIDE><<<g_shade, 128, 0, st>>>(A);
-        if (standard) k_continue<NL, GUIDE, true><<<g_shade, 128, 0, st>>>(A);
+        k_continue<NL, GUIDE><<<sms * sh.cont, 128, 0, st>>>(A);
+        if (standard) k_continue<NL, GUIDE, true><<<sms * sh.cont_std, 128, 0, st>>>(A);
         prof->mark(3, st);
         prof->launches += standard ? 6 : 4;
     }
@@ -1616,6 +1644,7 @@ fl_status render_waves(Scene *s, const CamDev &cam, const fl_render_params &p, d
     // path (instantiating a graph allocates), when every launch is timed with events, nor by
     // fl_li (its small batches would replace the render's graph with one of their own size).
     const bool use_graph = !fixed_scratch && !prof->on && !li;
+    shade_shapes<NL, false>();  // launch shapes, outside any capture
     if (use_graph && (!ctx->wave_graph || ctx->graph_base != W.A.cnt || ctx->graph_cap != W.cap ||
                       ctx->graph_depth != kStreamIters || ctx->graph_nl_mode != NL || ctx->graph_count != (int)count ||
                       ctx->graph_std != (int)standard)) {

@@ -621,6 +621,7 @@ fl_status fl_server_create(fl_context *ctx_h, const fl_server_config *cfg, fl_se
     cudaMemsetAsync(S->W.d_wave, 0, offsetof(WaveDesc, seg), S->stream);
     cudaMemsetAsync(S->d_job_done, 0, sizeof(unsigned long long) * kMaxJobs, S->stream);
     k_stream_init<<<std::min<uint32_t>(((uint32_t)S->W.cap + 127) / 128, (uint32_t)sms * 8), 128, 0, S->stream>>>(S->W.A);
+    shade_shapes<4, false>();  // launch shapes, outside the capture
     // capture kServeIters streaming iterations once; the worker replays them
     RenderProfile prof;
     cudaGraph_t g = nullptr;
