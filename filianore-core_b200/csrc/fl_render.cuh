@@ -714,7 +714,7 @@ __global__ void __launch_bounds__(256) k_regen(RenderArgs A) {
     const uint32_t dst = A.cnt->regen_dst, base = A.cnt->regen_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __shared__ uint32_t wcnt[8];
-    uint32_t rank0 = off;  // rank of the first free slot of this round
+    uint32_t rank0 = off;  // rank of the first free slot of the next 256 slots
     const uint32_t c0 = blockIdx.x * kFreeChunk, c1 = min(c0 + kFreeChunk, A.cap);
     for (uint32_t r0 = c0; r0 < c1 && rank0 < nn; r0 += 256) {
         const uint32_t slot = r0 + threadIdx.x;
@@ -1456,7 +1456,7 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
 // depend on the wave's content (kernels read their counts from device memory).
 // Blocks per SM of the grid-stride shading kernels: as many as are resident at once, so
 // that every block of a launch runs from the start (a grid of more blocks than fit leaves a
-// second, partial round of blocks that starts late and ends the launch alone).
+// second, partial wave of blocks that starts late and ends the launch alone).
 // FL_SHADE_GRID_OCC 0: 8 per SM whatever fits.
 #ifndef FL_SHADE_GRID_OCC
 #define FL_SHADE_GRID_OCC 1
