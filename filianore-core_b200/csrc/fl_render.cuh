@@ -1451,9 +1451,6 @@ inline fl_status wave_buffers(Context *ctx, int NL, int nl, size_t cap_request, 
     return FL_OK;
 }
 
-// Enqueues bounces [b_begin, b_end) of a wave on `st`. Bounce b reads the trace queue of
-// parity b (qa for even b) and appends survivors to the other one. Launch shapes do not
-// depend on the wave's content (kernels read their counts from device memory).
 // Blocks per SM of the grid-stride shading kernels: as many as are resident at once, so
 // that every block of a launch runs from the start (a grid of more blocks than fit leaves a
 // second, partial wave of blocks that starts late and ends the launch alone).
@@ -1481,6 +1478,9 @@ const ShadeShapes &shade_shapes() {
     return s;
 }
 
+// Enqueues bounces [b_begin, b_end) of a wave on `st`. Bounce b reads the trace queue of
+// parity b (qa for even b) and appends survivors to the other one. Launch shapes do not
+// depend on the wave's content (kernels read their counts from device memory).
 template <int NL, bool GUIDE = false>
 void enqueue_bounces(const WaveBuffers &W, int b_begin, int b_end, bool count, RenderProfile *prof, int sms,
                      cudaStream_t st, bool standard, bool stream = false) {
