@@ -1479,8 +1479,10 @@ const ShadeShapes &shade_shapes() {
 }
 
 // Enqueues bounces [b_begin, b_end) of a wave on `st`. Bounce b reads the trace queue of
-// parity b (qa for even b) and appends survivors to the other one. Launch shapes do not
-// depend on the wave's content (kernels read their counts from device memory).
+// parity b (qa for even b) and appends survivors to the other one. With `stream` each is an
+// iteration of a streaming wave: it first starts new paths in the free slots (k_free_count,
+// k_stream_step, k_regen). Launch shapes do not depend on the wave's content (kernels read
+// their counts from device memory).
 template <int NL, bool GUIDE = false>
 void enqueue_bounces(const WaveBuffers &W, int b_begin, int b_end, bool count, RenderProfile *prof, int sms,
                      cudaStream_t st, bool standard, bool stream = false) {
